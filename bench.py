@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""SDOT serving benchmark: Newton solves/s and p50/p99 latency, batched vs the plain one-at-a-time GPU solve,
+every solve to max |m - nu| / nu <= 1e-8.
+
+Workload: the serving stream -- requests with Poisson arrivals, dimension 2 (70 %) or 3 (30 %), N log-uniform
+in [1e3, 2e5], Diracs uniform in the unit box, target uniform or a 4-gaussian mixture (50/50; centres
+U[0.2, 0.8]^d, sigma U[0.05, 0.15], equal masses, support clipped to the unit box), nu = 1/N.  Seeded
+synthetic inputs; a STEP is one slice of `--requests-per-step` requests of that stream.  Requests this build
+cannot solve (recorded in `config.skipped`) are left out of the stream before it is sliced.
+
+  value      solves/s of the batched engine (sdot_solve_batch) on a step's requests, inputs already resident
+             in HBM, CUDA events on the library's stream, max over ranks;
+  e2e        solves/s of the served stream (sdot_server_*: host buffers in and out, continuous batching),
+             arrivals at rate lambda = 2 x the plain solves/s, with p50 / p99 latency (arrival -> result);
+  plain_gpu  solves/s of the one-at-a-time GPU solve (sdot_solve per request, host buffers).
+
+Multi-GPU: replicas only (each rank owns its own slice of the stream, no collective on the data path).
+`--impl reference` times the CPU oracle (the restatement of the reference's algorithm) instead.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sdot-ffi_b200"))
+
+METRIC = "SDOT Newton solves/s + p50/p99 latency, batched vs plain GPU, mass err ≤1e-8"
+RTOL = 1e-8
+BYTES_PER_CELL = {2: 96.0, 3: 188.0}      # compulsory bytes of one cell per diagram (seed, weight, mass, centroid, upper facets)
+
+
+def request(seed, k):
+    """request k of the stream: (d, n, kind, gaussian params, arrival gap)"""
+    rng = np.random.default_rng([seed, k])
+    d = 2 if rng.uniform() < 0.7 else 3
+    n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e5)))))
+    gauss = rng.uniform() < 0.5
+    c = rng.uniform(0.2, 0.8, size=(4, d))
+    s = rng.uniform(0.05, 0.15, size=4)
+    return dict(k=k, d=d, n=n, gauss=gauss, c=c, s=s, gap=rng.exponential())
+
+
+def positions(seed, req):
+    return np.random.default_rng([seed, req["k"], 1]).uniform(size=(req["n"], req["d"]))
+
+
+def target_of(req):
+    import sdot
+    d = req["d"]
+    if req["gauss"]:
+        return sdot.SumOfGaussians(req["c"], req["s"], np.full(4, 0.25), support_box=(np.zeros(d), np.ones(d)))
+    return sdot.Box(nb_dims=d)
+
+
+def capabilities():
+    """which (d, gaussian) kinds this build solves, probed on a tiny diagram"""
+    import sdot
+    caps = {}
+    rng = np.random.default_rng(0)
+    for d in (2, 3):
+        for g in (False, True):
+            r = dict(d=d, gauss=g, c=rng.uniform(0.2, 0.8, size=(4, d)), s=np.full(4, 0.1))
+            try:
+                sdot.PowerDiagram(rng.uniform(size=(16, d)), distribution=target_of(r)).measures
+                caps[(d, g)] = True
+            except NotImplementedError:
+                caps[(d, g)] = False
+    return caps
+
+
+def stream(seed, count, probe):
+    out, skipped, k = [], 0, 0
+    while len(out) < count:
+        r = request(seed, k)
+        k += 1
+        if probe(r):
+            out.append(r)
+        else:
+            skipped += 1
+    return out, skipped
+
+
+def settings():
+    from sdot import Iterative, Tuning
+    return Iterative(tol=0.0, tuning=Tuning(mass_rtol=RTOL))
+
+
+# ---- clocks during a timed region ---------------------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ---- the GPU arm ---------------------------------------------------------------------------------------------------------
+def device_batch(reqs, seed, torch):
+    """the step's inputs resident on the device, and the descriptors pointing at them"""
+    import ctypes
+    from sdot import _lib
+    from sdot.PowerDiagram import _domain_box
+    from sdot.SdotPlanNd import solver_options
+    keep, descs, outs, h2d = [], (_lib.SolveDesc * len(reqs))(), (_lib.SolveOut * len(reqs))(), 0
+    opts = solver_options(settings(), 0)
+    for k, r in enumerate(reqs):
+        pos = torch.from_numpy(positions(seed, r)).cuda()
+        h2d += pos.numel() * 8
+        t = target_of(r).normalized_version(nb_dims=r["d"])
+        lo, hi = _domain_box(t.bounding_half_spaces(), r["d"])
+        dens = t._sdot_density()
+        dev = []
+        if dens[0] == "gauss":
+            arrs = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda() for a in dens[1:]]
+            dev = arrs
+            h2d += sum(a.numel() * 8 for a in arrs)
+        sd = _lib.SolveDesc()
+        sd.diagram.dim, sd.diagram.n = r["d"], r["n"]
+        sd.diagram.positions = pos.data_ptr()
+        sd.diagram.weights = None
+        for a in range(r["d"]):
+            sd.diagram.box_lo[a], sd.diagram.box_hi[a] = float(lo[a]), float(hi[a])
+        D = _lib.Density()
+        if dens[0] == "uniform":
+            D.kind, D.value = _lib.DENSITY_UNIFORM, float(dens[1])
+        else:
+            D.kind, D.count = _lib.DENSITY_GAUSSIANS, 4
+            D.centres, D.sigmas, D.masses = dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr()
+        sd.diagram.density = D
+        sd.diagram.memory = _lib.SDOT_DEVICE
+        sd.nu = None
+        for q, name in enumerate(_lib.OPTIONS):
+            sd.options[q] = float(opts[name])
+        descs[k] = sd
+        o = dict(w=torch.empty(r["n"], dtype=torch.float64, device="cuda"), m=torch.empty(r["n"], dtype=torch.float64, device="cuda"),
+                 b=torch.empty(r["n"] * r["d"], dtype=torch.float64, device="cuda"), c=torch.empty(1, dtype=torch.float64, device="cuda"))
+        so = _lib.SolveOut()
+        so.weights, so.masses, so.barycentres, so.cost = o["w"].data_ptr(), o["m"].data_ptr(), o["b"].data_ptr(), o["c"].data_ptr()
+        outs[k] = so
+        keep.append((pos, dev, o))
+    return descs, outs, keep, h2d
+
+
+def run_value_step(reqs, seed, torch, check):
+    """one timed step of the batched engine on device-resident inputs: (seconds, launches)"""
+    import ctypes
+    from sdot import _lib
+    L = _lib.load()
+    ctx = _lib.context()
+    descs, outs, keep, _ = device_batch(reqs, seed, torch)
+    stream = torch.cuda.ExternalStream(_lib.stream())
+    torch.cuda.synchronize()
+    l0 = _lib.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sts = (_lib.Status * len(reqs))()
+    code = L.sdot_solve_batch(ctx, len(reqs), descs, outs, sts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if code != 0:
+        raise RuntimeError(f"sdot_solve_batch: {[s.message for s in sts if s.code][:1]}")
+    secs = e0.elapsed_time(e1) / 1000
+    worst = 0.0
+    for r, (_, _, o), so in zip(reqs, keep, outs):
+        st = np.array(so.stats[:])
+        if check and st[0] != 1:
+            raise RuntimeError(f"request {r['k']} did not converge: status {st[0]}")
+        m = o["m"].cpu().numpy()
+        worst = max(worst, float(np.abs(m * r["n"] / st[12] - 1).max()) if st[12] > 0 else 1.0)
+    return secs, _lib.kernel_launches() - l0, worst
+
+
+def run_plain(reqs, seed):
+    """one-at-a-time GPU solves through the public API (host arrays): seconds, worst mass error"""
+    from sdot import OtProblem, SumOfDiracs
+    from sdot.SdotPlanNd import SdotPlanNd
+    t0 = time.perf_counter()
+    worst = 0.0
+    for r in reqs:
+        plan = OtProblem(SumOfDiracs(positions(seed, r)), target_of(r)).solve(settings())
+        worst = max(worst, float(np.abs(plan.cell_masses / plan.target_masses - 1).max()))
+    return time.perf_counter() - t0, worst
+
+
+def run_served(reqs, seed, lam):
+    """the stream through the server: arrivals at rate `lam`; returns (seconds, latencies, h2d, d2h, worst, counters)"""
+    from sdot.server import Server
+    pos = [positions(seed, r) for r in reqs]
+    tg = [target_of(r) for r in reqs]
+    gaps = np.array([r["gap"] for r in reqs]) / lam
+    arrivals = np.cumsum(gaps) - gaps[0]
+    h2d = sum(p.nbytes for p in pos) + sum(32 * 4 * (r["d"] + 2) if r["gauss"] else 0 for r in reqs)
+    d2h = sum(r["n"] * (2 + r["d"]) * 8 + 8 + 31 * 8 for r in reqs)
+    done, lat, worst = {}, [], [0.0]
+    with Server(max_active=0) as srv:
+        tickets = [None] * len(reqs)
+        start = time.perf_counter()
+
+        def collect():
+            for i in range(len(reqs)):
+                while tickets[i] is None:
+                    time.sleep(0.0002)
+                res = srv.result(tickets[i])
+                now = time.perf_counter() - start
+                done[i] = now
+                lat.append(now - arrivals[i])
+                st = res["stats"]
+                worst[0] = max(worst[0], float(np.abs(res["masses"] * reqs[i]["n"] / st[12] - 1).max()) if st[12] > 0 else 1.0)
+                if st[0] != 1:
+                    raise RuntimeError(f"served request {reqs[i]['k']} did not converge")
+
+        th = threading.Thread(target=collect)
+        th.start()
+        for i, r in enumerate(reqs):
+            wait = arrivals[i] - (time.perf_counter() - start)
+            if wait > 0:
+                time.sleep(wait)
+            tickets[i] = srv.submit(pos[i], tg[i], settings=settings())
+        th.join()
+        counters = srv.counters()
+    return max(done.values()), np.array(lat), h2d, d2h, worst[0], counters
+
+
+def cpu_sample(reqs, seed, budget_s=20.0):
+    """the oracle (CPU restatement) on the first requests of the stream until `budget_s` of CPU work"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    count, n_tot = 0, 0
+    for r in reqs:
+        t = target_of(r).normalized_version(nb_dims=r["d"])
+        dens = t._sdot_density()
+        od = ("uniform", dens[1]) if dens[0] == "uniform" else ("gauss", dens[1], dens[2], dens[3])
+        lo, hi = t.box() if hasattr(t, "box") else (np.zeros(r["d"]), np.ones(r["d"]))
+        s = O.solve(positions(seed, r), box=(lo, hi), density=od, tol_abs=0.0, tol_rel=RTOL, lin_tol=1e-8)
+        if s["stats"]["status"] != 1:
+            raise RuntimeError("the oracle did not converge")
+        count += 1
+        n_tot += r["n"]
+        if time.perf_counter() - t0 > budget_s:
+            break
+    secs = time.perf_counter() - t0
+    return dict(value=count / secs, unit="solves/s", cores=threads, kind="port",
+                sample=f"the first {count} requests of the same seeded stream (sum N = {n_tot}), oracle/sdot_oracle.c FP64 + OpenMP, "
+                       f"same tolerance; CPU restatement of sdot's algorithm, not the reference binary")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_of(kernel):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--requests-per-step", type=int, default=32)
+    ap.add_argument("--plain-requests", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cells-only", type=int, default=0, help="one 2D uniform diagram of this many seeds (for a profiler), then exit")
+    a = ap.parse_args()
+    if a.cells_only:
+        import sdot
+        pos = np.random.default_rng(a.seed).uniform(size=(a.cells_only, 2))
+        w = np.random.default_rng(a.seed + 1).uniform(0, 1.0 / a.cells_only, size=a.cells_only)
+        pd = sdot.PowerDiagram(pos, w, boundaries=sdot.box_half_spaces([0, 0], [1, 1]))
+        m = pd.facets()
+        print(f"cells-only: n={a.cells_only} facets/cell {m[0].mean():.3f}")
+        return
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    R = a.requests_per_step
+    config = {"workload": "serving stream: Poisson arrivals, d=2 (70%) / 3 (30%), N log-uniform [1e3, 2e5], uniform or 4-gaussian "
+                          "target (50/50), nu = 1/N, mass_rtol 1e-8",
+              "requests_per_step": R, "seed": a.seed, "parallelism": f"replicas{world}" if world > 1 else "single",
+              "l2": "inputs of a step (~R x 37k seeds x 1.2 KB of working set) exceed the 126 MB L2"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        reqs, skipped = stream(a.seed, (a.warmup + a.steps) * R, lambda r: True)
+        cpu = cpu_sample(reqs[a.warmup * R:], a.seed, budget_s=a.cpu_budget)
+        v = cpu["value"]
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                          "ms_per_step": 1000.0 / v if v else None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
+                          "cpu_baseline": dict(cpu, value=v), "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                                                      "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    os.environ["SDOT_DEVICE"] = str(torch.cuda.current_device())
+    from sdot import _lib
+
+    caps = capabilities()
+
+    def probe(r):
+        return caps[(r["d"], r["gauss"])]
+
+    total = (a.warmup + a.steps) * R * world
+    reqs, skipped = stream(a.seed, total, probe)
+    config["skipped"] = (f"{skipped} requests of kinds this build does not solve yet left out of the stream: "
+                         + ", ".join(f"{d}D {'gaussian' if g else 'uniform'}" for (d, g), ok in caps.items() if not ok)) if skipped else "none"
+    mine = reqs[rank::world]
+    warm, timed = mine[: a.warmup * R], mine[a.warmup * R:]
+
+    # warm-up steps (untimed)
+    for s in range(a.warmup):
+        run_value_step(warm[s * R:(s + 1) * R], a.seed, torch, check=True)
+
+    # the timed steps: batched engine, device-resident inputs
+    _lib.set_timing(True)
+    _lib.kernel_stats(reset=True)
+    secs, launches, worst = 0.0, 0, 0.0
+    with Clocks(torch.cuda.current_device()) as clk:
+        for s in range(a.steps):
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t, l, w = run_value_step(timed[s * R:(s + 1) * R], a.seed, torch, check=True)
+            secs += t
+            launches += l
+            worst = max(worst, w)
+    kst = _lib.kernel_stats()
+    _lib.set_timing(False)
+    if world > 1:
+        tt = torch.tensor([secs], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        secs = float(tt.item())
+    value = a.steps * R * world / secs
+
+    # plain one-at-a-time on a sample of the timed requests
+    pr = timed[: a.plain_requests]
+    p_secs, p_worst = run_plain(pr, a.seed)
+    plain = len(pr) / p_secs
+
+    # served stream, arrivals at twice the plain throughput
+    lam = 2.0 * plain
+    e_secs, lat, h2d, d2h, e_worst, counters = run_served(timed, a.seed, lam)
+    e2e = len(timed) / e_secs
+
+    hbm, peak_kind = peaks()
+    ms, nl, units = kst["cells2d"]
+    cells_b = units * BYTES_PER_CELL[2]
+    achieved = cells_b / (ms / 1000) / 1e9 if ms > 0 else None
+    cg_ms, cg_n, cg_rows = kst["cg"]
+    cpu = cpu_sample(timed, a.seed, a.cpu_budget) if rank == 0 else None
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000 * secs / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config,
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d // max(1, a.steps), "d2h_bytes_per_step": d2h // max(1, a.steps),
+                "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000), "lambda_per_s": lam,
+                "max_active": counters["max_active"], "worst_mass_rel_err": e_worst},
+        "plain_gpu": {"value": plain, "unit": "solves/s", "requests": len(pr), "worst_mass_rel_err": p_worst},
+        "e2e_over_plain": e2e / plain,
+        "worst_mass_rel_err": worst,
+        "roofline": {"bound": "hbm", "kernel": "cells2d (k_cells2d)", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if achieved else None, "traffic": traffic_of("k_cells2d"), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_cell": BYTES_PER_CELL[2], "cells_per_launch": units / max(nl, 1),
+                     "avg_launch_ms": ms / max(nl, 1), "cg_ms_share": cg_ms / max(1e-9, 1000 * secs),
+                     "cells_ms_share": ms / max(1e-9, 1000 * secs)},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

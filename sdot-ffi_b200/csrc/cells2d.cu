@@ -1,0 +1,575 @@
+// 2D Laguerre cells: ONE WARP PER CELL.
+//
+// The cell of seed i is the domain box clipped by the power bisectors of its neighbours.  It is held
+// across the warp: lane k owns vertex k (FP64, in the frame of the seed) and the line of edge k -> k+1
+// (`n . y <= off` with its cut id: a seed rank >= 0, or a box side -1 bottom, -2 right, -3 top,
+// -4 left -- the conventions of src/sdot/include/sdot/gpu/Cell2D.cuh:453-463).  A cut is a ballot of
+// the vertices outside, two line-line intersections and one shuffle permutation; every vertex is
+// always the intersection of its two lines, so no error accumulates along the cuts (the reference
+// re-solves its float vertices in FP64 for the same reason, Cell2D.cuh:991-1042).
+//
+// Candidates come from the Morton grid, ring by ring around the seed's grid cell; 32 candidates are
+// loaded at a time and pre-tested in parallel (lane l tests candidate l against every vertex), so only
+// the candidates that do cut go through the serial clip.  The walk stops by the SECURITY RADIUS: every
+// unvisited seed q is at least `r h` away, and cannot cut the cell once
+//     r h >= R + sqrt( max( 0, R^2 + w_max - w_i ) ),    R = max_k |v_k|.
+//
+// Integration is a warp reduction over the edges: the shoelace terms for a constant density; for an
+// image, Green's theorem on rows (mass = closed integral of F dy, F = int rho dx, the edges walked pixel
+// by pixel from row prefix sums, cf. gpu/Density2D.cuh:16-26 for the reference's use of the same
+// identity); for gaussians the same identity with F in closed form (erf), Gauss-Legendre along the edge.
+#include "internal.h"
+
+namespace sdot {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- the density along one edge (seed frame) ------------------------------------------------------------
+struct EdgeInt {
+    double m, fx, fy, s2, meas, mx, my;   // mass, first moments, second moment, int_edge rho, int_edge x rho
+};
+
+__device__ __forceinline__ void isect( double a1, double b1, double c1, double a2, double b2, double c2, double &x, double &y, bool &ok ) {
+    double det = a1 * b2 - a2 * b1;
+    double sc = ( fabs( a1 ) + fabs( b1 ) ) * ( fabs( a2 ) + fabs( b2 ) );
+    ok = fabs( det ) > 1e-13 * sc;
+    double inv = 1.0 / det;
+    x = ( c1 * b2 - c2 * b1 ) * inv;
+    y = ( a1 * c2 - a2 * c1 ) * inv;
+}
+
+// uniform density: the shoelace terms of the edge (x0,y0)->(x1,y1)
+__device__ __forceinline__ void edge_uniform( double x0, double y0, double x1, double y1, double rho, bool moments, EdgeInt &e ) {
+    double c = x0 * y1 - x1 * y0;
+    e.m = rho * c * 0.5;
+    if ( moments ) {
+        e.fx = rho * ( x0 + x1 ) * c / 6;
+        e.fy = rho * ( y0 + y1 ) * c / 6;
+        e.s2 = rho * c * ( x0 * x0 + x0 * x1 + x1 * x1 + y0 * y0 + y0 * y1 + y1 * y1 ) / 12;
+    }
+    double len = sqrt( ( x1 - x0 ) * ( x1 - x0 ) + ( y1 - y0 ) * ( y1 - y0 ) );
+    e.meas = rho * len;
+    e.mx = rho * len * 0.5 * ( x0 + x1 );
+    e.my = rho * len * 0.5 * ( y0 + y1 );
+}
+
+// image: F(x, y) = int_{X_ref}^{x} rho(t, y) dt along each piece of the edge inside one pixel
+__device__ void edge_image( const ProbDev &P, double px, double py, int iref, double x0, double y0, double x1, double y1, bool moments,
+                            EdgeInt &e ) {
+    const int nx = P.dn[ 0 ], ny = P.dn[ 1 ];
+    const double hx = P.dstep[ 0 ], hy = P.dstep[ 1 ];
+    const double X0 = P.dorg[ 0 ] - px, Y0 = P.dorg[ 1 ] - py;      // pixel (0, 0) corner, seed frame
+    double dx = x1 - x0, dy = y1 - y0;
+    double len = sqrt( dx * dx + dy * dy );
+    e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+    if ( len == 0 ) return;
+    // next crossing parameters of the vertical / horizontal pixel lines
+    double tx = 2, ty = 2, stx = 0, sty = 0;
+    int kx = 0, ky = 0, ddx = 0, ddy = 0;
+    if ( dx != 0 ) {
+        double f = ( x0 - X0 ) / hx;
+        kx = dx > 0 ? int( floor( f ) ) + 1 : int( ceil( f ) ) - 1;
+        ddx = dx > 0 ? 1 : -1;
+        tx = ( X0 + kx * hx - x0 ) / dx;
+        stx = hx / fabs( dx );
+    }
+    if ( dy != 0 ) {
+        double f = ( y0 - Y0 ) / hy;
+        ky = dy > 0 ? int( floor( f ) ) + 1 : int( ceil( f ) ) - 1;
+        ddy = dy > 0 ? 1 : -1;
+        ty = ( Y0 + ky * hy - y0 ) / dy;
+        sty = hy / fabs( dy );
+    }
+    const double *pre = P.dpre;
+    const int irc = iref < 0 ? 0 : ( iref > nx ? nx : iref );
+    double t0 = 0;
+    for ( int guard = 0; guard < 4 * ( nx + ny ) + 8; ++guard ) {
+        double t1 = fmin( 1.0, fmin( tx, ty ) );
+        if ( t1 > t0 ) {
+            double tm = 0.5 * ( t0 + t1 );
+            int i = int( floor( ( x0 + tm * dx - X0 ) / hx ) ), j = int( floor( ( y0 + tm * dy - Y0 ) / hy ) );
+            if ( j >= 0 && j < ny ) {
+                double xa = x0 + t0 * dx, ya = y0 + t0 * dy, xb = x0 + t1 * dx, yb = y0 + t1 * dy;
+                double v = ( i >= 0 && i < nx ) ? P.dval[ ( size_t ) i * ny + j ] : 0.0;
+                int ic = i < 0 ? 0 : ( i > nx ? nx : i );
+                const double *row = pre + ( size_t ) j * ( nx + 1 );
+                double Xi = X0 + i * hx;
+                double C = row[ ic ] - row[ irc ];                   // int_{X_ref}^{X_i} rho
+                double Fa = C + v * ( xa - Xi ), Fb = C + v * ( xb - Xi );
+                double Dy = yb - ya;
+                e.m += Dy * 0.5 * ( Fa + Fb );
+                double pl = ( t1 - t0 ) * len;
+                e.meas += v * pl;
+                e.mx += v * pl * 0.5 * ( xa + xb );
+                e.my += v * pl * 0.5 * ( ya + yb );
+                if ( moments ) {
+                    // G = int_{X_ref}^{x} t rho dt and H = int t^2 rho dt (seed frame), prefixes summed locally
+                    double Cg = 0, Ch = 0;
+                    int lo = i < iref ? i : iref, hi = i < iref ? iref : i;
+                    for ( int k = lo; k < hi; ++k ) {
+                        double vk = ( k >= 0 && k < nx ) ? P.dval[ ( size_t ) k * ny + j ] : 0.0;
+                        double a = X0 + k * hx, b = a + hx;
+                        Cg += vk * ( b * b - a * a ) * 0.5;
+                        Ch += vk * ( b * b * b - a * a * a ) / 3;
+                    }
+                    if ( i < iref ) { Cg = -Cg; Ch = -Ch; }
+                    e.fx += Dy * ( Cg - v * Xi * Xi * 0.5 + v * ( xa * xa + xa * xb + xb * xb ) / 6 );
+                    e.fy += Dy * ( Fa * ( 2 * ya + yb ) + Fb * ( ya + 2 * yb ) ) / 6;
+                    e.s2 += Dy * ( Ch - v * Xi * Xi * Xi / 3 + v * ( xa * xa * xa + xa * xa * xb + xa * xb * xb + xb * xb * xb ) / 12 );
+                    e.s2 += Dy * ( Fa * ( 3 * ya * ya + 2 * ya * yb + yb * yb ) + Fb * ( ya * ya + 2 * ya * yb + 3 * yb * yb ) ) / 12;
+                }
+            }
+        }
+        if ( t1 >= 1.0 ) break;
+        t0 = t1;
+        if ( tx <= ty ) { tx += stx; kx += ddx; } else { ty += sty; ky += ddy; }
+    }
+}
+
+// gaussians: F(x, y) = int_{0}^{x} g(t, y) dt (seed frame, reference at the seed), Gauss-Legendre along the edge
+__constant__ double c_glx[ 8 ] = { -0.9602898564975363, -0.7966664774136267, -0.5255324099163290, -0.1834346424956498,
+                                    0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363 };
+__constant__ double c_glw[ 8 ] = { 0.1012285362903763, 0.2223810344533745, 0.3137066458778873, 0.3626837833783620,
+                                    0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763 };
+
+// erf( b ) - erf( a ) without cancellation in the tails
+__device__ __forceinline__ double erf_diff( double a, double b ) {
+    if ( a >= 0 && b >= 0 ) return erfc( a ) - erfc( b );
+    if ( a <= 0 && b <= 0 ) return erfc( -b ) - erfc( -a );
+    return erf( b ) - erf( a );
+}
+
+__device__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments, EdgeInt &e ) {
+    e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+    double dx = x1 - x0, dy = y1 - y0, len = sqrt( dx * dx + dy * dy );
+    if ( len == 0 ) return;
+    const int ng = P.dn[ 0 ];
+    const double r2 = 1.4142135623730951;
+    for ( int g = 0; g < ng; ++g ) {
+        const double *G = P.dval + g * 4;
+        double cx = G[ 0 ] - px, cy = G[ 1 ] - py, sg = G[ 2 ], mg = G[ 3 ];
+        double K = mg / ( 2 * M_PI * sg * sg ), s2g = sg * sg, sq = sg * r2;
+        double E0 = sg * 1.2533141373155003;              // sigma sqrt( pi / 2 )
+        double u0 = ( 0 - cx ) / sq;                       // reference abscissa: the seed
+        double e0 = exp( -( cx * cx ) / ( 2 * s2g ) );
+        // the facet measure: closed form
+        {
+            double ux = dx / len, uy = dy / len;
+            double sa = ( x0 - cx ) * ux + ( y0 - cy ) * uy, sb = sa + len;
+            double fx = x0 - sa * ux - cx, fy = y0 - sa * uy - cy;
+            double h2 = fx * fx + fy * fy;
+            double span = erf_diff( sa / sq, sb / sq );
+            double mm = K * exp( -h2 / ( 2 * s2g ) ) * E0 * span;
+            e.meas += mm;
+            // int_edge x rho ds: x = x0 + ux ( s - sa ); int s g ds closed form
+            double ea = exp( -sa * sa / ( 2 * s2g ) ), eb = exp( -sb * sb / ( 2 * s2g ) );
+            double ms = K * exp( -h2 / ( 2 * s2g ) ) * s2g * ( ea - eb );     // int s g ds
+            e.mx += ( x0 - ux * sa ) * mm + ux * ms;
+            e.my += ( y0 - uy * sa ) * mm + uy * ms;
+        }
+        // the closed integral, split so that each piece spans at most one sigma
+        int np = int( len / sg ) + 1;
+        if ( np > 64 ) np = 64;
+        for ( int p = 0; p < np; ++p ) {
+            double ta = double( p ) / np, tb = double( p + 1 ) / np;
+            double xa = x0 + ta * dx, ya = y0 + ta * dy, xb = x0 + tb * dx, yb = y0 + tb * dy;
+            double Dy = yb - ya;
+            if ( Dy == 0 ) continue;
+            double am = 0, afx = 0, afy = 0, as2 = 0;
+            for ( int q = 0; q < 8; ++q ) {
+                double t = 0.5 + 0.5 * c_glx[ q ], wq = 0.5 * c_glw[ q ];
+                double x = xa + t * ( xb - xa ), y = ya + t * ( yb - ya );
+                double ey = K * exp( -( y - cy ) * ( y - cy ) / ( 2 * s2g ) );
+                double u = ( x - cx ) / sq;
+                double F = ey * E0 * erf_diff( u0, u );
+                am += wq * F;
+                if ( moments ) {
+                    double ex = exp( -( x - cx ) * ( x - cx ) / ( 2 * s2g ) );
+                    // int_0^x t g dt = cx F - sigma^2 ey ( ex - e0 )
+                    double F1 = cx * F - s2g * ey * ( ex - e0 );
+                    // int_0^x t^2 g dt, with t = ( t - cx ) + cx
+                    double A = ey * ( s2g * E0 * erf_diff( u0, u ) - s2g * ( ( x - cx ) * ex - ( 0 - cx ) * e0 ) );
+                    double F2 = A + 2 * cx * ( -s2g * ey * ( ex - e0 ) ) + cx * cx * F;
+                    afx += wq * F1;
+                    afy += wq * y * F;
+                    as2 += wq * ( F2 + y * y * F );
+                }
+            }
+            e.m += Dy * am;
+            if ( moments ) { e.fx += Dy * afx; e.fy += Dy * afy; e.s2 += Dy * as2; }
+        }
+    }
+}
+
+// ---- the warp-held polygon ----------------------------------------------------------------------------------
+struct WPoly {
+    int m;                     // vertex count (warp uniform)
+    double vx, vy;             // vertex `lane`
+    double lnx, lny, loff;     // line of edge lane -> lane + 1
+    int lid;
+};
+
+// keep n . y <= off; false past 32 vertices
+__device__ __forceinline__ bool wclip( WPoly &C, int lane, double nx, double ny, double off, int id ) {
+    const int m = C.m;
+    double s = nx * C.vx + ny * C.vy - off;
+    unsigned out = __ballot_sync( FULL, lane < m && s > 0 );
+    if ( ! out ) return true;
+    unsigned valid = m >= 32 ? FULL : ( ( 1u << m ) - 1 );
+    if ( out == valid ) { C.m = 0; return true; }
+    unsigned in = valid & ~out;
+    unsigned rot_out = ( ( out >> 1 ) | ( out << ( m - 1 ) ) ) & valid;
+    unsigned rot_in = ( ( in >> 1 ) | ( in << ( m - 1 ) ) ) & valid;
+    unsigned A = in & rot_out, B = out & rot_in;
+    int a = __ffs( A ) - 1;
+    unsigned Bafter = a >= 31 ? 0u : ( B & ~( ( 2u << a ) - 1 ) );
+    int b = Bafter ? __ffs( Bafter ) - 1 : __ffs( B ) - 1;
+    int K = ( ( a - b - 1 ) % m + m ) % m + 1;
+    if ( K + 2 > 32 ) return false;
+    // the new vertices: line[a] ^ L and L ^ line[b]; near-parallel lines fall back on the edge interpolation
+    int a1 = a + 1 == m ? 0 : a + 1, b1 = b + 1 == m ? 0 : b + 1;
+    double anx = __shfl_sync( FULL, C.lnx, a ), any = __shfl_sync( FULL, C.lny, a ), aoff = __shfl_sync( FULL, C.loff, a );
+    double bnx = __shfl_sync( FULL, C.lnx, b ), bny = __shfl_sync( FULL, C.lny, b ), boff = __shfl_sync( FULL, C.loff, b );
+    int bid = __shfl_sync( FULL, C.lid, b );
+    double xa = __shfl_sync( FULL, C.vx, a ), ya = __shfl_sync( FULL, C.vy, a ), sa = __shfl_sync( FULL, s, a );
+    double xa1 = __shfl_sync( FULL, C.vx, a1 ), ya1 = __shfl_sync( FULL, C.vy, a1 ), sa1 = __shfl_sync( FULL, s, a1 );
+    double xb = __shfl_sync( FULL, C.vx, b ), yb = __shfl_sync( FULL, C.vy, b ), sb = __shfl_sync( FULL, s, b );
+    double xb1 = __shfl_sync( FULL, C.vx, b1 ), yb1 = __shfl_sync( FULL, C.vy, b1 ), sb1 = __shfl_sync( FULL, s, b1 );
+    double Px, Py, Qx, Qy;
+    bool okP, okQ;
+    isect( anx, any, aoff, nx, ny, off, Px, Py, okP );
+    isect( nx, ny, off, bnx, bny, boff, Qx, Qy, okQ );
+    if ( ! okP ) { double t = sa / ( sa - sa1 ); Px = xa + t * ( xa1 - xa ); Py = ya + t * ( ya1 - ya ); }
+    if ( ! okQ ) { double t = sb / ( sb - sb1 ); Qx = xb + t * ( xb1 - xb ); Qy = yb + t * ( yb1 - yb ); }
+    int src = ( b + 1 + lane ) % m;
+    double nvx = __shfl_sync( FULL, C.vx, src ), nvy = __shfl_sync( FULL, C.vy, src );
+    double nlx = __shfl_sync( FULL, C.lnx, src ), nly = __shfl_sync( FULL, C.lny, src ), nlo = __shfl_sync( FULL, C.loff, src );
+    int nli = __shfl_sync( FULL, C.lid, src );
+    if ( lane == K ) { nvx = Px; nvy = Py; nlx = nx; nly = ny; nlo = off; nli = id; }
+    if ( lane == K + 1 ) { nvx = Qx; nvy = Qy; nlx = bnx; nly = bny; nlo = boff; nli = bid; }
+    C.vx = nvx; C.vy = nvy; C.lnx = nlx; C.lny = nly; C.loff = nlo; C.lid = nli;
+    C.m = K + 2;
+    return true;
+}
+
+__device__ __forceinline__ void ring_offset( int r, int ci, int &dx, int &dy ) {
+    if ( r == 0 ) { dx = dy = 0; return; }
+    int side = ci / ( 2 * r ), t = ci % ( 2 * r );
+    if ( side == 0 ) { dx = -r + t; dy = -r; }
+    else if ( side == 1 ) { dx = r; dy = -r + t; }
+    else if ( side == 2 ) { dx = r - t; dy = r; }
+    else { dx = -r; dy = r - t; }
+}
+
+__device__ __forceinline__ void record_error( ErrRec *err, int code, int prob, int seed, int needed ) {
+    if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
+}
+
+// per-warp accumulators of the Newton report (lane 0 holds them)
+struct Rep {
+    double v[ NB_REPORT ];
+    SDOT_DEV void init() {
+        v[ R_WORST ] = 0; v[ R_WORST_REL ] = 0; v[ R_AMIN ] = 1e300; v[ R_ASUM ] = 0; v[ R_LIN2 ] = 0;
+        v[ R_GCOUNT ] = 0; v[ R_GMEAN ] = 0; v[ R_GM2 ] = 0; v[ R_SU ] = 0; v[ R_SUG ] = 0; v[ R_NUSUM ] = 0; v[ R_NEMPTY ] = 0;
+    }
+    SDOT_DEV void combine( const double *o ) {   // Chan's parallel combination for the mean / M2 of g
+        v[ R_WORST ] = fmax( v[ R_WORST ], o[ R_WORST ] );
+        v[ R_WORST_REL ] = fmax( v[ R_WORST_REL ], o[ R_WORST_REL ] );
+        v[ R_AMIN ] = fmin( v[ R_AMIN ], o[ R_AMIN ] );
+        v[ R_ASUM ] += o[ R_ASUM ];
+        v[ R_LIN2 ] += o[ R_LIN2 ];
+        double na = v[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
+        if ( nb > 0 ) {
+            double d = o[ R_GMEAN ] - v[ R_GMEAN ];
+            v[ R_GMEAN ] += d * nb / n;
+            v[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
+            v[ R_GCOUNT ] = n;
+        }
+        v[ R_SU ] += o[ R_SU ];
+        v[ R_SUG ] += o[ R_SUG ];
+        v[ R_NUSUM ] += o[ R_NUSUM ];
+        v[ R_NEMPTY ] += o[ R_NEMPTY ];
+    }
+};
+
+__device__ __forceinline__ double g_of( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return p == 0 ? log( x ) : ( pow( x, p ) - 1 ) / p;
+    return r == 1 ? log( x ) : x - 1;
+}
+__device__ __forceinline__ double gp_of( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return pow( x, p - 1 );
+    return r == 1 ? 1 / x : 1;
+}
+
+// the report of one problem's chunk, written by its block; the last block of the problem folds them in order
+__device__ void finish_report( const ProbDev &P, const Chunk &ch, Rep &warp_rep, double ( *sh )[ NB_REPORT ] ) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int am_last;
+    if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh[ warp ][ k ] = warp_rep.v[ k ];
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        Rep r;
+        r.init();
+        for ( int w = 0; w < int( blockDim.x >> 5 ); ++w ) r.combine( sh[ w ] );
+        double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
+        for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r.v[ k ];
+        __threadfence();
+        unsigned prev = atomicAdd( P.counter, 1u );
+        am_last = prev == unsigned( P.nchunk - 1 );
+    }
+    __syncthreads();
+    if ( am_last && threadIdx.x == 0 ) {
+        __threadfence();
+        Rep r;
+        r.init();
+        for ( int c = 0; c < P.nchunk; ++c ) {
+            double o[ NB_REPORT ];
+            const volatile double *src = P.partials + ( size_t ) c * NB_REPORT;
+            for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ k ];
+            r.combine( o );
+        }
+        for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r.v[ k ];
+        *P.counter = 0;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+                                                    unsigned flags, ErrRec *err ) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    __shared__ double sh_rep[ 8 ][ NB_REPORT ];
+    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+    for ( int c = blockIdx.x; c < nchunks; c += gridDim.x ) {
+        const Chunk ch = chunks[ c ];
+        const ProbDev &P = probs[ ch.prob ];
+        Rep rep;
+        rep.init();
+        const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
+        for ( int s = ch.begin + warp; s < ch.end; s += nwarps ) {
+            const double px = P.pos[ 2 * ( size_t ) s ], py = P.pos[ 2 * ( size_t ) s + 1 ];
+            const double wi = P.w ? P.w[ s ] : 0.0;
+            WPoly C;
+            C.m = 4;
+            {
+                double lx = P.lo[ 0 ] - px, ly = P.lo[ 1 ] - py, hx = P.hi[ 0 ] - px, hy = P.hi[ 1 ] - py;
+                C.vx = ( lane == 1 || lane == 2 ) ? hx : lx;
+                C.vy = ( lane >= 2 ) ? hy : ly;
+                C.lnx = lane == 1 ? 1.0 : ( lane == 3 ? -1.0 : 0.0 );
+                C.lny = lane == 0 ? -1.0 : ( lane == 2 ? 1.0 : 0.0 );
+                C.loff = lane == 0 ? -ly : ( lane == 1 ? hx : ( lane == 2 ? hy : -lx ) );
+                C.lid = -1 - lane;
+            }
+            bool overflow = false;
+            // ---- the walk over the grid rings
+            const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
+            int cx = int( floor( ( px - P.go[ 0 ] ) / P.gh[ 0 ] ) ), cy = int( floor( ( py - P.go[ 1 ] ) / P.gh[ 1 ] ) );
+            cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
+            cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
+            int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
+            for ( int r = 0; r <= rmax && C.m > 0 && ! overflow; ++r ) {
+                const int ncell = r == 0 ? 1 : 8 * r;
+                for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
+                    int ci = cb + lane, beg = 0, cnt = 0;
+                    if ( ci < ncell ) {
+                        int dx, dy;
+                        ring_offset( r, ci, dx, dy );
+                        int x = cx + dx, y = cy + dy;
+                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
+                            int2 rg = P.cell_range[ ( size_t ) y * g0 + x ];
+                            beg = rg.x;
+                            cnt = rg.y - rg.x;
+                        }
+                    }
+                    int inc = cnt;
+#pragma unroll
+                    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL, inc, o ); if ( lane >= o ) inc += t; }
+                    const int total = __shfl_sync( FULL, inc, 31 );
+                    const int exc = inc - cnt;
+                    for ( int t0 = 0; t0 < total && C.m > 0 && ! overflow; t0 += 32 ) {
+                        const int t = t0 + lane;
+                        int owner = 0;
+#pragma unroll
+                        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
+                        owner = owner > 31 ? 31 : owner;
+                        int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
+                        int j = obeg + ( t - oexc );
+                        bool valid = t < total && j != s;
+                        double qx = 0, qy = 0, off = 0;
+                        if ( valid ) {
+                            qx = P.pos[ 2 * ( size_t ) j ] - px;
+                            qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
+                            double qw = P.w ? P.w[ j ] : 0.0;
+                            off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+                        }
+                        // the parallel pre-test: does candidate `lane` cut the current polygon at all?
+                        bool cuts = false;
+                        for ( int k = 0; k < C.m; ++k ) {
+                            double X = __shfl_sync( FULL, C.vx, k ), Y = __shfl_sync( FULL, C.vy, k );
+                            cuts |= qx * X + qy * Y > off;
+                        }
+                        unsigned todo = __ballot_sync( FULL, valid && cuts );
+                        while ( todo ) {
+                            int k = __ffs( todo ) - 1;
+                            todo &= todo - 1;
+                            double nx = __shfl_sync( FULL, qx, k ), ny = __shfl_sync( FULL, qy, k ), no = __shfl_sync( FULL, off, k );
+                            int nid = __shfl_sync( FULL, j, k );
+                            if ( ! wclip( C, lane, nx, ny, no, nid ) ) { overflow = true; break; }
+                            if ( C.m == 0 ) break;
+                        }
+                    }
+                }
+                if ( C.m == 0 || overflow ) break;
+                double R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
+                double ex = R2 + wmax - wi;
+                if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+            }
+            const int user = P.user[ s ];
+            if ( overflow ) {
+                if ( lane == 0 ) record_error( err, 4, ch.prob, user, 33 );
+                C.m = 0;
+            }
+            // ---- integration over the edges
+            const int m = C.m;
+            const bool act = lane < m;
+            int nxt = lane + 1 >= m ? 0 : lane + 1;
+            double x1 = __shfl_sync( FULL, C.vx, nxt ), y1 = __shfl_sync( FULL, C.vy, nxt );
+            EdgeInt e;
+            e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+            if ( act ) {
+                if ( P.dkind == D_UNIFORM ) edge_uniform( C.vx, C.vy, x1, y1, P.rho, moments, e );
+                else if ( P.dkind == D_IMAGE ) {
+                    int iref = int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) );
+                    edge_image( P, px, py, iref, C.vx, C.vy, x1, y1, moments, e );
+                } else edge_gauss( P, px, py, C.vx, C.vy, x1, y1, moments, e );
+            }
+            double mass = warp_sum( e.m );
+            if ( mass < 0 && mass > -1e-300 ) mass = 0;
+            // facets
+            bool fac = act && C.lid >= 0 && e.meas > 0;
+            unsigned fmask = __ballot_sync( FULL, fac );
+            int nf = __popc( fmask );
+            if ( facets && nf > P.cap ) {
+                if ( lane == 0 ) record_error( err, 4, ch.prob, user, nf );
+                fmask = 0;
+                nf = 0;
+            }
+            double dist = sqrt( C.lnx * C.lnx + C.lny * C.lny );
+            double cij = fac ? e.meas / ( 2 * dist ) : 0.0;
+            if ( facets ) {
+                const int row = user_order ? user : s;
+                if ( fac && nf ) {
+                    int slot = __popc( fmask & ( ( 1u << lane ) - 1 ) );
+                    size_t at = ( size_t ) row * P.cap + slot;
+                    P.nid[ at ] = user_order ? P.user[ C.lid ] : C.lid;
+                    P.nc[ at ] = cij;
+                    if ( P.nm ) P.nm[ at ] = e.meas;
+                }
+                if ( lane == 0 ) P.nb[ row ] = nf;
+            }
+            if ( flags & F_VJP ) {
+                // grad_w_i = sum_j c_ij ( g_i - g_j ); grad_p_i = sum_j 2 c_ij ( g_i - g_j ) ( x_ij - p_i )
+                double gi = P.gm[ user_order ? user : s ];
+                double gw = 0, gpx = 0, gpy = 0;
+                if ( fac ) {
+                    double gj = P.gm[ user_order ? P.user[ C.lid ] : C.lid ];
+                    double dg = gi - gj;
+                    gw = cij * dg;
+                    double cxm = e.mx / e.meas, cym = e.my / e.meas;      // facet centroid, seed frame
+                    gpx = 2 * cij * dg * cxm;
+                    gpy = 2 * cij * dg * cym;
+                }
+                gw = warp_sum( gw ); gpx = warp_sum( gpx ); gpy = warp_sum( gpy );
+                if ( lane == 0 ) {
+                    int row = user_order ? user : s;
+                    if ( P.gw ) P.gw[ row ] = gw;
+                    if ( P.gpos ) { P.gpos[ 2 * ( size_t ) row ] = gpx; P.gpos[ 2 * ( size_t ) row + 1 ] = gpy; }
+                }
+            }
+            if ( moments ) {
+                double fx = warp_sum( e.fx ), fy = warp_sum( e.fy ), s2 = warp_sum( e.s2 );
+                if ( lane == 0 ) {
+                    if ( user_order ) {
+                        if ( P.first ) {
+                            P.first[ 2 * ( size_t ) user ] = mass > 0 ? px + fx / mass : px;
+                            P.first[ 2 * ( size_t ) user + 1 ] = mass > 0 ? py + fy / mass : py;
+                        }
+                        if ( P.cost ) P.cost[ user ] = s2;
+                    } else {
+                        if ( P.first ) { P.first[ 2 * ( size_t ) s ] = fx; P.first[ 2 * ( size_t ) s + 1 ] = fy; }
+                        if ( P.cost ) P.cost[ s ] = s2;
+                    }
+                }
+            }
+            if ( lane == 0 && P.mass ) P.mass[ user_order ? user : s ] = mass;
+            if ( ( flags & F_REPORT ) && lane == 0 ) {
+                double nu = P.nu[ s ];
+                double e2 = fabs( nu - mass );
+                rep.v[ R_WORST ] = fmax( rep.v[ R_WORST ], e2 );
+                rep.v[ R_WORST_REL ] = fmax( rep.v[ R_WORST_REL ], e2 / nu );
+                rep.v[ R_AMIN ] = fmin( rep.v[ R_AMIN ], mass );
+                rep.v[ R_ASUM ] += mass;
+                rep.v[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
+                double x = mass / nu, g = g_of( x, P.res, P.power );
+                double n1 = rep.v[ R_GCOUNT ] + 1, d = g - rep.v[ R_GMEAN ];
+                rep.v[ R_GMEAN ] += d / n1;
+                rep.v[ R_GM2 ] += d * ( g - rep.v[ R_GMEAN ] );
+                rep.v[ R_GCOUNT ] = n1;
+                double u = nu / gp_of( x, P.res, P.power );
+                rep.v[ R_SU ] += u;
+                rep.v[ R_SUG ] += u * g;
+                rep.v[ R_NUSUM ] += nu;
+                rep.v[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
+            }
+        }
+        if ( flags & F_REPORT ) finish_report( P, ch, rep, sh_rep );
+    }
+}
+
+// the Newton report alone, from masses and targets already in memory (after a rescale of the targets)
+__global__ void __launch_bounds__( 256 ) k_report( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks ) {
+    __shared__ double sh_rep[ 8 ][ NB_REPORT ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for ( int c = blockIdx.x; c < nchunks; c += gridDim.x ) {
+        const Chunk ch = chunks[ c ];
+        const ProbDev &P = probs[ ch.prob ];
+        Rep rep;
+        rep.init();
+        if ( lane == 0 )
+            for ( int s = ch.begin + warp; s < ch.end; s += 8 ) {
+                double mass = P.mass[ s ], nu = P.nu[ s ];
+                double e2 = fabs( nu - mass );
+                rep.v[ R_WORST ] = fmax( rep.v[ R_WORST ], e2 );
+                rep.v[ R_WORST_REL ] = fmax( rep.v[ R_WORST_REL ], e2 / nu );
+                rep.v[ R_AMIN ] = fmin( rep.v[ R_AMIN ], mass );
+                rep.v[ R_ASUM ] += mass;
+                rep.v[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
+                double x = mass / nu, g = g_of( x, P.res, P.power );
+                double n1 = rep.v[ R_GCOUNT ] + 1, d = g - rep.v[ R_GMEAN ];
+                rep.v[ R_GMEAN ] += d / n1;
+                rep.v[ R_GM2 ] += d * ( g - rep.v[ R_GMEAN ] );
+                rep.v[ R_GCOUNT ] = n1;
+                double u = nu / gp_of( x, P.res, P.power );
+                rep.v[ R_SU ] += u;
+                rep.v[ R_SUG ] += u * g;
+                rep.v[ R_NUSUM ] += nu;
+                rep.v[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
+            }
+        finish_report( P, ch, rep, sh_rep );
+    }
+}
+
+void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks ) {
+    if ( nchunks <= 0 ) return;
+    k_report<<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks );
+    ++*L.launches;
+}
+
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err ) {
+    if ( nchunks <= 0 ) return;
+    k_cells2d<<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err );
+    ++*L.launches;
+}
+
+} // namespace sdot

@@ -1,0 +1,1064 @@
+// The host engine: device geometry of a problem, and the batched damped Newton.
+//
+// A solve is a state machine (start selection, stages of the width continuation, Newton iterations, trial
+// steps, final moments).  `job_run` / `jobs_tick` advance many solves together: each TICK launches
+//   A. one cell kernel over every solve that needs a diagram (trial weights, start weights, a new stage),
+//   B. up to CG_BURST CG iterations over every solve that is solving its Newton system,
+// then reads back every solve's scalars in ONE device->host copy and lets each solve take its decisions
+// (accept or halve the step, switch the residual, converge), and finally launches
+//   D. the Laplacian assembly + rhs + CG start of the solves that begin an iteration, and the trial
+//      weights w + t d of the solves that go on trying.
+// The semantics of the decisions are those of sdotplan/Newton.h:243-429 and sdotplan/Solve.h:111-371
+// (TRIALS step, no aggregation); only the scheduling is batched.
+#include "engine.h"
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+namespace sdot {
+
+void check_cuda( cudaError_t e, const char *what ) {
+    if ( e == cudaSuccess ) return;
+    if ( e == cudaErrorMemoryAllocation ) {
+        cudaGetLastError();
+        throw Error( SDOT_ERR_NO_MEMORY, std::string( what ) + ": out of device memory" );
+    }
+    throw Error( SDOT_ERR_CUDA, std::string( what ) + ": " + cudaGetErrorString( e ) );
+}
+
+void *dalloc( Ctx &c, size_t bytes ) {
+    void *p = nullptr;
+    if ( bytes == 0 ) bytes = 256;
+    cudaError_t e = cudaMallocFromPoolAsync( &p, bytes, c.pool, c.stream );
+    if ( e == cudaErrorMemoryAllocation ) {
+        cudaGetLastError();
+        throw Error( SDOT_ERR_NO_MEMORY, "device pool refused " + std::to_string( bytes ) + " bytes", -1, ( long long ) bytes );
+    }
+    CK( e );
+    return p;
+}
+
+void dfree( Ctx &c, void *p ) {
+    if ( p ) CK( cudaFreeAsync( p, c.stream ) );
+}
+
+void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
+    c.device = device;
+    CK( cudaSetDevice( device ) );
+    CK( cudaStreamCreateWithFlags( &c.stream, cudaStreamNonBlocking ) );
+    cudaMemPoolProps props;
+    std::memset( &props, 0, sizeof( props ) );
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CK( cudaMemPoolCreate( &c.pool, &props ) );
+    uint64_t thr = pool_limit ? pool_limit : UINT64_MAX;
+    CK( cudaMemPoolSetAttribute( c.pool, cudaMemPoolAttrReleaseThreshold, &thr ) );
+    c.max_slots = 4096;
+    c.dscal = ( double * ) dalloc( c, size_t( c.max_slots ) * SLOT_DOUBLES * 8 );
+    CK( cudaMemsetAsync( c.dscal, 0, size_t( c.max_slots ) * SLOT_DOUBLES * 8, c.stream ) );
+    c.dcount = ( unsigned * ) dalloc( c, size_t( c.max_slots ) * 4 * sizeof( unsigned ) );
+    CK( cudaMemsetAsync( c.dcount, 0, size_t( c.max_slots ) * 4 * sizeof( unsigned ), c.stream ) );
+    c.derr = ( ErrRec * ) dalloc( c, sizeof( ErrRec ) );
+    CK( cudaMemsetAsync( c.derr, 0, sizeof( ErrRec ), c.stream ) );
+    CK( cudaMallocHost( &c.hscal, size_t( c.max_slots ) * SLOT_DOUBLES * 8 ) );
+    CK( cudaMallocHost( &c.herr, sizeof( ErrRec ) ) );
+    std::memset( c.herr, 0, sizeof( ErrRec ) );
+    for ( int s = c.max_slots - 1; s >= 0; --s ) c.free_slots.push_back( s );
+    const char *t = std::getenv( "SDOT_KERNEL_TIMING" );
+    c.timer.on = t && t[ 0 ] == '1';
+    CK( cudaStreamSynchronize( c.stream ) );
+}
+
+void ctx_release( Ctx &c ) {
+    cudaSetDevice( c.device );
+    c.timer.release();
+    if ( c.stream ) {
+        if ( c.desc ) cudaFreeAsync( c.desc, c.stream );
+        if ( c.dscal ) cudaFreeAsync( c.dscal, c.stream );
+        if ( c.dcount ) cudaFreeAsync( c.dcount, c.stream );
+        if ( c.derr ) cudaFreeAsync( c.derr, c.stream );
+        cudaStreamSynchronize( c.stream );
+        cudaStreamDestroy( c.stream );
+    }
+    if ( c.hscal ) cudaFreeHost( c.hscal );
+    if ( c.herr ) cudaFreeHost( c.herr );
+    if ( c.pool ) cudaMemPoolDestroy( c.pool );
+    c = Ctx{};
+}
+
+// ---- kernel timing ------------------------------------------------------------------------------------------------------
+static cudaEvent_t take_event( Timer &T ) {
+    if ( T.npool ) return T.pool[ --T.npool ];
+    cudaEvent_t e;
+    CK( cudaEventCreate( &e ) );
+    return e;
+}
+void Timer::begin( cudaStream_t s, int kind, double u ) {
+    if ( ! on ) return;
+    open_kind = kind;
+    open_units = u;
+    open_a = take_event( *this );
+    CK( cudaEventRecord( open_a, s ) );
+}
+void Timer::end( cudaStream_t s, unsigned long long launches ) {
+    if ( ! on || open_kind < 0 ) return;
+    cudaEvent_t b = take_event( *this );
+    CK( cudaEventRecord( b, s ) );
+    if ( npending == cap ) {
+        cap = cap ? 2 * cap : 256;
+        Rec *p = new Rec[ cap ];
+        for ( int k = 0; k < npending; ++k ) p[ k ] = pending[ k ];
+        delete[] pending;
+        pending = p;
+    }
+    pending[ npending++ ] = Rec{ open_kind, open_a, b, open_units };
+    count[ open_kind ] += launches;
+    open_kind = -1;
+}
+void Timer::resolve() {
+    for ( int k = 0; k < npending; ++k ) {
+        Rec &r = pending[ k ];
+        CK( cudaEventSynchronize( r.b ) );
+        float t = 0;
+        CK( cudaEventElapsedTime( &t, r.a, r.b ) );
+        ms[ r.kind ] += t;
+        units[ r.kind ] += r.units;
+        for ( cudaEvent_t e : { r.a, r.b } ) {
+            if ( npool == cappool ) {
+                cappool = cappool ? 2 * cappool : 512;
+                cudaEvent_t *p = new cudaEvent_t[ cappool ];
+                for ( int q = 0; q < npool; ++q ) p[ q ] = pool[ q ];
+                delete[] pool;
+                pool = p;
+            }
+            pool[ npool++ ] = e;
+        }
+    }
+    npending = 0;
+}
+void Timer::release() {
+    for ( int k = 0; k < npending; ++k ) { cudaEventDestroy( pending[ k ].a ); cudaEventDestroy( pending[ k ].b ); }
+    for ( int k = 0; k < npool; ++k ) cudaEventDestroy( pool[ k ] );
+    delete[] pending;
+    delete[] pool;
+    pending = nullptr;
+    pool = nullptr;
+    npending = npool = cap = cappool = 0;
+}
+
+int take_slot( Ctx &c ) {
+    if ( c.free_slots.empty() ) throw Error( SDOT_ERR_NO_MEMORY, "too many solves in flight on one context" );
+    int s = c.free_slots.back();
+    c.free_slots.pop_back();
+    return s;
+}
+void give_slot( Ctx &c, int s ) { c.free_slots.push_back( s ); }
+
+static double now_s() {
+    return std::chrono::duration<double>( std::chrono::steady_clock::now().time_since_epoch() ).count();
+}
+
+// copies `count` elements to the device buffer `dst`, from host or device memory
+template<class T>
+static void to_device( Ctx &c, T *dst, const T *src, size_t count, int memory ) {
+    if ( count == 0 ) return;
+    CK( cudaMemcpyAsync( dst, src, count * sizeof( T ), memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream ) );
+}
+template<class T>
+static void to_host_vec( Ctx &c, std::vector<T> &dst, const T *src, size_t count, int memory ) {
+    dst.resize( count );
+    if ( count == 0 ) return;
+    if ( memory == SDOT_DEVICE ) {
+        CK( cudaMemcpyAsync( dst.data(), src, count * sizeof( T ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+    } else
+        std::memcpy( dst.data(), src, count * sizeof( T ) );
+}
+
+// uploads a descriptor block and returns its device address (stream ordered: the area is reused)
+static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
+    if ( bytes > c.desc_bytes ) {
+        if ( c.desc ) dfree( c, c.desc );
+        c.desc_bytes = std::max( bytes, size_t( 1 ) << 20 );
+        c.desc = ( char * ) dalloc( c, c.desc_bytes );
+    }
+    CK( cudaMemcpyAsync( c.desc, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
+    return c.desc;
+}
+
+void check_errors( Ctx &c, const char *where ) {
+    if ( c.herr->code == 0 ) return;
+    ErrRec e = *c.herr;
+    *c.herr = ErrRec{};
+    CK( cudaMemsetAsync( c.derr, 0, sizeof( ErrRec ), c.stream ) );
+    if ( e.code == SDOT_ERR_CAPACITY )
+        throw Error( SDOT_ERR_CAPACITY, std::string( where ) + ": a cell exceeded its capacity (seed " + std::to_string( e.seed ) + ")", e.seed,
+                     e.needed );
+    throw Error( e.code, std::string( where ) + ": device error", e.seed );
+}
+
+// ---- geometry ----------------------------------------------------------------------------------------------------------
+void Geometry::fill( ProbDev &P ) const {
+    std::memset( &P, 0, sizeof( P ) );
+    P.dim = dim;
+    P.n = n;
+    P.dkind = dkind;
+    for ( int a = 0; a < 3; ++a ) {
+        P.lo[ a ] = lo[ a ]; P.hi[ a ] = hi[ a ]; P.g[ a ] = g[ a ]; P.go[ a ] = go[ a ]; P.gh[ a ] = gh[ a ];
+        P.dn[ a ] = dn[ a ]; P.dorg[ a ] = dorg[ a ]; P.dstep[ a ] = dstep[ a ];
+    }
+    P.ghmin = ghmin;
+    P.cell_range = cell_range;
+    P.pos = pos;
+    P.user = user;
+    P.rank_of = rank_of;
+    P.rho = rho;
+    P.dval = dval;
+    P.dpre = dpre;
+    P.cap = dim == 2 ? CAP2 : CAP3;
+}
+
+void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positions, const double box_lo[ 3 ], const double box_hi[ 3 ],
+                     const sdot_density &dens, int memory ) {
+    if ( dim != 2 && dim != 3 ) throw Error( SDOT_ERR_ARGS, "dim must be 2 or 3" );
+    if ( n <= 0 || n >= ( 1l << 31 ) - 1 ) throw Error( SDOT_ERR_ARGS, "n must be in [1, 2^31)" );
+    if ( ! positions ) throw Error( SDOT_ERR_ARGS, "positions is NULL" );
+    if ( dens.kind == SDOT_DENSITY_IMAGE && dim != 2 ) throw Error( SDOT_ERR_UNSUPPORTED, "image densities are integrated in 2D only" );
+    if ( dens.kind < 0 || dens.kind > 2 ) throw Error( SDOT_ERR_ARGS, "unknown density kind" );
+    G.dim = dim;
+    G.n = int( n );
+    for ( int a = 0; a < dim; ++a ) {
+        G.lo[ a ] = box_lo[ a ];
+        G.hi[ a ] = box_hi[ a ];
+        if ( ! ( G.hi[ a ] > G.lo[ a ] ) ) throw Error( SDOT_ERR_ARGS, "the domain box is empty" );
+    }
+    to_host_vec( c, G.pos_host, positions, size_t( n ) * dim, memory );
+    // the grid covers the domain and every seed, about two seeds per grid cell
+    double mn[ 3 ], mx[ 3 ];
+    for ( int a = 0; a < dim; ++a ) { mn[ a ] = G.lo[ a ]; mx[ a ] = G.hi[ a ]; }
+    for ( long i = 0; i < n; ++i )
+        for ( int a = 0; a < dim; ++a ) {
+            double x = G.pos_host[ i * dim + a ];
+            if ( ! std::isfinite( x ) ) throw Error( SDOT_ERR_ARGS, "a position is not finite", i );
+            mn[ a ] = std::min( mn[ a ], x );
+            mx[ a ] = std::max( mx[ a ], x );
+        }
+    double vol = 1;
+    for ( int a = 0; a < dim; ++a ) vol *= mx[ a ] - mn[ a ];
+    double h = std::pow( vol / std::max( 1.0, n / 2.0 ), 1.0 / dim );
+    const int gmax = dim == 2 ? 32768 : 2048;
+    G.ncell = 1;
+    G.ghmin = 1e300;
+    int bits = 1;
+    for ( int a = 0; a < 3; ++a ) {
+        if ( a >= dim ) { G.g[ a ] = 1; G.go[ a ] = 0; G.gh[ a ] = 1; continue; }
+        double ext = mx[ a ] - mn[ a ];
+        int ga = int( std::ceil( ext / h ) );
+        ga = std::max( 1, std::min( ga, gmax ) );
+        G.g[ a ] = ga;
+        G.go[ a ] = mn[ a ];
+        G.gh[ a ] = ext / ga;
+        G.ghmin = std::min( G.ghmin, G.gh[ a ] );
+        G.ncell *= ga;
+        while ( ( 1 << bits ) < ga ) ++bits;
+    }
+    int key_bits = dim * bits;
+    // one allocation: ranked positions, user, rank_of, cell ranges, density
+    size_t dbytes = 0;
+    G.dkind = dens.kind;
+    G.rho = dens.value;
+    long nval = 0, npre = 0;
+    if ( dens.kind == SDOT_DENSITY_IMAGE ) {
+        if ( ! dens.values || dens.shape[ 0 ] <= 0 || dens.shape[ 1 ] <= 0 ) throw Error( SDOT_ERR_ARGS, "image without values" );
+        nval = long( dens.shape[ 0 ] ) * dens.shape[ 1 ];
+        npre = long( dens.shape[ 1 ] ) * ( dens.shape[ 0 ] + 1 );
+        for ( int a = 0; a < 2; ++a ) { G.dn[ a ] = dens.shape[ a ]; G.dorg[ a ] = dens.origin[ a ]; G.dstep[ a ] = dens.step[ a ]; }
+    } else if ( dens.kind == SDOT_DENSITY_GAUSSIANS ) {
+        if ( dens.count <= 0 || ! dens.centres || ! dens.sigmas || ! dens.masses ) throw Error( SDOT_ERR_ARGS, "gaussians without parameters" );
+        G.dn[ 0 ] = dens.count;
+        nval = long( dens.count ) * ( dim + 2 );
+        std::vector<double> cc, ss, mm;
+        to_host_vec( c, cc, dens.centres, size_t( dens.count ) * dim, memory );
+        to_host_vec( c, ss, dens.sigmas, dens.count, memory );
+        to_host_vec( c, mm, dens.masses, dens.count, memory );
+        G.gauss.resize( nval );
+        for ( int k = 0; k < dens.count; ++k ) {
+            for ( int a = 0; a < dim; ++a ) G.gauss[ k * ( dim + 2 ) + a ] = cc[ k * dim + a ];
+            if ( ! ( ss[ k ] > 0 ) ) throw Error( SDOT_ERR_ARGS, "a gaussian has a non-positive sigma", k );
+            G.gauss[ k * ( dim + 2 ) + dim ] = ss[ k ];
+            G.gauss[ k * ( dim + 2 ) + dim + 1 ] = mm[ k ];
+        }
+        if ( dim == 3 ) throw Error( SDOT_ERR_UNSUPPORTED, "3D gaussian densities are not integrated by this build" );
+    }
+    dbytes = size_t( nval + npre ) * 8 + 1024;
+    size_t bytes = size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( G.ncell ) * 8 + dbytes + 8 * 256;
+    G.mem = ( char * ) dalloc( c, bytes );
+    Arena A{ G.mem, bytes, 0 };
+    G.pos = A.take<double>( size_t( n ) * dim );
+    G.user = A.take<int>( n );
+    G.rank_of = A.take<int>( n );
+    G.cell_range = A.take<int2>( G.ncell );
+    if ( nval ) G.dval = A.take<double>( nval );
+    if ( npre ) G.dpre = A.take<double>( npre );
+    // the sort, in a temporary allocation
+    size_t tb = radix_temp_bytes( int( n ), key_bits );
+    size_t tbytes = size_t( n ) * ( 8 + 8 + 4 + 4 ) + size_t( n ) * dim * 8 + tb + 6 * 256;
+    char *tmp = ( char * ) dalloc( c, tbytes );
+    Arena T{ tmp, tbytes, 0 };
+    double *pos_user = T.take<double>( size_t( n ) * dim );
+    unsigned long long *k0 = T.take<unsigned long long>( n ), *k1 = T.take<unsigned long long>( n );
+    int *v0 = T.take<int>( n ), *v1 = T.take<int>( n );
+    void *sort_tmp = T.take<char>( tb );
+    CK( cudaMemcpyAsync( pos_user, G.pos_host.data(), size_t( n ) * dim * 8, cudaMemcpyHostToDevice, c.stream ) );
+    Launch L = c.L();
+    launch_keys( L, pos_user, int( n ), dim, G.g, G.go, G.gh, key_bits, k0, v0 );
+    radix_sort( L, sort_tmp, tb, k0, k1, v0, v1, int( n ), key_bits );
+    launch_gather( L, pos_user, v1, int( n ), dim, G.pos, G.user, G.rank_of, nullptr, nullptr );
+    CK( cudaMemsetAsync( G.cell_range, 0, size_t( G.ncell ) * sizeof( int2 ), c.stream ) );
+    launch_cell_ranges( L, k1, G.pos, int( n ), dim, G.g, G.go, G.gh, G.cell_range );
+    if ( dens.kind == SDOT_DENSITY_IMAGE ) {
+        to_device( c, G.dval, dens.values, nval, memory );
+        launch_image_prefix( L, G.dval, G.dn[ 0 ], G.dn[ 1 ], G.dstep[ 0 ], G.dpre );
+    } else if ( dens.kind == SDOT_DENSITY_GAUSSIANS ) {
+        CK( cudaMemcpyAsync( G.dval, G.gauss.data(), nval * 8, cudaMemcpyHostToDevice, c.stream ) );
+    }
+    dfree( c, tmp );
+}
+
+void free_geometry( Ctx &c, Geometry &G ) {
+    dfree( c, G.mem );
+    G.mem = nullptr;
+}
+
+// ---- the solve ---------------------------------------------------------------------------------------------------------
+enum JState { J_START0, J_START_VOR, J_START_SIM, J_STAGE_DIAG, J_REPORT, J_ITER, J_CG, J_TRIAL, J_FINAL, J_DONE };
+enum Pend : unsigned { P_NEWTON = 1, P_GAUGE = 2, P_TRIAL = 4, P_RESCALE = 8, P_SET_W2 = 16, P_ZERO_W2 = 32, P_DENSITY = 64 };
+enum NStatus { NS_RUNNING = 0, NS_CONVERGED = 1, NS_MAX_ITER = 2, NS_STAGNATION = 3, NS_LINEAR_FAILURE = 4, NS_CAPACITY = 5, NS_FAILURE = 6 };
+enum StatIdx {
+    ST_STATUS = 0, ST_RESIDUAL, ST_RESIDUAL0, ST_NB_ITER, ST_NB_DIAG, ST_NB_BACKTRACKS, ST_T_MAJORANT, ST_T_DIAG, ST_T_ASM, ST_T_LIN, ST_T_LIM, ST_EPS,
+    ST_DOMAIN_MASS, ST_NB_OVERFLOWED, ST_NB_CELL_LIM, ST_NB_LIMIT_ROUNDS, ST_LIN_NB_HIERARCHIES, ST_LIN_NB_ITER, ST_LIN_WORST, ST_START, ST_T_TOTAL,
+    ST_NB_CONTINUATION_STEPS, ST_MIN_START_MASS, ST_IT_SWITCH, ST_IT_DOUBLE, ST_SCRATCH_BYTES, ST_NB_CLUSTERS, ST_NB_AGGREGATED, ST_NB_DUPLICATES,
+    ST_RESIDUAL_FULL, ST_NB_POLISH
+};
+
+struct SolveJob {
+    Geometry G;
+    int slot = -1;
+    double opt[ SDOT_NB_OPTIONS ];
+    std::vector<double> nu_user;
+    double nu_min = 0, nu_sum = 0;
+    bool given = false;
+    int start = 1;
+    char *mem = nullptr;
+    size_t mem_bytes = 0;
+    double *w, *w2, *a, *a2, *d, *nu, *nu_dev_user, *b, *x, *r, *z, *p, *q, *dia, *val, *tmpw;
+    int *nb[ 2 ], *nid[ 2 ];
+    double *nc[ 2 ];
+    int cur = 0;
+    int *row_ptr, *col, *rowcnt;
+    double *part_cells, *part_vec;
+    unsigned long long *wslot;          // [2]
+    int wcur = 0;                       // wslot[ wcur ] belongs to w
+    double *obary = nullptr, *ocost = nullptr;
+    int cap = CAP2, nch_cells = 0, nch_vec = 0;
+    int rank0 = 0;                      // rank of user seed 0: the gauge w_0 = 0
+    int repA = 0;                       // which report holds the accepted diagram's
+    // Newton state
+    JState state = J_START0;
+    unsigned pend = 0;
+    int res_cur = 1;
+    double t_last = 1, t = 1, eps = 0, nr = 0, worst = 0, worst_rel = 0;
+    int it = 0, trial = 0, nb_evals = 0;
+    bool redo = false;
+    double h_tprev = 0, h_sprev = 0;
+    bool h_has = false;
+    std::vector<double> scales;
+    int stage = 0;
+    double stats[ SDOT_NB_STATS ];
+    std::vector<double> hist;
+    long steps_before = 0;
+    int nstatus = NS_RUNNING;
+    double domain_mass = 0, nu_scale = 1;
+    double t_begin = 0;
+    std::vector<double> wsim;           // similarity weights (user order)
+    double amin_best = 0;
+    bool first_stage = true;
+    int err_code = 0;
+    std::string err_msg;
+    long long err_id = -1;
+};
+
+size_t job_bytes( int dim, long n, int dkind, long dcount ) {
+    const int cap = dim == 2 ? CAP2 : CAP3;
+    const long nch = ( n + CHUNK - 1 ) / CHUNK, nv = ( n + VCHUNK - 1 ) / VCHUNK;
+    size_t b = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
+               size_t( n ) * 4 + size_t( nch ) * NB_REPORT * 8 + size_t( nv ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) + 40 * 256;
+    // geometry: ranked positions, user, rank_of, the grid (about n / 2 cells), the density, and the sort's scratch
+    b += size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( n ) * 4 + 1024;
+    b += dkind == D_IMAGE ? size_t( dcount ) * 16 : size_t( dcount ) * 8 * ( dim + 2 );
+    b += size_t( n ) * ( 24 + dim * 8 ) + 4096;
+    return b;
+}
+
+static void alloc_job( Ctx &c, SolveJob &J ) {
+    const long n = J.G.n;
+    const int dim = J.G.dim, cap = J.cap;
+    J.nch_cells = int( ( n + CHUNK - 1 ) / CHUNK );
+    J.nch_vec = int( ( n + VCHUNK - 1 ) / VCHUNK );
+    size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
+                   size_t( n ) * 4 + size_t( J.nch_cells ) * NB_REPORT * 8 + size_t( J.nch_vec ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) +
+                   40 * 256;
+    J.mem_bytes = bytes;
+    J.mem = ( char * ) dalloc( c, bytes );
+    Arena A{ J.mem, bytes, 0 };
+    J.w = A.take<double>( n ); J.w2 = A.take<double>( n ); J.a = A.take<double>( n ); J.a2 = A.take<double>( n );
+    J.d = A.take<double>( n ); J.nu = A.take<double>( n ); J.nu_dev_user = A.take<double>( n ); J.b = A.take<double>( n );
+    J.x = A.take<double>( n ); J.r = A.take<double>( n ); J.z = A.take<double>( n ); J.p = A.take<double>( n );
+    J.q = A.take<double>( n ); J.dia = A.take<double>( n ); J.tmpw = A.take<double>( n );
+    for ( int k = 0; k < 2; ++k ) { J.nb[ k ] = A.take<int>( n ); J.nid[ k ] = A.take<int>( size_t( n ) * cap ); J.nc[ k ] = A.take<double>( size_t( n ) * cap ); }
+    J.row_ptr = A.take<int>( n + 1 );
+    J.col = A.take<int>( size_t( n ) * cap );
+    J.val = A.take<double>( size_t( n ) * cap );
+    J.rowcnt = A.take<int>( n );
+    J.part_cells = A.take<double>( size_t( J.nch_cells ) * NB_REPORT );
+    J.part_vec = A.take<double>( size_t( J.nch_vec ) * 4 );
+    J.wslot = A.take<unsigned long long>( 2 );
+    J.obary = A.take<double>( size_t( n ) * dim );
+    J.ocost = A.take<double>( n );
+}
+
+SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
+    const sdot_diagram_desc &D = desc.diagram;
+    SolveJob *J = new SolveJob;
+    try {
+        J->t_begin = now_s();
+        build_geometry( c, J->G, D.dim, D.n, D.positions, D.box_lo, D.box_hi, D.density, D.memory );
+        J->cap = D.dim == 2 ? CAP2 : CAP3;
+        std::memcpy( J->opt, desc.options, sizeof( J->opt ) );
+        for ( int k = 0; k < SDOT_NB_STATS; ++k ) J->stats[ k ] = 0;
+        const long n = D.n;
+        if ( desc.nu ) to_host_vec( c, J->nu_user, desc.nu, n, D.memory );
+        else J->nu_user.assign( n, 1.0 / n );
+        J->nu_min = 1e300;
+        J->nu_sum = 0;
+        for ( long i = 0; i < n; ++i ) {
+            if ( ! ( J->nu_user[ i ] > 0 ) ) throw Error( SDOT_ERR_ARGS, "a target mass is not positive", i );
+            J->nu_min = std::min( J->nu_min, J->nu_user[ i ] );
+            J->nu_sum += J->nu_user[ i ];
+        }
+        std::vector<double> w0;
+        if ( D.weights ) to_host_vec( c, w0, D.weights, n, D.memory );
+        else w0.assign( n, 0.0 );
+        J->given = false;
+        for ( double v : w0 ) J->given |= v != 0;
+        J->start = J->given ? 0 : 1;
+        double g0 = w0[ 0 ];
+        for ( double &v : w0 ) v -= g0;
+        alloc_job( c, *J );
+        J->slot = take_slot( c );
+        CK( cudaMemcpyAsync( &J->rank0, J->G.rank_of, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+        Launch L = c.L();
+        // targets and start weights, ranked
+        CK( cudaMemcpyAsync( J->nu_dev_user, J->nu_user.data(), n * 8, cudaMemcpyHostToDevice, c.stream ) );
+        launch_gather_vec( L, J->nu_dev_user, J->G.user, int( n ), J->nu, 1.0 );
+        CK( cudaMemcpyAsync( J->tmpw, w0.data(), n * 8, cudaMemcpyHostToDevice, c.stream ) );
+        launch_gather_vec( L, J->tmpw, J->G.user, int( n ), J->w, 1.0 );
+        CK( cudaMemsetAsync( J->wslot, 0, 16, c.stream ) );
+        launch_wmax( L, J->w, int( n ), J->wslot );
+        CK( cudaMemsetAsync( c.dcount + 4 * J->slot, 0, 16, c.stream ) );
+        J->res_cur = int( J->opt[ SDOT_OPT_RESIDUAL ] );
+        J->stats[ ST_SCRATCH_BYTES ] = double( J->mem_bytes );
+        J->stats[ ST_IT_DOUBLE ] = -1;
+        J->stats[ ST_IT_SWITCH ] = -1;
+        J->state = J_START0;
+        J->scales.assign( 1, 0.0 );
+    } catch ( ... ) {
+        job_destroy( c, J );
+        throw;
+    }
+    return J;
+}
+
+void job_destroy( Ctx &c, SolveJob *J ) {
+    if ( ! J ) return;
+    if ( J->mem ) dfree( c, J->mem );
+    if ( J->G.mem ) free_geometry( c, J->G );
+    if ( J->slot >= 0 ) give_slot( c, J->slot );
+    delete J;
+}
+
+bool job_done( const SolveJob *j ) { return j->state == J_DONE; }
+
+static double *rep_dev( Ctx &c, const SolveJob &J, int which ) { return c.dscal + size_t( J.slot ) * SLOT_DOUBLES + which * NB_REPORT; }
+static const double *rep_host( Ctx &c, const SolveJob &J, int which ) { return c.hscal + size_t( J.slot ) * SLOT_DOUBLES + which * NB_REPORT; }
+static double *sc_dev( Ctx &c, const SolveJob &J ) { return c.dscal + size_t( J.slot ) * SLOT_DOUBLES + 2 * NB_REPORT; }
+static const double *sc_host( Ctx &c, const SolveJob &J ) { return c.hscal + size_t( J.slot ) * SLOT_DOUBLES + 2 * NB_REPORT; }
+
+static double merit_of( const double *rep, int res ) { return res == 0 ? std::sqrt( rep[ R_LIN2 ] ) : std::sqrt( rep[ R_GM2 ] ); }
+
+// the diagram a job needs now: weights / outputs / report slot
+struct DiagReq {
+    SolveJob *job;
+    const double *w;
+    const unsigned long long *wslot;
+    double *mass;
+    int table;          // -1: none
+    int report;         // -1: none
+    bool moments;
+    bool report_only;
+};
+
+static bool needs_diagram( SolveJob &J, DiagReq &R ) {
+    R = DiagReq{ &J, nullptr, nullptr, nullptr, -1, -1, false, false };
+    switch ( J.state ) {
+    case J_START0:
+    case J_STAGE_DIAG:
+        R.w = J.w; R.wslot = J.wslot + J.wcur; R.mass = J.a; R.table = J.cur; R.report = J.repA; return true;
+    case J_START_VOR:
+    case J_START_SIM:
+    case J_TRIAL:
+        R.w = J.w2; R.wslot = J.wslot + ( 1 - J.wcur ); R.mass = J.a2; R.table = 1 - J.cur; R.report = 1 - J.repA; return true;
+    case J_REPORT:
+        R.mass = J.a; R.report = J.repA; R.report_only = true; return true;
+    case J_FINAL:
+        R.w = J.w; R.wslot = J.wslot + J.wcur; R.moments = true; return true;
+    default:
+        return false;
+    }
+}
+
+static void hist_push( SolveJob &J, int it, double t, int nb_evals, const double *rep ) {
+    double row[ SDOT_NB_HIST ] = { double( J.steps_before + it ), t, std::sqrt( rep[ R_LIN2 ] ), rep[ R_AMIN ], rep[ R_WORST ],
+                                   J.stats[ ST_NB_DIAG ], double( nb_evals ), J.scales[ J.stage ] };
+    J.hist.insert( J.hist.end(), row, row + SDOT_NB_HIST );
+}
+
+// the stages of the width continuation (sdotplan/Continuation.h:33-40): s0, s0 / r, ... >= s_min, then 0
+static std::vector<double> continuation_scales( const SolveJob &J ) {
+    const int dim = J.G.dim;
+    double s0 = J.opt[ SDOT_OPT_CONV_S0 ];
+    if ( s0 <= 0 ) {
+        double d2 = 0;
+        for ( int a = 0; a < dim; ++a ) d2 += ( J.G.hi[ a ] - J.G.lo[ a ] ) * ( J.G.hi[ a ] - J.G.lo[ a ] );
+        s0 = 0.5 * std::sqrt( d2 );
+    }
+    double smin = J.opt[ SDOT_OPT_CONV_MIN ];
+    if ( smin <= 0 ) {
+        double sg = 1e300;
+        for ( int k = 0; k < J.G.dn[ 0 ]; ++k ) sg = std::min( sg, J.G.gauss[ k * ( dim + 2 ) + dim ] );
+        smin = sg / 4;
+    }
+    double ratio = J.opt[ SDOT_OPT_CONV_RATIO ] > 1 ? J.opt[ SDOT_OPT_CONV_RATIO ] : std::sqrt( 2.0 );
+    std::vector<double> res;
+    for ( double s = s0; s >= smin * ( 1 - 1e-12 ) && s > 0 && res.size() < 200; s /= ratio ) res.push_back( s );
+    res.push_back( 0 );
+    return res;
+}
+
+static void set_stage_density( Ctx &c, SolveJob &J ) {
+    if ( J.G.dkind != D_GAUSS ) return;
+    const int dim = J.G.dim, st = dim + 2;
+    std::vector<double> g = J.G.gauss;
+    double s = J.scales[ J.stage ];
+    for ( int k = 0; k < J.G.dn[ 0 ]; ++k ) g[ k * st + dim ] = std::sqrt( g[ k * st + dim ] * g[ k * st + dim ] + s * s );
+    CK( cudaMemcpyAsync( J.G.dval, g.data(), g.size() * 8, cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );       // `g` leaves scope
+}
+
+static void end_stage( Ctx &c, SolveJob &J );
+
+static void begin_iterations( Ctx &c, SolveJob &J ) {
+    // the domain mass of this density and the targets rescaled to it (sdotplan/Solve.h:250-257)
+    const double *rep = rep_host( c, J, J.repA );
+    J.domain_mass = rep[ R_ASUM ];
+    double f = ( J.domain_mass > 0 && J.nu_sum > 0 && J.domain_mass != J.nu_sum ) ? J.domain_mass / J.nu_sum : 1.0;
+    J.it = 0;
+    J.t_last = 1;
+    J.res_cur = int( J.opt[ SDOT_OPT_RESIDUAL ] );
+    if ( f != J.nu_scale ) {
+        J.nu_scale = f;
+        J.pend |= P_RESCALE;
+        J.state = J_REPORT;
+    } else
+        J.state = J_ITER;
+}
+
+// one Newton iteration's decision, from the accepted diagram's report (sdotplan/Newton.h:293-343)
+static void newton_iter( Ctx &c, SolveJob &J ) {
+    const double *rep = rep_host( c, J, J.repA );
+    if ( J.it == 0 && ! J.redo ) hist_push( J, 0, 0, 1, rep );
+    J.redo = false;
+    J.worst = rep[ R_WORST ];
+    J.worst_rel = rep[ R_WORST_REL ];
+    if ( J.opt[ SDOT_OPT_SWITCH ] > 0 && J.res_cur != 0 && J.worst_rel <= J.opt[ SDOT_OPT_SWITCH ] ) {
+        J.res_cur = 0;
+        if ( J.first_stage ) J.stats[ ST_IT_SWITCH ] = J.it;
+    }
+    if ( J.it == 0 ) {
+        J.eps = 0.5 * std::min( J.nu_min * J.nu_scale, rep[ R_AMIN ] );
+        if ( J.first_stage ) { J.stats[ ST_EPS ] = J.eps; J.stats[ ST_RESIDUAL0 ] = J.worst; }
+    }
+    J.nr = merit_of( rep, J.res_cur );
+    J.stats[ ST_RESIDUAL ] = J.worst;
+    if ( J.worst <= J.opt[ SDOT_OPT_TOL_ABS ] || ( J.opt[ SDOT_OPT_TOL_REL ] > 0 && J.worst_rel <= J.opt[ SDOT_OPT_TOL_REL ] ) ) {
+        J.nstatus = NS_CONVERGED;
+        end_stage( c, J );
+        return;
+    }
+    if ( J.it >= int( J.opt[ SDOT_OPT_MAXIT ] ) ) {
+        J.nstatus = NS_MAX_ITER;
+        end_stage( c, J );
+        return;
+    }
+    J.stats[ ST_NB_ITER ] += 1;
+    J.pend |= P_NEWTON;
+    J.state = J_CG;
+}
+
+static void end_stage( Ctx &c, SolveJob &J ) {
+    J.first_stage = false;
+    J.steps_before = J.hist.empty() ? 0 : long( J.hist[ J.hist.size() - SDOT_NB_HIST ] ) + 1;
+    if ( J.nstatus != NS_LINEAR_FAILURE && J.stage + 1 < int( J.scales.size() ) ) {
+        ++J.stage;
+        J.nstatus = NS_RUNNING;
+        set_stage_density( c, J );
+        J.state = J_STAGE_DIAG;
+        return;
+    }
+    if ( J.G.dkind == D_GAUSS && J.scales[ J.stage ] != 0 ) {
+        J.stage = int( J.scales.size() ) - 1;
+        set_stage_density( c, J );
+    }
+    J.stats[ ST_STATUS ] = J.nstatus;
+    J.state = J_FINAL;
+}
+
+static void after_start( Ctx &c, SolveJob &J ) {
+    // seeds outside the domain leave cells empty: the similarity start (sdotplan/Solve.h:66-97, 212-226)
+    const double amin = rep_host( c, J, J.repA )[ R_AMIN ];
+    const bool keep = J.opt[ SDOT_OPT_KEEP_START ] != 0;
+    if ( J.state != J_START_SIM && amin <= 0 && ! ( J.given && keep ) ) {
+        const int dim = J.G.dim;
+        const long n = J.G.n;
+        double plo[ 3 ], phi[ 3 ], al = 1, bb[ 3 ];
+        for ( int a = 0; a < dim; ++a ) { plo[ a ] = 1e300; phi[ a ] = -1e300; }
+        for ( long i = 0; i < n; ++i )
+            for ( int a = 0; a < dim; ++a ) { plo[ a ] = std::min( plo[ a ], J.G.pos_host[ i * dim + a ] ); phi[ a ] = std::max( phi[ a ], J.G.pos_host[ i * dim + a ] ); }
+        for ( int a = 0; a < dim; ++a ) al = std::min( al, ( J.G.hi[ a ] - J.G.lo[ a ] ) * 0.8 / std::max( phi[ a ] - plo[ a ], 1e-300 ) );
+        for ( int a = 0; a < dim; ++a ) bb[ a ] = ( J.G.lo[ a ] + J.G.hi[ a ] ) / 2 - al * ( plo[ a ] + phi[ a ] ) / 2;
+        J.wsim.assign( n, 0.0 );
+        for ( long i = 0; i < n; ++i ) {
+            double pp = 0, qq = 0;
+            for ( int a = 0; a < dim; ++a ) { double x = J.G.pos_host[ i * dim + a ], y = al * x + bb[ a ]; pp += x * x; qq += y * y; }
+            J.wsim[ i ] = pp - qq / al;
+        }
+        double g0 = J.wsim[ 0 ];
+        for ( double &v : J.wsim ) v -= g0;
+        J.amin_best = amin;
+        J.pend |= P_SET_W2;
+        J.state = J_START_SIM;
+        return;
+    }
+    // the continuation, decided on the start (sdotplan/Solve.h:229-235)
+    J.stats[ ST_MIN_START_MASS ] = amin;
+    J.stats[ ST_START ] = J.start;
+    int cont = int( J.opt[ SDOT_OPT_CONTINUATION ] );
+    if ( J.G.dkind == D_GAUSS && ( cont == 2 || ( cont == 1 && amin < J.opt[ SDOT_OPT_CONV_THRESHOLD ] * J.nu_min ) ) ) {
+        J.scales = continuation_scales( J );
+        J.stage = 0;
+        set_stage_density( c, J );
+        J.state = J_STAGE_DIAG;
+    } else
+        begin_iterations( c, J );
+    J.stats[ ST_NB_CONTINUATION_STEPS ] = double( J.scales.size() );
+}
+
+static void accept_trial( SolveJob &J ) {
+    std::swap( J.w, J.w2 );
+    std::swap( J.a, J.a2 );
+    J.cur ^= 1;
+    J.wcur ^= 1;
+    J.repA ^= 1;
+}
+
+// after the tick's read-back: the decisions of every job
+static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
+    if ( had_diag ) {
+        const double *B = nullptr;
+        switch ( J.state ) {
+        case J_START0:
+            J.stats[ ST_NB_DIAG ] += 1;
+            {
+                const double amin = rep_host( c, J, J.repA )[ R_AMIN ];
+                // a warm start that empties a cell: the Voronoi start if it does better (sdotplan/Solve.h:203-210)
+                if ( J.given && J.opt[ SDOT_OPT_KEEP_START ] == 0 && amin < 1e-3 * J.nu_min ) {
+                    J.amin_best = amin;
+                    J.pend |= P_ZERO_W2;
+                    J.state = J_START_VOR;
+                } else
+                    after_start( c, J );
+            }
+            break;
+        case J_START_VOR:
+        case J_START_SIM: {
+            J.stats[ ST_NB_DIAG ] += 1;
+            B = rep_host( c, J, 1 - J.repA );
+            bool vor = J.state == J_START_VOR;
+            if ( B[ R_AMIN ] > J.amin_best ) {
+                accept_trial( J );
+                J.start = vor ? 1 : 2;
+            }
+            if ( vor ) { J.state = J_START0; after_start( c, J ); }
+            else { J.state = J_START_SIM; after_start( c, J ); }
+            break;
+        }
+        case J_STAGE_DIAG:
+            J.stats[ ST_NB_DIAG ] += 1;
+            begin_iterations( c, J );
+            break;
+        case J_REPORT:
+            J.state = J_ITER;
+            break;
+        case J_TRIAL: {
+            J.stats[ ST_NB_DIAG ] += 1;
+            ++J.nb_evals;
+            ++J.trial;
+            B = rep_host( c, J, 1 - J.repA );
+            double m2 = B[ R_AMIN ], n2r = merit_of( B, J.res_cur );
+            bool ok = m2 >= J.eps && std::isfinite( n2r );
+            if ( ok && n2r <= ( 1 - J.t / 2 ) * J.nr && n2r < J.nr ) {
+                accept_trial( J );
+                J.t_last = J.t;
+                ++J.it;
+                hist_push( J, J.it, J.t, J.nb_evals, rep_host( c, J, J.repA ) );
+                J.state = J_ITER;
+            } else {
+                // the hopeless damping (sdotplan/Report.h:33-57)
+                bool hopeless = false;
+                if ( ! ok || ! ( J.nr > 0 ) ) J.h_has = false;
+                else {
+                    double s = ( J.nr - n2r ) / J.t, sp = J.h_sprev, asp = std::fabs( sp );
+                    hopeless = J.h_has && J.h_tprev == 2 * J.t && s < J.nr / 4 && sp < J.nr / 4 && s - sp <= 0.25 * asp && sp - s <= 0.25 * asp &&
+                               2 * s - sp < J.nr / 4;
+                    J.h_tprev = J.t; J.h_sprev = s; J.h_has = true;
+                }
+                J.t /= 2;
+                J.stats[ ST_NB_BACKTRACKS ] += 1;
+                if ( J.t < J.opt[ SDOT_OPT_T_MIN ] || hopeless || J.trial >= int( J.opt[ SDOT_OPT_MAX_BACKTRACKS ] ) ) {
+                    if ( J.res_cur != 0 ) {
+                        // a refused step of the log residual: the iteration again, in LIN (sdotplan/Newton.h:375-389)
+                        J.res_cur = 0;
+                        if ( J.first_stage ) J.stats[ ST_IT_SWITCH ] = J.it;
+                        J.stats[ ST_NB_ITER ] -= 1;
+                        J.redo = true;
+                        J.state = J_ITER;
+                    } else {
+                        J.nstatus = NS_STAGNATION;
+                        end_stage( c, J );
+                    }
+                } else {
+                    J.pend |= P_TRIAL;
+                    J.state = J_TRIAL;
+                }
+            }
+            break;
+        }
+        case J_FINAL:
+            J.stats[ ST_T_TOTAL ] = now_s() - J.t_begin;
+            J.state = J_DONE;
+            break;
+        default:
+            break;
+        }
+    }
+    if ( had_cg && J.state == J_CG ) {
+        const double *S = sc_host( c, J );
+        if ( S[ SC_CONV ] != 0 ) {
+            J.stats[ ST_LIN_NB_ITER ] += S[ SC_ITER ];
+            if ( S[ SC_BNORM ] > 0 ) J.stats[ ST_LIN_WORST ] = std::max( J.stats[ ST_LIN_WORST ], S[ SC_RNORM ] / S[ SC_BNORM ] );
+            if ( S[ SC_FAIL ] != 0 ) {
+                J.nstatus = NS_LINEAR_FAILURE;
+                end_stage( c, J );
+            } else {
+                J.pend |= P_GAUGE | P_TRIAL;
+                J.t = std::min( 1.0, J.opt[ SDOT_OPT_MULT_OK ] * J.t_last );
+                J.trial = 0;
+                J.nb_evals = 0;
+                J.h_has = false;
+                J.state = J_TRIAL;
+            }
+        }
+    }
+    if ( J.state == J_ITER ) newton_iter( c, J );
+}
+
+static VecDev vec_of( Ctx &c, SolveJob &J ) {
+    VecDev V;
+    std::memset( &V, 0, sizeof( V ) );
+    V.n = J.G.n;
+    V.cap = J.cap;
+    V.rank0 = J.rank0;
+    V.res = J.res_cur;
+    V.power = J.opt[ SDOT_OPT_POWER ];
+    V.nb = J.nb[ J.cur ];
+    V.nid = J.nid[ J.cur ];
+    V.nc = J.nc[ J.cur ];
+    V.row_ptr = J.row_ptr;
+    V.col = J.col;
+    V.val = J.val;
+    V.dia = J.dia;
+    V.rowcnt = J.rowcnt;
+    V.x = J.x; V.r = J.r; V.z = J.z; V.p = J.p; V.q = J.q; V.b = J.b;
+    V.nu = J.nu;
+    V.a = J.a;
+    V.w = J.w; V.w2 = J.w2; V.d = J.d;
+    V.t = J.t;
+    V.tol = J.opt[ SDOT_OPT_LIN_TOL ] > 0 ? J.opt[ SDOT_OPT_LIN_TOL ] : 1e-8;
+    V.maxit = J.opt[ SDOT_OPT_LIN_MAXIT ] > 0 ? int( J.opt[ SDOT_OPT_LIN_MAXIT ] ) : 20000;
+    V.report = rep_dev( c, J, J.repA );
+    V.wmax_slot = J.wslot + ( 1 - J.wcur );
+    V.sc = sc_dev( c, J );
+    V.partials = J.part_vec;
+    V.counter = c.dcount + 4 * J.slot + 1;
+    V.nchunk = J.nch_vec;
+    V.active = 1;
+    return V;
+}
+
+struct VecBatch {
+    std::vector<VecDev> v;
+    std::vector<Chunk> ch;
+    void add( const VecDev &d ) {
+        int p = int( v.size() );
+        VecDev x = d;
+        x.chunk0 = int( ch.size() );
+        v.push_back( x );
+        int k = 0;
+        for ( int b = 0; b < d.n; b += VCHUNK, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + VCHUNK ), k } );
+    }
+    // uploads both arrays in one copy; returns device pointers
+    void upload( Ctx &c, VecDev *&dv, Chunk *&dch ) {
+        size_t b1 = v.size() * sizeof( VecDev ), b2 = ch.size() * sizeof( Chunk );
+        size_t o2 = ( b1 + 255 ) & ~size_t( 255 );
+        std::vector<char> buf( o2 + b2 );
+        std::memcpy( buf.data(), v.data(), b1 );
+        std::memcpy( buf.data() + o2, ch.data(), b2 );
+        char *d = upload_desc( c, buf.data(), buf.size() );
+        dv = reinterpret_cast<VecDev *>( d );
+        dch = reinterpret_cast<Chunk *>( d + o2 );
+    }
+};
+
+// phase D: the vector work the decisions asked for
+static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
+    Launch L = c.L();
+    VecBatch newton, gauge, trial;
+    for ( SolveJob *J : jobs ) {
+        if ( ! J->pend ) continue;
+        if ( J->pend & P_RESCALE ) launch_gather_vec( L, J->nu_dev_user, J->G.user, J->G.n, J->nu, J->nu_scale );
+        if ( J->pend & P_ZERO_W2 ) {
+            CK( cudaMemsetAsync( J->w2, 0, size_t( J->G.n ) * 8, c.stream ) );
+            CK( cudaMemsetAsync( J->wslot + ( 1 - J->wcur ), 0, 8, c.stream ) );
+            launch_wmax( L, J->w2, J->G.n, J->wslot + ( 1 - J->wcur ) );
+        }
+        if ( J->pend & P_SET_W2 ) {
+            CK( cudaMemcpyAsync( J->tmpw, J->wsim.data(), size_t( J->G.n ) * 8, cudaMemcpyHostToDevice, c.stream ) );
+            launch_gather_vec( L, J->tmpw, J->G.user, J->G.n, J->w2, 1.0 );
+            CK( cudaMemsetAsync( J->wslot + ( 1 - J->wcur ), 0, 8, c.stream ) );
+            launch_wmax( L, J->w2, J->G.n, J->wslot + ( 1 - J->wcur ) );
+        }
+        VecDev V = vec_of( c, *J );
+        if ( J->pend & P_NEWTON ) newton.add( V );
+        if ( J->pend & P_GAUGE ) gauge.add( V );
+        if ( J->pend & P_TRIAL ) {
+            CK( cudaMemsetAsync( J->wslot + ( 1 - J->wcur ), 0, 8, c.stream ) );
+            trial.add( V );
+        }
+    }
+    VecDev *dv;
+    Chunk *dch;
+    if ( ! newton.v.empty() ) {
+        newton.upload( c, dv, dch );
+        double rows = 0;
+        for ( auto &v : newton.v ) rows += v.n;
+        c.timer.begin( c.stream, K_LAPLACIAN, rows );
+        launch_lap_count( L, dv, dch, int( newton.ch.size() ) );
+        launch_lap_scan( L, dv, int( newton.v.size() ) );
+        launch_lap_fill( L, dv, dch, int( newton.ch.size() ) );
+        launch_rhs( L, dv, dch, int( newton.ch.size() ) );
+        launch_cg_init( L, dv, dch, int( newton.ch.size() ) );
+        c.timer.end( c.stream, 5 );
+    }
+    if ( ! gauge.v.empty() ) {
+        gauge.upload( c, dv, dch );
+        launch_gauge( L, dv, dch, int( gauge.ch.size() ) );
+    }
+    if ( ! trial.v.empty() ) {
+        trial.upload( c, dv, dch );
+        launch_trial( L, dv, dch, int( trial.ch.size() ) );
+    }
+    for ( SolveJob *J : jobs ) J->pend = 0;
+}
+
+constexpr int CG_BURST = 32;
+
+void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
+    Launch L = c.L();
+    // A. the diagrams
+    std::vector<ProbDev> P2, P3, PR;
+    std::vector<Chunk> C2, C3, CR;
+    std::vector<SolveJob *> with_diag;
+    for ( SolveJob *J : jobs ) {
+        DiagReq R;
+        if ( J->state == J_DONE || ! needs_diagram( *J, R ) ) continue;
+        with_diag.push_back( J );
+        ProbDev P;
+        J->G.fill( P );
+        P.cap = J->cap;
+        P.w = R.w;
+        P.wmax_slot = R.wslot;
+        P.mass = R.mass;
+        if ( R.table >= 0 ) { P.nb = J->nb[ R.table ]; P.nid = J->nid[ R.table ]; P.nc = J->nc[ R.table ]; }
+        P.nu = J->nu;
+        P.res = J->res_cur;
+        P.power = J->opt[ SDOT_OPT_POWER ];
+        if ( R.report >= 0 ) {
+            P.report = rep_dev( c, *J, R.report );
+            P.partials = J->part_cells;
+            P.counter = c.dcount + 4 * J->slot;
+            P.nchunk = J->nch_cells;
+        }
+        if ( R.moments ) { P.first = J->obary; P.cost = J->ocost; }
+        std::vector<ProbDev> &PP = R.report_only ? PR : ( J->G.dim == 2 ? P2 : P3 );
+        std::vector<Chunk> &CC = R.report_only ? CR : ( J->G.dim == 2 ? C2 : C3 );
+        int pi = int( PP.size() );
+        P.chunk0 = int( CC.size() );
+        PP.push_back( P );
+        int k = 0;
+        for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) CC.push_back( Chunk{ pi, b, std::min( J->G.n, b + CHUNK ), k } );
+    }
+    auto run_cells = [&]( std::vector<ProbDev> &PP, std::vector<Chunk> &CC, int dim, bool report_only ) {
+        if ( PP.empty() ) return;
+        // flags are uniform per launch: a final (moments) diagram goes with its own launch
+        std::vector<ProbDev> PA, PB;
+        std::vector<Chunk> CA, CB;
+        for ( auto &ch : CC ) {
+            bool mom = PP[ ch.prob ].first != nullptr;
+            auto &PX = mom ? PB : PA;
+            auto &CX = mom ? CB : CA;
+            if ( ch.index == 0 ) { ProbDev q = PP[ ch.prob ]; q.chunk0 = int( CX.size() ); PX.push_back( q ); }
+            Chunk x = ch;
+            x.prob = int( PX.size() ) - 1;
+            CX.push_back( x );
+        }
+        for ( int pass = 0; pass < 2; ++pass ) {
+            auto &PX = pass ? PB : PA;
+            auto &CX = pass ? CB : CA;
+            if ( PX.empty() ) continue;
+            size_t b1 = PX.size() * sizeof( ProbDev ), o2 = ( b1 + 255 ) & ~size_t( 255 ), b2 = CX.size() * sizeof( Chunk );
+            std::vector<char> buf( o2 + b2 );
+            std::memcpy( buf.data(), PX.data(), b1 );
+            std::memcpy( buf.data() + o2, CX.data(), b2 );
+            char *d = upload_desc( c, buf.data(), buf.size() );
+            ProbDev *dp = reinterpret_cast<ProbDev *>( d );
+            Chunk *dc = reinterpret_cast<Chunk *>( d + o2 );
+            double seeds = 0;
+            for ( auto &ch : CX ) seeds += ch.end - ch.begin;
+            if ( report_only ) {
+                c.timer.begin( c.stream, K_REPORT, seeds );
+                launch_report( L, dp, dc, int( CX.size() ) );
+                c.timer.end( c.stream );
+            } else {
+                unsigned flags = pass ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
+                c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
+                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX.size() ), flags, c.derr );
+                else launch_cells3d( L, dp, dc, int( CX.size() ), flags, c.derr );
+                c.timer.end( c.stream );
+            }
+        }
+    };
+    run_cells( P2, C2, 2, false );
+    run_cells( P3, C3, 3, false );
+    run_cells( PR, CR, 2, true );
+    // B. CG iterations
+    VecBatch cg;
+    std::vector<SolveJob *> with_cg;
+    for ( SolveJob *J : jobs )
+        if ( J->state == J_CG ) { cg.add( vec_of( c, *J ) ); with_cg.push_back( J ); }
+    if ( ! cg.v.empty() ) {
+        VecDev *dv;
+        Chunk *dch;
+        cg.upload( c, dv, dch );
+        int burst = with_diag.empty() ? 4 * CG_BURST : CG_BURST;
+        double rows = 0;
+        for ( auto &v : cg.v ) rows += v.n;
+        c.timer.begin( c.stream, K_CG, rows * burst );
+        for ( int k = 0; k < burst; ++k ) launch_cg_iter( L, dv, dch, int( cg.ch.size() ) );
+        c.timer.end( c.stream, 3ull * burst );
+    }
+    // C. one read-back, then the decisions
+    int top = 0;
+    for ( SolveJob *J : jobs ) top = std::max( top, J->slot + 1 );
+    CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    check_errors( c, "cells" );
+    for ( SolveJob *J : jobs ) {
+        if ( J->state == J_DONE ) continue;
+        bool hd = std::find( with_diag.begin(), with_diag.end(), J ) != with_diag.end();
+        bool hc = std::find( with_cg.begin(), with_cg.end(), J ) != with_cg.end();
+        decide( c, *J, hd, hc );
+    }
+    // D. the vector work
+    launch_pending( c, jobs );
+}
+
+void job_run( Ctx &c, std::vector<SolveJob *> &jobs, int max_ticks ) {
+    for ( int tick = 0; max_ticks < 0 || tick < max_ticks; ++tick ) {
+        bool any = false;
+        for ( SolveJob *J : jobs ) any |= J->state != J_DONE;
+        if ( ! any ) break;
+        jobs_tick( c, jobs );
+    }
+}
+
+void job_outputs( Ctx &c, SolveJob *J, sdot_solve_out &out, int memory ) {
+    const long n = J->G.n;
+    const int dim = J->G.dim;
+    Launch L = c.L();
+    // weights and masses back to user order, in the job's scratch
+    double *wu = J->x, *au = J->r;
+    launch_scatter( L, J->w, J->G.user, int( n ), 1, wu );
+    launch_scatter( L, J->a, J->G.user, int( n ), 1, au );
+    auto kind = memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if ( out.weights ) CK( cudaMemcpyAsync( out.weights, wu, n * 8, kind, c.stream ) );
+    if ( out.masses ) CK( cudaMemcpyAsync( out.masses, au, n * 8, kind, c.stream ) );
+    if ( out.barycentres ) CK( cudaMemcpyAsync( out.barycentres, J->obary, size_t( n ) * dim * 8, kind, c.stream ) );
+    std::vector<double> costs( n );
+    CK( cudaMemcpyAsync( costs.data(), J->ocost, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    double cost = 0;
+    for ( double v : costs ) cost += v;
+    if ( out.cost ) {
+        if ( memory == SDOT_DEVICE ) CK( cudaMemcpyAsync( out.cost, &cost, 8, cudaMemcpyHostToDevice, c.stream ) );
+        else *out.cost = cost;
+    }
+    J->stats[ ST_DOMAIN_MASS ] = J->domain_mass;
+    J->stats[ ST_RESIDUAL_FULL ] = J->stats[ ST_RESIDUAL ];
+    J->stats[ ST_IT_DOUBLE ] = -1;
+    std::memcpy( out.stats, J->stats, sizeof( out.stats ) );
+    int rows = int( J->hist.size() / SDOT_NB_HIST );
+    if ( out.history && out.cap_history > 0 ) {
+        int k = std::min( rows, out.cap_history );
+        std::memcpy( out.history, J->hist.data(), size_t( k ) * SDOT_NB_HIST * 8 );
+        out.nb_history = k;
+    } else
+        out.nb_history = rows;
+    CK( cudaStreamSynchronize( c.stream ) );
+}
+
+} // namespace sdot

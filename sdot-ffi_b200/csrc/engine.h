@@ -1,0 +1,103 @@
+// Host side of the B200 SDOT core: the context, a problem's device geometry, and the batched Newton engine.
+#pragma once
+#include "internal.h"
+#include "../../include/sdot_b200.h"
+#include <exception>
+#include <string>
+#include <vector>
+
+namespace sdot {
+
+struct Error : std::exception {
+    int code;
+    std::string msg;
+    long long id = -1, needed = 0;
+    Error( int c, std::string m, long long i = -1, long long nd = 0 ) : code( c ), msg( std::move( m ) ), id( i ), needed( nd ) {}
+    const char *what() const noexcept override { return msg.c_str(); }
+};
+
+void check_cuda( cudaError_t e, const char *what );
+#define CK( x ) ::sdot::check_cuda( ( x ), #x )
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    unsigned long long launches = 0;
+    // engine-wide per-slot scalars: [slot][ 2 * NB_REPORT + NB_SC ] doubles, and two counters per slot
+    int max_slots = 0;
+    double *dscal = nullptr;
+    double *hscal = nullptr;          // pinned mirror
+    unsigned *dcount = nullptr;       // [slot][4]
+    std::vector<int> free_slots;
+    ErrRec *derr = nullptr;
+    ErrRec *herr = nullptr;           // pinned
+    // descriptor upload area
+    char *desc = nullptr;
+    size_t desc_bytes = 0;
+    Timer timer;
+    Launch L() { return Launch{ stream, &launches, &timer }; }
+};
+constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC;
+
+void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
+void ctx_release( Ctx &c );
+void *dalloc( Ctx &c, size_t bytes );
+void dfree( Ctx &c, void *p );
+
+// a bump allocator over one device allocation
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, off = 0;
+    template<class T> T *take( size_t count ) {
+        off = ( off + 255 ) & ~size_t( 255 );
+        T *p = reinterpret_cast<T *>( base + off );
+        off += count * sizeof( T );
+        return p;
+    }
+};
+
+// the seeds of one problem, ranked on the device, with their grid and density
+struct Geometry {
+    int dim = 2, n = 0;
+    double lo[ 3 ] = { 0, 0, 0 }, hi[ 3 ] = { 1, 1, 1 };
+    int g[ 3 ] = { 1, 1, 1 };
+    double go[ 3 ] = { 0, 0, 0 }, gh[ 3 ] = { 1, 1, 1 }, ghmin = 1;
+    long ncell = 0;
+    double *pos = nullptr;            // ranked
+    int *user = nullptr, *rank_of = nullptr;
+    int2 *cell_range = nullptr;
+    int dkind = D_UNIFORM;
+    double rho = 1;
+    double *dval = nullptr, *dpre = nullptr;
+    int dn[ 3 ] = { 0, 0, 0 };
+    double dorg[ 3 ] = { 0, 0, 0 }, dstep[ 3 ] = { 0, 0, 0 };
+    std::vector<double> gauss;        // [ng, dim + 2] as given (continuation widens it)
+    std::vector<double> pos_host;     // user order (similarity start)
+    char *mem = nullptr;
+    void fill( ProbDev &P ) const;
+};
+
+// builds the geometry (copies `positions` / density arrays from where `memory` says)
+void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positions, const double box_lo[ 3 ], const double box_hi[ 3 ],
+                     const sdot_density &dens, int memory );
+void free_geometry( Ctx &c, Geometry &G );
+
+int take_slot( Ctx &c );
+void give_slot( Ctx &c, int s );
+
+void check_errors( Ctx &c, const char *where );
+
+// the batched Newton engine: advances `solves` together until all are done
+struct SolveJob;
+SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc );
+void job_run( Ctx &c, std::vector<SolveJob *> &jobs, int max_ticks = -1 );
+bool job_done( const SolveJob *j );
+void job_outputs( Ctx &c, SolveJob *j, sdot_solve_out &out, int memory );
+void job_destroy( Ctx &c, SolveJob *j );
+size_t job_bytes( int dim, long n, int dkind, long dcount );
+struct Engine;
+// continuous batching: one step of every active job (used by the server)
+void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs );
+
+} // namespace sdot

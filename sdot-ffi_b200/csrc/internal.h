@@ -1,0 +1,218 @@
+// Internal types shared by the host engine and the kernels of the B200 SDOT core.
+//
+// Layout in HBM (one "problem" = one diagram or one solve):
+//   - seeds are RANKED in Morton order of the uniform grid cell that holds them (ties: user order), so a
+//     rank range is a compact blob of space -- the neighbour search, the candidate loads and the
+//     aggregation multigrid (rank >> k packets) all rely on it;
+//   - positions are kept ranked, FP64, AoS `[n, dim]`; weights, masses and every Newton/CG vector are
+//     FP64 `[n]` in rank order; `user[rank]` / `rank_of[user]` convert at the boundary;
+//   - the grid is `g[0] x g[1] (x g[2])` cells of size `gh`, `cell_range[cell] = (first rank, last rank + 1)`
+//     with cells numbered row-major (x fastest);
+//   - facets are written per cell into a fixed-capacity neighbour table `[n, cap]` (rank ids, c_ij),
+//     then mirrored into a bit-symmetric CSR by the "mutual" rule (laplacian kernels).
+// Every kernel is batched: it takes an array of ProbDev and a table of chunks (problem, first rank, end rank),
+// so one launch serves any mix of problems of one dimension (the serving batch, the batch of 64 gradients).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SDOT_DEV __device__ __forceinline__
+
+namespace sdot {
+
+constexpr int CHUNK = 64;              // seeds per chunk (one block of the cell kernels)
+constexpr int CAP2 = 32;               // neighbour table capacity per cell, 2D
+constexpr int CAP3 = 64;               // ... 3D
+constexpr int NB_REPORT = 12;          // doubles of the per-diagram report
+
+enum DensKind : int { D_UNIFORM = 0, D_IMAGE = 1, D_GAUSS = 2 };
+
+// what a diagram computes
+enum DiagFlags : unsigned {
+    F_MASS = 1u,            // masses (always cheap)
+    F_FACETS = 2u,          // neighbour table (ids, c_ij)
+    F_MEASURES = 4u,        // int_facet rho in the table
+    F_MOMENTS = 8u,         // first moment and int |x - p|^2 rho
+    F_REPORT = 16u,         // the Newton report (needs nu)
+    F_USER_ORDER = 32u,     // write outputs at user index instead of rank
+    F_VJP = 64u,            // adjoint gather (grad of masses)
+    F_FP32 = 128u           // FP32 clipping with FP64 re-check
+};
+
+struct ProbDev {
+    int dim, dkind, cap, n;
+    double lo[3], hi[3];
+    int g[3];
+    double go[3], gh[3], ghmin;
+    const int2 *cell_range;
+    const double *pos;            // ranked [n, dim]
+    const int *user;              // rank -> user
+    const int *rank_of;           // user -> rank
+    // density
+    double rho;
+    const double *dval;           // image values [nx * ny] (i along x) | gaussians [ng, dim + 2]
+    const double *dpre;           // image: per row prefix of mass, [ny, nx + 1]
+    int dn[3];
+    double dorg[3], dstep[3];
+    // this evaluation
+    const double *w;              // ranked weights (NULL: zero)
+    const unsigned long long *wmax_slot;   // -> ordered-integer max weight; NULL: 0
+    double *mass;                 // [n]
+    double *first;                // [n, dim] first moment about the seed, or barycentre if F_USER_ORDER
+    double *cost;                 // [n]
+    int *nb;                      // [n]
+    int *nid;                     // [n, cap]
+    double *nc;                   // [n, cap]
+    double *nm;                   // [n, cap]
+    const double *nu;             // [n] ranked targets (report)
+    const double *gm;             // [n] cotangent of masses (vjp), ranked
+    double *gpos;                 // [n, dim] (vjp)
+    double *gw;                   // [n] (vjp)
+    double *report;               // [NB_REPORT] per problem (report)
+    double *partials;             // [nchunks_of_problem, NB_REPORT]
+    unsigned *counter;            // chunk counter for the last-block finalisation
+    int chunk0, nchunk;           // this problem's chunks in the launch's table
+    int res;                      // residual kind for the report (0 lin, 1 log, 2 power)
+    double power;
+};
+
+struct Chunk {
+    int prob;      // index into the launch's ProbDev array
+    int begin;     // first rank
+    int end;       // end rank
+    int index;     // chunk index within its problem
+};
+
+// device-side error record (first error wins)
+struct ErrRec {
+    int code;      // 0 none, 4 capacity
+    int kind;
+    int prob;
+    int seed;      // user index
+    int needed;
+};
+
+// report layout (per problem, after a diagram with F_REPORT)
+enum Report : int {
+    R_WORST = 0, R_WORST_REL, R_AMIN, R_ASUM, R_LIN2, R_GCOUNT, R_GMEAN, R_GM2, R_SU, R_SUG, R_NUSUM, R_NEMPTY
+};
+
+// per-problem view for the Laplacian, CG and Newton vector kernels
+struct VecDev {
+    int n, cap, rank0, res;
+    double power;
+    // the neighbour table of the accepted diagram -> CSR (row_ptr local to the problem)
+    const int *nb;
+    const int *nid;
+    const double *nc;
+    int *row_ptr;                 // [n + 1]
+    int *col;                     // [n * cap]
+    double *val;                  // [n * cap]  c_ij > 0 (the matrix holds -c_ij)
+    double *dia;                  // [n]
+    int *rowcnt;                  // [n] scratch
+    // vectors (ranked)
+    double *x, *r, *z, *p, *q, *b;
+    const double *nu, *a;
+    double *w, *w2, *d;
+    double t;                     // the trial step of this launch
+    double tol;                   // relative residual of the CG
+    int maxit;                    // CG iterations at most
+    const double *report;         // the Newton report of the accepted diagram (rhs)
+    unsigned long long *wmax_slot;   // ordered-integer max of the trial weights
+    double *sc;                   // [NB_SC] scalars of the problem
+    double *partials;             // [nchunk * 4]
+    unsigned *counter;
+    int chunk0, nchunk;
+    int active;
+};
+enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, SC_ITER, SC_MEAN, SC_C, SC_TOL, SC_PQ, SC_FAIL, SC_NNZ, NB_SC };
+constexpr int VCHUNK = 1024;     // rows per chunk of the vector kernels
+
+// ---- warp helpers ------------------------------------------------------------------------------------
+SDOT_DEV double warp_sum( double v ) {
+#pragma unroll
+    for ( int o = 16; o > 0; o >>= 1 ) v += __shfl_xor_sync( 0xffffffffu, v, o );
+    return v;
+}
+SDOT_DEV double warp_max( double v ) {
+#pragma unroll
+    for ( int o = 16; o > 0; o >>= 1 ) v = fmax( v, __shfl_xor_sync( 0xffffffffu, v, o ) );
+    return v;
+}
+SDOT_DEV double warp_min( double v ) {
+#pragma unroll
+    for ( int o = 16; o > 0; o >>= 1 ) v = fmin( v, __shfl_xor_sync( 0xffffffffu, v, o ) );
+    return v;
+}
+SDOT_DEV int lane_id() { return threadIdx.x & 31; }
+
+// ordered-integer image of a double, for exact atomic max
+SDOT_DEV unsigned long long dbl_order( double x ) {
+    unsigned long long u = __double_as_longlong( x );
+    return ( u >> 63 ) ? ~u : ( u | 0x8000000000000000ull );
+}
+SDOT_DEV double order_dbl( unsigned long long u ) {
+    return __longlong_as_double( ( u >> 63 ) ? ( u & 0x7fffffffffffffffull ) : ~u );
+}
+
+// ---- launchers (each in the .cu next to its kernels) --------------------------------------------------
+// CUDA-event timing per kernel class (off by default; `sdot_context_set_timing`)
+enum KClass : int { K_CELLS2D = 0, K_CELLS3D, K_LAPLACIAN, K_CG, K_VECTOR, K_INDEX, K_REPORT, NB_KCLASS };
+struct Timer {
+    bool on = false;
+    struct Rec { int kind; cudaEvent_t a, b; double units; };
+    Rec *pending = nullptr;
+    int npending = 0, cap = 0;
+    cudaEvent_t *pool = nullptr;
+    int npool = 0, cappool = 0;
+    double ms[ NB_KCLASS ] = {}, units[ NB_KCLASS ] = {};
+    unsigned long long count[ NB_KCLASS ] = {};
+    int open_kind = -1;
+    double open_units = 0;
+    cudaEvent_t open_a = nullptr;
+    void begin( cudaStream_t s, int kind, double units );
+    void end( cudaStream_t s, unsigned long long launches = 1 );
+    void resolve();
+    void release();
+};
+
+struct Launch {
+    cudaStream_t stream;
+    unsigned long long *launches;   // incremented per kernel launched
+    Timer *timer = nullptr;
+};
+
+// index.cu
+void launch_bbox( const Launch &L, const double *pos, int n, int dim, unsigned long long *mm /* [2*dim] */ );
+void launch_keys( const Launch &L, const double *pos, int n, int dim, const int *g, const double *go, const double *gh, int bits,
+                  unsigned long long *keys, int *vals );
+void launch_gather( const Launch &L, const double *pos, const int *vals, int n, int dim, double *pos_ranked, int *user, int *rank_of,
+                    const double *w_user, double *w_ranked );
+void launch_cell_ranges( const Launch &L, const unsigned long long *keys, const double *pos_ranked, int n, int dim, const int *g,
+                         const double *go, const double *gh, int2 *cell_range );
+size_t radix_temp_bytes( int n, int bits );
+void radix_sort( const Launch &L, void *temp, size_t temp_bytes, const unsigned long long *kin, unsigned long long *kout, const int *vin,
+                 int *vout, int n, int bits );
+void launch_image_prefix( const Launch &L, const double *values, int nx, int ny, double hx, double *pre );
+void launch_wmax( const Launch &L, const double *w, int n, unsigned long long *slot );
+void launch_finish_wmax( const Launch &L, unsigned long long *slot, double *wmax, int count );
+
+// linalg.cu
+void launch_lap_count( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_lap_scan( const Launch &L, const VecDev *v, int nprob );
+void launch_lap_fill( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_rhs( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_cg_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+
+// cells2d.cu / cells3d.cu
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err );
+void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks );
+void launch_scale( const Launch &L, double *v, int n, double s );
+void launch_scatter( const Launch &L, const double *ranked, const int *user, int n, int dim, double *out_user );
+void launch_gather_vec( const Launch &L, const double *user_vals, const int *user, int n, double *ranked, double scale );
+void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err );
+
+} // namespace sdot

@@ -1,0 +1,383 @@
+// The Newton Hessian and its solve, batched over problems (block-diagonal).
+//
+// CSR assembly (the reference: gpu/Laplacian2D.cuh:139-297, sdotplan/Laplacian.h:37-62).  Each cell wrote
+// its facets into a fixed-capacity table.  An entry (i, j) enters the CSR when BOTH cells saw the facet
+// (the "mutual" rule), with the value measured by the cell of the smaller rank: the matrix is symmetric
+// to the bit, a facet seen by one side only (a sliver below rounding) is dropped on both, and the rows
+// come out in table order, which is deterministic.  `dia` = the row sum, 1 for an empty row.
+//
+// CG: preconditioned by the diagonal, FP64, one chunk of VCHUNK rows per block.  Every reduction is a
+// fixed tree inside the block, then a fold of the chunk partials in chunk order by the last block of the
+// problem to finish (a counter per problem): bitwise reproducible whatever the scheduling, the
+// reference's requirement too (gpu/Reduce.cuh:3-20, gpu/Linear2D.cuh:39-41).
+#include "internal.h"
+#include <cub/block/block_scan.cuh>
+
+namespace sdot {
+
+constexpr int VT = 256;                       // threads per block of the vector kernels
+constexpr int VPT = VCHUNK / VT;              // rows per thread
+
+// deterministic block sum of NV values; thread 0 gets the result
+template<int NV>
+__device__ __forceinline__ void block_sum( double ( &v )[ NV ] ) {
+    __shared__ double sh[ VT / 32 ][ NV ];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for ( int k = 0; k < NV; ++k ) v[ k ] = warp_sum( v[ k ] );
+    if ( lane == 0 )
+#pragma unroll
+        for ( int k = 0; k < NV; ++k ) sh[ warp ][ k ] = v[ k ];
+    __syncthreads();
+    if ( threadIdx.x == 0 )
+#pragma unroll
+        for ( int k = 0; k < NV; ++k ) {
+            double s = 0;
+            for ( int w = 0; w < VT / 32; ++w ) s += sh[ w ][ k ];
+            v[ k ] = s;
+        }
+    __syncthreads();
+}
+
+// thread 0 of the chunk writes its partials; returns true in thread 0 of the last chunk of the problem,
+// which then holds the folded sums in `tot`
+template<int NV>
+__device__ __forceinline__ bool fold_last( const VecDev &V, const Chunk &ch, const double ( &v )[ NV ], double ( &tot )[ NV ] ) {
+    __shared__ int last;
+    if ( threadIdx.x == 0 ) {
+        double *dst = V.partials + ( size_t ) ch.index * 4;
+#pragma unroll
+        for ( int k = 0; k < NV; ++k ) dst[ k ] = v[ k ];
+        __threadfence();
+        unsigned prev = atomicAdd( V.counter, 1u );
+        last = prev == unsigned( V.nchunk - 1 );
+        if ( last ) {
+            __threadfence();
+#pragma unroll
+            for ( int k = 0; k < NV; ++k ) tot[ k ] = 0;
+            for ( int c = 0; c < V.nchunk; ++c ) {
+                const volatile double *src = V.partials + ( size_t ) c * 4;
+#pragma unroll
+                for ( int k = 0; k < NV; ++k ) tot[ k ] += src[ k ];
+            }
+            *V.counter = 0;
+        }
+    }
+    __syncthreads();
+    return threadIdx.x == 0 && last;
+}
+
+// ---- CSR -------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int find_in_row( const VecDev &V, int row, int key ) {
+    const int nb = V.nb[ row ];
+    const int *ids = V.nid + ( size_t ) row * V.cap;
+    for ( int l = 0; l < nb; ++l ) if ( ids[ l ] == key ) return l;
+    return -1;
+}
+
+__global__ void __launch_bounds__( VT ) k_lap_count( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    double tot = 0;
+    for ( int row = ch.begin + threadIdx.x; row < ch.end; row += VT ) {
+        int cnt = 0;
+        const int nb = V.nb[ row ];
+        for ( int k = 0; k < nb; ++k ) {
+            int j = V.nid[ ( size_t ) row * V.cap + k ];
+            cnt += find_in_row( V, j, row ) >= 0;
+        }
+        V.rowcnt[ row ] = cnt;
+        tot += cnt;
+    }
+    double v[ 1 ] = { tot };
+    block_sum<1>( v );
+    if ( threadIdx.x == 0 ) V.partials[ ( size_t ) ch.index * 4 ] = v[ 0 ];
+}
+
+void launch_lap_count( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_lap_count<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// one block per problem: exclusive scan of the chunk totals, in place
+__global__ void __launch_bounds__( 1024 ) k_lap_scan( const VecDev *__restrict__ vs ) {
+    const VecDev &V = vs[ blockIdx.x ];
+    if ( ! V.active ) return;
+    typedef cub::BlockScan<long long, 1024> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ long long carry;
+    if ( threadIdx.x == 0 ) carry = 0;
+    __syncthreads();
+    for ( int base = 0; base < V.nchunk; base += 1024 ) {
+        int c = base + threadIdx.x;
+        long long x = c < V.nchunk ? ( long long ) V.partials[ ( size_t ) c * 4 ] : 0, ex, agg;
+        Scan( tmp ).ExclusiveSum( x, ex, agg );
+        if ( c < V.nchunk ) V.partials[ ( size_t ) c * 4 + 1 ] = double( carry + ex );
+        __syncthreads();
+        if ( threadIdx.x == 0 ) carry += agg;
+        __syncthreads();
+    }
+    if ( threadIdx.x == 0 ) {
+        V.sc[ SC_NNZ ] = double( carry );
+        V.row_ptr[ V.n ] = int( carry );
+    }
+}
+
+void launch_lap_scan( const Launch &L, const VecDev *v, int nprob ) {
+    if ( nprob <= 0 ) return;
+    k_lap_scan<<<nprob, 1024, 0, L.stream>>>( v );
+    ++*L.launches;
+}
+
+__global__ void __launch_bounds__( VT ) k_lap_fill( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    typedef cub::BlockScan<int, VT> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    const int r0 = ch.begin + threadIdx.x * VPT;
+    int cnt[ VPT ], loc = 0;
+#pragma unroll
+    for ( int q = 0; q < VPT; ++q ) { int row = r0 + q; cnt[ q ] = row < ch.end ? V.rowcnt[ row ] : 0; loc += cnt[ q ]; }
+    int ex;
+    Scan( tmp ).ExclusiveSum( loc, ex );
+    int at = int( V.partials[ ( size_t ) ch.index * 4 + 1 ] ) + ex;
+#pragma unroll
+    for ( int q = 0; q < VPT; ++q ) {
+        int row = r0 + q;
+        if ( row >= ch.end ) break;
+        V.row_ptr[ row ] = at;
+        double s = 0;
+        const int nb = V.nb[ row ];
+        for ( int k = 0; k < nb; ++k ) {
+            int j = V.nid[ ( size_t ) row * V.cap + k ];
+            int l = find_in_row( V, j, row );
+            if ( l < 0 ) continue;
+            double c = row < j ? V.nc[ ( size_t ) row * V.cap + k ] : V.nc[ ( size_t ) j * V.cap + l ];
+            V.col[ at ] = j;
+            V.val[ at ] = c;
+            s += c;
+            ++at;
+        }
+        V.dia[ row ] = s > 0 ? s : 1.0;
+    }
+}
+
+void launch_lap_fill( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_lap_fill<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// ---- Newton right-hand side (sdotplan/Newton.h:178-203), then projected on the range of L ------------------------
+__device__ __forceinline__ double g_of( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return p == 0 ? log( x ) : ( pow( x, p ) - 1 ) / p;
+    return r == 1 ? log( x ) : x - 1;
+}
+__device__ __forceinline__ double gp_of( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return pow( x, p - 1 );
+    return r == 1 ? 1 / x : 1;
+}
+
+__global__ void __launch_bounds__( VT ) k_rhs( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    const double c = V.res == 0 ? 0.0 : V.report[ R_SUG ] / V.report[ R_SU ];
+    double s = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        double nu = V.nu[ i ], a = V.a[ i ], b;
+        if ( V.res == 0 ) b = nu > 0 ? nu - a : 0.0;
+        else {
+            double x = a / nu;
+            b = nu > 0 ? nu / gp_of( x, V.res, V.power ) * ( c - g_of( x, V.res, V.power ) ) : 0.0;
+        }
+        V.b[ i ] = b;
+        s += b;
+    }
+    double v[ 1 ] = { s }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) V.sc[ SC_MEAN ] = tot[ 0 ] / V.n;
+}
+
+void launch_rhs( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_rhs<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// ---- CG --------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__( VT ) k_cg_init( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    const double mean = V.sc[ SC_MEAN ];
+    double rz = 0, bb = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        double b = V.b[ i ] - mean;
+        V.b[ i ] = b;
+        V.x[ i ] = 0;
+        V.r[ i ] = b;
+        double z = b / V.dia[ i ];
+        V.z[ i ] = z;
+        V.p[ i ] = z;
+        rz += b * z;
+        bb += b * b;
+    }
+    double v[ 2 ] = { rz, bb }, tot[ 2 ];
+    block_sum<2>( v );
+    if ( fold_last<2>( V, ch, v, tot ) ) {
+        V.sc[ SC_RZ ] = tot[ 0 ];
+        V.sc[ SC_BNORM ] = sqrt( tot[ 1 ] );
+        V.sc[ SC_RNORM ] = sqrt( tot[ 1 ] );
+        V.sc[ SC_ITER ] = 0;
+        V.sc[ SC_FAIL ] = 0;
+        V.sc[ SC_CONV ] = tot[ 1 ] == 0 ? 1.0 : 0.0;
+    }
+}
+
+__global__ void __launch_bounds__( VT ) k_cg_spmv( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    double pq = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        double pi = V.p[ i ];
+        double s = V.dia[ i ] * pi;
+        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) s -= V.val[ e ] * V.p[ V.col[ e ] ];
+        V.q[ i ] = s;
+        pq += pi * s;
+    }
+    double v[ 1 ] = { pq }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) {
+        if ( tot[ 0 ] > 0 ) V.sc[ SC_ALPHA ] = V.sc[ SC_RZ ] / tot[ 0 ];
+        else { V.sc[ SC_ALPHA ] = 0; V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
+    }
+}
+
+__global__ void __launch_bounds__( VT ) k_cg_update( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    const double al = V.sc[ SC_ALPHA ];
+    double rz = 0, rr = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        V.x[ i ] += al * V.p[ i ];
+        double r = V.r[ i ] - al * V.q[ i ];
+        V.r[ i ] = r;
+        double z = r / V.dia[ i ];
+        V.z[ i ] = z;
+        rz += r * z;
+        rr += r * r;
+    }
+    double v[ 2 ] = { rz, rr }, tot[ 2 ];
+    block_sum<2>( v );
+    if ( fold_last<2>( V, ch, v, tot ) ) {
+        double it = V.sc[ SC_ITER ] + 1;
+        V.sc[ SC_ITER ] = it;
+        V.sc[ SC_BETA ] = tot[ 0 ] / V.sc[ SC_RZ ];
+        V.sc[ SC_RZ ] = tot[ 0 ];
+        double rn = sqrt( tot[ 1 ] );
+        V.sc[ SC_RNORM ] = rn;
+        if ( rn <= V.tol * V.sc[ SC_BNORM ] ) V.sc[ SC_CONV ] = 1;
+        else if ( it >= V.maxit ) { V.sc[ SC_CONV ] = 2; V.sc[ SC_FAIL ] = 1; }
+    }
+}
+
+__global__ void __launch_bounds__( VT ) k_cg_p( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    const double be = V.sc[ SC_BETA ];
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) V.p[ i ] = V.z[ i ] + be * V.p[ i ];
+}
+
+void launch_cg_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_init<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_spmv<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_cg_update<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_cg_p<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 3;
+}
+
+// d = x - x[ rank of user seed 0 ]: the gauge w_0 = 0 kept by the direction
+__global__ void k_gauge( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    const double x0 = V.x[ V.rank0 ];
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) V.d[ i ] = V.x[ i ] - x0;
+}
+
+void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_gauge<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// w2 = w + t d, and the max of w2 for the security radius of the next diagram
+__global__ void k_trial( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    double m = -1e300;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
+        double w2 = i == V.rank0 ? 0.0 : V.w[ i ] + V.t * V.d[ i ];
+        V.w2[ i ] = w2;
+        m = fmax( m, w2 );
+    }
+    m = warp_max( m );
+    if ( ( threadIdx.x & 31 ) == 0 ) atomicMax( V.wmax_slot, dbl_order( m ) );
+}
+
+void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_trial<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+__global__ void k_scale( double *v, int n, double s ) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( i < n ) v[ i ] *= s;
+}
+void launch_scale( const Launch &L, double *v, int n, double s ) {
+    if ( n <= 0 ) return;
+    k_scale<<<( n + 255 ) / 256, 256, 0, L.stream>>>( v, n, s );
+    ++*L.launches;
+}
+
+// out_user[ user[ s ] ] = ranked[ s ]  (dim values per seed)
+__global__ void k_scatter( const double *__restrict__ ranked, const int *__restrict__ user, int n, int dim, double *out ) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( s >= n ) return;
+    int u = user[ s ];
+    for ( int a = 0; a < dim; ++a ) out[ ( size_t ) u * dim + a ] = ranked[ ( size_t ) s * dim + a ];
+}
+void launch_scatter( const Launch &L, const double *ranked, const int *user, int n, int dim, double *out_user ) {
+    if ( n <= 0 ) return;
+    k_scatter<<<( n + 255 ) / 256, 256, 0, L.stream>>>( ranked, user, n, dim, out_user );
+    ++*L.launches;
+}
+
+// ranked[ s ] = scale * user_vals[ user[ s ] ]  (user_vals NULL: scale)
+__global__ void k_gather_vec( const double *__restrict__ uv, const int *__restrict__ user, int n, double *ranked, double scale ) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( s >= n ) return;
+    ranked[ s ] = uv ? scale * uv[ user[ s ] ] : scale;
+}
+void launch_gather_vec( const Launch &L, const double *user_vals, const int *user, int n, double *ranked, double scale ) {
+    if ( n <= 0 ) return;
+    k_gather_vec<<<( n + 255 ) / 256, 256, 0, L.stream>>>( user_vals, user, n, ranked, scale );
+    ++*L.launches;
+}
+
+} // namespace sdot

@@ -1,0 +1,179 @@
+"""`SdotPlanNd`: the solution of a semi-discrete transport in dimension 2 or 3 (src/sdot/SdotPlanNd.py:281-1122).
+
+The whole fit is ONE call of the C ABI (`sdot_solve`, or `sdot_solve_batch` for many problems at once): the
+start, the stages, the damped Newton with its diagrams, Laplacians and CG solves, and the final moments all
+run on the GPU; Python only sets up the problem and reads what comes out -- the reference's split
+(SdotPlanNd.py:1-24).  `stats` and `history` carry the reference's keys in the reference's order.
+"""
+import numpy as np
+
+from . import _lib
+from .PowerDiagram import PowerDiagram
+
+_STATS = ["status", "residual", "residual0", "nb_iter", "nb_diag", "nb_backtracks", "t_majorant", "t_diag", "t_asm", "t_lin", "t_lim", "eps",
+          "domain_mass", "nb_overflowed", "nb_cell_lim", "nb_limit_rounds", "lin_nb_hierarchies", "lin_nb_iter", "lin_worst", "start", "t_total",
+          "nb_continuation_steps", "min_start_mass", "it_switch", "it_double", "scratch_bytes",
+          "nb_clusters", "nb_aggregated", "nb_duplicates", "residual_full", "nb_polish"]
+_HISTORY = ["step", "t", "residual_l2", "min_measure", "max_abs_residual", "nb_diag", "nb_evals", "s"]
+_STATUS = {0: "running", 1: "converged", 2: "max iterations", 3: "stagnation", 4: "linear solver failure", 5: "card capacity",
+           6: "failure", 7: "converged (aggregated)"}
+_START = {0: "weights0", 1: "voronoi", 2: "similarity"}
+_RESIDUAL = {"lin": 0, "log": 1, "power": 2}
+_CONTINUATION = {"never": 0, "auto": 1, "always": 2}
+_INT_STATS = ("nb_iter", "nb_diag", "nb_backtracks", "nb_overflowed", "nb_cell_lim", "nb_limit_rounds", "lin_nb_hierarchies", "lin_nb_iter",
+              "nb_continuation_steps", "scratch_bytes", "nb_clusters", "nb_aggregated", "nb_duplicates", "nb_polish")
+
+
+def exact_duplicates(positions):
+    """`( dup, rep )`: each exact duplicate and the smallest index at its position (SdotPlanNd.py:124-148)"""
+    P = np.ascontiguousarray(np.asarray(positions, dtype=np.float64)) + 0.0
+    n = P.shape[0]
+    none = (np.zeros(0, np.int64), np.zeros(0, np.int64))
+    if n < 2:
+        return none
+    _, idx, inv = np.unique(P.reshape(n, -1), axis=0, return_index=True, return_inverse=True)
+    if len(idx) == n:
+        return none
+    rep = idx[inv.reshape(-1)]
+    dup = np.nonzero(rep != np.arange(n))[0]
+    return dup.astype(np.int64), rep[dup].astype(np.int64)
+
+
+def solver_options(settings, n):
+    """the option vector of `sdot_solve_desc` from `Iterative` / `Tuning`"""
+    tun = settings.tuning
+    if tun.step not in ("auto", "trials"):
+        raise NotImplementedError(f"step = {tun.step!r}: this build takes the TRIALS step ( 'auto' or 'trials' )")
+    if tun.residual not in _RESIDUAL:
+        raise ValueError(f"unknown residual: {tun.residual!r} ( {', '.join(_RESIDUAL)} )")
+    if tun.linear_solver not in ("auto", "cg"):
+        raise NotImplementedError(f"linear_solver = {tun.linear_solver!r}: 'auto' / 'cg' (Jacobi-PCG on the device) in this build")
+    if settings.kernel_dtype != "FP64":
+        raise NotImplementedError(f"precision = {settings.precision!r}: FP64 cells only in this build")
+    return dict(tol_abs=settings.tol, tol_rel=float(tun.mass_rtol), maxit=settings.max_iter, max_backtracks=tun.max_backtracks,
+                t_min=tun.t_min, mult_ok=tun.restart_factor, residual=_RESIDUAL[tun.residual], power=tun.residual_power,
+                switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-8), lin_maxit=int(tun.linear_maxit or 20000),
+                keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
+                conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
+                lin_method=0, precision=0, lin_precision=0)
+
+
+def _box_of(problem):
+    d = problem.nb_dims
+    from .PowerDiagram import _domain_box
+    return _domain_box(problem.domain, d)
+
+
+class SdotPlanNd:
+    """see the module docstring"""
+
+    @classmethod
+    def _solve(cls, problem, settings, verbose=False, warm=None):
+        return cls._solve_many([problem], settings, [warm])[0]
+
+    @classmethod
+    def _solve_many(cls, problems, settings, warms=None):
+        """many problems in ONE batched call (their cells, Laplacians and CG iterations share launches)"""
+        warms = warms or [None] * len(problems)
+        plans, pbs, opts = [], [], []
+        for problem, warm in zip(problems, warms):
+            self = cls.__new__(cls)
+            self.problem = problem
+            src, dst = problem.source, problem.target
+            n, d = src.nb_diracs, src.nb_dims
+            if settings.aggregate:
+                dup, _ = exact_duplicates(src.positions)
+                if len(dup):
+                    raise NotImplementedError(f"{len(dup)} exact duplicate seeds: their aggregation is not built yet (remove the duplicates)")
+            plan = settings.ot_plan if settings.ot_plan is not None else warm
+            if settings.weights0 is not None:
+                w0, self._warm_start = np.asarray(settings.weights0, dtype=np.float64).reshape(-1), "weights0"
+            elif plan is not None:
+                if len(plan.weights) != n:
+                    if settings.ot_plan is not None:
+                        raise ValueError(f"Iterative( ot_plan = ... ): this plan carries {len(plan.weights)} weights and the source has {n}")
+                    w0, self._warm_start = None, f"none ( the kept plan carries {len(plan.weights)} weights, the source has {n} )"
+                else:
+                    w0, self._warm_start = plan.weights, "ot_plan"
+            else:
+                w0, self._warm_start = None, "none"
+            lo, hi = _box_of(problem)
+            self._box = (lo, hi)
+            self._settings = settings
+            pbs.append((src.positions, src.weights, w0, lo, hi, dst._sdot_density()))
+            opts.append(solver_options(settings, n))
+            plans.append(self)
+        results = _lib.solve_batch(pbs, opts, cap_history=8 * (settings.max_iter + 1) + 64)
+        for self, r in zip(plans, results):
+            if isinstance(r, Exception):
+                raise r
+            self._read(r, settings)
+        for self in plans:
+            self._check_converged(settings)
+        return plans
+
+    def _read(self, r, settings):
+        #: the fitted weights, [n], user order, `weights[ 0 ] == 0`
+        self.weights = r["weights"]
+        self._weights_fit = self.weights
+        #: the mass of each cell at the fitted weights (the one Newton measured)
+        self.cell_masses = r["masses"]
+        #: the barycentre of each cell [n, d] (its seed if it is empty)
+        self.barycenters = r["barycentres"]
+        #: the transport cost W2^2
+        self.cost = r["cost"]
+        st = r["stats"]
+        self.stats = {name: float(st[k]) for k, name in enumerate(_STATS)}
+        self.stats["status"] = _STATUS.get(int(self.stats["status"]), "?")
+        self.stats["it_switch"] = int(self.stats["it_switch"])
+        self.stats["it_double"] = int(self.stats["it_double"])
+        self.stats["start"] = _START.get(int(self.stats["start"]), "?")
+        for name in _INT_STATS:
+            self.stats[name] = int(self.stats[name])
+        self.stats["aggregation"] = "none" if settings.aggregate else "off"
+        self.stats["duplicates"] = "none"
+        self.stats["warm_start"] = self._warm_start
+        self.history = []
+        for row in r["history"]:
+            e = {name: float(row[k]) for k, name in enumerate(_HISTORY)}
+            e["step"] = int(e["step"])
+            self.history.append(e)
+
+    def _check_converged(self, settings):
+        if settings.on_failure == "raise" and not self.converged:
+            from .OtProblem import OtNotConverged
+            raise OtNotConverged(self)
+
+    @property
+    def converged(self):
+        return self.stats["status"] in ("converged", "converged (aggregated)")
+
+    @property
+    def clusters(self):
+        """`None`: no seeds were merged (the aggregation is not built in this version)"""
+        return None
+
+    @property
+    def target_masses(self):
+        nu = self.problem.source.weights
+        return nu * (self.stats["domain_mass"] / float(nu.sum()))
+
+    def power_diagram(self, weights=None):
+        w = self._weights_fit if weights is None else weights
+        return PowerDiagram(self.problem.source.positions, w, boundaries=_box_half(self._box), distribution=self.problem.target)
+
+    def residual(self, weights=None):
+        return self.power_diagram(weights).measures - self.target_masses
+
+    def transport(self):
+        return self.cost, self.barycenters, self.cell_masses
+
+    def cost_and_position_grad(self):
+        """`( cost, grad )`: the derivative of the cost wrt the positions, `2 m_i ( p_i - b_i )` (envelope theorem,
+        SdotPlanNd.py:1107-1122)"""
+        return self.cost, 2 * self.cell_masses[:, None] * (self.problem.source.positions - self.barycenters)
+
+
+def _box_half(box):
+    from .PowerDiagram import box_half_spaces
+    return box_half_spaces(*box)

@@ -1,0 +1,87 @@
+"""The C ABI, checked without a GPU: the library loads, exports every function include/sdot_b200.h declares,
+and the ctypes mirrors of its structs have the header's sizes and offsets (gcc compiles the header here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from sdot import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "sdot_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(sdot_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    L = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 18
+    for name in names:
+        assert hasattr(L, name), name
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+    assert L.sdot_abi_version() == 1
+
+
+STRUCTS = {
+    "sdot_status": (_lib.Status, ["code", "kind", "id", "value", "needed", "message"]),
+    "sdot_density": (_lib.Density, ["kind", "value", "shape", "origin", "step", "values", "count", "centres", "sigmas", "masses"]),
+    "sdot_diagram_desc": (_lib.DiagramDesc, ["dim", "n", "positions", "weights", "box_lo", "box_hi", "density", "memory"]),
+    "sdot_cells_out": (_lib.CellsOut, ["masses", "barycentres", "costs", "cap", "nb_count", "nb_ids", "nb_coef", "nb_measure", "precision"]),
+    "sdot_solve_desc": (_lib.SolveDesc, ["diagram", "nu", "options"]),
+    "sdot_solve_out": (_lib.SolveOut, ["weights", "masses", "barycentres", "cost", "stats", "history", "cap_history", "nb_history"]),
+    "sdot_server_config": (_lib.ServerConfig, ["device", "memory_budget", "max_active"]),
+}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, (_, fields) in STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append('printf("SDOT_NB_OPTIONS %d\\n", (int)SDOT_NB_OPTIONS);')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        parts = line.split()
+        if len(parts) == 3:
+            got[(parts[0], parts[1])] = int(parts[2])
+        elif len(parts) == 2:
+            got[parts[0]] = int(parts[1])
+    assert got["SDOT_NB_OPTIONS"] == _lib.NB_OPTIONS
+    for cname, (cls, fields) in STRUCTS.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for f in fields:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)
+
+
+def test_options_enum_order_matches_the_header():
+    src = open(HEADER).read()
+    body = src[src.index("enum sdot_option {"): src.index("SDOT_NB_OPTIONS\n")]
+    names = [m.lower() for m in re.findall(r"SDOT_OPT_([A-Z_0-9]+)", body)]
+    assert names == _lib.OPTIONS
+
+
+def test_calls_fail_loudly_without_a_device():
+    """no CPU fallback: without a CUDA device the context cannot be made and the error says why"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    st = _lib.Status()
+    code = L.sdot_context_create(0, 0, ctypes.byref(h), ctypes.byref(st))
+    assert code == _lib.SDOT_ERR_CUDA
+    assert st.message

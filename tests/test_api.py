@@ -1,0 +1,76 @@
+"""The host side of the drop-in API, without a GPU: domains, normalisation, settings and refusals."""
+import numpy as np
+import pytest
+
+import sdot
+from sdot import Box, Image, Iterative, OtProblem, SumOfDiracs, SumOfGaussians, Tuning, box_half_spaces
+from sdot.PowerDiagram import _domain_box, axis_aligned_box
+from sdot.SdotPlanNd import exact_duplicates, solver_options
+
+
+def test_box_half_spaces_round_trip():
+    d, o = box_half_spaces([0, -1], [2, 3])
+    mi, ma, kept = axis_aligned_box(d, o)
+    assert np.allclose(mi, [0, -1]) and np.allclose(ma, [2, 3]) and not kept.any()
+    assert np.allclose(_domain_box((d, o), 2)[0], [0, -1])
+
+
+def test_a_polytope_domain_is_refused():
+    d, o = box_half_spaces([0, 0], [1, 1])
+    d = np.vstack([d, [[1, 1]]])
+    o = np.concatenate([o, [1.5]])
+    with pytest.raises(NotImplementedError):
+        _domain_box((d, o), 2)
+    # a plane that does not cut the box is harmless
+    o[-1] = 2.5
+    assert np.allclose(_domain_box((d, o), 2)[1], [1, 1])
+
+
+def test_distributions_normalise_like_the_reference():
+    s = SumOfDiracs(np.zeros((4, 2))).normalized_version()
+    assert np.allclose(s.weights, 0.25)
+    s = SumOfDiracs(np.zeros((2, 2)), [1, 3]).normalized_version()
+    assert np.allclose(s.weights, [0.25, 0.75])
+    im = Image(np.ones((4, 2)), frame=[0.5, 1.0]).normalized_version()
+    assert abs(im.mass - 1) < 1e-15
+    assert np.allclose(im.box()[1], [2.0, 2.0])
+    g = SumOfGaussians([[0.5, 0.5], [0.2, 0.3]], [0.1, 0.05], [2, 6]).normalized_version()
+    assert np.allclose(g.weights, [0.25, 0.75])
+    lo, hi = g.box()
+    assert np.allclose(lo, [-0.1, -0.1]) and np.allclose(hi, [1.1, 1.1])
+    b = Box().normalized_version(nb_dims=3)
+    assert b._sdot_density() == ("uniform", 1.0)
+
+
+def test_settings_map_onto_the_option_vector():
+    o = solver_options(Iterative(tol=0, tuning=Tuning(mass_rtol=1e-8, residual="lin")), 10)
+    assert o["tol_abs"] == 0 and o["tol_rel"] == 1e-8 and o["residual"] == 0 and o["continuation"] == 1
+    with pytest.raises(NotImplementedError):
+        solver_options(Iterative(tuning=Tuning(step="limits")), 10)
+    with pytest.raises(NotImplementedError):
+        solver_options(Iterative(precision="mixed"), 10)
+    with pytest.raises(ValueError):
+        Iterative(precision="fp16")
+    with pytest.raises(ValueError):
+        Iterative(ot_plan=object(), weights0=np.zeros(3))
+
+
+def test_the_problem_refuses_what_it_does_not_solve():
+    pb = OtProblem(SumOfDiracs(np.zeros((3, 1))), Image(np.ones(4)))
+    with pytest.raises(NotImplementedError):
+        pb.solve()
+    with pytest.raises(TypeError):
+        OtProblem(Image(np.ones((2, 2))), Image(np.ones((2, 2))))
+
+
+def test_exact_duplicates():
+    p = np.array([[0, 0], [1, 1], [0, 0], [2, 2], [1, 1.0]])
+    dup, rep = exact_duplicates(p)
+    assert list(dup) == [2, 4] and list(rep) == [0, 1]
+    assert len(exact_duplicates(np.random.default_rng(0).uniform(size=(100, 2)))[0]) == 0
+
+
+def test_public_names():
+    for name in ("PowerDiagram", "Voronoi", "OtProblem", "Iterative", "Tuning", "OtNotConverged", "ot_solve", "SdotPlanNd", "SumOfDiracs",
+                 "Image", "SumOfGaussians", "Box", "box_half_spaces", "KernelFailure"):
+        assert hasattr(sdot, name)

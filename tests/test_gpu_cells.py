@@ -1,0 +1,188 @@
+"""Parity of the GPU cells (through the C ABI) with the oracle and with the reference's known answers.
+
+Tolerances: FP64 masses within 1e-10 relative of the oracle's (the reference pins its
+FP64 card at 1e-9, tests/test_CardCells.py:48-73); neighbour sets of non-degenerate facets bit-exact (a facet
+below 1e-9 of its cell's largest is degenerate: its presence is decided by rounding); c_ij within 1e-9.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import sdot
+from helpers import compare_neighbours, degenerate_pairs, neighbour_sets
+from sdot import PowerDiagram, box_half_spaces
+
+pytestmark = pytest.mark.gpu
+
+
+def _pd(pos, w=None, lo=None, hi=None, dist=None):
+    d = pos.shape[1]
+    lo = np.zeros(d) if lo is None else lo
+    hi = np.ones(d) if hi is None else hi
+    return PowerDiagram(pos, w, boundaries=box_half_spaces(lo, hi), distribution=dist)
+
+
+def test_known_answers(known_answers):
+    for case in known_answers:
+        pos = np.array(case["positions"], float)
+        if pos.shape[1] != 2:
+            continue
+        w = None if case["weights"] is None else np.array(case["weights"], float)
+        m = _pd(pos, w, np.array(case["lo"], float), np.array(case["hi"], float)).measures
+        tol = case["atol"]
+        if case.get("masses") is not None:
+            assert np.abs(m - np.array(case["masses"])).max() < tol, (case["name"], m)
+        for k, v in case.get("mass_at", {}).items():
+            assert abs(m[int(k)] - v) < tol, (case["name"], m)
+        if "total" in case:
+            assert abs(m.sum() - case["total"]) < tol * max(1, case["total"]), case["name"]
+
+
+def _compare(pos, w, dens=None, n_check=None):
+    d = pos.shape[1]
+    lo, hi = np.zeros(d), np.ones(d)
+    od = None
+    dist = None
+    if dens is not None:
+        od, dist = dens
+    ref = O.cells(pos, w, box=(lo, hi), density=od)
+    pd = _pd(pos, w, lo, hi, dist)
+    nb, ids, coef, meas = pd.facets()
+    m, bary, cost = pd.barycenters_and_costs()
+    assert ref["status"] == 0
+    rm = ref["mass"]
+    full = rm > 1e-14 * rm.max()
+    assert np.abs(m[full] - rm[full]).max() <= 1e-10 * rm[full].max()
+    assert (np.abs(m - rm) <= 1e-10 * np.maximum(rm, 1e-300) + 1e-18).mean() > 0.999
+    assert np.abs(bary - ref["bary"]).max() < 1e-9
+    assert np.abs(cost - ref["cost"]).max() <= 1e-9 * ref["cost"].max()
+    # neighbour sets of the non-degenerate facets, bit-exact
+    ga = neighbour_sets(nb, ids, meas)
+    gb = neighbour_sets(ref["nb"], ref["nid"], ref["nm"])
+    skip = degenerate_pairs(ref["nb"], ref["nid"], ref["nm"]) | degenerate_pairs(nb, ids, meas)
+    assert compare_neighbours(ga, gb, skip) == 0
+    # c_ij of the non-degenerate facets: relative to the row's largest coefficient (a short facet's own relative
+    # error grows as its length shrinks), and the median relative error (tests/test_CardCells.py:259-312)
+    worst, rels = 0.0, []
+    for i in range(0, len(pos), max(1, len(pos) // 2000)):
+        a = {int(j): c for j, c in zip(ids[i, : nb[i]], coef[i, : nb[i]])}
+        top = ref["nc"][i, : ref["nb"][i]].max() if ref["nb"][i] else 0
+        for j, c in zip(ref["nid"][i, : ref["nb"][i]], ref["nc"][i, : ref["nb"][i]]):
+            if int(j) in a and c > 1e-9 * top:
+                worst = max(worst, abs(a[int(j)] - c) / top)
+                rels.append(abs(a[int(j)] - c) / c)
+    assert worst < 1e-10, worst
+    assert np.median(rels) < 1e-12
+    return m
+
+
+@pytest.mark.parametrize("n,wscale", [(1000, 0.0), (20000, 0.0), (20000, 2e-5), (100000, 5e-6)])
+def test_uniform_cells_match_the_oracle(n, wscale):
+    rng = np.random.default_rng(n + int(wscale * 1e7))
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, wscale, size=n) if wscale else None
+    m = _compare(pos, w)
+    assert abs(m.sum() - 1) < 1e-12
+
+
+def test_cells_are_deterministic():
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(size=(30000, 2))
+    w = rng.uniform(0, 1e-5, size=30000)
+    a = _pd(pos, w).hessian_rows()
+    b = _pd(pos, w).hessian_rows()
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_image_density_matches_the_oracle():
+    rng = np.random.default_rng(21)
+    vals = rng.uniform(0.1, 1.0, size=(64, 48))
+    vals[:5, :7] = 0
+    img = sdot.Image(vals, frame=[1 / 64, 1 / 48])
+    norm = img.normalized_version()
+    pos = rng.uniform(size=(3000, 2))
+    w = rng.uniform(0, 1e-4, size=3000)
+    m = _compare(pos, w, (("image", [0, 0], [1 / 64, 1 / 48], norm.values), img))
+    assert abs(m.sum() - 1) < 1e-12
+
+
+def test_gaussian_density_matches_the_oracle():
+    rng = np.random.default_rng(22)
+    c = rng.uniform(0.3, 0.7, size=(4, 2))
+    s = rng.uniform(0.05, 0.15, size=4)
+    g = sdot.SumOfGaussians(c, s, support_box=(np.zeros(2), np.ones(2)))
+    ng = g.normalized_version()
+    pos = rng.uniform(size=(2000, 2))
+    _compare(pos, None, (("gauss", c, s, ng.weights), g))
+
+
+def test_the_laplacian_is_bit_symmetric():
+    rng = np.random.default_rng(4)
+    n = 20000
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, 1e-5, size=n)
+    row, cols, vals, dia = _pd(pos, w).laplacian()
+    import scipy.sparse as sp
+    A = sp.csr_matrix((vals, cols, row[:-1].tolist() + [row[-1]]), shape=(n, n))
+    assert (A != A.T).nnz == 0
+    assert np.array_equal(A.data, A.T.tocsr().data) or (abs(A - A.T)).max() == 0
+    rs = np.asarray(A.sum(axis=1)).reshape(-1)
+    assert np.abs(rs - dia).max() <= 1e-15 * dia.max()
+    ref = O.cells(pos, w)
+    for i in range(0, n, 97):
+        a = dict(zip(cols[row[i]:row[i + 1]], vals[row[i]:row[i + 1]]))
+        for j, c in zip(ref["nid"][i, : ref["nb"][i]], ref["nc"][i, : ref["nb"][i]]):
+            if c > 1e-8 * ref["nc"][i].max():
+                assert abs(a[int(j)] - c) <= 1e-10 * ref["nc"][i].max()
+
+
+def test_the_linear_solve_matches_a_direct_solve():
+    rng = np.random.default_rng(5)
+    n = 5000
+    pos = rng.uniform(size=(n, 2))
+    pd = _pd(pos)
+    row, cols, vals, dia = pd.laplacian()
+    b = rng.standard_normal(n)
+    b -= b.mean()
+    x = pd.laplacian_solve(b, tol=1e-13)
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    L = sp.diags(dia) - sp.csr_matrix((vals, cols, row), shape=(n, n))
+    y = np.zeros(n)
+    y[1:] = sla.spsolve(L[1:, 1:].tocsc(), b[1:])
+    assert x[0] == 0
+    assert np.abs(x - y).max() < 1e-8 * np.abs(y).max()
+
+
+def test_the_adjoint_is_the_derivative_of_the_measures():
+    rng = np.random.default_rng(6)
+    n = 300
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, 1e-3, size=n)
+    g = rng.standard_normal(n)
+    pd = _pd(pos, w)
+    gp, gw = pd.measures_vjp(g)
+    h = 1e-7
+    for i in range(0, n, 37):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        fd = (g @ _pd(pos, wp).measures - g @ _pd(pos, wm).measures) / (2 * h)
+        assert abs(fd - gw[i]) < 1e-5 * max(1, abs(fd))
+        for a in range(2):
+            pp, pm = pos.copy(), pos.copy()
+            pp[i, a] += h
+            pm[i, a] -= h
+            fd = (g @ _pd(pp, w).measures - g @ _pd(pm, w).measures) / (2 * h)
+            assert abs(fd - gp[i, a]) < 1e-5 * max(1, abs(fd))
+
+
+def test_a_cell_past_its_capacity_is_a_kernel_failure():
+    """a ring of 40 seeds around one seed: its cell has 40 vertices, past the 32 a warp holds"""
+    k = 40
+    ang = 2 * np.pi * np.arange(k) / k
+    pos = np.r_[[[0.5, 0.5]], np.c_[0.5 + 0.2 * np.cos(ang), 0.5 + 0.2 * np.sin(ang)]]
+    with pytest.raises(sdot.KernelFailure) as e:
+        _pd(pos).measures
+    assert e.value.seed == 0

@@ -1,0 +1,135 @@
+"""Parity of the GPU damped Newton (sdot_solve / sdot_solve_batch through the C ABI) with the oracle's.
+
+The bar (the reference's card-vs-CPU tests tests/test_SdotPlanNd.py:612-656, 966-1072):
+the solve converges to `max |m - nu| / nu <= 1e-8`; an independent oracle diagram at the GPU's weights
+confirms the masses; the weights agree with the oracle's converged weights within 1e-7 of max|w|; masses,
+barycentres and cost agree; a solve in a batch is bitwise the solve alone.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import sdot
+from sdot import Iterative, OtProblem, SumOfDiracs, Tuning
+from sdot.SdotPlanNd import SdotPlanNd
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(pos, target=None, rtol=1e-8, **kw):
+    target = target or sdot.Box()
+    return OtProblem(SumOfDiracs(pos), target).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=rtol), **kw))
+
+
+def test_plain_2d_fp64_n10000_matches_the_oracle():
+    """config: N = 10,000 uniform in [0,1]^2, uniform density, nu = 1/N, w0 = 0, FP64, max rel mass error <= 1e-8"""
+    n = 10000
+    rng = np.random.default_rng(20260101)
+    pos = rng.uniform(size=(n, 2))
+    plan = _solve(pos, rtol=1e-10)
+    assert plan.converged, plan.stats
+    nu = 1.0 / n
+    assert np.abs(plan.cell_masses - nu).max() / nu <= 1e-10
+    assert plan.weights[0] == 0
+    # independent check: the oracle's diagram at the GPU's weights
+    chk = O.cells(pos, plan.weights)["mass"]
+    assert np.abs(chk - nu).max() / nu <= 1e-8
+    ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-10)
+    assert ref["stats"]["status"] == 1
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+    assert np.abs(plan.barycenters - ref["bary"]).max() < 1e-9
+    assert abs(plan.cost - ref["cost"]) <= 1e-9 * ref["cost"]
+    assert plan.stats["start"] == "voronoi"
+    assert len(plan.history) >= plan.stats["nb_iter"] + 1
+
+
+def test_a_solve_in_a_batch_is_the_solve_alone():
+    rng = np.random.default_rng(3)
+    pbs = [OtProblem(SumOfDiracs(rng.uniform(size=(n, 2))), sdot.Box()) for n in (1500, 4000, 700, 2500)]
+    s = Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-9))
+    batch = SdotPlanNd._solve_many(pbs, s)
+    for pb, b in zip(pbs, batch):
+        a = SdotPlanNd._solve(pb, s)
+        assert np.array_equal(a.weights, b.weights)
+        assert np.array_equal(a.cell_masses, b.cell_masses)
+        assert a.stats["nb_diag"] == b.stats["nb_diag"]
+
+
+def test_an_image_target_matches_the_oracle():
+    rng = np.random.default_rng(31)
+    xs = (np.arange(128) + 0.5) / 128
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    vals = 0.2 + np.exp(-((X - 0.3) ** 2 + (Y - 0.6) ** 2) / 0.02) + 0.5 * np.exp(-((X - 0.7) ** 2 + (Y - 0.3) ** 2) / 0.01)
+    img = sdot.Image(vals, frame=[1 / 128, 1 / 128])
+    n = 3000
+    pos = rng.uniform(size=(n, 2))
+    plan = _solve(pos, img, rtol=1e-10)
+    assert plan.converged
+    norm = img.normalized_version()
+    ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-10, density=("image", [0, 0], [1 / 128, 1 / 128], norm.values))
+    assert ref["stats"]["status"] == 1
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+    assert abs(plan.cost - ref["cost"]) <= 1e-9 * ref["cost"]
+    assert np.abs(plan.barycenters - ref["bary"]).max() < 1e-8
+
+
+def test_gaussians_with_the_continuation_match_the_oracle():
+    rng = np.random.default_rng(33)
+    c = rng.uniform(0.2, 0.8, size=(4, 2))
+    s = rng.uniform(0.05, 0.15, size=4)
+    g = sdot.SumOfGaussians(c, s, support_box=(np.zeros(2), np.ones(2)))
+    n = 800
+    pos = rng.uniform(size=(n, 2))
+    plan = _solve(pos, g, rtol=1e-9)
+    assert plan.converged
+    ng = g.normalized_version()
+    ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-9, density=("gauss", c, s, ng.weights))
+    assert ref["stats"]["status"] == 1
+    assert plan.stats["nb_continuation_steps"] == ref["stats"]["nb_continuation_steps"]
+    assert abs(plan.stats["domain_mass"] - ref["stats"]["domain_mass"]) < 1e-10
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-6 * np.abs(ref["weights"]).max()
+    assert abs(plan.cost - ref["cost"]) <= 1e-8 * ref["cost"]
+
+
+def test_the_similarity_start():
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(0.5, 1.5, size=(500, 2))
+    plan = _solve(pos, rtol=1e-9)
+    assert plan.stats["start"] == "similarity"
+    assert plan.converged
+
+
+def test_a_solve_that_misses_its_tolerance_raises():
+    rng = np.random.default_rng(10)
+    pos = rng.uniform(size=(1000, 2))
+    with pytest.raises(sdot.OtNotConverged) as e:
+        OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=1e-14, max_iter=1))
+    assert e.value.solution.stats["status"] == "max iterations"
+
+
+def test_the_warm_start_is_the_last_plan():
+    rng = np.random.default_rng(12)
+    pos = rng.uniform(size=(2000, 2))
+    pb = OtProblem(SumOfDiracs(pos), sdot.Box())
+    a = pb.solve(Iterative(tol=1e-12))
+    pb.source = SumOfDiracs(pos + 1e-4 * rng.standard_normal(pos.shape))
+    b = pb.solve(Iterative(tol=1e-12))
+    assert b.stats["warm_start"] == "ot_plan"
+    assert b.stats["nb_iter"] <= a.stats["nb_iter"]
+
+
+def test_the_envelope_gradient_by_finite_differences():
+    """tests/test_SdotPlanNd.py:500-534: d cost / d p = 2 m (p - b), central differences h = 1e-4"""
+    rng = np.random.default_rng(13)
+    n = 200
+    pos = rng.uniform(0.1, 0.9, size=(n, 2))
+    plan = _solve(pos, rtol=1e-12)
+    _, grad = plan.cost_and_position_grad()
+    h = 1e-4
+    for i in range(0, n, 41):
+        for a in range(2):
+            pp, pm = pos.copy(), pos.copy()
+            pp[i, a] += h
+            pm[i, a] -= h
+            fd = (_solve(pp, rtol=1e-12).cost - _solve(pm, rtol=1e-12).cost) / (2 * h)
+            assert abs(fd - grad[i, a]) < 1e-4 * max(1, abs(fd))

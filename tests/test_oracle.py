@@ -1,0 +1,210 @@
+"""Pins the CPU oracle (oracle/sdot_oracle.c) before anything is compared with it: the reference's own
+known-answer tests (tests/golden/known_answers.json), and independent checks that share no code with it --
+brute force versus the grid search, Monte-Carlo sampling of `argmin |x - p|^2 - w`, the lifted convex hull,
+finite differences for the Laplacian.  CPU only."""
+import numpy as np
+import pytest
+from scipy.spatial import ConvexHull
+
+import oracle as O
+from helpers import monte_carlo_masses, neighbour_sets
+
+
+def _cells(case, brute):
+    pos = np.array(case["positions"], float)
+    w = None if case["weights"] is None else np.array(case["weights"], float)
+    return O.cells(pos, w, box=(np.array(case["lo"], float), np.array(case["hi"], float)), brute=brute)
+
+
+@pytest.mark.parametrize("brute", [False, True])
+def test_known_answers(known_answers, brute):
+    for case in known_answers:
+        r = _cells(case, brute)
+        assert r["status"] == 0, case["name"]
+        m = r["mass"]
+        tol = case["atol"]
+        if case.get("masses") is not None:
+            assert np.abs(m - np.array(case["masses"])).max() < tol, (case["name"], m)
+        for k, v in case.get("mass_at", {}).items():
+            assert abs(m[int(k)] - v) < tol, (case["name"], m)
+        if "total" in case:
+            assert abs(m.sum() - case["total"]) < tol * max(1, case["total"]), (case["name"], m.sum())
+        if case.get("positive"):
+            assert (m > 0).all()
+
+
+@pytest.mark.parametrize("d,n", [(2, 3000), (3, 600)])
+def test_grid_search_is_the_brute_force(d, n):
+    rng = np.random.default_rng(40 + d)
+    pos = rng.uniform(size=(n, d))
+    w = rng.uniform(0, 2e-3 if d == 2 else 5e-3, size=n)
+    a, b = O.cells(pos, w), O.cells(pos, w, brute=True)
+    assert a["status"] == 0 and b["status"] == 0
+    assert np.abs(a["mass"] - b["mass"]).max() < 1e-14
+    sa = neighbour_sets(a["nb"], a["nid"], a["nm"])
+    sb = neighbour_sets(b["nb"], b["nid"], b["nm"])
+    assert sa == sb
+    assert abs(a["mass"].sum() - 1) < 1e-12
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_monte_carlo_partition(d):
+    rng = np.random.default_rng(100 + d)
+    pos = rng.uniform(0.1, 0.9, size=(8, d))
+    w = rng.uniform(-0.02, 0.02, size=8)
+    m = O.cells(pos, w)["mass"]
+    mc = monte_carlo_masses(pos, np.zeros(d), np.ones(d), weights=w, nb_samples=200000)
+    assert np.abs(m - mc).max() < 5e-3
+
+
+def test_lifted_hull_gives_the_neighbours():
+    """interior cells: their neighbours are the edges of the regular triangulation, the lower hull of (p, |p|^2 - w)"""
+    rng = np.random.default_rng(3)
+    n = 400
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, 1e-3, size=n)
+    r = O.cells(pos, w)
+    lifted = np.c_[pos, (pos ** 2).sum(axis=1) - w]
+    hull = ConvexHull(lifted)
+    edges = {i: set() for i in range(n)}
+    for simplex, eq in zip(hull.simplices, hull.equations):
+        if eq[2] < 0:                                   # lower facets
+            for a in range(3):
+                for b in range(3):
+                    if a != b:
+                        edges[simplex[a]].add(int(simplex[b]))
+    got = neighbour_sets(r["nb"], r["nid"], r["nm"], rel_floor=0)
+    checked = 0
+    for i in range(n):
+        if r["nb"][i] == len(got[i]) and 0.15 < pos[i, 0] < 0.85 and 0.15 < pos[i, 1] < 0.85:
+            assert got[i] == edges[i], i
+            checked += 1
+    assert checked > 100
+
+
+def test_a_constant_image_is_the_volume_up_to_its_mass():
+    """tests/test_PowerDiagram.py:1527-1551: a constant image integrates to volume / total"""
+    rng = np.random.default_rng(902)
+    shape = (3, 4)
+    pos = rng.uniform(0.2, np.array(shape) - 0.2, size=(12, 2))
+    box = (np.zeros(2), np.array(shape, float))
+    plain = O.cells(pos, box=box)["mass"]
+    img = O.cells(pos, box=box, density=("image", [0, 0], [1, 1], np.full(shape, 1.0 / 12)))["mass"]
+    assert np.abs(img - plain / 12).max() < 1e-12
+    assert abs(img.sum() - 1) < 1e-12
+
+
+def test_an_image_integrates_what_a_sampling_says():
+    rng = np.random.default_rng(904)
+    shape = (4, 3)
+    values = rng.uniform(0, 1, size=shape)
+    values[0, 0] = 0
+    values /= values.sum()
+    pos = rng.uniform(0.1, np.array(shape) - 0.1, size=(10, 2))
+    got = O.cells(pos, box=(np.zeros(2), np.array(shape, float)), density=("image", [0, 0], [1, 1], values))["mass"]
+    pts = rng.uniform(np.zeros(2), np.array(shape, float), size=(400000, 2))
+    owner = ((pts[:, None, :] - pos[None]) ** 2).sum(axis=2).argmin(axis=1)
+    dens = values[pts[:, 0].astype(int), pts[:, 1].astype(int)]
+    ref = np.bincount(owner, weights=dens, minlength=10) / len(pts) * 12
+    assert abs(got.sum() - 1) < 1e-12
+    assert np.abs(got - ref).max() < 0.02
+
+
+def test_gaussians_integrate_what_a_sampling_says():
+    rng = np.random.default_rng(905)
+    c = rng.uniform(0.3, 0.7, size=(3, 2))
+    s = rng.uniform(0.08, 0.15, size=3)
+    m = np.array([0.5, 0.3, 0.2])
+    pos = rng.uniform(0.1, 0.9, size=(12, 2))
+    got = O.cells(pos, density=("gauss", c, s, m))
+    # the gaussian masses inside the unit box, by sampling the mixture and counting owners
+    k = rng.choice(3, size=600000, p=m)
+    pts = c[k] + s[k, None] * rng.standard_normal((600000, 2))
+    inside = ((pts >= 0) & (pts <= 1)).all(axis=1)
+    owner = ((pts[inside][:, None, :] - pos[None]) ** 2).sum(axis=2).argmin(axis=1)
+    ref = np.bincount(owner, minlength=12) / len(pts)
+    assert np.abs(got["mass"] - ref).max() < 3e-3
+    # the exact closed-form facet fluxes are consistent with the masses: d m_i / d w_j = - c_ij
+    w = np.zeros(12)
+    i, j = 0, int(got["nid"][0, 0])
+    h = 1e-7
+    wp = w.copy(); wp[j] += h
+    wm = w.copy(); wm[j] -= h
+    fd = (O.cells(pos, wp, density=("gauss", c, s, m))["mass"][i] - O.cells(pos, wm, density=("gauss", c, s, m))["mass"][i]) / (2 * h)
+    assert abs(fd + got["nc"][0, 0]) < 1e-6 * max(1, abs(fd))
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_laplacian_is_the_jacobian_of_the_measures(d):
+    """tests/test_SdotPlanNd.py:184-243: d m_i / d w_j = - c_ij, d m_i / d w_i = sum_j c_ij"""
+    rng = np.random.default_rng(70 + d)
+    n = 30 if d == 2 else 20
+    pos = rng.uniform(size=(n, d))
+    w = rng.uniform(0, 1e-3, size=n)
+    r = O.cells(pos, w)
+    h = 1e-7
+    for i in range(0, n, 7):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        col = (O.cells(pos, wp)["mass"] - O.cells(pos, wm)["mass"]) / (2 * h)
+        expect = np.zeros(n)
+        for k in range(r["nb"][i]):
+            expect[r["nid"][i, k]] -= r["nc"][i, k]
+        expect[i] = r["nc"][i, : r["nb"][i]].sum()
+        assert np.abs(col - expect).max() < 1e-5 * np.abs(expect).max(), i
+
+
+def test_moments_match_a_sampling():
+    rng = np.random.default_rng(11)
+    pos = rng.uniform(0.1, 0.9, size=(6, 2))
+    r = O.cells(pos)
+    pts = rng.uniform(size=(400000, 2))
+    owner = ((pts[:, None, :] - pos[None]) ** 2).sum(axis=2).argmin(axis=1)
+    for i in range(6):
+        sel = pts[owner == i]
+        assert np.abs(sel.mean(axis=0) - r["bary"][i]).max() < 5e-3
+        assert abs(((sel - pos[i]) ** 2).sum(axis=1).sum() / len(pts) - r["cost"][i]) < 2e-4
+
+
+def test_newton_reaches_the_target_masses():
+    """tests/test_SdotPlanNd.py:39-62: the fitted masses are the targets"""
+    rng = np.random.default_rng(1)
+    n = 2000
+    pos = rng.uniform(size=(n, 2))
+    s = O.solve(pos, tol_abs=0.0, tol_rel=1e-8)
+    assert s["stats"]["status"] == 1
+    assert np.abs(s["masses"] - 1 / n).max() * n <= 1e-8
+    assert s["weights"][0] == 0
+    # an independent diagram at the fitted weights agrees
+    m = O.cells(pos, s["weights"], brute=True)["mass"]
+    assert np.abs(m - 1 / n).max() * n < 1e-8
+
+
+def test_log_and_lin_residuals_reach_the_same_plan():
+    """tests/test_SdotPlanNd.py:327-348"""
+    rng = np.random.default_rng(2)
+    n = 500
+    pos = rng.uniform(size=(n, 2))
+    a = O.solve(pos, tol_abs=1e-13, residual=1)
+    b = O.solve(pos, tol_abs=1e-13, residual=0)
+    assert a["stats"]["status"] == 1 and b["stats"]["status"] == 1
+    assert np.abs(a["weights"] - b["weights"]).max() < 1e-9 * np.abs(a["weights"]).max()
+
+
+def test_newton_in_3d():
+    rng = np.random.default_rng(5)
+    n = 400
+    pos = rng.uniform(size=(n, 3))
+    s = O.solve(pos, tol_abs=0.0, tol_rel=1e-8)
+    assert s["stats"]["status"] == 1
+    assert np.abs(s["masses"] * n - 1).max() <= 1e-8
+
+
+def test_the_similarity_start_when_seeds_are_outside():
+    """tests/test_SdotPlanNd.py:279-306: the Voronoi start has empty cells, the similarity start does not"""
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(0.5, 1.5, size=(200, 2))
+    s = O.solve(pos, tol_abs=1e-11)
+    assert s["stats"]["start"] == 2
+    assert s["stats"]["status"] == 1
