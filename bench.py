@@ -315,15 +315,25 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=16)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--cells-only", type=int, default=0, help="one 2D uniform diagram of this many seeds (for a profiler), then exit")
+    ap.add_argument("--cells-only", type=int, default=0, help="diagrams of this many uniform seeds (for a profiler), then exit")
+    ap.add_argument("--cells-dim", type=int, default=2)
+    ap.add_argument("--cells-repeat", type=int, default=0)
     a = ap.parse_args()
     if a.cells_only:
         import sdot
-        pos = np.random.default_rng(a.seed).uniform(size=(a.cells_only, 2))
-        w = np.random.default_rng(a.seed + 1).uniform(0, 1.0 / a.cells_only, size=a.cells_only)
-        pd = sdot.PowerDiagram(pos, w, boundaries=sdot.box_half_spaces([0, 0], [1, 1]))
+        from sdot import _lib
+        d = a.cells_dim
+        pos = np.random.default_rng(a.seed).uniform(size=(a.cells_only, d))
+        w = np.random.default_rng(a.seed + 1).uniform(0, a.cells_only ** (-2.0 / d), size=a.cells_only)
+        pd = sdot.PowerDiagram(pos, w, boundaries=sdot.box_half_spaces(np.zeros(d), np.ones(d)))
         m = pd.facets()
-        print(f"cells-only: n={a.cells_only} facets/cell {m[0].mean():.3f}")
+        _lib.set_timing(True)
+        for _ in range(a.cells_repeat):
+            pd.facets()
+        ms, nl, units = _lib.kernel_stats()["cells2d" if d == 2 else "cells3d"]
+        print(json.dumps({"cells_only": a.cells_only, "dim": d, "facets_per_cell": float(m[0].mean()), "launches": nl,
+                          "ms_per_launch": ms / max(nl, 1), "ns_per_cell": 1e6 * ms / max(units, 1),
+                          "algorithmic_GBps": units * BYTES_PER_CELL[d] / (ms / 1000) / 1e9 if ms else None}))
         return
 
     rank = int(os.environ.get("RANK", "0"))

@@ -55,6 +55,19 @@ struct InArr {
     ~InArr() { delete own; }
 };
 
+// after a standalone diagram: the cells queued as too big for a warp's registers, rebuilt in global memory
+void run_big_cells( Ctx &c, ProbDev *dprob, unsigned flags ) {
+    CK( cudaMemcpyAsync( c.hovf, &c.dovf->count, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    const int count = *c.hovf;
+    if ( count <= 0 ) return;
+    Launch L = c.L();
+    c.timer.begin( c.stream, K_CELLS2D, double( count ) );
+    launch_cells2d_big( L, dprob, c.dovf, std::min( count, 1 << 16 ), flags, c.derr, c.big_scratch, c.big_warps );
+    c.timer.end( c.stream );
+    CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+}
+
 } // namespace
 
 struct sdot_context_s {
@@ -152,6 +165,11 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         launch_gather_vec( L, w.d, G.user, int( n ), wr, w.d ? 1.0 : 0.0 );
         CK( cudaMemsetAsync( slot, 0, 8, c.stream ) );
         launch_wmax( L, wr, int( n ), slot );
+        if ( facets ) {       // the unused tail of each row reads as (-1, 0, 0)
+            CK( cudaMemsetAsync( dnid, 0xff, size_t( n ) * cap * 4, c.stream ) );
+            CK( cudaMemsetAsync( dnc, 0, size_t( n ) * cap * 8, c.stream ) );
+            if ( dnm ) CK( cudaMemsetAsync( dnm, 0, size_t( n ) * cap * 8, c.stream ) );
+        }
         ProbDev P;
         G.fill( P );
         P.cap = cap;
@@ -168,8 +186,12 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         DevVec dd( c, o2 + ch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
-        if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr );
+        CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, double( n ) );
+        if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
         else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr );
+        c.timer.end( c.stream );
+        if ( dim == 2 ) run_big_cells( c, dd.as<ProbDev>(), flags );
         CK( cudaGetLastError() );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         if ( host ) {
@@ -228,7 +250,9 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         DevVec dd( c, o2 + ch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
-        launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr );
+        CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr, c.dovf );
+        run_big_cells( c, dd.as<ProbDev>(), F_VJP | F_USER_ORDER );
         CK( cudaGetLastError() );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         if ( host ) {
@@ -265,7 +289,13 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         double *nc = A.take<double>( size_t( n ) * cap ), *val = A.take<double>( size_t( n ) * cap ), *ddia = A.take<double>( n );
         double *part = A.take<double>( size_t( nch ) * 4 ), *sc = A.take<double>( NB_SC );
         unsigned *counter = A.take<unsigned>( 2 );
+        // the facets of cells past the table's row (2D): an overflow store
+        DevVec ovf( c, ( size_t( n ) + 4096 ) * 12 + 512 );
+        Arena B{ ( char * ) ovf.p, ( size_t( n ) + 4096 ) * 12 + 512, 0 };
+        int *ovf_count = B.take<int>( 4 ), *ovf_ids = B.take<int>( n + 4096 );
+        double *ovf_c = B.take<double>( n + 4096 );
         CK( cudaMemsetAsync( counter, 0, 8, c.stream ) );
+        CK( cudaMemsetAsync( ovf_count, 0, 16, c.stream ) );
         Launch L = c.L();
         InArr w( c, desc->weights, n, desc->memory );
         launch_gather_vec( L, w.d, G.user, int( n ), wr, w.d ? 1.0 : 0.0 );
@@ -277,6 +307,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         P.w = wr;
         P.wmax_slot = slot;
         P.nb = nb; P.nid = nid; P.nc = nc;
+        if ( dim == 2 ) { P.ovf_count = ovf_count; P.ovf_cap = int( n ) + 4096; P.ovf_ids = ovf_ids; P.ovf_c = ovf_c; }
         std::vector<Chunk> ch;
         for ( int b = 0, k = 0; b < n; b += CHUNK, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + CHUNK ) ), k } );
         std::vector<Chunk> vch;
@@ -285,6 +316,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         std::memset( &V, 0, sizeof( V ) );
         V.n = int( n ); V.cap = cap; V.nb = nb; V.nid = nid; V.nc = nc; V.row_ptr = rp; V.col = col; V.val = val; V.dia = ddia; V.rowcnt = rowcnt;
         V.sc = sc; V.partials = part; V.counter = counter; V.nchunk = int( vch.size() ); V.active = 1;
+        V.ovf_ids = ovf_ids; V.ovf_c = ovf_c;
         size_t o1 = ( sizeof( ProbDev ) + 255 ) & ~size_t( 255 ), o2 = o1 + ( ( ch.size() * sizeof( Chunk ) + 255 ) & ~size_t( 255 ) ),
                o3 = o2 + ( ( sizeof( VecDev ) + 255 ) & ~size_t( 255 ) );
         DevVec dd( c, o3 + vch.size() * sizeof( Chunk ) );
@@ -294,8 +326,10 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         CK( cudaMemcpyAsync( base + o2, &V, sizeof( V ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemcpyAsync( base + o3, vch.data(), vch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         // the cells in USER order: the table holds user ids, and the CSR comes out in user order
-        if ( dim == 2 ) launch_cells2d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr );
+        CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        if ( dim == 2 ) launch_cells2d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
         else launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr );
+        if ( dim == 2 ) run_big_cells( c, ( ProbDev * ) base, F_FACETS | F_USER_ORDER );
         launch_lap_count( L, ( VecDev * ) ( base + o2 ), ( Chunk * ) ( base + o3 ), int( vch.size() ) );
         launch_lap_scan( L, ( VecDev * ) ( base + o2 ), 1 );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );

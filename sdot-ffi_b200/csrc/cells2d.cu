@@ -54,7 +54,7 @@ __device__ __forceinline__ void edge_uniform( double x0, double y0, double x1, d
 }
 
 // image: F(x, y) = int_{X_ref}^{x} rho(t, y) dt along each piece of the edge inside one pixel
-__device__ void edge_image( const ProbDev &P, double px, double py, int iref, double x0, double y0, double x1, double y1, bool moments,
+__device__ __noinline__ void edge_image( const ProbDev &P, double px, double py, int iref, double x0, double y0, double x1, double y1, bool moments,
                             EdgeInt &e ) {
     const int nx = P.dn[ 0 ], ny = P.dn[ 1 ];
     const double hx = P.dstep[ 0 ], hy = P.dstep[ 1 ];
@@ -139,7 +139,7 @@ __device__ __forceinline__ double erf_diff( double a, double b ) {
     return erf( b ) - erf( a );
 }
 
-__device__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments, EdgeInt &e ) {
+__device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments, EdgeInt &e ) {
     e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
     double dx = x1 - x0, dy = y1 - y0, len = sqrt( dx * dx + dy * dy );
     if ( len == 0 ) return;
@@ -304,10 +304,8 @@ __device__ __forceinline__ double gp_of( double x, int r, double p ) {
 }
 
 // the report of one problem's chunk, written by its block; the last block of the problem folds them in order
-__device__ void finish_report( const ProbDev &P, const Chunk &ch, Rep &warp_rep, double ( *sh )[ NB_REPORT ] ) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )[ NB_REPORT ] ) {
     __shared__ int am_last;
-    if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh[ warp ][ k ] = warp_rep.v[ k ];
     __syncthreads();
     if ( threadIdx.x == 0 ) {
         Rep r;
@@ -336,16 +334,20 @@ __device__ void finish_report( const ProbDev &P, const Chunk &ch, Rep &warp_rep,
     __syncthreads();
 }
 
-__global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
-                                                    unsigned flags, ErrRec *err ) {
+__global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+                                                    unsigned flags, ErrRec *err, OvfList *ovf ) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     __shared__ double sh_rep[ 8 ][ NB_REPORT ];
     const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     for ( int c = blockIdx.x; c < nchunks; c += gridDim.x ) {
         const Chunk ch = chunks[ c ];
         const ProbDev &P = probs[ ch.prob ];
-        Rep rep;
-        rep.init();
+        double *rep = sh_rep[ warp ];          // this warp's report accumulators (lane 0 updates them)
+        if ( lane == 0 ) {
+            Rep r0;
+            r0.init();
+            for ( int k = 0; k < NB_REPORT; ++k ) rep[ k ] = r0.v[ k ];
+        }
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
         for ( int s = ch.begin + warp; s < ch.end; s += nwarps ) {
             const double px = P.pos[ 2 * ( size_t ) s ], py = P.pos[ 2 * ( size_t ) s + 1 ];
@@ -370,13 +372,18 @@ __global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ 
             int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
             for ( int r = 0; r <= rmax && C.m > 0 && ! overflow; ++r ) {
                 const int ncell = r == 0 ? 1 : 8 * r;
+                // the security ball of the current cell: a grid cell farther than its radius holds no cutting seed
+                double R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
+                double ex = R2 + wmax - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
                 for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
                     int ci = cb + lane, beg = 0, cnt = 0;
                     if ( ci < ncell ) {
                         int dx, dy;
                         ring_offset( r, ci, dx, dy );
                         int x = cx + dx, y = cy + dy;
-                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
+                        double bx0 = P.go[ 0 ] + x * P.gh[ 0 ] - px, by0 = P.go[ 1 ] + y * P.gh[ 1 ] - py;
+                        double ddx = fmax( 0.0, fmax( bx0, -( bx0 + P.gh[ 0 ] ) ) ), ddy = fmax( 0.0, fmax( by0, -( by0 + P.gh[ 1 ] ) ) );
+                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 && ddx * ddx + ddy * ddy < rb * rb ) {
                             int2 rg = P.cell_range[ ( size_t ) y * g0 + x ];
                             beg = rg.x;
                             cnt = rg.y - rg.x;
@@ -421,14 +428,22 @@ __global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ 
                     }
                 }
                 if ( C.m == 0 || overflow ) break;
-                double R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
-                double ex = R2 + wmax - wi;
+                R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
+                ex = R2 + wmax - wi;
                 if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
             }
             const int user = P.user[ s ];
             if ( overflow ) {
-                if ( lane == 0 ) record_error( err, 4, ch.prob, user, 33 );
-                C.m = 0;
+                // past the 32 vertices a warp holds: the global-memory pass rebuilds it (report included)
+                if ( lane == 0 ) {
+                    if ( ovf ) {
+                        int k = atomicAdd( &ovf->count, 1 );
+                        if ( k < ovf->cap ) ovf->items[ k ] = OvfItem{ ch.prob, s };
+                        else record_error( err, 4, ch.prob, user, 33 );
+                    } else
+                        record_error( err, 4, ch.prob, user, 33 );
+                }
+                continue;
             }
             // ---- integration over the edges
             const int m = C.m;
@@ -451,9 +466,15 @@ __global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ 
             unsigned fmask = __ballot_sync( FULL, fac );
             int nf = __popc( fmask );
             if ( facets && nf > P.cap ) {
-                if ( lane == 0 ) record_error( err, 4, ch.prob, user, nf );
-                fmask = 0;
-                nf = 0;
+                if ( lane == 0 ) {
+                    if ( ovf ) {
+                        int k = atomicAdd( &ovf->count, 1 );
+                        if ( k < ovf->cap ) ovf->items[ k ] = OvfItem{ ch.prob, s };
+                        else record_error( err, 4, ch.prob, user, nf );
+                    } else
+                        record_error( err, 4, ch.prob, user, nf );
+                }
+                continue;
             }
             double dist = sqrt( C.lnx * C.lnx + C.lny * C.lny );
             double cij = fac ? e.meas / ( 2 * dist ) : 0.0;
@@ -506,24 +527,24 @@ __global__ void __launch_bounds__( 256 ) k_cells2d( const ProbDev *__restrict__ 
             if ( ( flags & F_REPORT ) && lane == 0 ) {
                 double nu = P.nu[ s ];
                 double e2 = fabs( nu - mass );
-                rep.v[ R_WORST ] = fmax( rep.v[ R_WORST ], e2 );
-                rep.v[ R_WORST_REL ] = fmax( rep.v[ R_WORST_REL ], e2 / nu );
-                rep.v[ R_AMIN ] = fmin( rep.v[ R_AMIN ], mass );
-                rep.v[ R_ASUM ] += mass;
-                rep.v[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
+                rep[ R_WORST ] = fmax( rep[ R_WORST ], e2 );
+                rep[ R_WORST_REL ] = fmax( rep[ R_WORST_REL ], e2 / nu );
+                rep[ R_AMIN ] = fmin( rep[ R_AMIN ], mass );
+                rep[ R_ASUM ] += mass;
+                rep[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
                 double x = mass / nu, g = g_of( x, P.res, P.power );
-                double n1 = rep.v[ R_GCOUNT ] + 1, d = g - rep.v[ R_GMEAN ];
-                rep.v[ R_GMEAN ] += d / n1;
-                rep.v[ R_GM2 ] += d * ( g - rep.v[ R_GMEAN ] );
-                rep.v[ R_GCOUNT ] = n1;
+                double n1 = rep[ R_GCOUNT ] + 1, d = g - rep[ R_GMEAN ];
+                rep[ R_GMEAN ] += d / n1;
+                rep[ R_GM2 ] += d * ( g - rep[ R_GMEAN ] );
+                rep[ R_GCOUNT ] = n1;
                 double u = nu / gp_of( x, P.res, P.power );
-                rep.v[ R_SU ] += u;
-                rep.v[ R_SUG ] += u * g;
-                rep.v[ R_NUSUM ] += nu;
-                rep.v[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
+                rep[ R_SU ] += u;
+                rep[ R_SUG ] += u * g;
+                rep[ R_NUSUM ] += nu;
+                rep[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
             }
         }
-        if ( flags & F_REPORT ) finish_report( P, ch, rep, sh_rep );
+        if ( flags & F_REPORT ) finish_report( P, ch, sh_rep );
     }
 }
 
@@ -556,7 +577,8 @@ __global__ void __launch_bounds__( 256 ) k_report( const ProbDev *__restrict__ p
                 rep.v[ R_NUSUM ] += nu;
                 rep.v[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
             }
-        finish_report( P, ch, rep, sh_rep );
+        if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep.v[ k ];
+        finish_report( P, ch, sh_rep );
     }
 }
 
@@ -566,9 +588,248 @@ void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, 
     ++*L.launches;
 }
 
-void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err ) {
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf ) {
     if ( nchunks <= 0 ) return;
-    k_cells2d<<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err );
+    k_cells2d<<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+    ++*L.launches;
+}
+
+// ---- the big cells: one warp per cell, the polygon in global memory (two buffers of VBIG vertices) ---------------------------
+struct BigPoly {
+    double *x, *y, *nx, *ny, *off;
+    int *id;
+    unsigned char *out;
+};
+
+__device__ __forceinline__ BigPoly big_buffer( char *base, int which ) {
+    BigPoly B;
+    char *p = base + size_t( which ) * VBIG * ( 5 * 8 + 4 + 1 );
+    B.x = ( double * ) p; B.y = B.x + VBIG; B.nx = B.y + VBIG; B.ny = B.nx + VBIG; B.off = B.ny + VBIG;
+    B.id = ( int * ) ( B.off + VBIG );
+    B.out = ( unsigned char * ) ( B.id + VBIG );
+    return B;
+}
+
+__device__ __forceinline__ int warp_min_int( int v ) {
+#pragma unroll
+    for ( int o = 16; o > 0; o >>= 1 ) v = min( v, __shfl_xor_sync( FULL, v, o ) );
+    return v;
+}
+
+// keep n . y <= off; returns the new vertex count, -1 past VBIG; `moved`: the new polygon is in D
+__device__ int big_clip( BigPoly &S, BigPoly &D, int m, int lane, double nx, double ny, double off, int id, bool &moved ) {
+    moved = false;
+    int nout = 0;
+    for ( int k = lane; k - lane < m; k += 32 ) {
+        bool o = k < m && nx * S.x[ k ] + ny * S.y[ k ] - off > 0;
+        if ( k < m ) S.out[ k ] = o;
+        nout += __popc( __ballot_sync( FULL, o ) );
+    }
+    __syncwarp();
+    if ( nout == 0 ) return m;
+    if ( nout == m ) return 0;
+    int a = 1 << 30;
+    for ( int k = lane; k < m; k += 32 ) {
+        int k1 = k + 1 == m ? 0 : k + 1;
+        if ( ! S.out[ k ] && S.out[ k1 ] ) a = min( a, k );
+    }
+    a = warp_min_int( a );
+    int db = 1 << 30;
+    for ( int k = lane; k < m; k += 32 ) {
+        int k1 = k + 1 == m ? 0 : k + 1;
+        if ( S.out[ k ] && ! S.out[ k1 ] ) db = min( db, ( ( k - a - 1 ) % m + m ) % m );
+    }
+    db = warp_min_int( db );
+    const int b = ( a + 1 + db ) % m;
+    const int K = ( ( a - b - 1 ) % m + m ) % m + 1;
+    if ( K + 2 > VBIG ) return -1;
+    for ( int t = lane; t < K; t += 32 ) {
+        int src = ( b + 1 + t ) % m;
+        D.x[ t ] = S.x[ src ]; D.y[ t ] = S.y[ src ]; D.nx[ t ] = S.nx[ src ]; D.ny[ t ] = S.ny[ src ]; D.off[ t ] = S.off[ src ];
+        D.id[ t ] = S.id[ src ];
+    }
+    if ( lane == 0 ) {
+        int a1 = a + 1 == m ? 0 : a + 1, b1 = b + 1 == m ? 0 : b + 1;
+        double Px, Py, Qx, Qy;
+        bool okP, okQ;
+        isect( S.nx[ a ], S.ny[ a ], S.off[ a ], nx, ny, off, Px, Py, okP );
+        isect( nx, ny, off, S.nx[ b ], S.ny[ b ], S.off[ b ], Qx, Qy, okQ );
+        if ( ! okP ) {
+            double sa = nx * S.x[ a ] + ny * S.y[ a ] - off, sa1 = nx * S.x[ a1 ] + ny * S.y[ a1 ] - off, t = sa / ( sa - sa1 );
+            Px = S.x[ a ] + t * ( S.x[ a1 ] - S.x[ a ] ); Py = S.y[ a ] + t * ( S.y[ a1 ] - S.y[ a ] );
+        }
+        if ( ! okQ ) {
+            double sb = nx * S.x[ b ] + ny * S.y[ b ] - off, sb1 = nx * S.x[ b1 ] + ny * S.y[ b1 ] - off, t = sb / ( sb - sb1 );
+            Qx = S.x[ b ] + t * ( S.x[ b1 ] - S.x[ b ] ); Qy = S.y[ b ] + t * ( S.y[ b1 ] - S.y[ b ] );
+        }
+        D.x[ K ] = Px; D.y[ K ] = Py; D.nx[ K ] = nx; D.ny[ K ] = ny; D.off[ K ] = off; D.id[ K ] = id;
+        D.x[ K + 1 ] = Qx; D.y[ K + 1 ] = Qy; D.nx[ K + 1 ] = S.nx[ b ]; D.ny[ K + 1 ] = S.ny[ b ]; D.off[ K + 1 ] = S.off[ b ];
+        D.id[ K + 1 ] = S.id[ b ];
+    }
+    __syncwarp();
+    moved = true;
+    return K + 2;
+}
+
+__global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict__ probs, const OvfList *__restrict__ ovf, int count,
+                                                        unsigned flags, ErrRec *err, char *scratch ) {
+    const int lane = threadIdx.x;
+    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+    char *mine = scratch + size_t( blockIdx.x ) * 2 * VBIG * ( 5 * 8 + 4 + 1 );
+    for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
+        const OvfItem item = ovf->items[ it ];
+        const ProbDev &P = probs[ item.prob ];
+        const int s = item.seed;
+        BigPoly A = big_buffer( mine, 0 ), B = big_buffer( mine, 1 );
+        BigPoly *S = &A, *D = &B;
+        const double px = P.pos[ 2 * ( size_t ) s ], py = P.pos[ 2 * ( size_t ) s + 1 ];
+        const double wi = P.w ? P.w[ s ] : 0.0;
+        const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
+        if ( lane < 4 ) {
+            double lx = P.lo[ 0 ] - px, ly = P.lo[ 1 ] - py, hx = P.hi[ 0 ] - px, hy = P.hi[ 1 ] - py;
+            S->x[ lane ] = ( lane == 1 || lane == 2 ) ? hx : lx;
+            S->y[ lane ] = ( lane >= 2 ) ? hy : ly;
+            S->nx[ lane ] = lane == 1 ? 1.0 : ( lane == 3 ? -1.0 : 0.0 );
+            S->ny[ lane ] = lane == 0 ? -1.0 : ( lane == 2 ? 1.0 : 0.0 );
+            S->off[ lane ] = lane == 0 ? -ly : ( lane == 1 ? hx : ( lane == 2 ? hy : -lx ) );
+            S->id[ lane ] = -1 - lane;
+        }
+        __syncwarp();
+        int m = 4;
+        bool overflow = false;
+        const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
+        int cx = int( floor( ( px - P.go[ 0 ] ) / P.gh[ 0 ] ) ), cy = int( floor( ( py - P.go[ 1 ] ) / P.gh[ 1 ] ) );
+        cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
+        cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
+        const int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
+        for ( int r = 0; r <= rmax && m > 0 && ! overflow; ++r ) {
+            double R2 = 0;
+            for ( int k = lane; k < m; k += 32 ) R2 = fmax( R2, S->x[ k ] * S->x[ k ] + S->y[ k ] * S->y[ k ] );
+            R2 = warp_max( R2 );
+            double ex = R2 + wmax - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
+            if ( r > 0 && ( r - 1 ) * P.ghmin >= rb ) break;
+            const int ncell = r == 0 ? 1 : 8 * r;
+            for ( int ci = 0; ci < ncell && m > 0 && ! overflow; ++ci ) {
+                int dx, dy;
+                ring_offset( r, ci, dx, dy );
+                int x = cx + dx, y = cy + dy;
+                if ( x < 0 || x >= g0 || y < 0 || y >= g1 ) continue;
+                double bx0 = P.go[ 0 ] + x * P.gh[ 0 ] - px, by0 = P.go[ 1 ] + y * P.gh[ 1 ] - py;
+                double ddx = fmax( 0.0, fmax( bx0, -( bx0 + P.gh[ 0 ] ) ) ), ddy = fmax( 0.0, fmax( by0, -( by0 + P.gh[ 1 ] ) ) );
+                if ( ddx * ddx + ddy * ddy >= rb * rb ) continue;
+                int2 rg = P.cell_range[ ( size_t ) y * g0 + x ];
+                for ( int j = rg.x; j < rg.y && m > 0 && ! overflow; ++j ) {
+                    if ( j == s ) continue;
+                    double qx = P.pos[ 2 * ( size_t ) j ] - px, qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
+                    double qw = P.w ? P.w[ j ] : 0.0;
+                    double off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+                    bool moved;
+                    int nm = big_clip( *S, *D, m, lane, qx, qy, off, j, moved );
+                    if ( nm < 0 ) { overflow = true; break; }
+                    if ( moved ) { BigPoly *t = S; S = D; D = t; }
+                    m = nm;
+                }
+            }
+        }
+        const int user = P.user[ s ];
+        if ( overflow ) {
+            if ( lane == 0 ) record_error( err, 4, item.prob, user, VBIG );
+            continue;
+        }
+        // integration, edges strided over the lanes
+        double em = 0, efx = 0, efy = 0, es2 = 0;
+        int nf = 0;
+        for ( int base = 0; base < m; base += 32 ) {
+            int k = base + lane;
+            EdgeInt e;
+            e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+            if ( k < m ) {
+                int k1 = k + 1 == m ? 0 : k + 1;
+                double x0 = S->x[ k ], y0 = S->y[ k ], x1 = S->x[ k1 ], y1 = S->y[ k1 ];
+                if ( P.dkind == D_UNIFORM ) edge_uniform( x0, y0, x1, y1, P.rho, moments, e );
+                else if ( P.dkind == D_IMAGE ) {
+                    int iref = int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) );
+                    edge_image( P, px, py, iref, x0, y0, x1, y1, moments, e );
+                } else edge_gauss( P, px, py, x0, y0, x1, y1, moments, e );
+            }
+            em += e.m; efx += e.fx; efy += e.fy; es2 += e.s2;
+            bool fac = k < m && S->id[ k ] >= 0 && e.meas > 0;
+            if ( k < m ) { D->off[ k ] = fac ? e.meas : -1.0; }   // the facet measure of edge k (scratch)
+            nf += __popc( __ballot_sync( FULL, fac ) );
+        }
+        __syncwarp();
+        double mass = warp_sum( em );
+        const int row = user_order ? user : s;
+        if ( facets ) {
+            const bool to_store = nf > P.cap;
+            if ( to_store && ! P.ovf_ids ) {
+                if ( lane == 0 ) record_error( err, 4, item.prob, user, nf );
+                continue;
+            }
+            int base_at = 0;
+            if ( to_store ) {
+                if ( lane == 0 ) base_at = atomicAdd( P.ovf_count, nf );
+                base_at = __shfl_sync( FULL, base_at, 0 );
+                if ( base_at + nf > P.ovf_cap ) {
+                    if ( lane == 0 ) record_error( err, 4, item.prob, user, nf );
+                    continue;
+                }
+            }
+            int written = 0;
+            for ( int base = 0; base < m; base += 32 ) {
+                int k = base + lane;
+                double meas = k < m ? D->off[ k ] : -1.0;
+                bool fac = meas > 0;
+                unsigned fm = __ballot_sync( FULL, fac );
+                int slot = written + __popc( fm & ( ( 1u << lane ) - 1 ) );
+                if ( fac ) {
+                    int j = S->id[ k ];
+                    double dist = sqrt( S->nx[ k ] * S->nx[ k ] + S->ny[ k ] * S->ny[ k ] );
+                    double cij = meas / ( 2 * dist );
+                    int jid = user_order ? P.user[ j ] : j;
+                    if ( to_store ) { P.ovf_ids[ base_at + slot ] = jid; P.ovf_c[ base_at + slot ] = cij; }
+                    else {
+                        size_t at = ( size_t ) row * P.cap + slot;
+                        P.nid[ at ] = jid;
+                        P.nc[ at ] = cij;
+                        if ( P.nm ) P.nm[ at ] = meas;
+                    }
+                }
+                written += __popc( fm );
+            }
+            if ( lane == 0 ) {
+                P.nb[ row ] = nf;
+                if ( to_store ) P.nid[ ( size_t ) row * P.cap ] = base_at;
+            }
+        }
+        if ( moments ) {
+            double fx = warp_sum( efx ), fy = warp_sum( efy ), s2 = warp_sum( es2 );
+            if ( lane == 0 ) {
+                if ( user_order ) {
+                    if ( P.first ) {
+                        P.first[ 2 * ( size_t ) user ] = mass > 0 ? px + fx / mass : px;
+                        P.first[ 2 * ( size_t ) user + 1 ] = mass > 0 ? py + fy / mass : py;
+                    }
+                    if ( P.cost ) P.cost[ user ] = s2;
+                } else {
+                    if ( P.first ) { P.first[ 2 * ( size_t ) s ] = fx; P.first[ 2 * ( size_t ) s + 1 ] = fy; }
+                    if ( P.cost ) P.cost[ s ] = s2;
+                }
+            }
+        }
+        if ( ( flags & F_VJP ) && lane == 0 ) record_error( err, 4, item.prob, user, m );
+        if ( lane == 0 && P.mass ) P.mass[ row ] = mass;
+        __syncwarp();
+    }
+}
+
+size_t big_scratch_bytes( int warps ) { return size_t( warps ) * 2 * VBIG * ( 5 * 8 + 4 + 1 ) + 256; }
+
+void launch_cells2d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, char *scratch,
+                         int warps ) {
+    if ( count <= 0 ) return;
+    int grid = count < warps ? count : warps;
+    k_cells2d_big<<<grid, 32, 0, L.stream>>>( probs, ovf, count, flags, err, scratch );
     ++*L.launches;
 }
 

@@ -1,15 +1,464 @@
-// 3D Laguerre cells (placeholder until the warp-per-cell polyhedron clipper lands): refuses with a status.
+// 3D Laguerre cells: ONE WARP PER CELL, the polyhedron in the warp's slice of shared memory.
+//
+// The cell is kept as its dual: every vertex is a triple of plane ids (a, b, c) -- the three faces meeting there,
+// ordered so that the triples form a consistently oriented triangulation of the sphere -- and its position is
+// ALWAYS re-solved from those three planes (Cramer's rule, FP64, seed frame), so no error accumulates along the
+// cuts (the reference re-solves its float vertices for the same reason, gpu/Cell3D.cuh:1093-1147).  A cut by the
+// plane P: lanes mark the vertices outside; for each directed edge (e0, e1) of a removed vertex whose twin (e1, e0)
+// belongs to a kept vertex, the new vertex (e0, e1, P) is created; kept vertices are compacted in order and the
+// new ones appended.  This is the dual-triangulation clipping published by Ray, Sokolov, Lefebvre and Levy
+// ("Meshless Voronoi on the GPU", ACM TOG 2018), written here for a warp.
+//
+// Candidates: the Morton grid, shell by shell around the seed's grid cell, 32 at a time, each candidate pre-tested
+// by one lane against every vertex; the walk stops by the same security radius as in 2D.  Integration: signed
+// tetrahedra (seed, point of face f, K, T) for every vertex K and directed edge (f, b) of K, T the vertex across
+// that edge -- exact for volume, first and second moments; per-face areas summed in plane order (deterministic).
 #include "internal.h"
 
 namespace sdot {
 
-__global__ void k_cells3d_refuse( ErrRec *err ) {
-    if ( atomicCAS( &err->code, 0, 5 ) == 0 ) { err->kind = 2; err->prob = 0; err->seed = -1; err->needed = 0; }
+constexpr unsigned FULL3 = 0xffffffffu;
+constexpr int VC = 128;          // vertices per cell
+constexpr int PC = 96;           // planes per cell
+constexpr int W3 = 4;            // warps per block
+
+struct Cell3 {
+    double vx[ VC ], vy[ VC ], vz[ VC ];
+    double area[ 3 * VC ];                       // per (vertex, edge): the face-triangle contribution (integration)
+    double nx[ PC ], ny[ PC ], nz[ PC ], no[ PC ];
+    int pid[ PC ];
+    unsigned char va[ VC ], vb[ VC ], vc[ VC ];
+    unsigned char out[ VC ];
+    unsigned char nt[ VC ][ 3 ];                 // new triples of a cut
+    int nv, np;
+};
+
+__device__ __forceinline__ void solve3( const Cell3 &C, int a, int b, int c, double &x, double &y, double &z ) {
+    // x = ( o_a ( n_b x n_c ) + o_b ( n_c x n_a ) + o_c ( n_a x n_b ) ) / ( n_a . ( n_b x n_c ) )
+    double bcx = C.ny[ b ] * C.nz[ c ] - C.nz[ b ] * C.ny[ c ], bcy = C.nz[ b ] * C.nx[ c ] - C.nx[ b ] * C.nz[ c ],
+           bcz = C.nx[ b ] * C.ny[ c ] - C.ny[ b ] * C.nx[ c ];
+    double cax = C.ny[ c ] * C.nz[ a ] - C.nz[ c ] * C.ny[ a ], cay = C.nz[ c ] * C.nx[ a ] - C.nx[ c ] * C.nz[ a ],
+           caz = C.nx[ c ] * C.ny[ a ] - C.ny[ c ] * C.nx[ a ];
+    double abx = C.ny[ a ] * C.nz[ b ] - C.nz[ a ] * C.ny[ b ], aby = C.nz[ a ] * C.nx[ b ] - C.nx[ a ] * C.nz[ b ],
+           abz = C.nx[ a ] * C.ny[ b ] - C.ny[ a ] * C.nx[ b ];
+    double det = C.nx[ a ] * bcx + C.ny[ a ] * bcy + C.nz[ a ] * bcz;
+    double inv = 1.0 / det;
+    x = ( C.no[ a ] * bcx + C.no[ b ] * cax + C.no[ c ] * abx ) * inv;
+    y = ( C.no[ a ] * bcy + C.no[ b ] * cay + C.no[ c ] * aby ) * inv;
+    z = ( C.no[ a ] * bcz + C.no[ b ] * caz + C.no[ c ] * abz ) * inv;
+}
+
+// the vertex holding the directed edge (e0, e1), -1 if none
+__device__ __forceinline__ int twin_of( const Cell3 &C, int e0, int e1 ) {
+    for ( int t = 0; t < C.nv; ++t ) {
+        int a = C.va[ t ], b = C.vb[ t ], c = C.vc[ t ];
+        if ( ( a == e0 && b == e1 ) || ( b == e0 && c == e1 ) || ( c == e0 && a == e1 ) ) return t;
+    }
+    return -1;
+}
+
+__device__ void init_box3( Cell3 &C, int lane, const double *lo, const double *hi, double px, double py, double pz ) {
+    // planes: 0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z ; ids -1 .. -6
+    if ( lane < 6 ) {
+        int ax = lane >> 1, sg = lane & 1;
+        double p = ax == 0 ? px : ( ax == 1 ? py : pz );
+        C.nx[ lane ] = ax == 0 ? ( sg ? 1.0 : -1.0 ) : 0.0;
+        C.ny[ lane ] = ax == 1 ? ( sg ? 1.0 : -1.0 ) : 0.0;
+        C.nz[ lane ] = ax == 2 ? ( sg ? 1.0 : -1.0 ) : 0.0;
+        C.no[ lane ] = sg ? hi[ ax ] - p : p - lo[ ax ];
+        C.pid[ lane ] = -1 - lane;
+    }
+    if ( lane < 8 ) {
+        int sx = lane & 1, sy = ( lane >> 1 ) & 1, sz = ( lane >> 2 ) & 1;
+        int a = sx, b = 2 + sy, c = 4 + sz;
+        // orientation: det( n_a, n_b, n_c ) > 0 ; det( +-x, +-y, +-z ) = sx' sy' sz'
+        int s = ( sx ? 1 : -1 ) * ( sy ? 1 : -1 ) * ( sz ? 1 : -1 );
+        if ( s < 0 ) { int t = b; b = c; c = t; }
+        C.va[ lane ] = a; C.vb[ lane ] = b; C.vc[ lane ] = c;
+        C.vx[ lane ] = ( sx ? hi[ 0 ] : lo[ 0 ] ) - px;
+        C.vy[ lane ] = ( sy ? hi[ 1 ] : lo[ 1 ] ) - py;
+        C.vz[ lane ] = ( sz ? hi[ 2 ] : lo[ 2 ] ) - pz;
+    }
+    if ( lane == 0 ) { C.nv = 8; C.np = 6; }
+    __syncwarp();
+}
+
+// drops the planes no vertex uses (when the plane table is full); false if it cannot make room
+__device__ bool compact_planes( Cell3 &C, int lane ) {
+    __shared__ unsigned char used_all[ W3 ][ PC ];
+    unsigned char *used = used_all[ threadIdx.x >> 5 ];
+    for ( int p = lane; p < PC; p += 32 ) used[ p ] = 0;
+    __syncwarp();
+    for ( int k = lane; k < C.nv; k += 32 ) { used[ C.va[ k ] ] = 1; used[ C.vb[ k ] ] = 1; used[ C.vc[ k ] ] = 1; }
+    __syncwarp();
+    // new index of each used plane: a serial prefix by lane 0 (rare path)
+    __shared__ unsigned char remap_all[ W3 ][ PC ];
+    unsigned char *remap = remap_all[ threadIdx.x >> 5 ];
+    if ( lane == 0 ) {
+        int q = 0;
+        for ( int p = 0; p < C.np; ++p ) {
+            if ( ! used[ p ] ) continue;
+            remap[ p ] = ( unsigned char ) q;
+            C.nx[ q ] = C.nx[ p ]; C.ny[ q ] = C.ny[ p ]; C.nz[ q ] = C.nz[ p ]; C.no[ q ] = C.no[ p ]; C.pid[ q ] = C.pid[ p ];
+            ++q;
+        }
+        C.np = q;
+    }
+    __syncwarp();
+    for ( int k = lane; k < C.nv; k += 32 ) { C.va[ k ] = remap[ C.va[ k ] ]; C.vb[ k ] = remap[ C.vb[ k ] ]; C.vc[ k ] = remap[ C.vc[ k ] ]; }
+    __syncwarp();
+    return C.np < PC;
+}
+
+// keep n . y <= off; false past a capacity
+__device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, double off, int id ) {
+    const int nv = C.nv;
+    int nout = 0;
+    for ( int base = 0; base < nv; base += 32 ) {
+        int k = base + lane;
+        bool o = k < nv && nx * C.vx[ k ] + ny * C.vy[ k ] + nz * C.vz[ k ] > off;
+        if ( k < nv ) C.out[ k ] = o;
+        nout += __popc( __ballot_sync( FULL3, o ) );
+    }
+    __syncwarp();
+    if ( nout == 0 ) return true;
+    if ( nout == nv ) {
+        if ( lane == 0 ) C.nv = 0;
+        __syncwarp();
+        return true;
+    }
+    const bool full = C.np >= PC;
+    __syncwarp();
+    if ( full && ! compact_planes( C, lane ) ) return false;
+    const int P = C.np;
+    __syncwarp();
+    if ( lane == 0 ) { C.nx[ P ] = nx; C.ny[ P ] = ny; C.nz[ P ] = nz; C.no[ P ] = off; C.pid[ P ] = id; C.np = P + 1; }
+    // the boundary edges: directed edges of removed vertices whose twin is kept
+    int nnew = 0;
+    for ( int base = 0; base < nv; base += 32 ) {
+        int k = base + lane;
+        unsigned char tr[ 3 ][ 3 ];
+        int cnt = 0;
+        if ( k < nv && C.out[ k ] ) {
+            int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+            for ( int q = 0; q < 3; ++q ) {
+                int e0 = e[ q ], e1 = e[ ( q + 1 ) % 3 ];
+                int t = twin_of( C, e1, e0 );
+                if ( t >= 0 && ! C.out[ t ] ) { tr[ cnt ][ 0 ] = e0; tr[ cnt ][ 1 ] = e1; tr[ cnt ][ 2 ] = P; ++cnt; }
+            }
+        }
+        int inc = cnt;
+#pragma unroll
+        for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL3, inc, o ); if ( lane >= o ) inc += t; }
+        int total = __shfl_sync( FULL3, inc, 31 );
+        int at = nnew + inc - cnt;
+        for ( int q = 0; q < cnt; ++q )
+            if ( at + q < VC ) { C.nt[ at + q ][ 0 ] = tr[ q ][ 0 ]; C.nt[ at + q ][ 1 ] = tr[ q ][ 1 ]; C.nt[ at + q ][ 2 ] = tr[ q ][ 2 ]; }
+        nnew += total;
+    }
+    __syncwarp();
+    const int nkeep = nv - nout;
+    if ( nkeep + nnew > VC || nnew >= VC ) return false;
+    // compaction of the kept vertices, in order (destinations never pass their sources)
+    int kept_before = 0;
+    for ( int base = 0; base < nv; base += 32 ) {
+        int k = base + lane;
+        bool keep = k < nv && ! C.out[ k ];
+        unsigned m = __ballot_sync( FULL3, keep );
+        int dst = kept_before + __popc( m & ( ( 1u << lane ) - 1 ) );
+        double x = 0, y = 0, z = 0;
+        unsigned char a = 0, b = 0, c = 0;
+        if ( keep ) { x = C.vx[ k ]; y = C.vy[ k ]; z = C.vz[ k ]; a = C.va[ k ]; b = C.vb[ k ]; c = C.vc[ k ]; }
+        __syncwarp();
+        if ( keep ) { C.vx[ dst ] = x; C.vy[ dst ] = y; C.vz[ dst ] = z; C.va[ dst ] = a; C.vb[ dst ] = b; C.vc[ dst ] = c; }
+        __syncwarp();
+        kept_before += __popc( m );
+    }
+    // the new vertices, re-solved from their three planes
+    for ( int j = lane; j < nnew; j += 32 ) {
+        int a = C.nt[ j ][ 0 ], b = C.nt[ j ][ 1 ], c = C.nt[ j ][ 2 ];
+        double x, y, z;
+        solve3( C, a, b, c, x, y, z );
+        int d = nkeep + j;
+        C.va[ d ] = a; C.vb[ d ] = b; C.vc[ d ] = c;
+        C.vx[ d ] = x; C.vy[ d ] = y; C.vz[ d ] = z;
+    }
+    if ( lane == 0 ) C.nv = nkeep + nnew;
+    __syncwarp();
+    return true;
+}
+
+__device__ __forceinline__ void record_error3( ErrRec *err, int code, int prob, int seed, int needed ) {
+    if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
+}
+
+__device__ __forceinline__ double g_of3( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return p == 0 ? log( x ) : ( pow( x, p ) - 1 ) / p;
+    return r == 1 ? log( x ) : x - 1;
+}
+__device__ __forceinline__ double gp_of3( double x, int r, double p ) {
+    x = fmax( x, 1e-300 );
+    if ( r == 2 ) return pow( x, p - 1 );
+    return r == 1 ? 1 / x : 1;
+}
+
+__global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+                                                        unsigned flags, ErrRec *err ) {
+    extern __shared__ char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Cell3 &C = reinterpret_cast<Cell3 *>( smem )[ warp ];
+    __shared__ double sh_rep[ W3 ][ NB_REPORT ];
+    __shared__ int sh_last;
+    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+    for ( int cidx = blockIdx.x; cidx < nchunks; cidx += gridDim.x ) {
+        const Chunk ch = chunks[ cidx ];
+        const ProbDev &P = probs[ ch.prob ];
+        double rep[ NB_REPORT ];
+        rep[ R_WORST ] = 0; rep[ R_WORST_REL ] = 0; rep[ R_AMIN ] = 1e300; rep[ R_ASUM ] = 0; rep[ R_LIN2 ] = 0; rep[ R_GCOUNT ] = 0;
+        rep[ R_GMEAN ] = 0; rep[ R_GM2 ] = 0; rep[ R_SU ] = 0; rep[ R_SUG ] = 0; rep[ R_NUSUM ] = 0; rep[ R_NEMPTY ] = 0;
+        const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
+        for ( int s = ch.begin + warp; s < ch.end; s += W3 ) {
+            const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
+            const double wi = P.w ? P.w[ s ] : 0.0;
+            init_box3( C, lane, P.lo, P.hi, px, py, pz );
+            bool overflow = false;
+            int c0[ 3 ];
+            for ( int a = 0; a < 3; ++a ) {
+                double x = a == 0 ? px : ( a == 1 ? py : pz );
+                int k = int( floor( ( x - P.go[ a ] ) / P.gh[ a ] ) );
+                c0[ a ] = k < 0 ? 0 : ( k >= P.g[ a ] ? P.g[ a ] - 1 : k );
+            }
+            int rmax = 0;
+            for ( int a = 0; a < 3; ++a ) rmax = max( rmax, max( c0[ a ], P.g[ a ] - 1 - c0[ a ] ) );
+            for ( int r = 0; r <= rmax && C.nv > 0 && ! overflow; ++r ) {
+                const int side = 2 * r + 1, ncube = side * side * side;
+                for ( int cb = 0; cb < ncube && C.nv > 0 && ! overflow; cb += 32 ) {
+                    int ci = cb + lane, beg = 0, cnt = 0;
+                    if ( ci < ncube ) {
+                        int dx = ci % side - r, dy = ( ci / side ) % side - r, dz = ci / ( side * side ) - r;
+                        bool shell = max( abs( dx ), max( abs( dy ), abs( dz ) ) ) == r;
+                        int x = c0[ 0 ] + dx, y = c0[ 1 ] + dy, z = c0[ 2 ] + dz;
+                        if ( shell && x >= 0 && x < P.g[ 0 ] && y >= 0 && y < P.g[ 1 ] && z >= 0 && z < P.g[ 2 ] ) {
+                            int2 rg = P.cell_range[ ( ( size_t ) z * P.g[ 1 ] + y ) * P.g[ 0 ] + x ];
+                            beg = rg.x;
+                            cnt = rg.y - rg.x;
+                        }
+                    }
+                    int inc = cnt;
+#pragma unroll
+                    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL3, inc, o ); if ( lane >= o ) inc += t; }
+                    const int total = __shfl_sync( FULL3, inc, 31 );
+                    const int exc = inc - cnt;
+                    for ( int t0 = 0; t0 < total && C.nv > 0 && ! overflow; t0 += 32 ) {
+                        const int t = t0 + lane;
+                        int owner = 0;
+#pragma unroll
+                        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL3, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
+                        owner = owner > 31 ? 31 : owner;
+                        int obeg = __shfl_sync( FULL3, beg, owner ), oexc = __shfl_sync( FULL3, exc, owner );
+                        int j = obeg + ( t - oexc );
+                        bool valid = t < total && j != s;
+                        double qx = 0, qy = 0, qz = 0, off = 0;
+                        if ( valid ) {
+                            qx = P.pos[ 3 * ( size_t ) j ] - px;
+                            qy = P.pos[ 3 * ( size_t ) j + 1 ] - py;
+                            qz = P.pos[ 3 * ( size_t ) j + 2 ] - pz;
+                            double qw = P.w ? P.w[ j ] : 0.0;
+                            off = 0.5 * ( qx * qx + qy * qy + qz * qz + wi - qw );
+                        }
+                        bool cuts = false;
+                        for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] > off;
+                        unsigned todo = __ballot_sync( FULL3, valid && cuts );
+                        while ( todo ) {
+                            int k = __ffs( todo ) - 1;
+                            todo &= todo - 1;
+                            double nx = __shfl_sync( FULL3, qx, k ), ny = __shfl_sync( FULL3, qy, k ), nz = __shfl_sync( FULL3, qz, k );
+                            double no = __shfl_sync( FULL3, off, k );
+                            int nid = __shfl_sync( FULL3, j, k );
+                            if ( ! wclip3( C, lane, nx, ny, nz, no, nid ) ) { overflow = true; break; }
+                            if ( C.nv == 0 ) break;
+                        }
+                    }
+                }
+                if ( C.nv == 0 || overflow ) break;
+                double R2 = 0;
+                for ( int k = lane; k < C.nv; k += 32 ) R2 = fmax( R2, C.vx[ k ] * C.vx[ k ] + C.vy[ k ] * C.vy[ k ] + C.vz[ k ] * C.vz[ k ] );
+                R2 = warp_max( R2 );
+                double ex = R2 + wmax - wi;
+                if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+            }
+            const int user = P.user[ s ];
+            if ( overflow ) {
+                if ( lane == 0 ) record_error3( err, 4, ch.prob, user, VC );
+                if ( lane == 0 ) C.nv = 0;
+                __syncwarp();
+            }
+            // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once
+            double vol = 0, fx = 0, fy = 0, fz = 0, s2 = 0;
+            const int nv = C.nv;
+            for ( int k = lane; k < nv; k += 32 ) {
+                int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+                double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
+                for ( int q = 0; q < 3; ++q ) {
+                    int f = e[ q ], b = e[ ( q + 1 ) % 3 ];
+                    int t = twin_of( C, b, f );
+                    double a2 = 0;
+                    if ( t >= 0 ) {
+                        double Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
+                        double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
+                        double cf = C.no[ f ] / nn;
+                        double Cx = C.nx[ f ] * cf, Cy = C.ny[ f ] * cf, Cz = C.nz[ f ] * cf;
+                        // det( c_f, K, T ) with the sign that makes the box positive
+                        double det = -( Cx * ( Ky * Tz - Kz * Ty ) - Cy * ( Kx * Tz - Kz * Tx ) + Cz * ( Kx * Ty - Ky * Tx ) );
+                        double tv = det / 6;
+                        vol += tv;
+                        if ( moments ) {
+                            fx += tv * ( Cx + Kx + Tx ) / 4;
+                            fy += tv * ( Cy + Ky + Ty ) / 4;
+                            fz += tv * ( Cz + Kz + Tz ) / 4;
+                            s2 += tv / 10 * ( Cx * Cx + Cy * Cy + Cz * Cz + Kx * Kx + Ky * Ky + Kz * Kz + Tx * Tx + Ty * Ty + Tz * Tz +
+                                              Cx * Kx + Cy * Ky + Cz * Kz + Cx * Tx + Cy * Ty + Cz * Tz + Kx * Tx + Ky * Ty + Kz * Tz );
+                        }
+                        // the area of the face triangle ( c_f, K, T ) along the unit normal
+                        double ux = Kx - Cx, uy = Ky - Cy, uz = Kz - Cz, vx = Tx - Cx, vy = Ty - Cy, vz = Tz - Cz;
+                        double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+                        a2 = -( cx * C.nx[ f ] + cy * C.ny[ f ] + cz * C.nz[ f ] ) / ( 2 * sqrt( nn ) );
+                    }
+                    C.area[ 3 * k + q ] = a2;
+                }
+            }
+            __syncwarp();
+            double mass = P.rho * warp_sum( vol );
+            // the facets: per plane, its triangles summed in vertex order
+            int nf = 0;
+            if ( facets || ( flags & F_REPORT ) ) {
+                const int row = user_order ? user : s;
+                int written = 0;
+                for ( int pbase = 0; pbase < C.np; pbase += 32 ) {
+                    int p = pbase + lane;
+                    double ar = 0;
+                    bool seed_plane = p < C.np && C.pid[ p ] >= 0;
+                    if ( seed_plane )
+                        for ( int k = 0; k < nv; ++k ) {
+                            if ( C.va[ k ] == p ) ar += C.area[ 3 * k ];
+                            if ( C.vb[ k ] == p ) ar += C.area[ 3 * k + 1 ];
+                            if ( C.vc[ k ] == p ) ar += C.area[ 3 * k + 2 ];
+                        }
+                    bool fac = seed_plane && ar > 0;
+                    unsigned fm = __ballot_sync( FULL3, fac );
+                    int slot = written + __popc( fm & ( ( 1u << lane ) - 1 ) );
+                    if ( facets && fac && slot < P.cap ) {
+                        double dist = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
+                        size_t at = ( size_t ) row * P.cap + slot;
+                        int j = C.pid[ p ];
+                        P.nid[ at ] = user_order ? P.user[ j ] : j;
+                        P.nc[ at ] = P.rho * ar / ( 2 * dist );
+                        if ( P.nm ) P.nm[ at ] = P.rho * ar;
+                    }
+                    written += __popc( fm );
+                }
+                nf = written;
+                if ( facets && nf > P.cap ) {
+                    if ( lane == 0 ) record_error3( err, 4, ch.prob, user, nf );
+                    nf = P.cap;
+                }
+                if ( facets && lane == 0 ) P.nb[ row ] = nf;
+            }
+            if ( moments ) {
+                double mx = warp_sum( fx ), my = warp_sum( fy ), mz = warp_sum( fz ), ss = warp_sum( s2 );
+                double vv = mass / P.rho;
+                if ( lane == 0 ) {
+                    if ( user_order ) {
+                        if ( P.first ) {
+                            P.first[ 3 * ( size_t ) user ] = vv > 0 ? px + mx / vv : px;
+                            P.first[ 3 * ( size_t ) user + 1 ] = vv > 0 ? py + my / vv : py;
+                            P.first[ 3 * ( size_t ) user + 2 ] = vv > 0 ? pz + mz / vv : pz;
+                        }
+                        if ( P.cost ) P.cost[ user ] = P.rho * ss;
+                    } else {
+                        if ( P.first ) { P.first[ 3 * ( size_t ) s ] = P.rho * mx; P.first[ 3 * ( size_t ) s + 1 ] = P.rho * my; P.first[ 3 * ( size_t ) s + 2 ] = P.rho * mz; }
+                        if ( P.cost ) P.cost[ s ] = P.rho * ss;
+                    }
+                }
+            }
+            if ( lane == 0 && P.mass ) P.mass[ user_order ? user : s ] = mass;
+            if ( ( flags & F_REPORT ) && lane == 0 ) {
+                double nu = P.nu[ s ];
+                double e2 = fabs( nu - mass );
+                rep[ R_WORST ] = fmax( rep[ R_WORST ], e2 );
+                rep[ R_WORST_REL ] = fmax( rep[ R_WORST_REL ], e2 / nu );
+                rep[ R_AMIN ] = fmin( rep[ R_AMIN ], mass );
+                rep[ R_ASUM ] += mass;
+                rep[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
+                double x = mass / nu, g = g_of3( x, P.res, P.power );
+                double n1 = rep[ R_GCOUNT ] + 1, d = g - rep[ R_GMEAN ];
+                rep[ R_GMEAN ] += d / n1;
+                rep[ R_GM2 ] += d * ( g - rep[ R_GMEAN ] );
+                rep[ R_GCOUNT ] = n1;
+                double u = nu / gp_of3( x, P.res, P.power );
+                rep[ R_SU ] += u;
+                rep[ R_SUG ] += u * g;
+                rep[ R_NUSUM ] += nu;
+                rep[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
+            }
+            __syncwarp();
+        }
+        if ( flags & F_REPORT ) {
+            // the chunk's report, then the last chunk of the problem folds them in chunk order
+            if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
+            __syncthreads();
+            if ( threadIdx.x == 0 ) {
+                double r[ NB_REPORT ];
+                for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = sh_rep[ 0 ][ k ];
+                auto fold = [&]( const double *o ) {
+                    r[ R_WORST ] = fmax( r[ R_WORST ], o[ R_WORST ] );
+                    r[ R_WORST_REL ] = fmax( r[ R_WORST_REL ], o[ R_WORST_REL ] );
+                    r[ R_AMIN ] = fmin( r[ R_AMIN ], o[ R_AMIN ] );
+                    r[ R_ASUM ] += o[ R_ASUM ];
+                    r[ R_LIN2 ] += o[ R_LIN2 ];
+                    double na = r[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
+                    if ( nb > 0 ) {
+                        double d = o[ R_GMEAN ] - r[ R_GMEAN ];
+                        r[ R_GMEAN ] += d * nb / n;
+                        r[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
+                        r[ R_GCOUNT ] = n;
+                    }
+                    r[ R_SU ] += o[ R_SU ]; r[ R_SUG ] += o[ R_SUG ]; r[ R_NUSUM ] += o[ R_NUSUM ]; r[ R_NEMPTY ] += o[ R_NEMPTY ];
+                };
+                for ( int w = 1; w < W3; ++w ) fold( sh_rep[ w ] );
+                double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
+                for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r[ k ];
+                __threadfence();
+                unsigned prev = atomicAdd( P.counter, 1u );
+                sh_last = prev == unsigned( P.nchunk - 1 );
+                if ( sh_last ) {
+                    __threadfence();
+                    const volatile double *src = P.partials;
+                    for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = src[ k ];
+                    for ( int c = 1; c < P.nchunk; ++c ) {
+                        double o[ NB_REPORT ];
+                        for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ ( size_t ) c * NB_REPORT + k ];
+                        fold( o );
+                    }
+                    for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r[ k ];
+                    *P.counter = 0;
+                }
+            }
+            __syncthreads();
+        }
+    }
 }
 
 void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err ) {
-    (void) probs; (void) chunks; (void) nchunks; (void) flags;
-    k_cells3d_refuse<<<1, 1, 0, L.stream>>>( err );
+    if ( nchunks <= 0 ) return;
+    const size_t smem = sizeof( Cell3 ) * W3;
+    static bool configured = false;
+    if ( ! configured ) {
+        cudaFuncSetAttribute( k_cells3d, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
+        configured = true;
+    }
+    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err );
     ++*L.launches;
 }
 

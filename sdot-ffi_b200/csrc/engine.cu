@@ -67,6 +67,15 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
     CK( cudaMallocHost( &c.herr, sizeof( ErrRec ) ) );
     std::memset( c.herr, 0, sizeof( ErrRec ) );
     for ( int s = c.max_slots - 1; s >= 0; --s ) c.free_slots.push_back( s );
+    // the big-cell queue: OvfList header then its items, in one allocation
+    const int ovf_cap = 1 << 16;
+    char *q = ( char * ) dalloc( c, 256 + size_t( ovf_cap ) * sizeof( OvfItem ) );
+    c.dovf = ( OvfList * ) q;
+    OvfList hl{ 0, ovf_cap, ( OvfItem * ) ( q + 256 ) };
+    CK( cudaMemcpyAsync( c.dovf, &hl, sizeof( hl ), cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaMallocHost( &c.hovf, sizeof( int ) ) );
+    *c.hovf = 0;
+    c.big_scratch = ( char * ) dalloc( c, big_scratch_bytes( c.big_warps ) );
     const char *t = std::getenv( "SDOT_KERNEL_TIMING" );
     c.timer.on = t && t[ 0 ] == '1';
     CK( cudaStreamSynchronize( c.stream ) );
@@ -80,11 +89,14 @@ void ctx_release( Ctx &c ) {
         if ( c.dscal ) cudaFreeAsync( c.dscal, c.stream );
         if ( c.dcount ) cudaFreeAsync( c.dcount, c.stream );
         if ( c.derr ) cudaFreeAsync( c.derr, c.stream );
+        if ( c.dovf ) cudaFreeAsync( c.dovf, c.stream );
+        if ( c.big_scratch ) cudaFreeAsync( c.big_scratch, c.stream );
         cudaStreamSynchronize( c.stream );
         cudaStreamDestroy( c.stream );
     }
     if ( c.hscal ) cudaFreeHost( c.hscal );
     if ( c.herr ) cudaFreeHost( c.herr );
+    if ( c.hovf ) cudaFreeHost( c.hovf );
     if ( c.pool ) cudaMemPoolDestroy( c.pool );
     c = Ctx{};
 }
@@ -187,6 +199,14 @@ static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
     }
     CK( cudaMemcpyAsync( c.desc, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
     return c.desc;
+}
+
+// a second block in the upload area, after `offset` bytes already uploaded by this step (stream ordered)
+static char *upload_desc_at( Ctx &c, const void *src, size_t bytes, size_t offset ) {
+    offset = ( offset + 255 ) & ~size_t( 255 );
+    if ( offset + bytes > c.desc_bytes ) throw Error( SDOT_ERR_NO_MEMORY, "descriptor area too small for the big cells" );
+    CK( cudaMemcpyAsync( c.desc + offset, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
+    return c.desc + offset;
 }
 
 void check_errors( Ctx &c, const char *where ) {
@@ -357,6 +377,9 @@ struct SolveJob {
     double *w, *w2, *a, *a2, *d, *nu, *nu_dev_user, *b, *x, *r, *z, *p, *q, *dia, *val, *tmpw;
     int *nb[ 2 ], *nid[ 2 ];
     double *nc[ 2 ];
+    int *ovf_count[ 2 ], *ovf_ids[ 2 ];
+    double *ovf_c[ 2 ];
+    int ovf_cap = 0;
     int cur = 0;
     int *row_ptr, *col, *rowcnt;
     double *part_cells, *part_vec;
@@ -408,9 +431,10 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     const int dim = J.G.dim, cap = J.cap;
     J.nch_cells = int( ( n + CHUNK - 1 ) / CHUNK );
     J.nch_vec = int( ( n + VCHUNK - 1 ) / VCHUNK );
+    J.ovf_cap = dim == 2 ? int( n ) + 4096 : 0;
     size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                    size_t( n ) * 4 + size_t( J.nch_cells ) * NB_REPORT * 8 + size_t( J.nch_vec ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) +
-                   40 * 256;
+                   2 * ( size_t( J.ovf_cap ) * 12 + 16 ) + 48 * 256;
     J.mem_bytes = bytes;
     J.mem = ( char * ) dalloc( c, bytes );
     Arena A{ J.mem, bytes, 0 };
@@ -418,7 +442,10 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     J.d = A.take<double>( n ); J.nu = A.take<double>( n ); J.nu_dev_user = A.take<double>( n ); J.b = A.take<double>( n );
     J.x = A.take<double>( n ); J.r = A.take<double>( n ); J.z = A.take<double>( n ); J.p = A.take<double>( n );
     J.q = A.take<double>( n ); J.dia = A.take<double>( n ); J.tmpw = A.take<double>( n );
-    for ( int k = 0; k < 2; ++k ) { J.nb[ k ] = A.take<int>( n ); J.nid[ k ] = A.take<int>( size_t( n ) * cap ); J.nc[ k ] = A.take<double>( size_t( n ) * cap ); }
+    for ( int k = 0; k < 2; ++k ) {
+        J.nb[ k ] = A.take<int>( n ); J.nid[ k ] = A.take<int>( size_t( n ) * cap ); J.nc[ k ] = A.take<double>( size_t( n ) * cap );
+        J.ovf_count[ k ] = A.take<int>( 4 ); J.ovf_ids[ k ] = A.take<int>( J.ovf_cap ); J.ovf_c[ k ] = A.take<double>( J.ovf_cap );
+    }
     J.row_ptr = A.take<int>( n + 1 );
     J.col = A.take<int>( size_t( n ) * cap );
     J.val = A.take<double>( size_t( n ) * cap );
@@ -807,6 +834,8 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.nb = J.nb[ J.cur ];
     V.nid = J.nid[ J.cur ];
     V.nc = J.nc[ J.cur ];
+    V.ovf_ids = J.ovf_ids[ J.cur ];
+    V.ovf_c = J.ovf_c[ J.cur ];
     V.row_ptr = J.row_ptr;
     V.col = J.col;
     V.val = J.val;
@@ -922,7 +951,13 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         P.w = R.w;
         P.wmax_slot = R.wslot;
         P.mass = R.mass;
-        if ( R.table >= 0 ) { P.nb = J->nb[ R.table ]; P.nid = J->nid[ R.table ]; P.nc = J->nc[ R.table ]; }
+        if ( R.table >= 0 ) {
+            P.nb = J->nb[ R.table ]; P.nid = J->nid[ R.table ]; P.nc = J->nc[ R.table ];
+            if ( J->ovf_cap ) {
+                P.ovf_count = J->ovf_count[ R.table ]; P.ovf_cap = J->ovf_cap; P.ovf_ids = J->ovf_ids[ R.table ]; P.ovf_c = J->ovf_c[ R.table ];
+                CK( cudaMemsetAsync( P.ovf_count, 0, sizeof( int ), c.stream ) );
+            }
+        }
         P.nu = J->nu;
         P.res = J->res_cur;
         P.power = J->opt[ SDOT_OPT_POWER ];
@@ -941,31 +976,35 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         int k = 0;
         for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) CC.push_back( Chunk{ pi, b, std::min( J->G.n, b + CHUNK ), k } );
     }
+    // the launch arrays of the 2D cells, kept for the big-cell pass: [ normal diagrams | final (moments) diagrams ]
+    std::vector<ProbDev> big_probs;
+    std::vector<std::vector<Chunk>> big_chunks;      // per problem of big_probs, its chunks (for a report recompute)
     auto run_cells = [&]( std::vector<ProbDev> &PP, std::vector<Chunk> &CC, int dim, bool report_only ) {
         if ( PP.empty() ) return;
-        // flags are uniform per launch: a final (moments) diagram goes with its own launch
-        std::vector<ProbDev> PA, PB;
+        // flags are uniform per launch: final (moments) diagrams go in their own launch, after the others in one array
+        std::vector<ProbDev> PX;
         std::vector<Chunk> CA, CB;
+        std::vector<int> idx( PP.size(), -1 );
+        for ( int pass = 0; pass < 2; ++pass )
+            for ( size_t k = 0; k < PP.size(); ++k )
+                if ( ( PP[ k ].first != nullptr ) == ( pass == 1 ) ) { idx[ k ] = int( PX.size() ); PX.push_back( PP[ k ] ); }
         for ( auto &ch : CC ) {
-            bool mom = PP[ ch.prob ].first != nullptr;
-            auto &PX = mom ? PB : PA;
-            auto &CX = mom ? CB : CA;
-            if ( ch.index == 0 ) { ProbDev q = PP[ ch.prob ]; q.chunk0 = int( CX.size() ); PX.push_back( q ); }
             Chunk x = ch;
-            x.prob = int( PX.size() ) - 1;
-            CX.push_back( x );
+            x.prob = idx[ ch.prob ];
+            ( PP[ ch.prob ].first != nullptr ? CB : CA ).push_back( x );
         }
+        size_t b1 = PX.size() * sizeof( ProbDev ), o2 = ( b1 + 255 ) & ~size_t( 255 ), b2 = CA.size() * sizeof( Chunk ),
+               o3 = o2 + ( ( b2 + 255 ) & ~size_t( 255 ) ), b3 = CB.size() * sizeof( Chunk );
+        std::vector<char> buf( o3 + b3 );
+        std::memcpy( buf.data(), PX.data(), b1 );
+        if ( b2 ) std::memcpy( buf.data() + o2, CA.data(), b2 );
+        if ( b3 ) std::memcpy( buf.data() + o3, CB.data(), b3 );
+        char *d = upload_desc( c, buf.data(), buf.size() );
+        ProbDev *dp = reinterpret_cast<ProbDev *>( d );
         for ( int pass = 0; pass < 2; ++pass ) {
-            auto &PX = pass ? PB : PA;
-            auto &CX = pass ? CB : CA;
-            if ( PX.empty() ) continue;
-            size_t b1 = PX.size() * sizeof( ProbDev ), o2 = ( b1 + 255 ) & ~size_t( 255 ), b2 = CX.size() * sizeof( Chunk );
-            std::vector<char> buf( o2 + b2 );
-            std::memcpy( buf.data(), PX.data(), b1 );
-            std::memcpy( buf.data() + o2, CX.data(), b2 );
-            char *d = upload_desc( c, buf.data(), buf.size() );
-            ProbDev *dp = reinterpret_cast<ProbDev *>( d );
-            Chunk *dc = reinterpret_cast<Chunk *>( d + o2 );
+            std::vector<Chunk> &CX = pass ? CB : CA;
+            if ( CX.empty() ) continue;
+            Chunk *dc = reinterpret_cast<Chunk *>( d + ( pass ? o3 : o2 ) );
             double seeds = 0;
             for ( auto &ch : CX ) seeds += ch.end - ch.begin;
             if ( report_only ) {
@@ -975,12 +1014,18 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             } else {
                 unsigned flags = pass ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
                 c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
-                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX.size() ), flags, c.derr );
+                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX.size() ), flags, c.derr, c.dovf );
                 else launch_cells3d( L, dp, dc, int( CX.size() ), flags, c.derr );
                 c.timer.end( c.stream );
             }
         }
+        if ( dim == 2 && ! report_only ) {
+            big_probs = PX;
+            big_chunks.assign( PX.size(), {} );
+            for ( auto &ch : CA ) big_chunks[ ch.prob ].push_back( ch );
+        }
     };
+    CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
     run_cells( P2, C2, 2, false );
     run_cells( P3, C3, 3, false );
     run_cells( PR, CR, 2, true );
@@ -1005,8 +1050,38 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     for ( SolveJob *J : jobs ) top = std::max( top, J->slot + 1 );
     CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaMemcpyAsync( c.hovf, &c.dovf->count, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaStreamSynchronize( c.stream ) );
     check_errors( c, "cells" );
+    if ( *c.hovf > 0 ) {
+        // the big cells: rebuilt in global memory, then the reports of their problems recomputed from the masses
+        const int count = std::min( *c.hovf, ( 1 << 16 ) );
+        std::vector<OvfItem> items( count );
+        CK( cudaMemcpy( items.data(), ( char * ) c.dovf + 256, count * sizeof( OvfItem ), cudaMemcpyDeviceToHost ) );
+        ProbDev *dp = reinterpret_cast<ProbDev *>( upload_desc( c, big_probs.data(), big_probs.size() * sizeof( ProbDev ) ) );
+        bool moments = false, normal = false;
+        std::vector<char> touched( big_probs.size(), 0 );
+        for ( auto &it : items ) {
+            touched[ it.prob ] = 1;
+            ( big_probs[ it.prob ].first ? moments : normal ) = true;
+        }
+        if ( normal && moments ) throw Error( SDOT_ERR_CAPACITY, "big cells in a normal and a final diagram of one tick" );
+        c.timer.begin( c.stream, K_CELLS2D, double( count ) );
+        launch_cells2d_big( L, dp, c.dovf, count, moments ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ), c.derr, c.big_scratch,
+                            c.big_warps );
+        c.timer.end( c.stream );
+        std::vector<Chunk> rc;
+        for ( size_t k = 0; k < big_probs.size(); ++k )
+            if ( touched[ k ] && big_probs[ k ].report ) rc.insert( rc.end(), big_chunks[ k ].begin(), big_chunks[ k ].end() );
+        if ( ! rc.empty() ) {
+            Chunk *dc = reinterpret_cast<Chunk *>( upload_desc_at( c, rc.data(), rc.size() * sizeof( Chunk ), big_probs.size() * sizeof( ProbDev ) ) );
+            launch_report( L, dp, dc, int( rc.size() ) );
+        }
+        CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+        check_errors( c, "big cells" );
+    }
     for ( SolveJob *J : jobs ) {
         if ( J->state == J_DONE ) continue;
         bool hd = std::find( with_diag.begin(), with_diag.end(), J ) != with_diag.end();

@@ -32,6 +32,11 @@ struct Ctx {
     std::vector<int> free_slots;
     ErrRec *derr = nullptr;
     ErrRec *herr = nullptr;           // pinned
+    // the queue of big cells (device) and its count's host mirror; the global-memory polygons of the big-cell pass
+    OvfList *dovf = nullptr;
+    int *hovf = nullptr;
+    char *big_scratch = nullptr;
+    int big_warps = 256;
     // descriptor upload area
     char *desc = nullptr;
     size_t desc_bytes = 0;

@@ -74,7 +74,21 @@ struct ProbDev {
     int chunk0, nchunk;           // this problem's chunks in the launch's table
     int res;                      // residual kind for the report (0 lin, 1 log, 2 power)
     double power;
+    // the facets of the cells past `cap` (rank order only): nb[ row ] > cap, nid[ row * cap ] = offset in the store
+    int *ovf_count;
+    int ovf_cap;
+    int *ovf_ids;
+    double *ovf_c;
 };
+
+// cells the warp-register kernel could not hold (more than 32 vertices, or more facets than the table's row):
+// queued here and rebuilt by the global-memory kernel
+struct OvfItem { int prob; int seed; };
+struct OvfList {
+    int count, cap;
+    OvfItem *items;
+};
+constexpr int VBIG = 4096;       // vertices of a cell in the global-memory pass
 
 struct Chunk {
     int prob;      // index into the launch's ProbDev array
@@ -105,6 +119,8 @@ struct VecDev {
     const int *nb;
     const int *nid;
     const double *nc;
+    const int *ovf_ids;           // the facets of the rows past `cap` (see ProbDev)
+    const double *ovf_c;
     int *row_ptr;                 // [n + 1]
     int *col;                     // [n * cap]
     double *val;                  // [n * cap]  c_ij > 0 (the matrix holds -c_ij)
@@ -208,7 +224,11 @@ void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 
 // cells2d.cu / cells3d.cu
-void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err );
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
+// the queued big cells (count known on the host), polygons in `scratch` (VBIG vertices x 2 buffers per warp)
+void launch_cells2d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, char *scratch,
+                         int warps );
+size_t big_scratch_bytes( int warps );
 void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks );
 void launch_scale( const Launch &L, double *v, int n, double s );
 void launch_scatter( const Launch &L, const double *ranked, const int *user, int n, int dim, double *out_user );

@@ -68,9 +68,17 @@ __device__ __forceinline__ bool fold_last( const VecDev &V, const Chunk &ch, con
 }
 
 // ---- CSR -------------------------------------------------------------------------------------------------------
+// the facets of a row: its table row, or its slice of the overflow store when it has more than `cap`
+__device__ __forceinline__ const int *row_ids( const VecDev &V, int row, int nb ) {
+    return nb > V.cap ? V.ovf_ids + V.nid[ ( size_t ) row * V.cap ] : V.nid + ( size_t ) row * V.cap;
+}
+__device__ __forceinline__ const double *row_cs( const VecDev &V, int row, int nb ) {
+    return nb > V.cap ? V.ovf_c + V.nid[ ( size_t ) row * V.cap ] : V.nc + ( size_t ) row * V.cap;
+}
+
 __device__ __forceinline__ int find_in_row( const VecDev &V, int row, int key ) {
     const int nb = V.nb[ row ];
-    const int *ids = V.nid + ( size_t ) row * V.cap;
+    const int *ids = row_ids( V, row, nb );
     for ( int l = 0; l < nb; ++l ) if ( ids[ l ] == key ) return l;
     return -1;
 }
@@ -82,10 +90,8 @@ __global__ void __launch_bounds__( VT ) k_lap_count( const VecDev *__restrict__ 
     for ( int row = ch.begin + threadIdx.x; row < ch.end; row += VT ) {
         int cnt = 0;
         const int nb = V.nb[ row ];
-        for ( int k = 0; k < nb; ++k ) {
-            int j = V.nid[ ( size_t ) row * V.cap + k ];
-            cnt += find_in_row( V, j, row ) >= 0;
-        }
+        const int *ids = row_ids( V, row, nb );
+        for ( int k = 0; k < nb; ++k ) cnt += find_in_row( V, ids[ k ], row ) >= 0;
         V.rowcnt[ row ] = cnt;
         tot += cnt;
     }
@@ -149,11 +155,13 @@ __global__ void __launch_bounds__( VT ) k_lap_fill( const VecDev *__restrict__ v
         V.row_ptr[ row ] = at;
         double s = 0;
         const int nb = V.nb[ row ];
+        const int *ids = row_ids( V, row, nb );
+        const double *cs = row_cs( V, row, nb );
         for ( int k = 0; k < nb; ++k ) {
-            int j = V.nid[ ( size_t ) row * V.cap + k ];
+            int j = ids[ k ];
             int l = find_in_row( V, j, row );
             if ( l < 0 ) continue;
-            double c = row < j ? V.nc[ ( size_t ) row * V.cap + k ] : V.nc[ ( size_t ) j * V.cap + l ];
+            double c = row < j ? cs[ k ] : row_cs( V, j, V.nb[ j ] )[ l ];
             V.col[ at ] = j;
             V.val[ at ] = c;
             s += c;

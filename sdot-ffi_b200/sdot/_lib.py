@@ -208,7 +208,19 @@ def diagram_desc(pos, weights, lo, hi, dens, keep, memory=SDOT_HOST):
 
 
 def cells(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None):
-    """one diagram on the GPU; host arrays in and out"""
+    """one diagram on the GPU; host arrays in and out.  A cell with more facets than the table's row is reported
+    with the capacity it needs, and the call runs again with that capacity (PowerDiagram.py:198-215)."""
+    while True:
+        try:
+            return _cells_once(pos, weights, lo, hi, dens, want_facets, want_moments, cap)
+        except KernelFailure as e:
+            grown = max(int(e.needed), 2 * (cap or 32))
+            if not want_facets or e.needed <= (cap or 0) or grown > 8192:
+                raise
+            cap = grown
+
+
+def _cells_once(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None):
     L = load()
     keep = []
     pos = f64(pos)

@@ -133,3 +133,18 @@ def test_the_envelope_gradient_by_finite_differences():
             pm[i, a] -= h
             fd = (_solve(pp, rtol=1e-12).cost - _solve(pm, rtol=1e-12).cost) / (2 * h)
             assert abs(fd - grad[i, a]) < 1e-4 * max(1, abs(fd))
+
+
+def test_a_3d_solve_matches_the_oracle():
+    """tests/test_SdotPlanNd.py:308-325 and 1621-1660: 3D uniform, the card against the CPU"""
+    rng = np.random.default_rng(41)
+    n = 3000
+    pos = rng.uniform(size=(n, 3))
+    plan = _solve(pos, rtol=1e-10)
+    assert plan.converged
+    assert np.abs(plan.cell_masses * n - 1).max() <= 1e-10
+    ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-10)
+    assert ref["stats"]["status"] == 1
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+    assert np.abs(plan.barycenters - ref["bary"]).max() < 1e-9
+    assert abs(plan.cost - ref["cost"]) <= 1e-9 * ref["cost"]
