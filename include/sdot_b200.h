@@ -207,6 +207,15 @@ int32_t sdot_solve(sdot_context ctx, const sdot_solve_desc *desc, sdot_solve_out
    (block-diagonal batching).  Problems of both dimensions may be mixed.  Each `st[k]` reports solve k. */
 int32_t sdot_solve_batch(sdot_context ctx, int32_t count, const sdot_solve_desc *descs, sdot_solve_out *outs, sdot_status *st);
 
+/* The backward of the W2 loss of `batch` solved transports of `n` seeds each (device pointers, problem-major):
+   grad_positions = g_b * 2 m_i (p_i - b_i) and grad_nu = g_b * (w_i - mean_b(w)) -- the envelope theorem at the fitted
+   weights, the gradient in nu projected on sum(d nu) = 0.  `positions` / `grad_positions` / `grad_nu` are FP32 when
+   `positions_fp32`, else FP64; either gradient may be NULL.  Enqueued on the context's stream, not waited for.
+   Replaces the reference's envelope derivatives (SdotPlanNd.py:1037-1040, 1107-1122, `cost_and_position_grad`). */
+int32_t sdot_w2_backward(sdot_context ctx, int32_t batch, int64_t n, int32_t dim, const void *positions, int32_t positions_fp32,
+                         const double *masses, const double *barycentres, const double *weights, const double *grad_cost,
+                         void *grad_positions, void *grad_nu, sdot_status *st);
+
 /* ---- serving: continuous batching of solves ------------------------------------------------------------
  * A server owns a worker thread that advances every admitted solve one Newton step at a time.  Requests
  * submitted while others run are admitted at the next step boundary when the memory budget allows

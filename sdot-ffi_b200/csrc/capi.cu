@@ -463,6 +463,23 @@ int32_t sdot_solve_batch( sdot_context ctx, int32_t count, const sdot_solve_desc
     return worst;
 }
 
+int32_t sdot_w2_backward( sdot_context ctx, int32_t batch, int64_t n, int32_t dim, const void *positions, int32_t positions_fp32,
+                          const double *masses, const double *barycentres, const double *weights, const double *grad_cost, void *grad_positions,
+                          void *grad_nu, sdot_status *st ) {
+    if ( ! ctx || batch <= 0 || n <= 0 || ( dim != 2 && dim != 3 ) || ! positions || ! masses || ! barycentres || ! weights || ! grad_cost ) {
+        set_status( st, SDOT_ERR_ARGS, "bad argument" );
+        return SDOT_ERR_ARGS;
+    }
+    std::lock_guard<std::mutex> lock( ctx->mu );
+    return guard( st, [&] {
+        Ctx &c = ctx->c;
+        CK( cudaSetDevice( c.device ) );
+        launch_w2_backward( c.L(), batch, int( n ), dim, positions, positions_fp32, masses, barycentres, weights, grad_cost, grad_positions,
+                            grad_nu );
+        CK( cudaGetLastError() );
+    } );
+}
+
 int32_t sdot_solve( sdot_context ctx, const sdot_solve_desc *desc, sdot_solve_out *out, sdot_status *st ) {
     return sdot_solve_batch( ctx, 1, desc, out, st );
 }

@@ -381,6 +381,15 @@ struct SolveJob {
     double *ovf_c[ 2 ];
     int ovf_cap = 0;
     int cur = 0;
+    // the multigrid hierarchy (sizes fixed by n; values rebuilt every Newton iteration)
+    int mg_L = 0, mg_pack = 4;
+    int mg_n[ MG_MAX_LEVELS ], mg_cap[ MG_MAX_LEVELS ], mg_nch[ MG_MAX_LEVELS ];
+    int *mg_rp[ MG_MAX_LEVELS ], *mg_col[ MG_MAX_LEVELS ], *mg_rc[ MG_MAX_LEVELS ];
+    float *mg_val[ MG_MAX_LEVELS ], *mg_dia[ MG_MAX_LEVELS ], *mg_dinv[ MG_MAX_LEVELS ], *mg_b[ MG_MAX_LEVELS ], *mg_x[ MG_MAX_LEVELS ],
+        *mg_y[ MG_MAX_LEVELS ];
+    double *mg_part[ MG_MAX_LEVELS ];
+    float *mg_inv = nullptr;
+    char *mg_mem = nullptr;
     int *row_ptr, *col, *rowcnt;
     double *part_cells, *part_vec;
     unsigned long long *wslot;          // [2]
@@ -414,6 +423,8 @@ struct SolveJob {
     long long err_id = -1;
 };
 
+static size_t mg_bytes( int dim, long n, int cap );
+
 size_t job_bytes( int dim, long n, int dkind, long dcount ) {
     const int cap = dim == 2 ? CAP2 : CAP3;
     const long nch = ( n + CHUNK - 1 ) / CHUNK, nv = ( n + VCHUNK - 1 ) / VCHUNK;
@@ -423,7 +434,7 @@ size_t job_bytes( int dim, long n, int dkind, long dcount ) {
     b += size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( n ) * 4 + 1024;
     b += dkind == D_IMAGE ? size_t( dcount ) * 16 : size_t( dcount ) * 8 * ( dim + 2 );
     b += size_t( n ) * ( 24 + dim * 8 ) + 4096;
-    return b;
+    return b + mg_bytes( dim, n, cap );
 }
 
 static void alloc_job( Ctx &c, SolveJob &J ) {
@@ -457,6 +468,95 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     J.ocost = A.take<double>( n );
 }
 
+constexpr int MG_CCH = 256;          // coarse rows per chunk of the coarsening kernels
+
+// the level sizes of the hierarchy of a problem of n seeds; 0 levels when it is too small to need one
+static int mg_levels( int dim, long n, int *sizes ) {
+    const int pack = dim == 2 ? 4 : 8;
+    if ( n <= MG_BOTTOM ) return 0;
+    int L = 0;
+    long m = n;
+    sizes[ L++ ] = int( m );
+    while ( m > MG_BOTTOM && L < MG_MAX_LEVELS ) {
+        m = ( m + pack - 1 ) / pack;
+        sizes[ L++ ] = int( m );
+    }
+    return sizes[ L - 1 ] <= MG_BOTTOM ? L : 0;
+}
+
+static size_t mg_bytes( int dim, long n, int cap ) {
+    int sz[ MG_MAX_LEVELS ];
+    int L = mg_levels( dim, n, sz );
+    if ( ! L ) return 0;
+    size_t b = size_t( n ) * cap * 4 + size_t( n ) * 4 * 4;
+    const int capc = dim == 2 ? 8 : 64;
+    for ( int l = 1; l < L; ++l ) b += size_t( sz[ l ] + 1 ) * 4 * 2 + size_t( sz[ l ] ) * capc * 8 + size_t( sz[ l ] ) * 5 * 4 +
+                                        size_t( sz[ l ] / MG_CCH + 1 ) * 16 + 12 * 256;
+    return b + MG_BOTTOM * MG_BOTTOM * 4 + 16 * 256;
+}
+
+static void alloc_mg( Ctx &c, SolveJob &J ) {
+    const int dim = J.G.dim;
+    J.mg_L = mg_levels( dim, J.G.n, J.mg_n );
+    if ( ! J.mg_L ) return;
+    J.mg_pack = dim == 2 ? 4 : 8;
+    const size_t bytes = mg_bytes( dim, J.G.n, J.cap );
+    J.mg_mem = ( char * ) dalloc( c, bytes );
+    Arena A{ J.mg_mem, bytes, 0 };
+    const int capc = dim == 2 ? 8 : 64;
+    for ( int l = 0; l < J.mg_L; ++l ) {
+        const int n = J.mg_n[ l ];
+        if ( l == 0 ) {
+            J.mg_rp[ 0 ] = J.row_ptr;
+            J.mg_col[ 0 ] = J.col;
+            J.mg_rc[ 0 ] = nullptr;
+            J.mg_cap[ 0 ] = n * J.cap;
+            J.mg_val[ 0 ] = A.take<float>( size_t( n ) * J.cap );
+            J.mg_part[ 0 ] = nullptr;
+            J.mg_nch[ 0 ] = 0;
+            J.mg_y[ 0 ] = nullptr;
+        } else {
+            J.mg_rp[ l ] = A.take<int>( n + 1 );
+            J.mg_rc[ l ] = A.take<int>( n + 1 );
+            J.mg_cap[ l ] = n * capc;
+            J.mg_col[ l ] = A.take<int>( size_t( n ) * capc );
+            J.mg_val[ l ] = A.take<float>( size_t( n ) * capc );
+            J.mg_nch[ l ] = ( n + MG_CCH - 1 ) / MG_CCH;
+            J.mg_part[ l ] = A.take<double>( size_t( J.mg_nch[ l ] ) * 2 );
+            J.mg_y[ l ] = A.take<float>( n );
+        }
+        J.mg_dia[ l ] = A.take<float>( n );
+        J.mg_dinv[ l ] = A.take<float>( n );
+        J.mg_b[ l ] = A.take<float>( n );
+        J.mg_x[ l ] = A.take<float>( n );
+    }
+    J.mg_inv = A.take<float>( MG_BOTTOM * MG_BOTTOM );
+}
+
+// the level-l descriptor of a job for a CG batch in which its VecDev sits at `vec`
+static MgLevel mg_level( const SolveJob &J, int l, int vec ) {
+    MgLevel M;
+    std::memset( &M, 0, sizeof( M ) );
+    M.level = l;
+    M.vec = vec;
+    M.n = J.mg_n[ l ];
+    M.pack = J.mg_pack;
+    M.rp = J.mg_rp[ l ]; M.col = J.mg_col[ l ]; M.val = J.mg_val[ l ]; M.dia = J.mg_dia[ l ]; M.dinv = J.mg_dinv[ l ];
+    M.b = J.mg_b[ l ]; M.x = J.mg_x[ l ]; M.y = J.mg_y[ l ];
+    if ( l + 1 < J.mg_L ) {
+        M.nn = J.mg_n[ l + 1 ];
+        M.bn = J.mg_b[ l + 1 ];
+        M.xn = J.mg_y[ l + 1 ];
+        M.rcn = J.mg_rc[ l + 1 ]; M.rpn = J.mg_rp[ l + 1 ]; M.coln = J.mg_col[ l + 1 ]; M.valn = J.mg_val[ l + 1 ];
+        M.dian = J.mg_dia[ l + 1 ]; M.dinvn = J.mg_dinv[ l + 1 ];
+        M.part = J.mg_part[ l + 1 ];
+        M.nchunk = J.mg_nch[ l + 1 ];
+        M.capn = J.mg_cap[ l + 1 ];
+    }
+    if ( l == J.mg_L - 1 ) M.inv = J.mg_inv;
+    return M;
+}
+
 SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
     const sdot_diagram_desc &D = desc.diagram;
     SolveJob *J = new SolveJob;
@@ -485,6 +585,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         double g0 = w0[ 0 ];
         for ( double &v : w0 ) v -= g0;
         alloc_job( c, *J );
+        if ( int( J->opt[ SDOT_OPT_LIN_METHOD ] ) == 1 ) alloc_mg( c, *J );
         J->slot = take_slot( c );
         CK( cudaMemcpyAsync( &J->rank0, J->G.rank_of, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
@@ -512,6 +613,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
 
 void job_destroy( Ctx &c, SolveJob *J ) {
     if ( ! J ) return;
+    if ( J->mg_mem ) dfree( c, J->mg_mem );
     if ( J->mem ) dfree( c, J->mem );
     if ( J->G.mem ) free_geometry( c, J->G );
     if ( J->slot >= 0 ) give_slot( c, J->slot );
@@ -855,30 +957,95 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.counter = c.dcount + 4 * J.slot + 1;
     V.nchunk = J.nch_vec;
     V.active = 1;
+    V.precond = J.mg_L > 0 ? 1 : 0;
     return V;
 }
 
 struct VecBatch {
     std::vector<VecDev> v;
     std::vector<Chunk> ch;
-    void add( const VecDev &d ) {
+    std::vector<const SolveJob *> jobs;
+    // the multigrid part: per level the descriptors of the jobs that have it and their chunk tables
+    int maxL = 0;
+    std::vector<MgLevel> lv[ MG_MAX_LEVELS ];
+    std::vector<Chunk> down[ MG_MAX_LEVELS ], up[ MG_MAX_LEVELS ], crs[ MG_MAX_LEVELS ];
+    std::vector<MgLevel> bottom;
+    // device copies
+    VecDev *dv = nullptr;
+    Chunk *dch = nullptr;
+    MgLevel *dlv[ MG_MAX_LEVELS ], *dbottom = nullptr;
+    Chunk *ddown[ MG_MAX_LEVELS ], *dup[ MG_MAX_LEVELS ], *dcrs[ MG_MAX_LEVELS ];
+
+    void add( const VecDev &d, const SolveJob *J = nullptr ) {
         int p = int( v.size() );
         VecDev x = d;
         x.chunk0 = int( ch.size() );
         v.push_back( x );
+        jobs.push_back( J );
         int k = 0;
         for ( int b = 0; b < d.n; b += VCHUNK, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + VCHUNK ), k } );
+        if ( ! J || ! J->mg_L || ! d.precond ) return;
+        maxL = std::max( maxL, J->mg_L );
+        for ( int l = 0; l < J->mg_L; ++l ) {
+            int q = int( lv[ l ].size() );
+            lv[ l ].push_back( mg_level( *J, l, p ) );
+            if ( l + 1 < J->mg_L ) {
+                const int nn = J->mg_n[ l + 1 ];
+                int kk = 0;
+                for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
+                kk = 0;
+                for ( int b = 0; b < nn; b += MG_CCH, ++kk ) crs[ l ].push_back( Chunk{ q, b, std::min( nn, b + MG_CCH ), kk } );
+                kk = 0;
+                const int n = J->mg_n[ l ];
+                for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
+            } else
+                bottom.push_back( lv[ l ].back() );
+        }
     }
-    // uploads both arrays in one copy; returns device pointers
-    void upload( Ctx &c, VecDev *&dv, Chunk *&dch ) {
-        size_t b1 = v.size() * sizeof( VecDev ), b2 = ch.size() * sizeof( Chunk );
-        size_t o2 = ( b1 + 255 ) & ~size_t( 255 );
-        std::vector<char> buf( o2 + b2 );
-        std::memcpy( buf.data(), v.data(), b1 );
-        std::memcpy( buf.data() + o2, ch.data(), b2 );
-        char *d = upload_desc( c, buf.data(), buf.size() );
-        dv = reinterpret_cast<VecDev *>( d );
-        dch = reinterpret_cast<Chunk *>( d + o2 );
+    bool mg() const { return maxL > 0; }
+    // everything in one copy
+    void upload( Ctx &c ) {
+        std::vector<std::pair<const void *, size_t>> parts;
+        parts.push_back( { v.data(), v.size() * sizeof( VecDev ) } );
+        parts.push_back( { ch.data(), ch.size() * sizeof( Chunk ) } );
+        for ( int l = 0; l < maxL; ++l ) {
+            parts.push_back( { lv[ l ].data(), lv[ l ].size() * sizeof( MgLevel ) } );
+            parts.push_back( { down[ l ].data(), down[ l ].size() * sizeof( Chunk ) } );
+            parts.push_back( { up[ l ].data(), up[ l ].size() * sizeof( Chunk ) } );
+            parts.push_back( { crs[ l ].data(), crs[ l ].size() * sizeof( Chunk ) } );
+        }
+        parts.push_back( { bottom.data(), bottom.size() * sizeof( MgLevel ) } );
+        std::vector<size_t> off;
+        size_t total = 0;
+        for ( auto &p : parts ) { off.push_back( total ); total += ( p.second + 255 ) & ~size_t( 255 ); }
+        std::vector<char> buf( total + 256 );
+        for ( size_t k = 0; k < parts.size(); ++k ) if ( parts[ k ].second ) std::memcpy( buf.data() + off[ k ], parts[ k ].first, parts[ k ].second );
+        char *d = upload_desc( c, buf.data(), total + 256 );
+        int k = 0;
+        dv = reinterpret_cast<VecDev *>( d + off[ k++ ] );
+        dch = reinterpret_cast<Chunk *>( d + off[ k++ ] );
+        for ( int l = 0; l < maxL; ++l ) {
+            dlv[ l ] = reinterpret_cast<MgLevel *>( d + off[ k++ ] );
+            ddown[ l ] = reinterpret_cast<Chunk *>( d + off[ k++ ] );
+            dup[ l ] = reinterpret_cast<Chunk *>( d + off[ k++ ] );
+            dcrs[ l ] = reinterpret_cast<Chunk *>( d + off[ k++ ] );
+        }
+        dbottom = reinterpret_cast<MgLevel *>( d + off[ k++ ] );
+    }
+    // the hierarchies of every job, from their fresh Laplacians
+    void build( const Launch &L, ErrRec *err ) {
+        if ( ! mg() ) return;
+        std::vector<Chunk> l0;
+        // level 0 rows: the vector chunks, re-indexed to the level-0 array
+        launch_mg_level0( L, dlv[ 0 ], dv, dup[ 0 ], int( up[ 0 ].size() ) );
+        for ( int l = 0; l + 1 < maxL; ++l ) launch_mg_coarsen( L, dlv[ l ], int( lv[ l ].size() ), dcrs[ l ], int( crs[ l ].size() ), err );
+        launch_mg_bottom_build( L, dbottom, int( bottom.size() ) );
+    }
+    // z = M^-1 r for every job
+    void vcycle( const Launch &L ) {
+        for ( int l = 0; l + 1 < maxL; ++l ) launch_mg_down( L, dlv[ l ], dv, ddown[ l ], int( down[ l ].size() ) );
+        launch_mg_bottom( L, dbottom, dv, int( bottom.size() ) );
+        for ( int l = maxL - 2; l >= 0; --l ) launch_mg_up( L, dlv[ l ], dv, dup[ l ], int( up[ l ].size() ) );
     }
 };
 
@@ -901,39 +1068,51 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             launch_wmax( L, J->w2, J->G.n, J->wslot + ( 1 - J->wcur ) );
         }
         VecDev V = vec_of( c, *J );
-        if ( J->pend & P_NEWTON ) newton.add( V );
+        if ( J->pend & P_NEWTON ) newton.add( V, J );
         if ( J->pend & P_GAUGE ) gauge.add( V );
         if ( J->pend & P_TRIAL ) {
             CK( cudaMemsetAsync( J->wslot + ( 1 - J->wcur ), 0, 8, c.stream ) );
             trial.add( V );
         }
     }
-    VecDev *dv;
-    Chunk *dch;
     if ( ! newton.v.empty() ) {
-        newton.upload( c, dv, dch );
-        double rows = 0;
-        for ( auto &v : newton.v ) rows += v.n;
-        c.timer.begin( c.stream, K_LAPLACIAN, rows );
-        launch_lap_count( L, dv, dch, int( newton.ch.size() ) );
-        launch_lap_scan( L, dv, int( newton.v.size() ) );
-        launch_lap_fill( L, dv, dch, int( newton.ch.size() ) );
-        launch_rhs( L, dv, dch, int( newton.ch.size() ) );
-        launch_cg_init( L, dv, dch, int( newton.ch.size() ) );
-        c.timer.end( c.stream, 5 );
+        // Jacobi-preconditioned and multigrid-preconditioned problems go in two batches
+        VecBatch jac, mgb;
+        for ( size_t k = 0; k < newton.v.size(); ++k ) ( newton.v[ k ].precond ? mgb : jac ).add( newton.v[ k ], newton.jobs[ k ] );
+        for ( VecBatch *B : { &jac, &mgb } ) {
+            if ( B->v.empty() ) continue;
+            B->upload( c );
+            const int nch = int( B->ch.size() );
+            double rows = 0;
+            for ( auto &v : B->v ) rows += v.n;
+            c.timer.begin( c.stream, K_LAPLACIAN, rows );
+            launch_lap_count( L, B->dv, B->dch, nch );
+            launch_lap_scan( L, B->dv, int( B->v.size() ) );
+            launch_lap_fill( L, B->dv, B->dch, nch );
+            launch_rhs( L, B->dv, B->dch, nch );
+            if ( B->mg() ) {
+                B->build( L, c.derr );
+                launch_cg_init0( L, B->dv, B->dch, nch );
+                B->vcycle( L );
+                launch_cg_init1( L, B->dv, B->dch, nch );
+            } else
+                launch_cg_init( L, B->dv, B->dch, nch );
+            c.timer.end( c.stream, 5 );
+        }
     }
     if ( ! gauge.v.empty() ) {
-        gauge.upload( c, dv, dch );
-        launch_gauge( L, dv, dch, int( gauge.ch.size() ) );
+        gauge.upload( c );
+        launch_gauge( L, gauge.dv, gauge.dch, int( gauge.ch.size() ) );
     }
     if ( ! trial.v.empty() ) {
-        trial.upload( c, dv, dch );
-        launch_trial( L, dv, dch, int( trial.ch.size() ) );
+        trial.upload( c );
+        launch_trial( L, trial.dv, trial.dch, int( trial.ch.size() ) );
     }
     for ( SolveJob *J : jobs ) J->pend = 0;
 }
 
 constexpr int CG_BURST = 32;
+constexpr int MG_BURST = 8;
 
 void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     Launch L = c.L();
@@ -1030,20 +1209,33 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     run_cells( P3, C3, 3, false );
     run_cells( PR, CR, 2, true );
     // B. CG iterations
-    VecBatch cg;
+    VecBatch cgj, cgm;
     std::vector<SolveJob *> with_cg;
     for ( SolveJob *J : jobs )
-        if ( J->state == J_CG ) { cg.add( vec_of( c, *J ) ); with_cg.push_back( J ); }
-    if ( ! cg.v.empty() ) {
-        VecDev *dv;
-        Chunk *dch;
-        cg.upload( c, dv, dch );
-        int burst = with_diag.empty() ? 4 * CG_BURST : CG_BURST;
+        if ( J->state == J_CG ) {
+            VecDev V = vec_of( c, *J );
+            ( V.precond ? cgm : cgj ).add( V, J );
+            with_cg.push_back( J );
+        }
+    for ( VecBatch *B : { &cgj, &cgm } ) {
+        if ( B->v.empty() ) continue;
+        B->upload( c );
+        const int nch = int( B->ch.size() );
+        int burst = B->mg() ? MG_BURST : CG_BURST;
+        if ( with_diag.empty() ) burst *= 4;
         double rows = 0;
-        for ( auto &v : cg.v ) rows += v.n;
+        for ( auto &v : B->v ) rows += v.n;
+        unsigned long long l0 = c.launches;
         c.timer.begin( c.stream, K_CG, rows * burst );
-        for ( int k = 0; k < burst; ++k ) launch_cg_iter( L, dv, dch, int( cg.ch.size() ) );
-        c.timer.end( c.stream, 3ull * burst );
+        for ( int k = 0; k < burst; ++k ) {
+            if ( B->mg() ) {
+                launch_cg_spmv_update( L, B->dv, B->dch, nch );
+                B->vcycle( L );
+                launch_cg_rz_p( L, B->dv, B->dch, nch );
+            } else
+                launch_cg_iter( L, B->dv, B->dch, nch );
+        }
+        c.timer.end( c.stream, c.launches - l0 );
     }
     // C. one read-back, then the decisions
     int top = 0;

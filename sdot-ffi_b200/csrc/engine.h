@@ -101,6 +101,8 @@ bool job_done( const SolveJob *j );
 void job_outputs( Ctx &c, SolveJob *j, sdot_solve_out &out, int memory );
 void job_destroy( Ctx &c, SolveJob *j );
 size_t job_bytes( int dim, long n, int dkind, long dcount );
+void launch_w2_backward( const Launch &L, int batch, int n, int dim, const void *pos, int fp32, const double *mass, const double *bary,
+                         const double *w, const double *gcost, void *gpos, void *gnu );
 struct Engine;
 // continuous batching: one step of every active job (used by the server)
 void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs );

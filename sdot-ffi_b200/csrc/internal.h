@@ -140,7 +140,27 @@ struct VecDev {
     unsigned *counter;
     int chunk0, nchunk;
     int active;
+    int precond;                  // 0 Jacobi, 1 multigrid (the V-cycle writes z)
 };
+// one level of the multigrid preconditioner of one problem (mg.cu)
+constexpr int MG_BOTTOM = 32;          // the coarsest level has at most this many rows (dense inverse)
+constexpr int MG_MAX_LEVELS = 12;
+struct MgLevel {
+    int level, vec;                    // level index; the problem's index in the CG batch's VecDev array
+    int n, pack, nn;                   // rows of this level, aggregate size, rows of the next level
+    const int *rp, *col;               // this level's CSR (level 0: the Newton CSR's)
+    float *val, *dia, *dinv;
+    float *b, *x, *y;                  // rhs, pre-smoothed x, post-smoothed y (level 0 writes z instead)
+    float *bn;                         // the next level's rhs
+    const float *xn;                   // the next level's solution (its y)
+    int *rcn, *rpn, *coln;             // the next level's CSR, being built
+    float *valn, *dian, *dinvn;
+    double *part;                      // [nchunk * 2] chunk totals and offsets of the build
+    int nchunk;
+    int capn;                          // entries the next level's col / val can hold
+    float *inv;                        // the coarsest level: dense inverse [n * n]
+};
+
 enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, SC_ITER, SC_MEAN, SC_C, SC_TOL, SC_PQ, SC_FAIL, SC_NNZ, NB_SC };
 constexpr int VCHUNK = 1024;     // rows per chunk of the vector kernels
 
@@ -221,6 +241,19 @@ void launch_rhs( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the multigrid-preconditioned CG: init in two halves around the first V-cycle, then per iteration
+// spmv -> update -> V-cycle -> r.z -> p
+void launch_cg_init0( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_cg_init1( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_cg_spmv_update( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+void launch_cg_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// mg.cu
+void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
+void launch_mg_coarsen( const Launch &L, const MgLevel *lv, int nprob, const Chunk *ch, int nch, ErrRec *err );
+void launch_mg_bottom_build( const Launch &L, const MgLevel *lv, int nprob );
+void launch_mg_down( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
+void launch_mg_bottom( const Launch &L, const MgLevel *lv, const VecDev *vs, int nprob );
+void launch_mg_up( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
 void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 
 // cells2d.cu / cells3d.cu

@@ -317,6 +317,110 @@ void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch 
     *L.launches += 3;
 }
 
+// ---- the multigrid-preconditioned CG -----------------------------------------------------------------------------------
+__global__ void __launch_bounds__( VT ) k_cg_init0( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    const double mean = V.sc[ SC_MEAN ];
+    double bb = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        double b = V.b[ i ] - mean;
+        V.b[ i ] = b;
+        V.x[ i ] = 0;
+        V.r[ i ] = b;
+        bb += b * b;
+    }
+    double v[ 1 ] = { bb }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) {
+        V.sc[ SC_BNORM ] = sqrt( tot[ 0 ] );
+        V.sc[ SC_RNORM ] = sqrt( tot[ 0 ] );
+        V.sc[ SC_ITER ] = 0;
+        V.sc[ SC_FAIL ] = 0;
+        V.sc[ SC_CONV ] = tot[ 0 ] == 0 ? 1.0 : 0.0;
+    }
+}
+
+// after the V-cycle wrote z: p = z, rz = r . z
+__global__ void __launch_bounds__( VT ) k_cg_init1( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    double rz = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        double z = V.z[ i ];
+        V.p[ i ] = z;
+        rz += V.r[ i ] * z;
+    }
+    double v[ 1 ] = { rz }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) V.sc[ SC_RZ ] = tot[ 0 ];
+}
+
+// x += alpha p, r -= alpha q, |r| and the convergence test (z comes from the V-cycle)
+__global__ void __launch_bounds__( VT ) k_cg_update_mg( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    const double al = V.sc[ SC_ALPHA ];
+    double rr = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        V.x[ i ] += al * V.p[ i ];
+        double r = V.r[ i ] - al * V.q[ i ];
+        V.r[ i ] = r;
+        rr += r * r;
+    }
+    double v[ 1 ] = { rr }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) {
+        double it = V.sc[ SC_ITER ] + 1;
+        V.sc[ SC_ITER ] = it;
+        double rn = sqrt( tot[ 0 ] );
+        V.sc[ SC_RNORM ] = rn;
+        if ( rn <= V.tol * V.sc[ SC_BNORM ] ) V.sc[ SC_CONV ] = 1;
+        else if ( it >= V.maxit ) { V.sc[ SC_CONV ] = 2; V.sc[ SC_FAIL ] = 1; }
+    }
+}
+
+// rz' = r . z, beta = rz' / rz
+__global__ void __launch_bounds__( VT ) k_cg_rz( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
+    double rz = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) rz += V.r[ i ] * V.z[ i ];
+    double v[ 1 ] = { rz }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) {
+        V.sc[ SC_BETA ] = tot[ 0 ] / V.sc[ SC_RZ ];
+        V.sc[ SC_RZ ] = tot[ 0 ];
+    }
+}
+
+void launch_cg_init0( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_init0<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+void launch_cg_init1( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_init1<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+void launch_cg_spmv_update( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_spmv<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_cg_update_mg<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 2;
+}
+void launch_cg_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_cg_rz<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_cg_p<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 2;
+}
+
 // d = x - x[ rank of user seed 0 ]: the gauge w_0 = 0 kept by the direction
 __global__ void k_gauge( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];

@@ -1,0 +1,297 @@
+// Aggregation multigrid preconditioner of the Laplacian CG, batched over problems.
+//
+// Levels: level 0 is the Newton Laplacian (its FP64 CSR copied to FP32); level l+1 aggregates PACK consecutive
+// Morton ranks of level l (4 in 2D, 8 in 3D) -- consecutive ranks are neighbours in space, the reference's own
+// aggregation by `rank >> shift` (gpu/Linear2D.cuh:15-16, sdotplan/Multigrid.h:10-18) -- with the Galerkin
+// operator P^T A P of the piecewise-constant prolongation, which is again a graph Laplacian: off-diagonals
+// c_IJ = sum of the c_ij between the two aggregates, dia = the row sum.  The coarsest level (<= MG_BOTTOM rows)
+// is solved exactly by the dense inverse of A + mu 1 1^T, which acts as the pseudo-inverse on zero-sum vectors.
+// One V(1,1)-cycle with damped Jacobi on both sides (symmetric, so it is a valid CG preconditioner), all in FP32:
+// the outer CG stays in FP64 and plays the part of the iterative refinement.
+//
+// Each launch covers one level of every problem that has it; pre-smoothing from zero, the residual and the
+// restriction are one kernel (the smoothed x of a neighbour is recomputed from its rhs), prolongation and
+// post-smoothing another.  Coarse rows are built by one warp each from the aggregate's fine rows, summing equal
+// columns in gather order -- deterministic.
+#include "internal.h"
+#include <cub/block/block_scan.cuh>
+
+namespace sdot {
+
+constexpr int MGT = 256;                // threads per block
+constexpr int MG_PAIRS = 1024;          // (column, value) pairs a warp gathers for one coarse row
+constexpr int MG_WARPS = 4;             // warps per block of the coarsening kernels
+
+// ---- build -------------------------------------------------------------------------------------------------------------
+// level 0 from the FP64 CSR of the Newton Laplacian
+__global__ void k_mg_level0( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    const VecDev &V = vs[ M.vec ];
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
+        M.dia[ i ] = float( V.dia[ i ] );
+        M.dinv[ i ] = float( 1.0 / V.dia[ i ] );
+        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) M.val[ e ] = float( V.val[ e ] );
+    }
+}
+
+// the (column, value) pairs of coarse row I, gathered by one warp into shared memory; returns their count (-1: too many)
+__device__ int gather_pairs( const MgLevel &M, int I, int *cj, float *cv, int lane ) {
+    const int i0 = I * M.pack, i1 = min( M.n, i0 + M.pack );
+    int cnt = 0;
+    for ( int i = i0; i < i1; ++i ) {
+        const int b = M.rp[ i ], e = M.rp[ i + 1 ];
+        for ( int base = b; base < e; base += 32 ) {
+            int k = base + lane;
+            if ( k < e && cnt + ( k - base ) < MG_PAIRS ) {
+                cj[ cnt + k - base ] = M.col[ k ] / M.pack;
+                cv[ cnt + k - base ] = M.val[ k ];
+            }
+            cnt += min( 32, e - base );
+        }
+    }
+    __syncwarp();
+    return cnt <= MG_PAIRS ? cnt : -1;
+}
+
+// for each pair: is it the first one of its column (and not the diagonal)?  the sum of its column in pair order
+__device__ __forceinline__ bool first_of_column( const int *cj, int cnt, int k, int I ) {
+    const int J = cj[ k ];
+    if ( J == I ) return false;
+    for ( int q = 0; q < k; ++q ) if ( cj[ q ] == J ) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_count( const MgLevel *__restrict__ lv, const Chunk *__restrict__ chunks, int nch,
+                                                              ErrRec *err ) {
+    __shared__ int sj[ MG_WARPS ][ MG_PAIRS ];
+    __shared__ float sv[ MG_WARPS ][ MG_PAIRS ];
+    __shared__ double tot_w[ MG_WARPS ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    double tot = 0;
+    for ( int I = ch.begin + warp; I < ch.end; I += MG_WARPS ) {
+        int cnt = gather_pairs( M, I, sj[ warp ], sv[ warp ], lane );
+        if ( cnt < 0 ) {
+            if ( lane == 0 && atomicCAS( &err->code, 0, 4 ) == 0 ) { err->kind = 3; err->prob = ch.prob; err->seed = I; err->needed = MG_PAIRS; }
+            cnt = 0;
+        }
+        int distinct = 0;
+        for ( int k = lane; k < cnt; k += 32 ) distinct += first_of_column( sj[ warp ], cnt, k, I );
+        for ( int o = 16; o > 0; o >>= 1 ) distinct += __shfl_xor_sync( 0xffffffffu, distinct, o );
+        if ( lane == 0 ) M.rcn[ I ] = distinct;
+        tot += distinct;
+        __syncwarp();
+    }
+    if ( lane == 0 ) tot_w[ warp ] = tot;
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        double s = 0;
+        for ( int w = 0; w < MG_WARPS; ++w ) s += tot_w[ w ];
+        M.part[ ( size_t ) ch.index * 2 ] = s;
+    }
+}
+
+// one block per problem: exclusive scan of the chunk totals -> part[ 2 c + 1 ]; the coarse row_ptr end
+__global__ void __launch_bounds__( 1024 ) k_mg_scan( const MgLevel *__restrict__ lv ) {
+    const MgLevel &M = lv[ blockIdx.x ];
+    typedef cub::BlockScan<long long, 1024> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ long long carry;
+    if ( threadIdx.x == 0 ) carry = 0;
+    __syncthreads();
+    for ( int base = 0; base < M.nchunk; base += 1024 ) {
+        int c = base + threadIdx.x;
+        long long x = c < M.nchunk ? ( long long ) M.part[ ( size_t ) c * 2 ] : 0, ex, agg;
+        Scan( tmp ).ExclusiveSum( x, ex, agg );
+        if ( c < M.nchunk ) M.part[ ( size_t ) c * 2 + 1 ] = double( carry + ex );
+        __syncthreads();
+        if ( threadIdx.x == 0 ) carry += agg;
+        __syncthreads();
+    }
+    if ( threadIdx.x == 0 ) M.rpn[ M.nn ] = int( carry > M.capn ? M.capn : carry );
+    if ( threadIdx.x == 0 && carry > M.capn ) M.part[ 0 ] = -1;        // refused: the fill writes nothing
+}
+
+__global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__restrict__ lv, const Chunk *__restrict__ chunks, int nch ) {
+    __shared__ int sj[ MG_WARPS ][ MG_PAIRS ];
+    __shared__ float sv[ MG_WARPS ][ MG_PAIRS ];
+    __shared__ int run[ MG_WARPS ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    if ( M.part[ 0 ] < 0 ) return;                                     // the next level did not fit (see k_mg_scan)
+    // the chunk's rows in order: each warp needs the offset of its row, i.e. the counts of the rows before it
+    int at = int( M.part[ ( size_t ) ch.index * 2 + 1 ] );
+    for ( int I0 = ch.begin; I0 < ch.end; I0 += MG_WARPS ) {
+        const int I = I0 + warp;
+        if ( lane == 0 ) run[ warp ] = I < ch.end ? M.rcn[ I ] : 0;
+        __syncthreads();
+        int my = at;
+        for ( int w = 0; w < warp; ++w ) my += run[ w ];
+        int step = 0;
+        for ( int w = 0; w < MG_WARPS; ++w ) step += run[ w ];
+        __syncthreads();
+        if ( I < ch.end ) {
+            int cnt = gather_pairs( M, I, sj[ warp ], sv[ warp ], lane );
+            if ( cnt < 0 ) cnt = 0;
+            // the distinct columns in pair order, each with its sum in pair order
+            int done = 0;
+            float dsum = 0;
+            for ( int base = 0; base < cnt; base += 32 ) {
+                int k = base + lane;
+                bool first = k < cnt && first_of_column( sj[ warp ], cnt, k, I );
+                float s = 0;
+                if ( first ) {
+                    const int J = sj[ warp ][ k ];
+                    for ( int q = k; q < cnt; ++q ) if ( sj[ warp ][ q ] == J ) s += sv[ warp ][ q ];
+                }
+                unsigned m = __ballot_sync( 0xffffffffu, first );
+                int slot = done + __popc( m & ( ( 1u << lane ) - 1 ) );
+                if ( first ) { M.coln[ my + slot ] = sj[ warp ][ k ]; M.valn[ my + slot ] = s; }
+                float ws = first ? s : 0.f;
+                for ( int o = 16; o > 0; o >>= 1 ) ws += __shfl_xor_sync( 0xffffffffu, ws, o );
+                dsum += ws;
+                done += __popc( m );
+            }
+            if ( lane == 0 ) {
+                M.rpn[ I ] = my;
+                M.dian[ I ] = dsum > 0 ? dsum : 1.f;
+                M.dinvn[ I ] = 1.f / ( dsum > 0 ? dsum : 1.f );
+            }
+        }
+        at += step;
+        __syncwarp();
+    }
+}
+
+// the coarsest level: the dense inverse of A + mu 1 1^T (Gauss-Jordan in FP64), one warp per problem
+__global__ void __launch_bounds__( 32 ) k_mg_bottom_build( const MgLevel *__restrict__ lv ) {
+    const MgLevel &M = lv[ blockIdx.x ];
+    const int n = M.n, lane = threadIdx.x;
+    __shared__ double A[ MG_BOTTOM ][ 2 * MG_BOTTOM ];
+    double mu = 0;
+    for ( int i = 0; i < n; ++i ) mu += M.dia[ i ];
+    mu = mu / ( n * n );
+    for ( int i = 0; i < n; ++i )
+        for ( int j = lane; j < 2 * n; j += 32 ) A[ i ][ j ] = j < n ? ( i == j ? double( M.dia[ i ] ) : 0.0 ) + mu : ( j - n == i ? 1.0 : 0.0 );
+    __syncwarp();
+    for ( int i = 0; i < n; ++i )
+        for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e )
+            if ( lane == 0 ) A[ i ][ M.col[ e ] ] -= M.val[ e ];
+    __syncwarp();
+    for ( int k = 0; k < n; ++k ) {
+        double piv = A[ k ][ k ];
+        __syncwarp();
+        for ( int j = lane; j < 2 * n; j += 32 ) A[ k ][ j ] /= piv;
+        __syncwarp();
+        for ( int i = 0; i < n; ++i ) {
+            if ( i == k ) continue;
+            double f = A[ i ][ k ];
+            __syncwarp();
+            for ( int j = lane; j < 2 * n; j += 32 ) A[ i ][ j ] -= f * A[ k ][ j ];
+            __syncwarp();
+        }
+    }
+    for ( int i = 0; i < n; ++i )
+        for ( int j = lane; j < n; j += 32 ) M.inv[ i * n + j ] = float( A[ i ][ n + j ] );
+}
+
+// ---- apply: one V(1,1) cycle --------------------------------------------------------------------------------------------
+constexpr float OMEGA = 0.8f;
+
+// pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level; one thread per coarse row
+__global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
+                                                   int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    const bool top = M.level == 0;
+    const VecDev *V = vs + M.vec;
+    if ( V->sc[ SC_CONV ] != 0 ) return;
+    for ( int I = ch.begin + threadIdx.x; I < ch.end; I += blockDim.x ) {
+        const int i0 = I * M.pack, i1 = min( M.n, i0 + M.pack );
+        float acc = 0;
+        for ( int i = i0; i < i1; ++i ) {
+            float bi = top ? float( V->r[ i ] ) : M.b[ i ];
+            if ( top ) M.b[ i ] = bi;
+            float xi = OMEGA * M.dinv[ i ] * bi;
+            M.x[ i ] = xi;
+            float ax = M.dia[ i ] * xi;
+            for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e ) {
+                const int j = M.col[ e ];
+                float bj = top ? float( V->r[ j ] ) : M.b[ j ];
+                ax -= M.val[ e ] * OMEGA * M.dinv[ j ] * bj;
+            }
+            acc += bi - ax;
+        }
+        M.bn[ I ] = acc;
+    }
+}
+
+// the coarsest level: x = inv b (one warp per problem)
+__global__ void __launch_bounds__( 32 ) k_mg_bottom( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs ) {
+    const MgLevel &M = lv[ blockIdx.x ];
+    if ( vs[ M.vec ].sc[ SC_CONV ] != 0 ) return;
+    const int n = M.n;
+    for ( int i = threadIdx.x; i < n; i += 32 ) {
+        float s = 0;
+        for ( int j = 0; j < n; ++j ) s += M.inv[ i * n + j ] * M.b[ j ];
+        M.y[ i ] = s;
+    }
+}
+
+// prolongation of the next level's solution and post-smoothing; level 0 writes z (FP64)
+__global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
+                                                 int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    const VecDev &V = vs[ M.vec ];
+    if ( V.sc[ SC_CONV ] != 0 ) return;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
+        float xi = M.x[ i ] + M.xn[ i / M.pack ];
+        float s = M.dia[ i ] * xi;
+        for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e ) {
+            const int j = M.col[ e ];
+            s -= M.val[ e ] * ( M.x[ j ] + M.xn[ j / M.pack ] );
+        }
+        float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
+        if ( M.level == 0 ) V.z[ i ] = double( yi );
+        else M.y[ i ] = yi;
+    }
+}
+
+void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mg_level0<<<nch, MGT, 0, L.stream>>>( lv, vs, ch, nch );
+    ++*L.launches;
+}
+void launch_mg_coarsen( const Launch &L, const MgLevel *lv, int nprob, const Chunk *ch, int nch, ErrRec *err ) {
+    if ( nch <= 0 ) return;
+    k_mg_count<<<nch, 32 * MG_WARPS, 0, L.stream>>>( lv, ch, nch, err );
+    k_mg_scan<<<nprob, 1024, 0, L.stream>>>( lv );
+    k_mg_fill<<<nch, 32 * MG_WARPS, 0, L.stream>>>( lv, ch, nch );
+    *L.launches += 3;
+}
+void launch_mg_bottom_build( const Launch &L, const MgLevel *lv, int nprob ) {
+    if ( nprob <= 0 ) return;
+    k_mg_bottom_build<<<nprob, 32, 0, L.stream>>>( lv );
+    ++*L.launches;
+}
+void launch_mg_down( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mg_down<<<nch, MGT, 0, L.stream>>>( lv, vs, ch, nch );
+    ++*L.launches;
+}
+void launch_mg_bottom( const Launch &L, const MgLevel *lv, const VecDev *vs, int nprob ) {
+    if ( nprob <= 0 ) return;
+    k_mg_bottom<<<nprob, 32, 0, L.stream>>>( lv, vs );
+    ++*L.launches;
+}
+void launch_mg_up( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mg_up<<<nch, MGT, 0, L.stream>>>( lv, vs, ch, nch );
+    ++*L.launches;
+}
+
+} // namespace sdot

@@ -46,8 +46,8 @@ def solver_options(settings, n):
         raise NotImplementedError(f"step = {tun.step!r}: this build takes the TRIALS step ( 'auto' or 'trials' )")
     if tun.residual not in _RESIDUAL:
         raise ValueError(f"unknown residual: {tun.residual!r} ( {', '.join(_RESIDUAL)} )")
-    if tun.linear_solver not in ("auto", "cg"):
-        raise NotImplementedError(f"linear_solver = {tun.linear_solver!r}: 'auto' / 'cg' (Jacobi-PCG on the device) in this build")
+    if tun.linear_solver not in ("auto", "cg", "mg", "amg"):
+        raise NotImplementedError(f"linear_solver = {tun.linear_solver!r}: 'auto' / 'mg' (multigrid-PCG) or 'cg' (Jacobi-PCG) in this build")
     if settings.kernel_dtype != "FP64":
         raise NotImplementedError(f"precision = {settings.precision!r}: FP64 cells only in this build")
     return dict(tol_abs=settings.tol, tol_rel=float(tun.mass_rtol), maxit=settings.max_iter, max_backtracks=tun.max_backtracks,
@@ -55,7 +55,7 @@ def solver_options(settings, n):
                 switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-8), lin_maxit=int(tun.linear_maxit or 20000),
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
-                lin_method=0, precision=0, lin_precision=0)
+                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0)
 
 
 def _box_of(problem):

@@ -92,6 +92,8 @@ SIGNATURES = {
     "sdot_solve": (ctypes.c_int32, [_P, ctypes.POINTER(SolveDesc), ctypes.POINTER(SolveOut), ctypes.POINTER(Status)]),
     "sdot_solve_batch": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.POINTER(SolveDesc), ctypes.POINTER(SolveOut), ctypes.POINTER(Status)]),
     "sdot_solve_bytes": (ctypes.c_uint64, [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Density)]),
+    "sdot_w2_backward": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, _P, ctypes.c_int32, _P, _P, _P, _P, _P, _P,
+                                          ctypes.POINTER(Status)]),
     "sdot_server_create": (ctypes.c_int32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P), ctypes.POINTER(Status)]),
     "sdot_server_submit": (ctypes.c_int32, [_P, ctypes.POINTER(SolveDesc), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(Status)]),
     "sdot_server_poll": (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.POINTER(SolveOut), ctypes.c_int32, ctypes.POINTER(Status)]),

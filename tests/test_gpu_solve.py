@@ -43,6 +43,18 @@ def test_plain_2d_fp64_n10000_matches_the_oracle():
     assert len(plan.history) >= plan.stats["nb_iter"] + 1
 
 
+@pytest.mark.parametrize("lin", ["cg", "mg"])
+def test_both_linear_solvers_reach_the_same_plan(lin):
+    """tests/test_SdotPlanNd.py:536-561: the multigrid reaches the plan of the reference solver"""
+    rng = np.random.default_rng(50)
+    n = 20000
+    pos = rng.uniform(size=(n, 2))
+    plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-10, linear_solver=lin)))
+    assert plan.converged
+    ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-10)
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+
+
 def test_a_solve_in_a_batch_is_the_solve_alone():
     rng = np.random.default_rng(3)
     pbs = [OtProblem(SumOfDiracs(rng.uniform(size=(n, 2))), sdot.Box()) for n in (1500, 4000, 700, 2500)]
