@@ -70,11 +70,6 @@ void run_big_cells( Ctx &c, ProbDev *dprob, unsigned flags ) {
 
 } // namespace
 
-struct sdot_context_s {
-    Ctx c;
-    std::mutex mu;
-};
-
 extern "C" {
 
 int32_t sdot_abi_version( void ) { return SDOT_ABI_VERSION; }
@@ -340,6 +335,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         const long long total = ( long long ) hs[ SC_NNZ ];
         if ( nnz ) *nnz = total;
         if ( total > cap_nnz ) throw Error( SDOT_ERR_CAPACITY, "sdot_laplacian: cap_nnz too small", -1, total );
+        if ( total > ( long long ) n * cap ) throw Error( SDOT_ERR_CAPACITY, "sdot_laplacian: more entries than the CSR work area holds", -1, total );
         launch_lap_fill( L, ( VecDev * ) ( base + o2 ), ( Chunk * ) ( base + o3 ), int( vch.size() ) );
         std::vector<int> hrp( n + 1 );
         CK( cudaMemcpyAsync( hrp.data(), rp, ( n + 1 ) * 4, cudaMemcpyDeviceToHost, c.stream ) );

@@ -221,9 +221,22 @@ __device__ __forceinline__ bool wclip( WPoly &C, int lane, double nx, double ny,
     unsigned rot_out = ( ( out >> 1 ) | ( out << ( m - 1 ) ) ) & valid;
     unsigned rot_in = ( ( in >> 1 ) | ( in << ( m - 1 ) ) ) & valid;
     unsigned A = in & rot_out, B = out & rot_in;
-    int a = __ffs( A ) - 1;
-    unsigned Bafter = a >= 31 ? 0u : ( B & ~( ( 2u << a ) - 1 ) );
-    int b = Bafter ? __ffs( Bafter ) - 1 : __ffs( B ) - 1;
+    int a, b;
+    if ( __popc( A ) == 1 ) {
+        a = __ffs( A ) - 1;
+        b = __ffs( B ) - 1;
+    } else {
+        // several outside runs: rounding near a vertex where many lines meet.  The run holding the most outside
+        // vertex is the real one; the others (noise-level) are kept
+        double sv = lane < m ? s : -1e300;
+        double smax = warp_max( sv );
+        int kstar = __ffs( __ballot_sync( FULL, lane < m && sv == smax ) ) - 1;
+        int da = ( A >> lane ) & 1 ? ( ( kstar - lane ) % m + m ) % m : 1 << 20;       // a: the in->out edge before kstar
+        int db = ( B >> lane ) & 1 ? ( ( lane - kstar ) % m + m ) % m : 1 << 20;       // b: the out->in edge from kstar on
+        for ( int o = 16; o > 0; o >>= 1 ) { da = min( da, __shfl_xor_sync( FULL, da, o ) ); db = min( db, __shfl_xor_sync( FULL, db, o ) ); }
+        a = ( ( kstar - da ) % m + m ) % m;
+        b = ( kstar + db ) % m;
+    }
     int K = ( ( a - b - 1 ) % m + m ) % m + 1;
     if ( K + 2 > 32 ) return false;
     // the new vertices: line[a] ^ L and L ^ line[b]; near-parallel lines fall back on the edge interpolation
@@ -628,19 +641,26 @@ __device__ int big_clip( BigPoly &S, BigPoly &D, int m, int lane, double nx, dou
     __syncwarp();
     if ( nout == 0 ) return m;
     if ( nout == m ) return 0;
-    int a = 1 << 30;
+    // the outside run that holds the most outside vertex (other runs are rounding noise, kept)
+    double smax = -1e300;
+    int kstar = 0;
+    for ( int k = lane; k < m; k += 32 ) {
+        double sk = nx * S.x[ k ] + ny * S.y[ k ] - off;
+        if ( sk > smax ) { smax = sk; kstar = k; }
+    }
+    double wmaxs = warp_max( smax );
+    int kcand = smax == wmaxs ? kstar : 1 << 30;
+    kstar = warp_min_int( kcand );
+    int da = 1 << 30, db = 1 << 30;
     for ( int k = lane; k < m; k += 32 ) {
         int k1 = k + 1 == m ? 0 : k + 1;
-        if ( ! S.out[ k ] && S.out[ k1 ] ) a = min( a, k );
+        if ( ! S.out[ k ] && S.out[ k1 ] ) da = min( da, ( ( kstar - k ) % m + m ) % m );
+        if ( S.out[ k ] && ! S.out[ k1 ] ) db = min( db, ( ( k - kstar ) % m + m ) % m );
     }
-    a = warp_min_int( a );
-    int db = 1 << 30;
-    for ( int k = lane; k < m; k += 32 ) {
-        int k1 = k + 1 == m ? 0 : k + 1;
-        if ( S.out[ k ] && ! S.out[ k1 ] ) db = min( db, ( ( k - a - 1 ) % m + m ) % m );
-    }
+    da = warp_min_int( da );
     db = warp_min_int( db );
-    const int b = ( a + 1 + db ) % m;
+    const int a = ( ( kstar - da ) % m + m ) % m;
+    const int b = ( kstar + db ) % m;
     const int K = ( ( a - b - 1 ) % m + m ) % m + 1;
     if ( K + 2 > VBIG ) return -1;
     for ( int t = lane; t < K; t += 32 ) {

@@ -3,6 +3,7 @@
 #include "internal.h"
 #include "../../include/sdot_b200.h"
 #include <exception>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -108,3 +109,9 @@ struct Engine;
 void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs );
 
 } // namespace sdot
+
+// the object behind `sdot_context`: the device state and the mutex that serialises the calls made through it
+struct sdot_context_s {
+    sdot::Ctx c;
+    std::mutex mu;
+};

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__( 1024 ) k_lap_scan( const VecDev *__restrict__
     }
     if ( threadIdx.x == 0 ) {
         V.sc[ SC_NNZ ] = double( carry );
-        V.row_ptr[ V.n ] = int( carry );
+        V.row_ptr[ V.n ] = carry > ( long long ) V.n * V.cap ? 0 : int( carry );   // past the capacity: empty rows, CG fails
     }
 }
 
@@ -147,6 +147,10 @@ __global__ void __launch_bounds__( VT ) k_lap_fill( const VecDev *__restrict__ v
     for ( int q = 0; q < VPT; ++q ) { int row = r0 + q; cnt[ q ] = row < ch.end ? V.rowcnt[ row ] : 0; loc += cnt[ q ]; }
     int ex;
     Scan( tmp ).ExclusiveSum( loc, ex );
+    if ( V.sc[ SC_NNZ ] > double( V.n ) * V.cap ) {                // past the CSR's capacity: empty rows (k_lap_scan)
+        for ( int q = 0; q < VPT && r0 + q < ch.end; ++q ) { V.row_ptr[ r0 + q ] = 0; V.dia[ r0 + q ] = 1.0; }
+        return;
+    }
     int at = int( V.partials[ ( size_t ) ch.index * 4 + 1 ] ) + ex;
 #pragma unroll
     for ( int q = 0; q < VPT; ++q ) {
@@ -243,6 +247,7 @@ __global__ void __launch_bounds__( VT ) k_cg_init( const VecDev *__restrict__ vs
         V.sc[ SC_ITER ] = 0;
         V.sc[ SC_FAIL ] = 0;
         V.sc[ SC_CONV ] = tot[ 1 ] == 0 ? 1.0 : 0.0;
+        if ( V.sc[ SC_NNZ ] > double( V.n ) * V.cap ) { V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
     }
 }
 
@@ -339,6 +344,7 @@ __global__ void __launch_bounds__( VT ) k_cg_init0( const VecDev *__restrict__ v
         V.sc[ SC_ITER ] = 0;
         V.sc[ SC_FAIL ] = 0;
         V.sc[ SC_CONV ] = tot[ 0 ] == 0 ? 1.0 : 0.0;
+        if ( V.sc[ SC_NNZ ] > double( V.n ) * V.cap ) { V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
     }
 }
 

@@ -73,13 +73,10 @@ __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_count( const MgLevel *__
     double tot = 0;
     for ( int I = ch.begin + warp; I < ch.end; I += MG_WARPS ) {
         int cnt = gather_pairs( M, I, sj[ warp ], sv[ warp ], lane );
-        if ( cnt < 0 ) {
-            if ( lane == 0 && atomicCAS( &err->code, 0, 4 ) == 0 ) { err->kind = 3; err->prob = ch.prob; err->seed = I; err->needed = MG_PAIRS; }
-            cnt = 0;
-        }
         int distinct = 0;
         for ( int k = lane; k < cnt; k += 32 ) distinct += first_of_column( sj[ warp ], cnt, k, I );
         for ( int o = 16; o > 0; o >>= 1 ) distinct += __shfl_xor_sync( 0xffffffffu, distinct, o );
+        if ( cnt < 0 ) distinct = M.capn + 1;                           // too many pairs: the level is refused (k_mg_scan)
         if ( lane == 0 ) M.rcn[ I ] = distinct;
         tot += distinct;
         __syncwarp();
@@ -96,6 +93,7 @@ __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_count( const MgLevel *__
 // one block per problem: exclusive scan of the chunk totals -> part[ 2 c + 1 ]; the coarse row_ptr end
 __global__ void __launch_bounds__( 1024 ) k_mg_scan( const MgLevel *__restrict__ lv ) {
     const MgLevel &M = lv[ blockIdx.x ];
+    if ( ! M.rpn ) return;                                              // this job's coarsest level: nothing to build
     typedef cub::BlockScan<long long, 1024> Scan;
     __shared__ typename Scan::TempStorage tmp;
     __shared__ long long carry;
@@ -110,8 +108,8 @@ __global__ void __launch_bounds__( 1024 ) k_mg_scan( const MgLevel *__restrict__
         if ( threadIdx.x == 0 ) carry += agg;
         __syncthreads();
     }
-    if ( threadIdx.x == 0 ) M.rpn[ M.nn ] = int( carry > M.capn ? M.capn : carry );
-    if ( threadIdx.x == 0 && carry > M.capn ) M.part[ 0 ] = -1;        // refused: the fill writes nothing
+    if ( threadIdx.x == 0 ) M.rpn[ M.nn ] = int( carry > M.capn ? 0 : carry );
+    if ( threadIdx.x == 0 && carry > M.capn ) M.part[ 0 ] = -1;        // refused: the next level is diagonal
 }
 
 __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__restrict__ lv, const Chunk *__restrict__ chunks, int nch ) {
@@ -121,12 +119,13 @@ __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__r
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
-    if ( M.part[ 0 ] < 0 ) return;                                     // the next level did not fit (see k_mg_scan)
+    // a refused level (see k_mg_scan) keeps only its diagonal: empty rows, nothing written past the capacity
+    const bool refused = M.part[ 0 ] < 0;
     // the chunk's rows in order: each warp needs the offset of its row, i.e. the counts of the rows before it
-    int at = int( M.part[ ( size_t ) ch.index * 2 + 1 ] );
+    int at = refused ? 0 : int( M.part[ ( size_t ) ch.index * 2 + 1 ] );
     for ( int I0 = ch.begin; I0 < ch.end; I0 += MG_WARPS ) {
         const int I = I0 + warp;
-        if ( lane == 0 ) run[ warp ] = I < ch.end ? M.rcn[ I ] : 0;
+        if ( lane == 0 ) run[ warp ] = I < ch.end && ! refused ? M.rcn[ I ] : 0;
         __syncthreads();
         int my = at;
         for ( int w = 0; w < warp; ++w ) my += run[ w ];
@@ -149,14 +148,14 @@ __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__r
                 }
                 unsigned m = __ballot_sync( 0xffffffffu, first );
                 int slot = done + __popc( m & ( ( 1u << lane ) - 1 ) );
-                if ( first ) { M.coln[ my + slot ] = sj[ warp ][ k ]; M.valn[ my + slot ] = s; }
+                if ( first && ! refused ) { M.coln[ my + slot ] = sj[ warp ][ k ]; M.valn[ my + slot ] = s; }
                 float ws = first ? s : 0.f;
                 for ( int o = 16; o > 0; o >>= 1 ) ws += __shfl_xor_sync( 0xffffffffu, ws, o );
                 dsum += ws;
                 done += __popc( m );
             }
             if ( lane == 0 ) {
-                M.rpn[ I ] = my;
+                M.rpn[ I ] = refused ? 0 : my;
                 M.dian[ I ] = dsum > 0 ? dsum : 1.f;
                 M.dinvn[ I ] = 1.f / ( dsum > 0 ? dsum : 1.f );
             }
@@ -181,7 +180,13 @@ __global__ void __launch_bounds__( 32 ) k_mg_bottom_build( const MgLevel *__rest
         for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e )
             if ( lane == 0 ) A[ i ][ M.col[ e ] ] -= M.val[ e ];
     __syncwarp();
+    double dmax = 0;
+    for ( int i = 0; i < n; ++i ) dmax = fmax( dmax, double( M.dia[ i ] ) );
+    dmax = dmax > 0 ? dmax : 1.0;
     for ( int k = 0; k < n; ++k ) {
+        __syncwarp();
+        if ( lane == 0 && ! ( A[ k ][ k ] > 1e-12 * dmax ) ) A[ k ][ k ] += dmax;
+        __syncwarp();
         double piv = A[ k ][ k ];
         __syncwarp();
         for ( int j = lane; j < 2 * n; j += 32 ) A[ k ][ j ] /= piv;
