@@ -152,6 +152,19 @@ int32_t sdot_linear_solve(sdot_context ctx, int64_t n, const int64_t *row_ptr, c
                           const double *dia, int32_t nrhs, const double *rhs, double *x, int32_t method, double tol,
                           int32_t maxit, int32_t memory, int32_t *iterations, sdot_status *st);
 
+/* ---- the linear solve without allocations (no counterpart in the reference) -------------------------------
+ * `sdot_linear_solve` with method 0 (Jacobi-PCG), its work vectors held in a static device array of the
+ * library instead of memory allocated per call: no cudaMalloc / cudaFree / pool allocation in the call, for a
+ * caller that cannot allocate while it solves (its framework holds the GPU's free memory, or it cannot pay the
+ * device-wide synchronisation of cudaFree).  Every array is device memory.  At most SDOT_NOALLOC_MAX_ROWS rows
+ * (past it: SDOT_ERR_CAPACITY, `needed` = n).  The array is shared by every call on a device: calls that
+ * overlap in time race (one context serialises its own calls).  The first call on a device looks the array's
+ * address up; make it before any stream capture on that device. */
+#define SDOT_NOALLOC_MAX_ROWS 262144
+int32_t sdot_linear_solve_noalloc(sdot_context ctx, int64_t n, const int64_t *row_ptr, const int32_t *cols, const double *vals,
+                                  const double *dia, int32_t nrhs, const double *rhs, double *x, double tol, int32_t maxit,
+                                  int32_t *iterations, sdot_status *st);
+
 /* ---- the Newton solve -----------------------------------------------------------------------------------
  * Options, in this order (`sdot_solve_desc.options`, `SDOT_NB_OPTIONS` values; SdotPlanNd._CARD_OPTIONS holds
  * the reference's card list, gpu/Newton2D.cuh:98-110): */

@@ -89,6 +89,8 @@ SIGNATURES = {
                                         ctypes.POINTER(Status)]),
     "sdot_linear_solve": (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P, _P, _P, ctypes.c_int32, _P, _P, ctypes.c_int32, ctypes.c_double,
                                            ctypes.c_int32, ctypes.c_int32, _P, ctypes.POINTER(Status)]),
+    "sdot_linear_solve_noalloc": (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P, _P, _P, ctypes.c_int32, _P, _P, ctypes.c_double,
+                                                   ctypes.c_int32, _P, ctypes.POINTER(Status)]),
     "sdot_solve": (ctypes.c_int32, [_P, ctypes.POINTER(SolveDesc), ctypes.POINTER(SolveOut), ctypes.POINTER(Status)]),
     "sdot_solve_batch": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.POINTER(SolveDesc), ctypes.POINTER(SolveOut), ctypes.POINTER(Status)]),
     "sdot_solve_bytes": (ctypes.c_uint64, [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Density)]),
