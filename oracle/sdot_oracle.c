@@ -29,7 +29,10 @@
  *     width continuation stages, final moments on the true density (sdotplan/Solve.h:66-97, 111-371;
  *     sdotplan/Continuation.h:33-40; sdotplan/convolved/SumOfGaussians.h:38-41);
  *   - cut identifiers: box sides are negative (-1 .. -2d), seeds are their user index
- *     (src/sdot/include/sdot/gpu/Cell2D.cuh:453-463).
+ *     (src/sdot/include/sdot/gpu/Cell2D.cuh:453-463);
+ *   - 3D sums of gaussians: the reference integrates them on the CPU only, facets exactly and masses by
+ *     adaptive quadrature (src/sdot/.../SumOfGaussians.cxx:120-210, PointwiseDensity.h); here both by
+ *     adaptive Gauss product rules over tetrahedra / triangles (gauss_cell3, gauss_face3).
  * The neighbour search is a uniform grid visited ring by ring and stopped by a security radius (or,
  * `brute != 0`, every other seed) -- it changes what a cell costs, never what it is.
  */
@@ -55,6 +58,8 @@ enum { DENS_UNIFORM = 0, DENS_IMAGE = 1, DENS_GAUSS = 2 };
 #define GL_N 12
 static double gl_x[ GL_N ], gl_w[ GL_N ];
 static int gl_ready = 0;
+#define TQ_N 6
+static double tq_x[ TQ_N ], tq_w[ TQ_N ];      /* the same construction with 6 points: the tetrahedral rules */
 static void gl_init( void ) {
     if ( gl_ready ) return;
     for ( int i = 0; i < GL_N; ++i ) {
@@ -69,6 +74,19 @@ static void gl_init( void ) {
         }
         gl_x[ i ] = x;
         gl_w[ i ] = 2 / ( ( 1 - x * x ) * dp * dp );
+    }
+    for ( int i = 0; i < TQ_N; ++i ) {
+        double x = cos( M_PI * ( i + 0.75 ) / ( TQ_N + 0.5 ) ), dp = 0;
+        for ( int it = 0; it < 100; ++it ) {
+            double p0 = 1, p1 = x;
+            for ( int k = 2; k <= TQ_N; ++k ) { double p2 = ( ( 2 * k - 1 ) * x * p1 - ( k - 1 ) * p0 ) / k; p0 = p1; p1 = p2; }
+            dp = TQ_N * ( x * p1 - p0 ) / ( x * x - 1 );
+            double dx = p1 / dp;
+            x -= dx;
+            if ( fabs( dx ) < 1e-16 ) break;
+        }
+        tq_x[ i ] = x;
+        tq_w[ i ] = 2 / ( ( 1 - x * x ) * dp * dp );
     }
     gl_ready = 1;
 }
@@ -656,6 +674,136 @@ static void poly3_integrals( const poly3 *P, double *V, double F[ 3 ], double *S
     *V = vol; F[ 0 ] = f[ 0 ]; F[ 1 ] = f[ 1 ]; F[ 2 ] = f[ 2 ]; *S = s;
 }
 
+/* ---- sums of isotropic gaussians (3D) ------------------------------------------------------------
+ * Volume quadrature, independent of any closed form: the polyhedron is cut into tetrahedra (a fan of each
+ * face from the vertex mean), each integrated by the collapsed (Duffy) product of TQ_N-point Gauss-Legendre
+ * rules and refined by 8-way subdivision until the children agree with their parent.  Faces likewise by
+ * collapsed 2D rules and 4-way subdivision.  rho_g = m / ((2 pi)^{3/2} s^3) exp(-|x - c|^2 / 2 s^2). */
+typedef struct { double c[ 3 ], s, m, k; } g3;
+static void g3_tet_rule( const g3 *g, const double T[ 4 ][ 3 ], double out[ 5 ] ) {
+    double e1[ 3 ], e2[ 3 ], e3[ 3 ];
+    for ( int q = 0; q < 3; ++q ) { e1[ q ] = T[ 1 ][ q ] - T[ 0 ][ q ]; e2[ q ] = T[ 2 ][ q ] - T[ 0 ][ q ]; e3[ q ] = T[ 3 ][ q ] - T[ 0 ][ q ]; }
+    double vol6 = fabs( e1[ 0 ] * ( e2[ 1 ] * e3[ 2 ] - e2[ 2 ] * e3[ 1 ] ) - e1[ 1 ] * ( e2[ 0 ] * e3[ 2 ] - e2[ 2 ] * e3[ 0 ] ) +
+                        e1[ 2 ] * ( e2[ 0 ] * e3[ 1 ] - e2[ 1 ] * e3[ 0 ] ) );
+    for ( int q = 0; q < 5; ++q ) out[ q ] = 0;
+    for ( int i = 0; i < TQ_N; ++i ) {
+        double a = 0.5 * ( tq_x[ i ] + 1 ), wa = 0.5 * tq_w[ i ];
+        for ( int j = 0; j < TQ_N; ++j ) {
+            double b = 0.5 * ( tq_x[ j ] + 1 ), wb = 0.5 * tq_w[ j ];
+            for ( int l = 0; l < TQ_N; ++l ) {
+                double t = 0.5 * ( tq_x[ l ] + 1 ), wt_ = 0.5 * tq_w[ l ];
+                double u = a, v = b * ( 1 - a ), z = t * ( 1 - a ) * ( 1 - b );
+                double J = ( 1 - a ) * ( 1 - a ) * ( 1 - b ) * wa * wb * wt_ * vol6;
+                double x[ 3 ], r2 = 0;
+                for ( int q = 0; q < 3; ++q ) { x[ q ] = T[ 0 ][ q ] + u * e1[ q ] + v * e2[ q ] + z * e3[ q ]; r2 += ( x[ q ] - g->c[ q ] ) * ( x[ q ] - g->c[ q ] ); }
+                double f = J * g->k * exp( -r2 / ( 2 * g->s * g->s ) );
+                out[ 0 ] += f;
+                out[ 1 ] += f * x[ 0 ]; out[ 2 ] += f * x[ 1 ]; out[ 3 ] += f * x[ 2 ];
+                out[ 4 ] += f * ( x[ 0 ] * x[ 0 ] + x[ 1 ] * x[ 1 ] + x[ 2 ] * x[ 2 ] );
+            }
+        }
+    }
+}
+static void g3_tet_adapt( const g3 *g, const double T[ 4 ][ 3 ], const double whole[ 5 ], int depth, double out[ 5 ] ) {
+    double m[ 6 ][ 3 ];
+    static const int pr[ 6 ][ 2 ] = { { 0, 1 }, { 0, 2 }, { 0, 3 }, { 1, 2 }, { 1, 3 }, { 2, 3 } };
+    for ( int e = 0; e < 6; ++e ) for ( int q = 0; q < 3; ++q ) m[ e ][ q ] = 0.5 * ( T[ pr[ e ][ 0 ] ][ q ] + T[ pr[ e ][ 1 ] ][ q ] );
+    /* the 8 children: 4 corners, and the inner octahedron cut along the diagonal m02-m13 */
+    const double *C[ 8 ][ 4 ] = {
+        { T[ 0 ], m[ 0 ], m[ 1 ], m[ 2 ] }, { m[ 0 ], T[ 1 ], m[ 3 ], m[ 4 ] }, { m[ 1 ], m[ 3 ], T[ 2 ], m[ 5 ] }, { m[ 2 ], m[ 4 ], m[ 5 ], T[ 3 ] },
+        { m[ 0 ], m[ 1 ], m[ 2 ], m[ 4 ] }, { m[ 0 ], m[ 1 ], m[ 3 ], m[ 4 ] }, { m[ 1 ], m[ 2 ], m[ 4 ], m[ 5 ] }, { m[ 1 ], m[ 3 ], m[ 4 ], m[ 5 ] } };
+    double ch[ 8 ][ 5 ], sum[ 5 ] = { 0, 0, 0, 0, 0 };
+    double Tc[ 8 ][ 4 ][ 3 ];
+    for ( int c = 0; c < 8; ++c ) {
+        for ( int k = 0; k < 4; ++k ) for ( int q = 0; q < 3; ++q ) Tc[ c ][ k ][ q ] = C[ c ][ k ][ q ];
+        g3_tet_rule( g, ( const double( * )[ 3 ] ) Tc[ c ], ch[ c ] );
+        for ( int q = 0; q < 5; ++q ) sum[ q ] += ch[ c ][ q ];
+    }
+    double err = 0, mag = 0;
+    for ( int q = 0; q < 5; ++q ) { err = fmax( err, fabs( sum[ q ] - whole[ q ] ) ); mag = fmax( mag, fabs( sum[ q ] ) ); }
+    if ( err <= 1e-12 * mag + 1e-20 * g->m || depth >= 5 ) { for ( int q = 0; q < 5; ++q ) out[ q ] = sum[ q ]; return; }
+    for ( int q = 0; q < 5; ++q ) out[ q ] = 0;
+    for ( int c = 0; c < 8; ++c ) {
+        double r[ 5 ];
+        g3_tet_adapt( g, ( const double( * )[ 3 ] ) Tc[ c ], ch[ c ], depth + 1, r );
+        for ( int q = 0; q < 5; ++q ) out[ q ] += r[ q ];
+    }
+}
+static void g3_tri_rule( const g3 *g, const double *A, const double *B, const double *C, double *out ) {
+    double e1[ 3 ], e2[ 3 ], cr[ 3 ];
+    for ( int q = 0; q < 3; ++q ) { e1[ q ] = B[ q ] - A[ q ]; e2[ q ] = C[ q ] - A[ q ]; }
+    cr[ 0 ] = e1[ 1 ] * e2[ 2 ] - e1[ 2 ] * e2[ 1 ]; cr[ 1 ] = e1[ 2 ] * e2[ 0 ] - e1[ 0 ] * e2[ 2 ]; cr[ 2 ] = e1[ 0 ] * e2[ 1 ] - e1[ 1 ] * e2[ 0 ];
+    double area2 = sqrt( dot3( cr, cr ) );
+    *out = 0;
+    for ( int i = 0; i < GL_N; ++i ) {
+        double a = 0.5 * ( gl_x[ i ] + 1 ), wa = 0.5 * gl_w[ i ];
+        for ( int j = 0; j < GL_N; ++j ) {
+            double b = 0.5 * ( gl_x[ j ] + 1 ), wb = 0.5 * gl_w[ j ];
+            double u = a, v = b * ( 1 - a ), r2 = 0;
+            for ( int q = 0; q < 3; ++q ) { double x = A[ q ] + u * e1[ q ] + v * e2[ q ]; r2 += ( x - g->c[ q ] ) * ( x - g->c[ q ] ); }
+            *out += wa * wb * ( 1 - a ) * area2 * g->k * exp( -r2 / ( 2 * g->s * g->s ) );
+        }
+    }
+}
+static double g3_tri_adapt( const g3 *g, const double *A, const double *B, const double *C, double whole, int depth ) {
+    double ab[ 3 ], bc[ 3 ], ca[ 3 ];
+    for ( int q = 0; q < 3; ++q ) { ab[ q ] = 0.5 * ( A[ q ] + B[ q ] ); bc[ q ] = 0.5 * ( B[ q ] + C[ q ] ); ca[ q ] = 0.5 * ( C[ q ] + A[ q ] ); }
+    double r[ 4 ];
+    g3_tri_rule( g, A, ab, ca, &r[ 0 ] ); g3_tri_rule( g, ab, B, bc, &r[ 1 ] ); g3_tri_rule( g, ca, bc, C, &r[ 2 ] ); g3_tri_rule( g, ab, bc, ca, &r[ 3 ] );
+    double sum = r[ 0 ] + r[ 1 ] + r[ 2 ] + r[ 3 ];
+    if ( fabs( sum - whole ) <= 1e-13 * fabs( sum ) + 1e-22 * g->m || depth >= 8 ) return sum;
+    return g3_tri_adapt( g, A, ab, ca, r[ 0 ], depth + 1 ) + g3_tri_adapt( g, ab, B, bc, r[ 1 ], depth + 1 ) +
+           g3_tri_adapt( g, ca, bc, C, r[ 2 ], depth + 1 ) + g3_tri_adapt( g, ab, bc, ca, r[ 3 ], depth + 1 );
+}
+static void g3_of( const od_pb *pb, int gi, const double *p, g3 *g ) {
+    const double *G = pb->dval + gi * 5;
+    for ( int q = 0; q < 3; ++q ) g->c[ q ] = G[ q ] - p[ q ];
+    g->s = G[ 3 ]; g->m = G[ 4 ];
+    g->k = g->m / ( pow( 2 * M_PI, 1.5 ) * g->s * g->s * g->s );
+}
+/* mass, first moment and `int |y|^2 rho` of the polyhedron (seed frame), summed over the gaussians */
+static void gauss_cell3( const od_pb *pb, const poly3 *P, const double *p, double *M, double F[ 3 ], double *S ) {
+    double apex[ 3 ] = { 0, 0, 0 };
+    int cnt = 0;
+    for ( int f = 0; f < P->nf; ++f )
+        for ( int k = 0; k < P->nv[ f ]; ++k ) { for ( int q = 0; q < 3; ++q ) apex[ q ] += P->v[ f ][ k ].p[ q ]; ++cnt; }
+    for ( int q = 0; q < 3; ++q ) apex[ q ] /= cnt ? cnt : 1;
+    double acc[ 5 ] = { 0, 0, 0, 0, 0 };
+    const int ng = ( int ) pb->dpar[ 0 ];
+    for ( int gi = 0; gi < ng; ++gi ) {
+        g3 g;
+        g3_of( pb, gi, p, &g );
+        for ( int f = 0; f < P->nf; ++f )
+            for ( int k = 1; k + 1 < P->nv[ f ]; ++k ) {
+                double T[ 4 ][ 3 ];
+                for ( int q = 0; q < 3; ++q ) {
+                    T[ 0 ][ q ] = apex[ q ]; T[ 1 ][ q ] = P->v[ f ][ 0 ].p[ q ]; T[ 2 ][ q ] = P->v[ f ][ k ].p[ q ]; T[ 3 ][ q ] = P->v[ f ][ k + 1 ].p[ q ];
+                }
+                double whole[ 5 ], r[ 5 ];
+                g3_tet_rule( &g, ( const double( * )[ 3 ] ) T, whole );
+                g3_tet_adapt( &g, ( const double( * )[ 3 ] ) T, whole, 0, r );
+                for ( int q = 0; q < 5; ++q ) acc[ q ] += r[ q ];
+            }
+    }
+    *M = acc[ 0 ]; F[ 0 ] = acc[ 1 ]; F[ 1 ] = acc[ 2 ]; F[ 2 ] = acc[ 3 ]; *S = acc[ 4 ];
+}
+/* `int_face rho` of face f (seed frame) */
+static double gauss_face3( const od_pb *pb, const poly3 *P, int f, const double *p ) {
+    const int ng = ( int ) pb->dpar[ 0 ];
+    double r = 0;
+    for ( int gi = 0; gi < ng; ++gi ) {
+        g3 g;
+        g3_of( pb, gi, p, &g );
+        for ( int k = 1; k + 1 < P->nv[ f ]; ++k ) {
+            const double *A = P->v[ f ][ 0 ].p, *B = P->v[ f ][ k ].p, *C = P->v[ f ][ k + 1 ].p;
+            double whole;
+            g3_tri_rule( &g, A, B, C, &whole );
+            r += g3_tri_adapt( &g, A, B, C, whole, 0 );
+        }
+    }
+    return r;
+}
+
 static int cell3( const od_pb *pb, long i, int brute, poly3 *P ) {
     const double *p = pb->pos + 3 * i, wi = wt( pb, i );
     double lo[ 3 ], hi[ 3 ];
@@ -712,13 +860,20 @@ static int cell3( const od_pb *pb, long i, int brute, poly3 *P ) {
 
 static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
     const double *p = pb->pos + 3 * i;
-    double V, F[ 3 ], S;
-    poly3_integrals( P, &V, F, &S );
-    double r = pb->dpar[ 0 ];
-    double M = r * V;
+    double V, F[ 3 ], S, M;
+    const int gauss = pb->dkind == DENS_GAUSS;
+    double r = gauss ? 1.0 : pb->dpar[ 0 ];
+    if ( gauss ) {
+        gauss_cell3( pb, P, p, &M, F, &S );
+        V = M;
+    } else {
+        poly3_integrals( P, &V, F, &S );
+        M = r * V;
+        S *= r;
+    }
     if ( o->mass ) o->mass[ i ] = M;
     if ( o->bary ) for ( int a = 0; a < 3; ++a ) o->bary[ 3 * i + a ] = V > 0 ? p[ a ] + F[ a ] / V : p[ a ];
-    if ( o->cost ) o->cost[ i ] = r * S;
+    if ( o->cost ) o->cost[ i ] = S;
     if ( o->nvert ) {
         int nv = 0;
         for ( int f = 0; f < P->nf; ++f ) nv += P->nv[ f ];
@@ -730,7 +885,7 @@ static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
             int j = P->id[ f ];
             if ( j < 0 ) continue;
             if ( c >= o->cap ) { o->nb[ i ] = c; return OD_ERR_NEIGHBOURS; }
-            double meas = r * face_area3( P, f );
+            double meas = gauss ? gauss_face3( pb, P, f, p ) : r * face_area3( P, f );
             double q[ 3 ] = { pb->pos[ 3 * j ] - p[ 0 ], pb->pos[ 3 * j + 1 ] - p[ 1 ], pb->pos[ 3 * j + 2 ] - p[ 2 ] };
             o->nid[ ( long ) i * o->cap + c ] = j;
             o->nm[ ( long ) i * o->cap + c ] = meas;
@@ -748,13 +903,13 @@ static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
 static int diagram( od_pb *pb, int brute, const od_out *o, long *bad ) {
     int status = OD_OK;
     long first_bad = -1;
-    if ( pb->dim == 3 && pb->dkind != DENS_UNIFORM ) return OD_ERR_UNSUPPORTED;
+    if ( pb->dim == 3 && pb->dkind == DENS_IMAGE ) return OD_ERR_UNSUPPORTED;
     gl_init();
     build_grid( pb );
 #pragma omp parallel
     {
         void *buf = malloc( pb->dim == 2 ? 2 * sizeof( poly2 ) : sizeof( poly3 ) );
-#pragma omp for schedule( dynamic, 64 )
+#pragma omp for schedule( dynamic, 4 )
         for ( long i = 0; i < pb->n; ++i ) {
             int st;
             if ( pb->dim == 2 ) {

@@ -134,6 +134,38 @@ def test_gaussians_integrate_what_a_sampling_says():
     assert abs(fd + got["nc"][0, 0]) < 1e-6 * max(1, abs(fd))
 
 
+def test_3d_gaussians_integrate_what_a_sampling_says():
+    """the oracle's tetrahedral quadrature of 3D gaussians: total = the mixture's mass in the cube (erf products),
+    cells = what a sampling of the mixture gives, and the face integrals are the Jacobian: d m_i / d w_j = - c_ij"""
+    from scipy.special import erf
+    rng = np.random.default_rng(906)
+    c = rng.uniform(0.3, 0.7, size=(2, 3))
+    s = np.array([0.1, 0.13])
+    m = np.array([0.6, 0.4])
+    pos = rng.uniform(0.1, 0.9, size=(40, 3))
+    got = O.cells(pos, density=("gauss", c, s, m))
+    assert got["status"] == 0
+    inside = sum(m[k] * np.prod([0.5 * (erf((1 - c[k, a]) / (s[k] * np.sqrt(2))) - erf(-c[k, a] / (s[k] * np.sqrt(2)))) for a in range(3)])
+                 for k in range(2))
+    assert abs(got["mass"].sum() - inside) < 1e-12
+    k = rng.choice(2, size=600000, p=m)
+    pts = c[k] + s[k, None] * rng.standard_normal((600000, 3))
+    keep = ((pts >= 0) & (pts <= 1)).all(axis=1)
+    owner = ((pts[keep][:, None, :] - pos[None]) ** 2).sum(axis=2).argmin(axis=1)
+    ref = np.bincount(owner, minlength=40) / len(pts)
+    assert np.abs(got["mass"] - ref).max() < 3e-3
+    big = np.nonzero(got["mass"] > 0.02)[0]
+    bref = np.array([pts[keep][owner == i].mean(axis=0) for i in big])
+    assert np.abs(got["bary"][big] - bref).max() < 5e-3
+    w = np.zeros(40)
+    i, j = 0, int(got["nid"][0, 0])
+    h = 1e-6
+    wp = w.copy(); wp[j] += h
+    wm = w.copy(); wm[j] -= h
+    fd = (O.cells(pos, wp, density=("gauss", c, s, m))["mass"][i] - O.cells(pos, wm, density=("gauss", c, s, m))["mass"][i]) / (2 * h)
+    assert abs(fd + got["nc"][0, 0]) < 1e-5 * max(1e-3, abs(fd))
+
+
 @pytest.mark.parametrize("d", [2, 3])
 def test_the_laplacian_is_the_jacobian_of_the_measures(d):
     """tests/test_SdotPlanNd.py:184-243: d m_i / d w_j = - c_ij, d m_i / d w_i = sum_j c_ij"""
