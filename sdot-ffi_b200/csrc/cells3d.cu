@@ -13,6 +13,7 @@
 // by one lane against every vertex; the walk stops by the same security radius as in 2D.  Integration: signed
 // tetrahedra (seed, point of face f, K, T) for every vertex K and directed edge (f, b) of K, T the vertex across
 // that edge -- exact for volume, first and second moments; per-face areas summed in plane order (deterministic).
+// Sums of gaussians: face integrals only, by Gauss's theorem (integrate_gauss3).
 #include "internal.h"
 
 namespace sdot {
@@ -30,6 +31,8 @@ struct Cell3 {
     unsigned char va[ VC ], vb[ VC ], vc[ VC ];
     unsigned char out[ VC ];
     unsigned char nt[ VC ][ 3 ];                 // new triples of a cut
+    unsigned char tw[ 3 * VC ];                  // gaussians: the vertex across each (vertex, edge) entry, 255 if none
+    double fmp[ PC ];                            // gaussians: the winding-angle part of each face's integral
     int nv, np;
 };
 
@@ -188,6 +191,161 @@ __device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, dou
     return true;
 }
 
+// ---- sums of isotropic gaussians over the polyhedron ------------------------------------------------------------------
+// rho_g = m / ((2 pi)^{3/2} s^3) exp(-|y - c|^2 / 2 s^2).  Everything reduces to integrals over the faces:
+//  * mass (Gauss's theorem with the radial field G(r)/(4 pi r^2), G the gaussian's mass within radius r, minus the
+//    point mass m at c, which leaves erfc tails and no cancellation far from c):
+//        M = m [c inside] + sum_f h_f/(4 pi) int_face-angle [ Ht( r_out ) - Ht( |h_f| ) ] dtheta,  Ht(r) = m erfc(r/(s sqrt2))/r
+//    with h_f = (y - c).n_f on face f and the angle taken about the foot of c on the face;
+//  * face integrals: int_face rho = K e^{-h^2/2s^2} s^2 [ Theta_f - int exp(-R(theta)^2/2s^2) dtheta ], Theta_f the
+//    winding angle of the face about the foot (2 pi or 0), R(theta) the distance from the foot to the face's edge;
+//  * moments from (y - c) rho = -s^2 grad rho and |y - c|^2 rho = s^2 (3 rho - div((y - c) rho)):
+//        int (y - c) rho = -s^2 sum_f n_f int_face rho,   int |y - c|^2 rho = s^2 ( 3 M - sum_f h_f int_face rho ).
+// The angle integrals run per edge in phi, the angle from the foot's perpendicular on the edge line (R = d / cos phi),
+// in Gauss-Legendre pieces over which R changes by at most s/2 and that stay within half their distance of +-pi/2.
+__constant__ double c_g3x[ 8 ] = { -0.9602898564975363, -0.7966664774136267, -0.5255324099163290, -0.1834346424956498,
+                                    0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363 };
+__constant__ double c_g3w[ 8 ] = { 0.1012285362903763, 0.2223810344533745, 0.3137066458778873, 0.3626837833783620,
+                                    0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763 };
+constexpr double HALF_PI = 1.5707963267948966;
+constexpr int G3_MAX_PIECES = 128;
+
+// the signed angle of the edge K -> T about F, positive counterclockwise about -n (the cell's edges run clockwise
+// about the outward normal n, so a foot inside the face gets +2 pi in total)
+__device__ __forceinline__ double edge_angle3( double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty,
+                                               double Tz, double nx, double ny, double nz ) {
+    double ax = Kx - Fx, ay = Ky - Fy, az = Kz - Fz, bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
+    double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
+    return atan2( o, ax * bx + ay * by + az * bz );
+}
+
+// A = int Ht( sqrt( h^2 + R^2 ) ) / m dtheta and B = int exp( -R^2 / 2 s^2 ) dtheta along the edge K -> T (signed as above)
+__device__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty, double Tz, double nx,
+                             double ny, double nz, double h, double sg, double &A, double &B ) {
+    A = B = 0;
+    double ax = Kx - Fx, ay = Ky - Fy, az = Kz - Fz, ex = Tx - Kx, ey = Ty - Ky, ez = Tz - Kz;
+    double L = sqrt( ex * ex + ey * ey + ez * ez );
+    if ( ! ( L > 0 ) ) return;
+    double ux = ex / L, uy = ey / L, uz = ez / L;
+    double s0 = ax * ux + ay * uy + az * uz, s1 = s0 + L;
+    double qx = ax - s0 * ux, qy = ay - s0 * uy, qz = az - s0 * uz;
+    double d = sqrt( qx * qx + qy * qy + qz * qz );
+    if ( ! ( d > 0 ) ) return;
+    double bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
+    double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
+    const double sgn = o >= 0 ? 1.0 : -1.0;
+    const double p0 = atan2( s0, d ), p1 = atan2( s1, d );
+    const double inv2s2 = 0.5 / ( sg * sg ), kr = 0.7071067811865476 / sg, h2 = h * h;
+    double phi = p0;
+    for ( int piece = 0; piece < G3_MAX_PIECES && phi < p1; ++piece ) {
+        double R = d / cos( phi ), nxt;
+        if ( phi < 0 ) {
+            nxt = phi + 0.5 * ( HALF_PI + phi );
+            double Rn = fmax( d, R - 0.5 * sg );
+            nxt = fmin( nxt, -acos( fmin( 1.0, d / Rn ) ) );
+            nxt = fmin( nxt, 0.0 );
+            if ( nxt <= phi ) nxt = 0.0;
+        } else {
+            nxt = ( phi + 0.5 * HALF_PI ) / 1.5;
+            nxt = fmin( nxt, acos( fmin( 1.0, d / ( R + 0.5 * sg ) ) ) );
+        }
+        nxt = fmin( nxt, p1 );
+        if ( piece == G3_MAX_PIECES - 1 ) nxt = p1;
+        const double hw = 0.5 * ( nxt - phi ), mid = 0.5 * ( nxt + phi );
+        for ( int q = 0; q < 8; ++q ) {
+            double f = mid + hw * c_g3x[ q ], w = hw * c_g3w[ q ];
+            double Rq = d / cos( f ), R2 = Rq * Rq;
+            if ( h != 0 ) {
+                double r = sqrt( h2 + R2 );
+                A += w * erfc( r * kr ) / r;
+            }
+            B += w * exp( -R2 * inv2s2 );
+        }
+        phi = nxt;
+    }
+    A *= sgn;
+    B *= sgn;
+}
+
+// the gaussian sums over the clipped cell: lane parts of the mass, of the first moment about the seed and of
+// int |y|^2 rho (seed frame); C.area receives each (vertex, edge) entry's part of its face integral and C.fmp each
+// face's winding-angle part (both summed over the gaussians)
+__device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int lane, double px, double py, double pz, double &M, double &Fx,
+                                                double &Fy, double &Fz, double &S2 ) {
+    const int nv = C.nv, np = C.np;
+    for ( int k = lane; k < nv; k += 32 ) {
+        const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+        for ( int q = 0; q < 3; ++q ) {
+            int t = twin_of( C, e[ ( q + 1 ) % 3 ], e[ q ] );
+            C.tw[ 3 * k + q ] = t < 0 ? 255 : ( unsigned char ) t;
+            C.area[ 3 * k + q ] = 0;
+        }
+    }
+    for ( int p = lane; p < np; p += 32 ) C.fmp[ p ] = 0;
+    __syncwarp();
+    if ( nv == 0 ) return;
+    const double INV4PI = 0.07957747154594767, TWO_PI = 6.283185307179586;
+    const int ng = P.dn[ 0 ];
+    for ( int g = 0; g < ng; ++g ) {
+        const double *G = P.dval + g * 5;
+        const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
+        const double s2g = sg * sg, K = mg / ( 15.749609945653303 * s2g * sg ), kr = 0.7071067811865476 / sg;   // (2 pi)^{3/2}
+        double Mg = 0, Gx = 0, Gy = 0, Gz = 0, Sg = 0;
+        for ( int k = lane; k < nv; k += 32 ) {
+            const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+            const double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
+            for ( int q = 0; q < 3; ++q ) {
+                const int t = C.tw[ 3 * k + q ];
+                if ( t == 255 ) continue;
+                const int f = e[ q ];
+                const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] );
+                const double nhx = C.nx[ f ] / nn, nhy = C.ny[ f ] / nn, nhz = C.nz[ f ] / nn;
+                const double h = ( C.no[ f ] - ( C.nx[ f ] * cx + C.ny[ f ] * cy + C.nz[ f ] * cz ) ) / nn;
+                double A, B;
+                edge_gauss3( cx + h * nhx, cy + h * nhy, cz + h * nhz, Kx, Ky, Kz, C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz, h, sg, A, B );
+                Mg += h * INV4PI * mg * A;
+                const double b = -K * exp( -h * h * 0.5 / s2g ) * s2g * B;
+                C.area[ 3 * k + q ] += b;
+                Gx -= s2g * nhx * b; Gy -= s2g * nhy * b; Gz -= s2g * nhz * b;
+                Sg += h * b;
+            }
+        }
+        // per face: the winding angle of the face about the foot of c, and whether c is on the inner side
+        bool ok = true;
+        for ( int p = lane; p < np; p += 32 ) {
+            const double nn = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
+            const double nhx = C.nx[ p ] / nn, nhy = C.ny[ p ] / nn, nhz = C.nz[ p ] / nn;
+            const double h = ( C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) ) / nn;
+            ok = ok && h >= 0;
+            const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
+            double th = 0;
+            for ( int k = 0; k < nv; ++k ) {
+                const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+                for ( int q = 0; q < 3; ++q ) {
+                    const int t = C.tw[ 3 * k + q ];
+                    if ( e[ q ] != p || t == 255 ) continue;
+                    th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
+                }
+            }
+            const double kk = rint( th / TWO_PI );
+            const double Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
+            if ( Th != 0 ) {
+                const double I = K * exp( -h * h * 0.5 / s2g ) * s2g * Th;
+                C.fmp[ p ] += I;
+                // the flux of the erfc field's constant part; at h = 0 its limit from the inner side
+                Mg -= h != 0 ? h * INV4PI * mg * erfc( fabs( h ) * kr ) / fabs( h ) * Th : INV4PI * mg * Th;
+                Gx -= s2g * nhx * I; Gy -= s2g * nhy * I; Gz -= s2g * nhz * I;
+                Sg += h * I;
+            }
+        }
+        if ( __all_sync( FULL3, ok ) && lane == 0 ) Mg += mg;          // the point mass taken out of the field
+        M += Mg;
+        Fx += Gx + cx * Mg; Fy += Gy + cy * Mg; Fz += Gz + cz * Mg;
+        S2 += s2g * ( 3 * Mg - Sg ) + 2 * ( cx * Gx + cy * Gy + cz * Gz ) + ( cx * cx + cy * cy + cz * cz ) * Mg;
+        __syncwarp();
+    }
+}
+
 __device__ __forceinline__ void record_error3( ErrRec *err, int code, int prob, int seed, int needed ) {
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
 }
@@ -203,7 +361,7 @@ __device__ __forceinline__ double gp_of3( double x, int r, double p ) {
     return r == 1 ? 1 / x : 1;
 }
 
-__global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+__global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                         unsigned flags, ErrRec *err ) {
     extern __shared__ char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -294,10 +452,14 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
                 if ( lane == 0 ) C.nv = 0;
                 __syncwarp();
             }
-            // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once
+            // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once; gaussians by
+            // their face integrals (the sums below are then already density-weighted)
             double vol = 0, fx = 0, fy = 0, fz = 0, s2 = 0;
             const int nv = C.nv;
-            for ( int k = lane; k < nv; k += 32 ) {
+            const bool gauss = P.dkind == D_GAUSS;
+            const double rho = gauss ? 1.0 : P.rho;
+            if ( gauss ) integrate_gauss3( C, P, lane, px, py, pz, vol, fx, fy, fz, s2 );
+            for ( int k = lane; k < nv && ! gauss; k += 32 ) {
                 int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
                 double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
                 for ( int q = 0; q < 3; ++q ) {
@@ -329,7 +491,7 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
                 }
             }
             __syncwarp();
-            double mass = P.rho * warp_sum( vol );
+            double mass = rho * warp_sum( vol );
             // the facets: per plane, its triangles summed in vertex order
             int nf = 0;
             if ( facets || ( flags & F_REPORT ) ) {
@@ -339,12 +501,14 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
                     int p = pbase + lane;
                     double ar = 0;
                     bool seed_plane = p < C.np && C.pid[ p ] >= 0;
-                    if ( seed_plane )
+                    if ( seed_plane ) {
                         for ( int k = 0; k < nv; ++k ) {
                             if ( C.va[ k ] == p ) ar += C.area[ 3 * k ];
                             if ( C.vb[ k ] == p ) ar += C.area[ 3 * k + 1 ];
                             if ( C.vc[ k ] == p ) ar += C.area[ 3 * k + 2 ];
                         }
+                        if ( gauss ) ar += C.fmp[ p ];
+                    }
                     bool fac = seed_plane && ar > 0;
                     unsigned fm = __ballot_sync( FULL3, fac );
                     int slot = written + __popc( fm & ( ( 1u << lane ) - 1 ) );
@@ -353,8 +517,8 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
                         size_t at = ( size_t ) row * P.cap + slot;
                         int j = C.pid[ p ];
                         P.nid[ at ] = user_order ? P.user[ j ] : j;
-                        P.nc[ at ] = P.rho * ar / ( 2 * dist );
-                        if ( P.nm ) P.nm[ at ] = P.rho * ar;
+                        P.nc[ at ] = rho * ar / ( 2 * dist );
+                        if ( P.nm ) P.nm[ at ] = rho * ar;
                     }
                     written += __popc( fm );
                 }
@@ -367,7 +531,7 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
             }
             if ( moments ) {
                 double mx = warp_sum( fx ), my = warp_sum( fy ), mz = warp_sum( fz ), ss = warp_sum( s2 );
-                double vv = mass / P.rho;
+                double vv = mass / rho;
                 if ( lane == 0 ) {
                     if ( user_order ) {
                         if ( P.first ) {
@@ -375,10 +539,10 @@ __global__ void __launch_bounds__( 32 * W3 ) k_cells3d( const ProbDev *__restric
                             P.first[ 3 * ( size_t ) user + 1 ] = vv > 0 ? py + my / vv : py;
                             P.first[ 3 * ( size_t ) user + 2 ] = vv > 0 ? pz + mz / vv : pz;
                         }
-                        if ( P.cost ) P.cost[ user ] = P.rho * ss;
+                        if ( P.cost ) P.cost[ user ] = rho * ss;
                     } else {
-                        if ( P.first ) { P.first[ 3 * ( size_t ) s ] = P.rho * mx; P.first[ 3 * ( size_t ) s + 1 ] = P.rho * my; P.first[ 3 * ( size_t ) s + 2 ] = P.rho * mz; }
-                        if ( P.cost ) P.cost[ s ] = P.rho * ss;
+                        if ( P.first ) { P.first[ 3 * ( size_t ) s ] = rho * mx; P.first[ 3 * ( size_t ) s + 1 ] = rho * my; P.first[ 3 * ( size_t ) s + 2 ] = rho * mz; }
+                        if ( P.cost ) P.cost[ s ] = rho * ss;
                     }
                 }
             }

@@ -311,7 +311,6 @@ void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positio
             G.gauss[ k * ( dim + 2 ) + dim ] = ss[ k ];
             G.gauss[ k * ( dim + 2 ) + dim + 1 ] = mm[ k ];
         }
-        if ( dim == 3 ) throw Error( SDOT_ERR_UNSUPPORTED, "3D gaussian densities are not integrated by this build" );
     }
     dbytes = size_t( nval + npre ) * 8 + 1024;
     size_t bytes = size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( G.ncell ) * 8 + dbytes + 8 * 256;

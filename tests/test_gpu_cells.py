@@ -132,6 +132,23 @@ def test_gaussian_density_matches_the_oracle():
     _compare(pos, None, (("gauss", c, s, ng.weights), g))
 
 
+@pytest.mark.parametrize("n", [400, 1500])
+def test_3d_gaussian_density_matches_the_oracle(n):
+    """3D sums of gaussians: face integrals (Gauss's theorem, angular Gauss-Legendre) on the GPU against the
+    oracle's adaptive tetrahedral quadrature; the total is the mixture's mass inside the cube (erf products)"""
+    from scipy.special import erf
+    rng = np.random.default_rng(23 + n)
+    c = rng.uniform(0.2, 0.8, size=(4, 3))
+    s = rng.uniform(0.05, 0.15, size=4)
+    g = sdot.SumOfGaussians(c, s, support_box=(np.zeros(3), np.ones(3)))
+    ng = g.normalized_version()
+    pos = rng.uniform(size=(n, 3))
+    m = _compare(pos, None, (("gauss", c, s, ng.weights), g))
+    inside = sum(wk * np.prod([0.5 * (erf((1 - c[k, a]) / (s[k] * np.sqrt(2))) - erf(-c[k, a] / (s[k] * np.sqrt(2)))) for a in range(3)])
+                 for k, wk in enumerate(ng.weights))
+    assert abs(m.sum() - inside) < 1e-12
+
+
 def test_the_laplacian_is_bit_symmetric():
     rng = np.random.default_rng(4)
     n = 20000

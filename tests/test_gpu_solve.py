@@ -103,6 +103,25 @@ def test_gaussians_with_the_continuation_match_the_oracle():
     assert abs(plan.cost - ref["cost"]) <= 1e-8 * ref["cost"]
 
 
+def test_a_3d_gaussian_target_is_solved():
+    """3D, 4 gaussians (the continuation runs): the plan reaches 1e-8, and the oracle's cells at the plan's weights
+    give the same masses (1e-9 relative) and barycentres"""
+    rng = np.random.default_rng(34)
+    c = rng.uniform(0.2, 0.8, size=(4, 3))
+    s = rng.uniform(0.05, 0.15, size=4)
+    g = sdot.SumOfGaussians(c, s, support_box=(np.zeros(3), np.ones(3)))
+    n = 1200
+    pos = rng.uniform(size=(n, 3))
+    plan = _solve(pos, g, rtol=1e-8)
+    assert plan.converged
+    assert np.abs(plan.cell_masses / plan.target_masses - 1).max() <= 1e-8
+    ng = g.normalized_version()
+    ref = O.cells(pos, plan.weights, box=(np.zeros(3), np.ones(3)), density=("gauss", c, s, ng.weights))
+    assert ref["status"] == 0
+    assert np.abs(ref["mass"] / plan.cell_masses - 1).max() <= 1e-9
+    assert np.abs(ref["bary"] - plan.barycenters).max() <= 1e-9
+
+
 def test_the_similarity_start():
     rng = np.random.default_rng(9)
     pos = rng.uniform(0.5, 1.5, size=(500, 2))
