@@ -325,6 +325,8 @@ def main():
     ap.add_argument("--cells-only", type=int, default=0, help="diagrams of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--cells-dim", type=int, default=2)
     ap.add_argument("--cells-repeat", type=int, default=0)
+    ap.add_argument("--cells-density", default="uniform", choices=["uniform", "gauss"],
+                    help="cells-only target: uniform, or a 4-gaussian mixture like the stream's")
     a = ap.parse_args()
     if a.cells_only:
         import sdot
@@ -332,13 +334,17 @@ def main():
         d = a.cells_dim
         pos = np.random.default_rng(a.seed).uniform(size=(a.cells_only, d))
         w = np.random.default_rng(a.seed + 1).uniform(0, a.cells_only ** (-2.0 / d), size=a.cells_only)
-        pd = sdot.PowerDiagram(pos, w, boundaries=sdot.box_half_spaces(np.zeros(d), np.ones(d)))
+        dist = None
+        if a.cells_density == "gauss":
+            rq = request(a.seed, 0)
+            dist = target_of(dict(rq, d=d, gauss=True, c=np.random.default_rng(a.seed + 2).uniform(0.2, 0.8, size=(4, d))))
+        pd = sdot.PowerDiagram(pos, w, boundaries=sdot.box_half_spaces(np.zeros(d), np.ones(d)), distribution=dist)
         m = pd.facets()
         _lib.set_timing(True)
         for _ in range(a.cells_repeat):
             pd.facets()
         ms, nl, units = _lib.kernel_stats()["cells2d" if d == 2 else "cells3d"]
-        print(json.dumps({"cells_only": a.cells_only, "dim": d, "facets_per_cell": float(m[0].mean()), "launches": nl,
+        print(json.dumps({"cells_only": a.cells_only, "dim": d, "density": a.cells_density, "facets_per_cell": float(m[0].mean()), "launches": nl,
                           "ms_per_launch": ms / max(nl, 1), "ns_per_cell": 1e6 * ms / max(units, 1),
                           "algorithmic_GBps": units * BYTES_PER_CELL[d] / (ms / 1000) / 1e9 if ms else None}))
         return

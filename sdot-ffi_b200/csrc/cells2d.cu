@@ -132,14 +132,21 @@ __constant__ double c_glx[ 8 ] = { -0.9602898564975363, -0.7966664774136267, -0.
 __constant__ double c_glw[ 8 ] = { 0.1012285362903763, 0.2223810344533745, 0.3137066458778873, 0.3626837833783620,
                                     0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763 };
 
-// erf( b ) - erf( a ) without cancellation in the tails
+// erf( u ) - erf( u0 ) without cancellation in the tails, with the u0 terms of an edge computed once:
+// c0 = erfc( |u0| ), f0 = erf( |u0| ); one erf or erfc per call
+__device__ __forceinline__ double erf_from( double u0, double c0, double f0, double u ) {
+    if ( u0 >= 0 && u >= 0 ) return c0 - erfc( u );
+    if ( u0 <= 0 && u <= 0 ) return erfc( -u ) - c0;
+    return u > 0 ? erf( u ) + f0 : -( erf( -u ) + f0 );
+}
 __device__ __forceinline__ double erf_diff( double a, double b ) {
     if ( a >= 0 && b >= 0 ) return erfc( a ) - erfc( b );
     if ( a <= 0 && b <= 0 ) return erfc( -b ) - erfc( -a );
     return erf( b ) - erf( a );
 }
 
-__device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments, EdgeInt &e ) {
+__device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments,
+                                         bool measures, EdgeInt &e ) {
     e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
     double dx = x1 - x0, dy = y1 - y0, len = sqrt( dx * dx + dy * dy );
     if ( len == 0 ) return;
@@ -150,10 +157,8 @@ __device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py,
         double cx = G[ 0 ] - px, cy = G[ 1 ] - py, sg = G[ 2 ], mg = G[ 3 ];
         double K = mg / ( 2 * M_PI * sg * sg ), s2g = sg * sg, sq = sg * r2;
         double E0 = sg * 1.2533141373155003;              // sigma sqrt( pi / 2 )
-        double u0 = ( 0 - cx ) / sq;                       // reference abscissa: the seed
-        double e0 = exp( -( cx * cx ) / ( 2 * s2g ) );
-        // the facet measure: closed form
-        {
+        if ( measures ) {
+            // the facet measure: closed form
             double ux = dx / len, uy = dy / len;
             double sa = ( x0 - cx ) * ux + ( y0 - cy ) * uy, sb = sa + len;
             double fx = x0 - sa * ux - cx, fy = y0 - sa * uy - cy;
@@ -167,6 +172,10 @@ __device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py,
             e.mx += ( x0 - ux * sa ) * mm + ux * ms;
             e.my += ( y0 - uy * sa ) * mm + uy * ms;
         }
+        if ( dy == 0 ) continue;                           // no part in the closed integral of F dy
+        double u0 = ( 0 - cx ) / sq;                       // reference abscissa: the seed
+        double e0 = exp( -( cx * cx ) / ( 2 * s2g ) );
+        double c0 = erfc( fabs( u0 ) ), f0 = erf( fabs( u0 ) );
         // the closed integral, split so that each piece spans at most one sigma
         int np = int( len / sg ) + 1;
         if ( np > 64 ) np = 64;
@@ -174,21 +183,21 @@ __device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py,
             double ta = double( p ) / np, tb = double( p + 1 ) / np;
             double xa = x0 + ta * dx, ya = y0 + ta * dy, xb = x0 + tb * dx, yb = y0 + tb * dy;
             double Dy = yb - ya;
-            if ( Dy == 0 ) continue;
             double am = 0, afx = 0, afy = 0, as2 = 0;
             for ( int q = 0; q < 8; ++q ) {
                 double t = 0.5 + 0.5 * c_glx[ q ], wq = 0.5 * c_glw[ q ];
                 double x = xa + t * ( xb - xa ), y = ya + t * ( yb - ya );
                 double ey = K * exp( -( y - cy ) * ( y - cy ) / ( 2 * s2g ) );
                 double u = ( x - cx ) / sq;
-                double F = ey * E0 * erf_diff( u0, u );
+                double D = erf_from( u0, c0, f0, u );
+                double F = ey * E0 * D;
                 am += wq * F;
                 if ( moments ) {
                     double ex = exp( -( x - cx ) * ( x - cx ) / ( 2 * s2g ) );
                     // int_0^x t g dt = cx F - sigma^2 ey ( ex - e0 )
                     double F1 = cx * F - s2g * ey * ( ex - e0 );
                     // int_0^x t^2 g dt, with t = ( t - cx ) + cx
-                    double A = ey * ( s2g * E0 * erf_diff( u0, u ) - s2g * ( ( x - cx ) * ex - ( 0 - cx ) * e0 ) );
+                    double A = ey * ( s2g * E0 * D - s2g * ( ( x - cx ) * ex - ( 0 - cx ) * e0 ) );
                     double F2 = A + 2 * cx * ( -s2g * ey * ( ex - e0 ) ) + cx * cx * F;
                     afx += wq * F1;
                     afy += wq * y * F;
@@ -470,7 +479,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
                 else if ( P.dkind == D_IMAGE ) {
                     int iref = int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) );
                     edge_image( P, px, py, iref, C.vx, C.vy, x1, y1, moments, e );
-                } else edge_gauss( P, px, py, C.vx, C.vy, x1, y1, moments, e );
+                } else edge_gauss( P, px, py, C.vx, C.vy, x1, y1, moments, facets || ( flags & F_VJP ), e );
             }
             double mass = warp_sum( e.m );
             if ( mass < 0 && mass > -1e-300 ) mass = 0;
@@ -770,7 +779,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
                 else if ( P.dkind == D_IMAGE ) {
                     int iref = int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) );
                     edge_image( P, px, py, iref, x0, y0, x1, y1, moments, e );
-                } else edge_gauss( P, px, py, x0, y0, x1, y1, moments, e );
+                } else edge_gauss( P, px, py, x0, y0, x1, y1, moments, true, e );
             }
             em += e.m; efx += e.fx; efy += e.fy; es2 += e.s2;
             bool fac = k < m && S->id[ k ] >= 0 && e.meas > 0;
