@@ -183,6 +183,7 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
         c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, double( n ) );
+        launch_wpyr( L, dd.as<ProbDev>(), 1 );
         if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
         else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr );
         c.timer.end( c.stream );
@@ -246,6 +247,7 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        launch_wpyr( L, dd.as<ProbDev>(), 1 );
         launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr, c.dovf );
         run_big_cells( c, dd.as<ProbDev>(), F_VJP | F_USER_ORDER );
         CK( cudaGetLastError() );
@@ -322,6 +324,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         CK( cudaMemcpyAsync( base + o3, vch.data(), vch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         // the cells in USER order: the table holds user ids, and the CSR comes out in user order
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        launch_wpyr( L, ( ProbDev * ) base, 1 );
         if ( dim == 2 ) launch_cells2d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
         else launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr );
         if ( dim == 2 ) run_big_cells( c, ( ProbDev * ) base, F_FACETS | F_USER_ORDER );

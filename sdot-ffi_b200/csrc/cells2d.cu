@@ -283,6 +283,137 @@ __device__ __forceinline__ void ring_offset( int r, int ci, int &dx, int &dy ) {
     else { dx = -r; dy = r - t; }
 }
 
+// may a seed of weight at most W, whose nearest possible position is sqrt( d2 ) away, cut a cell of squared radius R2
+// around a seed of weight wi?  Its bisector is ( |q|^2 + wi - wj ) / ( 2 |q| ) from the seed: it reaches the cell's
+// ball only if |q| < R + sqrt( R^2 + wj - wi ).  W < -1e299: an empty cell or block
+__device__ __forceinline__ bool may_cut( double d2, double W, double R2, double wi ) {
+    if ( W < -1e299 ) return false;
+    double ex = R2 + W - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
+    return d2 < rb * rb;
+}
+
+// squared distance from ( px, py ) to the grid cells [ x0, x1 ] x [ y0, y1 ] (inclusive)
+__device__ __forceinline__ double cells_dist2( const ProbDev &P, int x0, int x1, int y0, int y1, double px, double py ) {
+    double bx0 = P.go[ 0 ] + x0 * P.gh[ 0 ], bx1 = P.go[ 0 ] + ( x1 + 1 ) * P.gh[ 0 ];
+    double by0 = P.go[ 1 ] + y0 * P.gh[ 1 ], by1 = P.go[ 1 ] + ( y1 + 1 ) * P.gh[ 1 ];
+    double dx = fmax( 0.0, fmax( bx0 - px, px - bx1 ) ), dy = fmax( 0.0, fmax( by0 - py, py - by1 ) );
+    return dx * dx + dy * dy;
+}
+
+constexpr int WALK_STACK = 64;       // pyramid walk: at most 3 entries per level stay on the stack (16 levels in 2D)
+constexpr int RINGS_FIRST = 2;       // rings walked before the pyramid takes over
+constexpr int WALK_LEAF = 2;         // the walk's leaves: blocks of 4 x 4 grid cells, one cell per lane
+
+// The pyramid of weight majorants walked depth first, nearest child first, skipping the cells within Chebyshev
+// distance rd of ( cx, cy ) (the rings already walked) and every block that claims no vertex of the current cell
+// (`claims( lo, hi, a, b )`, warp-uniform).  At a leaf block, lane k holds the seed range of its k-th cell (empty if
+// `may_cut` rules it out) and `cut( beg, cnt )` clips by them; it returns false to stop.  `radius2()` is the cell's
+// squared radius.  Lane 0 writes the stack.
+template<class Cut, class Radius2, class Claims>
+__device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py, double wi, int cx, int cy, int rd, int2 *stk, Cut cut,
+                               Radius2 radius2, Claims claims ) {
+    const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
+    if ( lane == 0 ) stk[ 0 ] = make_int2( ( P.nlev - 1 ) << 16, 0 );
+    int sp = 1;
+    __syncwarp();
+    double R2 = radius2();
+    for ( int guard = 0; sp > 0 && guard < ( 1 << 24 ); ++guard ) {
+        const int2 e = stk[ sp - 1 ];
+        --sp;
+        __syncwarp();
+        const int l = e.x >> 16, X = e.x & 0xffff, Y = e.y;
+        const int x0 = X << l, y0 = Y << l;
+        const int x1 = min( ( X + 1 ) << l, g0 ) - 1, y1 = min( ( Y + 1 ) << l, g1 ) - 1;
+        if ( x0 >= cx - rd && x1 <= cx + rd && y0 >= cy - rd && y1 <= cy + rd ) continue;
+        const size_t rec = P.poff[ l ] + ( size_t ) Y * lev_dim( g0, l ) + X;
+        const double b = wmaj_b( P, rec );
+        if ( b < -1e299 ) continue;
+        const double lo[ 2 ] = { P.go[ 0 ] + x0 * P.gh[ 0 ], P.go[ 1 ] + y0 * P.gh[ 1 ] };
+        const double hi[ 2 ] = { P.go[ 0 ] + ( x1 + 1 ) * P.gh[ 0 ], P.go[ 1 ] + ( y1 + 1 ) * P.gh[ 1 ] };
+        if ( ! claims( lo, hi, P.wpyr + rec * 3, b ) ) continue;
+        if ( l <= WALK_LEAF ) {
+            const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;           // at most 4 x 4
+            int beg = 0, cnt = 0;
+            if ( lane < bw * bh ) {
+                const int x = x0 + lane % bw, y = y0 + lane / bw;
+                const bool walked = x >= cx - rd && x <= cx + rd && y >= cy - rd && y <= cy + rd;
+                const size_t gc = ( size_t ) y * g0 + x;
+                if ( ! walked && may_cut( cells_dist2( P, x, x, y, y, px, py ), wmaj_b( P, gc ), R2, wi ) ) {
+                    int2 rg = P.cell_range[ gc ];
+                    beg = rg.x;
+                    cnt = rg.y - rg.x;
+                }
+            }
+            if ( ! cut( beg, cnt ) ) return;
+            R2 = radius2();
+            continue;
+        }
+        // the children, farthest pushed first so that the nearest is walked first
+        const int dx1 = lev_dim( g0, l - 1 ), dy1 = lev_dim( g1, l - 1 );
+        double cd[ 4 ];
+        int cc[ 4 ], nc = 0;
+        for ( int k = 0; k < 4; ++k ) {
+            const int X2 = 2 * X + ( k & 1 ), Y2 = 2 * Y + ( k >> 1 );
+            if ( X2 >= dx1 || Y2 >= dy1 ) continue;
+            const int a0 = X2 << ( l - 1 ), b0 = Y2 << ( l - 1 );
+            const int a1 = min( ( X2 + 1 ) << ( l - 1 ), g0 ) - 1, b1 = min( ( Y2 + 1 ) << ( l - 1 ), g1 ) - 1;
+            double d = cells_dist2( P, a0, a1, b0, b1, px, py );
+            int q = nc++;
+            while ( q > 0 && cd[ q - 1 ] < d ) { cd[ q ] = cd[ q - 1 ]; cc[ q ] = cc[ q - 1 ]; --q; }
+            cd[ q ] = d;
+            cc[ q ] = ( X2 << 16 ) | Y2;
+        }
+        if ( sp + nc > WALK_STACK ) return;                // cannot happen below 2^21 cells per side
+        if ( lane == 0 )
+            for ( int k = 0; k < nc; ++k ) stk[ sp + k ] = make_int2( ( ( l - 1 ) << 16 ) | ( cc[ k ] >> 16 ), cc[ k ] & 0xffff );
+        sp += nc;
+        __syncwarp();
+    }
+}
+
+// the seeds of up to 32 grid cells (lane k: the range [ beg, beg + cnt ) of one cell) as candidates, 32 at a time:
+// a parallel pre-test against the polygon, then the clips of those that cut, in lane order
+__device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int lane, int s, double px, double py, double wi, int beg, int cnt,
+                                               bool &overflow ) {
+    int inc = cnt;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL, inc, o ); if ( lane >= o ) inc += t; }
+    const int total = __shfl_sync( FULL, inc, 31 );
+    const int exc = inc - cnt;
+    for ( int t0 = 0; t0 < total && C.m > 0 && ! overflow; t0 += 32 ) {
+        const int t = t0 + lane;
+        int owner = 0;
+#pragma unroll
+        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
+        owner = owner > 31 ? 31 : owner;
+        int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
+        int j = obeg + ( t - oexc );
+        bool valid = t < total && j != s;
+        double qx = 0, qy = 0, off = 0;
+        if ( valid ) {
+            qx = P.pos[ 2 * ( size_t ) j ] - px;
+            qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
+            double qw = P.w ? P.w[ j ] : 0.0;
+            off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+        }
+        // the parallel pre-test: does candidate `lane` cut the current polygon at all?
+        bool cuts = false;
+        for ( int k = 0; k < C.m; ++k ) {
+            double X = __shfl_sync( FULL, C.vx, k ), Y = __shfl_sync( FULL, C.vy, k );
+            cuts |= qx * X + qy * Y > off;
+        }
+        unsigned todo = __ballot_sync( FULL, valid && cuts );
+        while ( todo ) {
+            int k = __ffs( todo ) - 1;
+            todo &= todo - 1;
+            double nx = __shfl_sync( FULL, qx, k ), ny = __shfl_sync( FULL, qy, k ), no = __shfl_sync( FULL, off, k );
+            int nid = __shfl_sync( FULL, j, k );
+            if ( ! wclip( C, lane, nx, ny, no, nid ) ) { overflow = true; break; }
+            if ( C.m == 0 ) break;
+        }
+    }
+}
+
 __device__ __forceinline__ void record_error( ErrRec *err, int code, int prob, int seed, int needed ) {
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
 }
@@ -360,6 +491,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
                                                     unsigned flags, ErrRec *err, OvfList *ovf ) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     __shared__ double sh_rep[ 8 ][ NB_REPORT ];
+    __shared__ int2 sh_stk[ 8 ][ WALK_STACK ];
     const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     for ( int c = blockIdx.x; c < nchunks; c += gridDim.x ) {
         const Chunk ch = chunks[ c ];
@@ -392,68 +524,50 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
             cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
             cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
             int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
+            int rd = -1;                 // the rings walked, when the pyramid takes over
             for ( int r = 0; r <= rmax && C.m > 0 && ! overflow; ++r ) {
                 const int ncell = r == 0 ? 1 : 8 * r;
-                // the security ball of the current cell: a grid cell farther than its radius holds no cutting seed
+                // a grid cell farther than the security radius of its own largest weight holds no cutting seed
                 double R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
-                double ex = R2 + wmax - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
                 for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
                     int ci = cb + lane, beg = 0, cnt = 0;
                     if ( ci < ncell ) {
                         int dx, dy;
                         ring_offset( r, ci, dx, dy );
                         int x = cx + dx, y = cy + dy;
-                        double bx0 = P.go[ 0 ] + x * P.gh[ 0 ] - px, by0 = P.go[ 1 ] + y * P.gh[ 1 ] - py;
-                        double ddx = fmax( 0.0, fmax( bx0, -( bx0 + P.gh[ 0 ] ) ) ), ddy = fmax( 0.0, fmax( by0, -( by0 + P.gh[ 1 ] ) ) );
-                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 && ddx * ddx + ddy * ddy < rb * rb ) {
-                            int2 rg = P.cell_range[ ( size_t ) y * g0 + x ];
-                            beg = rg.x;
-                            cnt = rg.y - rg.x;
+                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
+                            const size_t gc = ( size_t ) y * g0 + x;
+                            if ( may_cut( cells_dist2( P, x, x, y, y, px, py ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2, wi ) ) {
+                                int2 rg = P.cell_range[ gc ];
+                                beg = rg.x;
+                                cnt = rg.y - rg.x;
+                            }
                         }
                     }
-                    int inc = cnt;
-#pragma unroll
-                    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL, inc, o ); if ( lane >= o ) inc += t; }
-                    const int total = __shfl_sync( FULL, inc, 31 );
-                    const int exc = inc - cnt;
-                    for ( int t0 = 0; t0 < total && C.m > 0 && ! overflow; t0 += 32 ) {
-                        const int t = t0 + lane;
-                        int owner = 0;
-#pragma unroll
-                        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
-                        owner = owner > 31 ? 31 : owner;
-                        int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
-                        int j = obeg + ( t - oexc );
-                        bool valid = t < total && j != s;
-                        double qx = 0, qy = 0, off = 0;
-                        if ( valid ) {
-                            qx = P.pos[ 2 * ( size_t ) j ] - px;
-                            qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
-                            double qw = P.w ? P.w[ j ] : 0.0;
-                            off = 0.5 * ( qx * qx + qy * qy + wi - qw );
-                        }
-                        // the parallel pre-test: does candidate `lane` cut the current polygon at all?
-                        bool cuts = false;
-                        for ( int k = 0; k < C.m; ++k ) {
-                            double X = __shfl_sync( FULL, C.vx, k ), Y = __shfl_sync( FULL, C.vy, k );
-                            cuts |= qx * X + qy * Y > off;
-                        }
-                        unsigned todo = __ballot_sync( FULL, valid && cuts );
-                        while ( todo ) {
-                            int k = __ffs( todo ) - 1;
-                            todo &= todo - 1;
-                            double nx = __shfl_sync( FULL, qx, k ), ny = __shfl_sync( FULL, qy, k ), no = __shfl_sync( FULL, off, k );
-                            int nid = __shfl_sync( FULL, j, k );
-                            if ( ! wclip( C, lane, nx, ny, no, nid ) ) { overflow = true; break; }
-                            if ( C.m == 0 ) break;
-                        }
-                    }
+                    cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
                 }
                 if ( C.m == 0 || overflow ) break;
                 R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
-                ex = R2 + wmax - wi;
+                double ex = R2 + wmax - wi;
                 if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+                if ( P.wpyr && r >= RINGS_FIRST && r < rmax ) { rd = r; break; }
             }
+            if ( rd >= 0 && C.m > 0 && ! overflow )
+                walk_pyramid2(
+                    P, lane, px, py, wi, cx, cy, rd, sh_stk[ warp ],
+                    [&]( int beg, int cnt ) {
+                        cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
+                        return C.m > 0 && ! overflow;
+                    },
+                    [&]() { return warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 ); },
+                    [&]( const double *lo, const double *hi, const double *a, double b ) {
+                        bool may = false;
+                        if ( lane < C.m ) {
+                            const double X[ 2 ] = { px + C.vx, py + C.vy }, v[ 2 ] = { C.vx, C.vy };
+                            may = wmaj_claims( a, b, lo, hi, X, v, 2, wi );
+                        }
+                        return __any_sync( FULL, may ) != 0;
+                    } );
             const int user = P.user[ s ];
             if ( overflow ) {
                 // past the 32 vertices a warp holds: the global-memory pass rebuilds it (report included)
@@ -703,6 +817,7 @@ __device__ int big_clip( BigPoly &S, BigPoly &D, int m, int lane, double nx, dou
 __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict__ probs, const OvfList *__restrict__ ovf, int count,
                                                         unsigned flags, ErrRec *err, char *scratch ) {
     const int lane = threadIdx.x;
+    __shared__ int2 stk[ WALK_STACK ];
     const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     char *mine = scratch + size_t( blockIdx.x ) * 2 * VBIG * ( 5 * 8 + 4 + 1 );
     for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
@@ -731,35 +846,59 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
         cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
         cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
         const int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
-        for ( int r = 0; r <= rmax && m > 0 && ! overflow; ++r ) {
+        // the seeds of a range, clipped one by one
+        auto cut_range = [&]( int b, int e ) {
+            for ( int j = b; j < e && m > 0 && ! overflow; ++j ) {
+                if ( j == s ) continue;
+                double qx = P.pos[ 2 * ( size_t ) j ] - px, qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
+                double qw = P.w ? P.w[ j ] : 0.0;
+                double off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+                bool moved;
+                int nm = big_clip( *S, *D, m, lane, qx, qy, off, j, moved );
+                if ( nm < 0 ) { overflow = true; break; }
+                if ( moved ) { BigPoly *t = S; S = D; D = t; }
+                m = nm;
+            }
+        };
+        // the ranges held by the lanes (a leaf of the pyramid walk), lane by lane
+        auto cut_lanes = [&]( int beg, int cnt ) {
+            for ( int k = 0; k < 32 && m > 0 && ! overflow; ++k ) {
+                int b = __shfl_sync( FULL, beg, k ), c = __shfl_sync( FULL, cnt, k );
+                cut_range( b, b + c );
+            }
+            return m > 0 && ! overflow;
+        };
+        auto radius2 = [&]() {
             double R2 = 0;
             for ( int k = lane; k < m; k += 32 ) R2 = fmax( R2, S->x[ k ] * S->x[ k ] + S->y[ k ] * S->y[ k ] );
-            R2 = warp_max( R2 );
+            return warp_max( R2 );
+        };
+        int rd = -1;
+        for ( int r = 0; r <= rmax && m > 0 && ! overflow; ++r ) {
+            const double R2 = radius2();
             double ex = R2 + wmax - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
             if ( r > 0 && ( r - 1 ) * P.ghmin >= rb ) break;
+            if ( P.wpyr && r > RINGS_FIRST ) { rd = r - 1; break; }
             const int ncell = r == 0 ? 1 : 8 * r;
             for ( int ci = 0; ci < ncell && m > 0 && ! overflow; ++ci ) {
                 int dx, dy;
                 ring_offset( r, ci, dx, dy );
                 int x = cx + dx, y = cy + dy;
                 if ( x < 0 || x >= g0 || y < 0 || y >= g1 ) continue;
-                double bx0 = P.go[ 0 ] + x * P.gh[ 0 ] - px, by0 = P.go[ 1 ] + y * P.gh[ 1 ] - py;
-                double ddx = fmax( 0.0, fmax( bx0, -( bx0 + P.gh[ 0 ] ) ) ), ddy = fmax( 0.0, fmax( by0, -( by0 + P.gh[ 1 ] ) ) );
-                if ( ddx * ddx + ddy * ddy >= rb * rb ) continue;
+                if ( ! may_cut( cells_dist2( P, x, x, y, y, px, py ), P.wpyr ? wmaj_b( P, ( size_t ) y * g0 + x ) : wmax, R2, wi ) ) continue;
                 int2 rg = P.cell_range[ ( size_t ) y * g0 + x ];
-                for ( int j = rg.x; j < rg.y && m > 0 && ! overflow; ++j ) {
-                    if ( j == s ) continue;
-                    double qx = P.pos[ 2 * ( size_t ) j ] - px, qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
-                    double qw = P.w ? P.w[ j ] : 0.0;
-                    double off = 0.5 * ( qx * qx + qy * qy + wi - qw );
-                    bool moved;
-                    int nm = big_clip( *S, *D, m, lane, qx, qy, off, j, moved );
-                    if ( nm < 0 ) { overflow = true; break; }
-                    if ( moved ) { BigPoly *t = S; S = D; D = t; }
-                    m = nm;
-                }
+                cut_range( rg.x, rg.y );
             }
         }
+        auto claims = [&]( const double *lo, const double *hi, const double *a, double b ) {
+            bool may = false;
+            for ( int k = lane; k < m && ! may; k += 32 ) {
+                const double X[ 2 ] = { px + S->x[ k ], py + S->y[ k ] }, v[ 2 ] = { S->x[ k ], S->y[ k ] };
+                may = wmaj_claims( a, b, lo, hi, X, v, 2, wi );
+            }
+            return __any_sync( FULL, may ) != 0;
+        };
+        if ( rd >= 0 && m > 0 && ! overflow ) walk_pyramid2( P, lane, px, py, wi, cx, cy, rd, stk, cut_lanes, radius2, claims );
         const int user = P.user[ s ];
         if ( overflow ) {
             if ( lane == 0 ) record_error( err, 4, item.prob, user, VBIG );

@@ -191,6 +191,163 @@ __device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, dou
     return true;
 }
 
+// ---- the neighbour search ---------------------------------------------------------------------------------------------
+// may a seed of weight at most W, at least sqrt( d2 ) away, cut a cell of squared radius R2 around a seed of weight wi?
+// (its bisector reaches the cell's ball only if |q| < R + sqrt( R^2 + wj - wi ); W < -1e299: empty)
+__device__ __forceinline__ bool may_cut3( double d2, double W, double R2, double wi ) {
+    if ( W < -1e299 ) return false;
+    double ex = R2 + W - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
+    return d2 < rb * rb;
+}
+// squared distance from p to the grid cells [ a0, a1 ] (inclusive, per axis)
+__device__ __forceinline__ double cells_dist2_3( const ProbDev &P, const int *a0, const int *a1, double px, double py, double pz ) {
+    const double p[ 3 ] = { px, py, pz };
+    double d2 = 0;
+    for ( int a = 0; a < 3; ++a ) {
+        double lo = P.go[ a ] + a0[ a ] * P.gh[ a ], hi = P.go[ a ] + ( a1[ a ] + 1 ) * P.gh[ a ];
+        double d = fmax( 0.0, fmax( lo - p[ a ], p[ a ] - hi ) );
+        d2 += d * d;
+    }
+    return d2;
+}
+__device__ __forceinline__ double radius2_3( const Cell3 &C, int lane ) {
+    double R2 = 0;
+    for ( int k = lane; k < C.nv; k += 32 ) R2 = fmax( R2, C.vx[ k ] * C.vx[ k ] + C.vy[ k ] * C.vy[ k ] + C.vz[ k ] * C.vz[ k ] );
+    return warp_max( R2 );
+}
+
+// the seeds of up to 32 grid cells (lane k: the range [ beg, beg + cnt ) of one cell) as candidates, 32 at a time:
+// each lane pre-tests one candidate against every vertex, then the cuts run in lane order
+__device__ void cut_by_ranges3( Cell3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, int beg, int cnt,
+                                bool &overflow ) {
+    int inc = cnt;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL3, inc, o ); if ( lane >= o ) inc += t; }
+    const int total = __shfl_sync( FULL3, inc, 31 );
+    const int exc = inc - cnt;
+    for ( int t0 = 0; t0 < total && C.nv > 0 && ! overflow; t0 += 32 ) {
+        const int t = t0 + lane;
+        int owner = 0;
+#pragma unroll
+        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL3, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
+        owner = owner > 31 ? 31 : owner;
+        int obeg = __shfl_sync( FULL3, beg, owner ), oexc = __shfl_sync( FULL3, exc, owner );
+        int j = obeg + ( t - oexc );
+        bool valid = t < total && j != s;
+        double qx = 0, qy = 0, qz = 0, off = 0;
+        if ( valid ) {
+            qx = P.pos[ 3 * ( size_t ) j ] - px;
+            qy = P.pos[ 3 * ( size_t ) j + 1 ] - py;
+            qz = P.pos[ 3 * ( size_t ) j + 2 ] - pz;
+            double qw = P.w ? P.w[ j ] : 0.0;
+            off = 0.5 * ( qx * qx + qy * qy + qz * qz + wi - qw );
+        }
+        bool cuts = false;
+        for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] > off;
+        unsigned todo = __ballot_sync( FULL3, valid && cuts );
+        while ( todo ) {
+            int k = __ffs( todo ) - 1;
+            todo &= todo - 1;
+            double nx = __shfl_sync( FULL3, qx, k ), ny = __shfl_sync( FULL3, qy, k ), nz = __shfl_sync( FULL3, qz, k );
+            double no = __shfl_sync( FULL3, off, k );
+            int nid = __shfl_sync( FULL3, j, k );
+            if ( ! wclip3( C, lane, nx, ny, nz, no, nid ) ) { overflow = true; break; }
+            if ( C.nv == 0 ) break;
+        }
+    }
+}
+
+constexpr int WALK_STACK3 = 96;      // at most 7 entries per level stay on the stack (12 levels)
+constexpr int SHELLS_FIRST = 2;      // shells walked before the pyramid takes over
+constexpr int WALK_LEAF3 = 1;        // the walk's leaves: blocks of 2 x 2 x 2 grid cells, one cell per lane
+
+// the pyramid of weight majorants, depth first, nearest child first, skipping the cells within Chebyshev distance rd of
+// c0 (the shells already walked) and the blocks that claim no vertex of the cell (wmaj_claims); a leaf block has
+// one cell per lane, each tested by `may_cut3`, clipped together
+__device__ void walk_pyramid3( Cell3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, const int *c0, int rd,
+                               int2 *stk, bool &overflow ) {
+    const int *g = P.g;
+    if ( lane == 0 ) stk[ 0 ] = make_int2( ( P.nlev - 1 ) << 22, 0 );
+    int sp = 1;
+    __syncwarp();
+    double R2 = radius2_3( C, lane );
+    for ( int guard = 0; sp > 0 && guard < ( 1 << 24 ); ++guard ) {
+        const int2 e = stk[ sp - 1 ];
+        --sp;
+        __syncwarp();
+        const int l = e.x >> 22, X[ 3 ] = { ( e.x >> 11 ) & 0x7ff, e.x & 0x7ff, e.y };
+        int a0[ 3 ], a1[ 3 ];
+        bool inside = true;
+        for ( int a = 0; a < 3; ++a ) {
+            a0[ a ] = X[ a ] << l;
+            a1[ a ] = min( ( X[ a ] + 1 ) << l, g[ a ] ) - 1;
+            inside = inside && a0[ a ] >= c0[ a ] - rd && a1[ a ] <= c0[ a ] + rd;
+        }
+        if ( inside ) continue;
+        const size_t rec = P.poff[ l ] + ( ( size_t ) X[ 2 ] * lev_dim( g[ 1 ], l ) + X[ 1 ] ) * lev_dim( g[ 0 ], l ) + X[ 0 ];
+        const double b = wmaj_b( P, rec );
+        if ( b < -1e299 ) continue;
+        {
+            // does the block claim a vertex of the cell?
+            double lo[ 3 ], hi[ 3 ];
+            for ( int q = 0; q < 3; ++q ) { lo[ q ] = P.go[ q ] + a0[ q ] * P.gh[ q ]; hi[ q ] = P.go[ q ] + ( a1[ q ] + 1 ) * P.gh[ q ]; }
+            const double *am = P.wpyr + rec * 4;
+            bool may = false;
+            for ( int k = lane; k < C.nv && ! may; k += 32 ) {
+                const double v[ 3 ] = { C.vx[ k ], C.vy[ k ], C.vz[ k ] }, Xp[ 3 ] = { px + v[ 0 ], py + v[ 1 ], pz + v[ 2 ] };
+                may = wmaj_claims( am, b, lo, hi, Xp, v, 3, wi );
+            }
+            if ( ! __any_sync( FULL3, may ) ) continue;
+        }
+        if ( l <= WALK_LEAF3 ) {
+            const int bw[ 3 ] = { a1[ 0 ] - a0[ 0 ] + 1, a1[ 1 ] - a0[ 1 ] + 1, a1[ 2 ] - a0[ 2 ] + 1 };   // at most 2 x 2 x 2
+            int beg = 0, cnt = 0;
+            if ( lane < bw[ 0 ] * bw[ 1 ] * bw[ 2 ] ) {
+                int x[ 3 ] = { a0[ 0 ] + lane % bw[ 0 ], a0[ 1 ] + ( lane / bw[ 0 ] ) % bw[ 1 ], a0[ 2 ] + lane / ( bw[ 0 ] * bw[ 1 ] ) };
+                bool walked = true;
+                for ( int a = 0; a < 3; ++a ) walked = walked && x[ a ] >= c0[ a ] - rd && x[ a ] <= c0[ a ] + rd;
+                const size_t gc = ( ( size_t ) x[ 2 ] * g[ 1 ] + x[ 1 ] ) * g[ 0 ] + x[ 0 ];
+                if ( ! walked && may_cut3( cells_dist2_3( P, x, x, px, py, pz ), wmaj_b( P, gc ), R2, wi ) ) {
+                    int2 rg = P.cell_range[ gc ];
+                    beg = rg.x;
+                    cnt = rg.y - rg.x;
+                }
+            }
+            cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
+            if ( overflow || C.nv == 0 ) return;
+            R2 = radius2_3( C, lane );
+            continue;
+        }
+        // the (up to 8) children, sorted farthest first so that the nearest is popped first
+        int d1[ 3 ];
+        for ( int a = 0; a < 3; ++a ) d1[ a ] = lev_dim( g[ a ], l - 1 );
+        double cd[ 8 ];
+        int2 ce[ 8 ];
+        int nc = 0;
+        for ( int k = 0; k < 8; ++k ) {
+            int Y[ 3 ], b0[ 3 ], b1[ 3 ];
+            bool ok = true;
+            for ( int a = 0; a < 3; ++a ) {
+                Y[ a ] = 2 * X[ a ] + ( ( k >> a ) & 1 );
+                ok = ok && Y[ a ] < d1[ a ];
+                b0[ a ] = Y[ a ] << ( l - 1 );
+                b1[ a ] = min( ( Y[ a ] + 1 ) << ( l - 1 ), g[ a ] ) - 1;
+            }
+            if ( ! ok ) continue;
+            double d = cells_dist2_3( P, b0, b1, px, py, pz );
+            int q = nc++;
+            while ( q > 0 && cd[ q - 1 ] < d ) { cd[ q ] = cd[ q - 1 ]; ce[ q ] = ce[ q - 1 ]; --q; }
+            cd[ q ] = d;
+            ce[ q ] = make_int2( ( ( l - 1 ) << 22 ) | ( Y[ 0 ] << 11 ) | Y[ 1 ], Y[ 2 ] );
+        }
+        if ( sp + nc > WALK_STACK3 ) return;               // cannot happen below 2^13 cells per side
+        if ( lane == 0 )
+            for ( int k = 0; k < nc; ++k ) stk[ sp + k ] = ce[ k ];
+        sp += nc;
+        __syncwarp();
+    }
+}
+
 // ---- sums of isotropic gaussians over the polyhedron ------------------------------------------------------------------
 // rho_g = m / ((2 pi)^{3/2} s^3) exp(-|y - c|^2 / 2 s^2).  Everything reduces to integrals over the faces:
 //  * mass (Gauss's theorem with the radial field G(r)/(4 pi r^2), G the gaussian's mass within radius r, minus the
@@ -367,6 +524,7 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cell3 &C = reinterpret_cast<Cell3 *>( smem )[ warp ];
     __shared__ double sh_rep[ W3 ][ NB_REPORT ];
+    __shared__ int2 sh_stk[ W3 ][ WALK_STACK3 ];
     __shared__ int sh_last;
     const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     for ( int cidx = blockIdx.x; cidx < nchunks; cidx += gridDim.x ) {
@@ -389,63 +547,34 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
             }
             int rmax = 0;
             for ( int a = 0; a < 3; ++a ) rmax = max( rmax, max( c0[ a ], P.g[ a ] - 1 - c0[ a ] ) );
+            int rd = -1;                 // the shells walked, when the pyramid takes over
             for ( int r = 0; r <= rmax && C.nv > 0 && ! overflow; ++r ) {
                 const int side = 2 * r + 1, ncube = side * side * side;
+                const double R2s = radius2_3( C, lane );
                 for ( int cb = 0; cb < ncube && C.nv > 0 && ! overflow; cb += 32 ) {
                     int ci = cb + lane, beg = 0, cnt = 0;
                     if ( ci < ncube ) {
                         int dx = ci % side - r, dy = ( ci / side ) % side - r, dz = ci / ( side * side ) - r;
                         bool shell = max( abs( dx ), max( abs( dy ), abs( dz ) ) ) == r;
-                        int x = c0[ 0 ] + dx, y = c0[ 1 ] + dy, z = c0[ 2 ] + dz;
-                        if ( shell && x >= 0 && x < P.g[ 0 ] && y >= 0 && y < P.g[ 1 ] && z >= 0 && z < P.g[ 2 ] ) {
-                            int2 rg = P.cell_range[ ( ( size_t ) z * P.g[ 1 ] + y ) * P.g[ 0 ] + x ];
-                            beg = rg.x;
-                            cnt = rg.y - rg.x;
+                        int x[ 3 ] = { c0[ 0 ] + dx, c0[ 1 ] + dy, c0[ 2 ] + dz };
+                        if ( shell && x[ 0 ] >= 0 && x[ 0 ] < P.g[ 0 ] && x[ 1 ] >= 0 && x[ 1 ] < P.g[ 1 ] && x[ 2 ] >= 0 && x[ 2 ] < P.g[ 2 ] ) {
+                            const size_t gc = ( ( size_t ) x[ 2 ] * P.g[ 1 ] + x[ 1 ] ) * P.g[ 0 ] + x[ 0 ];
+                            if ( may_cut3( cells_dist2_3( P, x, x, px, py, pz ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2s, wi ) ) {
+                                int2 rg = P.cell_range[ gc ];
+                                beg = rg.x;
+                                cnt = rg.y - rg.x;
+                            }
                         }
                     }
-                    int inc = cnt;
-#pragma unroll
-                    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL3, inc, o ); if ( lane >= o ) inc += t; }
-                    const int total = __shfl_sync( FULL3, inc, 31 );
-                    const int exc = inc - cnt;
-                    for ( int t0 = 0; t0 < total && C.nv > 0 && ! overflow; t0 += 32 ) {
-                        const int t = t0 + lane;
-                        int owner = 0;
-#pragma unroll
-                        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL3, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
-                        owner = owner > 31 ? 31 : owner;
-                        int obeg = __shfl_sync( FULL3, beg, owner ), oexc = __shfl_sync( FULL3, exc, owner );
-                        int j = obeg + ( t - oexc );
-                        bool valid = t < total && j != s;
-                        double qx = 0, qy = 0, qz = 0, off = 0;
-                        if ( valid ) {
-                            qx = P.pos[ 3 * ( size_t ) j ] - px;
-                            qy = P.pos[ 3 * ( size_t ) j + 1 ] - py;
-                            qz = P.pos[ 3 * ( size_t ) j + 2 ] - pz;
-                            double qw = P.w ? P.w[ j ] : 0.0;
-                            off = 0.5 * ( qx * qx + qy * qy + qz * qz + wi - qw );
-                        }
-                        bool cuts = false;
-                        for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] > off;
-                        unsigned todo = __ballot_sync( FULL3, valid && cuts );
-                        while ( todo ) {
-                            int k = __ffs( todo ) - 1;
-                            todo &= todo - 1;
-                            double nx = __shfl_sync( FULL3, qx, k ), ny = __shfl_sync( FULL3, qy, k ), nz = __shfl_sync( FULL3, qz, k );
-                            double no = __shfl_sync( FULL3, off, k );
-                            int nid = __shfl_sync( FULL3, j, k );
-                            if ( ! wclip3( C, lane, nx, ny, nz, no, nid ) ) { overflow = true; break; }
-                            if ( C.nv == 0 ) break;
-                        }
-                    }
+                    cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
                 }
                 if ( C.nv == 0 || overflow ) break;
-                double R2 = 0;
-                for ( int k = lane; k < C.nv; k += 32 ) R2 = fmax( R2, C.vx[ k ] * C.vx[ k ] + C.vy[ k ] * C.vy[ k ] + C.vz[ k ] * C.vz[ k ] );
-                R2 = warp_max( R2 );
+                double R2 = radius2_3( C, lane );
                 double ex = R2 + wmax - wi;
                 if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+                if ( P.wpyr && r >= SHELLS_FIRST && r < rmax ) { rd = r; break; }
             }
+            if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, sh_stk[ warp ], overflow );
             const int user = P.user[ s ];
             if ( overflow ) {
                 if ( lane == 0 ) record_error3( err, 4, ch.prob, user, VC );

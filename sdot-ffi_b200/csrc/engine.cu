@@ -239,6 +239,10 @@ void Geometry::fill( ProbDev &P ) const {
     P.dval = dval;
     P.dpre = dpre;
     P.cap = dim == 2 ? CAP2 : CAP3;
+    P.wpyr = wpyr;
+    P.wmom = wmom;
+    P.nlev = nlev;
+    for ( int l = 0; l < MAX_LEV; ++l ) P.poff[ l ] = poff[ l ];
 }
 
 void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positions, const double box_lo[ 3 ], const double box_hi[ 3 ],
@@ -313,13 +317,17 @@ void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positio
         }
     }
     dbytes = size_t( nval + npre ) * 8 + 1024;
-    size_t bytes = size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( G.ncell ) * 8 + dbytes + 8 * 256;
+    const long npyr = wpyr_layout( dim, G.g, G.nlev, G.poff );
+    size_t bytes = size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( G.ncell ) * 8 + size_t( npyr ) * 8 * ( dim + 1 + wmom_size( dim ) ) + dbytes +
+                   10 * 256;
     G.mem = ( char * ) dalloc( c, bytes );
     Arena A{ G.mem, bytes, 0 };
     G.pos = A.take<double>( size_t( n ) * dim );
     G.user = A.take<int>( n );
     G.rank_of = A.take<int>( n );
     G.cell_range = A.take<int2>( G.ncell );
+    G.wpyr = A.take<double>( size_t( npyr ) * ( dim + 1 ) );
+    G.wmom = A.take<double>( size_t( npyr ) * wmom_size( dim ) );
     if ( nval ) G.dval = A.take<double>( nval );
     if ( npre ) G.dpre = A.take<double>( npre );
     // the sort, in a temporary allocation
@@ -431,6 +439,7 @@ size_t job_bytes( int dim, long n, int dkind, long dcount ) {
                size_t( n ) * 4 + size_t( nch ) * NB_REPORT * 8 + size_t( nv ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) + 40 * 256;
     // geometry: ranked positions, user, rank_of, the grid (about n / 2 cells), the density, and the sort's scratch
     b += size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( n ) * 4 + 1024;
+    b += size_t( n ) * ( dim == 2 ? 64 : 84 ) + 1024;    // the weight majorants and their moments (4/3, 8/7 of the grid's cells)
     b += dkind == D_IMAGE ? size_t( dcount ) * 16 : size_t( dcount ) * 8 * ( dim + 2 );
     b += size_t( n ) * ( 24 + dim * 8 ) + 4096;
     return b + mg_bytes( dim, n, cap );
@@ -1179,6 +1188,11 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         if ( b3 ) std::memcpy( buf.data() + o3, CB.data(), b3 );
         char *d = upload_desc( c, buf.data(), buf.size() );
         ProbDev *dp = reinterpret_cast<ProbDev *>( d );
+        if ( ! report_only ) {
+            c.timer.begin( c.stream, K_INDEX, double( PX.size() ) );
+            launch_wpyr( L, dp, int( PX.size() ) );
+            c.timer.end( c.stream );
+        }
         for ( int pass = 0; pass < 2; ++pass ) {
             std::vector<Chunk> &CX = pass ? CB : CA;
             if ( CX.empty() ) continue;

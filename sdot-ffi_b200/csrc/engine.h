@@ -73,6 +73,10 @@ struct Geometry {
     double *pos = nullptr;            // ranked
     int *user = nullptr, *rank_of = nullptr;
     int2 *cell_range = nullptr;
+    double *wpyr = nullptr;           // the weight majorants (rebuilt before each diagram) and their moments
+    double *wmom = nullptr;
+    int nlev = 0;
+    int poff[ MAX_LEV ] = {};
     int dkind = D_UNIFORM;
     double rho = 1;
     double *dval = nullptr, *dpre = nullptr;

@@ -1,8 +1,7 @@
 // The acceleration structure, built on the device: a uniform grid whose cells are ranked in Morton
 // order.  It plays the role of the reference's median-cut BSP (src/sdot/AaBsp.py:16-100,
 // gpu/Bsp2D.cuh:366-456): consecutive ranks are neighbours in space, and every seed is found by the
-// cell it falls in.  Unlike a tree it has no per-node majorants: the neighbour search is bounded by a
-// security radius on the largest weight instead (cells*.cu).
+// cell it falls in.  Its weight majorants are a pyramid of maxima over the grid (below).
 #include "internal.h"
 #include <cub/device/device_radix_sort.cuh>
 
@@ -172,6 +171,180 @@ __global__ void k_finish_wmax( unsigned long long *slot, double *wmax, int count
 void launch_finish_wmax( const Launch &L, unsigned long long *slot, double *wmax, int count ) {
     k_finish_wmax<<<( count + 127 ) / 128, 128, 0, L.stream>>>( slot, wmax, count );
     ++*L.launches;
+}
+
+// ---- weight majorants ------------------------------------------------------------------------------------------------
+// Every grid cell, then every 2x2 (2x2x2) block of the level below up to a single block, gets an affine majorant of the
+// weights of its seeds: w_j <= a . p_j + b.  a is the least-squares slope of the block's weights (0 on the grid's own
+// cells, which hold two seeds or so), b the exact max of w_j - a . p_j; correctness needs only b, the slope only
+// sharpens the pruning.  The cell kernels skip a block that cannot claim any vertex of the current cell (wmaj_may_cut):
+// the per-node affine majorants of the reference's tree (gpu/Majorant2D.cuh:3-28, 253; Pruning.h:1-30) on the grid's
+// pyramid.  Record of a node: a[ dim ], then b as an ordered integer (-1e300: no seed).
+long wpyr_layout( int dim, const int *g, int &nlev, int *poff ) {
+    long total = 0;
+    nlev = 0;
+    for ( int l = 0; l < MAX_LEV; ++l ) {
+        long sz = 1;
+        bool one = true;
+        for ( int a = 0; a < dim; ++a ) { int d = lev_dim( g[ a ], l ); sz *= d; one = one && d == 1; }
+        poff[ l ] = int( total );
+        total += sz;
+        nlev = l + 1;
+        if ( one ) break;
+    }
+    return total;
+}
+
+// level 0: the moments of each cell's seeds (n, sum p, sum w, sum p p^T (upper), sum p w) and its record (a = 0, b = max w)
+__global__ void k_wpyr0( const ProbDev *__restrict__ probs ) {
+    const ProbDev &P = probs[ blockIdx.y ];
+    if ( ! P.wpyr ) return;
+    const int dim = P.dim, RS = dim + 1, MS = wmom_size( dim );
+    long ncell = 1;
+    for ( int a = 0; a < dim; ++a ) ncell *= P.g[ a ];
+    for ( long c = long( blockIdx.x ) * blockDim.x + threadIdx.x; c < ncell; c += long( gridDim.x ) * blockDim.x ) {
+        int2 rg = P.cell_range[ c ];
+        double m = -1e300, mom[ 14 ];
+        for ( int k = 0; k < MS; ++k ) mom[ k ] = 0;
+        for ( int j = rg.x; j < rg.y; ++j ) {
+            const double w = P.w ? P.w[ j ] : 0.0;
+            m = fmax( m, w );
+            double x[ 3 ];
+            for ( int a = 0; a < dim; ++a ) x[ a ] = P.pos[ ( size_t ) j * dim + a ];
+            int k = 0;
+            mom[ k++ ] += 1;
+            for ( int a = 0; a < dim; ++a ) mom[ k++ ] += x[ a ];
+            mom[ k++ ] += w;
+            for ( int a = 0; a < dim; ++a )
+                for ( int b = a; b < dim; ++b ) mom[ k++ ] += x[ a ] * x[ b ];
+            for ( int a = 0; a < dim; ++a ) mom[ k++ ] += x[ a ] * w;
+        }
+        for ( int k = 0; k < MS; ++k ) P.wmom[ c * MS + k ] = mom[ k ];
+        for ( int a = 0; a < dim; ++a ) P.wpyr[ c * RS + a ] = 0;
+        reinterpret_cast<unsigned long long *>( P.wpyr )[ c * RS + dim ] = dbl_order( m );
+    }
+}
+
+// the least-squares slope of the weights from a node's moments (0 when too few or degenerate seeds)
+__device__ void fit_slope( const double *mom, int dim, double *a ) {
+    for ( int q = 0; q < dim; ++q ) a[ q ] = 0;
+    const double n = mom[ 0 ];
+    if ( n < dim + 1 ) return;
+    double mean[ 3 ], C[ 3 ][ 3 ], r[ 3 ];
+    for ( int q = 0; q < dim; ++q ) mean[ q ] = mom[ 1 + q ] / n;
+    const double mw = mom[ 1 + dim ] / n;
+    int k = 2 + dim;
+    for ( int q = 0; q < dim; ++q )
+        for ( int t = q; t < dim; ++t ) { C[ q ][ t ] = C[ t ][ q ] = mom[ k++ ] / n - mean[ q ] * mean[ t ]; }
+    for ( int q = 0; q < dim; ++q ) r[ q ] = mom[ k++ ] / n - mean[ q ] * mw;
+    double tr = 0;
+    for ( int q = 0; q < dim; ++q ) tr += C[ q ][ q ];
+    if ( ! ( tr > 0 ) ) return;
+    if ( dim == 2 ) {
+        double det = C[ 0 ][ 0 ] * C[ 1 ][ 1 ] - C[ 0 ][ 1 ] * C[ 0 ][ 1 ];
+        if ( ! ( det > 1e-6 * tr * tr ) ) return;
+        a[ 0 ] = ( r[ 0 ] * C[ 1 ][ 1 ] - r[ 1 ] * C[ 0 ][ 1 ] ) / det;
+        a[ 1 ] = ( r[ 1 ] * C[ 0 ][ 0 ] - r[ 0 ] * C[ 0 ][ 1 ] ) / det;
+    } else {
+        double c00 = C[ 1 ][ 1 ] * C[ 2 ][ 2 ] - C[ 1 ][ 2 ] * C[ 2 ][ 1 ], c01 = C[ 1 ][ 2 ] * C[ 2 ][ 0 ] - C[ 1 ][ 0 ] * C[ 2 ][ 2 ],
+               c02 = C[ 1 ][ 0 ] * C[ 2 ][ 1 ] - C[ 1 ][ 1 ] * C[ 2 ][ 0 ];
+        double det = C[ 0 ][ 0 ] * c00 + C[ 0 ][ 1 ] * c01 + C[ 0 ][ 2 ] * c02;
+        if ( ! ( det > 1e-9 * tr * tr * tr ) ) return;
+        for ( int q = 0; q < 3; ++q ) {
+            double M[ 3 ][ 3 ];
+            for ( int i = 0; i < 3; ++i )
+                for ( int j = 0; j < 3; ++j ) M[ i ][ j ] = j == q ? r[ i ] : C[ i ][ j ];
+            double d = M[ 0 ][ 0 ] * ( M[ 1 ][ 1 ] * M[ 2 ][ 2 ] - M[ 1 ][ 2 ] * M[ 2 ][ 1 ] ) - M[ 0 ][ 1 ] * ( M[ 1 ][ 0 ] * M[ 2 ][ 2 ] - M[ 1 ][ 2 ] * M[ 2 ][ 0 ] ) +
+                       M[ 0 ][ 2 ] * ( M[ 1 ][ 0 ] * M[ 2 ][ 1 ] - M[ 1 ][ 1 ] * M[ 2 ][ 0 ] );
+            a[ q ] = d / det;
+        }
+    }
+    for ( int q = 0; q < dim; ++q ) if ( ! isfinite( a[ q ] ) ) { for ( int t = 0; t < dim; ++t ) a[ t ] = 0; return; }
+}
+
+// the levels above: moments summed from the children, the slope fitted, b reset (one block per problem, level by level)
+__global__ void __launch_bounds__( 1024 ) k_wpyr_up( const ProbDev *__restrict__ probs ) {
+    const ProbDev &P = probs[ blockIdx.x ];
+    if ( ! P.wpyr ) return;
+    const int dim = P.dim, RS = dim + 1, MS = wmom_size( dim );
+    for ( int l = 1; l < P.nlev; ++l ) {
+        int d[ 3 ] = { 1, 1, 1 }, e[ 3 ] = { 1, 1, 1 };
+        for ( int a = 0; a < dim; ++a ) { d[ a ] = lev_dim( P.g[ a ], l ); e[ a ] = lev_dim( P.g[ a ], l - 1 ); }
+        const long src = P.poff[ l - 1 ], dst = P.poff[ l ];
+        const long cnt = long( d[ 0 ] ) * d[ 1 ] * d[ 2 ];
+        for ( long c = threadIdx.x; c < cnt; c += blockDim.x ) {
+            int X = int( c % d[ 0 ] ), Y = int( ( c / d[ 0 ] ) % d[ 1 ] ), Z = int( c / ( long( d[ 0 ] ) * d[ 1 ] ) );
+            double mom[ 14 ];
+            for ( int k = 0; k < MS; ++k ) mom[ k ] = 0;
+            for ( int dz = 0; dz < ( dim == 3 ? 2 : 1 ); ++dz )
+                for ( int dy = 0; dy < 2; ++dy )
+                    for ( int dx = 0; dx < 2; ++dx ) {
+                        int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+                        if ( x < e[ 0 ] && y < e[ 1 ] && z < e[ 2 ] ) {
+                            const double *cm = P.wmom + ( src + ( long( z ) * e[ 1 ] + y ) * e[ 0 ] + x ) * MS;
+                            for ( int k = 0; k < MS; ++k ) mom[ k ] += cm[ k ];
+                        }
+                    }
+            for ( int k = 0; k < MS; ++k ) P.wmom[ ( dst + c ) * MS + k ] = mom[ k ];
+            double a[ 3 ];
+            fit_slope( mom, dim, a );
+            for ( int q = 0; q < dim; ++q ) P.wpyr[ ( dst + c ) * RS + q ] = a[ q ];
+            reinterpret_cast<unsigned long long *>( P.wpyr )[ ( dst + c ) * RS + dim ] = dbl_order( -1e300 );
+        }
+        __syncthreads();
+    }
+}
+
+// b of the levels above the grid: the max of w_j - a . p_j over each node's seeds.  Seeds are in Morton order, so those
+// of one node are consecutive: a segmented max across the warp, then one atomic per segment
+__global__ void k_wpyr_b( const ProbDev *__restrict__ probs ) {
+    const ProbDev &P = probs[ blockIdx.y ];
+    if ( ! P.wpyr ) return;
+    const int dim = P.dim, RS = dim + 1, lane = threadIdx.x & 31;
+    unsigned long long *B = reinterpret_cast<unsigned long long *>( P.wpyr );
+    const long gw = ( long( blockIdx.x ) * blockDim.x + threadIdx.x ) >> 5, nw = ( long( gridDim.x ) * blockDim.x ) >> 5;
+    for ( long j0 = gw * 32; j0 < P.n; j0 += nw * 32 ) {      // 32 consecutive seeds per warp
+        const long j = j0 + lane;
+        const bool ok = j < P.n;
+        int c[ 3 ] = { 0, 0, 0 };
+        double x[ 3 ] = { 0, 0, 0 }, w = 0;
+        if ( ok ) {
+            w = P.w ? P.w[ j ] : 0.0;
+            for ( int a = 0; a < dim; ++a ) {
+                x[ a ] = P.pos[ ( size_t ) j * dim + a ];
+                int k = int( floor( ( x[ a ] - P.go[ a ] ) / P.gh[ a ] ) );
+                c[ a ] = k < 0 ? 0 : ( k >= P.g[ a ] ? P.g[ a ] - 1 : k );
+            }
+        }
+        for ( int l = 1; l < P.nlev; ++l ) {
+            long node = -1;
+            if ( ok ) {
+                long idx = 0;
+                for ( int a = dim - 1; a >= 0; --a ) idx = idx * lev_dim( P.g[ a ], l ) + ( c[ a ] >> l );
+                node = P.poff[ l ] + idx;
+            }
+            double v = -1e300;
+            if ( ok ) {
+                v = w;
+                for ( int a = 0; a < dim; ++a ) v -= P.wpyr[ node * RS + a ] * x[ a ];
+            }
+            for ( int o = 1; o < 32; o <<= 1 ) {
+                double vo = __shfl_down_sync( 0xffffffffu, v, o );
+                long no = __shfl_down_sync( 0xffffffffu, node, o );
+                if ( lane + o < 32 && no == node ) v = fmax( v, vo );
+            }
+            long prev = __shfl_up_sync( 0xffffffffu, node, 1 );
+            if ( ok && ( lane == 0 || prev != node ) ) atomicMax( &B[ node * RS + dim ], dbl_order( v ) );
+        }
+    }
+}
+
+void launch_wpyr( const Launch &L, const ProbDev *probs, int nprob ) {
+    if ( nprob <= 0 ) return;
+    k_wpyr0<<<dim3( 64, nprob ), 256, 0, L.stream>>>( probs );
+    k_wpyr_up<<<nprob, 1024, 0, L.stream>>>( probs );
+    k_wpyr_b<<<dim3( 64, nprob ), 256, 0, L.stream>>>( probs );
+    *L.launches += 3;
 }
 
 } // namespace sdot

@@ -39,6 +39,11 @@ enum DiagFlags : unsigned {
     F_FP32 = 128u           // FP32 clipping with FP64 re-check
 };
 
+constexpr int MAX_LEV = 24;      // levels of the weight majorants (grids up to 2^23 cells per side)
+__host__ __device__ inline int lev_dim( int g, int l ) { return ( g + ( 1 << l ) - 1 ) >> l; }
+// the moments of a node's seeds: n, sum p, sum w, sum p p^T (upper triangle), sum p w
+__host__ __device__ inline int wmom_size( int dim ) { return dim == 2 ? 9 : 14; }
+
 struct ProbDev {
     int dim, dkind, cap, n;
     double lo[3], hi[3];
@@ -79,6 +84,13 @@ struct ProbDev {
     int ovf_cap;
     int *ovf_ids;
     double *ovf_c;
+    // weight majorants w_j <= a . p_j + b of the seeds of each grid cell (level 0), then of each 2^l block of cells
+    // (level l, dims lev_dim( g, l )), up to one block: records [ a[ dim ], b as an ordered integer ] at
+    // wpyr + ( dim + 1 ) ( poff[ l ] + node ); b = -1e300: no seed.  NULL: the global max bounds the search
+    double *wpyr;
+    double *wmom;                 // [ nodes, wmom_size( dim ) ] the moments the slopes are fitted from
+    int nlev;
+    int poff[ MAX_LEV ];
 };
 
 // cells the warp-register kernel could not hold (more than 32 vertices, or more facets than the table's row):
@@ -191,6 +203,28 @@ SDOT_DEV double order_dbl( unsigned long long u ) {
     return __longlong_as_double( ( u >> 63 ) ? ( u & 0x7fffffffffffffffull ) : ~u );
 }
 
+// ---- weight majorants -------------------------------------------------------------------------------------------------
+// b of majorant record `node` (the grid's own cells are nodes 0 .. ncell - 1, with a = 0: b is their max weight)
+SDOT_DEV double wmaj_b( const ProbDev &P, size_t node ) {
+    return order_dbl( reinterpret_cast<const unsigned long long *>( P.wpyr )[ node * ( P.dim + 1 ) + P.dim ] );
+}
+// may a seed of a node with majorant w <= a . q + b, q in the box [ lo, hi ], claim the point X = p_i + v of seed i's
+// cell?  Its power distance there is at least min_q |X - q|^2 - a . q - b = dist^2( X + a/2, box ) - a . X - |a|^2/4 - b,
+// against |v|^2 - w_i for seed i (with a margin of rounding)
+SDOT_DEV bool wmaj_claims( const double *a, double b, const double *lo, const double *hi, const double *X, const double *v, int dim, double wi ) {
+    double d2 = 0, aX = 0, a2 = 0, v2 = 0;
+    for ( int q = 0; q < dim; ++q ) {
+        double u = X[ q ] + 0.5 * a[ q ];
+        double d = fmax( 0.0, fmax( lo[ q ] - u, u - hi[ q ] ) );
+        d2 += d * d;
+        aX += a[ q ] * X[ q ];
+        a2 += a[ q ] * a[ q ];
+        v2 += v[ q ] * v[ q ];
+    }
+    double lhs = d2 - aX - 0.25 * a2 - b, rhs = v2 - wi;
+    return lhs < rhs + 1e-12 * ( fabs( aX ) + fabs( b ) + fabs( wi ) + v2 + d2 );
+}
+
 // ---- launchers (each in the .cu next to its kernels) --------------------------------------------------
 // CUDA-event timing per kernel class (off by default; `sdot_context_set_timing`)
 enum KClass : int { K_CELLS2D = 0, K_CELLS3D, K_LAPLACIAN, K_CG, K_VECTOR, K_INDEX, K_REPORT, NB_KCLASS };
@@ -231,6 +265,10 @@ void radix_sort( const Launch &L, void *temp, size_t temp_bytes, const unsigned 
                  int *vout, int n, int bits );
 void launch_image_prefix( const Launch &L, const double *values, int nx, int ny, double hx, double *pre );
 void launch_wmax( const Launch &L, const double *w, int n, unsigned long long *slot );
+// the levels of the weight majorants of a grid: returns the doubles they take, fills nlev and poff
+long wpyr_layout( int dim, const int *g, int &nlev, int *poff );
+// (re)builds the weight majorants of every problem of `probs` (those with wpyr) from their current weights
+void launch_wpyr( const Launch &L, const ProbDev *probs, int nprob );
 void launch_finish_wmax( const Launch &L, unsigned long long *slot, double *wmax, int count );
 
 // linalg.cu
