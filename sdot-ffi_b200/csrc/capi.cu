@@ -362,7 +362,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
     return guard( st, [&] {
         Ctx &c = ctx->c;
         CK( cudaSetDevice( c.device ) );
-        if ( method != 0 ) throw Error( SDOT_ERR_UNSUPPORTED, "linear method: only 0 (Jacobi-PCG) in this build" );
+        if ( method != 0 && method != 1 ) throw Error( SDOT_ERR_ARGS, "linear method: 0 (Jacobi-PCG) or 1 (multigrid-PCG)" );
         std::vector<int64_t> hrp;
         if ( memory == SDOT_DEVICE ) {
             hrp.resize( n + 1 );
@@ -418,6 +418,13 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             double hsc[ NB_SC ] = {};
             hsc[ SC_MEAN ] = mean;
             CK( cudaMemcpyAsync( sc, hsc, sizeof( hsc ), cudaMemcpyHostToDevice, c.stream ) );
+            if ( method == 1 ) {
+                const int its = mg_linear_solve( c, V, nnz, hsc );
+                if ( iterations ) iterations[ k ] = its;
+                CK( cudaMemcpyAsync( x + size_t( k ) * n, d, n * 8, memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.stream ) );
+                CK( cudaStreamSynchronize( c.stream ) );
+                continue;
+            }
             launch_cg_init( L, dv, dch, int( vch.size() ) );
             for ( ;; ) {
                 for ( int s = 0; s < 32; ++s ) launch_cg_iter( L, dv, dch, int( vch.size() ) );

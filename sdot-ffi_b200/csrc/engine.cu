@@ -1057,6 +1057,57 @@ struct VecBatch {
     }
 };
 
+// one Laplacian given as a device CSR (V: matrix, work vectors, scalars; b and SC_MEAN uploaded): its solve by the CG
+// preconditioned with the aggregation multigrid of the Newton engine (aggregates of 4 consecutive rows, 8 when the rows
+// hold more than 10 entries on average, as in 3D),
+// x in V.x, the gauge-fixed direction in V.d.  Returns the CG iterations, -1 if the CG failed.
+constexpr int MG_BURST_SOLVE = 8;
+int mg_linear_solve( Ctx &c, const VecDev &V0, long nnz, double *hsc ) {
+    SolveJob J;                                      // only its hierarchy is used
+    J.G.dim = nnz > 10 * long( V0.n ) ? 3 : 2;       // the aggregates of a 3D Laplacian (about 15 entries a row) pack 8 rows
+    J.G.n = V0.n;
+    J.cap = int( ( nnz + V0.n - 1 ) / V0.n ) + 1;
+    J.row_ptr = V0.row_ptr;
+    J.col = V0.col;
+    alloc_mg( c, J );
+    struct Free {
+        Ctx &c;
+        SolveJob &J;
+        ~Free() { if ( J.mg_mem ) dfree( c, J.mg_mem ); }
+    } fr{ c, J };
+    VecDev V = V0;
+    V.precond = J.mg_L > 0 ? 1 : 0;
+    VecBatch B;
+    B.add( V, &J );
+    B.upload( c );
+    Launch L = c.L();
+    const int nch = int( B.ch.size() );
+    if ( B.mg() ) {
+        B.build( L, c.derr );
+        launch_cg_init0( L, B.dv, B.dch, nch );
+        B.vcycle( L );
+        launch_cg_init1( L, B.dv, B.dch, nch );
+    } else
+        launch_cg_init( L, B.dv, B.dch, nch );
+    for ( ;; ) {
+        for ( int k = 0; k < MG_BURST_SOLVE; ++k ) {
+            if ( B.mg() ) {
+                launch_cg_spmv_update( L, B.dv, B.dch, nch );
+                B.vcycle( L );
+                launch_cg_rz_p( L, B.dv, B.dch, nch );
+            } else
+                launch_cg_iter( L, B.dv, B.dch, nch );
+        }
+        CK( cudaMemcpyAsync( hsc, V.sc, NB_SC * sizeof( double ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+        check_errors( c, "multigrid" );
+        if ( hsc[ SC_CONV ] != 0 ) break;
+    }
+    launch_gauge( L, B.dv, B.dch, nch );
+    return hsc[ SC_FAIL ] != 0 ? -1 : int( hsc[ SC_ITER ] );
+}
+
 // phase D: the vector work the decisions asked for
 static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
     Launch L = c.L();

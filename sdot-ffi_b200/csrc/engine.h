@@ -111,6 +111,8 @@ void launch_w2_backward( const Launch &L, int batch, int n, int dim, const void 
 struct Engine;
 // continuous batching: one step of every active job (used by the server)
 void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs );
+// one Laplacian (device CSR in V, b and SC_MEAN uploaded) solved by the multigrid-preconditioned CG: iterations, -1 on failure
+int mg_linear_solve( Ctx &c, const VecDev &V, long nnz, double *hsc );
 
 } // namespace sdot
 

@@ -189,6 +189,33 @@ def test_the_linear_solve_matches_a_direct_solve():
     assert np.abs(x - y).max() < 1e-8 * np.abs(y).max()
 
 
+@pytest.mark.parametrize("d,n", [(2, 40000), (3, 20000)])
+def test_both_linear_methods_match_a_direct_solve(d, n):
+    """sdot_linear_solve with method 0 (Jacobi-PCG) and 1 (multigrid-PCG, FP32 levels) on the Laplacian of a
+    diagram with random weights, against scipy's direct solve of the gauge-fixed system, two right-hand sides"""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    from sdot import _lib
+    rng = np.random.default_rng(50 + d)
+    pos = rng.uniform(size=(n, d))
+    w = rng.uniform(0, 0.3 * n ** (-2.0 / d), size=n)
+    row, cols, vals, dia = _pd(pos, w).laplacian()
+    b = rng.standard_normal((2, n))
+    b -= b.mean(axis=1, keepdims=True)
+    L = sp.diags(dia) - sp.csr_matrix((vals, cols, row), shape=(n, n))
+    lu = sla.splu(L[1:, 1:].tocsc())
+    y = np.zeros((2, n))
+    for k in range(2):
+        y[k, 1:] = lu.solve(b[k, 1:])
+    its = {}
+    for method in (0, 1):
+        x, it = _lib.linear_solve(row, cols, vals, dia, b, tol=1e-12, method=method)
+        assert (x[:, 0] == 0).all()
+        assert np.abs(x - y).max() < 1e-8 * np.abs(y).max(), method
+        its[method] = np.asarray(it)
+    assert (its[1] > 0).all() and (its[1] < its[0]).all(), its
+
+
 def test_the_adjoint_is_the_derivative_of_the_measures():
     rng = np.random.default_rng(6)
     n = 300
