@@ -414,7 +414,8 @@ __device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int l
     }
 }
 
-__device__ __forceinline__ void record_error( ErrRec *err, int code, int prob, int seed, int needed ) {
+__device__ __forceinline__ void record_error( const ProbDev &P, ErrRec *err, int code, int prob, int seed, int needed ) {
+    if ( P.perr ) *P.perr = 1.0;
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
 }
 
@@ -550,7 +551,8 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
                 R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
                 double ex = R2 + wmax - wi;
                 if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
-                if ( P.wpyr && r >= RINGS_FIRST && r < rmax ) { rd = r; break; }
+                // the pyramid once the global bound reaches well past the next rings (non-uniform weights)
+                if ( P.wpyr && r >= RINGS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
             }
             if ( rd >= 0 && C.m > 0 && ! overflow )
                 walk_pyramid2(
@@ -575,9 +577,9 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
                     if ( ovf ) {
                         int k = atomicAdd( &ovf->count, 1 );
                         if ( k < ovf->cap ) ovf->items[ k ] = OvfItem{ ch.prob, s };
-                        else record_error( err, 4, ch.prob, user, 33 );
+                        else record_error( P, err, 4, ch.prob, user, 33 );
                     } else
-                        record_error( err, 4, ch.prob, user, 33 );
+                        record_error( P, err, 4, ch.prob, user, 33 );
                 }
                 continue;
             }
@@ -606,9 +608,9 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
                     if ( ovf ) {
                         int k = atomicAdd( &ovf->count, 1 );
                         if ( k < ovf->cap ) ovf->items[ k ] = OvfItem{ ch.prob, s };
-                        else record_error( err, 4, ch.prob, user, nf );
+                        else record_error( P, err, 4, ch.prob, user, nf );
                     } else
-                        record_error( err, 4, ch.prob, user, nf );
+                        record_error( P, err, 4, ch.prob, user, nf );
                 }
                 continue;
             }
@@ -818,11 +820,13 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
                                                         unsigned flags, ErrRec *err, char *scratch ) {
     const int lane = threadIdx.x;
     __shared__ int2 stk[ WALK_STACK ];
-    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     char *mine = scratch + size_t( blockIdx.x ) * 2 * VBIG * ( 5 * 8 + 4 + 1 );
     for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
         const OvfItem item = ovf->items[ it ];
         const ProbDev &P = probs[ item.prob ];
+        // flags 0: each problem's own pass (a final-moments diagram has `first`, a Newton diagram has not)
+        const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
+        const bool moments = fl & F_MOMENTS, facets = fl & F_FACETS, user_order = fl & F_USER_ORDER;
         const int s = item.seed;
         BigPoly A = big_buffer( mine, 0 ), B = big_buffer( mine, 1 );
         BigPoly *S = &A, *D = &B;
@@ -878,7 +882,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
             const double R2 = radius2();
             double ex = R2 + wmax - wi, rb = sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 );
             if ( r > 0 && ( r - 1 ) * P.ghmin >= rb ) break;
-            if ( P.wpyr && r > RINGS_FIRST ) { rd = r - 1; break; }
+            if ( P.wpyr && r > RINGS_FIRST && rb > ( r + 1 ) * P.ghmin ) { rd = r - 1; break; }
             const int ncell = r == 0 ? 1 : 8 * r;
             for ( int ci = 0; ci < ncell && m > 0 && ! overflow; ++ci ) {
                 int dx, dy;
@@ -901,7 +905,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
         if ( rd >= 0 && m > 0 && ! overflow ) walk_pyramid2( P, lane, px, py, wi, cx, cy, rd, stk, cut_lanes, radius2, claims );
         const int user = P.user[ s ];
         if ( overflow ) {
-            if ( lane == 0 ) record_error( err, 4, item.prob, user, VBIG );
+            if ( lane == 0 ) record_error( P, err, 4, item.prob, user, VBIG );
             continue;
         }
         // integration, edges strided over the lanes
@@ -931,7 +935,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
         if ( facets ) {
             const bool to_store = nf > P.cap;
             if ( to_store && ! P.ovf_ids ) {
-                if ( lane == 0 ) record_error( err, 4, item.prob, user, nf );
+                if ( lane == 0 ) record_error( P, err, 4, item.prob, user, nf );
                 continue;
             }
             int base_at = 0;
@@ -939,7 +943,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
                 if ( lane == 0 ) base_at = atomicAdd( P.ovf_count, nf );
                 base_at = __shfl_sync( FULL, base_at, 0 );
                 if ( base_at + nf > P.ovf_cap ) {
-                    if ( lane == 0 ) record_error( err, 4, item.prob, user, nf );
+                    if ( lane == 0 ) record_error( P, err, 4, item.prob, user, nf );
                     continue;
                 }
             }
@@ -985,7 +989,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
                 }
             }
         }
-        if ( ( flags & F_VJP ) && lane == 0 ) record_error( err, 4, item.prob, user, m );
+        if ( ( fl & F_VJP ) && lane == 0 ) record_error( P, err, 4, item.prob, user, m );
         if ( lane == 0 && P.mass ) P.mass[ row ] = mass;
         __syncwarp();
     }

@@ -446,7 +446,7 @@ __device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int l
     for ( int g = 0; g < ng; ++g ) {
         const double *G = P.dval + g * 5;
         const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
-        const double s2g = sg * sg, K = mg / ( 15.749609945653303 * s2g * sg ), kr = 0.7071067811865476 / sg;   // (2 pi)^{3/2}
+        const double s2g = sg * sg, K = mg / ( 15.749609945722419 * s2g * sg ), kr = 0.7071067811865476 / sg;   // (2 pi)^{3/2}
         double Mg = 0, Gx = 0, Gy = 0, Gz = 0, Sg = 0;
         for ( int k = lane; k < nv; k += 32 ) {
             const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
@@ -503,7 +503,8 @@ __device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int l
     }
 }
 
-__device__ __forceinline__ void record_error3( ErrRec *err, int code, int prob, int seed, int needed ) {
+__device__ __forceinline__ void record_error3( const ProbDev &P, ErrRec *err, int code, int prob, int seed, int needed ) {
+    if ( P.perr ) *P.perr = 1.0;
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
 }
 
@@ -572,12 +573,12 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
                 double R2 = radius2_3( C, lane );
                 double ex = R2 + wmax - wi;
                 if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
-                if ( P.wpyr && r >= SHELLS_FIRST && r < rmax ) { rd = r; break; }
+                if ( P.wpyr && r >= SHELLS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
             }
             if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, sh_stk[ warp ], overflow );
             const int user = P.user[ s ];
             if ( overflow ) {
-                if ( lane == 0 ) record_error3( err, 4, ch.prob, user, VC );
+                if ( lane == 0 ) record_error3( P, err, 4, ch.prob, user, VC );
                 if ( lane == 0 ) C.nv = 0;
                 __syncwarp();
             }
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
                 }
                 nf = written;
                 if ( facets && nf > P.cap ) {
-                    if ( lane == 0 ) record_error3( err, 4, ch.prob, user, nf );
+                    if ( lane == 0 ) record_error3( P, err, 4, ch.prob, user, nf );
                     nf = P.cap;
                 }
                 if ( facets && lane == 0 ) P.nb[ row ] = nf;

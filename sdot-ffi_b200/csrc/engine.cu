@@ -220,6 +220,13 @@ void check_errors( Ctx &c, const char *where ) {
     throw Error( e.code, std::string( where ) + ": device error", e.seed );
 }
 
+// a capacity error of the engine's kernels belongs to its problem (the per-slot flag read in `decide`): not a batch error
+static void clear_capacity_error( Ctx &c ) {
+    if ( c.herr->code != SDOT_ERR_CAPACITY ) return;
+    *c.herr = ErrRec{};
+    CK( cudaMemsetAsync( c.derr, 0, sizeof( ErrRec ), c.stream ) );
+}
+
 // ---- geometry ----------------------------------------------------------------------------------------------------------
 void Geometry::fill( ProbDev &P ) const {
     std::memset( &P, 0, sizeof( P ) );
@@ -595,6 +602,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         alloc_job( c, *J );
         if ( int( J->opt[ SDOT_OPT_LIN_METHOD ] ) == 1 ) alloc_mg( c, *J );
         J->slot = take_slot( c );
+        CK( cudaMemsetAsync( c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR, 0, sizeof( double ), c.stream ) );
         CK( cudaMemcpyAsync( &J->rank0, J->G.rank_of, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
         Launch L = c.L();
@@ -824,6 +832,20 @@ static void accept_trial( SolveJob &J ) {
 
 // after the tick's read-back: the decisions of every job
 static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
+    if ( had_diag && c.hscal[ size_t( J.slot ) * SLOT_DOUBLES + SLOT_ERR ] != 0 ) {
+        // a cell past every capacity: this solve stops with the reference's "card capacity" status (the others go on);
+        // its outputs are the moments at the last accepted weights
+        CK( cudaMemsetAsync( c.dscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_ERR, 0, sizeof( double ), c.stream ) );
+        J.nstatus = NS_CAPACITY;
+        J.stats[ ST_STATUS ] = NS_CAPACITY;
+        J.pend = 0;
+        if ( J.state == J_FINAL ) {
+            J.stats[ ST_T_TOTAL ] = now_s() - J.t_begin;
+            J.state = J_DONE;
+        } else
+            J.state = J_FINAL;
+        return;
+    }
     if ( had_diag ) {
         const double *B = nullptr;
         switch ( J.state ) {
@@ -1201,6 +1223,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         P.power = J->opt[ SDOT_OPT_POWER ];
         if ( R.report >= 0 ) {
             P.report = rep_dev( c, *J, R.report );
+            P.perr = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR;
             P.partials = J->part_cells;
             P.counter = c.dcount + 4 * J->slot;
             P.nchunk = J->nch_cells;
@@ -1308,6 +1331,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaMemcpyAsync( c.hovf, &c.dovf->count, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaStreamSynchronize( c.stream ) );
+    clear_capacity_error( c );
     check_errors( c, "cells" );
     if ( *c.hovf > 0 ) {
         // the big cells: rebuilt in global memory, then the reports of their problems recomputed from the masses
@@ -1315,16 +1339,10 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         std::vector<OvfItem> items( count );
         CK( cudaMemcpy( items.data(), ( char * ) c.dovf + 256, count * sizeof( OvfItem ), cudaMemcpyDeviceToHost ) );
         ProbDev *dp = reinterpret_cast<ProbDev *>( upload_desc( c, big_probs.data(), big_probs.size() * sizeof( ProbDev ) ) );
-        bool moments = false, normal = false;
         std::vector<char> touched( big_probs.size(), 0 );
-        for ( auto &it : items ) {
-            touched[ it.prob ] = 1;
-            ( big_probs[ it.prob ].first ? moments : normal ) = true;
-        }
-        if ( normal && moments ) throw Error( SDOT_ERR_CAPACITY, "big cells in a normal and a final diagram of one tick" );
+        for ( auto &it : items ) touched[ it.prob ] = 1;
         c.timer.begin( c.stream, K_CELLS2D, double( count ) );
-        launch_cells2d_big( L, dp, c.dovf, count, moments ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ), c.derr, c.big_scratch,
-                            c.big_warps );
+        launch_cells2d_big( L, dp, c.dovf, count, 0, c.derr, c.big_scratch, c.big_warps );     // flags per problem
         c.timer.end( c.stream );
         std::vector<Chunk> rc;
         for ( size_t k = 0; k < big_probs.size(); ++k )
@@ -1336,6 +1354,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
+        clear_capacity_error( c );
         check_errors( c, "big cells" );
     }
     for ( SolveJob *J : jobs ) {

@@ -44,7 +44,8 @@ struct Ctx {
     Timer timer;
     Launch L() { return Launch{ stream, &launches, &timer }; }
 };
-constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC;
+constexpr int SLOT_ERR = 2 * NB_REPORT + NB_SC;                 // a problem's capacity-failure flag
+constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 1;
 
 void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
 void ctx_release( Ctx &c );

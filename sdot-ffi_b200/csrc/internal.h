@@ -89,6 +89,7 @@ struct ProbDev {
     // wpyr + ( dim + 1 ) ( poff[ l ] + node ); b = -1e300: no seed.  NULL: the global max bounds the search
     double *wpyr;
     double *wmom;                 // [ nodes, wmom_size( dim ) ] the moments the slopes are fitted from
+    double *perr;                 // set to 1 when a cell of this problem exceeds every capacity (NULL: none)
     int nlev;
     int poff[ MAX_LEV ];
 };

@@ -67,6 +67,25 @@ def test_a_solve_in_a_batch_is_the_solve_alone():
         assert a.stats["nb_diag"] == b.stats["nb_diag"]
 
 
+def test_a_cell_past_every_capacity_fails_its_solve_only():
+    """a ring of 5000 seeds around one (its cell has 5000 vertices, past the 4096 of the global-memory pass) in the
+    same batch as two ordinary problems: it ends with status 5 ("card capacity", SdotPlanNd.py:106-107), and the
+    others are the solves alone, bit for bit"""
+    k = 5000
+    ang = 2 * np.pi * np.arange(k) / k
+    ring = np.r_[[[0.5, 0.5]], np.c_[0.5 + 0.3 * np.cos(ang), 0.5 + 0.3 * np.sin(ang)]]
+    rng = np.random.default_rng(12)
+    others = [rng.uniform(size=(n, 2)) for n in (2000, 900)]
+    s = Iterative(tol=0.0, on_failure="ignore", tuning=Tuning(mass_rtol=1e-9))
+    pbs = [OtProblem(SumOfDiracs(p), sdot.Box()) for p in (others[0], ring, others[1])]
+    batch = SdotPlanNd._solve_many(pbs, s)
+    assert batch[1].stats["status"] == "card capacity" and not batch[1].converged
+    for i in (0, 2):
+        alone = SdotPlanNd._solve(pbs[i], s)
+        assert batch[i].converged
+        assert np.array_equal(alone.weights, batch[i].weights)
+
+
 def test_an_image_target_matches_the_oracle():
     rng = np.random.default_rng(31)
     xs = (np.arange(128) + 0.5) / 128
