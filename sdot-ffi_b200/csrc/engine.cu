@@ -84,6 +84,8 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
 void ctx_release( Ctx &c ) {
     cudaSetDevice( c.device );
     c.timer.release();
+    for ( auto &g : c.graphs ) cudaGraphExecDestroy( g.exec );
+    c.graphs.clear();
     if ( c.stream ) {
         if ( c.desc ) cudaFreeAsync( c.desc, c.stream );
         if ( c.dscal ) cudaFreeAsync( c.dscal, c.stream );
@@ -193,6 +195,8 @@ static void to_host_vec( Ctx &c, std::vector<T> &dst, const T *src, size_t count
 // uploads a descriptor block and returns its device address (stream ordered: the area is reused)
 static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
     if ( bytes > c.desc_bytes ) {
+        for ( auto &g : c.graphs ) cudaGraphExecDestroy( g.exec );
+        c.graphs.clear();
         if ( c.desc ) dfree( c, c.desc );
         c.desc_bytes = std::max( bytes, size_t( 1 ) << 20 );
         c.desc = ( char * ) dalloc( c, c.desc_bytes );
@@ -1033,6 +1037,18 @@ struct VecBatch {
         }
     }
     bool mg() const { return maxL > 0; }
+    // what the launches of a CG burst depend on: the upload area, the burst, and every table's size
+    std::vector<long long> layout_key( const char *desc, int burst ) const {
+        std::vector<long long> k{ ( long long ) ( uintptr_t ) desc, burst, ( long long ) ch.size(), maxL, ( long long ) bottom.size() };
+        for ( auto &x : v ) { k.push_back( x.n ); k.push_back( x.precond ); }
+        for ( int l = 0; l < maxL; ++l ) {
+            k.push_back( ( long long ) lv[ l ].size() );
+            k.push_back( ( long long ) down[ l ].size() );
+            k.push_back( ( long long ) up[ l ].size() );
+            k.push_back( ( long long ) crs[ l ].size() );
+        }
+        return k;
+    }
     // everything in one copy
     void upload( Ctx &c ) {
         std::vector<std::pair<const void *, size_t>> parts;
@@ -1083,6 +1099,44 @@ struct VecBatch {
 // preconditioned with the aggregation multigrid of the Newton engine (aggregates of 4 consecutive rows, 8 when the rows
 // hold more than 10 entries on average, as in 3D),
 // x in V.x, the gauge-fixed direction in V.d.  Returns the CG iterations, -1 if the CG failed.
+// a CG burst as a CUDA graph: captured the first time a batch layout is seen, replayed while it stays the same (the
+// descriptors it reads are re-uploaded into the same area before every replay); direct launches if capture fails
+template<class Issue>
+static void run_burst( Ctx &c, const std::vector<long long> &key, Issue issue ) {
+    for ( auto &g : c.graphs )
+        if ( g.key == key ) {
+            CK( cudaGraphLaunch( g.exec, c.stream ) );
+            c.launches += g.launches;
+            return;
+        }
+    const unsigned long long l0 = c.launches;
+    if ( cudaStreamBeginCapture( c.stream, cudaStreamCaptureModeThreadLocal ) != cudaSuccess ) {
+        cudaGetLastError();
+        issue();
+        return;
+    }
+    issue();
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const unsigned long long n = c.launches - l0;
+    c.launches = l0;
+    bool ok = cudaStreamEndCapture( c.stream, &graph ) == cudaSuccess && graph &&
+              cudaGraphInstantiate( &exec, graph, 0 ) == cudaSuccess;
+    if ( graph ) cudaGraphDestroy( graph );
+    if ( ! ok ) {
+        cudaGetLastError();
+        issue();
+        return;
+    }
+    if ( c.graphs.size() >= 32 ) {
+        cudaGraphExecDestroy( c.graphs.front().exec );
+        c.graphs.erase( c.graphs.begin() );
+    }
+    c.graphs.push_back( Ctx::BurstGraph{ key, exec, n } );
+    CK( cudaGraphLaunch( exec, c.stream ) );
+    c.launches += n;
+}
+
 constexpr int MG_BURST_SOLVE = 8;
 int mg_linear_solve( Ctx &c, const VecDev &V0, long nnz, double *hsc ) {
     SolveJob J;                                      // only its hierarchy is used
@@ -1312,16 +1366,19 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         if ( with_diag.empty() ) burst *= 4;
         double rows = 0;
         for ( auto &v : B->v ) rows += v.n;
+        auto issue = [&]() {
+            for ( int k = 0; k < burst; ++k ) {
+                if ( B->mg() ) {
+                    launch_cg_spmv_update( L, B->dv, B->dch, nch );
+                    B->vcycle( L );
+                    launch_cg_rz_p( L, B->dv, B->dch, nch );
+                } else
+                    launch_cg_iter( L, B->dv, B->dch, nch );
+            }
+        };
         unsigned long long l0 = c.launches;
         c.timer.begin( c.stream, K_CG, rows * burst );
-        for ( int k = 0; k < burst; ++k ) {
-            if ( B->mg() ) {
-                launch_cg_spmv_update( L, B->dv, B->dch, nch );
-                B->vcycle( L );
-                launch_cg_rz_p( L, B->dv, B->dch, nch );
-            } else
-                launch_cg_iter( L, B->dv, B->dch, nch );
-        }
+        run_burst( c, B->layout_key( c.desc, burst ), issue );
         c.timer.end( c.stream, c.launches - l0 );
     }
     // C. one read-back, then the decisions

@@ -41,6 +41,13 @@ struct Ctx {
     // descriptor upload area
     char *desc = nullptr;
     size_t desc_bytes = 0;
+    // CUDA graphs of the CG bursts, keyed by the layout of the batch they were captured for
+    struct BurstGraph {
+        std::vector<long long> key;
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long launches = 0;
+    };
+    std::vector<BurstGraph> graphs;
     Timer timer;
     Launch L() { return Launch{ stream, &launches, &timer }; }
 };
