@@ -64,6 +64,7 @@ void run_big_cells( Ctx &c, ProbDev *dprob, unsigned flags ) {
     Launch L = c.L();
     c.timer.begin( c.stream, K_CELLS2D, double( count ) );
     launch_cells2d_big( L, dprob, c.dovf, std::min( count, 1 << 16 ), flags, c.derr, c.big_scratch, c.big_warps );
+    launch_cells3d_big( L, dprob, c.dovf, std::min( count, 1 << 16 ), flags, c.derr );
     c.timer.end( c.stream );
     CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
 }
@@ -185,9 +186,9 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, double( n ) );
         launch_wpyr( L, dd.as<ProbDev>(), 1 );
         if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
-        else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr );
+        else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
         c.timer.end( c.stream );
-        if ( dim == 2 ) run_big_cells( c, dd.as<ProbDev>(), flags );
+        run_big_cells( c, dd.as<ProbDev>(), flags );
         CK( cudaGetLastError() );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         if ( host ) {
@@ -304,7 +305,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         P.w = wr;
         P.wmax_slot = slot;
         P.nb = nb; P.nid = nid; P.nc = nc;
-        if ( dim == 2 ) { P.ovf_count = ovf_count; P.ovf_cap = int( n ) + 4096; P.ovf_ids = ovf_ids; P.ovf_c = ovf_c; }
+        P.ovf_count = ovf_count; P.ovf_cap = int( n ) + 4096; P.ovf_ids = ovf_ids; P.ovf_c = ovf_c;
         std::vector<Chunk> ch;
         for ( int b = 0, k = 0; b < n; b += CHUNK, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + CHUNK ) ), k } );
         std::vector<Chunk> vch;
@@ -326,8 +327,8 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
         launch_wpyr( L, ( ProbDev * ) base, 1 );
         if ( dim == 2 ) launch_cells2d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
-        else launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr );
-        if ( dim == 2 ) run_big_cells( c, ( ProbDev * ) base, F_FACETS | F_USER_ORDER );
+        else launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
+        run_big_cells( c, ( ProbDev * ) base, F_FACETS | F_USER_ORDER );
         launch_lap_count( L, ( VecDev * ) ( base + o2 ), ( Chunk * ) ( base + o3 ), int( vch.size() ) );
         launch_lap_scan( L, ( VecDev * ) ( base + o2 ), 1 );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );

@@ -824,6 +824,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
     for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
         const OvfItem item = ovf->items[ it ];
         const ProbDev &P = probs[ item.prob ];
+        if ( P.dim != 2 ) continue;                      // the 3D items are the 3D pass's
         // flags 0: each problem's own pass (a final-moments diagram has `first`, a Newton diagram has not)
         const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
         const bool moments = fl & F_MOMENTS, facets = fl & F_FACETS, user_order = fl & F_USER_ORDER;

@@ -19,24 +19,33 @@
 namespace sdot {
 
 constexpr unsigned FULL3 = 0xffffffffu;
-constexpr int VC = 128;          // vertices per cell
-constexpr int PC = 96;           // planes per cell
-constexpr int W3 = 4;            // warps per block
+constexpr int W3 = 4;            // warps per block (main kernel)
 
-struct Cell3 {
+// the cell of one warp: VC vertices, PC planes, I the type of a vertex / plane index
+template<int VC_, int PC_, class I_>
+struct Cell3T {
+    static constexpr int VC = VC_, PC = PC_;
+    typedef I_ I;
+    static constexpr int NONE = int( I_( ~I_( 0 ) ) );   // "no vertex" in `tw`
     double vx[ VC ], vy[ VC ], vz[ VC ];
     double area[ 3 * VC ];                       // per (vertex, edge): the face-triangle contribution (integration)
     double nx[ PC ], ny[ PC ], nz[ PC ], no[ PC ];
     int pid[ PC ];
-    unsigned char va[ VC ], vb[ VC ], vc[ VC ];
+    I va[ VC ], vb[ VC ], vc[ VC ];
     unsigned char out[ VC ];
-    unsigned char nt[ VC ][ 3 ];                 // new triples of a cut
-    unsigned char tw[ 3 * VC ];                  // gaussians: the vertex across each (vertex, edge) entry, 255 if none
+    I nt[ VC ][ 3 ];                             // new triples of a cut
+    I tw[ 3 * VC ];                              // gaussians: the vertex across each (vertex, edge) entry, NONE if none
     double fmp[ PC ];                            // gaussians: the winding-angle part of each face's integral
+    double par[ PC ];                            // each face's integral (facets pass)
+    unsigned char used[ PC ];                    // plane compaction
+    I remap[ PC ];
     int nv, np;
 };
+using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in shared memory
+using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 84 KB
 
-__device__ __forceinline__ void solve3( const Cell3 &C, int a, int b, int c, double &x, double &y, double &z ) {
+template<class C3>
+__device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double &x, double &y, double &z ) {
     // x = ( o_a ( n_b x n_c ) + o_b ( n_c x n_a ) + o_c ( n_a x n_b ) ) / ( n_a . ( n_b x n_c ) )
     double bcx = C.ny[ b ] * C.nz[ c ] - C.nz[ b ] * C.ny[ c ], bcy = C.nz[ b ] * C.nx[ c ] - C.nx[ b ] * C.nz[ c ],
            bcz = C.nx[ b ] * C.ny[ c ] - C.ny[ b ] * C.nx[ c ];
@@ -52,7 +61,8 @@ __device__ __forceinline__ void solve3( const Cell3 &C, int a, int b, int c, dou
 }
 
 // the vertex holding the directed edge (e0, e1), -1 if none
-__device__ __forceinline__ int twin_of( const Cell3 &C, int e0, int e1 ) {
+template<class C3>
+__device__ __forceinline__ int twin_of( const C3 &C, int e0, int e1 ) {
     for ( int t = 0; t < C.nv; ++t ) {
         int a = C.va[ t ], b = C.vb[ t ], c = C.vc[ t ];
         if ( ( a == e0 && b == e1 ) || ( b == e0 && c == e1 ) || ( c == e0 && a == e1 ) ) return t;
@@ -60,7 +70,8 @@ __device__ __forceinline__ int twin_of( const Cell3 &C, int e0, int e1 ) {
     return -1;
 }
 
-__device__ void init_box3( Cell3 &C, int lane, const double *lo, const double *hi, double px, double py, double pz ) {
+template<class C3>
+__device__ void init_box3( C3 &C, int lane, const double *lo, const double *hi, double px, double py, double pz ) {
     // planes: 0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z ; ids -1 .. -6
     if ( lane < 6 ) {
         int ax = lane >> 1, sg = lane & 1;
@@ -87,21 +98,21 @@ __device__ void init_box3( Cell3 &C, int lane, const double *lo, const double *h
 }
 
 // drops the planes no vertex uses (when the plane table is full); false if it cannot make room
-__device__ bool compact_planes( Cell3 &C, int lane ) {
-    __shared__ unsigned char used_all[ W3 ][ PC ];
-    unsigned char *used = used_all[ threadIdx.x >> 5 ];
+template<class C3>
+__device__ bool compact_planes( C3 &C, int lane ) {
+    constexpr int PC = C3::PC;
+    unsigned char *used = C.used;
     for ( int p = lane; p < PC; p += 32 ) used[ p ] = 0;
     __syncwarp();
     for ( int k = lane; k < C.nv; k += 32 ) { used[ C.va[ k ] ] = 1; used[ C.vb[ k ] ] = 1; used[ C.vc[ k ] ] = 1; }
     __syncwarp();
     // new index of each used plane: a serial prefix by lane 0 (rare path)
-    __shared__ unsigned char remap_all[ W3 ][ PC ];
-    unsigned char *remap = remap_all[ threadIdx.x >> 5 ];
+    typename C3::I *remap = C.remap;
     if ( lane == 0 ) {
         int q = 0;
         for ( int p = 0; p < C.np; ++p ) {
             if ( ! used[ p ] ) continue;
-            remap[ p ] = ( unsigned char ) q;
+            remap[ p ] = ( typename C3::I ) q;
             C.nx[ q ] = C.nx[ p ]; C.ny[ q ] = C.ny[ p ]; C.nz[ q ] = C.nz[ p ]; C.no[ q ] = C.no[ p ]; C.pid[ q ] = C.pid[ p ];
             ++q;
         }
@@ -114,7 +125,8 @@ __device__ bool compact_planes( Cell3 &C, int lane ) {
 }
 
 // keep n . y <= off; false past a capacity
-__device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, double off, int id ) {
+template<class C3>
+__device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double off, int id ) {
     const int nv = C.nv;
     int nout = 0;
     for ( int base = 0; base < nv; base += 32 ) {
@@ -130,6 +142,8 @@ __device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, dou
         __syncwarp();
         return true;
     }
+    constexpr int VC = C3::VC, PC = C3::PC;
+    typedef typename C3::I I;
     const bool full = C.np >= PC;
     __syncwarp();
     if ( full && ! compact_planes( C, lane ) ) return false;
@@ -140,7 +154,7 @@ __device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, dou
     int nnew = 0;
     for ( int base = 0; base < nv; base += 32 ) {
         int k = base + lane;
-        unsigned char tr[ 3 ][ 3 ];
+        I tr[ 3 ][ 3 ];
         int cnt = 0;
         if ( k < nv && C.out[ k ] ) {
             int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
@@ -170,7 +184,7 @@ __device__ bool wclip3( Cell3 &C, int lane, double nx, double ny, double nz, dou
         unsigned m = __ballot_sync( FULL3, keep );
         int dst = kept_before + __popc( m & ( ( 1u << lane ) - 1 ) );
         double x = 0, y = 0, z = 0;
-        unsigned char a = 0, b = 0, c = 0;
+        I a = 0, b = 0, c = 0;
         if ( keep ) { x = C.vx[ k ]; y = C.vy[ k ]; z = C.vz[ k ]; a = C.va[ k ]; b = C.vb[ k ]; c = C.vc[ k ]; }
         __syncwarp();
         if ( keep ) { C.vx[ dst ] = x; C.vy[ dst ] = y; C.vz[ dst ] = z; C.va[ dst ] = a; C.vb[ dst ] = b; C.vc[ dst ] = c; }
@@ -210,7 +224,8 @@ __device__ __forceinline__ double cells_dist2_3( const ProbDev &P, const int *a0
     }
     return d2;
 }
-__device__ __forceinline__ double radius2_3( const Cell3 &C, int lane ) {
+template<class C3>
+__device__ __forceinline__ double radius2_3( const C3 &C, int lane ) {
     double R2 = 0;
     for ( int k = lane; k < C.nv; k += 32 ) R2 = fmax( R2, C.vx[ k ] * C.vx[ k ] + C.vy[ k ] * C.vy[ k ] + C.vz[ k ] * C.vz[ k ] );
     return warp_max( R2 );
@@ -218,7 +233,8 @@ __device__ __forceinline__ double radius2_3( const Cell3 &C, int lane ) {
 
 // the seeds of up to 32 grid cells (lane k: the range [ beg, beg + cnt ) of one cell) as candidates, 32 at a time:
 // each lane pre-tests one candidate against every vertex, then the cuts run in lane order
-__device__ void cut_by_ranges3( Cell3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, int beg, int cnt,
+template<class C3>
+__device__ void cut_by_ranges3( C3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, int beg, int cnt,
                                 bool &overflow ) {
     int inc = cnt;
 #pragma unroll
@@ -264,7 +280,8 @@ constexpr int WALK_LEAF3 = 1;        // the walk's leaves: blocks of 2 x 2 x 2 g
 // the pyramid of weight majorants, depth first, nearest child first, skipping the cells within Chebyshev distance rd of
 // c0 (the shells already walked) and the blocks that claim no vertex of the cell (wmaj_claims); a leaf block has
 // one cell per lane, each tested by `may_cut3`, clipped together
-__device__ void walk_pyramid3( Cell3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, const int *c0, int rd,
+template<class C3>
+__device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, const int *c0, int rd,
                                int2 *stk, bool &overflow ) {
     const int *g = P.g;
     if ( lane == 0 ) stk[ 0 ] = make_int2( ( P.nlev - 1 ) << 22, 0 );
@@ -427,14 +444,15 @@ __device__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double 
 // the gaussian sums over the clipped cell: lane parts of the mass, of the first moment about the seed and of
 // int |y|^2 rho (seed frame); C.area receives each (vertex, edge) entry's part of its face integral and C.fmp each
 // face's winding-angle part (both summed over the gaussians)
-__device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int lane, double px, double py, double pz, double &M, double &Fx,
+template<class C3>
+__device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane, double px, double py, double pz, double &M, double &Fx,
                                                 double &Fy, double &Fz, double &S2 ) {
     const int nv = C.nv, np = C.np;
     for ( int k = lane; k < nv; k += 32 ) {
         const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
         for ( int q = 0; q < 3; ++q ) {
             int t = twin_of( C, e[ ( q + 1 ) % 3 ], e[ q ] );
-            C.tw[ 3 * k + q ] = t < 0 ? 255 : ( unsigned char ) t;
+            C.tw[ 3 * k + q ] = t < 0 ? ( typename C3::I ) C3::NONE : ( typename C3::I ) t;
             C.area[ 3 * k + q ] = 0;
         }
     }
@@ -453,7 +471,7 @@ __device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int l
             const double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
             for ( int q = 0; q < 3; ++q ) {
                 const int t = C.tw[ 3 * k + q ];
-                if ( t == 255 ) continue;
+                if ( t == C3::NONE ) continue;
                 const int f = e[ q ];
                 const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] );
                 const double nhx = C.nx[ f ] / nn, nhy = C.ny[ f ] / nn, nhz = C.nz[ f ] / nn;
@@ -480,7 +498,7 @@ __device__ __noinline__ void integrate_gauss3( Cell3 &C, const ProbDev &P, int l
                 const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
                 for ( int q = 0; q < 3; ++q ) {
                     const int t = C.tw[ 3 * k + q ];
-                    if ( e[ q ] != p || t == 255 ) continue;
+                    if ( e[ q ] != p || t == C3::NONE ) continue;
                     th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
                 }
             }
@@ -519,15 +537,222 @@ __device__ __forceinline__ double gp_of3( double x, int r, double p ) {
     return r == 1 ? 1 / x : 1;
 }
 
+// a cell for the big-cell pass: queued (prob, seed); past the queue's capacity, an error of its problem
+__device__ __forceinline__ void queue3( const ProbDev &P, ErrRec *err, OvfList *ovf, int prob, int s, int user, int lane ) {
+    if ( lane == 0 ) {
+        int k = atomicAdd( &ovf->count, 1 );
+        if ( k < ovf->cap ) ovf->items[ k ] = OvfItem{ prob, s };
+        else record_error3( P, err, 4, prob, user, 0 );
+    }
+    __syncwarp();
+}
+
+// THE CELL of seed s (rank) of problem `prob`: clip, integrate, write.  The main kernel (`big` false) queues a cell past
+// its capacities for the big-cell pass and returns false (nothing written); `rep` (lane 0, may be NULL) accumulates
+// the Newton report
+template<class C3>
+__device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, int2 *stk, double wmax,
+                       double *rep, bool big ) {
+    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+    const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
+    const double wi = P.w ? P.w[ s ] : 0.0;
+    init_box3( C, lane, P.lo, P.hi, px, py, pz );
+    bool overflow = false;
+    int c0[ 3 ];
+    for ( int a = 0; a < 3; ++a ) {
+        double x = a == 0 ? px : ( a == 1 ? py : pz );
+        int k = int( floor( ( x - P.go[ a ] ) / P.gh[ a ] ) );
+        c0[ a ] = k < 0 ? 0 : ( k >= P.g[ a ] ? P.g[ a ] - 1 : k );
+    }
+    int rmax = 0;
+    for ( int a = 0; a < 3; ++a ) rmax = max( rmax, max( c0[ a ], P.g[ a ] - 1 - c0[ a ] ) );
+    int rd = -1;                 // the shells walked, when the pyramid takes over
+    for ( int r = 0; r <= rmax && C.nv > 0 && ! overflow; ++r ) {
+        const int side = 2 * r + 1, ncube = side * side * side;
+        const double R2s = radius2_3( C, lane );
+        for ( int cb = 0; cb < ncube && C.nv > 0 && ! overflow; cb += 32 ) {
+            int ci = cb + lane, beg = 0, cnt = 0;
+            if ( ci < ncube ) {
+                int dx = ci % side - r, dy = ( ci / side ) % side - r, dz = ci / ( side * side ) - r;
+                bool shell = max( abs( dx ), max( abs( dy ), abs( dz ) ) ) == r;
+                int x[ 3 ] = { c0[ 0 ] + dx, c0[ 1 ] + dy, c0[ 2 ] + dz };
+                if ( shell && x[ 0 ] >= 0 && x[ 0 ] < P.g[ 0 ] && x[ 1 ] >= 0 && x[ 1 ] < P.g[ 1 ] && x[ 2 ] >= 0 && x[ 2 ] < P.g[ 2 ] ) {
+                    const size_t gc = ( ( size_t ) x[ 2 ] * P.g[ 1 ] + x[ 1 ] ) * P.g[ 0 ] + x[ 0 ];
+                    if ( may_cut3( cells_dist2_3( P, x, x, px, py, pz ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2s, wi ) ) {
+                        int2 rg = P.cell_range[ gc ];
+                        beg = rg.x;
+                        cnt = rg.y - rg.x;
+                    }
+                }
+            }
+            cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
+        }
+        if ( C.nv == 0 || overflow ) break;
+        double R2 = radius2_3( C, lane );
+        double ex = R2 + wmax - wi;
+        if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+        if ( P.wpyr && r >= SHELLS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
+    }
+    if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, stk, overflow );
+    const int user = P.user[ s ];
+    if ( overflow ) {
+        // past the capacity of this warp's cell: the big-cell pass rebuilds it (the main kernel only)
+        if ( ! big && ovf ) { queue3( P, err, ovf, prob, s, user, lane ); return false; }
+        if ( lane == 0 ) record_error3( P, err, 4, prob, user, C3::VC );
+        if ( lane == 0 ) C.nv = 0;
+        __syncwarp();
+    }
+    // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once; gaussians by
+    // their face integrals (the sums below are then already density-weighted)
+    double vol = 0, fx = 0, fy = 0, fz = 0, s2 = 0;
+    const int nv = C.nv;
+    const bool gauss = P.dkind == D_GAUSS;
+    const double rho = gauss ? 1.0 : P.rho;
+    if ( gauss ) integrate_gauss3( C, P, lane, px, py, pz, vol, fx, fy, fz, s2 );
+    for ( int k = lane; k < nv && ! gauss; k += 32 ) {
+        int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+        double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
+        for ( int q = 0; q < 3; ++q ) {
+            int f = e[ q ], b = e[ ( q + 1 ) % 3 ];
+            int t = twin_of( C, b, f );
+            double a2 = 0;
+            if ( t >= 0 ) {
+                double Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
+                double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
+                double cf = C.no[ f ] / nn;
+                double Cx = C.nx[ f ] * cf, Cy = C.ny[ f ] * cf, Cz = C.nz[ f ] * cf;
+                // det( c_f, K, T ) with the sign that makes the box positive
+                double det = -( Cx * ( Ky * Tz - Kz * Ty ) - Cy * ( Kx * Tz - Kz * Tx ) + Cz * ( Kx * Ty - Ky * Tx ) );
+                double tv = det / 6;
+                vol += tv;
+                if ( moments ) {
+                    fx += tv * ( Cx + Kx + Tx ) / 4;
+                    fy += tv * ( Cy + Ky + Ty ) / 4;
+                    fz += tv * ( Cz + Kz + Tz ) / 4;
+                    s2 += tv / 10 * ( Cx * Cx + Cy * Cy + Cz * Cz + Kx * Kx + Ky * Ky + Kz * Kz + Tx * Tx + Ty * Ty + Tz * Tz +
+                                      Cx * Kx + Cy * Ky + Cz * Kz + Cx * Tx + Cy * Ty + Cz * Tz + Kx * Tx + Ky * Ty + Kz * Tz );
+                }
+                // the area of the face triangle ( c_f, K, T ) along the unit normal
+                double ux = Kx - Cx, uy = Ky - Cy, uz = Kz - Cz, vx = Tx - Cx, vy = Ty - Cy, vz = Tz - Cz;
+                double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+                a2 = -( cx * C.nx[ f ] + cy * C.ny[ f ] + cz * C.nz[ f ] ) / ( 2 * sqrt( nn ) );
+            }
+            C.area[ 3 * k + q ] = a2;
+        }
+    }
+    __syncwarp();
+    double mass = rho * warp_sum( vol );
+    // the facets: per plane, its triangles summed in vertex order (first the count, then the writes)
+    if ( facets ) {
+        const int row = user_order ? user : s;
+        int nf = 0;
+        for ( int pbase = 0; pbase < C.np; pbase += 32 ) {
+            int p = pbase + lane;
+            double ar = 0;
+            bool seed_plane = p < C.np && C.pid[ p ] >= 0;
+            if ( seed_plane ) {
+                for ( int k = 0; k < nv; ++k ) {
+                    if ( C.va[ k ] == p ) ar += C.area[ 3 * k ];
+                    if ( C.vb[ k ] == p ) ar += C.area[ 3 * k + 1 ];
+                    if ( C.vc[ k ] == p ) ar += C.area[ 3 * k + 2 ];
+                }
+                if ( gauss ) ar += C.fmp[ p ];
+            }
+            if ( p < C.np ) C.par[ p ] = seed_plane && ar > 0 ? ar : 0.0;
+            nf += __popc( __ballot_sync( FULL3, seed_plane && ar > 0 ) );
+        }
+        __syncwarp();
+        // more facets than the table's row: the big-cell pass (main kernel), or the overflow store (big-cell pass)
+        const bool to_store = nf > P.cap;
+        if ( to_store && ! big && ovf ) { queue3( P, err, ovf, prob, s, user, lane ); return false; }
+        if ( to_store && ! P.ovf_ids ) {
+            if ( lane == 0 ) record_error3( P, err, 4, prob, user, nf );
+            return true;
+        }
+        int base_at = 0;
+        if ( to_store ) {
+            if ( lane == 0 ) base_at = atomicAdd( P.ovf_count, nf );
+            base_at = __shfl_sync( FULL3, base_at, 0 );
+            if ( base_at + nf > P.ovf_cap ) {
+                if ( lane == 0 ) record_error3( P, err, 4, prob, user, nf );
+                return true;
+            }
+        }
+        int written = 0;
+        for ( int pbase = 0; pbase < C.np; pbase += 32 ) {
+            int p = pbase + lane;
+            const double ar = p < C.np ? C.par[ p ] : 0.0;
+            const bool fac = ar > 0;
+            unsigned fm = __ballot_sync( FULL3, fac );
+            int slot = written + __popc( fm & ( ( 1u << lane ) - 1 ) );
+            if ( fac ) {
+                double dist = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
+                int j = C.pid[ p ];
+                const int jid = user_order ? P.user[ j ] : j;
+                if ( to_store ) { P.ovf_ids[ base_at + slot ] = jid; P.ovf_c[ base_at + slot ] = rho * ar / ( 2 * dist ); }
+                else {
+                    size_t at = ( size_t ) row * P.cap + slot;
+                    P.nid[ at ] = jid;
+                    P.nc[ at ] = rho * ar / ( 2 * dist );
+                    if ( P.nm ) P.nm[ at ] = rho * ar;
+                }
+            }
+            written += __popc( fm );
+        }
+        if ( lane == 0 ) {
+            P.nb[ row ] = nf;
+            if ( to_store ) P.nid[ ( size_t ) row * P.cap ] = base_at;
+        }
+    }
+    if ( moments ) {
+        double mx = warp_sum( fx ), my = warp_sum( fy ), mz = warp_sum( fz ), ss = warp_sum( s2 );
+        double vv = mass / rho;
+        if ( lane == 0 ) {
+            if ( user_order ) {
+                if ( P.first ) {
+                    P.first[ 3 * ( size_t ) user ] = vv > 0 ? px + mx / vv : px;
+                    P.first[ 3 * ( size_t ) user + 1 ] = vv > 0 ? py + my / vv : py;
+                    P.first[ 3 * ( size_t ) user + 2 ] = vv > 0 ? pz + mz / vv : pz;
+                }
+                if ( P.cost ) P.cost[ user ] = rho * ss;
+            } else {
+                if ( P.first ) { P.first[ 3 * ( size_t ) s ] = rho * mx; P.first[ 3 * ( size_t ) s + 1 ] = rho * my; P.first[ 3 * ( size_t ) s + 2 ] = rho * mz; }
+                if ( P.cost ) P.cost[ s ] = rho * ss;
+            }
+        }
+    }
+    if ( lane == 0 && P.mass ) P.mass[ user_order ? user : s ] = mass;
+    if ( rep && lane == 0 ) {
+        double nu = P.nu[ s ];
+        double e2 = fabs( nu - mass );
+        rep[ R_WORST ] = fmax( rep[ R_WORST ], e2 );
+        rep[ R_WORST_REL ] = fmax( rep[ R_WORST_REL ], e2 / nu );
+        rep[ R_AMIN ] = fmin( rep[ R_AMIN ], mass );
+        rep[ R_ASUM ] += mass;
+        rep[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
+        double x = mass / nu, g = g_of3( x, P.res, P.power );
+        double n1 = rep[ R_GCOUNT ] + 1, d = g - rep[ R_GMEAN ];
+        rep[ R_GMEAN ] += d / n1;
+        rep[ R_GM2 ] += d * ( g - rep[ R_GMEAN ] );
+        rep[ R_GCOUNT ] = n1;
+        double u = nu / gp_of3( x, P.res, P.power );
+        rep[ R_SU ] += u;
+        rep[ R_SUG ] += u * g;
+        rep[ R_NUSUM ] += nu;
+        rep[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
+    }
+    __syncwarp();
+    return true;
+}
+
 __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
-                                                        unsigned flags, ErrRec *err ) {
+                                                        unsigned flags, ErrRec *err, OvfList *ovf ) {
     extern __shared__ char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cell3 &C = reinterpret_cast<Cell3 *>( smem )[ warp ];
     __shared__ double sh_rep[ W3 ][ NB_REPORT ];
     __shared__ int2 sh_stk[ W3 ][ WALK_STACK3 ];
     __shared__ int sh_last;
-    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
     for ( int cidx = blockIdx.x; cidx < nchunks; cidx += gridDim.x ) {
         const Chunk ch = chunks[ cidx ];
         const ProbDev &P = probs[ ch.prob ];
@@ -535,216 +760,74 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
         rep[ R_WORST ] = 0; rep[ R_WORST_REL ] = 0; rep[ R_AMIN ] = 1e300; rep[ R_ASUM ] = 0; rep[ R_LIN2 ] = 0; rep[ R_GCOUNT ] = 0;
         rep[ R_GMEAN ] = 0; rep[ R_GM2 ] = 0; rep[ R_SU ] = 0; rep[ R_SUG ] = 0; rep[ R_NUSUM ] = 0; rep[ R_NEMPTY ] = 0;
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
-        for ( int s = ch.begin + warp; s < ch.end; s += W3 ) {
-            const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
-            const double wi = P.w ? P.w[ s ] : 0.0;
-            init_box3( C, lane, P.lo, P.hi, px, py, pz );
-            bool overflow = false;
-            int c0[ 3 ];
-            for ( int a = 0; a < 3; ++a ) {
-                double x = a == 0 ? px : ( a == 1 ? py : pz );
-                int k = int( floor( ( x - P.go[ a ] ) / P.gh[ a ] ) );
-                c0[ a ] = k < 0 ? 0 : ( k >= P.g[ a ] ? P.g[ a ] - 1 : k );
-            }
-            int rmax = 0;
-            for ( int a = 0; a < 3; ++a ) rmax = max( rmax, max( c0[ a ], P.g[ a ] - 1 - c0[ a ] ) );
-            int rd = -1;                 // the shells walked, when the pyramid takes over
-            for ( int r = 0; r <= rmax && C.nv > 0 && ! overflow; ++r ) {
-                const int side = 2 * r + 1, ncube = side * side * side;
-                const double R2s = radius2_3( C, lane );
-                for ( int cb = 0; cb < ncube && C.nv > 0 && ! overflow; cb += 32 ) {
-                    int ci = cb + lane, beg = 0, cnt = 0;
-                    if ( ci < ncube ) {
-                        int dx = ci % side - r, dy = ( ci / side ) % side - r, dz = ci / ( side * side ) - r;
-                        bool shell = max( abs( dx ), max( abs( dy ), abs( dz ) ) ) == r;
-                        int x[ 3 ] = { c0[ 0 ] + dx, c0[ 1 ] + dy, c0[ 2 ] + dz };
-                        if ( shell && x[ 0 ] >= 0 && x[ 0 ] < P.g[ 0 ] && x[ 1 ] >= 0 && x[ 1 ] < P.g[ 1 ] && x[ 2 ] >= 0 && x[ 2 ] < P.g[ 2 ] ) {
-                            const size_t gc = ( ( size_t ) x[ 2 ] * P.g[ 1 ] + x[ 1 ] ) * P.g[ 0 ] + x[ 0 ];
-                            if ( may_cut3( cells_dist2_3( P, x, x, px, py, pz ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2s, wi ) ) {
-                                int2 rg = P.cell_range[ gc ];
-                                beg = rg.x;
-                                cnt = rg.y - rg.x;
+        for ( int s = ch.begin + warp; s < ch.end; s += W3 )
+            cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, ( flags & F_REPORT ) ? rep : nullptr, false );
+                if ( flags & F_REPORT ) {
+                    // the chunk's report, then the last chunk of the problem folds them in chunk order
+                    if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
+                    __syncthreads();
+                    if ( threadIdx.x == 0 ) {
+                        double r[ NB_REPORT ];
+                        for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = sh_rep[ 0 ][ k ];
+                        auto fold = [&]( const double *o ) {
+                            r[ R_WORST ] = fmax( r[ R_WORST ], o[ R_WORST ] );
+                            r[ R_WORST_REL ] = fmax( r[ R_WORST_REL ], o[ R_WORST_REL ] );
+                            r[ R_AMIN ] = fmin( r[ R_AMIN ], o[ R_AMIN ] );
+                            r[ R_ASUM ] += o[ R_ASUM ];
+                            r[ R_LIN2 ] += o[ R_LIN2 ];
+                            double na = r[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
+                            if ( nb > 0 ) {
+                                double d = o[ R_GMEAN ] - r[ R_GMEAN ];
+                                r[ R_GMEAN ] += d * nb / n;
+                                r[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
+                                r[ R_GCOUNT ] = n;
                             }
+                            r[ R_SU ] += o[ R_SU ]; r[ R_SUG ] += o[ R_SUG ]; r[ R_NUSUM ] += o[ R_NUSUM ]; r[ R_NEMPTY ] += o[ R_NEMPTY ];
+                        };
+                        for ( int w = 1; w < W3; ++w ) fold( sh_rep[ w ] );
+                        double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
+                        for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r[ k ];
+                        __threadfence();
+                        unsigned prev = atomicAdd( P.counter, 1u );
+                        sh_last = prev == unsigned( P.nchunk - 1 );
+                        if ( sh_last ) {
+                            __threadfence();
+                            const volatile double *src = P.partials;
+                            for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = src[ k ];
+                            for ( int c = 1; c < P.nchunk; ++c ) {
+                                double o[ NB_REPORT ];
+                                for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ ( size_t ) c * NB_REPORT + k ];
+                                fold( o );
+                            }
+                            for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r[ k ];
+                            *P.counter = 0;
                         }
                     }
-                    cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
-                }
-                if ( C.nv == 0 || overflow ) break;
-                double R2 = radius2_3( C, lane );
-                double ex = R2 + wmax - wi;
-                if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
-                if ( P.wpyr && r >= SHELLS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
-            }
-            if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, sh_stk[ warp ], overflow );
-            const int user = P.user[ s ];
-            if ( overflow ) {
-                if ( lane == 0 ) record_error3( P, err, 4, ch.prob, user, VC );
-                if ( lane == 0 ) C.nv = 0;
-                __syncwarp();
-            }
-            // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once; gaussians by
-            // their face integrals (the sums below are then already density-weighted)
-            double vol = 0, fx = 0, fy = 0, fz = 0, s2 = 0;
-            const int nv = C.nv;
-            const bool gauss = P.dkind == D_GAUSS;
-            const double rho = gauss ? 1.0 : P.rho;
-            if ( gauss ) integrate_gauss3( C, P, lane, px, py, pz, vol, fx, fy, fz, s2 );
-            for ( int k = lane; k < nv && ! gauss; k += 32 ) {
-                int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
-                double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
-                for ( int q = 0; q < 3; ++q ) {
-                    int f = e[ q ], b = e[ ( q + 1 ) % 3 ];
-                    int t = twin_of( C, b, f );
-                    double a2 = 0;
-                    if ( t >= 0 ) {
-                        double Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
-                        double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
-                        double cf = C.no[ f ] / nn;
-                        double Cx = C.nx[ f ] * cf, Cy = C.ny[ f ] * cf, Cz = C.nz[ f ] * cf;
-                        // det( c_f, K, T ) with the sign that makes the box positive
-                        double det = -( Cx * ( Ky * Tz - Kz * Ty ) - Cy * ( Kx * Tz - Kz * Tx ) + Cz * ( Kx * Ty - Ky * Tx ) );
-                        double tv = det / 6;
-                        vol += tv;
-                        if ( moments ) {
-                            fx += tv * ( Cx + Kx + Tx ) / 4;
-                            fy += tv * ( Cy + Ky + Ty ) / 4;
-                            fz += tv * ( Cz + Kz + Tz ) / 4;
-                            s2 += tv / 10 * ( Cx * Cx + Cy * Cy + Cz * Cz + Kx * Kx + Ky * Ky + Kz * Kz + Tx * Tx + Ty * Ty + Tz * Tz +
-                                              Cx * Kx + Cy * Ky + Cz * Kz + Cx * Tx + Cy * Ty + Cz * Tz + Kx * Tx + Ky * Ty + Kz * Tz );
-                        }
-                        // the area of the face triangle ( c_f, K, T ) along the unit normal
-                        double ux = Kx - Cx, uy = Ky - Cy, uz = Kz - Cz, vx = Tx - Cx, vy = Ty - Cy, vz = Tz - Cz;
-                        double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
-                        a2 = -( cx * C.nx[ f ] + cy * C.ny[ f ] + cz * C.nz[ f ] ) / ( 2 * sqrt( nn ) );
-                    }
-                    C.area[ 3 * k + q ] = a2;
+                    __syncthreads();
                 }
             }
-            __syncwarp();
-            double mass = rho * warp_sum( vol );
-            // the facets: per plane, its triangles summed in vertex order
-            int nf = 0;
-            if ( facets || ( flags & F_REPORT ) ) {
-                const int row = user_order ? user : s;
-                int written = 0;
-                for ( int pbase = 0; pbase < C.np; pbase += 32 ) {
-                    int p = pbase + lane;
-                    double ar = 0;
-                    bool seed_plane = p < C.np && C.pid[ p ] >= 0;
-                    if ( seed_plane ) {
-                        for ( int k = 0; k < nv; ++k ) {
-                            if ( C.va[ k ] == p ) ar += C.area[ 3 * k ];
-                            if ( C.vb[ k ] == p ) ar += C.area[ 3 * k + 1 ];
-                            if ( C.vc[ k ] == p ) ar += C.area[ 3 * k + 2 ];
-                        }
-                        if ( gauss ) ar += C.fmp[ p ];
-                    }
-                    bool fac = seed_plane && ar > 0;
-                    unsigned fm = __ballot_sync( FULL3, fac );
-                    int slot = written + __popc( fm & ( ( 1u << lane ) - 1 ) );
-                    if ( facets && fac && slot < P.cap ) {
-                        double dist = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
-                        size_t at = ( size_t ) row * P.cap + slot;
-                        int j = C.pid[ p ];
-                        P.nid[ at ] = user_order ? P.user[ j ] : j;
-                        P.nc[ at ] = rho * ar / ( 2 * dist );
-                        if ( P.nm ) P.nm[ at ] = rho * ar;
-                    }
-                    written += __popc( fm );
-                }
-                nf = written;
-                if ( facets && nf > P.cap ) {
-                    if ( lane == 0 ) record_error3( P, err, 4, ch.prob, user, nf );
-                    nf = P.cap;
-                }
-                if ( facets && lane == 0 ) P.nb[ row ] = nf;
-            }
-            if ( moments ) {
-                double mx = warp_sum( fx ), my = warp_sum( fy ), mz = warp_sum( fz ), ss = warp_sum( s2 );
-                double vv = mass / rho;
-                if ( lane == 0 ) {
-                    if ( user_order ) {
-                        if ( P.first ) {
-                            P.first[ 3 * ( size_t ) user ] = vv > 0 ? px + mx / vv : px;
-                            P.first[ 3 * ( size_t ) user + 1 ] = vv > 0 ? py + my / vv : py;
-                            P.first[ 3 * ( size_t ) user + 2 ] = vv > 0 ? pz + mz / vv : pz;
-                        }
-                        if ( P.cost ) P.cost[ user ] = rho * ss;
-                    } else {
-                        if ( P.first ) { P.first[ 3 * ( size_t ) s ] = rho * mx; P.first[ 3 * ( size_t ) s + 1 ] = rho * my; P.first[ 3 * ( size_t ) s + 2 ] = rho * mz; }
-                        if ( P.cost ) P.cost[ s ] = rho * ss;
-                    }
-                }
-            }
-            if ( lane == 0 && P.mass ) P.mass[ user_order ? user : s ] = mass;
-            if ( ( flags & F_REPORT ) && lane == 0 ) {
-                double nu = P.nu[ s ];
-                double e2 = fabs( nu - mass );
-                rep[ R_WORST ] = fmax( rep[ R_WORST ], e2 );
-                rep[ R_WORST_REL ] = fmax( rep[ R_WORST_REL ], e2 / nu );
-                rep[ R_AMIN ] = fmin( rep[ R_AMIN ], mass );
-                rep[ R_ASUM ] += mass;
-                rep[ R_LIN2 ] += ( nu - mass ) * ( nu - mass );
-                double x = mass / nu, g = g_of3( x, P.res, P.power );
-                double n1 = rep[ R_GCOUNT ] + 1, d = g - rep[ R_GMEAN ];
-                rep[ R_GMEAN ] += d / n1;
-                rep[ R_GM2 ] += d * ( g - rep[ R_GMEAN ] );
-                rep[ R_GCOUNT ] = n1;
-                double u = nu / gp_of3( x, P.res, P.power );
-                rep[ R_SU ] += u;
-                rep[ R_SUG ] += u * g;
-                rep[ R_NUSUM ] += nu;
-                rep[ R_NEMPTY ] += mass > 0 ? 0.0 : 1.0;
-            }
-            __syncwarp();
         }
-        if ( flags & F_REPORT ) {
-            // the chunk's report, then the last chunk of the problem folds them in chunk order
-            if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
-            __syncthreads();
-            if ( threadIdx.x == 0 ) {
-                double r[ NB_REPORT ];
-                for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = sh_rep[ 0 ][ k ];
-                auto fold = [&]( const double *o ) {
-                    r[ R_WORST ] = fmax( r[ R_WORST ], o[ R_WORST ] );
-                    r[ R_WORST_REL ] = fmax( r[ R_WORST_REL ], o[ R_WORST_REL ] );
-                    r[ R_AMIN ] = fmin( r[ R_AMIN ], o[ R_AMIN ] );
-                    r[ R_ASUM ] += o[ R_ASUM ];
-                    r[ R_LIN2 ] += o[ R_LIN2 ];
-                    double na = r[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
-                    if ( nb > 0 ) {
-                        double d = o[ R_GMEAN ] - r[ R_GMEAN ];
-                        r[ R_GMEAN ] += d * nb / n;
-                        r[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
-                        r[ R_GCOUNT ] = n;
-                    }
-                    r[ R_SU ] += o[ R_SU ]; r[ R_SUG ] += o[ R_SUG ]; r[ R_NUSUM ] += o[ R_NUSUM ]; r[ R_NEMPTY ] += o[ R_NEMPTY ];
-                };
-                for ( int w = 1; w < W3; ++w ) fold( sh_rep[ w ] );
-                double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
-                for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r[ k ];
-                __threadfence();
-                unsigned prev = atomicAdd( P.counter, 1u );
-                sh_last = prev == unsigned( P.nchunk - 1 );
-                if ( sh_last ) {
-                    __threadfence();
-                    const volatile double *src = P.partials;
-                    for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = src[ k ];
-                    for ( int c = 1; c < P.nchunk; ++c ) {
-                        double o[ NB_REPORT ];
-                        for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ ( size_t ) c * NB_REPORT + k ];
-                        fold( o );
-                    }
-                    for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r[ k ];
-                    *P.counter = 0;
-                }
-            }
-            __syncthreads();
-        }
+
+
+// the big-cell pass: one warp a block, the cell in dynamic shared memory (Cell3B), over the queued 3D items (the 2D ones
+// are the 2D pass's); flags 0: each problem's own pass (a final-moments diagram has `first`)
+__global__ void __launch_bounds__( 32 ) k_cells3d_big( const ProbDev *__restrict__ probs, const OvfList *__restrict__ ovf, int count,
+                                                        unsigned flags, ErrRec *err ) {
+    extern __shared__ char smem[];
+    __shared__ int2 stk[ WALK_STACK3 ];
+    Cell3B &C = *reinterpret_cast<Cell3B *>( smem );
+    const int lane = threadIdx.x;
+    for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
+        const OvfItem item = ovf->items[ it ];
+        const ProbDev &P = probs[ item.prob ];
+        if ( P.dim != 3 ) continue;
+        const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
+        const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
+        cell3( C, P, item.prob, item.seed, lane, fl, err, nullptr, stk, wmax, nullptr, true );
     }
 }
 
-void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err ) {
+void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf ) {
     if ( nchunks <= 0 ) return;
     const size_t smem = sizeof( Cell3 ) * W3;
     static bool configured = false;
@@ -752,7 +835,19 @@ void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks,
         cudaFuncSetAttribute( k_cells3d, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
         configured = true;
     }
-    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err );
+    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+    ++*L.launches;
+}
+
+void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err ) {
+    if ( count <= 0 ) return;
+    const size_t smem = sizeof( Cell3B );
+    static bool configured = false;
+    if ( ! configured ) {
+        cudaFuncSetAttribute( k_cells3d_big, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
+        configured = true;
+    }
+    k_cells3d_big<<<count < 296 ? count : 296, 32, smem, L.stream>>>( probs, ovf, count, flags, err );
     ++*L.launches;
 }
 

@@ -461,7 +461,7 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     const int dim = J.G.dim, cap = J.cap;
     J.nch_cells = int( ( n + CHUNK - 1 ) / CHUNK );
     J.nch_vec = int( ( n + VCHUNK - 1 ) / VCHUNK );
-    J.ovf_cap = dim == 2 ? int( n ) + 4096 : 0;
+    J.ovf_cap = int( n ) + 4096;
     size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                    size_t( n ) * 4 + size_t( J.nch_cells ) * NB_REPORT * 8 + size_t( J.nch_vec ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) +
                    2 * ( size_t( J.ovf_cap ) * 12 + 16 ) + 48 * 256;
@@ -1275,9 +1275,9 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         P.nu = J->nu;
         P.res = J->res_cur;
         P.power = J->opt[ SDOT_OPT_POWER ];
+        P.perr = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR;
         if ( R.report >= 0 ) {
             P.report = rep_dev( c, *J, R.report );
-            P.perr = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR;
             P.partials = J->part_cells;
             P.counter = c.dcount + 4 * J->slot;
             P.nchunk = J->nch_cells;
@@ -1335,7 +1335,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
                 unsigned flags = pass ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
                 c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
                 if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX.size() ), flags, c.derr, c.dovf );
-                else launch_cells3d( L, dp, dc, int( CX.size() ), flags, c.derr );
+                else launch_cells3d( L, dp, dc, int( CX.size() ), flags, c.derr, c.dovf );
                 c.timer.end( c.stream );
             }
         }
@@ -1400,6 +1400,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         for ( auto &it : items ) touched[ it.prob ] = 1;
         c.timer.begin( c.stream, K_CELLS2D, double( count ) );
         launch_cells2d_big( L, dp, c.dovf, count, 0, c.derr, c.big_scratch, c.big_warps );     // flags per problem
+        launch_cells3d_big( L, dp, c.dovf, count, 0, c.derr );
         c.timer.end( c.stream );
         std::vector<Chunk> rc;
         for ( size_t k = 0; k < big_probs.size(); ++k )

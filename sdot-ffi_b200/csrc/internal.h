@@ -305,6 +305,8 @@ void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, 
 void launch_scale( const Launch &L, double *v, int n, double s );
 void launch_scatter( const Launch &L, const double *ranked, const int *user, int n, int dim, double *out_user );
 void launch_gather_vec( const Launch &L, const double *user_vals, const int *user, int n, double *ranked, double scale );
-void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err );
+void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
+// the queued 3D cells (past the warp cell's capacities) rebuilt one warp a block with larger capacities
+void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err );
 
 } // namespace sdot

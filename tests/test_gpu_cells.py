@@ -198,8 +198,9 @@ def test_both_linear_methods_match_a_direct_solve(d, n):
     from sdot import _lib
     rng = np.random.default_rng(50 + d)
     pos = rng.uniform(size=(n, d))
-    w = rng.uniform(0, 0.3 * n ** (-2.0 / d), size=n)
+    w = rng.uniform(0, 0.02 * n ** (-2.0 / d), size=n)     # no empty cell: one connected graph, a consistent system
     row, cols, vals, dia = _pd(pos, w).laplacian()
+    assert (np.diff(row) > 0).all()
     b = rng.standard_normal((2, n))
     b -= b.mean(axis=1, keepdims=True)
     L = sp.diags(dia) - sp.csr_matrix((vals, cols, row), shape=(n, n))
