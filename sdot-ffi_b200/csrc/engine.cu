@@ -206,11 +206,16 @@ static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
 }
 
 // a second block in the upload area, after `offset` bytes already uploaded by this step (stream ordered)
+// (past the area's end: a block of its own, freed in stream order at the end of the tick)
 static char *upload_desc_at( Ctx &c, const void *src, size_t bytes, size_t offset ) {
     offset = ( offset + 255 ) & ~size_t( 255 );
-    if ( offset + bytes > c.desc_bytes ) throw Error( SDOT_ERR_NO_MEMORY, "descriptor area too small for the big cells" );
-    CK( cudaMemcpyAsync( c.desc + offset, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
-    return c.desc + offset;
+    char *dst = c.desc + offset;
+    if ( offset + bytes > c.desc_bytes ) {
+        dst = ( char * ) dalloc( c, bytes );
+        c.desc_spill.push_back( dst );
+    }
+    CK( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
+    return dst;
 }
 
 void check_errors( Ctx &c, const char *where ) {
@@ -1291,64 +1296,73 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         int k = 0;
         for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) CC.push_back( Chunk{ pi, b, std::min( J->G.n, b + CHUNK ), k } );
     }
-    // the launch arrays of the 2D cells, kept for the big-cell pass: [ normal diagrams | final (moments) diagrams ]
+    // the problems of this tick's diagrams in ONE array (both dimensions), so that the big-cell queue's problem indices mean
+    // the same thing to every kernel: [ 2D normal | 2D final (moments) | 3D normal | 3D final ], flags uniform per launch
     std::vector<ProbDev> big_probs;
-    std::vector<std::vector<Chunk>> big_chunks;      // per problem of big_probs, its chunks (for a report recompute)
-    auto run_cells = [&]( std::vector<ProbDev> &PP, std::vector<Chunk> &CC, int dim, bool report_only ) {
-        if ( PP.empty() ) return;
-        // flags are uniform per launch: final (moments) diagrams go in their own launch, after the others in one array
+    std::vector<std::vector<Chunk>> big_chunks;      // per problem of big_probs, its chunks of a normal diagram (report recompute)
+    size_t desc_used = 0;                            // bytes of the upload area this tick's cells use
+    CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+    {
         std::vector<ProbDev> PX;
-        std::vector<Chunk> CA, CB;
-        std::vector<int> idx( PP.size(), -1 );
-        for ( int pass = 0; pass < 2; ++pass )
-            for ( size_t k = 0; k < PP.size(); ++k )
-                if ( ( PP[ k ].first != nullptr ) == ( pass == 1 ) ) { idx[ k ] = int( PX.size() ); PX.push_back( PP[ k ] ); }
-        for ( auto &ch : CC ) {
-            Chunk x = ch;
-            x.prob = idx[ ch.prob ];
-            ( PP[ ch.prob ].first != nullptr ? CB : CA ).push_back( x );
+        std::vector<Chunk> CX[ 4 ];                     // ( dim 2, 3 ) x ( normal, final )
+        for ( int dim = 2; dim <= 3; ++dim ) {
+            std::vector<ProbDev> &PP = dim == 2 ? P2 : P3;
+            std::vector<Chunk> &CC = dim == 2 ? C2 : C3;
+            std::vector<int> idx( PP.size(), -1 );
+            for ( int pass = 0; pass < 2; ++pass )
+                for ( size_t k = 0; k < PP.size(); ++k )
+                    if ( ( PP[ k ].first != nullptr ) == ( pass == 1 ) ) { idx[ k ] = int( PX.size() ); PX.push_back( PP[ k ] ); }
+            for ( auto &ch : CC ) {
+                Chunk x = ch;
+                x.prob = idx[ ch.prob ];
+                CX[ 2 * ( dim - 2 ) + ( PP[ ch.prob ].first != nullptr ) ].push_back( x );
+            }
         }
-        size_t b1 = PX.size() * sizeof( ProbDev ), o2 = ( b1 + 255 ) & ~size_t( 255 ), b2 = CA.size() * sizeof( Chunk ),
-               o3 = o2 + ( ( b2 + 255 ) & ~size_t( 255 ) ), b3 = CB.size() * sizeof( Chunk );
-        std::vector<char> buf( o3 + b3 );
-        std::memcpy( buf.data(), PX.data(), b1 );
-        if ( b2 ) std::memcpy( buf.data() + o2, CA.data(), b2 );
-        if ( b3 ) std::memcpy( buf.data() + o3, CB.data(), b3 );
-        char *d = upload_desc( c, buf.data(), buf.size() );
-        ProbDev *dp = reinterpret_cast<ProbDev *>( d );
-        if ( ! report_only ) {
+        if ( ! PX.empty() ) {
+            size_t off[ 5 ];
+            size_t total = ( PX.size() * sizeof( ProbDev ) + 255 ) & ~size_t( 255 );
+            for ( int q = 0; q < 4; ++q ) { off[ q ] = total; total += ( CX[ q ].size() * sizeof( Chunk ) + 255 ) & ~size_t( 255 ); }
+            std::vector<char> buf( total );
+            std::memcpy( buf.data(), PX.data(), PX.size() * sizeof( ProbDev ) );
+            for ( int q = 0; q < 4; ++q )
+                if ( ! CX[ q ].empty() ) std::memcpy( buf.data() + off[ q ], CX[ q ].data(), CX[ q ].size() * sizeof( Chunk ) );
+            char *d = upload_desc( c, buf.data(), buf.size() );
+            desc_used = total;
+            ProbDev *dp = reinterpret_cast<ProbDev *>( d );
             c.timer.begin( c.stream, K_INDEX, double( PX.size() ) );
             launch_wpyr( L, dp, int( PX.size() ) );
             c.timer.end( c.stream );
-        }
-        for ( int pass = 0; pass < 2; ++pass ) {
-            std::vector<Chunk> &CX = pass ? CB : CA;
-            if ( CX.empty() ) continue;
-            Chunk *dc = reinterpret_cast<Chunk *>( d + ( pass ? o3 : o2 ) );
-            double seeds = 0;
-            for ( auto &ch : CX ) seeds += ch.end - ch.begin;
-            if ( report_only ) {
-                c.timer.begin( c.stream, K_REPORT, seeds );
-                launch_report( L, dp, dc, int( CX.size() ) );
-                c.timer.end( c.stream );
-            } else {
-                unsigned flags = pass ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
+            for ( int q = 0; q < 4; ++q ) {
+                if ( CX[ q ].empty() ) continue;
+                const int dim = 2 + q / 2;
+                Chunk *dc = reinterpret_cast<Chunk *>( d + off[ q ] );
+                double seeds = 0;
+                for ( auto &ch : CX[ q ] ) seeds += ch.end - ch.begin;
+                unsigned flags = ( q & 1 ) ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
                 c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
-                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX.size() ), flags, c.derr, c.dovf );
-                else launch_cells3d( L, dp, dc, int( CX.size() ), flags, c.derr, c.dovf );
+                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf );
+                else launch_cells3d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf );
                 c.timer.end( c.stream );
             }
-        }
-        if ( dim == 2 && ! report_only ) {
             big_probs = PX;
             big_chunks.assign( PX.size(), {} );
-            for ( auto &ch : CA ) big_chunks[ ch.prob ].push_back( ch );
+            for ( int q : { 0, 2 } )
+                for ( auto &ch : CX[ q ] ) big_chunks[ ch.prob ].push_back( ch );
         }
-    };
-    CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
-    run_cells( P2, C2, 2, false );
-    run_cells( P3, C3, 3, false );
-    run_cells( PR, CR, 2, true );
+    }
+    // the report-only problems (targets rescaled): their report from the masses in memory
+    if ( ! PR.empty() ) {
+        size_t b1 = PR.size() * sizeof( ProbDev ), o2 = ( b1 + 255 ) & ~size_t( 255 );
+        std::vector<char> buf( o2 + CR.size() * sizeof( Chunk ) );
+        std::memcpy( buf.data(), PR.data(), b1 );
+        std::memcpy( buf.data() + o2, CR.data(), CR.size() * sizeof( Chunk ) );
+        char *d = desc_used ? upload_desc_at( c, buf.data(), buf.size(), desc_used ) : upload_desc( c, buf.data(), buf.size() );
+        double seeds = 0;
+        for ( auto &ch : CR ) seeds += ch.end - ch.begin;
+        c.timer.begin( c.stream, K_REPORT, seeds );
+        launch_report( L, reinterpret_cast<ProbDev *>( d ), reinterpret_cast<Chunk *>( d + o2 ), int( CR.size() ) );
+        c.timer.end( c.stream );
+    }
     // B. CG iterations
     VecBatch cgj, cgm;
     std::vector<SolveJob *> with_cg;
@@ -1423,6 +1437,8 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     }
     // D. the vector work
     launch_pending( c, jobs );
+    for ( void *p : c.desc_spill ) dfree( c, p );
+    c.desc_spill.clear();
 }
 
 void job_run( Ctx &c, std::vector<SolveJob *> &jobs, int max_ticks ) {

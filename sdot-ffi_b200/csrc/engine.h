@@ -41,6 +41,7 @@ struct Ctx {
     // descriptor upload area
     char *desc = nullptr;
     size_t desc_bytes = 0;
+    std::vector<void *> desc_spill;   // descriptor blocks past the area, freed at the end of the tick
     // CUDA graphs of the CG bursts, keyed by the layout of the batch they were captured for
     struct BurstGraph {
         std::vector<long long> key;
