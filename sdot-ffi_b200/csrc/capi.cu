@@ -33,6 +33,37 @@ int32_t guard( sdot_status *st, F &&f ) {
     }
 }
 
+// reverse Cuthill-McKee order of a symmetric pattern: perm[ new ] = old.  Consecutive rows are then neighbours, which
+// the multigrid's aggregates of consecutive rows need (a caller's CSR comes in any order)
+std::vector<int> rcm_order( long n, const std::vector<int> &rp, const std::vector<int> &col ) {
+    std::vector<int> perm, deg( n );
+    perm.reserve( n );
+    for ( long i = 0; i < n; ++i ) deg[ i ] = rp[ i + 1 ] - rp[ i ];
+    std::vector<char> seen( n, 0 );
+    std::vector<int> by_deg( n );
+    for ( long i = 0; i < n; ++i ) by_deg[ i ] = int( i );
+    std::stable_sort( by_deg.begin(), by_deg.end(), [&]( int a, int b ) { return deg[ a ] < deg[ b ]; } );
+    std::vector<int> nb;
+    for ( int start : by_deg ) {
+        if ( seen[ start ] ) continue;
+        seen[ start ] = 1;
+        size_t head = perm.size();
+        perm.push_back( start );
+        while ( head < perm.size() ) {
+            const int i = perm[ head++ ];
+            nb.clear();
+            for ( int e = rp[ i ]; e < rp[ i + 1 ]; ++e ) {
+                const int j = col[ e ];
+                if ( j >= 0 && j < n && ! seen[ j ] ) { seen[ j ] = 1; nb.push_back( j ); }
+            }
+            std::stable_sort( nb.begin(), nb.end(), [&]( int a, int b ) { return deg[ a ] < deg[ b ]; } );
+            perm.insert( perm.end(), nb.begin(), nb.end() );
+        }
+    }
+    std::reverse( perm.begin(), perm.end() );
+    return perm;
+}
+
 struct DevVec {
     Ctx &c;
     void *p = nullptr;
@@ -384,12 +415,41 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         unsigned *counter = A.take<unsigned>( 2 );
         CK( cudaMemsetAsync( counter, 0, 8, c.stream ) );
         auto kind = memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        CK( cudaMemcpyAsync( rp, rp32.data(), ( n + 1 ) * 4, cudaMemcpyHostToDevice, c.stream ) );
-        if ( nnz ) {
-            CK( cudaMemcpyAsync( col, cols, nnz * 4, kind, c.stream ) );
-            CK( cudaMemcpyAsync( val, vals, nnz * 8, kind, c.stream ) );
+        std::vector<int> perm, iperm;                       // method 1: the system in reverse Cuthill-McKee order
+        if ( method == 1 ) {
+            std::vector<int> hcol( nnz );
+            std::vector<double> hval( nnz ), hdia( n );
+            auto to_host = memory == SDOT_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+            if ( nnz ) {
+                CK( cudaMemcpy( hcol.data(), cols, nnz * 4, to_host ) );
+                CK( cudaMemcpy( hval.data(), vals, nnz * 8, to_host ) );
+            }
+            CK( cudaMemcpy( hdia.data(), dia, n * 8, to_host ) );
+            perm = rcm_order( n, rp32, hcol );
+            iperm.assign( n, 0 );
+            for ( long k = 0; k < n; ++k ) iperm[ perm[ k ] ] = int( k );
+            std::vector<int> prp( n + 1, 0 ), pcol( nnz );
+            std::vector<double> pval( nnz ), pdia( n );
+            for ( long k = 0; k < n; ++k ) {
+                const int i = perm[ k ];
+                prp[ k + 1 ] = prp[ k ] + ( rp32[ i + 1 ] - rp32[ i ] );
+                pdia[ k ] = hdia[ i ];
+                for ( int e = rp32[ i ], f = prp[ k ]; e < rp32[ i + 1 ]; ++e, ++f ) { pcol[ f ] = iperm[ hcol[ e ] ]; pval[ f ] = hval[ e ]; }
+            }
+            CK( cudaMemcpy( rp, prp.data(), ( n + 1 ) * 4, cudaMemcpyHostToDevice ) );
+            if ( nnz ) {
+                CK( cudaMemcpy( col, pcol.data(), nnz * 4, cudaMemcpyHostToDevice ) );
+                CK( cudaMemcpy( val, pval.data(), nnz * 8, cudaMemcpyHostToDevice ) );
+            }
+            CK( cudaMemcpy( ddia, pdia.data(), n * 8, cudaMemcpyHostToDevice ) );
+        } else {
+            CK( cudaMemcpyAsync( rp, rp32.data(), ( n + 1 ) * 4, cudaMemcpyHostToDevice, c.stream ) );
+            if ( nnz ) {
+                CK( cudaMemcpyAsync( col, cols, nnz * 4, kind, c.stream ) );
+                CK( cudaMemcpyAsync( val, vals, nnz * 8, kind, c.stream ) );
+            }
+            CK( cudaMemcpyAsync( ddia, dia, n * 8, kind, c.stream ) );
         }
-        CK( cudaMemcpyAsync( ddia, dia, n * 8, kind, c.stream ) );
         std::vector<Chunk> vch;
         for ( int bb = 0, k = 0; bb < n; bb += VCHUNK, ++k ) vch.push_back( Chunk{ 0, bb, int( std::min<long>( n, bb + VCHUNK ) ), k } );
         VecDev V;
@@ -399,7 +459,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         V.tol = tol > 0 ? tol : 1e-10;
         V.maxit = maxit > 0 ? maxit : 100000;
         V.sc = sc; V.partials = part; V.counter = counter; V.nchunk = int( vch.size() ); V.active = 1;
-        V.rank0 = 0;
+        V.rank0 = method == 1 ? iperm[ 0 ] : 0;            // the gauge x[ 0 ] = 0, row 0 wherever it went
         size_t o1 = ( sizeof( VecDev ) + 255 ) & ~size_t( 255 );
         DevVec dd( c, o1 + vch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &V, sizeof( V ), cudaMemcpyHostToDevice, c.stream ) );
@@ -415,6 +475,11 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             double mean = 0;
             for ( double v : hb ) mean += v;
             mean /= double( n );
+            if ( method == 1 ) {
+                std::vector<double> hp( n );
+                for ( long q = 0; q < n; ++q ) hp[ q ] = hb[ perm[ q ] ];
+                hb.swap( hp );
+            }
             CK( cudaMemcpyAsync( b, hb.data(), n * 8, cudaMemcpyHostToDevice, c.stream ) );
             double hsc[ NB_SC ] = {};
             hsc[ SC_MEAN ] = mean;
@@ -422,8 +487,11 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             if ( method == 1 ) {
                 const int its = mg_linear_solve( c, V, nnz, hsc );
                 if ( iterations ) iterations[ k ] = its;
-                CK( cudaMemcpyAsync( x + size_t( k ) * n, d, n * 8, memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.stream ) );
+                std::vector<double> hd( n ), hx( n );
+                CK( cudaMemcpyAsync( hd.data(), d, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
                 CK( cudaStreamSynchronize( c.stream ) );
+                for ( long q = 0; q < n; ++q ) hx[ perm[ q ] ] = hd[ q ];
+                CK( cudaMemcpy( x + size_t( k ) * n, hx.data(), n * 8, memory == SDOT_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost ) );
                 continue;
             }
             launch_cg_init( L, dv, dch, int( vch.size() ) );

@@ -513,7 +513,7 @@ static size_t mg_bytes( int dim, long n, int cap ) {
     int L = mg_levels( dim, n, sz );
     if ( ! L ) return 0;
     size_t b = size_t( n ) * cap * 4 + size_t( n ) * 4 * 4;
-    const int capc = dim == 2 ? 8 : 64;
+    const int capc = dim == 2 ? 16 : 64;   // coarse entries a row can take on average (about 8 in 2D, 22 in 3D)
     for ( int l = 1; l < L; ++l ) b += size_t( sz[ l ] + 1 ) * 4 * 2 + size_t( sz[ l ] ) * capc * 8 + size_t( sz[ l ] ) * 5 * 4 +
                                         size_t( sz[ l ] / MG_CCH + 1 ) * 16 + 12 * 256;
     return b + MG_BOTTOM * MG_BOTTOM * 4 + 16 * 256;
@@ -527,7 +527,7 @@ static void alloc_mg( Ctx &c, SolveJob &J ) {
     const size_t bytes = mg_bytes( dim, J.G.n, J.cap );
     J.mg_mem = ( char * ) dalloc( c, bytes );
     Arena A{ J.mg_mem, bytes, 0 };
-    const int capc = dim == 2 ? 8 : 64;
+    const int capc = dim == 2 ? 16 : 64;   // coarse entries a row can take on average (about 8 in 2D, 22 in 3D)
     for ( int l = 0; l < J.mg_L; ++l ) {
         const int n = J.mg_n[ l ];
         if ( l == 0 ) {

