@@ -189,6 +189,8 @@ enum sdot_option {
     SDOT_OPT_LIN_METHOD,          /* 0 Jacobi-PCG, 1 multigrid-PCG                                            */
     SDOT_OPT_PRECISION,           /* 0 FP64 clipping; 1 FP32 clipping with FP64 re-check                     */
     SDOT_OPT_LIN_PRECISION,       /* 0 FP64 CG; 1 FP32 inner CG with FP64 iterative refinement               */
+    SDOT_OPT_AGG_MARGIN,          /* aggregation of near-coincident seeds: merge a pair when c_ij ulp(w) margin  */
+                                  /* > the tolerance (sdotplan/Aggregation.h); 0: off; the reference uses 4      */
     SDOT_NB_OPTIONS
 };
 #define SDOT_NB_STATS 31          /* the order of SdotPlanNd._STATS (SdotPlanNd.py:100-103)                  */
@@ -209,6 +211,8 @@ typedef struct sdot_solve_out {
     double *history;              /* [cap_history, SDOT_NB_HIST] host (may be NULL)                          */
     int32_t cap_history;
     int32_t nb_history;           /* rows written                                                            */
+    int32_t *clusters;            /* [n] (may be NULL, memory as `weights`): the smallest user index of each   */
+                                  /* seed's cluster of near-coincident seeds, its own index if none             */
 } sdot_solve_out;
 
 /* One damped-Newton SDOT solve.  Replaces `sdot::gpu2d::solve<V,VD>(queue, pd, nu, w0, dups, options,

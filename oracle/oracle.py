@@ -23,10 +23,10 @@ _LIB = None
 
 #: the option vector of `od_solve`, in order
 OPTIONS = ["tol_abs", "tol_rel", "maxit", "max_backtracks", "t_min", "mult_ok", "residual", "power", "switch", "lin_tol",
-           "lin_maxit", "keep_start", "continuation", "conv_threshold", "conv_s0", "conv_ratio", "conv_min", "brute", "cap"]
+           "lin_maxit", "keep_start", "continuation", "conv_threshold", "conv_s0", "conv_ratio", "conv_min", "brute", "cap", "agg_margin"]
 DEFAULTS = dict(tol_abs=1e-8, tol_rel=0.0, maxit=100, max_backtracks=60, t_min=1e-10, mult_ok=4.0, residual=1, power=0.5,
                 switch=2.0, lin_tol=1e-12, lin_maxit=100000, keep_start=0, continuation=1, conv_threshold=1e-2, conv_s0=0.0,
-                conv_ratio=2 ** 0.5, conv_min=0.0, brute=0, cap=64)
+                conv_ratio=2 ** 0.5, conv_min=0.0, brute=0, cap=64, agg_margin=0.0)
 STATS = ["status", "residual", "residual0", "nb_iter", "nb_diag", "nb_backtracks", "t_majorant", "t_diag", "t_asm", "t_lin", "t_lim", "eps",
          "domain_mass", "nb_overflowed", "nb_cell_lim", "nb_limit_rounds", "lin_nb_hierarchies", "lin_nb_iter", "lin_worst", "start", "t_total",
          "nb_continuation_steps", "min_start_mass", "it_switch", "it_double", "scratch_bytes",
@@ -49,7 +49,7 @@ def lib():
         L.od_cells.restype = ctypes.c_int
         L.od_cells.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
         L.od_solve.restype = ctypes.c_int
-        L.od_solve.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, P, ctypes.c_int, P, P, P, P, P, P, P, P, P, ctypes.c_long, P]
+        L.od_solve.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, P, ctypes.c_int, P, P, P, P, P, P, P, P, P, ctypes.c_long, P, P]
         L.od_laplacian_solve.restype = ctypes.c_int
         L.od_laplacian_solve.argtypes = [ctypes.c_long, ctypes.c_int, P, P, P, P, P, ctypes.c_double, ctypes.c_int]
         L.od_max_threads.restype = ctypes.c_int
@@ -143,11 +143,12 @@ def solve(pos, nu=None, box=None, density=None, w0=None, max_steps=None, **optio
     cap_steps = int(max_steps or (int(o["maxit"]) + 1) * 8)
     hist = np.zeros((cap_steps, 8))
     nb_steps = ctypes.c_long(0)
+    clusters = np.zeros(n, dtype=np.int32)
     weights, masses, bary, cost, stats = np.zeros(n), np.zeros(n), np.zeros((n, d)), np.zeros(1), np.zeros(len(STATS))
     st = lib().od_solve(d, n, _p(pos), _p(nu), _p(w0a), _p(bx), kind, _p(par), _p(val), _p(opts), _p(weights), _p(masses), _p(bary),
-                        _p(cost), _p(stats), _p(hist), cap_steps, ctypes.byref(nb_steps))
+                        _p(cost), _p(stats), _p(hist), cap_steps, ctypes.byref(nb_steps), _p(clusters))
     return dict(weights=weights, masses=masses, bary=bary, cost=float(cost[0]), stats=dict(zip(STATS, stats.tolist())),
-                history=hist[:nb_steps.value].copy(), status=st)
+                history=hist[:nb_steps.value].copy(), status=st, clusters=clusters)
 
 
 def max_threads():

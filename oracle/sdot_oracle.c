@@ -446,7 +446,7 @@ static int cell2( const od_pb *pb, long i, int brute, poly2 *P, poly2 *T ) {
     P->x[ 3 ] = pb->lo[ 0 ] - px; P->y[ 3 ] = pb->hi[ 1 ] - py; P->id[ 3 ] = -4;   /* left */
 #define CUT2( j ) do { \
         double qx = pb->pos[ 2 * ( j ) ] - px, qy = pb->pos[ 2 * ( j ) + 1 ] - py; \
-        double off = 0.5 * ( qx * qx + qy * qy + wi - wt( pb, j ) ); \
+        double off = 0.5 * ( ( wi - wt( pb, j ) ) + ( qx * qx + qy * qy ) ); \
         if ( clip2( P, qx, qy, off, ( int ) ( j ), T ) ) return OD_ERR_VERTICES; } while ( 0 )
     if ( brute ) {
         for ( long j = 0; j < pb->n && P->m; ++j ) if ( j != i ) CUT2( j );
@@ -569,9 +569,12 @@ static int clip3( poly3 *P, const double *n, double off, int cid ) {
             if ( q + 2 >= OD_MAXFV ) return -1;
             if ( s[ k ] <= 0 ) out[ q++ ] = P->v[ f ][ k ];
             if ( ( s[ k ] <= 0 ) != ( s[ k1 ] <= 0 ) ) {
-                double t = s[ k ] / ( s[ k ] - s[ k1 ] );
+                /* from the kept end, whichever face reports the edge: the two faces of an edge then make the same point
+                   to the bit (an edge nearly parallel to the plane would place its two copies far apart) */
+                const int ui = s[ k ] <= 0 ? k : k1, vi = s[ k ] <= 0 ? k1 : k;
+                double t = s[ ui ] / ( s[ ui ] - s[ vi ] );
                 v3 x;
-                for ( int a = 0; a < 3; ++a ) x.p[ a ] = P->v[ f ][ k ].p[ a ] + t * ( P->v[ f ][ k1 ].p[ a ] - P->v[ f ][ k ].p[ a ] );
+                for ( int a = 0; a < 3; ++a ) x.p[ a ] = P->v[ f ][ ui ].p[ a ] + t * ( P->v[ f ][ vi ].p[ a ] - P->v[ f ][ ui ].p[ a ] );
                 out[ q++ ] = x;
                 if ( nc >= 2 * OD_MAXF ) return -1;
                 cross[ nc++ ] = x;
@@ -811,7 +814,7 @@ static int cell3( const od_pb *pb, long i, int brute, poly3 *P ) {
     box3( P, lo, hi );
 #define CUT3( j ) do { \
         double q[ 3 ] = { pb->pos[ 3 * ( j ) ] - p[ 0 ], pb->pos[ 3 * ( j ) + 1 ] - p[ 1 ], pb->pos[ 3 * ( j ) + 2 ] - p[ 2 ] }; \
-        double off = 0.5 * ( dot3( q, q ) + wi - wt( pb, j ) ); \
+        double off = 0.5 * ( ( wi - wt( pb, j ) ) + dot3( q, q ) ); \
         if ( clip3( P, q, off, ( int ) ( j ) ) ) return OD_ERR_VERTICES; } while ( 0 )
     if ( brute ) {
         for ( long j = 0; j < pb->n && P->nf; ++j ) if ( j != i ) CUT3( j );
@@ -1034,6 +1037,49 @@ static int lap_cg( const od_lap *L, const double *b, double *x, double tol, int 
     return ok ? it : -1;
 }
 
+/* the direct solve of small systems, as the reference's CPU path factors its Laplacian (sdotplan/Linear.h:67-68): the rows and
+   columns 1..n-1 (x[ 0 ] = 0) by a dense Cholesky. Returns 0, or -1 when the grounded matrix is not positive definite */
+static int lap_dense( const od_lap *L, const double *b, double *x ) {
+    long m = L->n - 1;
+    x[ 0 ] = 0;
+    if ( m <= 0 ) return 0;
+    double *A = ( double * ) calloc( ( size_t ) m * m, sizeof( double ) );
+    for ( long i = 1; i < L->n; ++i ) {
+        A[ ( i - 1 ) * m + i - 1 ] += L->dia[ i ];
+        for ( long e = L->row[ i ]; e < L->row[ i + 1 ]; ++e )
+            if ( L->col[ e ] > 0 ) A[ ( i - 1 ) * m + L->col[ e ] - 1 ] -= L->c[ e ];
+    }
+    int ok = 1;
+    for ( long j = 0; j < m && ok; ++j ) {
+        double d = A[ j * m + j ];
+        for ( long k = 0; k < j; ++k ) d -= A[ j * m + k ] * A[ j * m + k ];
+        if ( ! ( d > 0 ) ) { ok = 0; break; }
+        d = sqrt( d );
+        A[ j * m + j ] = d;
+#pragma omp parallel for schedule( static )
+        for ( long i = j + 1; i < m; ++i ) {
+            double s = A[ i * m + j ];
+            for ( long k = 0; k < j; ++k ) s -= A[ i * m + k ] * A[ j * m + k ];
+            A[ i * m + j ] = s / d;
+        }
+    }
+    if ( ok ) {
+        double *y = x + 1;
+        for ( long i = 0; i < m; ++i ) {
+            double s = b[ i + 1 ];
+            for ( long k = 0; k < i; ++k ) s -= A[ i * m + k ] * y[ k ];
+            y[ i ] = s / A[ i * m + i ];
+        }
+        for ( long i = m - 1; i >= 0; --i ) {
+            double s = y[ i ];
+            for ( long k = i + 1; k < m; ++k ) s -= A[ k * m + i ] * y[ k ];
+            y[ i ] = s / A[ i * m + i ];
+        }
+    }
+    free( A );
+    return ok ? 0 : -1;
+}
+
 /* the Laplacian solve alone, for the tests: CSR from a neighbour table, b of zero sum */
 int od_laplacian_solve( long n, int cap, const int *nb, const int *nid, const double *nc, const double *b, double *x, double tol, int maxit ) {
     od_lap L;
@@ -1047,13 +1093,14 @@ int od_laplacian_solve( long n, int cap, const int *nb, const int *nid, const do
 /* THE SOLVE                                                                                       */
 /* ------------------------------------------------------------------------------------------------ */
 enum { O_TOL_ABS = 0, O_TOL_REL, O_MAXIT, O_MAX_BACKTRACKS, O_T_MIN, O_MULT_OK, O_RESIDUAL, O_POWER, O_SWITCH, O_LIN_TOL, O_LIN_MAXIT,
-       O_KEEP_START, O_CONTINUATION, O_CONV_THRESHOLD, O_CONV_S0, O_CONV_RATIO, O_CONV_MIN, O_BRUTE, O_CAP, NB_OPTIONS };
+       O_KEEP_START, O_CONTINUATION, O_CONV_THRESHOLD, O_CONV_S0, O_CONV_RATIO, O_CONV_MIN, O_BRUTE, O_CAP, O_AGG_MARGIN, NB_OPTIONS };
 enum { S_STATUS = 0, S_RESIDUAL, S_RESIDUAL0, S_NB_ITER, S_NB_DIAG, S_NB_BACKTRACKS, S_T_MAJORANT, S_T_DIAG, S_T_ASM, S_T_LIN, S_T_LIM, S_EPS,
        S_DOMAIN_MASS, S_NB_OVERFLOWED, S_NB_CELL_LIM, S_NB_LIMIT_ROUNDS, S_LIN_NB_HIERARCHIES, S_LIN_NB_ITER, S_LIN_WORST, S_START, S_T_TOTAL,
        S_NB_CONTINUATION_STEPS, S_MIN_START_MASS, S_IT_SWITCH, S_IT_DOUBLE, S_SCRATCH_BYTES, S_NB_CLUSTERS, S_NB_AGGREGATED, S_NB_DUPLICATES,
        S_RESIDUAL_FULL, S_NB_POLISH, NB_STATS };
 enum { RES_LIN = 0, RES_LOG = 1, RES_POWER = 2 };
-enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAX_ITER = 2, ST_STAGNATION = 3, ST_LINEAR_FAILURE = 4, ST_CAPACITY = 5, ST_FAILURE = 6 };
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAX_ITER = 2, ST_STAGNATION = 3, ST_LINEAR_FAILURE = 4, ST_CAPACITY = 5, ST_FAILURE = 6,
+       ST_CONVERGED_AGG = 7 };
 
 static double now_s( void ) {
 #ifdef _OPENMP
@@ -1069,6 +1116,10 @@ typedef struct {
     int *nb, *nid;
     double *nc, *nm;
     double *gauss_conv;             /* the gaussians at the width of the stage */
+    /* the aggregation of near-coincident seeds (sdotplan/Aggregation.h): margin, tolerance, union-find (NULL: none) */
+    double agg_margin, agg_tol_abs, agg_tol_rel;
+    int *agg_parent;
+    int agg_changed;
     int nb_diag;
     double t_diag;
     int status;
@@ -1165,6 +1216,45 @@ static void hist_push( od_hist *H, int it, double t, int nb_evals, long n, const
 }
 
 /* one stage of Newton from (w, a, facets of w); the accepted w and a come back in place */
+/* ---- the aggregation of near-coincident seeds (restates sdotplan/Aggregation.h:109-168, 229-250) ---- */
+static int agg_find( int *p, int i ) {
+    while ( p[ i ] != i ) { p[ i ] = p[ p[ i ] ]; i = p[ i ]; }
+    return i;
+}
+/* the pairs whose facet the doubles of the weights cannot place, c_ij ulp( max |w| ) margin > tau, merged */
+static void agg_detect( od_sweep *sw, const od_lap *L, const double *w, const double *nu ) {
+    if ( ! ( sw->agg_margin > 0 ) ) return;
+    const long n = L->n;
+    for ( long i = 0; i < n; ++i )
+        for ( long e = L->row[ i ]; e < L->row[ i + 1 ]; ++e ) {
+            const long j = L->col[ e ];
+            if ( j <= i ) continue;
+            const double wm = fmax( fabs( w[ i ] ), fabs( w[ j ] ) );
+            const double ulp = nextafter( wm, INFINITY ) - wm;
+            const double nm = fmin( nu[ i ], nu[ j ] );
+            const double tau = fmax( sw->agg_tol_abs, fmax( sw->agg_tol_rel * nm, 1e-12 * nm ) );
+            if ( ! ( L->c[ e ] * ulp * sw->agg_margin > tau ) ) continue;
+            if ( ! sw->agg_parent ) {
+                sw->agg_parent = ( int * ) malloc( n * sizeof( int ) );
+                for ( long k = 0; k < n; ++k ) sw->agg_parent[ k ] = ( int ) k;
+            }
+            int a = agg_find( sw->agg_parent, ( int ) i ), b = agg_find( sw->agg_parent, ( int ) j );
+            if ( a != b ) { sw->agg_parent[ a > b ? a : b ] = a < b ? a : b; sw->agg_changed = 1; }
+        }
+}
+/* the masses the tests read: each member of a cluster gets nu_i a_C / nu_C (members summed in index order) */
+static const double *agg_shares( od_sweep *sw, long n, const double *a, const double *nu, double *ae ) {
+    if ( ! sw->agg_parent ) return a;
+    double *sa = calloc( n, sizeof( double ) ), *sn = calloc( n, sizeof( double ) );
+    for ( long i = 0; i < n; ++i ) { int r = agg_find( sw->agg_parent, ( int ) i ); sa[ r ] += a[ i ]; sn[ r ] += nu[ i ]; }
+    for ( long i = 0; i < n; ++i ) {
+        int r = agg_find( sw->agg_parent, ( int ) i );
+        ae[ i ] = r == i && sn[ r ] == nu[ i ] ? a[ i ] : nu[ i ] * ( sn[ r ] > 0 ? sa[ r ] / sn[ r ] : 0.0 );
+    }
+    free( sa ); free( sn );
+    return ae;
+}
+
 static int newton_stage( od_sweep *sw, const double *o, const double *nu, double *w, double *a, double *stats, od_hist *H, int first_stage ) {
     long n = sw->pb.n;
     double *b = malloc( n * sizeof( double ) ), *d = malloc( n * sizeof( double ) ), *w2 = malloc( n * sizeof( double ) ), *a2 = malloc( n * sizeof( double ) );
@@ -1175,12 +1265,14 @@ static int newton_stage( od_sweep *sw, const double *o, const double *nu, double
     double t_last = 1, eps = 0;
     int nb_iter = 0, nb_bt = 0, it_switch = -1;
     double t_asm = 0, t_lin = 0;
+    double *ae = malloc( n * sizeof( double ) ), *ae2 = malloc( n * sizeof( double ) );
     hist_push( H, 0, 0, 1, n, a, nu, sw->nb_diag );
     const int maxit = ( int ) o[ O_MAXIT ];
     for ( int it = 0; it < maxit; ++it ) {
+        const double *A = agg_shares( sw, n, a, nu, ae );      /* the tests read the clusters' masses */
         double worst = 0, worst_rel = 0;
         for ( long i = 0; i < n; ++i ) {
-            double e = fabs( nu[ i ] - a[ i ] );
+            double e = fabs( nu[ i ] - A[ i ] );
             if ( e > worst ) worst = e;
             if ( e / nu[ i ] > worst_rel ) worst_rel = e / nu[ i ];
         }
@@ -1188,19 +1280,21 @@ static int newton_stage( od_sweep *sw, const double *o, const double *nu, double
         rhs_of( n, a, nu, res_cur, o[ O_POWER ], b );
         project_on_range( n, b );
         if ( it == 0 ) {
-            eps = 0.5 * fmin( vmin( n, nu ), vmin( n, a ) );
+            eps = 0.5 * fmin( vmin( n, nu ), vmin( n, A ) );
             if ( first_stage ) { stats[ S_EPS ] = eps; stats[ S_RESIDUAL0 ] = worst; }
         }
-        double nr = merit( n, a, nu, res_cur, o[ O_POWER ] );
+        double nr = merit( n, A, nu, res_cur, o[ O_POWER ] );
         stats[ S_RESIDUAL ] = worst;
         if ( worst <= o[ O_TOL_ABS ] || ( o[ O_TOL_REL ] > 0 && worst_rel <= o[ O_TOL_REL ] ) ) { status = ST_CONVERGED; break; }
         ++nb_iter;
         double t0 = now_s();
         od_lap L;
         lap_build( &L, n, cap, sw->nb, sw->nid, sw->nc );
+        agg_detect( sw, &L, w, nu );
         t_asm += now_s() - t0;
         t0 = now_s();
         int lit = lap_cg( &L, b, d, o[ O_LIN_TOL ], ( int ) o[ O_LIN_MAXIT ] );
+        if ( lit < 0 && n <= 4096 && lap_dense( &L, b, d ) == 0 ) lit = 0;    /* CG lost to the conditioning: factor */
         t_lin += now_s() - t0;
         lap_free( &L );
         if ( lit < 0 ) { status = ST_LINEAR_FAILURE; break; }
@@ -1217,7 +1311,8 @@ static int newton_stage( od_sweep *sw, const double *o, const double *nu, double
             sweep( sw, w2, a2 );
             sw->nb = sb; sw->nid = si; sw->nc = sc; sw->nm = sm;
             ++nb_evals;
-            double m2 = vmin( n, a2 ), n2r = merit( n, a2, nu, res_cur, o[ O_POWER ] );
+            const double *A2 = agg_shares( sw, n, a2, nu, ae2 );
+            double m2 = vmin( n, A2 ), n2r = merit( n, A2, nu, res_cur, o[ O_POWER ] );
             if ( m2 >= eps && isfinite( n2r ) && n2r <= ( 1 - t / 2 ) * nr && n2r < nr ) { taken = 1; break; }
             int hl = hopeless_refused( &hope, t, n2r, nr, m2 >= eps && isfinite( n2r ) );
             t /= 2;
@@ -1236,11 +1331,13 @@ static int newton_stage( od_sweep *sw, const double *o, const double *nu, double
         hist_push( H, it + 1, t, nb_evals, n, a, nu, sw->nb_diag );
     }
     if ( status == ST_RUNNING ) {
+        const double *A = agg_shares( sw, n, a, nu, ae );
         double worst = 0;
-        for ( long i = 0; i < n; ++i ) worst = fmax( worst, fabs( nu[ i ] - a[ i ] ) );
+        for ( long i = 0; i < n; ++i ) worst = fmax( worst, fabs( nu[ i ] - A[ i ] ) );
         stats[ S_RESIDUAL ] = worst;
         status = ST_MAX_ITER;
     }
+    free( ae ); free( ae2 );
     stats[ S_NB_ITER ] += nb_iter;
     stats[ S_NB_BACKTRACKS ] += nb_bt;
     stats[ S_T_ASM ] += t_asm;
@@ -1265,13 +1362,16 @@ static void gauss_at( od_sweep *sw, const double *dval, int dim, double s ) {
  * cost [1], stats [NB_STATS], hist [cap_steps, 8] (may be NULL) and the number of rows written. */
 int od_solve( int dim, long n, const double *pos, const double *nu_in, const double *w0, const double *box, int dkind, const double *dpar,
               const double *dval, const double *opts, double *weights, double *masses, double *bary, double *cost, double *stats,
-              double *hist, long cap_steps, long *nb_steps ) {
+              double *hist, long cap_steps, long *nb_steps, int *clusters ) {
     double t_begin = now_s();
     od_sweep sw;
     memset( &sw, 0, sizeof( sw ) );
     init_pb( &sw.pb, dim, n, pos, NULL, box, dkind, dpar, dval );
     sw.brute = ( int ) opts[ O_BRUTE ];
     sw.cap = ( int ) opts[ O_CAP ];
+    sw.agg_margin = opts[ O_AGG_MARGIN ];
+    sw.agg_tol_abs = opts[ O_TOL_ABS ];
+    sw.agg_tol_rel = opts[ O_TOL_REL ];
     sw.nb = malloc( n * sizeof( int ) );
     sw.nid = malloc( ( size_t ) n * sw.cap * sizeof( int ) );
     sw.nc = malloc( ( size_t ) n * sw.cap * sizeof( double ) );
@@ -1393,6 +1493,27 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     stats[ S_NB_CONTINUATION_STEPS ] = nsc;
     stats[ S_MIN_START_MASS ] = min_start_mass;
     stats[ S_RESIDUAL_FULL ] = stats[ S_RESIDUAL ];
+    if ( clusters ) for ( long i = 0; i < n; ++i ) clusters[ i ] = sw.agg_parent ? agg_find( sw.agg_parent, ( int ) i ) : ( int ) i;
+    if ( sw.agg_parent ) {
+        /* the full problem's residual; "converged (aggregated)" when only the clusters' masses pass (sdotplan/Solve.h:300-306) */
+        double wf = 0, wfr = 0;
+        long ncl = 0, nagg = 0;
+        int *size = calloc( n, sizeof( int ) );
+        for ( long i = 0; i < n; ++i ) {
+            const double e = fabs( a[ i ] - nu_s[ i ] );
+            wf = fmax( wf, e );
+            wfr = fmax( wfr, e / nu_s[ i ] );
+            ++size[ agg_find( sw.agg_parent, ( int ) i ) ];
+        }
+        for ( long i = 0; i < n; ++i ) if ( size[ i ] > 1 ) { ++ncl; nagg += size[ i ]; }
+        free( size );
+        stats[ S_RESIDUAL_FULL ] = wf;
+        stats[ S_NB_CLUSTERS ] = ( double ) ncl;
+        stats[ S_NB_AGGREGATED ] = ( double ) nagg;
+        if ( status == ST_CONVERGED && ! ( wf <= opts[ O_TOL_ABS ] || ( opts[ O_TOL_REL ] > 0 && wfr <= opts[ O_TOL_REL ] ) ) )
+            stats[ S_STATUS ] = ST_CONVERGED_AGG;
+        free( sw.agg_parent );
+    }
     if ( nb_steps ) *nb_steps = H.nb_steps;
     free( nu ); free( w ); free( a ); free( wt0 ); free( at0 ); free( nu_s );
     free( sw.nb ); free( sw.nid ); free( sw.nc ); free( sw.nm ); free( sw.gauss_conv );

@@ -394,7 +394,9 @@ __device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int l
             qx = P.pos[ 2 * ( size_t ) j ] - px;
             qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
             double qw = P.w ? P.w[ j ] : 0.0;
-            off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+            // the weights' difference first: added to a weight, the |q|^2 of two seeds 1e-10 apart is lost and the two
+            // cells of the pair cut planes |q| apart
+            off = 0.5 * ( ( wi - qw ) + ( qx * qx + qy * qy ) );
         }
         // the parallel pre-test: does candidate `lane` cut the current polygon at all?
         bool cuts = false;
@@ -857,7 +859,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
                 if ( j == s ) continue;
                 double qx = P.pos[ 2 * ( size_t ) j ] - px, qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
                 double qw = P.w ? P.w[ j ] : 0.0;
-                double off = 0.5 * ( qx * qx + qy * qy + wi - qw );
+                double off = 0.5 * ( ( wi - qw ) + ( qx * qx + qy * qy ) );
                 bool moved;
                 int nm = big_clip( *S, *D, m, lane, qx, qy, off, j, moved );
                 if ( nm < 0 ) { overflow = true; break; }

@@ -256,7 +256,7 @@ __device__ void cut_by_ranges3( C3 &C, const ProbDev &P, int lane, int s, double
             qy = P.pos[ 3 * ( size_t ) j + 1 ] - py;
             qz = P.pos[ 3 * ( size_t ) j + 2 ] - pz;
             double qw = P.w ? P.w[ j ] : 0.0;
-            off = 0.5 * ( qx * qx + qy * qy + qz * qz + wi - qw );
+            off = 0.5 * ( ( wi - qw ) + ( qx * qx + qy * qy + qz * qz ) );
         }
         bool cuts = false;
         for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] > off;

@@ -379,7 +379,9 @@ void free_geometry( Ctx &c, Geometry &G ) {
 // ---- the solve ---------------------------------------------------------------------------------------------------------
 enum JState { J_START0, J_START_VOR, J_START_SIM, J_STAGE_DIAG, J_REPORT, J_ITER, J_CG, J_TRIAL, J_FINAL, J_DONE };
 enum Pend : unsigned { P_NEWTON = 1, P_GAUGE = 2, P_TRIAL = 4, P_RESCALE = 8, P_SET_W2 = 16, P_ZERO_W2 = 32, P_DENSITY = 64 };
-enum NStatus { NS_RUNNING = 0, NS_CONVERGED = 1, NS_MAX_ITER = 2, NS_STAGNATION = 3, NS_LINEAR_FAILURE = 4, NS_CAPACITY = 5, NS_FAILURE = 6 };
+enum NStatus { NS_RUNNING = 0, NS_CONVERGED = 1, NS_MAX_ITER = 2, NS_STAGNATION = 3, NS_LINEAR_FAILURE = 4, NS_CAPACITY = 5, NS_FAILURE = 6,
+               NS_CONVERGED_AGG = 7 };
+constexpr int AGG_CAP = 4096;        // near-coincident pairs one Laplacian can report
 enum StatIdx {
     ST_STATUS = 0, ST_RESIDUAL, ST_RESIDUAL0, ST_NB_ITER, ST_NB_DIAG, ST_NB_BACKTRACKS, ST_T_MAJORANT, ST_T_DIAG, ST_T_ASM, ST_T_LIN, ST_T_LIM, ST_EPS,
     ST_DOMAIN_MASS, ST_NB_OVERFLOWED, ST_NB_CELL_LIM, ST_NB_LIMIT_ROUNDS, ST_LIN_NB_HIERARCHIES, ST_LIN_NB_ITER, ST_LIN_WORST, ST_START, ST_T_TOTAL,
@@ -444,6 +446,15 @@ struct SolveJob {
     int err_code = 0;
     std::string err_msg;
     long long err_id = -1;
+    // the aggregation of near-coincident seeds (sdotplan/Aggregation.h): a union-find over the ranks, the clusters
+    // (CSR over ranks, members increasing), their device copy [ begins | members ] and the shares the tests read
+    double agg_margin = 0;
+    int2 *agg_pairs = nullptr;
+    std::vector<int> agg_parent, cl_begin, cl_members;
+    int *d_cl = nullptr;
+    double *ae = nullptr;
+    int ncl = 0;
+    bool full_set = false;              // stats[ residual_full ] computed on the full problem
 };
 
 static size_t mg_bytes( int dim, long n, int cap );
@@ -469,7 +480,7 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     J.ovf_cap = int( n ) + 4096;
     size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                    size_t( n ) * 4 + size_t( J.nch_cells ) * NB_REPORT * 8 + size_t( J.nch_vec ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) +
-                   2 * ( size_t( J.ovf_cap ) * 12 + 16 ) + 48 * 256;
+                   2 * ( size_t( J.ovf_cap ) * 12 + 16 ) + ( J.agg_margin > 0 ? AGG_CAP * sizeof( int2 ) : 0 ) + 49 * 256;
     J.mem_bytes = bytes;
     J.mem = ( char * ) dalloc( c, bytes );
     Arena A{ J.mem, bytes, 0 };
@@ -481,6 +492,7 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
         J.nb[ k ] = A.take<int>( n ); J.nid[ k ] = A.take<int>( size_t( n ) * cap ); J.nc[ k ] = A.take<double>( size_t( n ) * cap );
         J.ovf_count[ k ] = A.take<int>( 4 ); J.ovf_ids[ k ] = A.take<int>( J.ovf_cap ); J.ovf_c[ k ] = A.take<double>( J.ovf_cap );
     }
+    if ( J.agg_margin > 0 ) J.agg_pairs = A.take<int2>( AGG_CAP );
     J.row_ptr = A.take<int>( n + 1 );
     J.col = A.take<int>( size_t( n ) * cap );
     J.val = A.take<double>( size_t( n ) * cap );
@@ -589,6 +601,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         build_geometry( c, J->G, D.dim, D.n, D.positions, D.box_lo, D.box_hi, D.density, D.memory );
         J->cap = D.dim == 2 ? CAP2 : CAP3;
         std::memcpy( J->opt, desc.options, sizeof( J->opt ) );
+        J->agg_margin = J->opt[ SDOT_OPT_AGG_MARGIN ];
         for ( int k = 0; k < SDOT_NB_STATS; ++k ) J->stats[ k ] = 0;
         const long n = D.n;
         if ( desc.nu ) to_host_vec( c, J->nu_user, desc.nu, n, D.memory );
@@ -611,7 +624,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         alloc_job( c, *J );
         if ( int( J->opt[ SDOT_OPT_LIN_METHOD ] ) == 1 ) alloc_mg( c, *J );
         J->slot = take_slot( c );
-        CK( cudaMemsetAsync( c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR, 0, sizeof( double ), c.stream ) );
+        CK( cudaMemsetAsync( c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR, 0, 2 * sizeof( double ), c.stream ) );
         CK( cudaMemcpyAsync( &J->rank0, J->G.rank_of, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
         Launch L = c.L();
@@ -639,6 +652,8 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
 void job_destroy( Ctx &c, SolveJob *J ) {
     if ( ! J ) return;
     if ( J->mg_mem ) dfree( c, J->mg_mem );
+    if ( J->d_cl ) dfree( c, J->d_cl );
+    if ( J->ae ) dfree( c, J->ae );
     if ( J->mem ) dfree( c, J->mem );
     if ( J->G.mem ) free_geometry( c, J->G );
     if ( J->slot >= 0 ) give_slot( c, J->slot );
@@ -724,6 +739,7 @@ static void set_stage_density( Ctx &c, SolveJob &J ) {
 }
 
 static void end_stage( Ctx &c, SolveJob &J );
+static void full_residual( Ctx &c, SolveJob &J, double &worst, double &worst_rel );
 
 static void begin_iterations( Ctx &c, SolveJob &J ) {
     // the domain mass of this density and the targets rescaled to it (sdotplan/Solve.h:250-257)
@@ -787,6 +803,15 @@ static void end_stage( Ctx &c, SolveJob &J ) {
         J.stage = int( J.scales.size() ) - 1;
         set_stage_density( c, J );
     }
+    if ( J.nstatus == NS_CONVERGED && J.ncl > 0 ) {
+        // the tests read the clusters' masses: the full problem's residual, and "converged (aggregated)" when only the
+        // aggregated problem passes (sdotplan/Solve.h:300-306)
+        double wf, wfr;
+        full_residual( c, J, wf, wfr );
+        J.stats[ ST_RESIDUAL_FULL ] = wf;
+        J.full_set = true;
+        if ( ! ( wf <= J.opt[ SDOT_OPT_TOL_ABS ] || ( J.opt[ SDOT_OPT_TOL_REL ] > 0 && wfr <= J.opt[ SDOT_OPT_TOL_REL ] ) ) ) J.nstatus = NS_CONVERGED_AGG;
+    }
     J.stats[ ST_STATUS ] = J.nstatus;
     J.state = J_FINAL;
 }
@@ -840,7 +865,76 @@ static void accept_trial( SolveJob &J ) {
 }
 
 // after the tick's read-back: the decisions of every job
+// ---- the aggregation of near-coincident seeds (sdotplan/Aggregation.h) ------------------------------------------------
+static int uf_find( std::vector<int> &p, int i ) {
+    while ( p[ i ] != i ) { p[ i ] = p[ p[ i ] ]; i = p[ i ]; }
+    return i;
+}
+
+// the pairs the last Laplacian showed: merged (latched, a cluster only grows), the clusters rebuilt and uploaded
+// (sdotplan/Aggregation.h:109-141, 229-250)
+static void agg_update( Ctx &c, SolveJob &J ) {
+    double *cnt = c.hscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_AGG;
+    const int k = std::min( int( *cnt ), AGG_CAP );
+    if ( k <= 0 ) return;
+    std::vector<int2> pairs( k );
+    CK( cudaMemcpy( pairs.data(), J.agg_pairs, size_t( k ) * sizeof( int2 ), cudaMemcpyDeviceToHost ) );
+    CK( cudaMemsetAsync( c.dscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_AGG, 0, sizeof( double ), c.stream ) );
+    *cnt = 0;
+    const int n = int( J.G.n );
+    if ( J.agg_parent.empty() ) {
+        J.agg_parent.resize( n );
+        for ( int i = 0; i < n; ++i ) J.agg_parent[ i ] = i;
+    }
+    bool changed = false;
+    for ( const int2 &p : pairs ) {
+        int a = uf_find( J.agg_parent, p.x ), b = uf_find( J.agg_parent, p.y );
+        if ( a == b ) continue;
+        J.agg_parent[ std::max( a, b ) ] = std::min( a, b );
+        changed = true;
+    }
+    if ( ! changed ) return;
+    std::vector<int> size( n, 0 ), id( n, -1 );
+    for ( int i = 0; i < n; ++i ) ++size[ uf_find( J.agg_parent, i ) ];
+    J.cl_begin.assign( 1, 0 );
+    for ( int i = 0; i < n; ++i )
+        if ( J.agg_parent[ i ] == i && size[ i ] > 1 ) { id[ i ] = int( J.cl_begin.size() ) - 1; J.cl_begin.push_back( J.cl_begin.back() + size[ i ] ); }
+    J.ncl = int( J.cl_begin.size() ) - 1;
+    J.cl_members.assign( J.cl_begin.back(), 0 );
+    std::vector<int> at( J.cl_begin.begin(), J.cl_begin.end() - 1 );
+    for ( int i = 0; i < n; ++i ) {
+        const int cidx = id[ uf_find( J.agg_parent, i ) ];
+        if ( cidx >= 0 ) J.cl_members[ at[ cidx ]++ ] = i;
+    }
+    std::vector<int> dev( J.cl_begin );
+    dev.insert( dev.end(), J.cl_members.begin(), J.cl_members.end() );
+    if ( J.d_cl ) dfree( c, J.d_cl );
+    J.d_cl = ( int * ) dalloc( c, dev.size() * sizeof( int ) );
+    CK( cudaMemcpyAsync( J.d_cl, dev.data(), dev.size() * sizeof( int ), cudaMemcpyHostToDevice, c.stream ) );
+    if ( ! J.ae ) J.ae = ( double * ) dalloc( c, size_t( n ) * 8 );
+    CK( cudaStreamSynchronize( c.stream ) );       // `dev` leaves scope
+    J.stats[ ST_NB_CLUSTERS ] = J.ncl;
+    J.stats[ ST_NB_AGGREGATED ] = double( J.cl_members.size() );
+}
+
+// the residual of the full problem (every cell its own target), at the accepted masses: max |a - nu| and its relative
+// form (sdotplan/Aggregation.h:199-209)
+static void full_residual( Ctx &c, SolveJob &J, double &worst, double &worst_rel ) {
+    const long n = J.G.n;
+    std::vector<double> a( n ), nu( n );
+    CK( cudaMemcpyAsync( a.data(), J.a, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaMemcpyAsync( nu.data(), J.nu, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    worst = worst_rel = 0;
+    for ( long i = 0; i < n; ++i ) {
+        const double e = std::fabs( a[ i ] - nu[ i ] );
+        worst = std::max( worst, e );
+        worst_rel = std::max( worst_rel, e / nu[ i ] );
+    }
+}
+
 static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
+    if ( J.agg_margin > 0 ) agg_update( c, J );
     if ( had_diag && c.hscal[ size_t( J.slot ) * SLOT_DOUBLES + SLOT_ERR ] != 0 ) {
         // a cell past every capacity: this solve stops with the reference's "card capacity" status (the others go on);
         // its outputs are the moments at the last accepted weights
@@ -997,6 +1091,14 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.nchunk = J.nch_vec;
     V.active = 1;
     V.precond = J.mg_L > 0 ? 1 : 0;
+    if ( J.agg_margin > 0 ) {
+        V.agg_pairs = J.agg_pairs;
+        V.agg_cap = AGG_CAP;
+        V.agg_count = c.dscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_AGG;
+        V.agg_margin = J.agg_margin;
+        V.agg_tol_abs = J.opt[ SDOT_OPT_TOL_ABS ];
+        V.agg_tol_rel = J.opt[ SDOT_OPT_TOL_REL ];
+    }
     return V;
 }
 
@@ -1229,6 +1331,9 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             launch_lap_count( L, B->dv, B->dch, nch );
             launch_lap_scan( L, B->dv, int( B->v.size() ) );
             launch_lap_fill( L, B->dv, B->dch, nch );
+            bool agg = false;
+            for ( auto &v : B->v ) agg |= v.agg_pairs != nullptr;
+            if ( agg ) launch_agg_detect( L, B->dv, B->dch, nch );
             launch_rhs( L, B->dv, B->dch, nch );
             if ( B->mg() ) {
                 B->build( L, c.derr );
@@ -1258,6 +1363,34 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     Launch L = c.L();
     // A. the diagrams
     std::vector<ProbDev> P2, P3, PR;
+    // the diagrams of solves with clusters: their reports again, from the clusters' shares of the masses
+    struct AggDiag { SolveJob *J; ProbDev P; };
+    std::vector<AggDiag> AG;
+    auto agg_reports = [&]() {
+        if ( AG.empty() ) return;
+        std::vector<ProbDev> Q;
+        std::vector<Chunk> QC;
+        for ( auto &e : AG ) {
+            SolveJob *J = e.J;
+            CK( cudaMemcpyAsync( J->ae, e.P.mass, size_t( J->G.n ) * 8, cudaMemcpyDeviceToDevice, c.stream ) );
+            launch_agg_shares( L, e.P.mass, J->nu, J->d_cl, J->d_cl + J->ncl + 1, J->ncl, J->ae );
+            ProbDev P = e.P;
+            P.mass = J->ae;
+            const int qi = int( Q.size() );
+            Q.push_back( P );
+            int k = 0;
+            for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) QC.push_back( Chunk{ qi, b, std::min( J->G.n, b + CHUNK ), k } );
+        }
+        const size_t oq = ( Q.size() * sizeof( ProbDev ) + 255 ) & ~size_t( 255 );
+        std::vector<char> buf( oq + QC.size() * sizeof( Chunk ) );
+        std::memcpy( buf.data(), Q.data(), Q.size() * sizeof( ProbDev ) );
+        std::memcpy( buf.data() + oq, QC.data(), QC.size() * sizeof( Chunk ) );
+        char *d = ( char * ) dalloc( c, buf.size() );
+        c.desc_spill.push_back( d );
+        CK( cudaMemcpyAsync( d, buf.data(), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
+        launch_report( L, reinterpret_cast<ProbDev *>( d ), reinterpret_cast<Chunk *>( d + oq ), int( QC.size() ) );
+        CK( cudaStreamSynchronize( c.stream ) );       // `buf` leaves scope
+    };
     std::vector<Chunk> C2, C3, CR;
     std::vector<SolveJob *> with_diag;
     for ( SolveJob *J : jobs ) {
@@ -1288,6 +1421,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             P.nchunk = J->nch_cells;
         }
         if ( R.moments ) { P.first = J->obary; P.cost = J->ocost; }
+        if ( J->ncl > 0 && R.report >= 0 ) AG.push_back( { J, P } );
         std::vector<ProbDev> &PP = R.report_only ? PR : ( J->G.dim == 2 ? P2 : P3 );
         std::vector<Chunk> &CC = R.report_only ? CR : ( J->G.dim == 2 ? C2 : C3 );
         int pi = int( PP.size() );
@@ -1363,6 +1497,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         launch_report( L, reinterpret_cast<ProbDev *>( d ), reinterpret_cast<Chunk *>( d + o2 ), int( CR.size() ) );
         c.timer.end( c.stream );
     }
+    agg_reports();
     // B. CG iterations
     VecBatch cgj, cgm;
     std::vector<SolveJob *> with_cg;
@@ -1423,6 +1558,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             Chunk *dc = reinterpret_cast<Chunk *>( upload_desc_at( c, rc.data(), rc.size() * sizeof( Chunk ), big_probs.size() * sizeof( ProbDev ) ) );
             launch_report( L, dp, dc, int( rc.size() ) );
         }
+        agg_reports();
         CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
@@ -1472,7 +1608,22 @@ void job_outputs( Ctx &c, SolveJob *J, sdot_solve_out &out, int memory ) {
         else *out.cost = cost;
     }
     J->stats[ ST_DOMAIN_MASS ] = J->domain_mass;
-    J->stats[ ST_RESIDUAL_FULL ] = J->stats[ ST_RESIDUAL ];
+    if ( ! J->full_set ) J->stats[ ST_RESIDUAL_FULL ] = J->stats[ ST_RESIDUAL ];
+    if ( out.clusters ) {
+        // each seed's cluster by its smallest user index
+        std::vector<int32_t> cl( n );
+        for ( long i = 0; i < n; ++i ) cl[ i ] = int32_t( i );
+        std::vector<int> user( n );
+        if ( J->ncl > 0 ) {
+            CK( cudaMemcpy( user.data(), J->G.user, n * sizeof( int ), cudaMemcpyDeviceToHost ) );
+            for ( int k = 0; k < J->ncl; ++k ) {
+                int rep = INT32_MAX;
+                for ( int q = J->cl_begin[ k ]; q < J->cl_begin[ k + 1 ]; ++q ) rep = std::min( rep, user[ J->cl_members[ q ] ] );
+                for ( int q = J->cl_begin[ k ]; q < J->cl_begin[ k + 1 ]; ++q ) cl[ user[ J->cl_members[ q ] ] ] = rep;
+            }
+        }
+        CK( cudaMemcpy( out.clusters, cl.data(), n * sizeof( int32_t ), memory == SDOT_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost ) );
+    }
     J->stats[ ST_IT_DOUBLE ] = -1;
     std::memcpy( out.stats, J->stats, sizeof( out.stats ) );
     int rows = int( J->hist.size() / SDOT_NB_HIST );

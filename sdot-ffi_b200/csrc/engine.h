@@ -53,7 +53,8 @@ struct Ctx {
     Launch L() { return Launch{ stream, &launches, &timer }; }
 };
 constexpr int SLOT_ERR = 2 * NB_REPORT + NB_SC;                 // a problem's capacity-failure flag
-constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 1;
+constexpr int SLOT_AGG = SLOT_ERR + 1;                           // the near-coincident pairs its last Laplacian showed
+constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 2;
 
 void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
 void ctx_release( Ctx &c );

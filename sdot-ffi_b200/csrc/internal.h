@@ -154,6 +154,12 @@ struct VecDev {
     int chunk0, nchunk;
     int active;
     int precond;                  // 0 Jacobi, 1 multigrid (the V-cycle writes z)
+    // the detection of near-coincident pairs on this Laplacian (NULL: off): the pairs (i < j, ranks) whose facet the
+    // doubles of the weights cannot place within the tolerance, c_ij ulp( max |w| ) margin > tau
+    int2 *agg_pairs;
+    int agg_cap;
+    double *agg_count;
+    double agg_margin, agg_tol_abs, agg_tol_rel;
 };
 // one level of the multigrid preconditioner of one problem (mg.cu)
 constexpr int MG_BOTTOM = 32;          // the coarsest level has at most this many rows (dense inverse)
@@ -280,6 +286,10 @@ void launch_rhs( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the pairs the aggregation merges (VecDev.agg_*)
+void launch_agg_detect( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the cluster shares of the masses: ae[ i ] = nu[ i ] a_C / nu_C for the members i of each cluster C (others untouched)
+void launch_agg_shares( const Launch &L, const double *a, const double *nu, const int *cl_begin, const int *cl_members, int ncl, double *ae );
 // the multigrid-preconditioned CG: init in two halves around the first V-cycle, then per iteration
 // spmv -> update -> V-cycle -> r.z -> p
 void launch_cg_init0( const Launch &L, const VecDev *v, const Chunk *ch, int nch );

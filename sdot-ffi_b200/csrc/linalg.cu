@@ -498,4 +498,51 @@ void launch_gather_vec( const Launch &L, const double *user_vals, const int *use
     ++*L.launches;
 }
 
+// ---- the aggregation of near-coincident seeds (sdotplan/Aggregation.h:1-44, 229-250) ---------------------------------
+// A facet's plane moves by ( w_i - w_j ) / ( 2 |p_i - p_j| ): the doubles of the weights place it no better than
+// m_ij = c_ij ulp( max( |w_i|, |w_j| ) ) of mass.  The pair is merged when m_ij margin > tau_ij,
+// tau_ij = max( tol_abs, tol_rel nu, 1e-12 nu ), nu = min( nu_i, nu_j ).
+__global__ void __launch_bounds__( VT ) k_agg_detect( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active || ! V.agg_pairs || ! ( V.agg_margin > 0 ) ) return;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) {
+            const int j = V.col[ e ];
+            if ( j <= i ) continue;
+            const double wm = fmax( fabs( V.w[ i ] ), fabs( V.w[ j ] ) );
+            const double ulp = __longlong_as_double( __double_as_longlong( wm ) + 1 ) - wm;     // the spacing of the doubles at wm
+            const double nm = fmin( V.nu[ i ], V.nu[ j ] );
+            const double tau = fmax( V.agg_tol_abs, fmax( V.agg_tol_rel * nm, 1e-12 * nm ) );
+            if ( V.val[ e ] * ulp * V.agg_margin > tau ) {
+                const int k = int( atomicAdd( V.agg_count, 1.0 ) );
+                if ( k < V.agg_cap ) V.agg_pairs[ k ] = make_int2( i, j );
+            }
+        }
+    }
+}
+
+void launch_agg_detect( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_agg_detect<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// one thread per cluster: its members' masses summed in member order, each member's share of it
+__global__ void k_agg_shares( const double *__restrict__ a, const double *__restrict__ nu, const int *__restrict__ clb,
+                              const int *__restrict__ clm, int ncl, double *ae ) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( c >= ncl ) return;
+    double sa = 0, sn = 0;
+    for ( int k = clb[ c ]; k < clb[ c + 1 ]; ++k ) { sa += a[ clm[ k ] ]; sn += nu[ clm[ k ] ]; }
+    const double r = sn > 0 ? sa / sn : 0.0;
+    for ( int k = clb[ c ]; k < clb[ c + 1 ]; ++k ) ae[ clm[ k ] ] = nu[ clm[ k ] ] * r;
+}
+
+void launch_agg_shares( const Launch &L, const double *a, const double *nu, const int *cl_begin, const int *cl_members, int ncl, double *ae ) {
+    if ( ncl <= 0 ) return;
+    k_agg_shares<<<( ncl + 127 ) / 128, 128, 0, L.stream>>>( a, nu, cl_begin, cl_members, ncl, ae );
+    ++*L.launches;
+}
+
 } // namespace sdot

@@ -24,6 +24,12 @@ _INT_STATS = ("nb_iter", "nb_diag", "nb_backtracks", "nb_overflowed", "nb_cell_l
               "nb_continuation_steps", "scratch_bytes", "nb_clusters", "nb_aggregated", "nb_duplicates", "nb_polish")
 
 
+#: the aggregation's margin `kappa` (SdotPlanNd.py:118): a pair is merged when its floor c_ij ulp(w) is within kappa of
+#: the tolerance; and the weight gap of an exact duplicate, relative to the cloud's squared extent (SdotPlanNd.py:121)
+_AGGREGATE_MARGIN = 4.0
+_DUPLICATE_GAP = 1e-6
+
+
 def exact_duplicates(positions):
     """`( dup, rep )`: each exact duplicate and the smallest index at its position (SdotPlanNd.py:124-148)"""
     P = np.ascontiguousarray(np.asarray(positions, dtype=np.float64)) + 0.0
@@ -55,7 +61,8 @@ def solver_options(settings, n):
                 switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-8), lin_maxit=int(tun.linear_maxit or 20000),
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
-                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0)
+                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0,
+                agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0))
 
 
 def _box_of(problem):
@@ -81,10 +88,13 @@ class SdotPlanNd:
             self.problem = problem
             src, dst = problem.source, problem.target
             n, d = src.nb_diracs, src.nb_dims
-            if settings.aggregate:
-                dup, _ = exact_duplicates(src.positions)
-                if len(dup):
-                    raise NotImplementedError(f"{len(dup)} exact duplicate seeds: their aggregation is not built yet (remove the duplicates)")
+            # EXACT DUPLICATES (sdotplan/Aggregation.h:24-31): each keeps an empty cell (its weight its representative's
+            # minus a gap) and its representative (the smallest index at that position) carries its target.  An empty cell
+            # cuts no other, so the solve runs on the cloud without them and their outputs are written back after it.
+            dup, rep = exact_duplicates(src.positions) if settings.aggregate else (np.zeros(0, np.int64), np.zeros(0, np.int64))
+            self._dups = (dup, rep)
+            keep = np.setdiff1d(np.arange(n), dup) if len(dup) else None
+            self._keep = keep
             plan = settings.ot_plan if settings.ot_plan is not None else warm
             if settings.weights0 is not None:
                 w0, self._warm_start = np.asarray(settings.weights0, dtype=np.float64).reshape(-1), "weights0"
@@ -100,7 +110,13 @@ class SdotPlanNd:
             lo, hi = _box_of(problem)
             self._box = (lo, hi)
             self._settings = settings
-            pbs.append((src.positions, src.weights, w0, lo, hi, dst._sdot_density()))
+            P, nu = src.positions, src.weights
+            if keep is not None:
+                nu = np.full(n, 1.0 / n) if nu is None else np.asarray(nu, dtype=np.float64).reshape(-1).copy()
+                np.add.at(nu, rep, nu[dup])
+                P, nu = P[keep], nu[keep]
+                w0 = None if w0 is None else np.asarray(w0, dtype=np.float64).reshape(-1)[keep]
+            pbs.append((P, nu, w0, lo, hi, dst._sdot_density()))
             opts.append(solver_options(settings, n))
             plans.append(self)
         results = _lib.solve_batch(pbs, opts, cap_history=8 * (settings.max_iter + 1) + 64)
@@ -112,7 +128,27 @@ class SdotPlanNd:
             self._check_converged(settings)
         return plans
 
+    def _expand(self, r):
+        """the outputs of the solve without the exact duplicates, written for every seed"""
+        dup, rep = self._dups
+        keep = self._keep
+        P = np.asarray(self.problem.source.positions, dtype=np.float64)
+        n, d = P.shape
+        w, m, b, cl = np.zeros(n), np.zeros(n), P.copy(), np.arange(n, dtype=np.int64)
+        w[keep], m[keep], b[keep] = r["weights"], r["masses"], r["barycentres"]
+        cl[keep] = keep[np.asarray(r["clusters"], dtype=np.int64)]
+        ext = P.max(axis=0) - P.min(axis=0)
+        gap = _DUPLICATE_GAP * max(float((P * P).sum(axis=1).max()), float((ext * ext).sum()), 1e-300)
+        count = {}
+        for i, j in zip(dup, rep):
+            count[j] = count.get(j, 0) + 1
+            w[i] = w[j] - gap * count[j]
+            cl[i] = cl[j]
+        return dict(r, weights=w, masses=m, barycentres=b, clusters=cl)
+
     def _read(self, r, settings):
+        if self._keep is not None:
+            r = self._expand(r)
         #: the fitted weights, [n], user order, `weights[ 0 ] == 0`
         self.weights = r["weights"]
         self._weights_fit = self.weights
@@ -130,8 +166,18 @@ class SdotPlanNd:
         self.stats["start"] = _START.get(int(self.stats["start"]), "?")
         for name in _INT_STATS:
             self.stats[name] = int(self.stats[name])
-        self.stats["aggregation"] = "none" if settings.aggregate else "off"
-        self.stats["duplicates"] = "none"
+        cl = np.asarray(r["clusters"], dtype=np.int64)
+        merged = cl != np.arange(len(cl))
+        reps = np.unique(cl[merged]) if merged.any() else np.zeros(0, np.int64)
+        self._clusters = cl if merged.any() else None
+        self.stats["nb_clusters"] = int(len(reps))
+        self.stats["nb_aggregated"] = int(merged.sum() + len(reps))
+        self.stats["nb_duplicates"] = int(len(self._dups[0]))
+        if not settings.aggregate:
+            self.stats["aggregation"] = "off"
+        else:
+            self.stats["aggregation"] = f"{len(reps)} clusters, {self.stats['nb_aggregated']} seeds" if len(reps) else "none"
+        self.stats["duplicates"] = "checked" if settings.aggregate else "not checked"
         self.stats["warm_start"] = self._warm_start
         self.history = []
         for row in r["history"]:
@@ -150,8 +196,8 @@ class SdotPlanNd:
 
     @property
     def clusters(self):
-        """`None`: no seeds were merged (the aggregation is not built in this version)"""
-        return None
+        """each seed's cluster by its smallest index, or `None` when no seeds were merged (SdotPlanNd.py:629-641)"""
+        return self._clusters
 
     @property
     def target_masses(self):

@@ -20,7 +20,8 @@ SDOT_HOST, SDOT_DEVICE = 0, 1
 DENSITY_UNIFORM, DENSITY_IMAGE, DENSITY_GAUSSIANS = 0, 1, 2
 
 OPTIONS = ["tol_abs", "tol_rel", "maxit", "max_backtracks", "t_min", "mult_ok", "residual", "power", "switch", "lin_tol", "lin_maxit",
-           "keep_start", "continuation", "conv_threshold", "conv_s0", "conv_ratio", "conv_min", "lin_method", "precision", "lin_precision"]
+           "keep_start", "continuation", "conv_threshold", "conv_s0", "conv_ratio", "conv_min", "lin_method", "precision", "lin_precision",
+           "agg_margin"]
 NB_OPTIONS = len(OPTIONS)
 NB_STATS = 31
 NB_HIST = 8
@@ -64,7 +65,7 @@ class SolveDesc(ctypes.Structure):
 class SolveOut(ctypes.Structure):
     _fields_ = [("weights", ctypes.c_void_p), ("masses", ctypes.c_void_p), ("barycentres", ctypes.c_void_p), ("cost", ctypes.c_void_p),
                 ("stats", ctypes.c_double * NB_STATS), ("history", ctypes.c_void_p), ("cap_history", ctypes.c_int32),
-                ("nb_history", ctypes.c_int32)]
+                ("nb_history", ctypes.c_int32), ("clusters", ctypes.c_void_p)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -317,9 +318,10 @@ def solve_desc(pos, nu, w0, lo, hi, dens, options, keep):
 def solve_out(n, d, cap_history, keep):
     so = SolveOut()
     res = dict(weights=np.zeros(n), masses=np.zeros(n), barycentres=np.zeros((n, d)), cost=np.zeros(1),
-               history=np.zeros((max(cap_history, 1), NB_HIST)))
+               history=np.zeros((max(cap_history, 1), NB_HIST)), clusters=np.zeros(n, np.int32))
     keep.append(res)
     so.weights, so.masses = res["weights"].ctypes.data, res["masses"].ctypes.data
+    so.clusters = res["clusters"].ctypes.data
     so.barycentres, so.cost = res["barycentres"].ctypes.data, res["cost"].ctypes.data
     so.history, so.cap_history = res["history"].ctypes.data, cap_history
     return so, res

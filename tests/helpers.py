@@ -53,3 +53,31 @@ def monte_carlo_masses(pos, lo, hi, weights=None, nb_samples=200000, seed=0):
         res += np.bincount(d2.argmin(axis=1), minlength=len(pos))
         done += m
     return res / nb_samples * float(np.prod(hi - lo))
+
+
+def degenerate_clouds(d, seed):
+    """`{ name: (positions, groups) }`: a uniform cloud in [0.05, 0.95]^d (400 seeds in 2D, 600 in 3D) with some seeds moved
+    onto others (tests/test_SdotPlanNd.py:1377-1404); `groups` lists `(members, exact)`, `exact` when the members share
+    one position"""
+    rng = np.random.default_rng(seed)
+    n = 400 if d == 2 else 600
+    base = rng.uniform(0.05, 0.95, size=(n, d))
+    diag = np.ones(d) / np.sqrt(d)
+    axis = np.eye(d)[0]
+
+    def cloud(*moves):
+        pos, groups = base.copy(), []
+        for members, shifts in moves:
+            for m, sh in zip(members[1:], shifts):
+                pos[m] = pos[members[0]] + sh
+            groups.append((list(members), all(not np.any(sh) for sh in shifts)))
+        return pos, groups
+
+    return {
+        "exact pair": cloud(([5, 7], [0 * diag])),
+        "exact triple": cloud(([3, 11, 29], [0 * diag, 0 * diag])),
+        "pair at 1e-9": cloud(([5, 7], [1e-9 * diag])),
+        "pair at 1e-12": cloud(([8, 2], [1e-12 * diag])),
+        "triple at 1e-10": cloud(([4, 9, 13], [1e-10 * diag, 2e-10 * axis])),
+        "pair and duplicate": cloud(([1, 6], [3e-10 * diag]), ([12, 15, 30], [0 * diag, 2e-10 * axis])),
+    }

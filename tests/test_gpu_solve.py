@@ -211,3 +211,62 @@ def test_a_3d_solve_matches_the_oracle():
     assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
     assert np.abs(plan.barycenters - ref["bary"]).max() < 1e-9
     assert abs(plan.cost - ref["cost"]) <= 1e-9 * ref["cost"]
+
+
+def _check_aggregated(name, plan, pos, groups, tol):
+    """tests/test_SdotPlanNd.py:1407-1432: converged (aggregated, unless the groups are exact duplicates only), the clusters
+    found, each cluster's mass its target, every other cell its own, an exact duplicate's cell empty"""
+    n = len(pos)
+    st = plan.stats
+    nu = np.asarray(plan.target_masses).reshape(-1)
+    m = np.asarray(plan.cell_masses).reshape(-1)
+    w = np.asarray(plan.weights).reshape(-1)
+    assert plan.converged, (name, st["status"], st["residual"])
+    only_exact = all(exact for _, exact in groups)
+    assert st["status"] == ("converged" if only_exact else "converged (aggregated)"), (name, st["status"])
+    assert st["residual"] <= tol, (name, st["residual"])
+    cl = np.asarray(plan.clusters).reshape(-1)
+    alone = np.ones(n, dtype=bool)
+    for members, exact in groups:
+        assert (cl[members] == min(members)).all(), (name, members, cl[members])
+        alone[members] = False
+        assert abs(m[members].sum() - nu[members].sum()) <= len(members) * tol * (1 + 1e-9), (name, m[members].sum() - nu[members].sum())
+        if exact:
+            assert (m[members[1:]] == 0).all() and (w[members[1:]] < w[members[0]]).all(), name
+    assert (cl[alone] == np.arange(n)[alone]).all(), name
+    assert np.abs(m[alone] - nu[alone]).max() <= tol, (name, np.abs(m[alone] - nu[alone]).max())
+    assert st["nb_clusters"] == len(groups) and st["nb_aggregated"] == sum(len(g) for g, _ in groups), (name, st["aggregation"])
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_card_aggregates_as_the_cpu(d):
+    """tests/test_SdotPlanNd.py:1510-1535, 1785-1805: seeds the doubles cannot separate are merged, and the oracle's
+    diagram at the GPU's weights gives each cluster its mass and every other cell its own"""
+    from helpers import degenerate_clouds
+    for name, (pos, groups) in degenerate_clouds(d, 17).items():
+        n = len(pos)
+        tol = (1e-9 if "1e-12" in name else 1e-11) / n
+        plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=tol, max_iter=60))
+        _check_aggregated(f"{d}D {name}", plan, pos, groups, tol)
+        g = O.cells(pos, np.asarray(plan.weights).reshape(-1))["mass"]
+        nu = np.asarray(plan.target_masses).reshape(-1)
+        alone = np.ones(n, dtype=bool)
+        for members, exact in groups:
+            alone[members] = False
+            if not exact:                # (two equal points: the oracle counts their cell twice)
+                assert abs(g[members].sum() - nu[members].sum()) < 1e-8 / n, (name, g[members].sum() - nu[members].sum())
+        assert np.abs(g[alone] - nu[alone]).max() < 1e-8 / n, name
+        if any(exact for _, exact in groups) or len(np.unique(pos, axis=0)) < n:
+            continue
+        # without the aggregation: the floor of the weights' doubles
+        off = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=tol, max_iter=60, aggregate=False, on_failure="ignore"))
+        assert not off.converged and off.stats["aggregation"] == "off" and off.clusters is None, (name, off.stats["status"])
+
+
+def test_the_aggregation_changes_nothing_without_such_seeds():
+    """tests/test_SdotPlanNd.py:1544-1552: a cloud without near pairs, the same plan to the bit"""
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(size=(4000, 2))
+    on, off = [OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=1e-10 / 4000, max_iter=60, aggregate=agg)) for agg in (True, False)]
+    assert on.clusters is None and on.stats["aggregation"] == "none" and on.stats["duplicates"] == "checked"
+    assert np.array_equal(np.asarray(on.weights), np.asarray(off.weights))

@@ -240,3 +240,59 @@ def test_the_similarity_start_when_seeds_are_outside():
     s = O.solve(pos, tol_abs=1e-11)
     assert s["stats"]["start"] == 2
     assert s["stats"]["status"] == 1
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_near_coincident_seeds_tile_the_domain(d):
+    """two cells of seeds 1e-12 apart share their plane to the bit: the diagram's masses sum to the domain's (the plane
+    offset takes the weights' difference before |q|^2, and both faces of an edge make the same crossing point)"""
+    from helpers import degenerate_clouds
+    for name in ("pair at 1e-9", "pair at 1e-12", "triple at 1e-10"):
+        pos, _ = degenerate_clouds(d, 17)[name]
+        rng = np.random.default_rng(1)
+        for w in (None, 1e-3 * rng.standard_normal(len(pos))):
+            for brute in (False, True):
+                m = O.cells(pos, w, brute=brute)["mass"]
+                assert abs(m.sum() - 1) < 1e-15, (d, name, brute, m.sum() - 1)
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_aggregation_merges_what_the_doubles_cannot_separate(d):
+    """tests/test_SdotPlanNd.py:1437-1453 on the oracle: with the aggregation the near-coincident groups are merged and
+    the solve converges on the clusters (status 7); without it, it stagnates at the floor of the weights' doubles"""
+    from helpers import degenerate_clouds
+    for name, (pos, groups) in degenerate_clouds(d, 17).items():
+        if len(np.unique(pos, axis=0)) < len(pos):
+            continue                     # exact duplicates are the API layer's (they never reach a solver)
+        n = len(pos)
+        tol = 1e-11 / n
+        r = O.solve(pos, tol_abs=tol, maxit=60, agg_margin=4.0)
+        st = r["stats"]
+        assert st["status"] == 7 and st["residual"] <= tol, (d, name, st["status"], st["residual"])
+        assert st["nb_clusters"] == len(groups) and st["nb_aggregated"] == sum(len(g) for g, _ in groups), (d, name)
+        cl = r["clusters"]
+        alone = np.ones(n, dtype=bool)
+        for members, _ in groups:
+            assert (cl[members] == min(members)).all(), (d, name, cl[members])
+            alone[members] = False
+            assert abs(r["masses"][members].sum() - len(members) / n) <= len(members) * tol * (1 + 1e-9), (d, name)
+        assert (cl[alone] == np.arange(n)[alone]).all()
+        assert np.abs(r["masses"][alone] - 1 / n).max() <= tol, (d, name)
+        off = O.solve(pos, tol_abs=tol, maxit=60)
+        assert off["stats"]["status"] not in (1, 7), (d, name, off["stats"]["status"])
+        assert off["stats"]["nb_clusters"] == 0
+
+
+def test_aggregation_changes_nothing_without_such_seeds():
+    """tests/test_SdotPlanNd.py:1486-1507: a cloud without near pairs gives the same plan, to the bit, with or without it"""
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(size=(1500, 2))
+    t = O.max_threads()
+    O.set_threads(1)                     # (the threads' reductions would differ in the last bits from run to run)
+    try:
+        on = O.solve(pos, tol_abs=1e-10 / 1500, agg_margin=4.0)
+        off = O.solve(pos, tol_abs=1e-10 / 1500)
+    finally:
+        O.set_threads(t)
+    assert on["stats"]["status"] == 1 and on["stats"]["nb_clusters"] == 0
+    assert np.array_equal(on["weights"], off["weights"])
