@@ -1119,6 +1119,7 @@ typedef struct {
     /* the aggregation of near-coincident seeds (sdotplan/Aggregation.h): margin, tolerance, union-find (NULL: none) */
     double agg_margin, agg_tol_abs, agg_tol_rel;
     int *agg_parent;
+    double *img_conv;                 /* image continuation: the blurred values [nx*ny] and a pass's output */
     int agg_changed;
     int nb_diag;
     double t_diag;
@@ -1357,7 +1358,40 @@ static void gauss_at( od_sweep *sw, const double *dval, int dim, double s ) {
     sw->pb.dval = sw->gauss_conv;
 }
 
-/* THE SOLVE (restates sdotplan/Solve.h::solve without aggregation and with the TRIALS step).
+/* the image at width s (sdotplan/convolved/Image.h:51-74): along each axis a gaussian of s / step pixels, truncated at
+ * ceil( 4 s / step ) pixels (at most the axis), each value renormalised by the taps inside the axis; axis x first */
+static void image_at( od_sweep *sw, const double *dval, double s ) {
+    const double *P = sw->pb.dpar;
+    const int nx = ( int ) P[ 4 ], ny = ( int ) P[ 5 ];
+    const long tot = ( long ) nx * ny;
+    double *buf = sw->img_conv, *tmp = sw->img_conv + tot;
+    memcpy( buf, dval, tot * sizeof( double ) );
+    for ( int a = 0; a < 2 && s > 0; ++a ) {
+        const double sp = s / P[ 2 + a ];
+        if ( ! ( sp > 1e-3 ) ) continue;
+        const int len = a ? ny : nx;
+        const long stride = a ? 1 : ny;
+        int r = ( int ) ceil( 4 * sp );
+        if ( r > len ) r = len;
+        double *ker = malloc( ( 2 * ( size_t ) r + 1 ) * sizeof( double ) );
+        for ( int k = -r; k <= r; ++k ) ker[ k + r ] = exp( -0.5 * ( double ) k * ( double ) k / ( sp * sp ) );
+#pragma omp parallel for schedule( static )
+        for ( long flat = 0; flat < tot; ++flat ) {
+            const int p = a ? ( int ) ( flat % ny ) : ( int ) ( flat / ny );
+            const int lo = -r > -p ? -r : -p, hi = r < len - 1 - p ? r : len - 1 - p;
+            double sum = 0, ws = 0;
+            for ( int k = lo; k <= hi; ++k ) { sum += ker[ k + r ] * buf[ flat + k * stride ]; ws += ker[ k + r ]; }
+            tmp[ flat ] = sum / ws;
+        }
+        free( ker );
+        double *t = buf; buf = tmp; tmp = t;
+    }
+    if ( buf != sw->img_conv ) memcpy( sw->img_conv, buf, tot * sizeof( double ) );
+    sw->pb.dval = sw->img_conv;
+}
+
+/* THE SOLVE (restates sdotplan/Solve.h::solve with the aggregation of near-coincident seeds, exact duplicates left to the
+ * caller, and the TRIALS step).
  * Inputs in user order; `w0` may be NULL; `opts` [NB_OPTIONS]; outputs: weights [n], masses [n], bary [n, d],
  * cost [1], stats [NB_STATS], hist [cap_steps, 8] (may be NULL) and the number of rows written. */
 int od_solve( int dim, long n, const double *pos, const double *nu_in, const double *w0, const double *box, int dkind, const double *dpar,
@@ -1378,6 +1412,7 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     sw.nm = malloc( ( size_t ) n * sw.cap * sizeof( double ) );
     int ng = dkind == DENS_GAUSS ? ( int ) dpar[ 0 ] : 0;
     sw.gauss_conv = malloc( ( ng > 0 ? ng : 1 ) * ( dim + 2 ) * sizeof( double ) );
+    if ( dkind == DENS_IMAGE ) sw.img_conv = malloc( 2 * ( size_t ) dpar[ 4 ] * ( size_t ) dpar[ 5 ] * sizeof( double ) );
     for ( int k = 0; k < NB_STATS; ++k ) stats[ k ] = 0;
     od_hist H = { hist, hist ? cap_steps : 0, 0, 0, 0 };
 
@@ -1390,7 +1425,7 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     for ( long i = 0; i < n; ++i ) w[ i ] -= gauge;
 
     /* the stages of the width continuation */
-    int possible = dkind == DENS_GAUSS;             /* an image stage would blur the values: not restated here */
+    int possible = dkind == DENS_GAUSS || ( dkind == DENS_IMAGE && dim == 2 );
     double s0 = opts[ O_CONV_S0 ];
     if ( s0 <= 0 ) {
         double diam2 = 0;
@@ -1403,6 +1438,7 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
         for ( int g = 0; g < ng; ++g ) sg = fmin( sg, dval[ g * ( dim + 2 ) + dim ] );
         smin = sg / 4;
     }
+    if ( smin <= 0 && dkind == DENS_IMAGE ) smin = fmin( dpar[ 2 ], dpar[ 3 ] ) / 4;      /* a quarter of a pixel */
     double scales[ 256 ];
     int nsc = 0;
     int cont = ( int ) opts[ O_CONTINUATION ];
@@ -1411,7 +1447,8 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     if ( cont == 2 && possible ) MAKE_SCALES();
     else { scales[ 0 ] = 0; nsc = 1; }
 
-    if ( dkind == DENS_GAUSS ) gauss_at( &sw, dval, dim, scales[ 0 ] );
+#define DENS_AT( s ) do { if ( dkind == DENS_GAUSS ) gauss_at( &sw, dval, dim, ( s ) ); else if ( possible ) image_at( &sw, dval, ( s ) ); } while ( 0 )
+    DENS_AT( scales[ 0 ] );
     H.s_current = scales[ 0 ];
     int st = sweep( &sw, w, a );
     double nu_min = vmin( n, nu );
@@ -1447,7 +1484,7 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     double min_start_mass = vmin( n, a );
     if ( cont == 1 && possible && nsc == 1 && min_start_mass < opts[ O_CONV_THRESHOLD ] * nu_min ) {
         MAKE_SCALES();
-        gauss_at( &sw, dval, dim, scales[ 0 ] );
+        DENS_AT( scales[ 0 ] );
         H.s_current = scales[ 0 ];
         sweep( &sw, w, a );
     }
@@ -1458,7 +1495,7 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     for ( int step = 0; step < nsc && status != ST_CAPACITY; ++step ) {
         H.s_current = scales[ step ];
         if ( step > 0 ) {
-            if ( dkind == DENS_GAUSS ) gauss_at( &sw, dval, dim, scales[ step ] );
+            DENS_AT( scales[ step ] );
             sweep( &sw, w, a );
         }
         double num = 0;
@@ -1473,7 +1510,8 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     int nb_diag_descent = sw.nb_diag;
     for ( long i = 0; i < n; ++i ) { weights[ i ] = w[ i ]; masses[ i ] = a[ i ]; }
     /* the moments on the true density at the fitted weights */
-    if ( dkind == DENS_GAUSS ) sw.pb.dval = dval;
+#undef DENS_AT
+    sw.pb.dval = dval;
     {
         double *cst = malloc( n * sizeof( double ) );
         sw.pb.w = w;
@@ -1516,6 +1554,6 @@ int od_solve( int dim, long n, const double *pos, const double *nu_in, const dou
     }
     if ( nb_steps ) *nb_steps = H.nb_steps;
     free( nu ); free( w ); free( a ); free( wt0 ); free( at0 ); free( nu_s );
-    free( sw.nb ); free( sw.nid ); free( sw.nc ); free( sw.nm ); free( sw.gauss_conv );
+    free( sw.nb ); free( sw.nid ); free( sw.nc ); free( sw.nm ); free( sw.gauss_conv ); free( sw.img_conv );
     return st == OD_OK ? OD_OK : st;
 }

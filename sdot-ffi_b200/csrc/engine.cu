@@ -332,7 +332,9 @@ void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positio
             G.gauss[ k * ( dim + 2 ) + dim + 1 ] = mm[ k ];
         }
     }
-    dbytes = size_t( nval + npre ) * 8 + 1024;
+    // an image also keeps its values as given and room for the continuation's blur (one pass's output, the taps)
+    const long nimg = dens.kind == SDOT_DENSITY_IMAGE ? 2 * nval + 2 * long( std::max( G.dn[ 0 ], G.dn[ 1 ] ) ) + 1 : 0;
+    dbytes = size_t( nval + npre + nimg ) * 8 + 4 * 256;
     const long npyr = wpyr_layout( dim, G.g, G.nlev, G.poff );
     size_t bytes = size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( G.ncell ) * 8 + size_t( npyr ) * 8 * ( dim + 1 + wmom_size( dim ) ) + dbytes +
                    10 * 256;
@@ -346,6 +348,11 @@ void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positio
     G.wmom = A.take<double>( size_t( npyr ) * wmom_size( dim ) );
     if ( nval ) G.dval = A.take<double>( nval );
     if ( npre ) G.dpre = A.take<double>( npre );
+    if ( nimg ) {
+        G.dorig = A.take<double>( nval );
+        G.dtmp = A.take<double>( nval );
+        G.dker = A.take<double>( 2 * size_t( std::max( G.dn[ 0 ], G.dn[ 1 ] ) ) + 1 );
+    }
     // the sort, in a temporary allocation
     size_t tb = radix_temp_bytes( int( n ), key_bits );
     size_t tbytes = size_t( n ) * ( 8 + 8 + 4 + 4 ) + size_t( n ) * dim * 8 + tb + 6 * 256;
@@ -364,6 +371,7 @@ void build_geometry( Ctx &c, Geometry &G, int dim, long n, const double *positio
     launch_cell_ranges( L, k1, G.pos, int( n ), dim, G.g, G.go, G.gh, G.cell_range );
     if ( dens.kind == SDOT_DENSITY_IMAGE ) {
         to_device( c, G.dval, dens.values, nval, memory );
+        CK( cudaMemcpyAsync( G.dorig, G.dval, size_t( nval ) * 8, cudaMemcpyDeviceToDevice, c.stream ) );
         launch_image_prefix( L, G.dval, G.dn[ 0 ], G.dn[ 1 ], G.dstep[ 0 ], G.dpre );
     } else if ( dens.kind == SDOT_DENSITY_GAUSSIANS ) {
         CK( cudaMemcpyAsync( G.dval, G.gauss.data(), nval * 8, cudaMemcpyHostToDevice, c.stream ) );
@@ -467,7 +475,7 @@ size_t job_bytes( int dim, long n, int dkind, long dcount ) {
     // geometry: ranked positions, user, rank_of, the grid (about n / 2 cells), the density, and the sort's scratch
     b += size_t( n ) * dim * 8 + size_t( n ) * 8 + size_t( n ) * 4 + 1024;
     b += size_t( n ) * ( dim == 2 ? 64 : 84 ) + 1024;    // the weight majorants and their moments (4/3, 8/7 of the grid's cells)
-    b += dkind == D_IMAGE ? size_t( dcount ) * 16 : size_t( dcount ) * 8 * ( dim + 2 );
+    b += dkind == D_IMAGE ? size_t( dcount ) * 32 + 32768 : size_t( dcount ) * 8 * ( dim + 2 );     // (image: values, prefix, original, blur pass)
     b += size_t( n ) * ( 24 + dim * 8 ) + 4096;
     return b + mg_bytes( dim, n, cap );
 }
@@ -593,6 +601,11 @@ static MgLevel mg_level( const SolveJob &J, int l, int vec ) {
     return M;
 }
 
+static std::vector<double> continuation_scales( const SolveJob &J );
+static void set_stage_density( Ctx &c, SolveJob &J );
+// the densities the width continuation can widen: gaussians, and 2D images (blurred on their grid)
+static bool convolvable( const SolveJob &J ) { return J.G.dkind == D_GAUSS || ( J.G.dkind == D_IMAGE && J.G.dim == 2 ); }
+
 SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
     const sdot_diagram_desc &D = desc.diagram;
     SolveJob *J = new SolveJob;
@@ -642,6 +655,12 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         J->stats[ ST_IT_SWITCH ] = -1;
         J->state = J_START0;
         J->scales.assign( 1, 0.0 );
+        if ( convolvable( *J ) && int( J->opt[ SDOT_OPT_CONTINUATION ] ) == 2 ) {
+            // continuation "always": the start is chosen on the first width already (sdotplan/Solve.h:196-199)
+            J->scales = continuation_scales( *J );
+            J->stage = 0;
+            set_stage_density( c, *J );
+        }
     } catch ( ... ) {
         job_destroy( c, J );
         throw;
@@ -716,6 +735,7 @@ static std::vector<double> continuation_scales( const SolveJob &J ) {
         s0 = 0.5 * std::sqrt( d2 );
     }
     double smin = J.opt[ SDOT_OPT_CONV_MIN ];
+    if ( smin <= 0 && J.G.dkind == D_IMAGE ) smin = std::min( J.G.dstep[ 0 ], J.G.dstep[ 1 ] ) / 4;   // a quarter of a pixel
     if ( smin <= 0 ) {
         double sg = 1e300;
         for ( int k = 0; k < J.G.dn[ 0 ]; ++k ) sg = std::min( sg, J.G.gauss[ k * ( dim + 2 ) + dim ] );
@@ -729,6 +749,33 @@ static std::vector<double> continuation_scales( const SolveJob &J ) {
 }
 
 static void set_stage_density( Ctx &c, SolveJob &J ) {
+    if ( J.G.dkind == D_IMAGE ) {
+        // the image at width s: blurred on its grid by a gaussian of s / step pixels along each axis, truncated at 4 of them
+        // and renormalised at the border (sdotplan/convolved/Image.h:37-74), then its prefix sums
+        Geometry &G = J.G;
+        const int nx = G.dn[ 0 ], ny = G.dn[ 1 ];
+        const size_t nval = size_t( nx ) * ny;
+        const double s = J.scales[ J.stage ];
+        Launch L = c.L();
+        CK( cudaMemcpyAsync( G.dval, G.dorig, nval * 8, cudaMemcpyDeviceToDevice, c.stream ) );
+        if ( s > 0 ) {
+            std::vector<double> ker;
+            for ( int a = 0; a < 2; ++a ) {
+                const double sp = s / G.dstep[ a ];
+                if ( ! ( sp > 1e-3 ) ) continue;
+                const int len = G.dn[ a ];
+                const int r = int( std::min( std::ceil( 4 * sp ), double( len ) ) );
+                ker.resize( 2 * size_t( r ) + 1 );
+                for ( int k = -r; k <= r; ++k ) ker[ k + r ] = std::exp( -0.5 * double( k ) * double( k ) / ( sp * sp ) );
+                CK( cudaMemcpyAsync( G.dker, ker.data(), ker.size() * 8, cudaMemcpyHostToDevice, c.stream ) );
+                launch_blur_axis( L, G.dval, G.dtmp, nx, ny, a, r, G.dker );
+                std::swap( G.dval, G.dtmp );
+                CK( cudaStreamSynchronize( c.stream ) );       // `ker` is refilled for the next axis
+            }
+        }
+        launch_image_prefix( L, G.dval, nx, ny, G.dstep[ 0 ], G.dpre );
+        return;
+    }
     if ( J.G.dkind != D_GAUSS ) return;
     const int dim = J.G.dim, st = dim + 2;
     std::vector<double> g = J.G.gauss;
@@ -799,7 +846,7 @@ static void end_stage( Ctx &c, SolveJob &J ) {
         J.state = J_STAGE_DIAG;
         return;
     }
-    if ( J.G.dkind == D_GAUSS && J.scales[ J.stage ] != 0 ) {
+    if ( ( J.G.dkind == D_GAUSS || J.G.dkind == D_IMAGE ) && J.scales[ J.stage ] != 0 ) {
         J.stage = int( J.scales.size() ) - 1;
         set_stage_density( c, J );
     }
@@ -846,7 +893,7 @@ static void after_start( Ctx &c, SolveJob &J ) {
     J.stats[ ST_MIN_START_MASS ] = amin;
     J.stats[ ST_START ] = J.start;
     int cont = int( J.opt[ SDOT_OPT_CONTINUATION ] );
-    if ( J.G.dkind == D_GAUSS && ( cont == 2 || ( cont == 1 && amin < J.opt[ SDOT_OPT_CONV_THRESHOLD ] * J.nu_min ) ) ) {
+    if ( convolvable( J ) && J.scales.size() == 1 && cont == 1 && amin < J.opt[ SDOT_OPT_CONV_THRESHOLD ] * J.nu_min ) {
         J.scales = continuation_scales( J );
         J.stage = 0;
         set_stage_density( c, J );

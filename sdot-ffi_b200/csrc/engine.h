@@ -90,6 +90,7 @@ struct Geometry {
     int dkind = D_UNIFORM;
     double rho = 1;
     double *dval = nullptr, *dpre = nullptr;
+    double *dorig = nullptr, *dtmp = nullptr, *dker = nullptr;   // image: the values as given, a pass's output, the taps
     int dn[ 3 ] = { 0, 0, 0 };
     double dorg[ 3 ] = { 0, 0, 0 }, dstep[ 3 ] = { 0, 0, 0 };
     std::vector<double> gauss;        // [ng, dim + 2] as given (continuation widens it)

@@ -152,6 +152,31 @@ void launch_image_prefix( const Launch &L, const double *values, int nx, int ny,
     ++*L.launches;
 }
 
+// the image continuation's blur along one axis (sdotplan/convolved/Image.h:51-74): dst = sum_k ker src( . + k ) / sum_k ker
+// over the taps inside the axis, k ascending, without contraction (the same sums as a plain CPU loop)
+__global__ void k_blur_axis( const double *__restrict__ src, double *__restrict__ dst, int nx, int ny, int axis, int r,
+                             const double *__restrict__ ker ) {
+    const size_t flat = size_t( blockIdx.x ) * blockDim.x + threadIdx.x;
+    if ( flat >= size_t( nx ) * ny ) return;
+    const int i = int( flat / ny ), j = int( flat % ny );
+    const int p = axis ? j : i, len = axis ? ny : nx;
+    const long stride = axis ? 1 : ny;
+    const int lo = -r > -p ? -r : -p, hi = r < len - 1 - p ? r : len - 1 - p;
+    double sum = 0, ws = 0;
+    for ( int k = lo; k <= hi; ++k ) {
+        const double t = ker[ k + r ];
+        sum = __dadd_rn( sum, __dmul_rn( t, src[ long( flat ) + k * stride ] ) );
+        ws = __dadd_rn( ws, t );
+    }
+    dst[ flat ] = sum / ws;
+}
+
+void launch_blur_axis( const Launch &L, const double *src, double *dst, int nx, int ny, int axis, int r, const double *ker ) {
+    const size_t tot = size_t( nx ) * ny;
+    k_blur_axis<<<unsigned( ( tot + 255 ) / 256 ), 256, 0, L.stream>>>( src, dst, nx, ny, axis, r, ker );
+    ++*L.launches;
+}
+
 __global__ void k_wmax( const double *__restrict__ w, int n, unsigned long long *slot ) {
     double m = -1e300;
     for ( int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x ) m = fmax( m, w[ i ] );

@@ -271,6 +271,9 @@ size_t radix_temp_bytes( int n, int bits );
 void radix_sort( const Launch &L, void *temp, size_t temp_bytes, const unsigned long long *kin, unsigned long long *kout, const int *vin,
                  int *vout, int n, int bits );
 void launch_image_prefix( const Launch &L, const double *values, int nx, int ny, double hx, double *pre );
+// one axis of the separable gaussian blur of an image [nx, ny] (i along x, j contiguous): taps ker[ 0 .. 2r ],
+// renormalised by the taps that fall inside the axis
+void launch_blur_axis( const Launch &L, const double *src, double *dst, int nx, int ny, int axis, int r, const double *ker );
 void launch_wmax( const Launch &L, const double *w, int n, unsigned long long *slot );
 // the levels of the weight majorants of a grid: returns the doubles they take, fills nlev and poff
 long wpyr_layout( int dim, const int *g, int &nlev, int *poff );

@@ -270,3 +270,41 @@ def test_the_aggregation_changes_nothing_without_such_seeds():
     on, off = [OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=1e-10 / 4000, max_iter=60, aggregate=agg)) for agg in (True, False)]
     assert on.clusters is None and on.stats["aggregation"] == "none" and on.stats["duplicates"] == "checked"
     assert np.array_equal(np.asarray(on.weights), np.asarray(off.weights))
+
+
+@pytest.mark.parametrize("continuation", ["auto", "always"])
+def test_an_image_with_a_hole_takes_the_blur_continuation(continuation):
+    """tests/test_SdotPlanNd.py:1032-1040: a contrasted image with zeros; the image blurred on its grid, stage by stage,
+    as the oracle does it: the same stages and the same plan"""
+    rng = np.random.default_rng(201)
+    n = 1500
+    pos = rng.uniform(0.001, 0.999, size=(n, 2))
+    nu = rng.uniform(0.5, 1.5, n)
+    nu /= nu.sum()
+    vals = 0.1 + 0.9 * rng.random((32, 32))
+    vals[4:12, 18:28] = 0
+    vals[20:23, :] += 4
+    img = sdot.Image(vals, frame=[1 / 32, 1 / 32])
+    plan = OtProblem(SumOfDiracs(pos, nu), img).solve(Iterative(tol=1e-10 / n, max_iter=80, continuation=continuation))
+    assert plan.converged and plan.stats["nb_continuation_steps"] > 1, plan.stats
+    norm = img.normalized_version()
+    ref = O.solve(pos, nu=nu, tol_abs=1e-10 / n, maxit=80, continuation={"auto": 1, "always": 2}[continuation],
+                  density=("image", [0, 0], [1 / 32, 1 / 32], norm.values))
+    assert ref["stats"]["status"] == 1
+    assert plan.stats["nb_continuation_steps"] == ref["stats"]["nb_continuation_steps"]
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+    ss = [h["s"] for h in plan.history]
+    assert ss[0] > 0 and ss[-1] == 0 and all(b <= a for a, b in zip(ss, ss[1:]))
+
+
+def test_an_almost_empty_image_takes_the_blur_continuation():
+    """tests/test_SdotPlanNd.py:397-405: two spots on a 1e-6 floor; `auto` starts the continuation and the plan converges"""
+    rng = np.random.default_rng(91)
+    pos = rng.uniform(0, 1, size=(400, 2))
+    values = np.full((32, 32), 1e-6)
+    values[6:10, 6:10] = 1.0
+    values[20:26, 18:24] = 0.7
+    img = sdot.Image(values, frame=[1 / 32, 1 / 32])
+    plan = OtProblem(SumOfDiracs(pos), img).solve(Iterative(max_iter=100, tuning=Tuning(mass_rtol=1e-6)))
+    assert plan.converged and plan.stats["nb_continuation_steps"] > 1, plan.stats
+    assert np.allclose(plan.cell_masses, plan.target_masses, rtol=1e-5)

@@ -296,3 +296,24 @@ def test_aggregation_changes_nothing_without_such_seeds():
         O.set_threads(t)
     assert on["stats"]["status"] == 1 and on["stats"]["nb_clusters"] == 0
     assert np.array_equal(on["weights"], off["weights"])
+
+
+def test_the_image_continuation_solves_what_direct_newton_cannot():
+    """tests/test_SdotPlanNd.py:397-405 on the oracle: an almost empty image but for two spots. Direct Newton fails; the
+    blur continuation (the image widened on its grid, sdotplan/convolved/Image.h) converges, and `auto` starts it"""
+    rng = np.random.default_rng(91)
+    pos = rng.uniform(0, 1, size=(400, 2))
+    values = np.full((32, 32), 1e-6)
+    values[6:10, 6:10] = 1.0
+    values[20:26, 18:24] = 0.7
+    dens = ("image", [0.0, 0.0], [1 / 32, 1 / 32], values)
+    direct = O.solve(pos, density=dens, tol_abs=0.0, tol_rel=1e-6, maxit=60, continuation=0)
+    assert direct["stats"]["status"] != 1
+    for cont in (1, 2):
+        r = O.solve(pos, density=dens, tol_abs=0.0, tol_rel=1e-6, maxit=100, continuation=cont)
+        st = r["stats"]
+        assert st["status"] == 1 and st["nb_continuation_steps"] > 1, (cont, st)
+        nu = np.full(400, st["domain_mass"] / 400)
+        assert np.abs(r["masses"] / nu - 1).max() <= 1e-6
+        s = r["history"][:, 7]
+        assert s[0] > 0 and s[-1] == 0 and (np.diff(s) <= 0).all()
