@@ -8,6 +8,7 @@ from .OtProblem import OtProblem, Iterative, Tuning, OtNotConverged, ot_solve
 from .SdotPlanNd import SdotPlanNd, exact_duplicates
 from .distributions import SumOfDiracs, Image, SumOfGaussians, Box
 from ._lib import KernelFailure
+from .quantization import quantization
 
 _KERNEL_DTYPE = "FP64"
 
@@ -34,4 +35,4 @@ def w2(f, g):
 
 __all__ = ["PowerDiagram", "Voronoi", "box_half_spaces", "axis_aligned_box", "OtProblem", "Iterative", "Tuning", "OtNotConverged", "ot_solve",
            "SdotPlanNd", "exact_duplicates", "SumOfDiracs", "Image", "SumOfGaussians", "Box", "KernelFailure", "set_kernel_dtype",
-           "kernel_dtype", "plan", "w2"]
+           "kernel_dtype", "plan", "w2", "quantization"]

@@ -75,3 +75,14 @@ def test_public_names():
     for name in ("PowerDiagram", "Voronoi", "OtProblem", "Iterative", "Tuning", "OtNotConverged", "ot_solve", "SdotPlanNd", "SumOfDiracs",
                  "Image", "SumOfGaussians", "Box", "box_half_spaces", "KernelFailure"):
         assert hasattr(sdot, name)
+
+
+def test_quantization_draws_its_start_in_the_support():
+    """quantization.py:113-130: rejection in the bounding box of the support's polytope"""
+    import sdot
+    from sdot.quantization import uniform_in_support
+    img = sdot.Image(np.ones((4, 3)), frame=[0.5, 0.25])
+    x = uniform_in_support(img, 300, seed=3)
+    assert x.shape == (300, 2) and (x >= 0).all() and (x[:, 0] <= 2).all() and (x[:, 1] <= 0.75).all()
+    assert np.array_equal(x, uniform_in_support(img, 300, seed=3))
+    assert x[:, 0].max() > 1.9 and x[:, 1].max() > 0.7
