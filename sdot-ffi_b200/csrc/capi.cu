@@ -94,8 +94,9 @@ void run_big_cells( Ctx &c, ProbDev *dprob, unsigned flags ) {
     if ( count <= 0 ) return;
     Launch L = c.L();
     c.timer.begin( c.stream, K_CELLS2D, double( count ) );
-    launch_cells2d_big( L, dprob, c.dovf, std::min( count, 1 << 16 ), flags, c.derr, c.big_scratch, c.big_warps );
-    launch_cells3d_big( L, dprob, c.dovf, std::min( count, 1 << 16 ), flags, c.derr );
+    launch_cells2d_big( L, dprob, c.dovf, std::min( count, c.ovf_cap ), flags, c.derr, c.big_scratch, c.big_warps );
+    launch_cells3d_big( L, dprob, c.dovf, std::min( count, c.ovf_cap ), flags, c.derr, c.dgiant );
+    run_giant_cells( c, dprob, flags );
     c.timer.end( c.stream );
     CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
 }

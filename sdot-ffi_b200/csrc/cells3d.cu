@@ -43,6 +43,7 @@ struct Cell3T {
 };
 using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in shared memory
 using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 84 KB
+using Cell3G = Cell3T<8192, 2048, unsigned short>;       // the giant-cell pass: one warp a block, about 660 KB in global memory
 
 template<class C3>
 __device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double &x, double &y, double &z ) {
@@ -547,9 +548,10 @@ __device__ __forceinline__ void queue3( const ProbDev &P, ErrRec *err, OvfList *
     __syncwarp();
 }
 
-// THE CELL of seed s (rank) of problem `prob`: clip, integrate, write.  The main kernel (`big` false) queues a cell past
-// its capacities for the big-cell pass and returns false (nothing written); `rep` (lane 0, may be NULL) accumulates
-// the Newton report
+// THE CELL of seed s (rank) of problem `prob`: clip, integrate, write.  A cell past the vertex / plane capacities of
+// this pass is queued on `ovf` for the next pass (main -> big -> giant; NULL: an error of its problem) and the call
+// returns false (nothing written).  The main kernel (`big` false) also queues a cell with more facets than the table's
+// row; the other passes write those to the overflow store.  `rep` (lane 0, may be NULL) accumulates the Newton report
 template<class C3>
 __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, int2 *stk, double wmax,
                        double *rep, bool big ) {
@@ -597,7 +599,7 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
     const int user = P.user[ s ];
     if ( overflow ) {
         // past the capacity of this warp's cell: the big-cell pass rebuilds it (the main kernel only)
-        if ( ! big && ovf ) { queue3( P, err, ovf, prob, s, user, lane ); return false; }
+        if ( ovf ) { queue3( P, err, ovf, prob, s, user, lane ); return false; }
         if ( lane == 0 ) record_error3( P, err, 4, prob, user, C3::VC );
         if ( lane == 0 ) C.nv = 0;
         __syncwarp();
@@ -812,7 +814,7 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
 // the big-cell pass: one warp a block, the cell in dynamic shared memory (Cell3B), over the queued 3D items (the 2D ones
 // are the 2D pass's); flags 0: each problem's own pass (a final-moments diagram has `first`)
 __global__ void __launch_bounds__( 32 ) k_cells3d_big( const ProbDev *__restrict__ probs, const OvfList *__restrict__ ovf, int count,
-                                                        unsigned flags, ErrRec *err ) {
+                                                        unsigned flags, ErrRec *err, OvfList *next ) {
     extern __shared__ char smem[];
     __shared__ int2 stk[ WALK_STACK3 ];
     Cell3B &C = *reinterpret_cast<Cell3B *>( smem );
@@ -823,8 +825,35 @@ __global__ void __launch_bounds__( 32 ) k_cells3d_big( const ProbDev *__restrict
         if ( P.dim != 3 ) continue;
         const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
+        cell3( C, P, item.prob, item.seed, lane, fl, err, next, stk, wmax, nullptr, true );
+    }
+}
+
+// the giant-cell pass: the cells past the big pass's capacities (hundreds of faces: a seed in a density desert whose cell
+// reaches across a dense cluster), one warp a block, each block's cell in its slot of `scratch` (global memory, L2-backed)
+__global__ void __launch_bounds__( 32 ) k_cells3d_giant( const ProbDev *__restrict__ probs, const OvfList *__restrict__ list, int count,
+                                                          unsigned flags, ErrRec *err, char *scratch ) {
+    __shared__ int2 stk[ WALK_STACK3 ];
+    Cell3G &C = *reinterpret_cast<Cell3G *>( scratch + size_t( blockIdx.x ) * sizeof( Cell3G ) );
+    const int lane = threadIdx.x;
+    for ( int it = blockIdx.x; it < count; it += gridDim.x ) {
+        const OvfItem item = list->items[ it ];
+        const ProbDev &P = probs[ item.prob ];
+        if ( P.dim != 3 ) continue;
+        const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
+        const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
         cell3( C, P, item.prob, item.seed, lane, fl, err, nullptr, stk, wmax, nullptr, true );
     }
+}
+
+size_t giant3_slot_bytes() { return ( sizeof( Cell3G ) + 255 ) & ~size_t( 255 ); }
+
+void launch_cells3d_giant( const Launch &L, const ProbDev *probs, const OvfList *list, int count, unsigned flags, ErrRec *err, char *scratch,
+                           int slots ) {
+    if ( count <= 0 ) return;
+    static_assert( sizeof( Cell3G ) % 8 == 0, "slots keep the doubles aligned" );
+    k_cells3d_giant<<<count < slots ? count : slots, 32, 0, L.stream>>>( probs, list, count, flags, err, scratch );
+    ++*L.launches;
 }
 
 void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf ) {
@@ -839,7 +868,7 @@ void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks,
     ++*L.launches;
 }
 
-void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err ) {
+void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, OvfList *next ) {
     if ( count <= 0 ) return;
     const size_t smem = sizeof( Cell3B );
     static bool configured = false;
@@ -847,7 +876,7 @@ void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *o
         cudaFuncSetAttribute( k_cells3d_big, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
         configured = true;
     }
-    k_cells3d_big<<<count < 296 ? count : 296, 32, smem, L.stream>>>( probs, ovf, count, flags, err );
+    k_cells3d_big<<<count < 296 ? count : 296, 32, smem, L.stream>>>( probs, ovf, count, flags, err, next );
     ++*L.launches;
 }
 

@@ -68,13 +68,18 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
     std::memset( c.herr, 0, sizeof( ErrRec ) );
     for ( int s = c.max_slots - 1; s >= 0; --s ) c.free_slots.push_back( s );
     // the big-cell queue: OvfList header then its items, in one allocation
-    const int ovf_cap = 1 << 16;
-    char *q = ( char * ) dalloc( c, 256 + size_t( ovf_cap ) * sizeof( OvfItem ) );
+    char *q = ( char * ) dalloc( c, 256 + size_t( c.ovf_cap ) * sizeof( OvfItem ) );
     c.dovf = ( OvfList * ) q;
-    OvfList hl{ 0, ovf_cap, ( OvfItem * ) ( q + 256 ) };
+    OvfList hl{ 0, c.ovf_cap, ( OvfItem * ) ( q + 256 ) };
     CK( cudaMemcpyAsync( c.dovf, &hl, sizeof( hl ), cudaMemcpyHostToDevice, c.stream ) );
     CK( cudaMallocHost( &c.hovf, sizeof( int ) ) );
     *c.hovf = 0;
+    char *gq = ( char * ) dalloc( c, 256 + size_t( c.giant_cap ) * sizeof( OvfItem ) );
+    c.dgiant = ( OvfList * ) gq;
+    OvfList gl{ 0, c.giant_cap, ( OvfItem * ) ( gq + 256 ) };
+    CK( cudaMemcpyAsync( c.dgiant, &gl, sizeof( gl ), cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaMallocHost( &c.hgiant, sizeof( int ) ) );
+    *c.hgiant = 0;
     c.big_scratch = ( char * ) dalloc( c, big_scratch_bytes( c.big_warps ) );
     const char *t = std::getenv( "SDOT_KERNEL_TIMING" );
     c.timer.on = t && t[ 0 ] == '1';
@@ -93,12 +98,15 @@ void ctx_release( Ctx &c ) {
         if ( c.derr ) cudaFreeAsync( c.derr, c.stream );
         if ( c.dovf ) cudaFreeAsync( c.dovf, c.stream );
         if ( c.big_scratch ) cudaFreeAsync( c.big_scratch, c.stream );
+        if ( c.dgiant ) cudaFreeAsync( c.dgiant, c.stream );
+        if ( c.giant_scratch ) cudaFreeAsync( c.giant_scratch, c.stream );
         cudaStreamSynchronize( c.stream );
         cudaStreamDestroy( c.stream );
     }
     if ( c.hscal ) cudaFreeHost( c.hscal );
     if ( c.herr ) cudaFreeHost( c.herr );
     if ( c.hovf ) cudaFreeHost( c.hovf );
+    if ( c.hgiant ) cudaFreeHost( c.hgiant );
     if ( c.pool ) cudaMemPoolDestroy( c.pool );
     c = Ctx{};
 }
@@ -230,8 +238,22 @@ void check_errors( Ctx &c, const char *where ) {
 }
 
 // a capacity error of the engine's kernels belongs to its problem (the per-slot flag read in `decide`): not a batch error
+int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags ) {
+    CK( cudaMemcpyAsync( c.hgiant, &c.dgiant->count, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    const int count = std::min( *c.hgiant, c.giant_cap );
+    if ( count <= 0 ) return 0;
+    if ( ! c.giant_scratch ) c.giant_scratch = ( char * ) dalloc( c, giant3_slot_bytes() * c.giant_slots );
+    Launch L = c.L();
+    launch_cells3d_giant( L, dprob, c.dgiant, count, flags, c.derr, c.giant_scratch, c.giant_slots );
+    CK( cudaMemsetAsync( &c.dgiant->count, 0, sizeof( int ), c.stream ) );
+    return count;
+}
+
 static void clear_capacity_error( Ctx &c ) {
     if ( c.herr->code != SDOT_ERR_CAPACITY ) return;
+    if ( std::getenv( "SDOT_TRACE" ) )
+        std::fprintf( stderr, "sdot: capacity: problem %d of the launch, seed %d, needed %d\n", c.herr->prob, c.herr->seed, c.herr->needed );
     *c.herr = ErrRec{};
     CK( cudaMemsetAsync( c.derr, 0, sizeof( ErrRec ), c.stream ) );
 }
@@ -1588,7 +1610,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     check_errors( c, "cells" );
     if ( *c.hovf > 0 ) {
         // the big cells: rebuilt in global memory, then the reports of their problems recomputed from the masses
-        const int count = std::min( *c.hovf, ( 1 << 16 ) );
+        const int count = std::min( *c.hovf, c.ovf_cap );
         std::vector<OvfItem> items( count );
         CK( cudaMemcpy( items.data(), ( char * ) c.dovf + 256, count * sizeof( OvfItem ), cudaMemcpyDeviceToHost ) );
         ProbDev *dp = reinterpret_cast<ProbDev *>( upload_desc( c, big_probs.data(), big_probs.size() * sizeof( ProbDev ) ) );
@@ -1596,7 +1618,8 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         for ( auto &it : items ) touched[ it.prob ] = 1;
         c.timer.begin( c.stream, K_CELLS2D, double( count ) );
         launch_cells2d_big( L, dp, c.dovf, count, 0, c.derr, c.big_scratch, c.big_warps );     // flags per problem
-        launch_cells3d_big( L, dp, c.dovf, count, 0, c.derr );
+        launch_cells3d_big( L, dp, c.dovf, count, 0, c.derr, c.dgiant );
+        run_giant_cells( c, dp, 0 );
         c.timer.end( c.stream );
         std::vector<Chunk> rc;
         for ( size_t k = 0; k < big_probs.size(); ++k )

@@ -38,6 +38,13 @@ struct Ctx {
     int *hovf = nullptr;
     char *big_scratch = nullptr;
     int big_warps = 256;
+    int ovf_cap = 1 << 18;
+    // 3D cells past the big pass: their queue, its count's host mirror, and the warps' cells (allocated at first use)
+    OvfList *dgiant = nullptr;
+    int *hgiant = nullptr;
+    char *giant_scratch = nullptr;
+    int giant_slots = 32;
+    int giant_cap = 1 << 14;
     // descriptor upload area
     char *desc = nullptr;
     size_t desc_bytes = 0;
@@ -58,6 +65,8 @@ constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 2;
 
 void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
 void ctx_release( Ctx &c );
+// after a big-cell pass that queued 3D cells on `dgiant`: the giant-cell pass over them (synchronises); their number
+int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags );
 void *dalloc( Ctx &c, size_t bytes );
 void dfree( Ctx &c, void *p );
 

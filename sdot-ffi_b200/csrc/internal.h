@@ -320,6 +320,10 @@ void launch_scatter( const Launch &L, const double *ranked, const int *user, int
 void launch_gather_vec( const Launch &L, const double *user_vals, const int *user, int n, double *ranked, double scale );
 void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
 // the queued 3D cells (past the warp cell's capacities) rebuilt one warp a block with larger capacities
-void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err );
+void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, OvfList *next );
+// the 3D cells past the big pass's capacities (queued on its `next`), each warp's cell in a slot of `scratch`
+size_t giant3_slot_bytes();
+void launch_cells3d_giant( const Launch &L, const ProbDev *probs, const OvfList *list, int count, unsigned flags, ErrRec *err, char *scratch,
+                           int slots );
 
 } // namespace sdot
