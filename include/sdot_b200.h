@@ -191,6 +191,8 @@ enum sdot_option {
     SDOT_OPT_LIN_PRECISION,       /* 0 FP64 CG; 1 FP32 inner CG with FP64 iterative refinement               */
     SDOT_OPT_AGG_MARGIN,          /* aggregation of near-coincident seeds: merge a pair when c_ij ulp(w) margin  */
                                   /* > the tolerance (sdotplan/Aggregation.h); 0: off; the reference uses 4      */
+    SDOT_OPT_STEP,                /* 0 trials (KMT backtracking); 1 limits (2D: the step brought under the limits */
+                                  /* of the cells below the floor, sdotplan/Newton.h:330-366); 3D takes trials   */
     SDOT_NB_OPTIONS
 };
 #define SDOT_NB_STATS 31          /* the order of SdotPlanNd._STATS (SdotPlanNd.py:100-103)                  */

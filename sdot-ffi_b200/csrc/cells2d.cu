@@ -1008,4 +1008,106 @@ void launch_cells2d_big( const Launch &L, const ProbDev *probs, const OvfList *o
     ++*L.launches;
 }
 
+// ---- THE LIMITS STEP (2D) -------------------------------------------------------------------------------------------
+// The cell of seed s at the weights w + a d, computed by one thread: the box clipped by the bisectors of the neighbours s
+// has in the accepted and in the trial diagram (a superset of the true cell when a neighbour appears in between: the
+// limit is then a little late, and the trial diagram at the step it gives says so), integrated edge by edge.
+constexpr int LIMV = 4 + 2 * CAP2 + 8;
+
+__device__ double lim_cell_mass( const LimDev &L, int s, double a, double px, double py, bool &ok ) {
+    const ProbDev &P = L.P;
+    double X[ LIMV ], Y[ LIMV ], U[ LIMV ], V[ LIMV ];
+    int m = 4;
+    X[ 0 ] = P.lo[ 0 ] - px; Y[ 0 ] = P.lo[ 1 ] - py;
+    X[ 1 ] = P.hi[ 0 ] - px; Y[ 1 ] = P.lo[ 1 ] - py;
+    X[ 2 ] = P.hi[ 0 ] - px; Y[ 2 ] = P.hi[ 1 ] - py;
+    X[ 3 ] = P.lo[ 0 ] - px; Y[ 3 ] = P.hi[ 1 ] - py;
+    const double wi = P.w[ s ] + a * L.d[ s ];
+    for ( int tab = 0; tab < 2 && m > 0; ++tab ) {
+        const int *nb = tab ? L.nb1 : L.nb0, *nid = tab ? L.nid1 : L.nid0;
+        const int k = nb[ s ];
+        for ( int q = 0; q < k && m > 0; ++q ) {
+            const int j = nid[ size_t( s ) * P.cap + q ];
+            const double qx = P.pos[ 2 * size_t( j ) ] - px, qy = P.pos[ 2 * size_t( j ) + 1 ] - py;
+            const double off = 0.5 * ( ( wi - ( P.w[ j ] + a * L.d[ j ] ) ) + ( qx * qx + qy * qy ) );
+            int m2 = 0;
+            for ( int v = 0; v < m; ++v ) {
+                const int v1 = v + 1 == m ? 0 : v + 1;
+                const double s0 = qx * X[ v ] + qy * Y[ v ] - off, s1 = qx * X[ v1 ] + qy * Y[ v1 ] - off;
+                if ( m2 + 2 > LIMV ) { ok = false; return 0; }
+                if ( s0 <= 0 ) { U[ m2 ] = X[ v ]; V[ m2 ] = Y[ v ]; ++m2; }
+                if ( ( s0 <= 0 ) != ( s1 <= 0 ) ) {
+                    // from the kept end (the two cells of an edge make the same point)
+                    const int ui = s0 <= 0 ? v : v1, vi = s0 <= 0 ? v1 : v;
+                    const double su = s0 <= 0 ? s0 : s1, sv = s0 <= 0 ? s1 : s0, tt = su / ( su - sv );
+                    U[ m2 ] = X[ ui ] + tt * ( X[ vi ] - X[ ui ] );
+                    V[ m2 ] = Y[ ui ] + tt * ( Y[ vi ] - Y[ ui ] );
+                    ++m2;
+                }
+            }
+            m = m2;
+            for ( int v = 0; v < m; ++v ) { X[ v ] = U[ v ]; Y[ v ] = V[ v ]; }
+        }
+    }
+    double mass = 0;
+    const int iref = P.dkind == D_IMAGE ? int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) ) : 0;
+    for ( int v = 0; v < m; ++v ) {
+        const int v1 = v + 1 == m ? 0 : v + 1;
+        EdgeInt e;
+        e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+        if ( P.dkind == D_UNIFORM ) edge_uniform( X[ v ], Y[ v ], X[ v1 ], Y[ v1 ], P.rho, false, e );
+        else if ( P.dkind == D_IMAGE ) edge_image( P, px, py, iref, X[ v ], Y[ v ], X[ v1 ], Y[ v1 ], false, e );
+        else edge_gauss( P, px, py, X[ v ], Y[ v ], X[ v1 ], Y[ v1 ], false, false, e );
+        mass += e.m;
+    }
+    return mass;
+}
+
+// the first a in ( 0, t ] where the mass of cell s falls below eps: the first of 8 even samples below it, then 30
+// bisections; t when no sample falls below (on these neighbours), 0 when the cell starts below, t / 2 past the capacity
+__device__ double lim_alpha( const LimDev &L, int s ) {
+    const double px = L.P.pos[ 2 * size_t( s ) ], py = L.P.pos[ 2 * size_t( s ) + 1 ];
+    bool ok = true;
+    const double m0 = lim_cell_mass( L, s, 0.0, px, py, ok );
+    if ( ! ok ) return 0.5 * L.t;
+    if ( ! ( m0 >= L.eps ) ) return 0.0;
+    double lo = 0, hi = -1;
+    for ( int k = 1; k <= 8; ++k ) {
+        const double a = L.t * k / 8;
+        const double m = lim_cell_mass( L, s, a, px, py, ok );
+        if ( ! ok ) return 0.5 * L.t;
+        if ( m < L.eps ) { hi = a; break; }
+        lo = a;
+    }
+    if ( hi < 0 ) return L.t;
+    for ( int it = 0; it < 30; ++it ) {
+        const double mid = 0.5 * ( lo + hi );
+        const double m = lim_cell_mass( L, s, mid, px, py, ok );
+        if ( ! ok ) break;
+        if ( m < L.eps ) hi = mid;
+        else lo = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__( CHUNK ) k_limits2d( const LimDev *__restrict__ lims, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const LimDev &L = lims[ ch.prob ];
+    for ( int s = ch.begin + int( threadIdx.x ); s < ch.end; s += blockDim.x ) {
+        if ( ! ( L.a2[ s ] < L.eps ) ) continue;
+        atomicAdd( L.out, 1.0 );
+        const int cap = L.P.cap;
+        // a row past the table (its facets in the overflow store): the trials' halving for this cell
+        const double alpha = ( L.nb0[ s ] > cap || L.nb1[ s ] > cap ) ? 0.5 * L.t : lim_alpha( L, s );
+        atomicMin( reinterpret_cast<unsigned long long *>( L.out + 1 ), dbl_order( alpha ) );
+    }
+}
+
+void launch_limits2d( const Launch &L, const LimDev *lims, const Chunk *chunks, int nchunks ) {
+    if ( nchunks <= 0 ) return;
+    k_limits2d<<<nchunks, CHUNK, 0, L.stream>>>( lims, chunks, nchunks );
+    ++*L.launches;
+}
+
+
 } // namespace sdot

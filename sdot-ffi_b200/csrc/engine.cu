@@ -462,6 +462,11 @@ struct SolveJob {
     bool redo = false;
     double h_tprev = 0, h_sprev = 0;
     bool h_has = false;
+    // the limits step (2D, sdotplan/Newton.h:330-366): the first trial at `beta`, kept from one iteration to the next;
+    // while a probe diagram has cells below the floor, the step is brought under their limits (8 rounds at most)
+    bool lim_on = false, lim_probe = false;
+    double beta = 0.25, t_done = 0;
+    int lim_round = 0;
     std::vector<double> scales;
     int stage = 0;
     double stats[ SDOT_NB_STATS ];
@@ -637,6 +642,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         J->cap = D.dim == 2 ? CAP2 : CAP3;
         std::memcpy( J->opt, desc.options, sizeof( J->opt ) );
         J->agg_margin = J->opt[ SDOT_OPT_AGG_MARGIN ];
+        J->lim_on = D.dim == 2 && int( J->opt[ SDOT_OPT_STEP ] ) == 1;     // (3D: the trials, as the reference)
         for ( int k = 0; k < SDOT_NB_STATS; ++k ) J->stats[ k ] = 0;
         const long n = D.n;
         if ( desc.nu ) to_host_vec( c, J->nu_user, desc.nu, n, D.memory );
@@ -805,6 +811,13 @@ static void set_stage_density( Ctx &c, SolveJob &J ) {
     for ( int k = 0; k < J.G.dn[ 0 ]; ++k ) g[ k * st + dim ] = std::sqrt( g[ k * st + dim ] * g[ k * st + dim ] + s * s );
     CK( cudaMemcpyAsync( J.G.dval, g.data(), g.size() * 8, cudaMemcpyHostToDevice, c.stream ) );
     CK( cudaStreamSynchronize( c.stream ) );       // `g` leaves scope
+}
+
+static double order_dbl_host( unsigned long long u ) {
+    u = ( u >> 63 ) ? ( u & 0x7fffffffffffffffull ) : ~u;
+    double x;
+    std::memcpy( &x, &u, 8 );
+    return x;
 }
 
 static void end_stage( Ctx &c, SolveJob &J );
@@ -1059,6 +1072,36 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
             ++J.nb_evals;
             ++J.trial;
             B = rep_host( c, J, 1 - J.repA );
+            if ( J.lim_probe ) {
+                // THE LIMITS (sdotplan/Newton.h:336-366): cells below the floor at this probe bring the step under their
+                // limits; none: this diagram is the damping's first trial
+                const double *S = c.hscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_LIM;
+                const double nbad = S[ 0 ];
+                bool end_probe = true;
+                if ( nbad > 0 ) {
+                    J.stats[ ST_NB_LIMIT_ROUNDS ] += 1;
+                    J.stats[ ST_NB_CELL_LIM ] += nbad;
+                    unsigned long long bits;
+                    std::memcpy( &bits, S + 1, 8 );
+                    const double al = std::min( J.t, order_dbl_host( bits ) );
+                    J.t_done = J.t;
+                    J.t = 0.9 * al;
+                    ++J.lim_round;
+                    if ( J.t < J.opt[ SDOT_OPT_T_MIN ] ) J.t = J.t_done / 2;     // no reason to stagnate: the trials, from half
+                    else end_probe = J.lim_round >= 8;
+                }
+                if ( end_probe ) {
+                    J.lim_probe = false;
+                    if ( J.t >= J.beta ) J.beta = std::min( 1.0, 2 * J.beta );  // a direct pass: the next probe goes further
+                    J.trial = 0;
+                }
+                if ( nbad > 0 ) {
+                    J.pend |= P_TRIAL;
+                    J.state = J_TRIAL;
+                    break;
+                }
+                J.trial = 1;
+            }
             double m2 = B[ R_AMIN ], n2r = merit_of( B, J.res_cur );
             bool ok = m2 >= J.eps && std::isfinite( n2r );
             if ( ok && n2r <= ( 1 - J.t / 2 ) * J.nr && n2r < J.nr ) {
@@ -1117,6 +1160,7 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
             } else {
                 J.pend |= P_GAUGE | P_TRIAL;
                 J.t = std::min( 1.0, J.opt[ SDOT_OPT_MULT_OK ] * J.t_last );
+                if ( J.lim_on ) { J.t = J.beta; J.lim_probe = true; J.lim_round = 0; }
                 J.trial = 0;
                 J.nb_evals = 0;
                 J.h_has = false;
@@ -1460,6 +1504,18 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         launch_report( L, reinterpret_cast<ProbDev *>( d ), reinterpret_cast<Chunk *>( d + oq ), int( QC.size() ) );
         CK( cudaStreamSynchronize( c.stream ) );       // `buf` leaves scope
     };
+    // the limits step's probes of this tick: their descriptors (uploaded once), launched after the diagrams, and again after
+    // a big-cell pass (which completes the masses the kernel reads)
+    struct LimLaunch { char *d = nullptr; size_t off = 0; int nch = 0; std::vector<SolveJob *> js; } LL;
+    auto limits_launch = [&]() {
+        if ( LL.js.empty() ) return;
+        for ( SolveJob *J : LL.js ) {
+            double *o = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_LIM;
+            CK( cudaMemsetAsync( o, 0, 8, c.stream ) );
+            CK( cudaMemsetAsync( o + 1, 0xff, 8, c.stream ) );
+        }
+        launch_limits2d( L, reinterpret_cast<LimDev *>( LL.d ), reinterpret_cast<Chunk *>( LL.d + LL.off ), LL.nch );
+    };
     std::vector<Chunk> C2, C3, CR;
     std::vector<SolveJob *> with_diag;
     for ( SolveJob *J : jobs ) {
@@ -1567,6 +1623,44 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         c.timer.end( c.stream );
     }
     agg_reports();
+    {
+        std::vector<LimDev> LD;
+        std::vector<Chunk> LC;
+        for ( SolveJob *J : with_diag ) {
+            if ( J->state != J_TRIAL || ! J->lim_probe ) continue;
+            LimDev D;
+            std::memset( &D, 0, sizeof( D ) );
+            J->G.fill( D.P );
+            D.P.cap = J->cap;
+            D.P.w = J->w;
+            D.d = J->d;
+            D.a2 = J->a2;
+            D.nb0 = J->nb[ J->cur ]; D.nid0 = J->nid[ J->cur ];
+            D.nb1 = J->nb[ 1 - J->cur ]; D.nid1 = J->nid[ 1 - J->cur ];
+            D.eps = J->eps;
+            D.t = J->t;
+            D.out = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_LIM;
+            const int li = int( LD.size() );
+            LD.push_back( D );
+            int k = 0;
+            for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) LC.push_back( Chunk{ li, b, std::min( J->G.n, b + CHUNK ), k } );
+            LL.js.push_back( J );
+        }
+        if ( ! LD.empty() ) {
+            LL.off = ( LD.size() * sizeof( LimDev ) + 255 ) & ~size_t( 255 );
+            std::vector<char> buf( LL.off + LC.size() * sizeof( Chunk ) );
+            std::memcpy( buf.data(), LD.data(), LD.size() * sizeof( LimDev ) );
+            std::memcpy( buf.data() + LL.off, LC.data(), LC.size() * sizeof( Chunk ) );
+            LL.d = ( char * ) dalloc( c, buf.size() );
+            c.desc_spill.push_back( LL.d );
+            LL.nch = int( LC.size() );
+            CK( cudaMemcpyAsync( LL.d, buf.data(), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
+            c.timer.begin( c.stream, K_CELLS2D, 0.0 );
+            limits_launch();
+            c.timer.end( c.stream );
+            CK( cudaStreamSynchronize( c.stream ) );       // `buf` leaves scope
+        }
+    }
     // B. CG iterations
     VecBatch cgj, cgm;
     std::vector<SolveJob *> with_cg;
@@ -1629,6 +1723,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             launch_report( L, dp, dc, int( rc.size() ) );
         }
         agg_reports();
+        limits_launch();
         CK( cudaMemcpyAsync( c.hscal, c.dscal, size_t( top ) * SLOT_DOUBLES * 8, cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );

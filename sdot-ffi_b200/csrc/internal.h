@@ -94,6 +94,19 @@ struct ProbDev {
     int poff[ MAX_LEV ];
 };
 
+// THE LIMITS STEP (2D; sdotplan/Bounds.h:1-40, gpu/Newton2D.cuh:538-776): for each cell of a trial diagram below the
+// mass floor, the first step along the Newton direction where its mass falls below the floor, the cell computed alone
+// from the neighbours it has in the accepted and in the trial diagram
+struct LimDev {
+    ProbDev P;                    // geometry and density; P.w the accepted weights (ranked)
+    const double *d;              // the Newton direction (ranked)
+    const double *a2;             // the trial's masses (ranked)
+    const int *nb0, *nid0;        // the accepted diagram's neighbour table
+    const int *nb1, *nid1;        // the trial's
+    double eps, t;                // the mass floor, the trial step (the horizon of the search)
+    double *out;                  // [0] the cells below the floor, [1] the smallest limit (ordered integer, atomic min)
+};
+
 // cells the warp-register kernel could not hold (more than 32 vertices, or more facets than the table's row):
 // queued here and rebuilt by the global-memory kernel
 struct OvfItem { int prob; int seed; };
@@ -309,6 +322,8 @@ void launch_mg_up( const Launch &L, const MgLevel *lv, const VecDev *vs, const C
 void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 
 // cells2d.cu / cells3d.cu
+// the limits of the cells below the floor (one thread a cell; chunks of CHUNK cells over the LimDev array)
+void launch_limits2d( const Launch &L, const LimDev *lims, const Chunk *chunks, int nchunks );
 void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
 // the queued big cells (count known on the host), polygons in `scratch` (VBIG vertices x 2 buffers per warp)
 void launch_cells2d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, char *scratch,

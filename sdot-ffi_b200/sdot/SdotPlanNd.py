@@ -27,6 +27,9 @@ _INT_STATS = ("nb_iter", "nb_diag", "nb_backtracks", "nb_overflowed", "nb_cell_l
 #: the aggregation's margin `kappa` (SdotPlanNd.py:118): a pair is merged when its floor c_ij ulp(w) is within kappa of
 #: the tolerance; and the weight gap of an exact duplicate, relative to the cloud's squared extent (SdotPlanNd.py:121)
 _AGGREGATE_MARGIN = 4.0
+
+#: `Tuning.step`: the trials of KMT's damping, or the limits of the cells below the floor (2D; 3D takes the trials)
+_STEP = {"auto": 0, "trials": 0, "limits": 1}
 _DUPLICATE_GAP = 1e-6
 
 
@@ -48,8 +51,8 @@ def exact_duplicates(positions):
 def solver_options(settings, n):
     """the option vector of `sdot_solve_desc` from `Iterative` / `Tuning`"""
     tun = settings.tuning
-    if tun.step not in ("auto", "trials"):
-        raise NotImplementedError(f"step = {tun.step!r}: this build takes the TRIALS step ( 'auto' or 'trials' )")
+    if tun.step not in ("auto", "trials", "limits"):
+        raise ValueError(f"unknown step : {tun.step!r} ( 'auto', 'trials' or 'limits' )")
     if tun.residual not in _RESIDUAL:
         raise ValueError(f"unknown residual: {tun.residual!r} ( {', '.join(_RESIDUAL)} )")
     if tun.linear_solver not in ("auto", "cg", "mg", "amg"):
@@ -62,7 +65,8 @@ def solver_options(settings, n):
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
                 lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0,
-                agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0))
+                agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0),
+                step=_STEP[tun.step])
 
 
 def _box_of(problem):

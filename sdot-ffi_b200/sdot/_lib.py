@@ -21,7 +21,7 @@ DENSITY_UNIFORM, DENSITY_IMAGE, DENSITY_GAUSSIANS = 0, 1, 2
 
 OPTIONS = ["tol_abs", "tol_rel", "maxit", "max_backtracks", "t_min", "mult_ok", "residual", "power", "switch", "lin_tol", "lin_maxit",
            "keep_start", "continuation", "conv_threshold", "conv_s0", "conv_ratio", "conv_min", "lin_method", "precision", "lin_precision",
-           "agg_margin"]
+           "agg_margin", "step"]
 NB_OPTIONS = len(OPTIONS)
 NB_STATS = 31
 NB_HIST = 8

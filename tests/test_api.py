@@ -46,8 +46,10 @@ def test_settings_map_onto_the_option_vector():
     o = solver_options(Iterative(tol=0, tuning=Tuning(mass_rtol=1e-8, residual="lin")), 10)
     assert o["tol_abs"] == 0 and o["tol_rel"] == 1e-8 and o["residual"] == 0 and o["continuation"] == 1
     assert o["lin_method"] == 1 and solver_options(Iterative(tuning=Tuning(linear_solver="cg")), 10)["lin_method"] == 0
-    with pytest.raises(NotImplementedError):
-        solver_options(Iterative(tuning=Tuning(step="limits")), 10)
+    assert solver_options(Iterative(tuning=Tuning(step="limits")), 10)["step"] == 1
+    assert solver_options(Iterative(tuning=Tuning(step="trials")), 10)["step"] == 0
+    with pytest.raises(ValueError):
+        solver_options(Iterative(tuning=Tuning(step="bisection")), 10)
     with pytest.raises(NotImplementedError):
         solver_options(Iterative(precision="mixed"), 10)
     with pytest.raises(ValueError):

@@ -308,3 +308,52 @@ def test_an_almost_empty_image_takes_the_blur_continuation():
     plan = OtProblem(SumOfDiracs(pos), img).solve(Iterative(max_iter=100, tuning=Tuning(mass_rtol=1e-6)))
     assert plan.converged and plan.stats["nb_continuation_steps"] > 1, plan.stats
     assert np.allclose(plan.cell_masses, plan.target_masses, rtol=1e-5)
+
+
+def _scattered_target(d, nb_gaussians, seed, sigma=0.13):
+    """tests/test_SdotPlanNd.py:24-32: narrow, separate bumps over [0.3, 0.7]^d (the hard case of the damping)"""
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0.3, 0.7, size=(nb_gaussians, d))
+    return sdot.SumOfGaussians(pos, np.full(nb_gaussians, sigma), weights=rng.uniform(0.7, 1.3, nb_gaussians))
+
+
+def test_the_limits_step_reaches_the_same_plan_with_fewer_diagrams():
+    """tests/test_SdotPlanNd.py:349-371: `step = "limits"` gives the weights of the trials with fewer diagrams, the step
+    brought under the limits of the cells below the floor instead of halved"""
+    rng = np.random.default_rng(81)
+    pos = rng.uniform(0.1, 0.9, size=(60, 2))
+    dst = _scattered_target(2, 4, seed=6)
+    it = dict(max_iter=200, tol=1e-12, continuation="never")
+    a = OtProblem(SumOfDiracs(pos), dst).solve(Iterative(**it, tuning=Tuning(step="trials", residual="lin")))
+    b = OtProblem(SumOfDiracs(pos), dst).solve(Iterative(**it, tuning=Tuning(step="limits", residual="lin")))
+    assert a.converged and b.converged, (a.stats, b.stats)
+    assert np.allclose(a.weights, b.weights, atol=1e-9)
+    assert b.stats["nb_diag"] <= a.stats["nb_diag"], (a.stats["nb_diag"], b.stats["nb_diag"])
+    assert b.stats["nb_cell_lim"] > 0 and b.stats["nb_limit_rounds"] > 0, b.stats
+
+
+@pytest.mark.parametrize("continuation", ["never", "auto"])
+def test_the_limits_step_reaches_the_oracle_plan(continuation):
+    """tests/test_SdotPlanNd.py:1023-1040: a soft image directly, and an image with a hole through the continuation, with
+    the limits step: the plan of the oracle's trials"""
+    rng = np.random.default_rng(201)
+    n = 1500
+    pos = rng.uniform(0.001, 0.999, size=(n, 2))
+    nu = rng.uniform(0.5, 1.5, n)
+    nu /= nu.sum()
+    if continuation == "never":
+        vals = 1 + 2 * rng.random((24, 17))
+    else:
+        vals = 0.1 + 0.9 * rng.random((32, 32))
+        vals[4:12, 18:28] = 0
+        vals[20:23, :] += 4
+    step = [1 / vals.shape[0], 1 / vals.shape[1]]
+    img = sdot.Image(vals, frame=step)
+    plan = OtProblem(SumOfDiracs(pos, nu), img).solve(Iterative(tol=1e-10 / n, max_iter=80, continuation=continuation,
+                                                                tuning=Tuning(step="limits")))
+    assert plan.converged, plan.stats
+    norm = img.normalized_version()
+    ref = O.solve(pos, nu=nu, tol_abs=1e-10 / n, maxit=80, continuation={"never": 0, "auto": 1}[continuation],
+                  density=("image", [0, 0], step, norm.values))
+    assert ref["stats"]["status"] == 1
+    assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
