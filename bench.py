@@ -455,7 +455,9 @@ def main():
                      "frac": achieved / hbm if achieved else None, "traffic": traffic_of("k_cells2d"), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_cell": BYTES_PER_CELL[2], "cells_per_launch": units / max(nl, 1),
                      "avg_launch_ms": ms / max(nl, 1), "cg_ms_share": cg_ms / max(1e-9, 1000 * secs),
-                     "cells_ms_share": ms / max(1e-9, 1000 * secs)},
+                     "cells_ms_share": ms / max(1e-9, 1000 * secs),
+                     "kernel_ms": {k: round(v[0], 3) for k, v in kst.items()},
+                     "busy_share": sum(v[0] for v in kst.values()) / max(1e-9, 1000 * secs)},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),

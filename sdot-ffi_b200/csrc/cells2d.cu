@@ -421,32 +421,6 @@ __device__ __forceinline__ void record_error( const ProbDev &P, ErrRec *err, int
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
 }
 
-// per-warp accumulators of the Newton report (lane 0 holds them)
-struct Rep {
-    double v[ NB_REPORT ];
-    SDOT_DEV void init() {
-        v[ R_WORST ] = 0; v[ R_WORST_REL ] = 0; v[ R_AMIN ] = 1e300; v[ R_ASUM ] = 0; v[ R_LIN2 ] = 0;
-        v[ R_GCOUNT ] = 0; v[ R_GMEAN ] = 0; v[ R_GM2 ] = 0; v[ R_SU ] = 0; v[ R_SUG ] = 0; v[ R_NUSUM ] = 0; v[ R_NEMPTY ] = 0;
-    }
-    SDOT_DEV void combine( const double *o ) {   // Chan's parallel combination for the mean / M2 of g
-        v[ R_WORST ] = fmax( v[ R_WORST ], o[ R_WORST ] );
-        v[ R_WORST_REL ] = fmax( v[ R_WORST_REL ], o[ R_WORST_REL ] );
-        v[ R_AMIN ] = fmin( v[ R_AMIN ], o[ R_AMIN ] );
-        v[ R_ASUM ] += o[ R_ASUM ];
-        v[ R_LIN2 ] += o[ R_LIN2 ];
-        double na = v[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
-        if ( nb > 0 ) {
-            double d = o[ R_GMEAN ] - v[ R_GMEAN ];
-            v[ R_GMEAN ] += d * nb / n;
-            v[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
-            v[ R_GCOUNT ] = n;
-        }
-        v[ R_SU ] += o[ R_SU ];
-        v[ R_SUG ] += o[ R_SUG ];
-        v[ R_NUSUM ] += o[ R_NUSUM ];
-        v[ R_NEMPTY ] += o[ R_NEMPTY ];
-    }
-};
 
 __device__ __forceinline__ double g_of( double x, int r, double p ) {
     x = fmax( x, 1e-300 );
@@ -459,7 +433,7 @@ __device__ __forceinline__ double gp_of( double x, int r, double p ) {
     return r == 1 ? 1 / x : 1;
 }
 
-// the report of one problem's chunk, written by its block; the last block of the problem folds them in order
+// the report of one problem's chunk, written by its block; the last block of the problem folds them (fixed tree)
 __device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )[ NB_REPORT ] ) {
     __shared__ int am_last;
     __syncthreads();
@@ -474,18 +448,9 @@ __device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )
         am_last = prev == unsigned( P.nchunk - 1 );
     }
     __syncthreads();
-    if ( am_last && threadIdx.x == 0 ) {
+    if ( am_last ) {
         __threadfence();
-        Rep r;
-        r.init();
-        for ( int c = 0; c < P.nchunk; ++c ) {
-            double o[ NB_REPORT ];
-            const volatile double *src = P.partials + ( size_t ) c * NB_REPORT;
-            for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ k ];
-            r.combine( o );
-        }
-        for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r.v[ k ];
-        *P.counter = 0;
+        fold_reports_block( P );
     }
     __syncthreads();
 }

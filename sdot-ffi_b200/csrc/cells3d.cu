@@ -765,45 +765,23 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
         for ( int s = ch.begin + warp; s < ch.end; s += W3 )
             cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, ( flags & F_REPORT ) ? rep : nullptr, false );
                 if ( flags & F_REPORT ) {
-                    // the chunk's report, then the last chunk of the problem folds them in chunk order
+                    // the chunk's report, then the last block of the problem folds them (fixed tree)
                     if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
                     __syncthreads();
                     if ( threadIdx.x == 0 ) {
-                        double r[ NB_REPORT ];
-                        for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = sh_rep[ 0 ][ k ];
-                        auto fold = [&]( const double *o ) {
-                            r[ R_WORST ] = fmax( r[ R_WORST ], o[ R_WORST ] );
-                            r[ R_WORST_REL ] = fmax( r[ R_WORST_REL ], o[ R_WORST_REL ] );
-                            r[ R_AMIN ] = fmin( r[ R_AMIN ], o[ R_AMIN ] );
-                            r[ R_ASUM ] += o[ R_ASUM ];
-                            r[ R_LIN2 ] += o[ R_LIN2 ];
-                            double na = r[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
-                            if ( nb > 0 ) {
-                                double d = o[ R_GMEAN ] - r[ R_GMEAN ];
-                                r[ R_GMEAN ] += d * nb / n;
-                                r[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
-                                r[ R_GCOUNT ] = n;
-                            }
-                            r[ R_SU ] += o[ R_SU ]; r[ R_SUG ] += o[ R_SUG ]; r[ R_NUSUM ] += o[ R_NUSUM ]; r[ R_NEMPTY ] += o[ R_NEMPTY ];
-                        };
-                        for ( int w = 1; w < W3; ++w ) fold( sh_rep[ w ] );
+                        Rep r;
+                        for ( int k = 0; k < NB_REPORT; ++k ) r.v[ k ] = sh_rep[ 0 ][ k ];
+                        for ( int w = 1; w < W3; ++w ) r.combine( sh_rep[ w ] );
                         double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
-                        for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r[ k ];
+                        for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r.v[ k ];
                         __threadfence();
                         unsigned prev = atomicAdd( P.counter, 1u );
                         sh_last = prev == unsigned( P.nchunk - 1 );
-                        if ( sh_last ) {
-                            __threadfence();
-                            const volatile double *src = P.partials;
-                            for ( int k = 0; k < NB_REPORT; ++k ) r[ k ] = src[ k ];
-                            for ( int c = 1; c < P.nchunk; ++c ) {
-                                double o[ NB_REPORT ];
-                                for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ ( size_t ) c * NB_REPORT + k ];
-                                fold( o );
-                            }
-                            for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = r[ k ];
-                            *P.counter = 0;
-                        }
+                    }
+                    __syncthreads();
+                    if ( sh_last ) {
+                        __threadfence();
+                        fold_reports_block( P );
                     }
                     __syncthreads();
                 }

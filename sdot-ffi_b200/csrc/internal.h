@@ -223,6 +223,65 @@ SDOT_DEV double order_dbl( unsigned long long u ) {
     return __longlong_as_double( ( u >> 63 ) ? ( u & 0x7fffffffffffffffull ) : ~u );
 }
 
+// accumulators of the Newton report of a warp, a chunk or a problem (Chan's parallel combination for the mean / M2
+// of g); combined in a fixed order, so that a report is bitwise reproducible
+struct Rep {
+    double v[ NB_REPORT ];
+    SDOT_DEV void init() {
+        v[ R_WORST ] = 0; v[ R_WORST_REL ] = 0; v[ R_AMIN ] = 1e300; v[ R_ASUM ] = 0; v[ R_LIN2 ] = 0;
+        v[ R_GCOUNT ] = 0; v[ R_GMEAN ] = 0; v[ R_GM2 ] = 0; v[ R_SU ] = 0; v[ R_SUG ] = 0; v[ R_NUSUM ] = 0; v[ R_NEMPTY ] = 0;
+    }
+    SDOT_DEV void combine( const double *o ) {   // Chan's parallel combination for the mean / M2 of g
+        v[ R_WORST ] = fmax( v[ R_WORST ], o[ R_WORST ] );
+        v[ R_WORST_REL ] = fmax( v[ R_WORST_REL ], o[ R_WORST_REL ] );
+        v[ R_AMIN ] = fmin( v[ R_AMIN ], o[ R_AMIN ] );
+        v[ R_ASUM ] += o[ R_ASUM ];
+        v[ R_LIN2 ] += o[ R_LIN2 ];
+        double na = v[ R_GCOUNT ], nb = o[ R_GCOUNT ], n = na + nb;
+        if ( nb > 0 ) {
+            double d = o[ R_GMEAN ] - v[ R_GMEAN ];
+            v[ R_GMEAN ] += d * nb / n;
+            v[ R_GM2 ] += o[ R_GM2 ] + d * d * na * nb / n;
+            v[ R_GCOUNT ] = n;
+        }
+        v[ R_SU ] += o[ R_SU ];
+        v[ R_SUG ] += o[ R_SUG ];
+        v[ R_NUSUM ] += o[ R_NUSUM ];
+        v[ R_NEMPTY ] += o[ R_NEMPTY ];
+    }
+};
+
+// the last block of a problem folds its chunks' reports: thread t the chunks t, t + blockDim, ... in order, then the
+// lanes of each warp by a shuffle tree, then the warps in order -- a fixed tree, whatever the scheduling. Every thread
+// of the block calls it (blockDim a multiple of 32); the result goes to P.report and the problem's counter is reset
+__device__ __forceinline__ void fold_reports_block( const ProbDev &P ) {
+    __shared__ double sh_fold[ 32 ][ NB_REPORT ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = int( blockDim.x >> 5 );
+    Rep r;
+    r.init();
+    for ( int c = threadIdx.x; c < P.nchunk; c += blockDim.x ) {
+        double o[ NB_REPORT ];
+        const volatile double *src = P.partials + ( size_t ) c * NB_REPORT;
+        for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = src[ k ];
+        r.combine( o );
+    }
+    for ( int off = 16; off > 0; off >>= 1 ) {
+        double o[ NB_REPORT ];
+        for ( int k = 0; k < NB_REPORT; ++k ) o[ k ] = __shfl_down_sync( 0xffffffffu, r.v[ k ], off );
+        if ( lane < off ) r.combine( o );
+    }
+    if ( lane == 0 )
+        for ( int k = 0; k < NB_REPORT; ++k ) sh_fold[ warp ][ k ] = r.v[ k ];
+    __syncthreads();
+    if ( threadIdx.x == 0 ) {
+        Rep f;
+        f.init();
+        for ( int w = 0; w < nw; ++w ) f.combine( sh_fold[ w ] );
+        for ( int k = 0; k < NB_REPORT; ++k ) P.report[ k ] = f.v[ k ];
+        *P.counter = 0;
+    }
+}
+
 // ---- weight majorants -------------------------------------------------------------------------------------------------
 // b of majorant record `node` (the grid's own cells are nodes 0 .. ncell - 1, with a = 0: b is their max weight)
 SDOT_DEV double wmaj_b( const ProbDev &P, size_t node ) {

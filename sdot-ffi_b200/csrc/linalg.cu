@@ -7,9 +7,9 @@
 // come out in table order, which is deterministic.  `dia` = the row sum, 1 for an empty row.
 //
 // CG: preconditioned by the diagonal, FP64, one chunk of VCHUNK rows per block.  Every reduction is a
-// fixed tree inside the block, then a fold of the chunk partials in chunk order by the last block of the
-// problem to finish (a counter per problem): bitwise reproducible whatever the scheduling, the
-// reference's requirement too (gpu/Reduce.cuh:3-20, gpu/Linear2D.cuh:39-41).
+// fixed tree inside the block, then a fixed-tree fold of the chunk partials by the last block of the problem to
+// finish (a counter per problem): bitwise reproducible whatever the scheduling, the reference's requirement too
+// (gpu/Reduce.cuh:3-20, gpu/Linear2D.cuh:39-41).
 #include "internal.h"
 #include <cub/block/block_scan.cuh>
 
@@ -39,8 +39,8 @@ __device__ __forceinline__ void block_sum( double ( &v )[ NV ] ) {
     __syncthreads();
 }
 
-// thread 0 of the chunk writes its partials; returns true in thread 0 of the last chunk of the problem,
-// which then holds the folded sums in `tot`
+// thread 0 of the chunk writes its partials; the last block of the problem folds them -- thread t the chunks t, t + VT,
+// ... in order, then the block's fixed tree -- and returns true in its thread 0, which then holds the sums in `tot`
 template<int NV>
 __device__ __forceinline__ bool fold_last( const VecDev &V, const Chunk &ch, const double ( &v )[ NV ], double ( &tot )[ NV ] ) {
     __shared__ int last;
@@ -51,20 +51,24 @@ __device__ __forceinline__ bool fold_last( const VecDev &V, const Chunk &ch, con
         __threadfence();
         unsigned prev = atomicAdd( V.counter, 1u );
         last = prev == unsigned( V.nchunk - 1 );
-        if ( last ) {
-            __threadfence();
-#pragma unroll
-            for ( int k = 0; k < NV; ++k ) tot[ k ] = 0;
-            for ( int c = 0; c < V.nchunk; ++c ) {
-                const volatile double *src = V.partials + ( size_t ) c * 4;
-#pragma unroll
-                for ( int k = 0; k < NV; ++k ) tot[ k ] += src[ k ];
-            }
-            *V.counter = 0;
-        }
     }
     __syncthreads();
-    return threadIdx.x == 0 && last;
+    if ( ! last ) return false;
+    __threadfence();
+    double acc[ NV ];
+#pragma unroll
+    for ( int k = 0; k < NV; ++k ) acc[ k ] = 0;
+    for ( int c = threadIdx.x; c < V.nchunk; c += VT ) {
+        const volatile double *src = V.partials + ( size_t ) c * 4;
+#pragma unroll
+        for ( int k = 0; k < NV; ++k ) acc[ k ] += src[ k ];
+    }
+    block_sum<NV>( acc );
+    if ( threadIdx.x != 0 ) return false;
+#pragma unroll
+    for ( int k = 0; k < NV; ++k ) tot[ k ] = acc[ k ];
+    *V.counter = 0;
+    return true;
 }
 
 // ---- CSR -------------------------------------------------------------------------------------------------------
