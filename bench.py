@@ -327,7 +327,31 @@ def main():
     ap.add_argument("--cells-repeat", type=int, default=0)
     ap.add_argument("--cells-density", default="uniform", choices=["uniform", "gauss"],
                     help="cells-only target: uniform, or a 4-gaussian mixture like the stream's")
+    ap.add_argument("--solve-only", type=int, default=0, help="one solve of this many uniform seeds (for a profiler), then exit")
+    ap.add_argument("--solve-linear", default="auto", choices=["auto", "cg", "mg"])
+    ap.add_argument("--solve-step", default="auto", choices=["auto", "trials", "limits"])
     a = ap.parse_args()
+    if a.solve_only:
+        import sdot
+        from sdot import Iterative, OtProblem, SumOfDiracs, Tuning, _lib
+        d = a.cells_dim
+        pos = np.random.default_rng(a.seed).uniform(size=(a.solve_only, d))
+        dist = sdot.Box(nb_dims=d)
+        if a.cells_density == "gauss":
+            rq = request(a.seed, 0)
+            dist = target_of(dict(rq, d=d, gauss=True, c=np.random.default_rng(a.seed + 2).uniform(0.2, 0.8, size=(4, d))))
+        _lib.set_timing(True)
+        t0 = time.perf_counter()
+        plan = OtProblem(SumOfDiracs(pos), dist).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=RTOL, linear_solver=a.solve_linear,
+                                                                                        step=a.solve_step)))
+        secs = time.perf_counter() - t0
+        st = plan.stats
+        kst = _lib.kernel_stats()
+        print(json.dumps({"solve_only": a.solve_only, "dim": d, "density": a.cells_density, "linear": a.solve_linear, "step": a.solve_step,
+                          "status": st["status"], "seconds": secs, "nb_iter": st["nb_iter"], "nb_diag": st["nb_diag"],
+                          "lin_nb_iter": st["lin_nb_iter"], "kernel_ms": {k: round(v[0], 3) for k, v in kst.items()},
+                          "kernel_launches": {k: v[1] for k, v in kst.items()}}))
+        return
     if a.cells_only:
         import sdot
         from sdot import _lib
