@@ -248,7 +248,9 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         CK( cudaSetDevice( c.device ) );
         const int dim = desc->dim;
         const long n = desc->n;
-        if ( dim != 2 ) throw Error( SDOT_ERR_UNSUPPORTED, "the adjoint of the masses is written for 2D cells" );
+        if ( dim != 2 && dim != 3 ) throw Error( SDOT_ERR_ARGS, "dim must be 2 or 3" );
+        if ( dim == 3 && desc->density.kind != SDOT_DENSITY_UNIFORM )
+            throw Error( SDOT_ERR_UNSUPPORTED, "the adjoint of 3D cells is written for a constant density (as the reference's card)" );
         Geometry G;
         build_geometry( c, G, dim, n, desc->positions, desc->box_lo, desc->box_hi, desc->density, desc->memory );
         struct Free { Ctx &c; Geometry &G; ~Free() { free_geometry( c, G ); } } fg{ c, G };
@@ -281,7 +283,8 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
         launch_wpyr( L, dd.as<ProbDev>(), 1 );
-        launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr, c.dovf );
+        if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr, c.dovf );
+        else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), F_VJP | F_USER_ORDER, c.derr, c.dovf );
         run_big_cells( c, dd.as<ProbDev>(), F_VJP | F_USER_ORDER );
         CK( cudaGetLastError() );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );

@@ -706,6 +706,37 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
             if ( to_store ) P.nid[ ( size_t ) row * P.cap ] = base_at;
         }
     }
+    if ( ( flags & F_VJP ) && ! gauss ) {
+        // THE ADJOINT of the masses (gpu/Cell3D.cuh:1954-1978), a constant density: grad_w_i = sum_j c_ij ( g_i - g_j ),
+        // grad_p_i = sum_j 2 c_ij ( g_i - g_j ) ( x_ij - p_i ), x_ij the facet's centroid -- summed triangle by triangle of
+        // the facets, c_f K T, each with its own centroid (no per-facet storage)
+        const double gi = P.gm[ user_order ? user : s ];
+        double gw = 0, gx = 0, gy = 0, gz = 0;
+        for ( int k = lane; k < nv; k += 32 ) {
+            const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+            for ( int q = 0; q < 3; ++q ) {
+                const int f = e[ q ], b = e[ ( q + 1 ) % 3 ], j = C.pid[ f ];
+                const double a2 = C.area[ 3 * k + q ];
+                if ( j < 0 || a2 == 0 ) continue;
+                const int t = twin_of( C, b, f );
+                if ( t < 0 ) continue;
+                const double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
+                const double cf = C.no[ f ] / nn;
+                const double gj = P.gm[ user_order ? P.user[ j ] : j ];
+                const double coef = rho * a2 / ( 2 * sqrt( nn ) ) * ( gi - gj );
+                gw += coef;
+                gx += 2 * coef * ( C.nx[ f ] * cf + C.vx[ k ] + C.vx[ t ] ) / 3;
+                gy += 2 * coef * ( C.ny[ f ] * cf + C.vy[ k ] + C.vy[ t ] ) / 3;
+                gz += 2 * coef * ( C.nz[ f ] * cf + C.vz[ k ] + C.vz[ t ] ) / 3;
+            }
+        }
+        gw = warp_sum( gw ); gx = warp_sum( gx ); gy = warp_sum( gy ); gz = warp_sum( gz );
+        if ( lane == 0 ) {
+            const int row = user_order ? user : s;
+            if ( P.gw ) P.gw[ row ] = gw;
+            if ( P.gpos ) { P.gpos[ 3 * ( size_t ) row ] = gx; P.gpos[ 3 * ( size_t ) row + 1 ] = gy; P.gpos[ 3 * ( size_t ) row + 2 ] = gz; }
+        }
+    }
     if ( moments ) {
         double mx = warp_sum( fx ), my = warp_sum( fy ), mz = warp_sum( fz ), ss = warp_sum( s2 );
         double vv = mass / rho;

@@ -239,6 +239,35 @@ def test_the_adjoint_is_the_derivative_of_the_measures():
             assert abs(fd - gp[i, a]) < 1e-5 * max(1, abs(fd))
 
 
+def test_the_3d_adjoint_is_the_derivative_of_the_measures():
+    """gpu/Cell3D.cuh:1954-1978: the adjoint of the 3D masses (constant density) against central differences"""
+    rng = np.random.default_rng(7)
+    n = 400
+    pos = rng.uniform(size=(n, 3))
+    w = rng.uniform(0, 1e-3, size=n)
+    g = rng.standard_normal(n)
+    pd = _pd(pos, w)
+    gp, gw = pd.measures_vjp(g)
+    assert gp.shape == (n, 3) and gw.shape == (n,)
+    h = 1e-6
+    for i in range(0, n, 41):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        fd = (g @ _pd(pos, wp).measures - g @ _pd(pos, wm).measures) / (2 * h)
+        assert abs(fd - gw[i]) < 1e-5 * max(1, abs(fd)), (i, fd, gw[i])
+        for a in range(3):
+            pp, pm = pos.copy(), pos.copy()
+            pp[i, a] += h
+            pm[i, a] -= h
+            fd = (g @ _pd(pp, w).measures - g @ _pd(pm, w).measures) / (2 * h)
+            assert abs(fd - gp[i, a]) < 1e-5 * max(1, abs(fd)), (i, a, fd, gp[i, a])
+    # the weights' part is the Laplacian's action: grad_w = L g (rows of c_ij)
+    row, cols, vals, dia = pd.laplacian()
+    Lg = dia * g - np.array([vals[row[i]:row[i + 1]] @ g[cols[row[i]:row[i + 1]]] for i in range(n)])
+    assert np.abs(gw - Lg).max() < 1e-9 * np.abs(Lg).max()
+
+
 def test_a_seed_with_hundreds_of_neighbours_is_solved():
     """tests/test_SdotPlanNd.py:1280-1300: a ring of 600 seeds around one seed -- its cell has 600 vertices, far past
     the 32 a warp holds in registers: the global-memory pass rebuilds it, and the facet table grows to hold its row"""
