@@ -1194,7 +1194,7 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.a = J.a;
     V.w = J.w; V.w2 = J.w2; V.d = J.d;
     V.t = J.t;
-    V.tol = J.opt[ SDOT_OPT_LIN_TOL ] > 0 ? J.opt[ SDOT_OPT_LIN_TOL ] : 1e-8;
+    V.tol = J.opt[ SDOT_OPT_LIN_TOL ] > 0 ? J.opt[ SDOT_OPT_LIN_TOL ] : 1e-6;     // the card's default (gpu/Linear2D.cuh:82)
     V.maxit = J.opt[ SDOT_OPT_LIN_MAXIT ] > 0 ? int( J.opt[ SDOT_OPT_LIN_MAXIT ] ) : 20000;
     V.report = rep_dev( c, J, J.repA );
     V.wmax_slot = J.wslot + ( 1 - J.wcur );

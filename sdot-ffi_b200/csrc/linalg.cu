@@ -255,17 +255,35 @@ __global__ void __launch_bounds__( VT ) k_cg_init( const VecDev *__restrict__ vs
     }
 }
 
+// q = L p: LPR lanes per row (the reference's `lanes`, gpu/Linear2D.cuh:96), each lane every LPR-th entry of the row,
+// the lanes' sums folded by a fixed shuffle tree -- independent loads in flight, deterministic sums
+constexpr int LPR = 4;
+__device__ __forceinline__ double row_dot_lanes( const VecDev &V, int i, int sub, const double *__restrict__ x ) {
+    double t = 0;
+    const int e1 = V.row_ptr[ i + 1 ];
+    for ( int e = V.row_ptr[ i ] + sub; e < e1; e += LPR ) t += V.val[ e ] * x[ V.col[ e ] ];
+#pragma unroll
+    for ( int o = 1; o < LPR; o <<= 1 ) t += __shfl_xor_sync( 0xffffffffu, t, o, LPR );
+    return t;
+}
+
 __global__ void __launch_bounds__( VT ) k_cg_spmv( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];
     const VecDev &V = vs[ ch.prob ];
     if ( ! V.active || V.sc[ SC_CONV ] != 0 ) return;
     double pq = 0;
-    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
-        double pi = V.p[ i ];
-        double s = V.dia[ i ] * pi;
-        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) s -= V.val[ e ] * V.p[ V.col[ e ] ];
-        V.q[ i ] = s;
-        pq += pi * s;
+    const int sub = threadIdx.x % LPR;
+    // every lane of a warp takes part in the shuffles: the loop runs to the chunk's end rounded up, rows past it idle
+    for ( int i0 = ch.begin + int( threadIdx.x ) / LPR; i0 < ch.begin + ( ( ch.end - ch.begin + VT / LPR - 1 ) / ( VT / LPR ) ) * ( VT / LPR );
+          i0 += VT / LPR ) {
+        const bool in = i0 < ch.end;
+        const double t = row_dot_lanes( V, in ? i0 : ch.begin, sub, V.p );
+        if ( in && sub == 0 ) {
+            const double pi = V.p[ i0 ];
+            const double s = V.dia[ i0 ] * pi - t;
+            V.q[ i0 ] = s;
+            pq += pi * s;
+        }
     }
     double v[ 1 ] = { pq }, tot[ 1 ];
     block_sum<1>( v );

@@ -61,7 +61,7 @@ def solver_options(settings, n):
         raise NotImplementedError(f"precision = {settings.precision!r}: FP64 cells only in this build")
     return dict(tol_abs=settings.tol, tol_rel=float(tun.mass_rtol), maxit=settings.max_iter, max_backtracks=tun.max_backtracks,
                 t_min=tun.t_min, mult_ok=tun.restart_factor, residual=_RESIDUAL[tun.residual], power=tun.residual_power,
-                switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-8), lin_maxit=int(tun.linear_maxit or 20000),
+                switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-6), lin_maxit=int(tun.linear_maxit or 20000),
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
                 lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0,
