@@ -211,7 +211,22 @@ constexpr float OMEGA = 0.8f;
 // cuts the CG iterations by about a quarter on Voronoi Laplacians
 constexpr float ALPHA = 1.5f;
 
-// pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level; one thread per coarse row
+// the cycle's kernels give MG_LANES lanes to a row: a coarse row's fine rows are split among them (down), a fine row's
+// entries (up); their sums are folded by a fixed shuffle tree (deterministic)
+constexpr int MG_LANES = 4;
+__device__ __forceinline__ float lanes_sum( float t ) {
+#pragma unroll
+    for ( int o = 1; o < MG_LANES; o <<= 1 ) t += __shfl_xor_sync( 0xffffffffu, t, o, MG_LANES );
+    return t;
+}
+// the rows a block's lanes walk: the chunk rounded up to whole passes, so that every lane of a warp reaches each shuffle
+__device__ __forceinline__ int lane_rows_end( const Chunk &ch ) {
+    constexpr int per = MGT / MG_LANES;
+    return ch.begin + ( ( ch.end - ch.begin + per - 1 ) / per ) * per;
+}
+
+// pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level; MG_LANES lanes per coarse
+// row, each lane every MG_LANES-th of its fine rows
 __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
                                                    int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];
@@ -219,10 +234,12 @@ __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ 
     const bool top = M.level == 0;
     const VecDev *V = vs + M.vec;
     if ( V->sc[ SC_CONV ] != 0 ) return;
-    for ( int I = ch.begin + threadIdx.x; I < ch.end; I += blockDim.x ) {
-        const int i0 = I * M.pack, i1 = min( M.n, i0 + M.pack );
+    const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
+    for ( int I = ch.begin + int( threadIdx.x ) / MG_LANES; I < end; I += MGT / MG_LANES ) {
+        const bool in = I < ch.end;
+        const int i0 = I * M.pack, i1 = in ? min( M.n, i0 + M.pack ) : i0;
         float acc = 0;
-        for ( int i = i0; i < i1; ++i ) {
+        for ( int i = i0 + sub; i < i1; i += MG_LANES ) {
             float bi = top ? float( V->r[ i ] ) : M.b[ i ];
             if ( top ) M.b[ i ] = bi;
             float xi = OMEGA * M.dinv[ i ] * bi;
@@ -235,7 +252,8 @@ __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ 
             }
             acc += bi - ax;
         }
-        M.bn[ I ] = acc;
+        acc = lanes_sum( acc );
+        if ( in && sub == 0 ) M.bn[ I ] = acc;
     }
 }
 
@@ -251,23 +269,30 @@ __global__ void __launch_bounds__( 32 ) k_mg_bottom( const MgLevel *__restrict__
     }
 }
 
-// prolongation of the next level's solution and post-smoothing; level 0 writes z (FP64)
+// prolongation of the next level's solution and post-smoothing; level 0 writes z (FP64); MG_LANES lanes per fine row
 __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
                                                  int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
     const VecDev &V = vs[ M.vec ];
     if ( V.sc[ SC_CONV ] != 0 ) return;
-    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
-        float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
-        float s = M.dia[ i ] * xi;
-        for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e ) {
+    const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
+    for ( int i = ch.begin + int( threadIdx.x ) / MG_LANES; i < end; i += MGT / MG_LANES ) {
+        const bool in = i < ch.end;
+        const int r = in ? i : ch.begin;
+        float t = 0;
+        for ( int e = M.rp[ r ] + sub; e < M.rp[ r + 1 ]; e += MG_LANES ) {
             const int j = M.col[ e ];
-            s -= M.val[ e ] * ( M.x[ j ] + ALPHA * M.xn[ j / M.pack ] );
+            t += M.val[ e ] * ( M.x[ j ] + ALPHA * M.xn[ j / M.pack ] );
         }
-        float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
-        if ( M.level == 0 ) V.z[ i ] = double( yi );
-        else M.y[ i ] = yi;
+        t = lanes_sum( t );
+        if ( in && sub == 0 ) {
+            const float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
+            const float s = M.dia[ i ] * xi - t;
+            const float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
+            if ( M.level == 0 ) V.z[ i ] = double( yi );
+            else M.y[ i ] = yi;
+        }
     }
 }
 
