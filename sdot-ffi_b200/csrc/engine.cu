@@ -74,6 +74,8 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
     CK( cudaMemcpyAsync( c.dovf, &hl, sizeof( hl ), cudaMemcpyHostToDevice, c.stream ) );
     CK( cudaMallocHost( &c.hovf, sizeof( int ) ) );
     *c.hovf = 0;
+    c.hstage_bytes = size_t( 16 ) << 20;
+    CK( cudaMallocHost( &c.hstage, c.hstage_bytes ) );
     char *gq = ( char * ) dalloc( c, 256 + size_t( c.giant_cap ) * sizeof( OvfItem ) );
     c.dgiant = ( OvfList * ) gq;
     OvfList gl{ 0, c.giant_cap, ( OvfItem * ) ( gq + 256 ) };
@@ -107,6 +109,7 @@ void ctx_release( Ctx &c ) {
     if ( c.herr ) cudaFreeHost( c.herr );
     if ( c.hovf ) cudaFreeHost( c.hovf );
     if ( c.hgiant ) cudaFreeHost( c.hgiant );
+    if ( c.hstage ) cudaFreeHost( c.hstage );
     if ( c.pool ) cudaMemPoolDestroy( c.pool );
     c = Ctx{};
 }
@@ -201,6 +204,16 @@ static void to_host_vec( Ctx &c, std::vector<T> &dst, const T *src, size_t count
 }
 
 // uploads a descriptor block and returns its device address (stream ordered: the area is reused)
+// a host block for an asynchronous upload: copied into the pinned ring (so that the copy does not wait for the stream),
+// or the block itself when the ring is full (a pageable copy, which the runtime stages)
+static const void *stage( Ctx &c, const void *src, size_t bytes ) {
+    if ( ! c.hstage || c.hstage_used + bytes > c.hstage_bytes ) return src;
+    char *p = c.hstage + c.hstage_used;
+    std::memcpy( p, src, bytes );
+    c.hstage_used += ( bytes + 255 ) & ~size_t( 255 );
+    return p;
+}
+
 static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
     if ( bytes > c.desc_bytes ) {
         for ( auto &g : c.graphs ) cudaGraphExecDestroy( g.exec );
@@ -209,7 +222,7 @@ static char *upload_desc( Ctx &c, const void *src, size_t bytes ) {
         c.desc_bytes = std::max( bytes, size_t( 1 ) << 20 );
         c.desc = ( char * ) dalloc( c, c.desc_bytes );
     }
-    CK( cudaMemcpyAsync( c.desc, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaMemcpyAsync( c.desc, stage( c, src, bytes ), bytes, cudaMemcpyHostToDevice, c.stream ) );
     return c.desc;
 }
 
@@ -222,7 +235,7 @@ static char *upload_desc_at( Ctx &c, const void *src, size_t bytes, size_t offse
         dst = ( char * ) dalloc( c, bytes );
         c.desc_spill.push_back( dst );
     }
-    CK( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaMemcpyAsync( dst, stage( c, src, bytes ), bytes, cudaMemcpyHostToDevice, c.stream ) );
     return dst;
 }
 
@@ -1500,9 +1513,8 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         std::memcpy( buf.data() + oq, QC.data(), QC.size() * sizeof( Chunk ) );
         char *d = ( char * ) dalloc( c, buf.size() );
         c.desc_spill.push_back( d );
-        CK( cudaMemcpyAsync( d, buf.data(), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
+        CK( cudaMemcpyAsync( d, stage( c, buf.data(), buf.size() ), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
         launch_report( L, reinterpret_cast<ProbDev *>( d ), reinterpret_cast<Chunk *>( d + oq ), int( QC.size() ) );
-        CK( cudaStreamSynchronize( c.stream ) );       // `buf` leaves scope
     };
     // the limits step's probes of this tick: their descriptors (uploaded once), launched after the diagrams, and again after
     // a big-cell pass (which completes the masses the kernel reads)
@@ -1654,11 +1666,10 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             LL.d = ( char * ) dalloc( c, buf.size() );
             c.desc_spill.push_back( LL.d );
             LL.nch = int( LC.size() );
-            CK( cudaMemcpyAsync( LL.d, buf.data(), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
+            CK( cudaMemcpyAsync( LL.d, stage( c, buf.data(), buf.size() ), buf.size(), cudaMemcpyHostToDevice, c.stream ) );
             c.timer.begin( c.stream, K_CELLS2D, 0.0 );
             limits_launch();
             c.timer.end( c.stream );
-            CK( cudaStreamSynchronize( c.stream ) );       // `buf` leaves scope
         }
     }
     // B. CG iterations
@@ -1700,6 +1711,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
     CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaMemcpyAsync( c.hovf, &c.dovf->count, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
     CK( cudaStreamSynchronize( c.stream ) );
+    c.hstage_used = 0;                   // every upload of the ring has completed
     clear_capacity_error( c );
     check_errors( c, "cells" );
     if ( *c.hovf > 0 ) {

@@ -45,9 +45,12 @@ struct Ctx {
     char *giant_scratch = nullptr;
     int giant_slots = 32;
     int giant_cap = 1 << 14;
-    // descriptor upload area
+    // descriptor upload area, and the pinned staging ring its uploads go through (refilled from the start after each
+    // tick's read-back, when every earlier copy has completed)
     char *desc = nullptr;
     size_t desc_bytes = 0;
+    char *hstage = nullptr;
+    size_t hstage_bytes = 0, hstage_used = 0;
     std::vector<void *> desc_spill;   // descriptor blocks past the area, freed at the end of the tick
     // CUDA graphs of the CG bursts, keyed by the layout of the batch they were captured for
     struct BurstGraph {
