@@ -43,7 +43,7 @@ struct Cell3T {
 };
 using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in shared memory
 using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 84 KB
-using Cell3G = Cell3T<8192, 2048, unsigned short>;       // the giant-cell pass: one warp a block, about 660 KB in global memory
+using Cell3G = Cell3T<32768, 8192, unsigned short>;      // the giant-cell pass (the reference's card_max_vertices, PowerDiagram_Bsp.py:122): one warp a block, about 2.6 MB in global memory
 
 template<class C3>
 __device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double &x, double &y, double &z ) {

@@ -43,7 +43,7 @@ struct Ctx {
     OvfList *dgiant = nullptr;
     int *hgiant = nullptr;
     char *giant_scratch = nullptr;
-    int giant_slots = 32;
+    int giant_slots = 16;
     int giant_cap = 1 << 14;
     // descriptor upload area, and the pinned staging ring its uploads go through (refilled from the start after each
     // tick's read-back, when every earlier copy has completed)

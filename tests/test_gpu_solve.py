@@ -243,10 +243,18 @@ def test_the_card_aggregates_as_the_cpu(d):
     """tests/test_SdotPlanNd.py:1510-1535, 1785-1805: seeds the doubles cannot separate are merged, and the oracle's
     diagram at the GPU's weights gives each cluster its mass and every other cell its own"""
     from helpers import degenerate_clouds
+    plans = {}
     for name, (pos, groups) in degenerate_clouds(d, 17).items():
         n = len(pos)
         tol = (1e-9 if "1e-12" in name else 1e-11) / n
-        plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=tol, max_iter=60))
+        plans[name] = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=tol, max_iter=60, on_failure="ignore"))
+    failed = {name: (p.stats["status"], p.stats["nb_iter"], p.stats["residual"], [h["max_abs_residual"] for h in p.history][-6:])
+              for name, p in plans.items() if not p.converged}
+    assert not failed, failed
+    for name, (pos, groups) in degenerate_clouds(d, 17).items():
+        n = len(pos)
+        tol = (1e-9 if "1e-12" in name else 1e-11) / n
+        plan = plans[name]
         _check_aggregated(f"{d}D {name}", plan, pos, groups, tol)
         g = O.cells(pos, np.asarray(plan.weights).reshape(-1))["mass"]
         nu = np.asarray(plan.target_masses).reshape(-1)
