@@ -145,14 +145,13 @@ __device__ __forceinline__ double erf_diff( double a, double b ) {
     return erf( b ) - erf( a );
 }
 
-__device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments,
-                                         bool measures, EdgeInt &e ) {
-    e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+// gaussian g's part of the edge (x0,y0)->(x1,y1), ADDED to e
+__device__ __noinline__ void edge_gauss_one( const ProbDev &P, int g, double px, double py, double x0, double y0, double x1, double y1,
+                                             bool moments, bool measures, EdgeInt &e ) {
     double dx = x1 - x0, dy = y1 - y0, len = sqrt( dx * dx + dy * dy );
     if ( len == 0 ) return;
-    const int ng = P.dn[ 0 ];
     const double r2 = 1.4142135623730951;
-    for ( int g = 0; g < ng; ++g ) {
+    {
         const double *G = P.dval + g * 4;
         double cx = G[ 0 ] - px, cy = G[ 1 ] - py, sg = G[ 2 ], mg = G[ 3 ];
         double K = mg / ( 2 * M_PI * sg * sg ), s2g = sg * sg, sq = sg * r2;
@@ -172,7 +171,7 @@ __device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py,
             e.mx += ( x0 - ux * sa ) * mm + ux * ms;
             e.my += ( y0 - uy * sa ) * mm + uy * ms;
         }
-        if ( dy == 0 ) continue;                           // no part in the closed integral of F dy
+        if ( dy == 0 ) return;                             // no part in the closed integral of F dy
         double u0 = ( 0 - cx ) / sq;                       // reference abscissa: the seed
         double e0 = exp( -( cx * cx ) / ( 2 * s2g ) );
         double c0 = erfc( fabs( u0 ) ), f0 = erf( fabs( u0 ) );
@@ -206,6 +205,44 @@ __device__ __noinline__ void edge_gauss( const ProbDev &P, double px, double py,
             }
             e.m += Dy * am;
             if ( moments ) { e.fx += Dy * afx; e.fy += Dy * afy; e.s2 += Dy * as2; }
+        }
+    }
+}
+
+// every gaussian's part of the edge, in gaussian order
+__device__ void edge_gauss( const ProbDev &P, double px, double py, double x0, double y0, double x1, double y1, bool moments, bool measures,
+                            EdgeInt &e ) {
+    e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+    for ( int g = 0; g < P.dn[ 0 ]; ++g ) edge_gauss_one( P, g, px, py, x0, y0, x1, y1, moments, measures, e );
+}
+
+// a warp's polygon (m edges, vertex `lane` in (vx, vy)) under a sum of gaussians: the (edge, gaussian) pairs spread over the
+// lanes -- lane t takes the pairs t, t + 32, ..., edge t % m and gaussian t / m -- so that a cell of 6 edges keeps 24
+// lanes busy, not 6.  `e` of each lane: its pairs' part of the cell integrals (summed over the warp by the caller), and
+// for lane < m the facet measure and moments of edge `lane`, its gaussians summed in order (as edge_gauss does)
+__device__ void warp_edges_gauss( const ProbDev &P, int m, int lane, double vx, double vy, double px, double py, bool moments, bool measures,
+                                  EdgeInt &e ) {
+    e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
+    const int ng = P.dn[ 0 ], pairs = m * ng;
+    for ( int r = 0; r * 32 < pairs; ++r ) {
+        const int t = lane + 32 * r;
+        const int ed = t < pairs ? t % m : 0, g = t < pairs ? t / m : 0;
+        const int nx = ed + 1 >= m ? 0 : ed + 1;
+        const double x0 = __shfl_sync( FULL, vx, ed ), y0 = __shfl_sync( FULL, vy, ed );
+        const double x1 = __shfl_sync( FULL, vx, nx ), y1 = __shfl_sync( FULL, vy, nx );
+        EdgeInt ep;
+        ep.m = ep.fx = ep.fy = ep.s2 = ep.meas = ep.mx = ep.my = 0;
+        if ( t < pairs ) edge_gauss_one( P, g, px, py, x0, y0, x1, y1, moments, measures, ep );
+        e.m += ep.m;
+        e.fx += ep.fx; e.fy += ep.fy; e.s2 += ep.s2;
+        if ( ! measures ) continue;
+        for ( int q = 0; q < ng; ++q ) {
+            const int src = lane + m * q - 32 * r;         // the pair ( edge lane, gaussian q ) in this round
+            const bool own = lane < m && src >= 0 && src < 32;
+            const double a = __shfl_sync( FULL, ep.meas, own ? src : 0 );
+            const double b = __shfl_sync( FULL, ep.mx, own ? src : 0 );
+            const double c = __shfl_sync( FULL, ep.my, own ? src : 0 );
+            if ( own ) { e.meas += a; e.mx += b; e.my += c; }
         }
     }
 }
@@ -557,12 +594,13 @@ __global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict
             double x1 = __shfl_sync( FULL, C.vx, nxt ), y1 = __shfl_sync( FULL, C.vy, nxt );
             EdgeInt e;
             e.m = e.fx = e.fy = e.s2 = e.meas = e.mx = e.my = 0;
-            if ( act ) {
+            if ( P.dkind == D_GAUSS ) warp_edges_gauss( P, m, lane, C.vx, C.vy, px, py, moments, facets || ( flags & F_VJP ), e );
+            else if ( act ) {
                 if ( P.dkind == D_UNIFORM ) edge_uniform( C.vx, C.vy, x1, y1, P.rho, moments, e );
-                else if ( P.dkind == D_IMAGE ) {
+                else {
                     int iref = int( floor( ( 0 - ( P.dorg[ 0 ] - px ) ) / P.dstep[ 0 ] ) );
                     edge_image( P, px, py, iref, C.vx, C.vy, x1, y1, moments, e );
-                } else edge_gauss( P, px, py, C.vx, C.vy, x1, y1, moments, facets || ( flags & F_VJP ), e );
+                }
             }
             double mass = warp_sum( e.m );
             if ( mass < 0 && mass > -1e-300 ) mass = 0;
