@@ -460,6 +460,25 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
     for ( int p = lane; p < np; p += 32 ) C.fmp[ p ] = 0;
     __syncwarp();
     if ( nv == 0 ) return;
+    // each face's boundary entries (vertex k, edge q with e[ q ] the face), as a list in vertex order, built once for all
+    // the gaussians: the head vertex in `remap`, the next vertex after (k, q) in `nt[ k ][ q ]` (both free once the cell
+    // is clipped)
+    for ( int p = lane; p < np; p += 32 ) {
+        int prev = -1, pq = 0;
+        for ( int k = 0; k < nv; ++k ) {
+            const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+            for ( int q = 0; q < 3; ++q ) {
+                if ( e[ q ] != p || C.tw[ 3 * k + q ] == C3::NONE ) continue;
+                if ( prev < 0 ) C.remap[ p ] = ( typename C3::I ) k;
+                else C.nt[ prev ][ pq ] = ( typename C3::I ) k;
+                prev = k;
+                pq = q;
+            }
+        }
+        if ( prev < 0 ) C.remap[ p ] = ( typename C3::I ) C3::NONE;
+        else C.nt[ prev ][ pq ] = ( typename C3::I ) C3::NONE;
+    }
+    __syncwarp();
     const double INV4PI = 0.07957747154594767, TWO_PI = 6.283185307179586;
     const int ng = P.dn[ 0 ];
     for ( int g = 0; g < ng; ++g ) {
@@ -495,13 +514,11 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
             ok = ok && h >= 0;
             const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
             double th = 0;
-            for ( int k = 0; k < nv; ++k ) {
-                const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
-                for ( int q = 0; q < 3; ++q ) {
-                    const int t = C.tw[ 3 * k + q ];
-                    if ( e[ q ] != p || t == C3::NONE ) continue;
-                    th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
-                }
+            for ( int k = C.remap[ p ]; k != C3::NONE; ) {
+                const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
+                const int t = C.tw[ 3 * k + q ];
+                th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
+                k = C.nt[ k ][ q ];
             }
             const double kk = rint( th / TWO_PI );
             const double Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
