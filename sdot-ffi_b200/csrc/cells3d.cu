@@ -481,7 +481,24 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
     __syncwarp();
     const double INV4PI = 0.07957747154594767, TWO_PI = 6.283185307179586;
     const int ng = P.dn[ 0 ];
+    // a gaussian whose centre lies beyond a face of the cell, at distance D from its plane, puts at most
+    // B = m erfc( D / sigma sqrt 2 ) / 2 in the cell (its mass in that half-space): one whose B is under 1e-20 of the
+    // largest B of the cell's gaussians is left out (its part is below the doubles of the cell's mass and measures)
+    auto bound = [&]( int g ) {
+        const double *G = P.dval + g * 5;
+        const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz;
+        double D = 0;
+        for ( int p = lane; p < np; p += 32 ) {
+            const double nn = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
+            D = fmax( D, ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz - C.no[ p ] ) / nn );
+        }
+        for ( int o = 16; o > 0; o >>= 1 ) D = fmax( D, __shfl_xor_sync( FULL3, D, o ) );
+        return 0.5 * G[ 4 ] * erfc( D * 0.7071067811865476 / G[ 3 ] );
+    };
+    double bmax = 0;
+    for ( int g = 0; g < ng; ++g ) bmax = fmax( bmax, bound( g ) );
     for ( int g = 0; g < ng; ++g ) {
+        if ( ng > 1 && bound( g ) < 1e-20 * bmax ) continue;          // (warp uniform: the bound is a warp max)
         const double *G = P.dval + g * 5;
         const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
         const double s2g = sg * sg, K = mg / ( 15.749609945722419 * s2g * sg ), kr = 0.7071067811865476 / sg;   // (2 pi)^{3/2}
