@@ -420,7 +420,7 @@ void free_geometry( Ctx &c, Geometry &G ) {
 }
 
 // ---- the solve ---------------------------------------------------------------------------------------------------------
-enum JState { J_START0, J_START_VOR, J_START_SIM, J_STAGE_DIAG, J_REPORT, J_ITER, J_CG, J_TRIAL, J_FINAL, J_DONE };
+enum JState { J_START0, J_START_VOR, J_START_SIM, J_STAGE_DIAG, J_REPORT, J_ITER, J_CG, J_TRIAL, J_POLISH, J_FINAL, J_DONE };
 enum Pend : unsigned { P_NEWTON = 1, P_GAUGE = 2, P_TRIAL = 4, P_RESCALE = 8, P_SET_W2 = 16, P_ZERO_W2 = 32, P_DENSITY = 64 };
 enum NStatus { NS_RUNNING = 0, NS_CONVERGED = 1, NS_MAX_ITER = 2, NS_STAGNATION = 3, NS_LINEAR_FAILURE = 4, NS_CAPACITY = 5, NS_FAILURE = 6,
                NS_CONVERGED_AGG = 7 };
@@ -503,6 +503,8 @@ struct SolveJob {
     double *ae = nullptr;
     int ncl = 0;
     bool full_set = false;              // stats[ residual_full ] computed on the full problem
+    int polish_round = 0;               // the re-splitting after an aggregated convergence: rounds done,
+    double polish_before = 0;           // ... and the members' residual before the current one
 };
 
 static size_t mg_bytes( int dim, long n, int cap );
@@ -750,6 +752,7 @@ static bool needs_diagram( SolveJob &J, DiagReq &R ) {
     case J_START_VOR:
     case J_START_SIM:
     case J_TRIAL:
+    case J_POLISH:
         R.w = J.w2; R.wslot = J.wslot + ( 1 - J.wcur ); R.mass = J.a2; R.table = 1 - J.cur; R.report = 1 - J.repA; return true;
     case J_REPORT:
         R.mass = J.a; R.report = J.repA; R.report_only = true; return true;
@@ -835,6 +838,8 @@ static double order_dbl_host( unsigned long long u ) {
 
 static void end_stage( Ctx &c, SolveJob &J );
 static void full_residual( Ctx &c, SolveJob &J, double &worst, double &worst_rel );
+static void final_status( Ctx &c, SolveJob &J );
+static bool polish_start( Ctx &c, SolveJob &J );
 
 static void begin_iterations( Ctx &c, SolveJob &J ) {
     // the domain mass of this density and the targets rescaled to it (sdotplan/Solve.h:250-257)
@@ -898,9 +903,14 @@ static void end_stage( Ctx &c, SolveJob &J ) {
         J.stage = int( J.scales.size() ) - 1;
         set_stage_density( c, J );
     }
+    if ( J.nstatus == NS_CONVERGED && J.ncl > 0 && polish_start( c, J ) ) return;
+    final_status( c, J );
+}
+
+// the status of a finished solve: the tests read the clusters' masses, so the full problem's residual is reported, and
+// "converged (aggregated)" when only the aggregated problem passes (sdotplan/Solve.h:300-306)
+static void final_status( Ctx &c, SolveJob &J ) {
     if ( J.nstatus == NS_CONVERGED && J.ncl > 0 ) {
-        // the tests read the clusters' masses: the full problem's residual, and "converged (aggregated)" when only the
-        // aggregated problem passes (sdotplan/Solve.h:300-306)
         double wf, wfr;
         full_residual( c, J, wf, wfr );
         J.stats[ ST_RESIDUAL_FULL ] = wf;
@@ -909,6 +919,98 @@ static void end_stage( Ctx &c, SolveJob &J ) {
     }
     J.stats[ ST_STATUS ] = J.nstatus;
     J.state = J_FINAL;
+}
+
+// THE RE-SPLITTING (sdotplan/Newton.h:434-471, Aggregation.h:250-276): once the aggregated problem has converged, each
+// cluster's members alone take a Newton step on their k x k block of the Laplacian (the rest of the diagram fixed,
+// the gauge kept by a shift of everyone), one diagram for all the clusters; kept while the members' residual
+// decreases and the aggregated problem stays converged, 4 rounds at most. False when there is nothing to do.
+static bool polish_start( Ctx &c, SolveJob &J ) {
+    if ( J.polish_round >= 4 ) return false;
+    const long n = J.G.n;
+    std::vector<double> a( n ), nu( n );
+    CK( cudaMemcpyAsync( a.data(), J.a, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaMemcpyAsync( nu.data(), J.nu, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+    CK( cudaStreamSynchronize( c.stream ) );
+    double wf = 0, wfr = 0, before = 0;
+    for ( long i = 0; i < n; ++i ) { const double e = std::fabs( a[ i ] - nu[ i ] ); wf = std::max( wf, e ); wfr = std::max( wfr, e / nu[ i ] ); }
+    if ( wf <= J.opt[ SDOT_OPT_TOL_ABS ] || ( J.opt[ SDOT_OPT_TOL_REL ] > 0 && wfr <= J.opt[ SDOT_OPT_TOL_REL ] ) ) return false;
+    for ( int m : J.cl_members ) before = std::max( before, std::fabs( a[ m ] - nu[ m ] ) );
+    const int cap = J.cap;
+    std::vector<int> idx;
+    std::vector<double> val;
+    std::vector<int> rid( cap );
+    std::vector<double> rc( cap );
+    for ( int k = 0; k < J.ncl; ++k ) {
+        const int b = J.cl_begin[ k ], e = J.cl_begin[ k + 1 ], m = e - b;
+        if ( m < 2 || m > 64 ) continue;
+        const int *mem = J.cl_members.data() + b;                  // increasing ranks
+        std::vector<double> M( size_t( m ) * m, 0.0 ), r( m );
+        bool ok = true;
+        for ( int u = 0; u < m && ok; ++u ) {
+            const int i = mem[ u ];
+            int nbi = 0;
+            CK( cudaMemcpy( &nbi, J.nb[ J.cur ] + i, sizeof( int ), cudaMemcpyDeviceToHost ) );
+            if ( nbi > cap ) { ok = false; break; }                 // (a row in the overflow store: this cluster stays)
+            if ( nbi > 0 ) {
+                CK( cudaMemcpy( rid.data(), J.nid[ J.cur ] + size_t( i ) * cap, nbi * sizeof( int ), cudaMemcpyDeviceToHost ) );
+                CK( cudaMemcpy( rc.data(), J.nc[ J.cur ] + size_t( i ) * cap, nbi * sizeof( double ), cudaMemcpyDeviceToHost ) );
+            }
+            double dia = 0;
+            for ( int q = 0; q < nbi; ++q ) {
+                dia += rc[ q ];
+                const int *at = std::lower_bound( mem, mem + m, rid[ q ] );
+                if ( at != mem + m && *at == rid[ q ] ) M[ size_t( u ) * m + ( at - mem ) ] -= rc[ q ];
+            }
+            M[ size_t( u ) * m + u ] += dia;
+            r[ u ] = nu[ i ] - a[ i ];
+        }
+        if ( ! ok ) continue;
+        // Cholesky (M symmetric positive definite unless the cluster has no neighbour)
+        for ( int p = 0; p < m && ok; ++p ) {
+            double d = M[ size_t( p ) * m + p ];
+            for ( int q = 0; q < p; ++q ) d -= M[ size_t( p ) * m + q ] * M[ size_t( p ) * m + q ];
+            if ( ! ( d > 0 ) ) { ok = false; break; }
+            d = std::sqrt( d );
+            M[ size_t( p ) * m + p ] = d;
+            for ( int u = p + 1; u < m; ++u ) {
+                double t = M[ size_t( u ) * m + p ];
+                for ( int q = 0; q < p; ++q ) t -= M[ size_t( u ) * m + q ] * M[ size_t( p ) * m + q ];
+                M[ size_t( u ) * m + p ] = t / d;
+            }
+        }
+        if ( ! ok ) continue;
+        for ( int u = 0; u < m; ++u ) {
+            double t = r[ u ];
+            for ( int q = 0; q < u; ++q ) t -= M[ size_t( u ) * m + q ] * r[ q ];
+            r[ u ] = t / M[ size_t( u ) * m + u ];
+        }
+        for ( int u = m - 1; u >= 0; --u ) {
+            double t = r[ u ];
+            for ( int q = u + 1; q < m; ++q ) t -= M[ size_t( q ) * m + u ] * r[ q ];
+            r[ u ] = t / M[ size_t( u ) * m + u ];
+        }
+        for ( int u = 0; u < m; ++u ) { idx.push_back( mem[ u ] ); val.push_back( r[ u ] ); }
+    }
+    if ( idx.empty() ) return false;
+    double d0 = 0;
+    for ( size_t t = 0; t < idx.size(); ++t ) if ( idx[ t ] == J.rank0 ) d0 = val[ t ];
+    const size_t k = idx.size();
+    char *d = ( char * ) dalloc( c, k * 12 + 256 );
+    c.desc_spill.push_back( d );
+    double *dv = reinterpret_cast<double *>( d );
+    int *di = reinterpret_cast<int *>( d + ( ( k * 8 + 255 ) & ~size_t( 255 ) ) );
+    CK( cudaMemcpyAsync( dv, val.data(), k * 8, cudaMemcpyHostToDevice, c.stream ) );
+    CK( cudaMemcpyAsync( di, idx.data(), k * 4, cudaMemcpyHostToDevice, c.stream ) );
+    Launch L = c.L();
+    launch_polish_weights( L, J.w, J.w2, int( n ), d0, di, dv, int( k ) );
+    unsigned long long *slot = J.wslot + ( 1 - J.wcur );
+    CK( cudaMemsetAsync( slot, 0, 8, c.stream ) );
+    launch_wmax( L, J.w2, int( n ), slot );
+    CK( cudaStreamSynchronize( c.stream ) );       // `val`, `idx` leave scope
+    J.polish_before = before;
+    J.state = J_POLISH;
+    return true;
 }
 
 static void after_start( Ctx &c, SolveJob &J ) {
@@ -1152,6 +1254,27 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
                     J.state = J_TRIAL;
                 }
             }
+            break;
+        }
+        case J_POLISH: {
+            J.stats[ ST_NB_DIAG ] += 1;
+            J.stats[ ST_NB_POLISH ] += 1;
+            B = rep_host( c, J, 1 - J.repA );
+            const long n = J.G.n;
+            std::vector<double> a2( n ), nu( n );
+            CK( cudaMemcpyAsync( a2.data(), J.a2, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+            CK( cudaMemcpyAsync( nu.data(), J.nu, n * 8, cudaMemcpyDeviceToHost, c.stream ) );
+            CK( cudaStreamSynchronize( c.stream ) );
+            double after = 0;
+            for ( int m : J.cl_members ) after = std::max( after, std::fabs( a2[ m ] - nu[ m ] ) );
+            const bool agg_ok = B[ R_WORST ] <= J.opt[ SDOT_OPT_TOL_ABS ] || ( J.opt[ SDOT_OPT_TOL_REL ] > 0 && B[ R_WORST_REL ] <= J.opt[ SDOT_OPT_TOL_REL ] );
+            if ( after < J.polish_before && B[ R_AMIN ] > 0 && agg_ok ) {
+                accept_trial( J );
+                J.stats[ ST_RESIDUAL ] = B[ R_WORST ];
+                ++J.polish_round;
+                if ( polish_start( c, J ) ) break;
+            }
+            final_status( c, J );
             break;
         }
         case J_FINAL:

@@ -361,6 +361,8 @@ void launch_rhs( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the re-splitting's trial weights: w2 = w - shift, then w2[ idx[ t ] ] += val[ t ] (idx distinct)
+void launch_polish_weights( const Launch &L, const double *w, double *w2, int n, double shift, const int *idx, const double *val, int k );
 // the pairs the aggregation merges (VecDev.agg_*)
 void launch_agg_detect( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 // the cluster shares of the masses: ae[ i ] = nu[ i ] a_C / nu_C for the members i of each cluster C (others untouched)

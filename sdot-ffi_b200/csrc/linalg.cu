@@ -520,6 +520,21 @@ void launch_gather_vec( const Launch &L, const double *user_vals, const int *use
     ++*L.launches;
 }
 
+// ---- the re-splitting's weights: w2 = w - shift, then the members' steps added ------------------------------------------
+__global__ void k_polish_shift( const double *__restrict__ w, double *__restrict__ w2, int n, double shift ) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( i < n ) w2[ i ] = w[ i ] - shift;
+}
+__global__ void k_polish_add( double *__restrict__ w2, const int *__restrict__ idx, const double *__restrict__ val, int k ) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( t < k ) w2[ idx[ t ] ] += val[ t ];
+}
+void launch_polish_weights( const Launch &L, const double *w, double *w2, int n, double shift, const int *idx, const double *val, int k ) {
+    k_polish_shift<<<( n + 255 ) / 256, 256, 0, L.stream>>>( w, w2, n, shift );
+    k_polish_add<<<( k + 255 ) / 256, 256, 0, L.stream>>>( w2, idx, val, k );
+    *L.launches += 2;
+}
+
 // ---- the aggregation of near-coincident seeds (sdotplan/Aggregation.h:1-44, 229-250) ---------------------------------
 // A facet's plane moves by ( w_i - w_j ) / ( 2 |p_i - p_j| ): the doubles of the weights place it no better than
 // m_ij = c_ij ulp( max( |w_i|, |w_j| ) ) of mass.  The pair is merged when m_ij margin > tau_ij,

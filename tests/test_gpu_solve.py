@@ -256,6 +256,10 @@ def test_the_card_aggregates_as_the_cpu(d):
         tol = (1e-9 if "1e-12" in name else 1e-11) / n
         plan = plans[name]
         _check_aggregated(f"{d}D {name}", plan, pos, groups, tol)
+        if plan.stats["status"] == "converged (aggregated)":
+            # the re-splitting ran (sdotplan/Newton.h:434-471): its diagrams are counted, and the full residual it left is
+            # the one reported
+            assert plan.stats["nb_polish"] >= 1 and plan.stats["residual_full"] > tol, (name, plan.stats["nb_polish"])
         g = O.cells(pos, np.asarray(plan.weights).reshape(-1))["mass"]
         nu = np.asarray(plan.target_masses).reshape(-1)
         alone = np.ones(n, dtype=bool)
