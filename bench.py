@@ -285,23 +285,22 @@ def cpu_sample(reqs, seed, budget_s=20.0):
     import oracle as O
     threads = O.max_threads()
     t0 = time.perf_counter()
-    count, n_tot = 0, 0
+    count, solved, n_tot = 0, 0, 0
     for r in reqs:
         t = target_of(r).normalized_version(nb_dims=r["d"])
         dens = t._sdot_density()
         od = ("uniform", dens[1]) if dens[0] == "uniform" else ("gauss", dens[1], dens[2], dens[3])
         lo, hi = t.box() if hasattr(t, "box") else (np.zeros(r["d"]), np.ones(r["d"]))
-        s = O.solve(positions(seed, r), box=(lo, hi), density=od, tol_abs=0.0, tol_rel=RTOL, lin_tol=1e-8)
-        if s["stats"]["status"] != 1:
-            raise RuntimeError("the oracle did not converge")
+        s = O.solve(positions(seed, r), box=(lo, hi), density=od, tol_abs=0.0, tol_rel=RTOL, lin_tol=1e-8, agg_margin=4.0)
         count += 1
+        solved += s["stats"]["status"] in CONVERGED          # (only the solves that met the tolerance count)
         n_tot += r["n"]
         if time.perf_counter() - t0 > budget_s:
             break
     secs = time.perf_counter() - t0
-    return dict(value=count / secs, unit="solves/s", cores=threads, kind="port",
-                sample=f"the first {count} requests of the same seeded stream (sum N = {n_tot}), oracle/sdot_oracle.c FP64 + OpenMP, "
-                       f"same tolerance; CPU restatement of sdot's algorithm, not the reference binary")
+    return dict(value=solved / secs, unit="solves/s", cores=threads, kind="port",
+                sample=f"the first {count} requests of the same seeded stream (sum N = {n_tot}, {solved} met the tolerance), "
+                       f"oracle/sdot_oracle.c FP64 + OpenMP, same tolerance; CPU restatement of sdot's algorithm, not the reference binary")
 
 
 def peaks():

@@ -911,7 +911,11 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
         if ( rd >= 0 && m > 0 && ! overflow ) walk_pyramid2( P, lane, px, py, wi, cx, cy, rd, stk, cut_lanes, radius2, claims );
         const int user = P.user[ s ];
         if ( overflow ) {
-            if ( lane == 0 ) record_error( P, err, 4, item.prob, user, VBIG );
+            // past the global-memory polygon: an error of its problem -- or, in a trial diagram, a refused step
+            if ( lane == 0 ) {
+                if ( P.prefuse ) *P.prefuse = 1.0;
+                else record_error( P, err, 4, item.prob, user, VBIG );
+            }
             continue;
         }
         // integration, edges strided over the lanes

@@ -632,7 +632,13 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
     if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, stk, overflow );
     const int user = P.user[ s ];
     if ( overflow ) {
-        // past the capacity of this warp's cell: the big-cell pass rebuilds it (the main kernel only)
+        // past the capacity of this warp's cell: the next pass rebuilds it -- but a trial diagram does not go past the big
+        // pass: a cell of more than its 1024 vertices there refuses the step (the damping halves it)
+        if ( big && P.prefuse ) {
+            if ( lane == 0 ) *P.prefuse = 1.0;
+            __syncwarp();
+            return false;
+        }
         if ( ovf ) { queue3( P, err, ovf, prob, s, user, lane ); return false; }
         if ( lane == 0 ) record_error3( P, err, 4, prob, user, C3::VC );
         if ( lane == 0 ) C.nv = 0;

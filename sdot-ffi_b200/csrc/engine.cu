@@ -1187,6 +1187,9 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
             ++J.nb_evals;
             ++J.trial;
             B = rep_host( c, J, 1 - J.repA );
+            // a cell past the big-cell pass in the trial: the step is refused (the damping halves it)
+            const bool giant = c.hscal[ size_t( J.slot ) * SLOT_DOUBLES + SLOT_REFUSE ] != 0;
+            if ( giant && J.lim_probe ) { J.lim_probe = false; J.trial = 1; }
             if ( J.lim_probe ) {
                 // THE LIMITS (sdotplan/Newton.h:336-366): cells below the floor at this probe bring the step under their
                 // limits; none: this diagram is the damping's first trial
@@ -1218,7 +1221,7 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
                 J.trial = 1;
             }
             double m2 = B[ R_AMIN ], n2r = merit_of( B, J.res_cur );
-            bool ok = m2 >= J.eps && std::isfinite( n2r );
+            bool ok = ! giant && m2 >= J.eps && std::isfinite( n2r );
             if ( ok && n2r <= ( 1 - J.t / 2 ) * J.nr && n2r < J.nr ) {
                 accept_trial( J );
                 J.t_last = J.t;
@@ -1268,7 +1271,8 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
             double after = 0;
             for ( int m : J.cl_members ) after = std::max( after, std::fabs( a2[ m ] - nu[ m ] ) );
             const bool agg_ok = B[ R_WORST ] <= J.opt[ SDOT_OPT_TOL_ABS ] || ( J.opt[ SDOT_OPT_TOL_REL ] > 0 && B[ R_WORST_REL ] <= J.opt[ SDOT_OPT_TOL_REL ] );
-            if ( after < J.polish_before && B[ R_AMIN ] > 0 && agg_ok ) {
+            const bool giant = c.hscal[ size_t( J.slot ) * SLOT_DOUBLES + SLOT_REFUSE ] != 0;
+            if ( ! giant && after < J.polish_before && B[ R_AMIN ] > 0 && agg_ok ) {
                 accept_trial( J );
                 J.stats[ ST_RESIDUAL ] = B[ R_WORST ];
                 ++J.polish_round;
@@ -1674,6 +1678,10 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         P.res = J->res_cur;
         P.power = J->opt[ SDOT_OPT_POWER ];
         P.perr = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR;
+        if ( J->state == J_TRIAL || J->state == J_POLISH ) {
+            P.prefuse = c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_REFUSE;
+            CK( cudaMemsetAsync( P.prefuse, 0, 8, c.stream ) );
+        }
         if ( R.report >= 0 ) {
             P.report = rep_dev( c, *J, R.report );
             P.partials = J->part_cells;

@@ -65,7 +65,8 @@ struct Ctx {
 constexpr int SLOT_ERR = 2 * NB_REPORT + NB_SC;                 // a problem's capacity-failure flag
 constexpr int SLOT_AGG = SLOT_ERR + 1;                           // the near-coincident pairs its last Laplacian showed
 constexpr int SLOT_LIM = SLOT_AGG + 1;                           // the limits step: cells below the floor, smallest limit
-constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 4;
+constexpr int SLOT_REFUSE = SLOT_LIM + 2;                        // a trial diagram with a cell past the big-cell pass
+constexpr int SLOT_DOUBLES = 2 * NB_REPORT + NB_SC + 5;
 
 void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
 void ctx_release( Ctx &c );

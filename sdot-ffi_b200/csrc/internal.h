@@ -90,6 +90,7 @@ struct ProbDev {
     double *wpyr;
     double *wmom;                 // [ nodes, wmom_size( dim ) ] the moments the slopes are fitted from
     double *perr;                 // set to 1 when a cell of this problem exceeds every capacity (NULL: none)
+    double *prefuse;              // a trial diagram: set to 1 instead when a cell exceeds the big-cell pass (NULL: not a trial)
     int nlev;
     int poff[ MAX_LEV ];
 };
