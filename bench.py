@@ -312,11 +312,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_of(kernel):
+def traffic_of(kernel, cells_per_launch):
+    """DRAM bytes per launch of `kernel`: the per-cell traffic of the committed ncu capture (a smaller case, see
+    profiles/), scaled to this run's cells per launch"""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f).get(kernel)
-    except (OSError, ValueError):
+            rec = json.load(f).get(kernel)
+        return None if rec is None else rec["bytes_per_cell"] * cells_per_launch
+    except (OSError, ValueError, KeyError, TypeError):
         return None
 
 
@@ -486,7 +489,7 @@ def main():
         "unconverged": {"count": nfail, "requests_status": failed[:16]},
         "aggregated": {"count": len(AGGREGATED), "requests_full_rel_err": AGGREGATED[:16]},
         "roofline": {"bound": "hbm", "kernel": "cells2d (k_cells2d)", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm if achieved else None, "traffic": traffic_of("k_cells2d"), "peak_kind": peak_kind,
+                     "frac": achieved / hbm if achieved else None, "traffic": traffic_of("k_cells2d", units / max(nl, 1)), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_cell": BYTES_PER_CELL[2], "cells_per_launch": units / max(nl, 1),
                      "avg_launch_ms": ms / max(nl, 1), "cg_ms_share": cg_ms / max(1e-9, 1000 * secs),
                      "cells_ms_share": ms / max(1e-9, 1000 * secs),
