@@ -45,20 +45,37 @@ using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in 
 using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 84 KB
 using Cell3G = Cell3T<32768, 8192, unsigned short>;      // the giant-cell pass (the reference's card_max_vertices, PowerDiagram_Bsp.py:122): one warp a block, about 2.6 MB in global memory
 
+// the vertex of planes a, b, c (n . y = o, seed frame), found on the line of the two most transverse of them: from the
+// line's point nearest the seed, by the step the third plane's equation asks for.  The vertex then lies on all three
+// planes to rounding, however close to parallel the third plane is to one of the others (two seeds 1e-10 apart make two
+// bisectors 1e-9 rad apart; Cramer's rule left such vertices off the planes by eps / sin(angle), and the polyhedron
+// lost up to 1e-4 of its volume)
 template<class C3>
 __device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double &x, double &y, double &z ) {
-    // x = ( o_a ( n_b x n_c ) + o_b ( n_c x n_a ) + o_c ( n_a x n_b ) ) / ( n_a . ( n_b x n_c ) )
-    double bcx = C.ny[ b ] * C.nz[ c ] - C.nz[ b ] * C.ny[ c ], bcy = C.nz[ b ] * C.nx[ c ] - C.nx[ b ] * C.nz[ c ],
-           bcz = C.nx[ b ] * C.ny[ c ] - C.ny[ b ] * C.nx[ c ];
-    double cax = C.ny[ c ] * C.nz[ a ] - C.nz[ c ] * C.ny[ a ], cay = C.nz[ c ] * C.nx[ a ] - C.nx[ c ] * C.nz[ a ],
-           caz = C.nx[ c ] * C.ny[ a ] - C.ny[ c ] * C.nx[ a ];
-    double abx = C.ny[ a ] * C.nz[ b ] - C.nz[ a ] * C.ny[ b ], aby = C.nz[ a ] * C.nx[ b ] - C.nx[ a ] * C.nz[ b ],
-           abz = C.nx[ a ] * C.ny[ b ] - C.ny[ a ] * C.nx[ b ];
-    double det = C.nx[ a ] * bcx + C.ny[ a ] * bcy + C.nz[ a ] * bcz;
-    double inv = 1.0 / det;
-    x = ( C.no[ a ] * bcx + C.no[ b ] * cax + C.no[ c ] * abx ) * inv;
-    y = ( C.no[ a ] * bcy + C.no[ b ] * cay + C.no[ c ] * aby ) * inv;
-    z = ( C.no[ a ] * bcz + C.no[ b ] * caz + C.no[ c ] * abz ) * inv;
+    auto cross2 = [&]( int p, int q ) {
+        const double cx = C.ny[ p ] * C.nz[ q ] - C.nz[ p ] * C.ny[ q ], cy = C.nz[ p ] * C.nx[ q ] - C.nx[ p ] * C.nz[ q ],
+                     cz = C.nx[ p ] * C.ny[ q ] - C.ny[ p ] * C.nx[ q ];
+        const double np = C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ];
+        const double nq = C.nx[ q ] * C.nx[ q ] + C.ny[ q ] * C.ny[ q ] + C.nz[ q ] * C.nz[ q ];
+        return ( cx * cx + cy * cy + cz * cz ) / ( np * nq );            // sin^2 of their angle
+    };
+    // the line: the pair with the largest angle; the plane: the third one
+    const double sab = cross2( a, b ), sbc = cross2( b, c ), sca = cross2( c, a );
+    int p = a, q = b, r = c;
+    if ( sbc > sab && sbc >= sca ) { p = b; q = c; r = a; }
+    else if ( sca > sab && sca > sbc ) { p = c; q = a; r = b; }
+    const double pn2 = C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ];
+    const double qn2 = C.nx[ q ] * C.nx[ q ] + C.ny[ q ] * C.ny[ q ] + C.nz[ q ] * C.nz[ q ];
+    const double pq = C.nx[ p ] * C.nx[ q ] + C.ny[ p ] * C.ny[ q ] + C.nz[ p ] * C.nz[ q ];
+    const double dx = C.ny[ p ] * C.nz[ q ] - C.nz[ p ] * C.ny[ q ], dy = C.nz[ p ] * C.nx[ q ] - C.nx[ p ] * C.nz[ q ],
+                 dz = C.nx[ p ] * C.ny[ q ] - C.ny[ p ] * C.nx[ q ];
+    const double G = pn2 * qn2 - pq * pq;                                    // |d|^2
+    const double al = ( C.no[ p ] * qn2 - C.no[ q ] * pq ) / G, be = ( C.no[ q ] * pn2 - C.no[ p ] * pq ) / G;
+    const double X0 = al * C.nx[ p ] + be * C.nx[ q ], Y0 = al * C.ny[ p ] + be * C.ny[ q ], Z0 = al * C.nz[ p ] + be * C.nz[ q ];
+    const double t = ( C.no[ r ] - ( C.nx[ r ] * X0 + C.ny[ r ] * Y0 + C.nz[ r ] * Z0 ) ) / ( C.nx[ r ] * dx + C.ny[ r ] * dy + C.nz[ r ] * dz );
+    x = X0 + t * dx;
+    y = Y0 + t * dy;
+    z = Z0 + t * dz;
 }
 
 // the vertex holding the directed edge (e0, e1), -1 if none
