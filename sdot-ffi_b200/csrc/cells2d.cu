@@ -497,7 +497,7 @@ __device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )
     __syncthreads();
 }
 
-__global__ void __launch_bounds__( 256, 2 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+__global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                     unsigned flags, ErrRec *err, OvfList *ovf ) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     __shared__ double sh_rep[ 8 ][ NB_REPORT ];

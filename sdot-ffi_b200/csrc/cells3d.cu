@@ -423,8 +423,6 @@ __device__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double 
     double qx = ax - s0 * ux, qy = ay - s0 * uy, qz = az - s0 * uz;
     double d = sqrt( qx * qx + qy * qy + qz * qz );
     if ( ! ( d > 0 ) ) return;
-    // every point of the edge is at least d from the foot: past 9 sigma both integrands are below 3e-18 of their peak
-    if ( d > 9 * sg ) return;
     double bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
     double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
     const double sgn = o >= 0 ? 1.0 : -1.0;
@@ -532,7 +530,6 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
                 const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] );
                 const double nhx = C.nx[ f ] / nn, nhy = C.ny[ f ] / nn, nhz = C.nz[ f ] / nn;
                 const double h = ( C.no[ f ] - ( C.nx[ f ] * cx + C.ny[ f ] * cy + C.nz[ f ] * cz ) ) / nn;
-                if ( fabs( h ) > 9 * sg ) continue;                // the face's plane 9 sigma from the centre: its parts are below 3e-18
                 double A, B;
                 edge_gauss3( cx + h * nhx, cy + h * nhy, cz + h * nhz, Kx, Ky, Kz, C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz, h, sg, A, B );
                 Mg += h * INV4PI * mg * A;
@@ -549,7 +546,6 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
             const double nhx = C.nx[ p ] / nn, nhy = C.ny[ p ] / nn, nhz = C.nz[ p ] / nn;
             const double h = ( C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) ) / nn;
             ok = ok && h >= 0;
-            if ( fabs( h ) > 9 * sg ) continue;                    // (as for its edges: its winding part is below 3e-18)
             const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
             double th = 0;
             for ( int k = C.remap[ p ]; k != C3::NONE; ) {

@@ -24,15 +24,45 @@ constexpr int MG_PAIRS = 1024;          // (column, value) pairs a warp gathers 
 constexpr int MG_WARPS = 4;             // warps per block of the coarsening kernels
 
 // ---- build -------------------------------------------------------------------------------------------------------------
-// level 0 from the FP64 CSR of the Newton Laplacian
+// level 0 from the FP64 CSR of the Newton Laplacian.  A coupling far above the rest of both its rows (two seeds 1e-12
+// apart: c_ij ~ 1e10 next to couplings ~ 1) would make the FP32 cycle's residuals cancel to noise (a row of
+// 1e10 x_i - 1e10 x_j loses everything to rounding) and the preconditioner would stop being positive: in the
+// PRECONDITIONER's copy it is capped at MG_CAP times the smaller of the two rows' other couplings (symmetric; the outer
+// FP64 CG keeps the exact matrix).  Ordinary diagrams never reach the cap.
+constexpr double MG_CAP = 1e3;
+
+// each row's couplings but its largest, summed (the cap's scale), into the level's x (free during the build)
+__global__ void k_mg_rest( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    const VecDev &V = vs[ M.vec ];
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
+        double sum = 0, mx = 0;
+        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) { sum += V.val[ e ]; mx = fmax( mx, V.val[ e ] ); }
+        M.x[ i ] = float( sum - mx );
+    }
+}
+
 __global__ void k_mg_level0( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
     const VecDev &V = vs[ M.vec ];
     for ( int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x ) {
-        M.dia[ i ] = float( V.dia[ i ] );
-        M.dinv[ i ] = float( 1.0 / V.dia[ i ] );
-        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) M.val[ e ] = float( V.val[ e ] );
+        const int b = V.row_ptr[ i ], e1 = V.row_ptr[ i + 1 ];
+        if ( b == e1 ) {                               // an empty row keeps the Newton Laplacian's unit diagonal
+            M.dia[ i ] = float( V.dia[ i ] );
+            M.dinv[ i ] = float( 1.0 / V.dia[ i ] );
+            continue;
+        }
+        double dia = 0;
+        for ( int e = b; e < e1; ++e ) {
+            const double rest = fmin( double( M.x[ i ] ), double( M.x[ V.col[ e ] ] ) );
+            const double c = rest > 0 ? fmin( V.val[ e ], MG_CAP * rest ) : V.val[ e ];
+            M.val[ e ] = float( c );
+            dia += c;
+        }
+        M.dia[ i ] = float( dia );
+        M.dinv[ i ] = float( 1.0 / dia );
     }
 }
 
@@ -298,6 +328,8 @@ __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv
 
 void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch ) {
     if ( nch <= 0 ) return;
+    k_mg_rest<<<nch, MGT, 0, L.stream>>>( lv, vs, ch, nch );
+    ++*L.launches;
     k_mg_level0<<<nch, MGT, 0, L.stream>>>( lv, vs, ch, nch );
     ++*L.launches;
 }
