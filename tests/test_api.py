@@ -88,3 +88,26 @@ def test_quantization_draws_its_start_in_the_support():
     assert x.shape == (300, 2) and (x >= 0).all() and (x[:, 0] <= 2).all() and (x[:, 1] <= 0.75).all()
     assert np.array_equal(x, uniform_in_support(img, 300, seed=3))
     assert x[:, 0].max() > 1.9 and x[:, 1].max() > 0.7
+
+
+def test_exact_duplicates_are_written_back_with_empty_cells():
+    """SdotPlanNd.py:124-148, sdotplan/Aggregation.h:24-31: the solve runs without the duplicates; each gets an empty cell,
+    its representative's weight minus k gaps (k its rank among the representative's duplicates), its cluster the
+    representative's; the other outputs are the solve's, in the caller's order"""
+    from sdot.SdotPlanNd import SdotPlanNd
+    pos = np.array([[0.1, 0.2], [0.5, 0.5], [0.1, 0.2], [0.9, 0.3], [0.1, 0.2]])
+    dup, rep = exact_duplicates(pos)
+    assert list(dup) == [2, 4] and list(rep) == [0, 0]
+    plan = SdotPlanNd.__new__(SdotPlanNd)
+    plan.problem = OtProblem(SumOfDiracs(pos), Box(nb_dims=2))
+    plan._dups = (dup, rep)
+    plan._keep = np.array([0, 1, 3])
+    r = dict(weights=np.array([0.0, 0.25, -0.125]), masses=np.array([0.6, 0.2, 0.2]),
+             barycentres=np.array([[0.2, 0.2], [0.5, 0.6], [0.8, 0.3]]), clusters=np.array([0, 1, 2]))
+    out = plan._expand(r)
+    w, m, b, cl = out["weights"], out["masses"], out["barycentres"], out["clusters"]
+    assert np.array_equal(m, [0.6, 0.2, 0.0, 0.2, 0.0])
+    assert np.array_equal(cl, [0, 1, 0, 3, 0])
+    assert w[0] == 0 and w[1] == 0.25 and w[3] == -0.125
+    assert w[4] < w[2] < w[0] and np.isclose(w[0] - w[2], w[2] - w[4])
+    assert np.array_equal(b[[0, 1, 3]], r["barycentres"]) and np.array_equal(b[2], pos[2]) and np.array_equal(b[4], pos[4])
