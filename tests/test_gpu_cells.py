@@ -1,6 +1,6 @@
 """Parity of the GPU cells (through the C ABI) with the oracle and with the reference's known answers.
 
-Tolerances: FP64 masses within 1e-10 relative of the oracle's (the reference pins its
+Tolerances: FP64 masses within 1e-10 relative of the oracle's (tighter than the reference, which pins its
 FP64 card at 1e-9, tests/test_CardCells.py:48-73); neighbour sets of non-degenerate facets bit-exact (a facet
 below 1e-9 of its cell's largest is degenerate: its presence is decided by rounding); c_ij within 1e-9.
 """

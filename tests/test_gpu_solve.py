@@ -1,6 +1,6 @@
 """Parity of the GPU damped Newton (sdot_solve / sdot_solve_batch through the C ABI) with the oracle's.
 
-The bar (the reference's card-vs-CPU tests tests/test_SdotPlanNd.py:612-656, 966-1072):
+The bar (the reference's card-vs-CPU tests tests/test_SdotPlanNd.py:612-656, 966-1072, tightened):
 the solve converges to `max |m - nu| / nu <= 1e-8`; an independent oracle diagram at the GPU's weights
 confirms the masses; the weights agree with the oracle's converged weights within 1e-7 of max|w|; masses,
 barycentres and cost agree; a solve in a batch is bitwise the solve alone.
