@@ -85,7 +85,8 @@ def encode_density(density, dim):
 
 
 def cells(pos, weights=None, box=None, density=None, brute=False, cap=64, want=("mass", "bary", "cost", "facets")):
-    """one diagram: dict with `mass`, `bary`, `cost`, `nb`, `nid`, `nc` (c_ij), `nm` (int_facet rho), `nvert`, `status`, `bad`"""
+    """one diagram: dict with `mass`, `bary`, `cost`, `nb`, `nid`, `nc` (c_ij), `nm` (int_facet rho), `nvert`, `status`, `bad`;
+    the outputs not in `want` are None (3D gaussians: `want=("facets",)` skips the volume quadrature)"""
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     n, d = pos.shape
     w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
@@ -94,7 +95,8 @@ def cells(pos, weights=None, box=None, density=None, brute=False, cap=64, want=(
     bx = np.ascontiguousarray(np.concatenate([np.asarray(box[0], float), np.asarray(box[1], float)]))
     kind, par, val = encode_density(density, d)
     out = {k: None for k in ("mass", "bary", "cost", "nb", "nid", "nc", "nm")}
-    out["mass"] = np.zeros(n)
+    if "mass" in want:
+        out["mass"] = np.zeros(n)
     if "bary" in want:
         out["bary"] = np.zeros((n, d))
     if "cost" in want:

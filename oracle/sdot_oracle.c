@@ -867,7 +867,8 @@ static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
     const int gauss = pb->dkind == DENS_GAUSS;
     double r = gauss ? 1.0 : pb->dpar[ 0 ];
     if ( gauss ) {
-        gauss_cell3( pb, P, p, &M, F, &S );
+        M = S = F[ 0 ] = F[ 1 ] = F[ 2 ] = 0;
+        if ( o->mass || o->bary || o->cost ) gauss_cell3( pb, P, p, &M, F, &S );   /* facets only: no volume quadrature */
         V = M;
     } else {
         poly3_integrals( P, &V, F, &S );

@@ -81,3 +81,33 @@ def degenerate_clouds(d, seed):
         "triple at 1e-10": cloud(([4, 9, 13], [1e-10 * diag, 2e-10 * axis])),
         "pair and duplicate": cloud(([1, 6], [3e-10 * diag]), ([12, 15, 30], [0 * diag, 2e-10 * axis])),
     }
+
+
+def gaussian_facet_case(d, perm=None, flip=None):
+    """the reference's closed-form facet of a sum of gaussians (tests/test_SumOfGaussians.py:20-43): two seeds at
+    x = 1/4 and 3/4 of the unit cube share the facet x = 1/2, on which each gaussian is a product of erf factors.
+    `d` 2 drops the last axis. `perm` / `flip` map the configuration by a symmetry of the cube (the facet then lies
+    across another axis, the seeds and centres move with it), so the same answer checks the frame of the face
+    integral. Returns `(positions, centres, sigmas, masses, c_01)`, the masses normalised to 1 and
+    `c_01 = int_facet rho / (2 |p_1 - p_0|)`."""
+    from math import erf, exp, pi, sqrt
+    c = np.array([[0.43, 0.58, 0.47], [0.52, 0.31, 0.66], [0.2, 0.7, 0.5]])[:, :d]
+    s = np.array([0.17, 0.05, 0.3])
+    m = np.array([0.5, 1.0, 0.7])
+    m = m / m.sum()
+    pos = np.array([[0.25, 0.5, 0.5], [0.75, 0.5, 0.5]])[:, :d]
+    seg = lambda a, sg: 0.5 * (erf((1 - a) / (sg * sqrt(2))) - erf(-a / (sg * sqrt(2))))
+    facet = sum(m[k] * exp(-(0.5 - c[k, 0]) ** 2 / (2 * s[k] ** 2)) / (s[k] * sqrt(2 * pi)) * np.prod([seg(c[k, a], s[k]) for a in range(1, d)])
+                for k in range(3))
+    perm = list(range(d)) if perm is None else list(perm)
+    pos, c = pos[:, perm].copy(), c[:, perm].copy()
+    for a in range(d):
+        if flip is not None and flip[a]:
+            pos[:, a], c[:, a] = 1 - pos[:, a], 1 - c[:, a]
+    return pos, c, s, m, facet / (2 * 0.5)
+
+
+def coefficient(nb, nid, nc, i, j):
+    """c_ij as row i holds it (0 if j is not a neighbour of i)"""
+    row = [int(x) for x in nid[i, : nb[i]]]
+    return float(nc[i, row.index(j)]) if j in row else 0.0

@@ -149,6 +149,48 @@ def test_3d_gaussian_density_matches_the_oracle(n):
     assert abs(m.sum() - inside) < 1e-12
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_a_gaussian_facet_is_the_closed_form(d):
+    """tests/test_SumOfGaussians.py:20-43 through the C ABI: the facet x = 1/2 of two seeds under a narrow, a mid and a
+    wide gaussian is a product of erf factors; 1e-12 relative (the reference's bar), from both cells, under a rotation
+    of the cube about each axis and a reflection (the box of this path is axis-aligned)"""
+    from helpers import coefficient, gaussian_facet_case
+    maps = [(None, None), ((1, 0), (0, 1))] if d == 2 else [(None, None), ((1, 2, 0), (0, 0, 1)), ((2, 0, 1), (1, 0, 0))]
+    for perm, flip in maps:
+        pos, c, s, m, ref = gaussian_facet_case(d, perm, flip)
+        nb, ids, vals = _pd(pos, dist=sdot.SumOfGaussians(c, s, m)).hessian_rows()
+        for i, j in ((0, 1), (1, 0)):
+            got = coefficient(nb, ids, vals, i, j)
+            assert abs(got - ref) < 1e-12 * ref, (perm, flip, i, got, ref)
+
+
+def test_3d_gaussian_facets_agree_from_both_sides():
+    """tests/test_SumOfGaussians.py:46-61 through the C ABI: 30 seeds under gaussians of widths 0.04, 0.2 and 0.35,
+    oblique facets each integrated by both of its cells; symmetric to 1e-12 of the largest entry, and each row's
+    coefficients those of the oracle to 1e-10 of that entry"""
+    rng = np.random.default_rng(33)
+    n = 30
+    pos = rng.uniform(0.1, 0.9, size=(n, 3))
+    w0 = rng.uniform(-0.01, 0.01, n)
+    c = rng.uniform(0.3, 0.7, size=(3, 3))
+    s = np.array([0.04, 0.2, 0.35])
+    m = np.array([0.5, 1.0, 0.7])
+    nb, ids, vals = _pd(pos, w0, dist=sdot.SumOfGaussians(c, s, m)).hessian_rows()
+    ref = O.cells(pos, w0, box=(np.zeros(3), np.ones(3)), density=("gauss", c, s, m / m.sum()), want=("facets",))
+
+    def dense(nb, ids, vals):
+        H = np.zeros((n, n))
+        for i in range(n):
+            for q in range(nb[i]):
+                H[i, ids[i, q]] -= vals[i, q]
+                H[i, i] += vals[i, q]
+        return H
+    H, R = dense(nb, ids, vals), dense(ref["nb"], ref["nid"], ref["nc"])
+    assert (H - np.diag(np.diag(H)) < 0).sum() > 2 * n
+    assert np.abs(H - H.T).max() < 1e-12 * np.abs(H).max()
+    assert np.abs(H - R).max() < 1e-10 * np.abs(R).max()
+
+
 def test_the_laplacian_is_bit_symmetric():
     rng = np.random.default_rng(4)
     n = 20000

@@ -167,6 +167,43 @@ def test_3d_gaussians_integrate_what_a_sampling_says():
 
 
 @pytest.mark.parametrize("d", [2, 3])
+def test_a_gaussian_facet_is_the_closed_form(d):
+    """tests/test_SumOfGaussians.py:20-43: the facet x = 1/2 of two seeds under three gaussians (narrow, mid, wide) is a
+    product of erf factors; 1e-12 relative, from both sides, under every symmetry of the cube (the reference rotates
+    its domain; the box of this path is axis-aligned, so the rotations are the cube's own)"""
+    import itertools
+    from helpers import coefficient, gaussian_facet_case
+    for perm in itertools.permutations(range(d)):
+        for flip in itertools.product([0, 1], repeat=d):
+            pos, c, s, m, ref = gaussian_facet_case(d, perm, flip)
+            r = O.cells(pos, density=("gauss", c, s, m), want=("facets",))
+            assert r["status"] == 0
+            for i, j in ((0, 1), (1, 0)):
+                got = coefficient(r["nb"], r["nid"], r["nc"], i, j)
+                assert abs(got - ref) < 1e-12 * ref, (perm, flip, i, got, ref)
+
+
+def test_3d_gaussian_facets_agree_from_both_sides():
+    """tests/test_SumOfGaussians.py:46-61: 30 seeds, oblique facets cut by their neighbours, each integrated from both
+    of its cells; the Laplacian is symmetric to 1e-12 of its largest entry"""
+    rng = np.random.default_rng(33)
+    n = 30
+    pos = rng.uniform(0.1, 0.9, size=(n, 3))
+    w0 = rng.uniform(-0.01, 0.01, n)
+    c = rng.uniform(0.3, 0.7, size=(3, 3))
+    m = np.array([0.5, 1.0, 0.7])
+    r = O.cells(pos, w0, density=("gauss", c, np.array([0.04, 0.2, 0.35]), m / m.sum()), want=("facets",))
+    assert r["status"] == 0
+    H = np.zeros((n, n))
+    for i in range(n):
+        for q in range(r["nb"][i]):
+            H[i, r["nid"][i, q]] -= r["nc"][i, q]
+            H[i, i] += r["nc"][i, q]
+    assert (H - np.diag(np.diag(H)) < 0).sum() > 2 * n
+    assert np.abs(H - H.T).max() < 1e-12 * np.abs(H).max()
+
+
+@pytest.mark.parametrize("d", [2, 3])
 def test_the_laplacian_is_the_jacobian_of_the_measures(d):
     """tests/test_SdotPlanNd.py:184-243: d m_i / d w_j = - c_ij, d m_i / d w_i = sum_j c_ij"""
     rng = np.random.default_rng(70 + d)
