@@ -236,6 +236,49 @@ def test_moments_match_a_sampling():
         assert abs(((sel - pos[i]) ** 2).sum(axis=1).sum() / len(pts) - r["cost"][i]) < 2e-4
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_moments_are_the_closed_forms(d):
+    """tests/test_SdotPlanNd.py:460-498: one seed owns the unit square (cube): mass 1, barycentre the centre,
+    `int |x|^2 = d / 3`; one lit pixel of an image puts the barycentre at that pixel's centre (the orientation of the
+    grid: `values[i, j]` at `origin + (i, j) * step`); 15 seeds share those moments"""
+    def second(r, pos):
+        first = r["mass"][:, None] * r["bary"]
+        return r["cost"] + 2 * (pos * first).sum(axis=1) - (pos * pos).sum(axis=1) * r["mass"]
+    one = np.array([[0.3, 0.6, 0.2][:d]])
+    r = O.cells(one)
+    assert abs(r["mass"][0] - 1) < 1e-12 and np.abs(r["bary"][0] - 0.5).max() < 1e-12
+    assert abs(second(r, one)[0] - d / 3) < 1e-12
+    pos = np.random.default_rng(11).uniform(0.1, 0.9, size=(15, d))
+    r = O.cells(pos)
+    assert np.abs((r["mass"][:, None] * r["bary"]).sum(axis=0) - 0.5).max() < 1e-12
+    assert abs(second(r, pos).sum() - d / 3) < 1e-12
+    if d == 2:
+        values = np.zeros((4, 3))
+        values[3, 1] = 1 / (0.5 * 0.25)     # normalised, as `Image.normalized_version` makes it
+        r = O.cells(one, box=(np.zeros(2), np.array([2.0, 0.75])), density=("image", [0, 0], [0.5, 0.25], values))
+        assert abs(r["mass"][0] - 1) < 1e-12
+        assert np.abs(r["bary"][0] - [3.5 * 0.5, 1.5 * 0.25]).max() < 1e-12
+
+
+def test_many_gaussians_stay_exact():
+    """tests/test_SdotPlanNd.py:1884-1902: 400 gaussians of width 0.01 along an arc, 100 seeds drawn in the unit square
+    (most outside the support box: the similarity start), `continuation = "always"`: converged to 1e-11 through more
+    than 5 widths, and a diagram at the fitted weights on the exact density gives the target masses to 1e-9"""
+    rng = np.random.default_rng(5)
+    G = 400
+    t = rng.uniform(0.2 * np.pi, 0.8 * np.pi, G)
+    r = 0.35 + 0.02 * rng.standard_normal(G)
+    c = np.c_[0.5 + r * np.cos(t), 0.2 + r * np.sin(t)]
+    s = np.full(G, 0.01)
+    lo, hi = (c - 6 * s[:, None]).min(axis=0), (c + 6 * s[:, None]).max(axis=0)
+    dens = ("gauss", c, s, np.full(G, 1 / G))
+    pos = rng.uniform(0, 1, (100, 2))
+    sol = O.solve(pos, box=(lo, hi), density=dens, tol_abs=1e-11, maxit=200, continuation=2)
+    assert sol["stats"]["status"] == 1 and sol["stats"]["nb_continuation_steps"] > 5, sol["stats"]
+    m = O.cells(pos, sol["weights"], box=(lo, hi), density=dens)["mass"]
+    assert np.abs(m - sol["stats"]["domain_mass"] / 100).max() < 1e-9
+
+
 def test_newton_reaches_the_target_masses():
     """tests/test_SdotPlanNd.py:39-62: the fitted masses are the targets"""
     rng = np.random.default_rng(1)
