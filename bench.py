@@ -323,6 +323,23 @@ def traffic_of(kernel, cells_per_launch):
         return None
 
 
+def rank_share(reqs, rank, world):
+    """the requests of one rank: every world-th of the stream from its rank on, so the ranks' shares are disjoint,
+    cover the stream, and hold the same mix of kinds and sizes"""
+    return reqs[rank::world]
+
+
+def over_ranks(secs, nfail, dist, device):
+    """the timed seconds as the max over the ranks and the unconverged solves summed over them; every rank takes both
+    collectives, in this order"""
+    import torch
+    t = torch.tensor([secs], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    f = torch.tensor([float(nfail)], dtype=torch.float64, device=device)
+    dist.all_reduce(f, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(f.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -422,7 +439,7 @@ def main():
     reqs, skipped = stream(a.seed, total, probe)
     config["skipped"] = (f"{skipped} requests of kinds this build does not solve yet left out of the stream: "
                          + ", ".join(f"{d}D {'gaussian' if g else 'uniform'}" for (d, g), ok in caps.items() if not ok)) if skipped else "none"
-    mine = reqs[rank::world]
+    mine = rank_share(reqs, rank, world)
     warm, timed = mine[: a.warmup * R], mine[a.warmup * R:]
 
     # warm-up steps (untimed)
@@ -446,16 +463,10 @@ def main():
             failed += f
     kst = _lib.kernel_stats()
     _lib.set_timing(False)
-    if world > 1:
-        tt = torch.tensor([secs], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        secs = float(tt.item())
     # only the solves that reached the mass tolerance count
     nfail = len(failed)
     if world > 1:
-        tf = torch.tensor([float(nfail)], device="cuda")
-        dist.all_reduce(tf, op=dist.ReduceOp.SUM)
-        nfail = int(tf.item())
+        secs, nfail = over_ranks(secs, nfail, dist, "cuda")
     value = ( a.steps * R * world - nfail ) / secs
 
     # plain one-at-a-time on a sample of the timed requests
@@ -477,6 +488,7 @@ def main():
     cg_ms, cg_n, cg_rows = kst["cg"]
     cpu = cpu_sample(timed, a.seed, a.cpu_budget) if rank == 0 else None
     if rank != 0:
+        dist.destroy_process_group()
         return
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
