@@ -163,6 +163,8 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         CK( cudaSetDevice( c.device ) );
         const int dim = desc->dim;
         const long n = desc->n;
+        if ( out->precision != 0 )
+            throw Error( SDOT_ERR_UNSUPPORTED, "precision 1 (FP32 clipping with an FP64 re-check) is not built: FP64 clipping only (precision 0)" );
         const bool facets = out->nb_count || out->nb_ids || out->nb_coef || out->nb_measure;
         if ( facets && ( ! out->nb_count || ! out->nb_ids || ! out->nb_coef || out->cap <= 0 ) )
             throw Error( SDOT_ERR_ARGS, "facets need nb_count, nb_ids, nb_coef and cap > 0" );

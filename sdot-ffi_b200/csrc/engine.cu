@@ -650,6 +650,8 @@ static bool convolvable( const SolveJob &J ) { return J.G.dkind == D_GAUSS || ( 
 
 SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
     const sdot_diagram_desc &D = desc.diagram;
+    if ( desc.options[ SDOT_OPT_PRECISION ] != 0 || desc.options[ SDOT_OPT_LIN_PRECISION ] != 0 )
+        throw Error( SDOT_ERR_UNSUPPORTED, "options precision / lin_precision: FP64 clipping and an FP64 CG only (both 0)" );
     SolveJob *J = new SolveJob;
     try {
         J->t_begin = now_s();
