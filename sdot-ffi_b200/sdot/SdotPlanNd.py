@@ -48,11 +48,14 @@ def exact_duplicates(positions):
     return dup.astype(np.int64), rep[dup].astype(np.int64)
 
 
-def solver_options(settings, n):
-    """the option vector of `sdot_solve_desc` from `Iterative` / `Tuning`"""
+def solver_options(settings, n, d=None):
+    """the option vector of `sdot_solve_desc` from `Iterative` / `Tuning` (`d`, when given, checks the step against the
+    dimension: `limits` is 2D only, SdotPlanNd.py:461-465)"""
     tun = settings.tuning
     if tun.step not in ("auto", "trials", "limits"):
         raise ValueError(f"unknown step : {tun.step!r} ( 'auto', 'trials' or 'limits' )")
+    if tun.step == "limits" and d is not None and d != 2:
+        raise ValueError("step = 'limits': 2D only (the area polynomials along the direction); in 3D: 'trials' or 'auto'")
     if tun.residual not in _RESIDUAL:
         raise ValueError(f"unknown residual: {tun.residual!r} ( {', '.join(_RESIDUAL)} )")
     if tun.linear_solver not in ("auto", "cg", "mg", "amg"):
@@ -121,7 +124,7 @@ class SdotPlanNd:
                 P, nu = P[keep], nu[keep]
                 w0 = None if w0 is None else np.asarray(w0, dtype=np.float64).reshape(-1)[keep]
             pbs.append((P, nu, w0, lo, hi, dst._sdot_density()))
-            opts.append(solver_options(settings, n))
+            opts.append(solver_options(settings, n, problem.nb_dims))
             plans.append(self)
         results = _lib.solve_batch(pbs, opts, cap_history=8 * (settings.max_iter + 1) + 64)
         for self, r in zip(plans, results):

@@ -38,7 +38,7 @@ class Server:
         from .PowerDiagram import _domain_box
         lo, hi = _domain_box(t.bounding_half_spaces(), d)
         keep = []
-        sd = _lib.solve_desc(pos, nu, weights0, lo, hi, t._sdot_density(), solver_options(settings, n), keep)
+        sd = _lib.solve_desc(pos, nu, weights0, lo, hi, t._sdot_density(), solver_options(settings, n, d), keep)
         ticket = ctypes.c_int64()
         st = _lib.Status()
         _lib.raise_for(_lib.load().sdot_server_submit(self._h, ctypes.byref(sd), ctypes.byref(ticket), ctypes.byref(st)), st, "sdot_server_submit")

@@ -48,6 +48,10 @@ def test_settings_map_onto_the_option_vector():
     assert o["lin_method"] == 1 and solver_options(Iterative(tuning=Tuning(linear_solver="cg")), 10)["lin_method"] == 0
     assert solver_options(Iterative(tuning=Tuning(step="limits")), 10)["step"] == 1
     assert solver_options(Iterative(tuning=Tuning(step="trials")), 10)["step"] == 0
+    assert solver_options(Iterative(tuning=Tuning(step="limits")), 10, 2)["step"] == 1
+    with pytest.raises(ValueError):                    # SdotPlanNd.py:461-465: the limits step is 2D only
+        solver_options(Iterative(tuning=Tuning(step="limits")), 10, 3)
+    assert solver_options(Iterative(), 10, 3)["step"] == 0
     with pytest.raises(ValueError):
         solver_options(Iterative(tuning=Tuning(step="bisection")), 10)
     with pytest.raises(NotImplementedError):
