@@ -293,6 +293,27 @@ def test_newton_reaches_the_target_masses():
     assert np.abs(m - 1 / n).max() * n < 1e-8
 
 
+def test_newton_converges_quadratically_on_an_image():
+    """tests/test_SdotPlanNd.py:245-277 on the oracle: 300 seeds on a soft 24 x 24 image converge in few steps, the last
+    two each an order of magnitude (the quadratic phase); a warm start from a neighbouring cloud's weights takes at most
+    6; a warm start that empties cells is dropped for the Voronoi start. (The reference's 2D default is its LIMITS step,
+    which takes no backtrack here; the oracle's TRIALS take one at the first step.)"""
+    rng = np.random.default_rng(41)
+    n = 300
+    pos = rng.uniform(0.05, 0.95, size=(n, 2))
+    vals = 1 + 0.5 * rng.random((24, 24))
+    dens = ("image", [0, 0], [1 / 24, 1 / 24], vals * (24 * 24 / vals.sum()))
+    s = O.solve(pos, density=dens, tol_abs=1e-10 / n, maxit=60)
+    res = s["history"][:, 4] * n
+    assert s["stats"]["status"] == 1 and res[-1] < 1e-9 and len(res) < 30
+    assert res[-1] < 0.1 * res[-2] < 0.01 * res[-3]
+    assert np.abs(s["masses"] - 1 / n).max() < 1e-11
+    warm = O.solve(pos + 1e-4 * rng.normal(size=pos.shape), density=dens, tol_abs=1e-10 / n, maxit=60, w0=s["weights"])
+    assert warm["stats"]["status"] == 1 and warm["stats"]["start"] == 0 and len(warm["history"]) <= 6
+    bad = O.solve(pos, density=dens, tol_abs=1e-10 / n, maxit=60, w0=rng.uniform(-1, 1, n))
+    assert bad["stats"]["status"] == 1 and bad["stats"]["start"] == 1
+
+
 def test_log_and_lin_residuals_reach_the_same_plan():
     """tests/test_SdotPlanNd.py:327-348"""
     rng = np.random.default_rng(2)
