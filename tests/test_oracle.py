@@ -293,6 +293,42 @@ def test_newton_reaches_the_target_masses():
     assert np.abs(m - 1 / n).max() * n < 1e-8
 
 
+def _gaussian_target(c, s, m):
+    """the oracle's density and domain of a sum of gaussians: the masses normalised, the box `c +- 6 sigma`
+    (distributions/SumOfGaussians.py, the declared support)"""
+    lo, hi = (c - 6 * s[:, None]).min(axis=0), (c + 6 * s[:, None]).max(axis=0)
+    return ("gauss", c, s, m / m.sum()), (lo, hi)
+
+
+def test_a_nonzero_start_is_kept_and_converges():
+    """tests/test_SdotPlanNd.py:137-158: 18 seeds, two overlapping gaussians (the soft case, the reference's
+    `_overlapping_target(2, 2, seed=3)`), small random start weights that empty no cell: kept, and converged"""
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(0.1, 0.9, size=(18, 2))
+    g = np.random.default_rng(3)
+    c = 0.5 + g.uniform(-0.12, 0.12, size=(2, 2))
+    dens, box = _gaussian_target(c, g.uniform(0.18, 0.24, 2), g.uniform(0.6, 1.4, 2))
+    w0 = rng.uniform(-0.003, 0.003, 18)
+    s = O.solve(pos, box=box, density=dens, w0=w0, tol_abs=1e-12, maxit=50)
+    assert s["stats"]["status"] == 1 and s["stats"]["start"] == 0
+    assert np.abs(s["masses"] - s["stats"]["domain_mass"] / 18).max() < 1e-10
+
+
+@pytest.mark.parametrize("continuation", [0, 1])
+def test_no_cell_dies_on_scattered_targets(continuation):
+    """tests/test_SdotPlanNd.py:160-182: 40 seeds, four narrow separate gaussians (the hard case, the reference's
+    `_scattered_target(2, 4, seed=6)`): no cell is empty at any step of the history, and the fit reaches the targets"""
+    rng = np.random.default_rng(5)
+    pos = rng.uniform(0.1, 0.9, size=(40, 2))
+    g = np.random.default_rng(6)
+    c = g.uniform(0.3, 0.7, size=(4, 2))
+    dens, box = _gaussian_target(c, np.full(4, 0.13), g.uniform(0.7, 1.3, 4))
+    s = O.solve(pos, box=box, density=dens, tol_abs=1e-12, maxit=200, continuation=continuation)
+    assert s["stats"]["status"] == 1
+    assert (s["history"][:, 3] > 0).all()
+    assert np.abs(s["masses"] - s["stats"]["domain_mass"] / 40).max() < 1e-10
+
+
 def test_newton_converges_quadratically_on_an_image():
     """tests/test_SdotPlanNd.py:245-277 on the oracle: 300 seeds on a soft 24 x 24 image converge in few steps, the last
     two each an order of magnitude (the quadratic phase); a warm start from a neighbouring cloud's weights takes at most
