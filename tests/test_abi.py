@@ -85,3 +85,18 @@ def test_calls_fail_loudly_without_a_device():
     code = L.sdot_context_create(0, 0, ctypes.byref(h), ctypes.byref(st))
     assert code == _lib.SDOT_ERR_CUDA
     assert st.message
+
+
+def test_a_c_program_binds_the_library(tmp_path):
+    """tests/c_caller.c, a plain C caller of the header (no Python in its process), compiles with gcc -std=c11
+    -Wall -Werror and links against the library; without a device it reports the context's CUDA error and stops"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the solve itself is the GPU test's")
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = tmp_path / "c_caller"
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_caller.c"), "-o", str(exe), "-L", libdir, "-lsdot_b200",
+                    f"-Wl,-rpath,{libdir}", "-lm"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out[0] == "context" and int(out[1]) == _lib.SDOT_ERR_CUDA, out
