@@ -27,6 +27,7 @@ struct Req {
     bool done = false;
     sdot_status status;
     std::vector<double> weights, masses, bary, history;
+    std::vector<int32_t> clusters;
     double cost = 0;
     double stats[ SDOT_NB_STATS ];
     int nb_history = 0;
@@ -94,9 +95,11 @@ void sdot_server_s::run() {
                 std::lock_guard<std::mutex> lock( mu );
                 active.push_back( r );
                 ++counters[ 0 ];
-            } catch ( const Error &e ) {
+            } catch ( const std::exception &e ) {
+                // (an Error carries the code; anything else, std::bad_alloc included, is the host running out)
+                const Error *E = dynamic_cast<const Error *>( &e );
                 std::lock_guard<std::mutex> lock( mu );
-                set_status( &r->status, e.code, e.msg, e.id, e.needed );
+                set_status( &r->status, E ? E->code : SDOT_ERR_NO_MEMORY, e.what(), E ? E->id : -1, E ? E->needed : 0 );
                 r->done = true;
                 used -= r->bytes;
                 ++counters[ 1 ];
@@ -116,9 +119,10 @@ void sdot_server_s::run() {
         try {
             jobs_tick( c, jobs );
             ++counters[ 4 ];
-        } catch ( const Error &e ) {
-            fail = e.msg;
-            fail_code = e.code;
+        } catch ( const std::exception &e ) {
+            const Error *E = dynamic_cast<const Error *>( &e );
+            fail = e.what();
+            fail_code = E ? E->code : SDOT_ERR_NO_MEMORY;
         }
         std::vector<Req *> keep, finished;
         for ( Req *r : active ) {
@@ -135,6 +139,7 @@ void sdot_server_s::run() {
                     r->masses.resize( n );
                     r->bary.resize( size_t( n ) * dim );
                     r->history.resize( size_t( 8 ) * 1024 );
+                    r->clusters.resize( n );
                     sdot_solve_out o;
                     std::memset( &o, 0, sizeof( o ) );
                     o.weights = r->weights.data();
@@ -143,12 +148,14 @@ void sdot_server_s::run() {
                     o.cost = &r->cost;
                     o.history = r->history.data();
                     o.cap_history = 1024;
+                    o.clusters = r->clusters.data();
                     job_outputs( c, r->job, o, SDOT_HOST );
                     std::memcpy( r->stats, o.stats, sizeof( r->stats ) );
                     r->nb_history = o.nb_history;
                     set_status( &r->status, SDOT_OK, "" );
-                } catch ( const Error &e ) {
-                    set_status( &r->status, e.code, e.msg, e.id, e.needed );
+                } catch ( const std::exception &e ) {
+                    const Error *E = dynamic_cast<const Error *>( &e );
+                    set_status( &r->status, E ? E->code : SDOT_ERR_NO_MEMORY, e.what(), E ? E->id : -1, E ? E->needed : 0 );
                 }
             }
             job_destroy( c, r->job );
@@ -256,6 +263,7 @@ int32_t sdot_server_poll( sdot_server srv, int64_t ticket, sdot_solve_out *out, 
         if ( out->masses ) std::memcpy( out->masses, r->masses.data(), n * 8 );
         if ( out->barycentres ) std::memcpy( out->barycentres, r->bary.data(), size_t( n ) * dim * 8 );
         if ( out->cost ) *out->cost = r->cost;
+        if ( out->clusters ) std::memcpy( out->clusters, r->clusters.data(), n * sizeof( int32_t ) );
         std::memcpy( out->stats, r->stats, sizeof( out->stats ) );
         int k = std::min( r->nb_history, out->cap_history );
         if ( out->history && k > 0 ) std::memcpy( out->history, r->history.data(), size_t( k ) * 8 * 8 );

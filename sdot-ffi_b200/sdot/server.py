@@ -2,7 +2,7 @@
 
     srv = Server()
     t = srv.submit(positions, target=SumOfGaussians(...), settings=Iterative(...))
-    plan = srv.result(t)            # dict: weights, masses, barycentres, cost, stats, history
+    plan = srv.result(t)            # dict: weights, masses, barycentres, cost, stats, history, clusters
 
 Requests are copied at submission; the server's worker thread admits them between two Newton steps of the
 solves already running (memory budget and `max_active` permitting) and returns each as soon as it is done.
