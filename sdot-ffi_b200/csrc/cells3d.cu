@@ -2,7 +2,7 @@
 //
 // The cell is kept as its dual: every vertex is a triple of plane ids (a, b, c) -- the three faces meeting there,
 // ordered so that the triples form a consistently oriented triangulation of the sphere -- and its position is
-// ALWAYS re-solved from those three planes (Cramer's rule, FP64, seed frame), so no error accumulates along the
+// ALWAYS re-solved from those three planes (solve3: FP64, seed frame), so no error accumulates along the
 // cuts (the reference re-solves its float vertices for the same reason, gpu/Cell3D.cuh:1093-1147).  A cut by the
 // plane P: lanes mark the vertices outside; for each directed edge (e0, e1) of a removed vertex whose twin (e1, e0)
 // belongs to a kept vertex, the new vertex (e0, e1, P) is created; kept vertices are compacted in order and the
