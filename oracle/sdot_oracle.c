@@ -8,13 +8,15 @@
  * `cpu_baseline` / `--impl reference` legs of `bench.py` may load this library, and only as the checker
  * or as the timed CPU baseline; the product (the CUDA library) never calls it.
  *
- * Parity status: UNPINNED against outputs of the reference itself -- the reference cannot be imported
- * or compiled here (its C++ needs the third-party `loom-ffi==2026.10.10.1` support headers and
- * loom-generated aggregate headers, absent from the tree; its CPU Cholesky needs Eigen 3.4.0, absent).
- * The restatement is pinned instead on the reference's own known-answer tests for this path
- * (tests/test_PowerDiagram.py:35-45, 46-57, 58-76, 217-244, 245-264, 266-284, 374-404; the
- * fixtures under tests/golden/) and on independent checks that share no code with it (Monte-Carlo
- * argmin partition, lifted convex hull neighbour sets, brute-force versus grid search).
+ * Parity status: PINNED on the reference's own known-answer tests for this path -- the fixtures under
+ * tests/golden/ (tests/test_PowerDiagram.py:35-45, 46-57, 58-76, 217-244, 245-264, 266-284, 374-404),
+ * the closed-form gaussian facet and its both-sides symmetry (tests/test_SumOfGaussians.py:20-61), the
+ * closed-form moments (tests/test_SdotPlanNd.py:460-498) and the reference's solver tests restated in
+ * the oracle's own test file -- and on independent checks that share no code with it (Monte-Carlo argmin
+ * partition, lifted convex hull neighbour sets, brute force versus grid search, finite differences).
+ * Not pinned against outputs of the reference itself: it cannot be imported or compiled here (its C++
+ * needs the third-party `loom-ffi==2026.10.10.1` support headers and loom-generated aggregate headers,
+ * absent from the tree; its CPU Cholesky needs Eigen 3.4.0, absent).
  *
  * What is restated, and from where (all paths relative to the reference project):
  *   - the power bisector `|x-p_i|^2 - w_i <= |x-p_j|^2 - w_j`, written in the frame of seed i as
