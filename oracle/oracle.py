@@ -4,8 +4,9 @@ ctypes wrapper of `libsdot_oracle.so`, the FP64 CPU restatement of the reference
 (`sdot_oracle.c` states what it restates and where from).  Only the tests, `__graft_entry__.smoke()`
 and the `cpu_baseline` / `--impl reference` legs of `bench.py` may import this module.
 
-Parity status: unpinned against outputs of the reference itself (the reference cannot be imported or
-compiled here); pinned on the reference's known-answer tests (tests/golden/) and on independent checks.
+Parity status: pinned on the reference's known-answer tests (tests/golden/, the closed-form gaussian facet and
+moments, the reference's solver tests restated in tests/test_oracle.py) and on independent checks; not pinned against
+outputs of the reference itself (it cannot be imported or compiled here).
 
 Densities are passed as tuples:
     ("uniform", rho)
