@@ -345,24 +345,3 @@ def test_big_cells_in_a_solve():
     plan = sdot.OtProblem(sdot.SumOfDiracs(pos), g).solve(sdot.Iterative(tol=0.0, tuning=sdot.Tuning(mass_rtol=1e-8)))
     assert plan.converged
     assert np.abs(plan.cell_masses / plan.target_masses - 1).max() <= 1e-8
-
-
-def test_the_unbuilt_precisions_are_refused():
-    """no silent FP64 in place of the FP32-clip variant or of an FP32 CG: `precision` 1 of a cells call, and the
-    `precision` / `lin_precision` options of a solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch"""
-    import ctypes
-    from sdot import Iterative, _lib
-    from sdot.SdotPlanNd import solver_options
-    pos = np.random.default_rng(3).uniform(size=(200, 2))
-    lo, hi = np.zeros(2), np.ones(2)
-    keep = []
-    desc = _lib.diagram_desc(pos, None, lo, hi, ("uniform", 1.0), keep)
-    m = np.zeros(200)
-    out = _lib.CellsOut(masses=m.ctypes.data, precision=1)
-    st = _lib.Status()
-    assert _lib.load().sdot_cells(_lib.context(), ctypes.byref(desc), ctypes.byref(out), ctypes.byref(st)) == _lib.SDOT_ERR_UNSUPPORTED
-    for key in ("precision", "lin_precision"):
-        opts = dict(solver_options(Iterative(), 200), **{key: 1})
-        r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
-        assert isinstance(r, NotImplementedError), r
-    assert np.abs(_pd(pos).measures.sum() - 1) < 1e-12          # the context is still usable

@@ -1,0 +1,70 @@
+"""The C ABI's serving layer and its refusals, on a device.
+
+The server (sdot_server_*: continuous batching) against the batched solve of the same requests, and the precision
+variants this build does not have, refused before any launch."""
+import numpy as np
+import pytest
+
+import sdot
+from sdot import Iterative, Tuning
+
+pytestmark = pytest.mark.gpu
+
+
+def _pd(pos):
+    d = pos.shape[1]
+    return sdot.PowerDiagram(pos, boundaries=sdot.box_half_spaces(np.zeros(d), np.ones(d)))
+
+
+def test_the_server_returns_the_plans_of_the_batched_solve():
+    """continuous batching (sdot_server_*): requests submitted one after the other, admitted while the others run, come
+    back with the plans the batched solve gives them -- weights, masses, status and the clusters of near-coincident
+    seeds (a pair 1e-9 apart, merged)"""
+    from helpers import degenerate_clouds
+    from sdot import _lib
+    from sdot.PowerDiagram import _domain_box
+    from sdot.SdotPlanNd import solver_options
+    from sdot.server import Server
+    rng = np.random.default_rng(61)
+    pair, _ = degenerate_clouds(2, 17)["pair at 1e-9"]
+    g = sdot.SumOfGaussians(rng.uniform(0.3, 0.7, size=(3, 2)), [0.1, 0.12, 0.08], support_box=(np.zeros(2), np.ones(2)))
+    cases = [(rng.uniform(size=(3000, 2)), sdot.Box()), (rng.uniform(size=(1500, 3)), sdot.Box()), (rng.uniform(size=(1000, 2)), g),
+             (pair, sdot.Box())]
+    settings = [Iterative(tol=0.0, max_iter=60, tuning=Tuning(mass_rtol=1e-9))] * 3 + [Iterative(tol=1e-11 / len(pair), max_iter=60)]
+    srv = Server()
+    try:
+        tickets = [srv.submit(pos, tg, settings=st) for (pos, tg), st in zip(cases, settings)]
+        served = [srv.result(t) for t in tickets]
+    finally:
+        srv.close()
+    for (pos, tg), st, r in zip(cases, settings, served):
+        n, d = pos.shape
+        t = tg.normalized_version(nb_dims=d)
+        lo, hi = _domain_box(t.bounding_half_spaces(), d)
+        b = _lib.solve_batch([(pos, None, None, lo, hi, t._sdot_density())], [solver_options(st, n, d)])[0]
+        assert r["stats"][0] == b["stats"][0] and b["stats"][0] in (1, 7), (r["stats"][0], b["stats"][0])
+        assert np.abs(r["weights"] - b["weights"]).max() <= 1e-12 * np.abs(b["weights"]).max()
+        assert np.abs(r["masses"] - b["masses"]).max() <= 1e-12 / n
+        assert np.array_equal(r["clusters"], b["clusters"])
+    assert served[-1]["stats"][0] == 7 and (served[-1]["clusters"] != np.arange(len(pair))).sum() == 1
+
+
+def test_the_unbuilt_precisions_are_refused():
+    """no silent FP64 in place of the FP32-clip variant or of an FP32 CG: `precision` 1 of a cells call, and the
+    `precision` / `lin_precision` options of a solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch"""
+    import ctypes
+    from sdot import _lib
+    from sdot.SdotPlanNd import solver_options
+    pos = np.random.default_rng(3).uniform(size=(200, 2))
+    lo, hi = np.zeros(2), np.ones(2)
+    keep = []
+    desc = _lib.diagram_desc(pos, None, lo, hi, ("uniform", 1.0), keep)
+    m = np.zeros(200)
+    out = _lib.CellsOut(masses=m.ctypes.data, precision=1)
+    st = _lib.Status()
+    assert _lib.load().sdot_cells(_lib.context(), ctypes.byref(desc), ctypes.byref(out), ctypes.byref(st)) == _lib.SDOT_ERR_UNSUPPORTED
+    for key in ("precision", "lin_precision"):
+        opts = dict(solver_options(Iterative(), 200), **{key: 1})
+        r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
+        assert isinstance(r, NotImplementedError), r
+    assert np.abs(_pd(pos).measures.sum() - 1) < 1e-12          # the context is still usable
