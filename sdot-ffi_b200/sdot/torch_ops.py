@@ -2,11 +2,13 @@
 
     cost = w2_batch(positions, nu=None, target=None)        # positions [B, N, d] on a CUDA device, FP32 or FP64
     cost.sum().backward()                                   # positions.grad, nu.grad
+    w = weights_batch(positions, nu)                        # the fitted weights [B, N], differentiable too
 
 Forward: ONE call of the C ABI (`sdot_solve_batch`) on the device pointers -- the B problems advance together.
 Backward: the hand-written kernel `sdot_w2_backward` -- the envelope theorem at the fitted weights,
 d W2 / d p_i = 2 m_i (p_i - b_i) and d W2 / d nu_i = w_i projected on sum(d nu) = 0 (SdotPlanNd.py:1037-1040,
-1107-1122).  PyTorch only owns the device memory and the autograd graph.
+1107-1122).  The weights' backward is the implicit-function derivative (SdotPlanNd.py:1018-1050): one Laplacian solve
+and one adjoint of the masses a problem, `weights_vjp`.  PyTorch only owns the device memory and the autograd graph.
 """
 import ctypes
 
@@ -97,6 +99,81 @@ class _W2Batch(torch.autograd.Function):
                                                     ctypes.byref(st)), st, "sdot_w2_backward")
         _lib.load().sdot_context_synchronize(_lib.context(pos.device.index), ctypes.byref(st))
         return gpos, (gnu.to(ctx.nu_dtype) if ctx.has_nu else None), None, None
+
+
+def weights_vjp(pos, w, nu, grad_w, laplacian, solve, masses_vjp, domain_mass=1.0):
+    """the implicit-function derivative of the fitted weights of one transport (SdotPlanNd.py:1018-1050).
+
+    At the fitted weights m(w, p) = nu_eff = M nu / sum(nu) (M the domain's mass, fixed), with the gauge w[0] = 0. The
+    jacobian of the masses in the weights is the Laplacian L, so dw = P L^+ (d nu_eff - J_p dp), P = I - 1 e_0^T. For a
+    cotangent g of the weights: lambda solves L lambda = P^T g = g - e_0 sum(g) (of zero sum), then
+        grad_p = - J_p^T lambda,     grad_nu = M / sum(nu) (lambda - (nu . lambda) / sum(nu)).
+    `laplacian(pos, w)` gives the CSR (row_ptr, cols, vals, dia) at the fitted weights, `solve(row_ptr, cols, vals, dia,
+    rhs)` one solution of L x = rhs, `masses_vjp(pos, w, lam)` J_p^T lam ([n, d]). Returns (grad_p, grad_nu or None)."""
+    g = np.asarray(grad_w, dtype=np.float64).reshape(-1)
+    rhs = g.copy()
+    rhs[0] -= g.sum()
+    row, cols, vals, dia = laplacian(pos, w)
+    lam = np.asarray(solve(row, cols, vals, dia, rhs), dtype=np.float64).reshape(-1)
+    gp = -np.asarray(masses_vjp(pos, w, lam), dtype=np.float64)
+    gnu = None
+    if nu is not None:
+        nu = np.asarray(nu, dtype=np.float64).reshape(-1)
+        s = nu.sum()
+        gnu = domain_mass / s * (lam - (nu @ lam) / s)
+    return gp, gnu
+
+
+def _solve_one(row, cols, vals, dia, rhs):
+    x, its = _lib.linear_solve(row, cols, vals, dia, rhs, tol=1e-12, method=1)
+    if its[0] < 0:
+        raise RuntimeError("weights_batch backward: the Laplacian solve did not converge")
+    return x[0]
+
+
+class _WeightsBatch(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, positions, nu, target, settings):
+        with torch.enable_grad():
+            p = positions.detach().requires_grad_(True)
+            cost = _W2Batch.apply(p, None if nu is None else nu.detach(), target, settings)
+        node = cost.grad_fn
+        weights, masses = node.saved_tensors[3], node.saved_tensors[1]
+        ctx.save_for_backward(positions, weights, masses, nu if nu is not None else torch.empty(0, device=positions.device))
+        ctx.has_nu, ctx.target = nu is not None, target
+        return weights.clone()
+
+    @staticmethod
+    def backward(ctx, grad_w):
+        positions, weights, masses, nu = ctx.saved_tensors
+        B, N, d = positions.shape
+        _, lo, hi = _target_density(ctx.target, d)
+        dens = _target_density(ctx.target, d)[0]
+        gp = torch.empty(B, N, d, dtype=torch.float64)
+        gn = torch.empty(B, N, dtype=torch.float64) if ctx.has_nu else None
+        for b in range(B):
+            pos = positions[b].detach().to(torch.float64).cpu().numpy()
+            w = weights[b].cpu().numpy()
+            nub = nu[b].detach().to(torch.float64).cpu().numpy() if ctx.has_nu else None
+            x, xn = weights_vjp(pos, w, nub, grad_w[b].detach().to(torch.float64).cpu().numpy(),
+                                lambda p, ww: _lib.laplacian(p, ww, lo, hi, dens),
+                                _solve_one,
+                                lambda p, ww, lam: _lib.cells_vjp(p, ww, lo, hi, dens, lam)[0],
+                                float(masses[b].sum()))
+            gp[b] = torch.from_numpy(x)
+            if ctx.has_nu:
+                gn[b] = torch.from_numpy(xn)
+        gp = gp.to(device=positions.device, dtype=positions.dtype)
+        gn = None if gn is None else gn.to(device=positions.device, dtype=nu.dtype)
+        return gp, gn, None, None
+
+
+def weights_batch(positions, nu=None, target=None, settings=None):
+    """the fitted weights of the B transports [B, N] (FP64, gauge w[0] = 0), differentiable wrt `positions` [B, N, d] and
+    `nu` [B, N] by the implicit function theorem (`weights_vjp`: one Laplacian solve and one masses adjoint a problem,
+    through the C ABI)"""
+    settings = settings or Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-12))
+    return _WeightsBatch.apply(positions, nu, target, settings)
 
 
 def w2_batch(positions, nu=None, target=None, settings=None):

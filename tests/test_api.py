@@ -115,3 +115,62 @@ def test_exact_duplicates_are_written_back_with_empty_cells():
     assert w[0] == 0 and w[1] == 0.25 and w[3] == -0.125
     assert w[4] < w[2] < w[0] and np.isclose(w[0] - w[2], w[2] - w[4])
     assert np.array_equal(b[[0, 1, 3]], r["barycentres"]) and np.array_equal(b[2], pos[2]) and np.array_equal(b[4], pos[4])
+
+
+def test_the_weights_derivative_is_the_derivative_of_the_solve():
+    """SdotPlanNd.py:1018-1050, tests/test_SdotPlanNd.py:2068-2104: the implicit-function derivative of the fitted
+    weights (`torch_ops.weights_vjp`, the backward of `weights_batch`), driven here by the oracle's diagram, a dense
+    solve and a finite-difference adjoint of the masses, against central differences of the whole oracle solve in the
+    positions and in the target masses (1e-7 of the largest component)"""
+    import oracle as O
+    from sdot.torch_ops import weights_vjp
+    rng = np.random.default_rng(0)
+    n, d = 16, 2
+    pos = rng.uniform(0.2, 0.8, size=(n, d))
+    nu = rng.uniform(0.5, 1.5, n)
+
+    def solve(p, q):
+        s = O.solve(p, nu=q / q.sum(), tol_abs=1e-15, maxit=100)
+        assert s["stats"]["status"] == 1
+        return s["weights"]
+
+    def laplacian(p, w):
+        r = O.cells(p, w)
+        row, cols, vals = [0], [], []
+        for i in range(n):
+            k = r["nb"][i]
+            cols += list(r["nid"][i, :k])
+            vals += list(r["nc"][i, :k])
+            row.append(row[-1] + k)
+        return np.array(row), np.array(cols), np.array(vals), np.array([r["nc"][i, : r["nb"][i]].sum() for i in range(n)])
+
+    def dense_solve(row, cols, vals, dia, rhs):
+        L = np.diag(dia)
+        for i in range(n):
+            L[i, cols[row[i]:row[i + 1]]] -= vals[row[i]:row[i + 1]]
+        return np.linalg.lstsq(0.5 * (L + L.T), rhs, rcond=None)[0]
+
+    def masses_vjp(p, w, lam, h=1e-7):
+        out = np.zeros_like(p)
+        for k in range(n):
+            for a in range(d):
+                pp, pm = p.copy(), p.copy()
+                pp[k, a] += h
+                pm[k, a] -= h
+                out[k, a] = lam @ (O.cells(pp, w)["mass"] - O.cells(pm, w)["mass"]) / (2 * h)
+        return out
+
+    w = solve(pos, nu)
+    g = rng.standard_normal(n)
+    gp, gn = weights_vjp(pos, w, nu, g, laplacian, dense_solve, masses_vjp, 1.0)
+    h = 1e-6
+    fp = np.zeros_like(pos)
+    for k in range(n):
+        for a in range(d):
+            pp, pm = pos.copy(), pos.copy()
+            pp[k, a] += h
+            pm[k, a] -= h
+            fp[k, a] = g @ (solve(pp, nu) - solve(pm, nu)) / (2 * h)
+    fn = np.array([g @ (solve(pos, nu + h * e) - solve(pos, nu - h * e)) / (2 * h) for e in np.eye(n)])
+    assert np.abs(gp - fp).max() < 1e-7 * np.abs(fp).max()
+    assert np.abs(gn - fn).max() < 1e-7 * np.abs(fn).max()

@@ -1,7 +1,8 @@
-"""The C ABI's serving layer and its refusals, on a device.
+"""The C ABI's serving layer, its refusals and the weights' derivative, on a device.
 
-The server (sdot_server_*: continuous batching) against the batched solve of the same requests, and the precision
-variants this build does not have, refused before any launch."""
+The server (sdot_server_*: continuous batching) against the batched solve of the same requests; the precision variants
+this build does not have, refused before any launch; the implicit-function derivative of the fitted weights against
+differences of the solve."""
 import numpy as np
 import pytest
 
@@ -68,3 +69,32 @@ def test_the_unbuilt_precisions_are_refused():
         r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
         assert isinstance(r, NotImplementedError), r
     assert np.abs(_pd(pos).measures.sum() - 1) < 1e-12          # the context is still usable
+
+
+def test_the_weights_are_differentiable():
+    """SdotPlanNd.py:1018-1050: `torch_ops.weights_batch`'s backward (one Laplacian solve and one adjoint of the masses
+    through the C ABI) against central differences of the GPU solve itself, in the positions and in the target masses"""
+    import torch
+    from sdot.torch_ops import weights_batch
+    rng = np.random.default_rng(7)
+    n = 200
+    pos = torch.tensor(rng.uniform(0.2, 0.8, size=(1, n, 2)), dtype=torch.float64, device="cuda", requires_grad=True)
+    nu = torch.tensor(rng.uniform(0.5, 1.5, size=(1, n)), dtype=torch.float64, device="cuda", requires_grad=True)
+    settings = Iterative(tol=0.0, max_iter=100, tuning=Tuning(mass_rtol=1e-13))
+    g = torch.tensor(rng.standard_normal((1, n)), dtype=torch.float64, device="cuda")
+    (weights_batch(pos, nu, settings=settings) * g).sum().backward()
+
+    def loss(p, q):
+        with torch.no_grad():
+            return float((weights_batch(p, q, settings=settings) * g).sum())
+    h = 1e-5
+    for k, a in ((3, 0), (50, 1), (117, 0), (199, 1)):
+        e = torch.zeros_like(pos)
+        e[0, k, a] = h
+        fd = (loss(pos.detach() + e, nu.detach()) - loss(pos.detach() - e, nu.detach())) / (2 * h)
+        assert abs(float(pos.grad[0, k, a]) - fd) < 1e-5 * max(1.0, abs(fd)), (k, a, float(pos.grad[0, k, a]), fd)
+    for k in (0, 77, 150):
+        e = torch.zeros_like(nu)
+        e[0, k] = h
+        fd = (loss(pos.detach(), nu.detach() + e) - loss(pos.detach(), nu.detach() - e)) / (2 * h)
+        assert abs(float(nu.grad[0, k]) - fd) < 1e-5 * max(1.0, abs(fd)), (k, float(nu.grad[0, k]), fd)
