@@ -174,3 +174,15 @@ def test_the_weights_derivative_is_the_derivative_of_the_solve():
     fn = np.array([g @ (solve(pos, nu + h * e) - solve(pos, nu - h * e)) / (2 * h) for e in np.eye(n)])
     assert np.abs(gp - fp).max() < 1e-7 * np.abs(fp).max()
     assert np.abs(gn - fn).max() < 1e-7 * np.abs(fn).max()
+
+
+def test_the_domain_comes_from_the_density_alone():
+    """tests/test_SdotPlanNd.py:409-438 (its host part): the domain of a gaussian target is the support it declares,
+    `centres +- 6 sigma`, not the envelope of the diracs; a target that declares no support is refused"""
+    from sdot.SdotPlanNd import _box_of
+    pos = np.random.default_rng(3).uniform(0.4, 0.6, size=(60, 2))
+    g = SumOfGaussians(np.array([[0.5, 0.5]]), np.array([0.15]), weights=np.array([1.0]))
+    lo, hi = _box_of(OtProblem(SumOfDiracs(pos), g))
+    assert np.allclose(lo, [0.5 - 0.9] * 2) and np.allclose(hi, [0.5 + 0.9] * 2)
+    with pytest.raises(ValueError):
+        OtProblem(SumOfDiracs(pos), SumOfGaussians(np.array([[0.5, 0.5]]), np.array([0.15]), support_sigmas=None)).solve()
