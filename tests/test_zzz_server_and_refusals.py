@@ -80,7 +80,7 @@ def test_the_weights_are_differentiable():
     n = 200
     pos = torch.tensor(rng.uniform(0.2, 0.8, size=(1, n, 2)), dtype=torch.float64, device="cuda", requires_grad=True)
     nu = torch.tensor(rng.uniform(0.5, 1.5, size=(1, n)), dtype=torch.float64, device="cuda", requires_grad=True)
-    settings = Iterative(tol=0.0, max_iter=100, tuning=Tuning(mass_rtol=1e-13))
+    settings = Iterative(tol=0.0, max_iter=100, tuning=Tuning(mass_rtol=1e-12))
     g = torch.tensor(rng.standard_normal((1, n)), dtype=torch.float64, device="cuda")
     (weights_batch(pos, nu, settings=settings) * g).sum().backward()
 
