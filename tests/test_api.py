@@ -117,15 +117,16 @@ def test_exact_duplicates_are_written_back_with_empty_cells():
     assert np.array_equal(b[[0, 1, 3]], r["barycentres"]) and np.array_equal(b[2], pos[2]) and np.array_equal(b[4], pos[4])
 
 
-def test_the_weights_derivative_is_the_derivative_of_the_solve():
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_weights_derivative_is_the_derivative_of_the_solve(d):
     """SdotPlanNd.py:1018-1050, tests/test_SdotPlanNd.py:2068-2104: the implicit-function derivative of the fitted
     weights (`torch_ops.weights_vjp`, the backward of `weights_batch`), driven here by the oracle's diagram, a dense
     solve and a finite-difference adjoint of the masses, against central differences of the whole oracle solve in the
     positions and in the target masses (1e-7 of the largest component)"""
     import oracle as O
     from sdot.torch_ops import weights_vjp
-    rng = np.random.default_rng(0)
-    n, d = 16, 2
+    rng = np.random.default_rng(d)
+    n = 16 if d == 2 else 10
     pos = rng.uniform(0.2, 0.8, size=(n, d))
     nu = rng.uniform(0.5, 1.5, n)
 
