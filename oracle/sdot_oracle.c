@@ -559,7 +559,7 @@ static int clip3( poly3 *P, const double *n, double off, int cid ) {
         for ( int k = 0; k < P->nv[ f ]; ++k ) { ntot++; nout += dot3( n, P->v[ f ][ k ].p ) - off > 0; }
     if ( nout == 0 ) return 0;
     if ( nout == ntot ) { P->nf = 0; return 0; }
-    v3 cross[ 2 * OD_MAXF ];
+    v3 cross[ 4 * OD_MAXF ];
     int nc = 0, nf = 0;
     for ( int f = 0; f < P->nf; ++f ) {
         int m = P->nv[ f ], q = 0;
@@ -570,6 +570,12 @@ static int clip3( poly3 *P, const double *n, double off, int cid ) {
             int k1 = k + 1 == m ? 0 : k + 1;
             if ( q + 2 >= OD_MAXFV ) return -1;
             if ( s[ k ] <= 0 ) out[ q++ ] = P->v[ f ][ k ];
+            /* a kept vertex ON the plane (to rounding) belongs to the new face although no edge of it crosses: on a
+               grid the planes pass through vertices, and a section made of the crossings alone lost its corners */
+            if ( s[ k ] <= 0 && fabs( s[ k ] ) <= 16 * DBL_EPSILON * ( sqrt( dot3( n, n ) * dot3( P->v[ f ][ k ].p, P->v[ f ][ k ].p ) ) + fabs( off ) ) ) {
+                if ( nc >= 4 * OD_MAXF ) return -1;
+                cross[ nc++ ] = P->v[ f ][ k ];
+            }
             if ( ( s[ k ] <= 0 ) != ( s[ k1 ] <= 0 ) ) {
                 /* from the kept end, whichever face reports the edge: the two faces of an edge then make the same point
                    to the bit (an edge nearly parallel to the plane would place its two copies far apart) */
@@ -578,7 +584,7 @@ static int clip3( poly3 *P, const double *n, double off, int cid ) {
                 v3 x;
                 for ( int a = 0; a < 3; ++a ) x.p[ a ] = P->v[ f ][ ui ].p[ a ] + t * ( P->v[ f ][ vi ].p[ a ] - P->v[ f ][ ui ].p[ a ] );
                 out[ q++ ] = x;
-                if ( nc >= 2 * OD_MAXF ) return -1;
+                if ( nc >= 4 * OD_MAXF ) return -1;
                 cross[ nc++ ] = x;
             }
         }
@@ -604,8 +610,8 @@ static int clip3( poly3 *P, const double *n, double off, int cid ) {
     double l1 = sqrt( dot3( e1, e1 ) );
     for ( int a = 0; a < 3; ++a ) e1[ a ] /= l1;
     e2[ 0 ] = un[ 1 ] * e1[ 2 ] - un[ 2 ] * e1[ 1 ]; e2[ 1 ] = un[ 2 ] * e1[ 0 ] - un[ 0 ] * e1[ 2 ]; e2[ 2 ] = un[ 0 ] * e1[ 1 ] - un[ 1 ] * e1[ 0 ];
-    double ang[ 2 * OD_MAXF ];
-    int ord[ 2 * OD_MAXF ];
+    double ang[ 4 * OD_MAXF ];
+    int ord[ 4 * OD_MAXF ];
     for ( int k = 0; k < nc; ++k ) {
         double d[ 3 ] = { cross[ k ].p[ 0 ] - ctr[ 0 ], cross[ k ].p[ 1 ] - ctr[ 1 ], cross[ k ].p[ 2 ] - ctr[ 2 ] };
         ang[ k ] = atan2( dot3( d, e2 ), dot3( d, e1 ) );

@@ -47,6 +47,36 @@ def test_grid_search_is_the_brute_force(d, n):
     assert abs(a["mass"].sum() - 1) < 1e-12
 
 
+@pytest.mark.parametrize("brute", [False, True])
+@pytest.mark.parametrize("shape", [(40, 30), (3, 3, 3), (12, 10, 8), (20, 20, 20)])
+def test_grids_give_the_exact_boxes(shape, brute):
+    """tests/test_CardCells.py:166-187, 900-941: seeds on a grid -- every vertex shared by 4 (2D) or 8 (3D) cells, cuts
+    through vertices already on them -- have the grid's boxes as cells, 1e-10 relative"""
+    d = len(shape)
+    g = np.stack(np.meshgrid(*[(np.arange(k) + 0.5) / k for k in shape], indexing="ij"), axis=-1).reshape(-1, d)
+    if brute and len(g) > 1000:
+        pytest.skip("the brute-force search is quadratic")
+    r = O.cells(g, brute=brute)
+    assert r["status"] == 0
+    assert np.abs(r["mass"] * len(g) - 1).max() < 1e-10
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_a_seed_outside_and_lighter_duplicates(d):
+    """tests/test_CardCells.py:180-187, 934-941: a seed outside the domain, and 19 seeds repeated with a weight 1e-4
+    lower: the repeats' cells are empty and every other cell is the one of the cloud without them"""
+    rng = np.random.default_rng(3 if d == 2 else 33)
+    pos = rng.uniform(0.1, 0.9, size=(500, d))
+    pos[0] = [1.5] + [0.5] * (d - 1)
+    both = np.concatenate([pos, pos[1:20]])
+    w = np.zeros(len(both))
+    w[500:] = -1e-4
+    a, b = O.cells(both, w), O.cells(pos)
+    assert a["status"] == 0 and b["status"] == 0
+    assert (a["mass"][500:] == 0).all()
+    assert np.abs(a["mass"][:500] - b["mass"]).max() < 1e-15 and abs(a["mass"].sum() - 1) < 1e-12
+
+
 @pytest.mark.parametrize("d", [2, 3])
 def test_monte_carlo_partition(d):
     rng = np.random.default_rng(100 + d)
