@@ -98,3 +98,13 @@ def test_the_weights_are_differentiable():
         e[0, k] = h
         fd = (loss(pos.detach(), nu.detach() + e) - loss(pos.detach(), nu.detach() - e)) / (2 * h)
         assert abs(float(nu.grad[0, k]) - fd) < 1e-5 * max(1.0, abs(fd)), (k, float(nu.grad[0, k]), fd)
+
+
+@pytest.mark.parametrize("shape", [(40, 30), (12, 10, 8), (20, 20, 20)])
+def test_grids_give_the_exact_boxes(shape):
+    """tests/test_CardCells.py:166-187, 900-941: seeds on a grid (cuts through vertices already on the cell, the ties a
+    clip must survive) have the grid's boxes as cells, 1e-10 relative"""
+    d = len(shape)
+    g = np.stack(np.meshgrid(*[(np.arange(k) + 0.5) / k for k in shape], indexing="ij"), axis=-1).reshape(-1, d)
+    m = _pd(g).measures
+    assert np.abs(m * len(g) - 1).max() < 1e-10 and abs(m.sum() - 1) < 1e-12
