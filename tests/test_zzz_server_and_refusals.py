@@ -1,8 +1,8 @@
-"""The C ABI's serving layer, its refusals and the weights' derivative, on a device.
+"""The C ABI's serving layer, its refusals, the weights' derivative and the grid clouds, on a device.
 
 The server (sdot_server_*: continuous batching) against the batched solve of the same requests; the precision variants
 this build does not have, refused before any launch; the implicit-function derivative of the fitted weights against
-differences of the solve."""
+differences of the solve; seeds on grids, whose cells are the grid's boxes."""
 import numpy as np
 import pytest
 
