@@ -279,28 +279,73 @@ def run_served(reqs, seed, lam):
     return max(done.values()), np.array(lat), h2d, d2h, worst[0], counters, failed[0]
 
 
-def cpu_sample(reqs, seed, budget_s=20.0):
-    """the oracle (CPU restatement) on the first requests of the stream until `budget_s` of CPU work"""
+# ---- the CPU legs: the oracle in a worker process under a hard wall limit ---------------------------------------------------
+# measured oracle cost per seed of one solve (8 threads): 2D uniform ~40 us, 3D uniform ~110 us, 2D gaussians ~1.5 ms
+# (13 continuation stages); 3D gaussians ~1 s (adaptive tetrahedral quadrature: 956 s for one solve of 1,000 seeds)
+CPU_COST_PER_SEED = {(2, False): 4e-5, (3, False): 1.1e-4, (2, True): 1.5e-3, (3, True): 1.0}
+
+
+def cpu_eligible(r, cap_s):
+    """a request the CPU leg runs: not a 3D gaussian (minutes to hours per solve on the oracle), and a predicted cost
+    under `cap_s` seconds"""
+    return not (r["d"] == 3 and r["gauss"]) and CPU_COST_PER_SEED[(r["d"], r["gauss"])] * r["n"] <= cap_s
+
+
+def cpu_worker(seed, ks):
+    """(child process) the oracle's solve of each request k of `ks` in turn, one JSON line per finished solve"""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    threads = O.max_threads()
-    t0 = time.perf_counter()
-    count, solved, n_tot = 0, 0, 0
-    for r in reqs:
+    print(json.dumps({"threads": O.max_threads()}), flush=True)
+    for k in ks:
+        r = request(seed, k)
         t = target_of(r).normalized_version(nb_dims=r["d"])
         dens = t._sdot_density()
         od = ("uniform", dens[1]) if dens[0] == "uniform" else ("gauss", dens[1], dens[2], dens[3])
         lo, hi = t.box() if hasattr(t, "box") else (np.zeros(r["d"]), np.ones(r["d"]))
+        t0 = time.perf_counter()
         s = O.solve(positions(seed, r), box=(lo, hi), density=od, tol_abs=0.0, tol_rel=RTOL, lin_tol=1e-8, agg_margin=4.0)
-        count += 1
-        solved += s["stats"]["status"] in CONVERGED          # (only the solves that met the tolerance count)
-        n_tot += r["n"]
-        if time.perf_counter() - t0 > budget_s:
-            break
-    secs = time.perf_counter() - t0
-    return dict(value=solved / secs, unit="solves/s", cores=threads, kind="port",
-                sample=f"the first {count} requests of the same seeded stream (sum N = {n_tot}, {solved} met the tolerance), "
-                       f"oracle/sdot_oracle.c FP64 + OpenMP, same tolerance; CPU restatement of sdot's algorithm, not the reference binary")
+        print(json.dumps({"k": k, "n": r["n"], "secs": time.perf_counter() - t0, "ok": s["stats"]["status"] in CONVERGED}), flush=True)
+
+
+def cpu_sample(reqs, seed, budget_s=20.0, cap_s=8.0):
+    """the oracle (the CPU restatement of the reference's algorithm) on the eligible requests of `reqs`, in stream order,
+    in a worker process killed at `budget_s` of wall time (a hard limit: no solve can overrun it).  value = the solves
+    that met the tolerance / the seconds of the finished solves; a solve cut by the limit is not counted"""
+    ks = [r["k"] for r in reqs if cpu_eligible(r, cap_s)]
+    left_out = sum(1 for r in reqs if r["d"] == 3 and r["gauss"])
+    too_big = len(reqs) - left_out - len(ks)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", ",".join(map(str, ks)), "--seed", str(seed)]
+    proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    rows, threads = [], [None]
+
+    def read():
+        for line in proc.stdout:
+            try:
+                d = json.loads(line)
+            except ValueError:
+                continue
+            if "threads" in d:
+                threads[0] = d["threads"]
+            else:
+                rows.append(d)
+
+    th = threading.Thread(target=read, daemon=True)
+    th.start()
+    try:
+        proc.wait(timeout=budget_s)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        proc.wait()
+    th.join(timeout=5)
+    secs = sum(d["secs"] for d in rows)
+    solved = sum(1 for d in rows if d["ok"])
+    n_tot = sum(d["n"] for d in rows)
+    return dict(value=solved / secs if secs > 0 else None, unit="solves/s", cores=threads[0] or os.cpu_count(), kind="port",
+                sample=f"{len(rows)} of the {len(ks)} eligible requests finished within a {budget_s:.0f} s wall limit (stream order, "
+                       f"sum N = {n_tot}, {solved} met the tolerance, {sum(d['secs'] for d in rows):.1f} s of solves); left out: "
+                       f"{left_out} 3D-gaussian requests (the oracle's adaptive quadrature takes ~1 s per seed per solve) and {too_big} "
+                       f"whose predicted oracle time exceeds {cap_s:.0f} s; both leave-outs flatter the CPU. oracle/sdot_oracle.c "
+                       f"FP64 + OpenMP, same tolerance: the CPU restatement of sdot's algorithm, not the reference binary")
 
 
 def peaks():
@@ -346,10 +391,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--requests-per-step", type=int, default=32)
-    ap.add_argument("--plain-requests", type=int, default=16)
+    ap.add_argument("--requests-per-step", type=int, default=8)
     ap.add_argument("--seed", type=int, default=2026)
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="wall limit (s) of the GPU arm's CPU-baseline leg")
+    ap.add_argument("--ref-budget", type=float, default=150.0, help="wall limit (s) of the reference arm's CPU solves")
+    ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cells-only", type=int, default=0, help="diagrams of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--cells-dim", type=int, default=2)
     ap.add_argument("--cells-repeat", type=int, default=0)
@@ -359,6 +405,9 @@ def main():
     ap.add_argument("--solve-linear", default="auto", choices=["auto", "cg", "mg"])
     ap.add_argument("--solve-step", default="auto", choices=["auto", "trials", "limits"])
     a = ap.parse_args()
+    if a.cpu_worker is not None:
+        cpu_worker(a.seed, [int(k) for k in a.cpu_worker.split(",") if k])
+        return
     if a.solve_only:
         import sdot
         from sdot import Iterative, OtProblem, SumOfDiracs, Tuning, _lib
@@ -412,11 +461,13 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
+        # the timed slices of the GPU arm's stream, solved by the oracle on every host core under a hard wall limit
         reqs, skipped = stream(a.seed, (a.warmup + a.steps) * R, lambda r: True)
-        cpu = cpu_sample(reqs[a.warmup * R:], a.seed, budget_s=a.cpu_budget)
+        cpu = cpu_sample(reqs[a.warmup * R:], a.seed, budget_s=a.ref_budget)
         v = cpu["value"]
+        config["reference_step"] = f"a step's {R} requests at the measured CPU throughput (ms_per_step = R / value)"
         print(json.dumps({"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-                          "ms_per_step": 1000.0 / v if v else None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "ms_per_step": 1000.0 * R / v if v else None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                           "dtype": "f64", "data": "synthetic", "impl": "reference", "config": config,
                           "cpu_baseline": dict(cpu, value=v), "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                                                                       "d2h_bytes_per_step": 0}}))
@@ -442,6 +493,8 @@ def main():
     mine = rank_share(reqs, rank, world)
     warm, timed = mine[: a.warmup * R], mine[a.warmup * R:]
 
+    legs = {}
+    t_leg = time.perf_counter()
     # warm-up steps (untimed)
     for s in range(a.warmup):
         run_value_step(warm[s * R:(s + 1) * R], a.seed, torch, check=True)
@@ -463,21 +516,27 @@ def main():
             failed += f
     kst = _lib.kernel_stats()
     _lib.set_timing(False)
+    legs["warmup_and_value"] = time.perf_counter() - t_leg
+    t_leg = time.perf_counter()
     # only the solves that reached the mass tolerance count
     nfail = len(failed)
     if world > 1:
         secs, nfail = over_ranks(secs, nfail, dist, "cuda")
     value = ( a.steps * R * world - nfail ) / secs
 
-    # plain one-at-a-time on a sample of the timed requests
-    pr = timed[: a.plain_requests]
+    # plain one-at-a-time on the same requests
+    pr = timed
     p_secs, p_worst, p_failed = run_plain(pr, a.seed)
     plain = (len(pr) - p_failed) / p_secs
+    legs["plain"] = time.perf_counter() - t_leg
+    t_leg = time.perf_counter()
 
     # served stream, arrivals at twice the plain throughput
     lam = 2.0 * plain
     e_secs, lat, h2d, d2h, e_worst, counters, e_failed = run_served(timed, a.seed, lam)
     e2e = (len(timed) - e_failed) / e_secs
+    legs["served"] = time.perf_counter() - t_leg
+    t_leg = time.perf_counter()
 
     hbm, peak_kind = peaks()
     # the dominant kernel of the timed region: the 2D or the 3D cells, whichever took more device time
@@ -487,6 +546,7 @@ def main():
     achieved = cells_b / (ms / 1000) / 1e9 if ms > 0 else None
     cg_ms, cg_n, cg_rows = kst["cg"]
     cpu = cpu_sample(timed, a.seed, a.cpu_budget) if rank == 0 else None
+    legs["cpu"] = time.perf_counter() - t_leg
     if rank != 0:
         dist.destroy_process_group()
         return
@@ -512,6 +572,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
+        "legs_wall_s": {k: round(v, 1) for k, v in legs.items()},
     }
     print(json.dumps(line))
     if world > 1:

@@ -37,7 +37,9 @@ enum sdot_code {
     SDOT_ERR_NO_MEMORY = 3,       /* the device pool refused; nothing was launched past the refusal          */
     SDOT_ERR_CAPACITY = 4,        /* a cell exceeded its vertex / neighbour capacity: `id` is the user seed  */
     SDOT_ERR_UNSUPPORTED = 5,     /* a density / dimension combination this build does not integrate         */
-    SDOT_ERR_NOT_CONVERGED = 6    /* (solve only, informational: `stats[0]` holds the solver status)        */
+    SDOT_ERR_NOT_CONVERGED = 6,   /* (solve only, informational: `stats[0]` holds the solver status)        */
+    SDOT_ERR_TOPOLOGY = 7         /* a cell's clip gave a non-finite measure: `id` is the user seed; the cell
+                                     is written empty, never NaN (gpu/Cell2D.cuh:99-102, 1214-1231)           */
 };
 
 /* the reference's error buffer records (kind, id, value) (src/sdot/include/sdot/gpu/Cell2D.cuh:99-102);
@@ -159,7 +161,10 @@ int32_t sdot_linear_solve(sdot_context ctx, int64_t n, const int64_t *row_ptr, c
  * device-wide synchronisation of cudaFree).  Every array is device memory.  At most SDOT_NOALLOC_MAX_ROWS rows
  * (past it: SDOT_ERR_CAPACITY, `needed` = n).  The array is shared by every call on a device: calls that
  * overlap in time race (one context serialises its own calls).  The first call on a device looks the array's
- * address up; make it before any stream capture on that device. */
+ * address up; make it before any stream capture on that device, and do not reset a device the library has
+ * used (the address is kept).  The array (16 MB) is reserved on every device where the library's device code
+ * is loaded, whether or not this entry point is called.  Every array must be memory of the context's own
+ * device (or managed memory): another GPU's memory is refused with SDOT_ERR_ARGS before any launch. */
 #define SDOT_NOALLOC_MAX_ROWS 262144
 int32_t sdot_linear_solve_noalloc(sdot_context ctx, int64_t n, const int64_t *row_ptr, const int32_t *cols, const double *vals,
                                   const double *dia, int32_t nrhs, const double *rhs, double *x, double tol, int32_t maxit,

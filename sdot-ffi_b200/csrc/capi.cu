@@ -12,7 +12,7 @@ void set_status( sdot_status *st, int code, const std::string &msg, long long id
     if ( ! st ) return;
     std::memset( st, 0, sizeof( *st ) );
     st->code = code;
-    st->kind = code == SDOT_ERR_CAPACITY ? 2 : 0;
+    st->kind = code == SDOT_ERR_CAPACITY || code == SDOT_ERR_TOPOLOGY ? 2 : 0;
     st->id = id;
     st->needed = needed;
     std::strncpy( st->message, msg.c_str(), sizeof( st->message ) - 1 );

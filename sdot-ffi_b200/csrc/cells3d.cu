@@ -39,6 +39,7 @@ struct Cell3T {
     double par[ PC ];                            // each face's integral (facets pass)
     unsigned char used[ PC ];                    // plane compaction
     I remap[ PC ];
+    double L;                                    // the farthest corner of the box from the seed (the tie band)
     int nv, np;
 };
 using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in shared memory
@@ -78,6 +79,16 @@ __device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double
     z = Z0 + t * dz;
 }
 
+// THE TIES: how far beyond the plane n . y = off a vertex must lie to count as outside -- what the rounding of
+// n . v - off can reach for a vertex of the cell (|v| <= L, off computed from |n|^2 and the weights), 32 doubles' eps.
+// A plane through vertices that lie on it in exact arithmetic (a grid: the bisector of a diagonal neighbour passes
+// through an edge of the box cell) then leaves them inside, instead of cutting them off at the noise and making new
+// vertices from three planes through one line.  The cell moves by tol / |n| at most.
+__device__ __forceinline__ double tie_tol3( double nx, double ny, double nz, double off, double L ) {
+    const double n = sqrt( nx * nx + ny * ny + nz * nz );
+    return 32 * 2.220446049250313e-16 * ( n * ( n + L ) + fabs( off ) );
+}
+
 // the vertex holding the directed edge (e0, e1), -1 if none
 template<class C3>
 __device__ __forceinline__ int twin_of( const C3 &C, int e0, int e1 ) {
@@ -111,7 +122,11 @@ __device__ void init_box3( C3 &C, int lane, const double *lo, const double *hi, 
         C.vy[ lane ] = ( sy ? hi[ 1 ] : lo[ 1 ] ) - py;
         C.vz[ lane ] = ( sz ? hi[ 2 ] : lo[ 2 ] ) - pz;
     }
-    if ( lane == 0 ) { C.nv = 8; C.np = 6; }
+    if ( lane == 0 ) {
+        C.nv = 8; C.np = 6;
+        const double ex = fmax( hi[ 0 ] - px, px - lo[ 0 ] ), ey = fmax( hi[ 1 ] - py, py - lo[ 1 ] ), ez = fmax( hi[ 2 ] - pz, pz - lo[ 2 ] );
+        C.L = sqrt( ex * ex + ey * ey + ez * ez );
+    }
     __syncwarp();
 }
 
@@ -142,14 +157,15 @@ __device__ bool compact_planes( C3 &C, int lane ) {
     return C.np < PC;
 }
 
-// keep n . y <= off; false past a capacity
+// keep n . y <= off (a vertex within the tie band of the plane stays); false past a capacity
 template<class C3>
 __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double off, int id ) {
     const int nv = C.nv;
+    const double tol = tie_tol3( nx, ny, nz, off, C.L );
     int nout = 0;
     for ( int base = 0; base < nv; base += 32 ) {
         int k = base + lane;
-        bool o = k < nv && nx * C.vx[ k ] + ny * C.vy[ k ] + nz * C.vz[ k ] > off;
+        bool o = k < nv && nx * C.vx[ k ] + ny * C.vy[ k ] + nz * C.vz[ k ] - off > tol;
         if ( k < nv ) C.out[ k ] = o;
         nout += __popc( __ballot_sync( FULL3, o ) );
     }
@@ -168,18 +184,23 @@ __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double
     const int P = C.np;
     __syncwarp();
     if ( lane == 0 ) { C.nx[ P ] = nx; C.ny[ P ] = ny; C.nz[ P ] = nz; C.no[ P ] = off; C.pid[ P ] = id; C.np = P + 1; }
-    // the boundary edges: directed edges of removed vertices whose twin is kept
+    __syncwarp();
+    // the boundary edges: directed edges of removed vertices whose twin is kept.  Each new vertex (e0, e1, P) is
+    // re-solved from its three planes; where that lands off the edge it replaces (three planes nearly through one
+    // line: a cut that grazes the edge), it is taken on the edge instead, from its kept end, where n . y = off.  Its
+    // position waits in `area` (free until the integration) while the kept vertices are compacted.
     int nnew = 0;
     for ( int base = 0; base < nv; base += 32 ) {
         int k = base + lane;
         I tr[ 3 ][ 3 ];
+        int tt[ 3 ];
         int cnt = 0;
         if ( k < nv && C.out[ k ] ) {
             int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
             for ( int q = 0; q < 3; ++q ) {
                 int e0 = e[ q ], e1 = e[ ( q + 1 ) % 3 ];
                 int t = twin_of( C, e1, e0 );
-                if ( t >= 0 && ! C.out[ t ] ) { tr[ cnt ][ 0 ] = e0; tr[ cnt ][ 1 ] = e1; tr[ cnt ][ 2 ] = P; ++cnt; }
+                if ( t >= 0 && ! C.out[ t ] ) { tr[ cnt ][ 0 ] = e0; tr[ cnt ][ 1 ] = e1; tr[ cnt ][ 2 ] = P; tt[ cnt ] = t; ++cnt; }
             }
         }
         int inc = cnt;
@@ -187,8 +208,22 @@ __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double
         for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL3, inc, o ); if ( lane >= o ) inc += t; }
         int total = __shfl_sync( FULL3, inc, 31 );
         int at = nnew + inc - cnt;
-        for ( int q = 0; q < cnt; ++q )
-            if ( at + q < VC ) { C.nt[ at + q ][ 0 ] = tr[ q ][ 0 ]; C.nt[ at + q ][ 1 ] = tr[ q ][ 1 ]; C.nt[ at + q ][ 2 ] = tr[ q ][ 2 ]; }
+        for ( int q = 0; q < cnt; ++q ) {
+            if ( at + q >= VC ) continue;
+            C.nt[ at + q ][ 0 ] = tr[ q ][ 0 ]; C.nt[ at + q ][ 1 ] = tr[ q ][ 1 ]; C.nt[ at + q ][ 2 ] = tr[ q ][ 2 ];
+            const int t = tt[ q ];
+            const double Rx = C.vx[ k ], Ry = C.vy[ k ], Rz = C.vz[ k ], Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
+            double x, y, z;
+            solve3( C, tr[ q ][ 0 ], tr[ q ][ 1 ], P, x, y, z );
+            const double ex = Rx - Tx, ey = Ry - Ty, ez = Rz - Tz, e2 = ex * ex + ey * ey + ez * ez;
+            const double u = ( ( x - Tx ) * ex + ( y - Ty ) * ey + ( z - Tz ) * ez ) / e2;   // NaN if the solve failed
+            if ( ! ( u >= -1e-9 && u <= 1 + 1e-9 ) ) {
+                const double dT = nx * Tx + ny * Ty + nz * Tz - off, dR = nx * Rx + ny * Ry + nz * Rz - off;   // dR > tol >= dT
+                const double s = fmin( 1.0, fmax( 0.0, -dT / ( dR - dT ) ) );
+                x = Tx + s * ex; y = Ty + s * ey; z = Tz + s * ez;
+            }
+            C.area[ at + q ] = x; C.area[ VC + at + q ] = y; C.area[ 2 * VC + at + q ] = z;
+        }
         nnew += total;
     }
     __syncwarp();
@@ -209,14 +244,11 @@ __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double
         __syncwarp();
         kept_before += __popc( m );
     }
-    // the new vertices, re-solved from their three planes
+    // the new vertices, placed above
     for ( int j = lane; j < nnew; j += 32 ) {
-        int a = C.nt[ j ][ 0 ], b = C.nt[ j ][ 1 ], c = C.nt[ j ][ 2 ];
-        double x, y, z;
-        solve3( C, a, b, c, x, y, z );
         int d = nkeep + j;
-        C.va[ d ] = a; C.vb[ d ] = b; C.vc[ d ] = c;
-        C.vx[ d ] = x; C.vy[ d ] = y; C.vz[ d ] = z;
+        C.va[ d ] = C.nt[ j ][ 0 ]; C.vb[ d ] = C.nt[ j ][ 1 ]; C.vc[ d ] = C.nt[ j ][ 2 ];
+        C.vx[ d ] = C.area[ j ]; C.vy[ d ] = C.area[ VC + j ]; C.vz[ d ] = C.area[ 2 * VC + j ];
     }
     if ( lane == 0 ) C.nv = nkeep + nnew;
     __syncwarp();
@@ -277,7 +309,8 @@ __device__ void cut_by_ranges3( C3 &C, const ProbDev &P, int lane, int s, double
             off = 0.5 * ( ( wi - qw ) + ( qx * qx + qy * qy + qz * qz ) );
         }
         bool cuts = false;
-        for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] > off;
+        const double tol = valid ? tie_tol3( qx, qy, qz, off, C.L ) : 0.0;
+        for ( int k = 0; k < C.nv && valid; ++k ) cuts |= qx * C.vx[ k ] + qy * C.vy[ k ] + qz * C.vz[ k ] - off > tol;
         unsigned todo = __ballot_sync( FULL3, valid && cuts );
         while ( todo ) {
             int k = __ffs( todo ) - 1;
@@ -701,6 +734,24 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
     }
     __syncwarp();
     double mass = rho * warp_sum( vol );
+    if ( ! isfinite( mass ) ) {
+        // a clip that lost its topology: never a NaN in the outputs -- an error of the problem (its user seed), an empty
+        // cell, no facet (the reference's failure record, gpu/Cell2D.cuh:99-102, 1214-1231)
+        if ( lane == 0 ) {
+            record_error3( P, err, 7, prob, user, 0 );
+            const int row = user_order ? user : s;
+            if ( P.mass ) P.mass[ row ] = 0;
+            if ( facets ) P.nb[ row ] = 0;
+            if ( moments && P.first ) {
+                P.first[ 3 * ( size_t ) row ] = user_order ? px : 0.0;
+                P.first[ 3 * ( size_t ) row + 1 ] = user_order ? py : 0.0;
+                P.first[ 3 * ( size_t ) row + 2 ] = user_order ? pz : 0.0;
+            }
+            if ( moments && P.cost ) P.cost[ row ] = 0;
+        }
+        __syncwarp();
+        return true;
+    }
     // the facets: per plane, its triangles summed in vertex order (first the count, then the writes)
     if ( facets ) {
         const int row = user_order ? user : s;

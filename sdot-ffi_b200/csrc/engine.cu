@@ -247,6 +247,8 @@ void check_errors( Ctx &c, const char *where ) {
     if ( e.code == SDOT_ERR_CAPACITY )
         throw Error( SDOT_ERR_CAPACITY, std::string( where ) + ": a cell exceeded its capacity (seed " + std::to_string( e.seed ) + ")", e.seed,
                      e.needed );
+    if ( e.code == SDOT_ERR_TOPOLOGY )
+        throw Error( SDOT_ERR_TOPOLOGY, std::string( where ) + ": a cell's clip lost its topology (seed " + std::to_string( e.seed ) + ")", e.seed );
     throw Error( e.code, std::string( where ) + ": device error", e.seed );
 }
 
@@ -263,8 +265,9 @@ int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags ) {
     return count;
 }
 
+// a capacity or topology error of a solve's cell is its problem's (the per-slot flag read in `decide`), not the batch's
 static void clear_capacity_error( Ctx &c ) {
-    if ( c.herr->code != SDOT_ERR_CAPACITY ) return;
+    if ( c.herr->code != SDOT_ERR_CAPACITY && c.herr->code != SDOT_ERR_TOPOLOGY ) return;
     if ( std::getenv( "SDOT_TRACE" ) )
         std::fprintf( stderr, "sdot: capacity: problem %d of the launch, seed %d, needed %d\n", c.herr->prob, c.herr->seed, c.herr->needed );
     *c.herr = ErrRec{};

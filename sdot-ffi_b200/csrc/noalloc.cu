@@ -10,7 +10,16 @@
 //
 // The array's device address is looked up once per device, on the first call made with that device current
 // (cudaGetSymbolAddress; host code cannot take the address of a __device__ symbol).  That first call should
-// come before any stream capture on the device.
+// come before any stream capture on the device.  The address is kept for the life of the process, so the library
+// must not outlive a reset of a device it has used (cudaDeviceReset, or the primary context destroyed and made
+// again): after one, the next call would write through the stale address.
+//
+// The array is part of the library's device code: every device on which the library's module is loaded holds its
+// 16 MB until the process exits, whether or not this entry point is ever called.
+//
+// The kernels read the caller's matrix and vectors in place (nothing is staged through a copy), so every array
+// must be memory of the context's own device, or managed memory; memory of another GPU is refused before any
+// launch (SDOT_ERR_ARGS) -- without peer access a kernel reading it would fault.
 //
 // The kernels are those of `sdot_linear_solve`: only the rhs' mean differs, a deterministic block reduction on
 // the device here, a sequential host sum there (the solutions agree to rounding).
@@ -73,10 +82,12 @@ void na_status( sdot_status *st, int code, const std::string &msg, long long nee
     std::strncpy( st->message, msg.c_str(), sizeof( st->message ) - 1 );
 }
 
-bool on_device( const void *p ) {
+// memory that kernels on `device` may read in place: that device's own memory, or managed memory
+bool on_device( const void *p, int device ) {
     cudaPointerAttributes a;
     if ( cudaPointerGetAttributes( &a, p ) != cudaSuccess ) { cudaGetLastError(); return false; }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if ( a.type == cudaMemoryTypeManaged ) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 // int64 row offsets -> the int32 ones of the CG kernels
@@ -125,14 +136,15 @@ extern "C" int32_t sdot_linear_solve_noalloc( sdot_context ctx, int64_t n, const
         Ctx &c = ctx->c;
         CK( cudaSetDevice( c.device ) );
         for ( const void *p : { ( const void * ) row_ptr, ( const void * ) dia, ( const void * ) rhs, ( const void * ) x } )
-            if ( ! on_device( p ) ) throw Error( SDOT_ERR_ARGS, "sdot_linear_solve_noalloc: every array must be device memory" );
+            if ( ! on_device( p, c.device ) )
+                throw Error( SDOT_ERR_ARGS, "sdot_linear_solve_noalloc: every array must be device memory of the context's device" );
         char *w = work_area( c.device );
         int64_t nnz = 0;
         CK( cudaMemcpyAsync( &nnz, row_ptr + n, sizeof( nnz ), cudaMemcpyDeviceToHost, c.stream ) );
         CK( cudaStreamSynchronize( c.stream ) );
         if ( nnz < 0 || nnz >= ( 1ll << 31 ) ) throw Error( SDOT_ERR_ARGS, "sdot_linear_solve_noalloc: nnz must fit int32" );
-        if ( nnz > 0 && ( ! cols || ! vals || ! on_device( cols ) || ! on_device( vals ) ) )
-            throw Error( SDOT_ERR_ARGS, "sdot_linear_solve_noalloc: cols / vals must be device memory" );
+        if ( nnz > 0 && ( ! cols || ! vals || ! on_device( cols, c.device ) || ! on_device( vals, c.device ) ) )
+            throw Error( SDOT_ERR_ARGS, "sdot_linear_solve_noalloc: cols / vals must be device memory of the context's device" );
         const int nch = int( ( n + VCHUNK - 1 ) / VCHUNK );
         int *rp = reinterpret_cast<int *>( w + OFF_RP );
         double *vec[ NA_VECS ];

@@ -15,7 +15,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libsdot_b200.so")
 
-SDOT_OK, SDOT_ERR_ARGS, SDOT_ERR_CUDA, SDOT_ERR_NO_MEMORY, SDOT_ERR_CAPACITY, SDOT_ERR_UNSUPPORTED, SDOT_ERR_NOT_CONVERGED = range(7)
+SDOT_OK, SDOT_ERR_ARGS, SDOT_ERR_CUDA, SDOT_ERR_NO_MEMORY, SDOT_ERR_CAPACITY, SDOT_ERR_UNSUPPORTED, SDOT_ERR_NOT_CONVERGED, SDOT_ERR_TOPOLOGY = range(8)
 SDOT_HOST, SDOT_DEVICE = 0, 1
 DENSITY_UNIFORM, DENSITY_IMAGE, DENSITY_GAUSSIANS = 0, 1, 2
 
@@ -132,6 +132,8 @@ def raise_for(code, st, what="sdot"):
     msg = f"{what}: {st.message.decode(errors='replace')}"
     if code == SDOT_ERR_CAPACITY:
         raise KernelFailure(msg + f" -- seed {st.id} needs {st.needed}", seed=int(st.id), needed=int(st.needed))
+    if code == SDOT_ERR_TOPOLOGY:
+        raise KernelFailure(msg + f" -- seed {st.id}", seed=int(st.id), needed=0)
     if code == SDOT_ERR_NO_MEMORY:
         raise MemoryError(msg)
     if code == SDOT_ERR_UNSUPPORTED:

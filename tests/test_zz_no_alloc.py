@@ -4,7 +4,9 @@
 The Laplacian is a weighted 250 x 200 grid graph (50,000 rows, random positive couplings).  Two calls in a row
 must match the allocating entry point within |x - x_ref| <= 1e-9 max|x_ref| (the rhs mean is summed in a
 different order), use the same CG iteration counts (+-1), leave the device's free memory unchanged, and a size past
-SDOT_NOALLOC_MAX_ROWS is refused with SDOT_ERR_CAPACITY."""
+SDOT_NOALLOC_MAX_ROWS is refused with SDOT_ERR_CAPACITY.  Also: a right-hand side with a nonzero mean on a grid whose
+row count is not a multiple of the CG's 1024-row chunks (the last chunk partial), a system with no coupling at all
+(cols and vals NULL), and host memory refused before any launch."""
 import ctypes
 
 import numpy as np
@@ -40,6 +42,33 @@ def _grid_laplacian(nx, ny, seed):
 
 def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _both(n, rp, cols, vals, dia, rhs, calls=2):
+    """the allocating solve once, then the no-alloc one `calls` times in a row: (reference, [solutions], iterations)"""
+    L = _lib.load()
+    ctx = _lib.context()
+    k = rhs.shape[0]
+    d_rp, d_dia, d_rhs = _dev(rp), _dev(dia), _dev(rhs)
+    d_cols = _dev(cols) if cols is not None else None
+    d_vals = _dev(vals) if vals is not None else None
+    pc = d_cols.data_ptr() if d_cols is not None else None
+    pv = d_vals.data_ptr() if d_vals is not None else None
+    x_ref = torch.empty(k, n, dtype=torch.float64, device="cuda")
+    its_ref = (ctypes.c_int32 * k)()
+    st = _lib.Status()
+    code = L.sdot_linear_solve(ctx, n, d_rp.data_ptr(), pc, pv, d_dia.data_ptr(), k, d_rhs.data_ptr(), x_ref.data_ptr(), 0, 1e-10, 100000,
+                               _lib.SDOT_DEVICE, its_ref, ctypes.byref(st))
+    assert code == 0, st.message
+    got = []
+    for _ in range(calls):
+        x = torch.full((k, n), np.nan, dtype=torch.float64, device="cuda")
+        its = (ctypes.c_int32 * k)()
+        code = L.sdot_linear_solve_noalloc(ctx, n, d_rp.data_ptr(), pc, pv, d_dia.data_ptr(), k, d_rhs.data_ptr(), x.data_ptr(), 1e-10,
+                                           100000, its, ctypes.byref(st))
+        assert code == 0, st.message
+        got.append((x.cpu().numpy(), list(its)))
+    return x_ref.cpu().numpy(), got, list(its_ref)
 
 
 def test_the_static_work_area_solve_matches_the_allocating_one():
@@ -99,3 +128,47 @@ def test_a_size_past_the_static_work_area_is_refused():
     code = L.sdot_linear_solve_noalloc(ctx, n, rp.data_ptr(), None, None, dia.data_ptr(), 1, rhs.data_ptr(), x.data_ptr(), 1e-10, 100,
                                        its, ctypes.byref(st))
     assert code == 4 and st.needed == n and b"past the static work area" in st.message
+
+
+def test_a_nonzero_mean_rhs_on_a_partial_last_chunk():
+    n, rp, cols, vals, dia = _grid_laplacian(123, 77, 8)          # 9,471 rows: the tenth 1024-row chunk is partial
+    assert n % 1024 != 0
+    rng = np.random.default_rng(9)
+    rhs = rng.standard_normal((2, n)) + np.array([[3.0], [-0.5]])  # nonzero means: both solves project them out
+    ref, got, its_ref = _both(n, rp, cols, vals, dia, rhs)
+    scale = np.abs(ref).max()
+    assert np.isfinite(ref).all() and scale > 0
+    for x, its in got:
+        assert np.isfinite(x).all()
+        assert np.abs(x - ref).max() <= 1e-9 * scale
+        assert all(abs(a - b) <= 1 for a, b in zip(its, its_ref))
+
+
+def test_a_system_without_couplings():
+    n = 3000
+    rp = np.zeros(n + 1, np.int64)
+    dia = np.random.default_rng(10).uniform(0.5, 2.0, size=n)
+    rhs = np.random.default_rng(11).standard_normal((1, n))
+    ref, got, its_ref = _both(n, rp, None, None, dia, rhs)
+    scale = max(np.abs(ref).max(), 1e-300)
+    for x, its in got:
+        assert np.isfinite(x).all()
+        assert np.abs(x - ref).max() <= 1e-9 * scale
+        assert list(its) == list(its_ref) or all(abs(a - b) <= 1 for a, b in zip(its, its_ref))
+
+
+def test_host_memory_is_refused_before_any_launch():
+    L = _lib.load()
+    ctx = _lib.context()
+    n = 1000
+    rp = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    dia = torch.ones(n, dtype=torch.float64, device="cuda")
+    host_rhs = np.zeros(n)                                          # pageable host memory
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    its = (ctypes.c_int32 * 1)()
+    st = _lib.Status()
+    launches = _lib.kernel_launches()
+    code = L.sdot_linear_solve_noalloc(ctx, n, rp.data_ptr(), None, None, dia.data_ptr(), 1, host_rhs.ctypes.data, x.data_ptr(), 1e-10,
+                                       100, its, ctypes.byref(st))
+    assert code == 1 and b"device memory of the context's device" in st.message
+    assert _lib.kernel_launches() == launches
