@@ -217,11 +217,12 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemcpyAsync( ( char * ) dd.p + o2, ch.data(), ch.size() * sizeof( Chunk ), cudaMemcpyHostToDevice, c.stream ) );
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
+        const Split3 *sp = dim == 3 && P.dkind == D_GAUSS ? split3_for( c, int( ch.size() ), n ) : nullptr;
         c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, double( n ) );
         launch_wpyr( L, dd.as<ProbDev>(), 1 );
         if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
-        else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
-        c.timer.end( c.stream );
+        else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf, sp );
+        c.timer.end( c.stream, sp ? 2 : 1 );
         run_big_cells( c, dd.as<ProbDev>(), flags );
         CK( cudaGetLastError() );
         CK( cudaMemcpyAsync( c.herr, c.derr, sizeof( ErrRec ), cudaMemcpyDeviceToHost, c.stream ) );
@@ -364,7 +365,9 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         CK( cudaMemsetAsync( &c.dovf->count, 0, sizeof( int ), c.stream ) );
         launch_wpyr( L, ( ProbDev * ) base, 1 );
         if ( dim == 2 ) launch_cells2d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
-        else launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf );
+        else
+            launch_cells3d( L, ( ProbDev * ) base, ( Chunk * ) ( base + o1 ), int( ch.size() ), F_FACETS | F_USER_ORDER, c.derr, c.dovf,
+                            P.dkind == D_GAUSS ? split3_for( c, int( ch.size() ), n ) : nullptr );
         run_big_cells( c, ( ProbDev * ) base, F_FACETS | F_USER_ORDER );
         launch_lap_count( L, ( VecDev * ) ( base + o2 ), ( Chunk * ) ( base + o3 ), int( vch.size() ) );
         launch_lap_scan( L, ( VecDev * ) ( base + o2 ), 1 );

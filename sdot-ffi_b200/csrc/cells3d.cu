@@ -426,14 +426,20 @@ __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double 
 //    winding angle of the face about the foot (2 pi or 0), R(theta) the distance from the foot to the face's edge;
 //  * moments from (y - c) rho = -s^2 grad rho and |y - c|^2 rho = s^2 (3 rho - div((y - c) rho)):
 //        int (y - c) rho = -s^2 sum_f n_f int_face rho,   int |y - c|^2 rho = s^2 ( 3 M - sum_f h_f int_face rho ).
-// The angle integrals run per edge in phi, the angle from the foot's perpendicular on the edge line (R = d / cos phi),
-// in Gauss-Legendre pieces over which R changes by at most s/2 and that stay within half their distance of +-pi/2.
+// The angle integrals run per edge, in u with s = d sinh u along the edge's line (s measured from the foot's
+// perpendicular on the line, d the foot's distance to it): R = d cosh u and dtheta = du / cosh u, so every kernel is
+// smooth in u (1 / cosh u has its only poles at +-i pi/2).  Gauss-Legendre pieces of 8 points are uniform in
+// V(u) = int max( 1 / G3_WU, d |sinh u| / ( G3_FR s ) ) du: at most G3_WU wide in u, and R changes by at most G3_FR s over
+// each, the gaussian's own scale.  Against 30-digit quadrature on the edges of real power cells (1e3 to 3e4 seeds in
+// the unit cube, 4 gaussians of sigma in [0.05, 0.15]) the rule is within 2e-14 and takes 1.2 pieces per edge on
+// average, 12 at most.
+// The work is spread over the warp as (gaussian, entry) and (gaussian, face) items, one per lane at a time.
 __constant__ double c_g3x[ 8 ] = { -0.9602898564975363, -0.7966664774136267, -0.5255324099163290, -0.1834346424956498,
                                     0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363 };
 __constant__ double c_g3w[ 8 ] = { 0.1012285362903763, 0.2223810344533745, 0.3137066458778873, 0.3626837833783620,
                                     0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763 };
-constexpr double HALF_PI = 1.5707963267948966;
-constexpr int G3_MAX_PIECES = 128;
+constexpr double G3_WU = 0.7, G3_FR = 0.5;
+constexpr int G3_MAX_PIECES = 64;
 
 // the signed angle of the edge K -> T about F, positive counterclockwise about -n (the cell's edges run clockwise
 // about the outward normal n, so a foot inside the face gets +2 pi in total)
@@ -444,49 +450,56 @@ __device__ __forceinline__ double edge_angle3( double Fx, double Fy, double Fz, 
     return atan2( o, ax * bx + ay * by + az * bz );
 }
 
-// A = int Ht( sqrt( h^2 + R^2 ) ) / m dtheta and B = int exp( -R^2 / 2 s^2 ) dtheta along the edge K -> T (signed as above)
-__device__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty, double Tz, double nx,
-                             double ny, double nz, double h, double sg, double &A, double &B ) {
+// A = int erfc( r / s sqrt2 ) / r dtheta and B = int exp( -R^2 / 2 s^2 ) dtheta along the edge K -> T of a face (F the
+// foot of the centre on the face's plane, n its unit normal, h the centre's distance to the plane, r^2 = h^2 + R^2),
+// signed as `edge_angle3`.  erfc( k r ) = exp( -k^2 h^2 ) exp( -k^2 R^2 ) erfcx( k r ): one exponential serves both
+__device__ __noinline__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty, double Tz,
+                                          double nx, double ny, double nz, double h, double sg, double &A, double &B ) {
     A = B = 0;
-    double ax = Kx - Fx, ay = Ky - Fy, az = Kz - Fz, ex = Tx - Kx, ey = Ty - Ky, ez = Tz - Kz;
-    double L = sqrt( ex * ex + ey * ey + ez * ez );
+    const double ax = Kx - Fx, ay = Ky - Fy, az = Kz - Fz, ex = Tx - Kx, ey = Ty - Ky, ez = Tz - Kz;
+    const double L = sqrt( ex * ex + ey * ey + ez * ez );
     if ( ! ( L > 0 ) ) return;
-    double ux = ex / L, uy = ey / L, uz = ez / L;
-    double s0 = ax * ux + ay * uy + az * uz, s1 = s0 + L;
-    double qx = ax - s0 * ux, qy = ay - s0 * uy, qz = az - s0 * uz;
-    double d = sqrt( qx * qx + qy * qy + qz * qz );
+    const double ux = ex / L, uy = ey / L, uz = ez / L;
+    const double s0 = ax * ux + ay * uy + az * uz, s1 = s0 + L;
+    const double qx = ax - s0 * ux, qy = ay - s0 * uy, qz = az - s0 * uz;
+    const double d = sqrt( qx * qx + qy * qy + qz * qz );
     if ( ! ( d > 0 ) ) return;
-    double bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
-    double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
+    const double bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
+    const double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
     const double sgn = o >= 0 ? 1.0 : -1.0;
-    const double p0 = atan2( s0, d ), p1 = atan2( s1, d );
-    const double inv2s2 = 0.5 / ( sg * sg ), kr = 0.7071067811865476 / sg, h2 = h * h;
-    double phi = p0;
-    for ( int piece = 0; piece < G3_MAX_PIECES && phi < p1; ++piece ) {
-        double R = d / cos( phi ), nxt;
-        if ( phi < 0 ) {
-            nxt = phi + 0.5 * ( HALF_PI + phi );
-            double Rn = fmax( d, R - 0.5 * sg );
-            nxt = fmin( nxt, -acos( fmin( 1.0, d / Rn ) ) );
-            nxt = fmin( nxt, 0.0 );
-            if ( nxt <= phi ) nxt = 0.0;
-        } else {
-            nxt = ( phi + 0.5 * HALF_PI ) / 1.5;
-            nxt = fmin( nxt, acos( fmin( 1.0, d / ( R + 0.5 * sg ) ) ) );
-        }
-        nxt = fmin( nxt, p1 );
-        if ( piece == G3_MAX_PIECES - 1 ) nxt = p1;
-        const double hw = 0.5 * ( nxt - phi ), mid = 0.5 * ( nxt + phi );
+    // (past |s / d| = 1e17, u = 40.4, the kernel 1 / cosh u is under 1e-17)
+    const double u0 = asinh( fmax( -1e17, fmin( 1e17, s0 / d ) ) ), u1 = asinh( fmax( -1e17, fmin( 1e17, s1 / d ) ) );
+    const double fs = G3_FR * sg, c = fmin( 1e17, fs / ( G3_WU * d ) );      // sinh of the u where the two bounds meet
+    const double us = asinh( c ), chs = sqrt( 1 + c * c ), vs = us / G3_WU, kd = d / fs;
+    auto V = [&]( double u ) {
+        const double a = fabs( u );
+        return copysign( a <= us ? a / G3_WU : vs + kd * ( cosh( a ) - chs ), u );
+    };
+    auto Vinv = [&]( double v ) {
+        const double a = fabs( v );
+        return copysign( a <= vs ? a * G3_WU : acosh( chs + ( a - vs ) / kd ), v );
+    };
+    const double v0 = V( u0 ), v1 = V( u1 );
+    const int np = max( 1, min( G3_MAX_PIECES, int( ceil( v1 - v0 ) ) ) );
+    const double dv = ( v1 - v0 ) / np, kr = 0.7071067811865476 / sg, k2 = kr * kr, h2 = h * h;
+    const double eh = exp( -k2 * h2 );
+    double ua = u0;
+    for ( int j = 0; j < np; ++j ) {
+        const double ub = j + 1 == np ? u1 : Vinv( v0 + ( j + 1 ) * dv );
+        const double hw = 0.5 * ( ub - ua ), mid = 0.5 * ( ub + ua );
+#pragma unroll 2
         for ( int q = 0; q < 8; ++q ) {
-            double f = mid + hw * c_g3x[ q ], w = hw * c_g3w[ q ];
-            double Rq = d / cos( f ), R2 = Rq * Rq;
+            const double uq = mid + hw * c_g3x[ q ], w = hw * c_g3w[ q ];
+            const double eu = exp( uq ), ich = 2 / ( eu + 1 / eu );       // 1 / cosh u
+            const double R = d / ich, R2 = R * R;
+            const double gw = w * ich * exp( -k2 * R2 );
+            B += gw;
             if ( h != 0 ) {
-                double r = sqrt( h2 + R2 );
-                A += w * erfc( r * kr ) / r;
+                const double r = sqrt( h2 + R2 );
+                A += gw * eh * erfcx( kr * r ) / r;
             }
-            B += w * exp( -R2 * inv2s2 );
         }
-        phi = nxt;
+        ua = ub;
     }
     A *= sgn;
     B *= sgn;
@@ -494,7 +507,7 @@ __device__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double 
 
 // the gaussian sums over the clipped cell: lane parts of the mass, of the first moment about the seed and of
 // int |y|^2 rho (seed frame); C.area receives each (vertex, edge) entry's part of its face integral and C.fmp each
-// face's winding-angle part (both summed over the gaussians)
+// face's winding-angle part (both summed over the gaussians, in gaussian order)
 template<class C3>
 __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane, double px, double py, double pz, double &M, double &Fx,
                                                 double &Fy, double &Fz, double &S2 ) {
@@ -547,61 +560,91 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
     };
     double bmax = 0;
     for ( int g = 0; g < ng; ++g ) bmax = fmax( bmax, bound( g ) );
-    for ( int g = 0; g < ng; ++g ) {
-        if ( ng > 1 && bound( g ) < 1e-20 * bmax ) continue;          // (warp uniform: the bound is a warp max)
-        const double *G = P.dval + g * 5;
-        const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
-        const double s2g = sg * sg, K = mg / ( 15.749609945722419 * s2g * sg ), kr = 0.7071067811865476 / sg;   // (2 pi)^{3/2}
-        double Mg = 0, Gx = 0, Gy = 0, Gz = 0, Sg = 0;
-        for ( int k = lane; k < nv; k += 32 ) {
-            const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
-            const double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
-            for ( int q = 0; q < 3; ++q ) {
-                const int t = C.tw[ 3 * k + q ];
-                if ( t == C3::NONE ) continue;
-                const int f = e[ q ];
+    // the parts of one item: dM of the mass, and the face integral b of the face f (unit normal n); with the gaussian's
+    // centre c (seed frame) and variance s2 they give the moments' parts (moments about c, moved to the seed)
+    auto add = [&]( double dM, double b, double h, double nhx, double nhy, double nhz, double cx, double cy, double cz, double s2g ) {
+        const double gx = -s2g * nhx * b, gy = -s2g * nhy * b, gz = -s2g * nhz * b;
+        M += dM;
+        Fx += gx + cx * dM; Fy += gy + cy * dM; Fz += gz + cz * dM;
+        S2 += s2g * ( 3 * dM - h * b ) + 2 * ( cx * gx + cy * gy + cz * gz ) + ( cx * cx + cy * cy + cz * cz ) * dM;
+    };
+    // items are (gaussian of the group's selection, entry or face), lane-consecutive; with at least 32 entries (faces)
+    // per gaussian, the 32 items of one round hold distinct entries (faces), so their sums into `area` (`fmp`) never
+    // meet, and each entry's (face's) sum runs in gaussian order
+    const int NE = 3 * nv, NEp = NE > 32 ? NE : 32, NPp = np > 32 ? np : 32;
+    for ( int g0 = 0; g0 < ng; g0 += 32 ) {
+        const int gn = min( 32, ng - g0 );
+        unsigned sel = 0;
+        for ( int j = 0; j < gn; ++j )
+            if ( ng == 1 || ! ( bound( g0 + j ) < 1e-20 * bmax ) ) sel |= 1u << j;      // (warp uniform: the bound is a warp max)
+        const int ns = __popc( sel );
+        auto nth = [&]( int i ) {          // the i-th selected gaussian
+            unsigned m = sel;
+            for ( int k = 0; k < i; ++k ) m &= m - 1;
+            return g0 + __ffs( m ) - 1;
+        };
+        // the edge integrals of every (gaussian, entry)
+        for ( int base = 0; base < ns * NEp; base += 32 ) {
+            const int idx = base + lane, gi = idx / NEp, e = idx - gi * NEp;
+            if ( gi < ns && e < NE && C.tw[ e ] != C3::NONE ) {
+                const int g = nth( gi ), k = e / 3, q = e - 3 * k, t = C.tw[ e ];
+                const int f = q == 0 ? C.va[ k ] : ( q == 1 ? C.vb[ k ] : C.vc[ k ] );
+                const double *G = P.dval + g * 5;
+                const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
+                const double s2g = sg * sg, KG = mg / ( 15.749609945722419 * s2g * sg );          // (2 pi)^{3/2}
                 const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] );
                 const double nhx = C.nx[ f ] / nn, nhy = C.ny[ f ] / nn, nhz = C.nz[ f ] / nn;
                 const double h = ( C.no[ f ] - ( C.nx[ f ] * cx + C.ny[ f ] * cy + C.nz[ f ] * cz ) ) / nn;
                 double A, B;
-                edge_gauss3( cx + h * nhx, cy + h * nhy, cz + h * nhz, Kx, Ky, Kz, C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz, h, sg, A, B );
-                Mg += h * INV4PI * mg * A;
-                const double b = -K * exp( -h * h * 0.5 / s2g ) * s2g * B;
-                C.area[ 3 * k + q ] += b;
-                Gx -= s2g * nhx * b; Gy -= s2g * nhy * b; Gz -= s2g * nhz * b;
-                Sg += h * b;
+                edge_gauss3( cx + h * nhx, cy + h * nhy, cz + h * nhz, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx,
+                             nhy, nhz, h, sg, A, B );
+                const double b = -KG * exp( -h * h * 0.5 / s2g ) * s2g * B;
+                C.area[ e ] += b;
+                add( h * INV4PI * mg * A, b, h, nhx, nhy, nhz, cx, cy, cz, s2g );
             }
+            __syncwarp();
         }
-        // per face: the winding angle of the face about the foot of c, and whether c is on the inner side
-        bool ok = true;
-        for ( int p = lane; p < np; p += 32 ) {
-            const double nn = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
-            const double nhx = C.nx[ p ] / nn, nhy = C.ny[ p ] / nn, nhz = C.nz[ p ] / nn;
-            const double h = ( C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) ) / nn;
-            ok = ok && h >= 0;
-            const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
-            double th = 0;
-            for ( int k = C.remap[ p ]; k != C3::NONE; ) {
-                const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
-                const int t = C.tw[ 3 * k + q ];
-                th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
-                k = C.nt[ k ][ q ];
+        // per (gaussian, face): the winding angle of the face about the foot of c, its part of the face integral and of
+        // the flux of the erfc field's constant part
+        for ( int base = 0; base < ns * NPp; base += 32 ) {
+            const int idx = base + lane, gi = idx / NPp, p = idx - gi * NPp;
+            if ( gi < ns && p < np ) {
+                const int g = nth( gi );
+                const double *G = P.dval + g * 5;
+                const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
+                const double s2g = sg * sg, KG = mg / ( 15.749609945722419 * s2g * sg ), kr = 0.7071067811865476 / sg;
+                const double nn = sqrt( C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ] );
+                const double nhx = C.nx[ p ] / nn, nhy = C.ny[ p ] / nn, nhz = C.nz[ p ] / nn;
+                const double h = ( C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) ) / nn;
+                const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
+                double th = 0;
+                for ( int k = C.remap[ p ]; k != C3::NONE; ) {
+                    const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
+                    const int t = C.tw[ 3 * k + q ];
+                    th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
+                    k = C.nt[ k ][ q ];
+                }
+                const double kk = rint( th / TWO_PI );
+                const double Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
+                if ( Th != 0 ) {
+                    const double I = KG * exp( -h * h * 0.5 / s2g ) * s2g * Th;
+                    C.fmp[ p ] += I;
+                    // the flux of the erfc field's constant part; at h = 0 its limit from the inner side
+                    const double dM = h != 0 ? -h * INV4PI * mg * erfc( fabs( h ) * kr ) / fabs( h ) * Th : -INV4PI * mg * Th;
+                    add( dM, I, h, nhx, nhy, nhz, cx, cy, cz, s2g );
+                }
             }
-            const double kk = rint( th / TWO_PI );
-            const double Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
-            if ( Th != 0 ) {
-                const double I = K * exp( -h * h * 0.5 / s2g ) * s2g * Th;
-                C.fmp[ p ] += I;
-                // the flux of the erfc field's constant part; at h = 0 its limit from the inner side
-                Mg -= h != 0 ? h * INV4PI * mg * erfc( fabs( h ) * kr ) / fabs( h ) * Th : INV4PI * mg * Th;
-                Gx -= s2g * nhx * I; Gy -= s2g * nhy * I; Gz -= s2g * nhz * I;
-                Sg += h * I;
-            }
+            __syncwarp();
         }
-        if ( __all_sync( FULL3, ok ) && lane == 0 ) Mg += mg;          // the point mass taken out of the field
-        M += Mg;
-        Fx += Gx + cx * Mg; Fy += Gy + cy * Mg; Fz += Gz + cz * Mg;
-        S2 += s2g * ( 3 * Mg - Sg ) + 2 * ( cx * Gx + cy * Gy + cz * Gz ) + ( cx * cx + cy * cy + cz * cz ) * Mg;
+        // the point mass taken out of the field, for a centre on the inner side of every face
+        for ( int gi = 0; gi < ns; ++gi ) {
+            const int g = nth( gi );
+            const double *G = P.dval + g * 5;
+            const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz;
+            bool ok = true;
+            for ( int p = lane; p < np; p += 32 ) ok = ok && C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) >= 0;
+            if ( __all_sync( FULL3, ok ) && lane == 0 ) add( G[ 4 ], 0.0, 0.0, 0.0, 0.0, 0.0, cx, cy, cz, G[ 3 ] * G[ 3 ] );
+        }
         __syncwarp();
     }
 }
@@ -632,14 +675,11 @@ __device__ __forceinline__ void queue3( const ProbDev &P, ErrRec *err, OvfList *
     __syncwarp();
 }
 
-// THE CELL of seed s (rank) of problem `prob`: clip, integrate, write.  A cell past the vertex / plane capacities of
-// this pass is queued on `ovf` for the next pass (main -> big -> giant; NULL: an error of its problem) and the call
-// returns false (nothing written).  The main kernel (`big` false) also queues a cell with more facets than the table's
-// row; the other passes write those to the overflow store.  `rep` (lane 0, may be NULL) accumulates the Newton report
+// THE CELL of seed s (rank) of problem `prob`, first half: the clip.  A cell past the vertex / plane capacities of this
+// pass is queued on `ovf` for the next pass (main -> big -> giant; NULL: an error of its problem) and the call returns
+// false (nothing written); true: the clipped cell is in C (possibly empty)
 template<class C3>
-__device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, int2 *stk, double wmax,
-                       double *rep, bool big ) {
-    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+__device__ __noinline__ bool clip3( C3 &C, const ProbDev &P, int prob, int s, int lane, ErrRec *err, OvfList *ovf, int2 *stk, double wmax, bool big ) {
     const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
     const double wi = P.w ? P.w[ s ] : 0.0;
     init_box3( C, lane, P.lo, P.hi, px, py, pz );
@@ -694,6 +734,17 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
         if ( lane == 0 ) C.nv = 0;
         __syncwarp();
     }
+    return true;
+}
+
+// THE CELL, second half: integrate the clipped cell in C, write.  The main kernel (`big` false) queues a cell with more
+// facets than the table's row (and returns false, nothing written); the other passes write those to the overflow
+// store.  `rep` (lane 0, may be NULL) accumulates the Newton report
+template<class C3>
+__device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, double *rep, bool big ) {
+    const bool moments = flags & F_MOMENTS, facets = flags & F_FACETS, user_order = flags & F_USER_ORDER;
+    const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
+    const int user = P.user[ s ];
     // ---- integration: signed tetrahedra ( 0, c_f, K, T ) -- every (vertex, directed edge) once; gaussians by
     // their face integrals (the sums below are then already density-weighted)
     double vol = 0, fx = 0, fy = 0, fz = 0, s2 = 0;
@@ -886,8 +937,76 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
     return true;
 }
 
+// THE CELL, both halves
+template<class C3>
+__device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, int2 *stk, double wmax,
+                       double *rep, bool big ) {
+    if ( ! clip3( C, P, prob, s, lane, err, ovf, stk, wmax, big ) ) return false;
+    return finish3( C, P, prob, s, lane, flags, err, ovf, rep, big );
+}
+
+// ---- the two passes of the gaussian cells -------------------------------------------------------------------------------
+// Under a sum of gaussians the integration is most of a cell's work, and one kernel doing both halves keeps the warps of an
+// SM in different code (the clip's walk, the quadrature, their math functions) that the instruction cache cannot hold at
+// once: the warps then mostly wait for instructions.  So the main kernel runs twice: pass 1 clips every gaussian cell and
+// stores it (its used planes and its vertices) in `Split3::mem`; pass 2 loads each one and integrates it.  A cell that
+// finds no room in `mem` is done whole by pass 2.  The record of a cell, 16-byte aligned: int nv, np (16 bytes), then
+// doubles vx, vy, vz [nv] and nx, ny, nz, no [np], ints pid [np], ushorts va, vb, vc [nv].
+__device__ __forceinline__ size_t rec3_bytes( int nv, int np ) {
+    return ( 16 + size_t( 8 ) * ( 3 * nv + 4 * np ) + size_t( 4 ) * np + size_t( 6 ) * nv + 15 ) & ~size_t( 15 );
+}
+
+template<class C3>
+__device__ long long store3( C3 &C, const Split3 &sp, int lane ) {
+    // only the planes a vertex uses
+    compact_planes( C, lane );
+    const int nv = C.nv, np = C.np;
+    const size_t bytes = rec3_bytes( nv, np );
+    unsigned long long at = 0;
+    if ( lane == 0 ) at = atomicAdd( sp.used, ( unsigned long long ) bytes );
+    at = __shfl_sync( FULL3, at, 0 );
+    if ( at + bytes > sp.cap ) return -1;
+    char *r = sp.mem + at;
+    if ( lane == 0 ) { reinterpret_cast<int *>( r )[ 0 ] = nv; reinterpret_cast<int *>( r )[ 1 ] = np; }
+    double *v = reinterpret_cast<double *>( r + 16 ), *pl = v + 3 * nv;
+    int *pid = reinterpret_cast<int *>( pl + 4 * np );
+    unsigned short *ids = reinterpret_cast<unsigned short *>( pid + np );
+    for ( int k = lane; k < nv; k += 32 ) {
+        v[ k ] = C.vx[ k ]; v[ nv + k ] = C.vy[ k ]; v[ 2 * nv + k ] = C.vz[ k ];
+        ids[ k ] = C.va[ k ]; ids[ nv + k ] = C.vb[ k ]; ids[ 2 * nv + k ] = C.vc[ k ];
+    }
+    for ( int p = lane; p < np; p += 32 ) {
+        pl[ p ] = C.nx[ p ]; pl[ np + p ] = C.ny[ p ]; pl[ 2 * np + p ] = C.nz[ p ]; pl[ 3 * np + p ] = C.no[ p ];
+        pid[ p ] = C.pid[ p ];
+    }
+    return ( long long ) at;
+}
+
+template<class C3>
+__device__ void load3( C3 &C, const Split3 &sp, long long at, int lane ) {
+    const char *r = sp.mem + at;
+    const int nv = reinterpret_cast<const int *>( r )[ 0 ], np = reinterpret_cast<const int *>( r )[ 1 ];
+    const double *v = reinterpret_cast<const double *>( r + 16 ), *pl = v + 3 * nv;
+    const int *pid = reinterpret_cast<const int *>( pl + 4 * np );
+    const unsigned short *ids = reinterpret_cast<const unsigned short *>( pid + np );
+    typedef typename C3::I I;
+    for ( int k = lane; k < nv; k += 32 ) {
+        C.vx[ k ] = v[ k ]; C.vy[ k ] = v[ nv + k ]; C.vz[ k ] = v[ 2 * nv + k ];
+        C.va[ k ] = I( ids[ k ] ); C.vb[ k ] = I( ids[ nv + k ] ); C.vc[ k ] = I( ids[ 2 * nv + k ] );
+    }
+    for ( int p = lane; p < np; p += 32 ) {
+        C.nx[ p ] = pl[ p ]; C.ny[ p ] = pl[ np + p ]; C.nz[ p ] = pl[ 2 * np + p ]; C.no[ p ] = pl[ 3 * np + p ];
+        C.pid[ p ] = pid[ p ];
+    }
+    if ( lane == 0 ) { C.nv = nv; C.np = np; }
+    __syncwarp();
+}
+
+// the main kernel: one warp per cell, W3 cells of a chunk at a time.  mode 0: every cell whole.  mode 1 (pass 1) and
+// mode 2 (pass 2): the cells of a gaussian problem are clipped and stored by pass 1 and integrated by pass 2 (the report
+// too); the other problems are done whole by pass 1 and skipped by pass 2
 __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
-                                                        unsigned flags, ErrRec *err, OvfList *ovf ) {
+                                                        unsigned flags, ErrRec *err, OvfList *ovf, int mode, Split3 sp ) {
     extern __shared__ char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Cell3 &C = reinterpret_cast<Cell3 *>( smem )[ warp ];
@@ -897,35 +1016,57 @@ __global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__rest
     for ( int cidx = blockIdx.x; cidx < nchunks; cidx += gridDim.x ) {
         const Chunk ch = chunks[ cidx ];
         const ProbDev &P = probs[ ch.prob ];
+        const bool two = mode != 0 && P.dkind == D_GAUSS;       // block-uniform: one problem per chunk
+        if ( mode == 2 && ! two ) continue;
+        const bool report = ( flags & F_REPORT ) && ! ( mode == 1 && two );
         double rep[ NB_REPORT ];
         rep[ R_WORST ] = 0; rep[ R_WORST_REL ] = 0; rep[ R_AMIN ] = 1e300; rep[ R_ASUM ] = 0; rep[ R_LIN2 ] = 0; rep[ R_GCOUNT ] = 0;
         rep[ R_GMEAN ] = 0; rep[ R_GM2 ] = 0; rep[ R_SU ] = 0; rep[ R_SUG ] = 0; rep[ R_NUSUM ] = 0; rep[ R_NEMPTY ] = 0;
+        double *rp = report ? rep : nullptr;
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
-        for ( int s = ch.begin + warp; s < ch.end; s += W3 )
-            cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, ( flags & F_REPORT ) ? rep : nullptr, false );
-                if ( flags & F_REPORT ) {
-                    // the chunk's report, then the last block of the problem folds them (fixed tree)
-                    if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
-                    __syncthreads();
-                    if ( threadIdx.x == 0 ) {
-                        Rep r;
-                        for ( int k = 0; k < NB_REPORT; ++k ) r.v[ k ] = sh_rep[ 0 ][ k ];
-                        for ( int w = 1; w < W3; ++w ) r.combine( sh_rep[ w ] );
-                        double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
-                        for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r.v[ k ];
-                        __threadfence();
-                        unsigned prev = atomicAdd( P.counter, 1u );
-                        sh_last = prev == unsigned( P.nchunk - 1 );
-                    }
-                    __syncthreads();
-                    if ( sh_last ) {
-                        __threadfence();
-                        fold_reports_block( P );
-                    }
-                    __syncthreads();
-                }
+        for ( int s = ch.begin + warp; s < ch.end; s += W3 ) {
+            if ( ! two ) {
+                cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
+                continue;
+            }
+            long long *slot = sp.slot + ( size_t ) cidx * CHUNK + ( s - ch.begin );
+            if ( mode == 1 ) {
+                long long at = -2;                  // queued for the big-cell pass
+                if ( clip3( C, P, ch.prob, s, lane, err, ovf, sh_stk[ warp ], wmax, false ) ) at = store3( C, sp, lane );
+                if ( lane == 0 ) *slot = at;
+                __syncwarp();
+            } else {
+                const long long at = *slot;
+                if ( at >= 0 ) {
+                    load3( C, sp, at, lane );
+                    finish3( C, P, ch.prob, s, lane, flags, err, ovf, rp, false );
+                } else if ( at == -1 )              // no room in pass 1: the whole cell here
+                    cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
             }
         }
+        if ( report ) {
+            // the chunk's report, then the last block of the problem folds them (fixed tree)
+            if ( lane == 0 ) for ( int k = 0; k < NB_REPORT; ++k ) sh_rep[ warp ][ k ] = rep[ k ];
+            __syncthreads();
+            if ( threadIdx.x == 0 ) {
+                Rep r;
+                for ( int k = 0; k < NB_REPORT; ++k ) r.v[ k ] = sh_rep[ 0 ][ k ];
+                for ( int w = 1; w < W3; ++w ) r.combine( sh_rep[ w ] );
+                double *dst = P.partials + ( size_t ) ch.index * NB_REPORT;
+                for ( int k = 0; k < NB_REPORT; ++k ) dst[ k ] = r.v[ k ];
+                __threadfence();
+                unsigned prev = atomicAdd( P.counter, 1u );
+                sh_last = prev == unsigned( P.nchunk - 1 );
+            }
+            __syncthreads();
+            if ( sh_last ) {
+                __threadfence();
+                fold_reports_block( P );
+            }
+            __syncthreads();
+        }
+    }
+}
 
 
 // the big-cell pass: one warp a block, the cell in dynamic shared memory (Cell3B), over the queued 3D items (the 2D ones
@@ -973,7 +1114,8 @@ void launch_cells3d_giant( const Launch &L, const ProbDev *probs, const OvfList 
     ++*L.launches;
 }
 
-void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf ) {
+void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
+                     const Split3 *sp ) {
     if ( nchunks <= 0 ) return;
     const size_t smem = sizeof( Cell3 ) * W3;
     static bool configured = false;
@@ -981,8 +1123,15 @@ void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks,
         cudaFuncSetAttribute( k_cells3d, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
         configured = true;
     }
-    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
-    ++*L.launches;
+    if ( ! sp ) {
+        k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 0, Split3{} );
+        ++*L.launches;
+        return;
+    }
+    cudaMemsetAsync( sp->used, 0, sizeof( unsigned long long ), L.stream );
+    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 1, *sp );
+    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 2, *sp );
+    *L.launches += 2;
 }
 
 void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, OvfList *next ) {

@@ -102,6 +102,9 @@ void ctx_release( Ctx &c ) {
         if ( c.big_scratch ) cudaFreeAsync( c.big_scratch, c.stream );
         if ( c.dgiant ) cudaFreeAsync( c.dgiant, c.stream );
         if ( c.giant_scratch ) cudaFreeAsync( c.giant_scratch, c.stream );
+        if ( c.split.mem ) cudaFreeAsync( c.split.mem, c.stream );
+        if ( c.split.used ) cudaFreeAsync( c.split.used, c.stream );
+        if ( c.split.slot ) cudaFreeAsync( c.split.slot, c.stream );
         cudaStreamSynchronize( c.stream );
         cudaStreamDestroy( c.stream );
     }
@@ -266,6 +269,34 @@ int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags ) {
 }
 
 // a capacity or topology error of a solve's cell is its problem's (the per-slot flag read in `decide`), not the batch's
+// about 1.5 KB a stored cell (25 vertices, 15 planes); the records never take more than 2 GiB (past it, pass 2 does the
+// cells that found no room whole)
+const Split3 *split3_for( Ctx &c, int nchunks, long gcells ) {
+    if ( gcells <= 0 || nchunks <= 0 ) return nullptr;
+    const unsigned long long want = std::min<unsigned long long>( 2ull << 30, std::max<unsigned long long>( 64ull << 20, gcells * 2048ull ) );
+    try {
+        if ( ! c.split.used ) c.split.used = ( unsigned long long * ) dalloc( c, 256 );
+        if ( c.split.cap < want ) {
+            if ( c.split.mem ) dfree( c, c.split.mem );
+            c.split.mem = nullptr;
+            c.split.cap = 0;
+            c.split.mem = ( char * ) dalloc( c, want );
+            c.split.cap = want;
+        }
+        const size_t slots = size_t( nchunks ) * CHUNK;
+        if ( c.split_slots < slots ) {
+            if ( c.split.slot ) dfree( c, c.split.slot );
+            c.split.slot = nullptr;
+            c.split_slots = 0;
+            c.split.slot = ( long long * ) dalloc( c, slots * sizeof( long long ) );
+            c.split_slots = slots;
+        }
+    } catch ( const Error & ) {
+        return nullptr;
+    }
+    return c.split.mem && c.split.slot ? &c.split : nullptr;
+}
+
 static void clear_capacity_error( Ctx &c ) {
     if ( c.herr->code != SDOT_ERR_CAPACITY && c.herr->code != SDOT_ERR_TOPOLOGY ) return;
     if ( std::getenv( "SDOT_TRACE" ) )
@@ -1746,10 +1777,14 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
                 double seeds = 0;
                 for ( auto &ch : CX[ q ] ) seeds += ch.end - ch.begin;
                 unsigned flags = ( q & 1 ) ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS | F_REPORT );
+                long gseeds = 0;
+                if ( dim == 3 )
+                    for ( auto &ch : CX[ q ] ) gseeds += PX[ ch.prob ].dkind == D_GAUSS ? ch.end - ch.begin : 0;
+                const Split3 *sp = dim == 3 ? split3_for( c, int( CX[ q ].size() ), gseeds ) : nullptr;
                 c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
                 if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf );
-                else launch_cells3d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf );
-                c.timer.end( c.stream );
+                else launch_cells3d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf, sp );
+                c.timer.end( c.stream, sp ? 2 : 1 );
             }
             big_probs = PX;
             big_chunks.assign( PX.size(), {} );

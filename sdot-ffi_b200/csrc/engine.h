@@ -59,6 +59,9 @@ struct Ctx {
         unsigned long long launches = 0;
     };
     std::vector<BurstGraph> graphs;
+    // the two passes of the gaussian 3D cells: their records and per-cell slots (grown on demand, see `split3_for`)
+    Split3 split{};
+    size_t split_slots = 0;
     Timer timer;
     Launch L() { return Launch{ stream, &launches, &timer }; }
 };
@@ -72,6 +75,9 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit );   // throws Error
 void ctx_release( Ctx &c );
 // after a big-cell pass that queued 3D cells on `dgiant`: the giant-cell pass over them (synchronises); their number
 int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags );
+// the scratch of the two-pass gaussian 3D cells for a launch of `nchunks` chunks that holds `gcells` cells of gaussian
+// problems: NULL when there are none, or when the pool cannot give it (the kernel then takes one pass)
+const Split3 *split3_for( Ctx &c, int nchunks, long gcells );
 void *dalloc( Ctx &c, size_t bytes );
 void dfree( Ctx &c, void *p );
 

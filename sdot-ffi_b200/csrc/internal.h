@@ -395,7 +395,16 @@ void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, 
 void launch_scale( const Launch &L, double *v, int n, double s );
 void launch_scatter( const Launch &L, const double *ranked, const int *user, int n, int dim, double *out_user );
 void launch_gather_vec( const Launch &L, const double *user_vals, const int *user, int n, double *ranked, double scale );
-void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
+// the clipped cells of the gaussian problems between the two passes of the 3D main kernel (cells3d.cu)
+struct Split3 {
+    char *mem;                        // the records
+    unsigned long long *used;         // bytes taken (zeroed before pass 1)
+    unsigned long long cap;           // bytes of `mem`
+    long long *slot;                  // [ chunk of the launch ][ CHUNK ]: a cell's record offset; -1 none (pass 2 does it whole), -2 queued
+};
+// sp NULL: one pass; else two passes for the gaussian problems (sp->slot holds nchunks * CHUNK entries)
+void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
+                     const Split3 *sp = nullptr );
 // the queued 3D cells (past the warp cell's capacities) rebuilt one warp a block with larger capacities
 void launch_cells3d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, OvfList *next );
 // the 3D cells past the big pass's capacities (queued on its `next`), each warp's cell in a slot of `scratch`
