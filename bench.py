@@ -404,6 +404,7 @@ def main():
     ap.add_argument("--solve-only", type=int, default=0, help="one solve of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--solve-linear", default="auto", choices=["auto", "cg", "mg"])
     ap.add_argument("--solve-step", default="auto", choices=["auto", "trials", "limits"])
+    ap.add_argument("--solve-lin-precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args()
     if a.cpu_worker is not None:
         cpu_worker(a.seed, [int(k) for k in a.cpu_worker.split(",") if k])
@@ -420,11 +421,13 @@ def main():
         _lib.set_timing(True)
         t0 = time.perf_counter()
         plan = OtProblem(SumOfDiracs(pos), dist).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=RTOL, linear_solver=a.solve_linear,
-                                                                                        step=a.solve_step)))
+                                                                                        step=a.solve_step,
+                                                                                        linear_precision=a.solve_lin_precision)))
         secs = time.perf_counter() - t0
         st = plan.stats
         kst = _lib.kernel_stats()
         print(json.dumps({"solve_only": a.solve_only, "dim": d, "density": a.cells_density, "linear": a.solve_linear, "step": a.solve_step,
+                          "lin_precision": a.solve_lin_precision,
                           "status": st["status"], "seconds": secs, "nb_iter": st["nb_iter"], "nb_diag": st["nb_diag"],
                           "lin_nb_iter": st["lin_nb_iter"], "kernel_ms": {k: round(v[0], 3) for k, v in kst.items()},
                           "kernel_launches": {k: v[1] for k, v in kst.items()}}))

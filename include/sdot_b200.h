@@ -147,7 +147,10 @@ int32_t sdot_laplacian(sdot_context ctx, const sdot_diagram_desc *desc, int64_t 
 /* ---- the linear solve alone -------------------------------------------------------------------------
  * `L x_k = rhs_k` for k < nrhs with L = diag(dia) - offdiag(vals) given as CSR (row_ptr int64, cols int32),
  * each rhs of zero sum; x gauge-fixed to `x[0] = 0`.  `method` 0 = preconditioned CG (Jacobi),
- * 1 = CG preconditioned by the aggregation multigrid.  `iterations[k]` = CG iterations (-1: failed).
+ * 1 = CG preconditioned by the aggregation multigrid; 2 and 3 = the same two with the CG in FP32 on FP32
+ * copies of the matrix and vectors, refined in FP64 (x and the residual b - L x kept in FP64, the inner CG
+ * restarted on each new residual until it meets `tol`).  `iterations[k]` = CG iterations (-1: failed).
+ * The reference's options of precision (gpu/Linear2D.cuh:80-102) map onto methods 2 / 3.
  * Replaces `sdot::gpu2d::linear_solves(queue, row, col, val, dia, rhs, options, solution, iterations,
  * allocator)` (gpu/Newton2D.cuh:1916-1960), the test hook `_card_linear_solves` (SdotPlanNd.py:204-236). */
 int32_t sdot_linear_solve(sdot_context ctx, int64_t n, const int64_t *row_ptr, const int32_t *cols, const double *vals,
@@ -193,7 +196,7 @@ enum sdot_option {
     SDOT_OPT_CONV_MIN,
     SDOT_OPT_LIN_METHOD,          /* 0 Jacobi-PCG, 1 multigrid-PCG                                            */
     SDOT_OPT_PRECISION,           /* 0 FP64 clipping (1, FP32 clipping + FP64 re-check: SDOT_ERR_UNSUPPORTED) */
-    SDOT_OPT_LIN_PRECISION,       /* 0 FP64 CG (1, FP32 inner CG + FP64 refinement: SDOT_ERR_UNSUPPORTED)    */
+    SDOT_OPT_LIN_PRECISION,       /* 0 FP64 CG; 1 FP32 inner CG with FP64 iterative refinement                */
     SDOT_OPT_AGG_MARGIN,          /* aggregation of near-coincident seeds: merge a pair when c_ij ulp(w) margin  */
                                   /* > the tolerance (sdotplan/Aggregation.h); 0: off; the reference uses 4      */
     SDOT_OPT_STEP,                /* 0 trials (KMT backtracking); 1 limits (2D: the step brought under the limits */

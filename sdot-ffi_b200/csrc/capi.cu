@@ -403,7 +403,9 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
     return guard( st, [&] {
         Ctx &c = ctx->c;
         CK( cudaSetDevice( c.device ) );
-        if ( method != 0 && method != 1 ) throw Error( SDOT_ERR_ARGS, "linear method: 0 (Jacobi-PCG) or 1 (multigrid-PCG)" );
+        if ( method < 0 || method > 3 )
+            throw Error( SDOT_ERR_ARGS, "linear method: 0 (Jacobi-PCG), 1 (multigrid-PCG), 2 / 3 (the same, FP32 CG with FP64 iterative refinement)" );
+        const bool mg = method & 1, mixed = method >= 2;
         std::vector<int64_t> hrp;
         if ( memory == SDOT_DEVICE ) {
             hrp.resize( n + 1 );
@@ -415,6 +417,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         std::vector<int> rp32( hrp.begin(), hrp.end() );
         const long nch = ( n + VCHUNK - 1 ) / VCHUNK;
         size_t bytes = size_t( n + 1 ) * 4 + size_t( nnz + 1 ) * 12 + size_t( n ) * 8 * 9 + size_t( nch ) * 32 + NB_SC * 8 + 64 + 16 * 256;
+        if ( mixed ) bytes += size_t( nnz + 1 ) * 4 + size_t( n ) * 4 * 6 + 8 * 256;
         DevVec mem( c, bytes );
         Arena A{ ( char * ) mem.p, bytes, 0 };
         int *rp = A.take<int>( n + 1 ), *col = A.take<int>( nnz + 1 );
@@ -422,10 +425,15 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         double *xx = A.take<double>( n ), *r = A.take<double>( n ), *z = A.take<double>( n ), *p = A.take<double>( n ), *q = A.take<double>( n );
         double *b = A.take<double>( n ), *d = A.take<double>( n ), *part = A.take<double>( size_t( nch ) * 4 ), *sc = A.take<double>( NB_SC );
         unsigned *counter = A.take<unsigned>( 2 );
+        float *m32[ 7 ] = {};
+        if ( mixed ) {
+            m32[ 0 ] = A.take<float>( nnz + 1 );
+            for ( int q = 1; q < 7; ++q ) m32[ q ] = A.take<float>( n );
+        }
         CK( cudaMemsetAsync( counter, 0, 8, c.stream ) );
         auto kind = memory == SDOT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        std::vector<int> perm, iperm;                       // method 1: the system in reverse Cuthill-McKee order
-        if ( method == 1 ) {
+        std::vector<int> perm, iperm;                       // multigrid: the system in reverse Cuthill-McKee order
+        if ( mg ) {
             std::vector<int> hcol( nnz );
             std::vector<double> hval( nnz ), hdia( n );
             auto to_host = memory == SDOT_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
@@ -468,7 +476,11 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         V.tol = tol > 0 ? tol : 1e-10;
         V.maxit = maxit > 0 ? maxit : 100000;
         V.sc = sc; V.partials = part; V.counter = counter; V.nchunk = int( vch.size() ); V.active = 1;
-        V.rank0 = method == 1 ? iperm[ 0 ] : 0;            // the gauge x[ 0 ] = 0, row 0 wherever it went
+        V.rank0 = mg ? iperm[ 0 ] : 0;                     // the gauge x[ 0 ] = 0, row 0 wherever it went
+        if ( mixed ) {
+            V.mixed = 1;
+            V.val32 = m32[ 0 ]; V.dia32 = m32[ 1 ]; V.x32 = m32[ 2 ]; V.r32 = m32[ 3 ]; V.z32 = m32[ 4 ]; V.p32 = m32[ 5 ]; V.q32 = m32[ 6 ];
+        }
         size_t o1 = ( sizeof( VecDev ) + 255 ) & ~size_t( 255 );
         DevVec dd( c, o1 + vch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &V, sizeof( V ), cudaMemcpyHostToDevice, c.stream ) );
@@ -484,7 +496,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             double mean = 0;
             for ( double v : hb ) mean += v;
             mean /= double( n );
-            if ( method == 1 ) {
+            if ( mg ) {
                 std::vector<double> hp( n );
                 for ( long q = 0; q < n; ++q ) hp[ q ] = hb[ perm[ q ] ];
                 hb.swap( hp );
@@ -493,7 +505,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             double hsc[ NB_SC ] = {};
             hsc[ SC_MEAN ] = mean;
             CK( cudaMemcpyAsync( sc, hsc, sizeof( hsc ), cudaMemcpyHostToDevice, c.stream ) );
-            if ( method == 1 ) {
+            if ( mg ) {
                 const int its = mg_linear_solve( c, V, nnz, hsc );
                 if ( iterations ) iterations[ k ] = its;
                 std::vector<double> hd( n ), hx( n );
@@ -503,9 +515,13 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
                 CK( cudaMemcpy( x + size_t( k ) * n, hx.data(), n * 8, memory == SDOT_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost ) );
                 continue;
             }
-            launch_cg_init( L, dv, dch, int( vch.size() ) );
+            if ( mixed ) launch_mx_init( L, dv, dch, int( vch.size() ) );
+            else launch_cg_init( L, dv, dch, int( vch.size() ) );
             for ( ;; ) {
-                for ( int s = 0; s < 32; ++s ) launch_cg_iter( L, dv, dch, int( vch.size() ) );
+                for ( int s = 0; s < 32; ++s ) {
+                    if ( mixed ) launch_mx_iter( L, dv, dch, int( vch.size() ) );
+                    else launch_cg_iter( L, dv, dch, int( vch.size() ) );
+                }
                 CK( cudaMemcpyAsync( hsc, sc, sizeof( hsc ), cudaMemcpyDeviceToHost, c.stream ) );
                 CK( cudaStreamSynchronize( c.stream ) );
                 if ( hsc[ SC_CONV ] != 0 ) break;

@@ -539,7 +539,20 @@ struct SolveJob {
     bool full_set = false;              // stats[ residual_full ] computed on the full problem
     int polish_round = 0;               // the re-splitting after an aggregated convergence: rounds done,
     double polish_before = 0;           // ... and the members' residual before the current one
+    // lin_precision 1: the FP32 copies of the inner CG (matrix values [n * cap], diagonal and five vectors [n])
+    char *mx_mem = nullptr;
+    float *val32 = nullptr, *dia32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr;
 };
+
+static void alloc_mixed( Ctx &c, SolveJob &J ) {
+    const size_t n = size_t( J.G.n );
+    const size_t bytes = n * J.cap * 4 + 6 * ( n * 4 + 256 ) + 256;
+    J.mx_mem = ( char * ) dalloc( c, bytes );
+    Arena A{ J.mx_mem, bytes, 0 };
+    J.val32 = A.take<float>( n * J.cap );
+    J.dia32 = A.take<float>( n ); J.x32 = A.take<float>( n ); J.r32 = A.take<float>( n );
+    J.z32 = A.take<float>( n ); J.p32 = A.take<float>( n ); J.q32 = A.take<float>( n );
+}
 
 static size_t mg_bytes( int dim, long n, int cap );
 
@@ -684,8 +697,10 @@ static bool convolvable( const SolveJob &J ) { return J.G.dkind == D_GAUSS || ( 
 
 SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
     const sdot_diagram_desc &D = desc.diagram;
-    if ( desc.options[ SDOT_OPT_PRECISION ] != 0 || desc.options[ SDOT_OPT_LIN_PRECISION ] != 0 )
-        throw Error( SDOT_ERR_UNSUPPORTED, "options precision / lin_precision: FP64 clipping and an FP64 CG only (both 0)" );
+    if ( desc.options[ SDOT_OPT_PRECISION ] != 0 )
+        throw Error( SDOT_ERR_UNSUPPORTED, "option precision: FP64 clipping only (0)" );
+    if ( desc.options[ SDOT_OPT_LIN_PRECISION ] != 0 && desc.options[ SDOT_OPT_LIN_PRECISION ] != 1 )
+        throw Error( SDOT_ERR_ARGS, "option lin_precision: 0 (FP64 CG) or 1 (FP32 CG with FP64 iterative refinement)" );
     SolveJob *J = new SolveJob;
     try {
         J->t_begin = now_s();
@@ -715,6 +730,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         for ( double &v : w0 ) v -= g0;
         alloc_job( c, *J );
         if ( int( J->opt[ SDOT_OPT_LIN_METHOD ] ) == 1 ) alloc_mg( c, *J );
+        if ( int( J->opt[ SDOT_OPT_LIN_PRECISION ] ) == 1 ) alloc_mixed( c, *J );
         J->slot = take_slot( c );
         CK( cudaMemsetAsync( c.dscal + size_t( J->slot ) * SLOT_DOUBLES + SLOT_ERR, 0, 2 * sizeof( double ), c.stream ) );
         CK( cudaMemcpyAsync( &J->rank0, J->G.rank_of, sizeof( int ), cudaMemcpyDeviceToHost, c.stream ) );
@@ -750,6 +766,7 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
 void job_destroy( Ctx &c, SolveJob *J ) {
     if ( ! J ) return;
     if ( J->mg_mem ) dfree( c, J->mg_mem );
+    if ( J->mx_mem ) dfree( c, J->mx_mem );
     if ( J->d_cl ) dfree( c, J->d_cl );
     if ( J->ae ) dfree( c, J->ae );
     if ( J->mem ) dfree( c, J->mem );
@@ -1380,6 +1397,10 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.nchunk = J.nch_vec;
     V.active = 1;
     V.precond = J.mg_L > 0 ? 1 : 0;
+    if ( J.mx_mem ) {
+        V.mixed = 1;
+        V.val32 = J.val32; V.dia32 = J.dia32; V.x32 = J.x32; V.r32 = J.r32; V.z32 = J.z32; V.p32 = J.p32; V.q32 = J.q32;
+    }
     if ( J.agg_margin > 0 ) {
         V.agg_pairs = J.agg_pairs;
         V.agg_cap = AGG_CAP;
@@ -1436,7 +1457,7 @@ struct VecBatch {
     // what the launches of a CG burst depend on: the upload area, the burst, and every table's size
     std::vector<long long> layout_key( const char *desc, int burst ) const {
         std::vector<long long> k{ ( long long ) ( uintptr_t ) desc, burst, ( long long ) ch.size(), maxL, ( long long ) bottom.size() };
-        for ( auto &x : v ) { k.push_back( x.n ); k.push_back( x.precond ); }
+        for ( auto &x : v ) { k.push_back( x.n ); k.push_back( x.precond ); k.push_back( x.mixed ); }
         for ( int l = 0; l < maxL; ++l ) {
             k.push_back( ( long long ) lv[ l ].size() );
             k.push_back( ( long long ) down[ l ].size() );
@@ -1554,20 +1575,29 @@ int mg_linear_solve( Ctx &c, const VecDev &V0, long nnz, double *hsc ) {
     B.upload( c );
     Launch L = c.L();
     const int nch = int( B.ch.size() );
+    const bool mixed = V.mixed != 0;
     if ( B.mg() ) {
         B.build( L, c.derr );
-        launch_cg_init0( L, B.dv, B.dch, nch );
+        if ( mixed ) launch_mx_init( L, B.dv, B.dch, nch );
+        else launch_cg_init0( L, B.dv, B.dch, nch );
         B.vcycle( L );
-        launch_cg_init1( L, B.dv, B.dch, nch );
-    } else
+        if ( mixed ) launch_mx_init1( L, B.dv, B.dch, nch );
+        else launch_cg_init1( L, B.dv, B.dch, nch );
+    } else if ( mixed )
+        launch_mx_init( L, B.dv, B.dch, nch );
+    else
         launch_cg_init( L, B.dv, B.dch, nch );
     for ( ;; ) {
         for ( int k = 0; k < MG_BURST_SOLVE; ++k ) {
             if ( B.mg() ) {
-                launch_cg_spmv_update( L, B.dv, B.dch, nch );
+                if ( mixed ) launch_mx_spmv_update( L, B.dv, B.dch, nch );
+                else launch_cg_spmv_update( L, B.dv, B.dch, nch );
                 B.vcycle( L );
-                launch_cg_rz_p( L, B.dv, B.dch, nch );
-            } else
+                if ( mixed ) launch_mx_rz_p( L, B.dv, B.dch, nch );
+                else launch_cg_rz_p( L, B.dv, B.dch, nch );
+            } else if ( mixed )
+                launch_mx_iter( L, B.dv, B.dch, nch );
+            else
                 launch_cg_iter( L, B.dv, B.dch, nch );
         }
         CK( cudaMemcpyAsync( hsc, V.sc, NB_SC * sizeof( double ), cudaMemcpyDeviceToHost, c.stream ) );
@@ -1607,10 +1637,13 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
         }
     }
     if ( ! newton.v.empty() ) {
-        // Jacobi-preconditioned and multigrid-preconditioned problems go in two batches
-        VecBatch jac, mgb;
-        for ( size_t k = 0; k < newton.v.size(); ++k ) ( newton.v[ k ].precond ? mgb : jac ).add( newton.v[ k ], newton.jobs[ k ] );
-        for ( VecBatch *B : { &jac, &mgb } ) {
+        // Jacobi- and multigrid-preconditioned problems, FP64 and mixed CG, go in four batches
+        VecBatch jac, mgb, jacx, mgbx;
+        for ( size_t k = 0; k < newton.v.size(); ++k ) {
+            const VecDev &v = newton.v[ k ];
+            ( v.precond ? ( v.mixed ? mgbx : mgb ) : ( v.mixed ? jacx : jac ) ).add( v, newton.jobs[ k ] );
+        }
+        for ( VecBatch *B : { &jac, &mgb, &jacx, &mgbx } ) {
             if ( B->v.empty() ) continue;
             B->upload( c );
             const int nch = int( B->ch.size() );
@@ -1624,12 +1657,17 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             for ( auto &v : B->v ) agg |= v.agg_pairs != nullptr;
             if ( agg ) launch_agg_detect( L, B->dv, B->dch, nch );
             launch_rhs( L, B->dv, B->dch, nch );
+            const bool mixed = B == &jacx || B == &mgbx;
             if ( B->mg() ) {
                 B->build( L, c.derr );
-                launch_cg_init0( L, B->dv, B->dch, nch );
+                if ( mixed ) launch_mx_init( L, B->dv, B->dch, nch );
+                else launch_cg_init0( L, B->dv, B->dch, nch );
                 B->vcycle( L );
-                launch_cg_init1( L, B->dv, B->dch, nch );
-            } else
+                if ( mixed ) launch_mx_init1( L, B->dv, B->dch, nch );
+                else launch_cg_init1( L, B->dv, B->dch, nch );
+            } else if ( mixed )
+                launch_mx_init( L, B->dv, B->dch, nch );
+            else
                 launch_cg_init( L, B->dv, B->dch, nch );
             c.timer.end( c.stream, 5 );
         }
@@ -1844,15 +1882,15 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         }
     }
     // B. CG iterations
-    VecBatch cgj, cgm;
+    VecBatch cgj, cgm, cgjx, cgmx;
     std::vector<SolveJob *> with_cg;
     for ( SolveJob *J : jobs )
         if ( J->state == J_CG ) {
             VecDev V = vec_of( c, *J );
-            ( V.precond ? cgm : cgj ).add( V, J );
+            ( V.precond ? ( V.mixed ? cgmx : cgm ) : ( V.mixed ? cgjx : cgj ) ).add( V, J );
             with_cg.push_back( J );
         }
-    for ( VecBatch *B : { &cgj, &cgm } ) {
+    for ( VecBatch *B : { &cgj, &cgm, &cgjx, &cgmx } ) {
         if ( B->v.empty() ) continue;
         B->upload( c );
         const int nch = int( B->ch.size() );
@@ -1860,13 +1898,18 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         if ( with_diag.empty() ) burst *= 4;
         double rows = 0;
         for ( auto &v : B->v ) rows += v.n;
+        const bool mixed = B == &cgjx || B == &cgmx;
         auto issue = [&]() {
             for ( int k = 0; k < burst; ++k ) {
                 if ( B->mg() ) {
-                    launch_cg_spmv_update( L, B->dv, B->dch, nch );
+                    if ( mixed ) launch_mx_spmv_update( L, B->dv, B->dch, nch );
+                    else launch_cg_spmv_update( L, B->dv, B->dch, nch );
                     B->vcycle( L );
-                    launch_cg_rz_p( L, B->dv, B->dch, nch );
-                } else
+                    if ( mixed ) launch_mx_rz_p( L, B->dv, B->dch, nch );
+                    else launch_cg_rz_p( L, B->dv, B->dch, nch );
+                } else if ( mixed )
+                    launch_mx_iter( L, B->dv, B->dch, nch );
+                else
                     launch_cg_iter( L, B->dv, B->dch, nch );
             }
         };

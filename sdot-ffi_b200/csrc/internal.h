@@ -168,6 +168,9 @@ struct VecDev {
     int chunk0, nchunk;
     int active;
     int precond;                  // 0 Jacobi, 1 multigrid (the V-cycle writes z)
+    // lin_precision 1: the inner CG on FP32 copies (matrix values, diagonal, e = x32, r32, z32, p32, q32); x, r, b stay FP64
+    int mixed;
+    float *val32, *dia32, *x32, *r32, *z32, *p32, *q32;
     // the detection of near-coincident pairs on this Laplacian (NULL: off): the pairs (i < j, ranks) whose facet the
     // doubles of the weights cannot place within the tolerance, c_ij ulp( max |w| ) margin > tau
     int2 *agg_pairs;
@@ -194,7 +197,12 @@ struct MgLevel {
     float *inv;                        // the coarsest level: dense inverse [n * n]
 };
 
-enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, SC_ITER, SC_MEAN, SC_C, SC_TOL, SC_PQ, SC_FAIL, SC_NNZ, NB_SC };
+enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, SC_ITER, SC_MEAN, SC_C, SC_TOL, SC_PQ, SC_FAIL, SC_NNZ,
+                    SC_REFINE,      // mixed CG: 1 once the inner FP32 CG has converged (x += e, then the FP64 residual)
+                    SC_IN0,         // mixed CG: the inner CG's starting residual norm
+                    SC_RPREV,       // mixed CG: the FP64 residual norm of the last refinement
+                    SC_NREF,        // mixed CG: refinements so far
+                    NB_SC };
 constexpr int VCHUNK = 1024;     // rows per chunk of the vector kernels
 
 // ---- warp helpers ------------------------------------------------------------------------------------
@@ -374,6 +382,12 @@ void launch_cg_init0( const Launch &L, const VecDev *v, const Chunk *ch, int nch
 void launch_cg_init1( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_spmv_update( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_cg_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the mixed CG (FP32 inner CG, FP64 iterative refinement): the same sequence of launches as the FP64 CG
+void launch_mx_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch );          // (Jacobi) or before the first V-cycle (multigrid)
+void launch_mx_init1( const Launch &L, const VecDev *v, const Chunk *ch, int nch );         // (multigrid) after the first V-cycle
+void launch_mx_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch );          // (Jacobi) one iteration
+void launch_mx_spmv_update( const Launch &L, const VecDev *v, const Chunk *ch, int nch );   // (multigrid) before the V-cycle
+void launch_mx_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch );          // (multigrid) after the V-cycle
 // mg.cu
 void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
 void launch_mg_coarsen( const Launch &L, const MgLevel *lv, int nprob, const Chunk *ch, int nch, ErrRec *err );

@@ -449,6 +449,226 @@ void launch_cg_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch 
     *L.launches += 2;
 }
 
+// ---- FP32 CG with FP64 iterative refinement (lin_precision 1) ----------------------------------------------------------
+// The inner CG runs on FP32 copies of the matrix values, of the diagonal and of its vectors (e, r32, z32, p32, q32): half
+// the bytes of every product and update.  x, the residual r and b stay FP64.  When the inner residual has fallen by
+// MX_INNER (or under half the outer target), x += e in FP64, the residual r = b - A x is recomputed with the FP64 matrix,
+// and the inner CG restarts on it; the outer stop is the FP64 residual's, tol |b|.  A refinement that does not cut the
+// FP64 residual by 10 % is a linear failure (FP32 cannot resolve the system).
+// Everything runs inside the ordinary sequence of CG launches (so a burst, and its CUDA graph, is unchanged), steered by
+// the problem's scalars: the update's fold sets SC_REFINE; the next p kernel adds e to x instead of updating p; the next
+// product computes the FP64 residual instead of q, resets e and p to 0 and sets alpha = 0, rz = 1 -- so that the
+// update, the V-cycle and p = z + beta p that follow start a fresh CG.  Dot products are summed in FP64, in fixed trees.
+constexpr double MX_INNER = 1e-3;
+
+__device__ __forceinline__ bool mx_idle( const VecDev &V ) { return ! V.active || V.sc[ SC_CONV ] != 0; }
+
+__device__ __forceinline__ float row_dot32( const VecDev &V, int i, int sub, const float *__restrict__ x ) {
+    float t = 0;
+    const int e1 = V.row_ptr[ i + 1 ];
+    for ( int e = V.row_ptr[ i ] + sub; e < e1; e += LPR ) t += V.val32[ e ] * x[ V.col[ e ] ];
+#pragma unroll
+    for ( int o = 1; o < LPR; o <<= 1 ) t += __shfl_xor_sync( 0xffffffffu, t, o, LPR );
+    return t;
+}
+
+// b -= mean; x = 0, r = b; the FP32 copies; e = 0, r32 = r; Jacobi: z32 = r32 / dia, p32 = z32; multigrid: p32 = 0 (set by
+// init1 after the first V-cycle)
+__global__ void __launch_bounds__( VT ) k_mx_init( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( ! V.active ) return;
+    const double mean = V.sc[ SC_MEAN ];
+    const bool jac = ! V.precond;
+    double bb = 0, ss = 0, rz = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        for ( int e = V.row_ptr[ i ]; e < V.row_ptr[ i + 1 ]; ++e ) V.val32[ e ] = float( V.val[ e ] );
+        const float d32 = float( V.dia[ i ] );
+        V.dia32[ i ] = d32;
+        const double b = V.b[ i ] - mean;
+        V.b[ i ] = b;
+        V.x[ i ] = 0;
+        V.r[ i ] = b;
+        const float r32 = float( b ), z32 = jac ? r32 / d32 : 0.0f;
+        V.x32[ i ] = 0; V.r32[ i ] = r32; V.q32[ i ] = 0; V.z32[ i ] = z32; V.p32[ i ] = z32;
+        bb += b * b;
+        ss += double( r32 ) * r32;
+        rz += double( r32 ) * z32;
+    }
+    double v[ 3 ] = { bb, ss, rz }, tot[ 3 ];
+    block_sum<3>( v );
+    if ( fold_last<3>( V, ch, v, tot ) ) {
+        const double bn = sqrt( tot[ 0 ] );
+        V.sc[ SC_BNORM ] = bn; V.sc[ SC_RNORM ] = bn; V.sc[ SC_RPREV ] = bn;
+        V.sc[ SC_IN0 ] = sqrt( tot[ 1 ] );
+        V.sc[ SC_RZ ] = jac ? tot[ 2 ] : 1.0;
+        V.sc[ SC_ITER ] = 0; V.sc[ SC_FAIL ] = 0; V.sc[ SC_REFINE ] = 0; V.sc[ SC_NREF ] = 0;
+        V.sc[ SC_CONV ] = tot[ 0 ] == 0 ? 1.0 : 0.0;
+        if ( V.sc[ SC_NNZ ] > double( V.n ) * V.cap ) { V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
+    }
+}
+
+// (multigrid) after the first V-cycle: p32 = z32, rz
+__global__ void __launch_bounds__( VT ) k_mx_init1( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( mx_idle( V ) ) return;
+    double rz = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        const float z = V.z32[ i ];
+        V.p32[ i ] = z;
+        rz += double( V.r32[ i ] ) * z;
+    }
+    double v[ 1 ] = { rz }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) V.sc[ SC_RZ ] = tot[ 0 ];
+}
+
+// q32 = A32 p32 and alpha; or, after an inner convergence, the refinement: r = b - A x (FP64), the inner CG restarted on it
+__global__ void __launch_bounds__( VT ) k_mx_spmv( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( mx_idle( V ) ) return;
+    const bool refine = V.sc[ SC_REFINE ] != 0;       // (read by every block before the last one's fold clears it)
+    const int sub = threadIdx.x % LPR;
+    double a0 = 0, a1 = 0;
+    const int end = ch.begin + ( ( ch.end - ch.begin + VT / LPR - 1 ) / ( VT / LPR ) ) * ( VT / LPR );
+    for ( int i0 = ch.begin + int( threadIdx.x ) / LPR; i0 < end; i0 += VT / LPR ) {
+        const bool in = i0 < ch.end;
+        const int row = in ? i0 : ch.begin;
+        if ( refine ) {
+            const double t = row_dot_lanes( V, row, sub, V.x );
+            if ( in && sub == 0 ) {
+                const double r = V.b[ i0 ] - ( V.dia[ i0 ] * V.x[ i0 ] - t );
+                V.r[ i0 ] = r;
+                const float r32 = float( r );
+                V.r32[ i0 ] = r32; V.x32[ i0 ] = 0; V.p32[ i0 ] = 0;
+                a0 += r * r;
+                a1 += double( r32 ) * r32;
+            }
+        } else {
+            const float t = row_dot32( V, row, sub, V.p32 );
+            if ( in && sub == 0 ) {
+                const float pi = V.p32[ i0 ], q = V.dia32[ i0 ] * pi - t;
+                V.q32[ i0 ] = q;
+                a0 += double( pi ) * q;
+            }
+        }
+    }
+    double v[ 2 ] = { a0, a1 }, tot[ 2 ];
+    block_sum<2>( v );
+    if ( fold_last<2>( V, ch, v, tot ) ) {
+        if ( refine ) {
+            const double rn = sqrt( tot[ 0 ] );
+            V.sc[ SC_RNORM ] = rn;
+            V.sc[ SC_NREF ] += 1;
+            V.sc[ SC_REFINE ] = 0;
+            if ( rn <= V.tol * V.sc[ SC_BNORM ] ) V.sc[ SC_CONV ] = 1;
+            else if ( ! ( rn < 0.9 * V.sc[ SC_RPREV ] ) ) { V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
+            else {
+                V.sc[ SC_RPREV ] = rn;
+                V.sc[ SC_IN0 ] = sqrt( tot[ 1 ] );
+                V.sc[ SC_ALPHA ] = 0;
+                V.sc[ SC_RZ ] = 1;
+            }
+        } else if ( tot[ 0 ] > 0 )
+            V.sc[ SC_ALPHA ] = V.sc[ SC_RZ ] / tot[ 0 ];
+        else { V.sc[ SC_ALPHA ] = 0; V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
+    }
+}
+
+// e += alpha p32, r32 -= alpha q32 (Jacobi: z32 = r32 / dia, rz, beta); the inner stop sets SC_REFINE
+__global__ void __launch_bounds__( VT ) k_mx_update( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( mx_idle( V ) ) return;
+    const float al = float( V.sc[ SC_ALPHA ] );
+    const bool jac = ! V.precond;
+    double rz = 0, rr = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) {
+        V.x32[ i ] += al * V.p32[ i ];
+        const float r = V.r32[ i ] - al * V.q32[ i ];
+        V.r32[ i ] = r;
+        if ( jac ) {
+            const float z = r / V.dia32[ i ];
+            V.z32[ i ] = z;
+            rz += double( r ) * z;
+        }
+        rr += double( r ) * r;
+    }
+    double v[ 2 ] = { rz, rr }, tot[ 2 ];
+    block_sum<2>( v );
+    if ( fold_last<2>( V, ch, v, tot ) ) {
+        const double it = V.sc[ SC_ITER ] + 1;
+        V.sc[ SC_ITER ] = it;
+        if ( jac ) {
+            V.sc[ SC_BETA ] = tot[ 0 ] / V.sc[ SC_RZ ];
+            V.sc[ SC_RZ ] = tot[ 0 ];
+        }
+        const double rn = sqrt( tot[ 1 ] );
+        if ( it >= V.maxit ) { V.sc[ SC_CONV ] = 2; V.sc[ SC_FAIL ] = 1; }
+        else if ( rn <= MX_INNER * V.sc[ SC_IN0 ] || rn <= 0.5 * V.tol * V.sc[ SC_BNORM ] ) V.sc[ SC_REFINE ] = 1;
+    }
+}
+
+// (multigrid) rz = r32 . z32 after the V-cycle, beta
+__global__ void __launch_bounds__( VT ) k_mx_rz( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( mx_idle( V ) || V.sc[ SC_REFINE ] != 0 ) return;
+    double rz = 0;
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) rz += double( V.r32[ i ] ) * V.z32[ i ];
+    double v[ 1 ] = { rz }, tot[ 1 ];
+    block_sum<1>( v );
+    if ( fold_last<1>( V, ch, v, tot ) ) {
+        V.sc[ SC_BETA ] = tot[ 0 ] / V.sc[ SC_RZ ];
+        V.sc[ SC_RZ ] = tot[ 0 ];
+    }
+}
+
+// p32 = z32 + beta p32; or, after an inner convergence, x += e (FP64)
+__global__ void __launch_bounds__( VT ) k_mx_p( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const VecDev &V = vs[ ch.prob ];
+    if ( mx_idle( V ) ) return;
+    if ( V.sc[ SC_REFINE ] != 0 ) {
+        for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) V.x[ i ] += double( V.x32[ i ] );
+        return;
+    }
+    const float be = float( V.sc[ SC_BETA ] );
+    for ( int i = ch.begin + threadIdx.x; i < ch.end; i += VT ) V.p32[ i ] = V.z32[ i ] + be * V.p32[ i ];
+}
+
+void launch_mx_init( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mx_init<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+void launch_mx_init1( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mx_init1<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+void launch_mx_iter( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mx_spmv<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_mx_update<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_mx_p<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 3;
+}
+void launch_mx_spmv_update( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mx_spmv<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_mx_update<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 2;
+}
+void launch_mx_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
+    if ( nch <= 0 ) return;
+    k_mx_rz<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    k_mx_p<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    *L.launches += 2;
+}
+
 // d = x - x[ rank of user seed 0 ]: the gauge w_0 = 0 kept by the direction
 __global__ void k_gauge( const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks, int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];

@@ -263,21 +263,21 @@ __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ 
     const MgLevel &M = lv[ ch.prob ];
     const bool top = M.level == 0;
     const VecDev *V = vs + M.vec;
-    if ( V->sc[ SC_CONV ] != 0 ) return;
+    if ( V->sc[ SC_CONV ] != 0 || V->sc[ SC_REFINE ] != 0 ) return;
     const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
     for ( int I = ch.begin + int( threadIdx.x ) / MG_LANES; I < end; I += MGT / MG_LANES ) {
         const bool in = I < ch.end;
         const int i0 = I * M.pack, i1 = in ? min( M.n, i0 + M.pack ) : i0;
         float acc = 0;
         for ( int i = i0 + sub; i < i1; i += MG_LANES ) {
-            float bi = top ? float( V->r[ i ] ) : M.b[ i ];
+            float bi = top ? ( V->mixed ? V->r32[ i ] : float( V->r[ i ] ) ) : M.b[ i ];
             if ( top ) M.b[ i ] = bi;
             float xi = OMEGA * M.dinv[ i ] * bi;
             M.x[ i ] = xi;
             float ax = M.dia[ i ] * xi;
             for ( int e = M.rp[ i ]; e < M.rp[ i + 1 ]; ++e ) {
                 const int j = M.col[ e ];
-                float bj = top ? float( V->r[ j ] ) : M.b[ j ];
+                float bj = top ? ( V->mixed ? V->r32[ j ] : float( V->r[ j ] ) ) : M.b[ j ];
                 ax -= M.val[ e ] * OMEGA * M.dinv[ j ] * bj;
             }
             acc += bi - ax;
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ 
 // the coarsest level: x = inv b (one warp per problem)
 __global__ void __launch_bounds__( 32 ) k_mg_bottom( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs ) {
     const MgLevel &M = lv[ blockIdx.x ];
-    if ( vs[ M.vec ].sc[ SC_CONV ] != 0 ) return;
+    if ( vs[ M.vec ].sc[ SC_CONV ] != 0 || vs[ M.vec ].sc[ SC_REFINE ] != 0 ) return;
     const int n = M.n;
     for ( int i = threadIdx.x; i < n; i += 32 ) {
         float s = 0;
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
     const VecDev &V = vs[ M.vec ];
-    if ( V.sc[ SC_CONV ] != 0 ) return;
+    if ( V.sc[ SC_CONV ] != 0 || V.sc[ SC_REFINE ] != 0 ) return;
     const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
     for ( int i = ch.begin + int( threadIdx.x ) / MG_LANES; i < end; i += MGT / MG_LANES ) {
         const bool in = i < ch.end;
@@ -320,7 +320,10 @@ __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv
             const float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
             const float s = M.dia[ i ] * xi - t;
             const float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
-            if ( M.level == 0 ) V.z[ i ] = double( yi );
+            if ( M.level == 0 ) {
+                if ( V.mixed ) V.z32[ i ] = yi;
+                else V.z[ i ] = double( yi );
+            }
             else M.y[ i ] = yi;
         }
     }

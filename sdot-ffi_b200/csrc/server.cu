@@ -232,6 +232,8 @@ int32_t sdot_server_submit( sdot_server srv, const sdot_solve_desc *desc, int64_
         r->desc.diagram.density.masses = r->dv2.data();
     }
     r->bytes = sdot_solve_bytes( D.dim, n, &dd );
+    if ( desc->options[ SDOT_OPT_LIN_PRECISION ] == 1 )      // the FP32 copies of the mixed CG
+        r->bytes += uint64_t( n ) * ( ( D.dim == 2 ? CAP2 : CAP3 ) * 4 + 24 ) + 4096;
     {
         std::lock_guard<std::mutex> lock( srv->mu );
         r->ticket = srv->next_ticket++;

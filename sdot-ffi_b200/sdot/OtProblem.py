@@ -24,7 +24,7 @@ class Tuning:
                  t_min=1e-10, max_backtracks=60, restart_factor=4.0, mass_rtol=0.0,
                  residual="log", residual_power=0.5, residual_switch=2.0,
                  aggregation_margin=None, accelerator=None, memory=None, scratch_capacity=None, keep_start=False,
-                 linear_maxit=None):
+                 linear_maxit=None, linear_precision="fp64"):
         self.step = step
         self.linear_solver = linear_solver
         self.amg_variant = amg_variant
@@ -38,6 +38,11 @@ class Tuning:
         self.keep_start = bool(keep_start)
         self.accelerator, self.memory, self.scratch_capacity = accelerator, memory, scratch_capacity
         self.linear_maxit = linear_maxit
+        # this build's: "mixed" runs each Newton system's CG in FP32 (FP32 copies of the Laplacian and of the CG's vectors)
+        # inside an FP64 iterative refinement that keeps the solution and the residual in FP64
+        if linear_precision not in ("fp64", "mixed"):
+            raise ValueError(f"unknown linear_precision : {linear_precision!r} ( 'fp64' or 'mixed' )")
+        self.linear_precision = linear_precision
 
 
 class OtNotConverged(RuntimeError):

@@ -67,7 +67,8 @@ def solver_options(settings, n, d=None):
                 switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-6), lin_maxit=int(tun.linear_maxit or 20000),
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
-                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0, lin_precision=0,
+                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0,
+                lin_precision=1 if getattr(tun, "linear_precision", "fp64") == "mixed" else 0,
                 agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0),
                 step=_STEP[tun.step])
 

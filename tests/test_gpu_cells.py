@@ -233,8 +233,9 @@ def test_the_linear_solve_matches_a_direct_solve():
 
 @pytest.mark.parametrize("d,n", [(2, 40000), (3, 20000)])
 def test_both_linear_methods_match_a_direct_solve(d, n):
-    """sdot_linear_solve with method 0 (Jacobi-PCG) and 1 (multigrid-PCG, FP32 levels) on the Laplacian of a
-    Voronoi diagram, against scipy's direct solve of the gauge-fixed system, two right-hand sides"""
+    """sdot_linear_solve with method 0 (Jacobi-PCG), 1 (multigrid-PCG, FP32 levels), and 2 / 3 (the same with the CG in
+    FP32 inside an FP64 iterative refinement) on the Laplacian of a Voronoi diagram, against scipy's direct solve of the
+    gauge-fixed system, two right-hand sides: the refinement reaches the FP64 solves' 1e-8 of the solution's size"""
     import scipy.sparse as sp
     import scipy.sparse.linalg as sla
     from sdot import _lib
@@ -250,12 +251,13 @@ def test_both_linear_methods_match_a_direct_solve(d, n):
     for k in range(2):
         y[k, 1:] = lu.solve(b[k, 1:])
     its = {}
-    for method in (0, 1):
+    for method in (0, 1, 2, 3):
         x, it = _lib.linear_solve(row, cols, vals, dia, b, tol=1e-12, method=method)
         assert (x[:, 0] == 0).all()
         assert np.abs(x - y).max() < 1e-8 * np.abs(y).max(), method
         its[method] = np.asarray(it)
     assert (its[1] > 0).all() and (its[1] < its[0]).all(), its
+    assert (its[2] > 0).all() and (its[3] > 0).all() and (its[3] < its[2]).all(), its
 
 
 def test_the_adjoint_is_the_derivative_of_the_measures():

@@ -44,15 +44,43 @@ def test_plain_2d_fp64_n10000_matches_the_oracle():
 
 
 @pytest.mark.parametrize("lin", ["cg", "mg"])
-def test_both_linear_solvers_reach_the_same_plan(lin):
-    """tests/test_SdotPlanNd.py:536-561: the multigrid reaches the plan of the reference solver"""
+@pytest.mark.parametrize("lp", ["fp64", "mixed"])
+def test_both_linear_solvers_reach_the_same_plan(lin, lp):
+    """tests/test_SdotPlanNd.py:536-561: the multigrid reaches the plan of the reference solver; so does each of them with
+    its CG in FP32 inside an FP64 iterative refinement (`linear_precision = "mixed"`)"""
     rng = np.random.default_rng(50)
     n = 20000
     pos = rng.uniform(size=(n, 2))
-    plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-10, linear_solver=lin)))
+    plan = OtProblem(SumOfDiracs(pos), sdot.Box()).solve(
+        Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-10, linear_solver=lin, linear_precision=lp)))
     assert plan.converged
     ref = O.solve(pos, tol_abs=0.0, tol_rel=1e-10)
     assert np.abs(plan.weights - ref["weights"]).max() <= 1e-7 * np.abs(ref["weights"]).max()
+
+
+@pytest.mark.parametrize("d,gauss", [(2, True), (3, False), (3, True)])
+def test_the_mixed_cg_reaches_the_fp64_plan(d, gauss):
+    """`linear_precision = "mixed"` (the Newton systems' CG in FP32, refined in FP64) against the FP64 CG: both converge
+    to max |m - nu| / nu <= 1e-8, to the same weights within 1e-7 of max |w|, and the oracle's diagram at the mixed
+    solve's weights confirms its masses (a constant density: the oracle's 3D gaussian quadrature is too slow here)"""
+    rng = np.random.default_rng(60 + d)
+    n = 6000 if d == 2 else 3000
+    pos = rng.uniform(size=(n, d))
+    target = sdot.Box(nb_dims=d)
+    if gauss:
+        c = rng.uniform(0.3, 0.7, size=(3, d))
+        target = sdot.SumOfGaussians(c, np.array([0.1, 0.15, 0.12]), np.full(3, 1 / 3), support_box=(np.zeros(d), np.ones(d)))
+    plans = {lp: OtProblem(SumOfDiracs(pos), target).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-8, linear_precision=lp)))
+             for lp in ("fp64", "mixed")}
+    for lp, plan in plans.items():
+        assert plan.converged, (lp, plan.stats["status"])
+        nu = np.asarray(plan.target_masses).reshape(-1)
+        assert np.abs(plan.cell_masses / nu - 1).max() <= 1e-8, lp
+    w64, wmx = plans["fp64"].weights, plans["mixed"].weights
+    assert np.abs(wmx - w64).max() <= 1e-7 * np.abs(w64).max()
+    if not gauss:
+        chk = O.cells(pos, wmx)["mass"]
+        assert np.abs(chk * n - 1).max() <= 1e-8
 
 
 def test_a_solve_in_a_batch_is_the_solve_alone():

@@ -51,8 +51,8 @@ def test_the_server_returns_the_plans_of_the_batched_solve():
 
 
 def test_the_unbuilt_precisions_are_refused():
-    """no silent FP64 in place of the FP32-clip variant or of an FP32 CG: `precision` 1 of a cells call, and the
-    `precision` / `lin_precision` options of a solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch"""
+    """no silent FP64 in place of the FP32-clip variant: `precision` 1 of a cells call, and the `precision` option of a
+    solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch; `lin_precision` 2 is an argument error"""
     import ctypes
     from sdot import _lib
     from sdot.SdotPlanNd import solver_options
@@ -64,10 +64,12 @@ def test_the_unbuilt_precisions_are_refused():
     out = _lib.CellsOut(masses=m.ctypes.data, precision=1)
     st = _lib.Status()
     assert _lib.load().sdot_cells(_lib.context(), ctypes.byref(desc), ctypes.byref(out), ctypes.byref(st)) == _lib.SDOT_ERR_UNSUPPORTED
-    for key in ("precision", "lin_precision"):
-        opts = dict(solver_options(Iterative(), 200), **{key: 1})
-        r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
-        assert isinstance(r, NotImplementedError), r
+    opts = dict(solver_options(Iterative(), 200), precision=1)
+    r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
+    assert isinstance(r, NotImplementedError), r
+    opts = dict(solver_options(Iterative(), 200), lin_precision=2)
+    r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
+    assert isinstance(r, ValueError), r
     assert np.abs(_pd(pos).measures.sum() - 1) < 1e-12          # the context is still usable
 
 
