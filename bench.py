@@ -91,6 +91,20 @@ def stream(seed, count, probe):
     return out, skipped
 
 
+def sixteen_gaussians_image(rng, res=1024):
+    """the image target of the 2D Newton workload: 16 isotropic gaussians (centres uniform, sigma uniform in [0.02, 0.1],
+    amplitudes uniform in [0.5, 2]) at the pixel centres of [0,1]^2, plus 1 % of the peak"""
+    c = rng.uniform(size=(16, 2))
+    s = rng.uniform(0.02, 0.1, size=16)
+    a = rng.uniform(0.5, 2.0, size=16)
+    xs = (np.arange(res) + 0.5) / res
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    v = np.zeros((res, res))
+    for k in range(16):
+        v += a[k] * np.exp(-((X - c[k, 0]) ** 2 + (Y - c[k, 1]) ** 2) / (2 * s[k] ** 2))
+    return v + 0.01 * v.max()
+
+
 def settings():
     from sdot import Iterative, Tuning
     return Iterative(tol=0.0, on_failure="ignore", tuning=Tuning(mass_rtol=RTOL))
@@ -399,8 +413,9 @@ def main():
     ap.add_argument("--cells-only", type=int, default=0, help="diagrams of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--cells-dim", type=int, default=2)
     ap.add_argument("--cells-repeat", type=int, default=0)
-    ap.add_argument("--cells-density", default="uniform", choices=["uniform", "gauss"],
-                    help="cells-only target: uniform, or a 4-gaussian mixture like the stream's")
+    ap.add_argument("--cells-density", default="uniform", choices=["uniform", "gauss", "image16"],
+                    help="cells-only / solve-only target: uniform, a 4-gaussian mixture like the stream's, or (2D solve-only) the "
+                         "1024 x 1024 image of 16 gaussians plus a 1 %% floor")
     ap.add_argument("--solve-only", type=int, default=0, help="one solve of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--solve-linear", default="auto", choices=["auto", "cg", "mg"])
     ap.add_argument("--solve-step", default="auto", choices=["auto", "trials", "limits"])
@@ -418,6 +433,8 @@ def main():
         if a.cells_density == "gauss":
             rq = request(a.seed, 0)
             dist = target_of(dict(rq, d=d, gauss=True, c=np.random.default_rng(a.seed + 2).uniform(0.2, 0.8, size=(4, d))))
+        if a.cells_density == "image16":
+            dist = sdot.Image(sixteen_gaussians_image(np.random.default_rng(a.seed + 3)), frame=[1 / 1024, 1 / 1024])
         _lib.set_timing(True)
         t0 = time.perf_counter()
         plan = OtProblem(SumOfDiracs(pos), dist).solve(Iterative(tol=0.0, tuning=Tuning(mass_rtol=RTOL, linear_solver=a.solve_linear,

@@ -49,6 +49,9 @@ def lib():
         P = ctypes.c_void_p
         L.od_cells.restype = ctypes.c_int
         L.od_cells.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
+        L.od_cells_rows.restype = ctypes.c_int
+        L.od_cells_rows.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, ctypes.c_int, P, P, ctypes.c_long, P, P, P, P, ctypes.c_int, P, P, P,
+                                    P, P, P]
         L.od_solve.restype = ctypes.c_int
         L.od_solve.argtypes = [ctypes.c_int, ctypes.c_long, P, P, P, P, ctypes.c_int, P, P, P, P, P, P, P, P, P, ctypes.c_long, P, P]
         L.od_laplacian_solve.restype = ctypes.c_int
@@ -112,6 +115,27 @@ def cells(pos, weights=None, box=None, density=None, brute=False, cap=64, want=(
     st = lib().od_cells(d, n, _p(pos), _p(w), _p(bx), kind, _p(par), _p(val), int(bool(brute)), _p(out["mass"]), _p(out["bary"]),
                         _p(out["cost"]), cap, _p(out["nb"]), _p(out["nid"]), _p(out["nc"]), _p(out["nm"]), _p(out["nvert"]),
                         ctypes.byref(bad))
+    out["status"], out["bad"] = st, bad.value
+    return out
+
+
+def cells_rows(pos, rows, weights=None, box=None, density=None, cap=64):
+    """the cells `rows` of the diagram of all of `pos` (the same outputs as `cells`, one row per entry of `rows`)"""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n, d = pos.shape
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    k = len(rows)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    if box is None:
+        box = (np.zeros(d), np.ones(d))
+    bx = np.ascontiguousarray(np.concatenate([np.asarray(box[0], float), np.asarray(box[1], float)]))
+    kind, par, val = encode_density(density, d)
+    out = dict(mass=np.zeros(k), bary=np.zeros((k, d)), cost=np.zeros(k), nb=np.zeros(k, dtype=np.int32), nid=np.zeros((k, cap), dtype=np.int32),
+               nc=np.zeros((k, cap)), nm=np.zeros((k, cap)), nvert=np.zeros(k, dtype=np.int32))
+    bad = ctypes.c_long(-1)
+    st = lib().od_cells_rows(d, n, _p(pos), _p(w), _p(bx), kind, _p(par), _p(val), k, _p(rows), _p(out["mass"]), _p(out["bary"]),
+                             _p(out["cost"]), cap, _p(out["nb"]), _p(out["nid"]), _p(out["nc"]), _p(out["nm"]), _p(out["nvert"]),
+                             ctypes.byref(bad))
     out["status"], out["bad"] = st, bad.value
     return out
 

@@ -486,32 +486,32 @@ static int cell2( const od_pb *pb, long i, int brute, poly2 *P, poly2 *T ) {
     return OD_OK;
 }
 
-static int write2( const od_pb *pb, long i, const poly2 *P, const od_out *o ) {
+static int write2( const od_pb *pb, long i, long oi, const poly2 *P, const od_out *o ) {
     const double px = pb->pos[ 2 * i ], py = pb->pos[ 2 * i + 1 ];
     double M, Fx, Fy, S;
     dens_cell2( pb, P, px, py, &M, &Fx, &Fy, &S );
-    if ( o->mass ) o->mass[ i ] = M;
+    if ( o->mass ) o->mass[ oi ] = M;
     if ( o->bary ) {
-        o->bary[ 2 * i ] = M > 0 ? px + Fx / M : px;
-        o->bary[ 2 * i + 1 ] = M > 0 ? py + Fy / M : py;
+        o->bary[ 2 * oi ] = M > 0 ? px + Fx / M : px;
+        o->bary[ 2 * oi + 1 ] = M > 0 ? py + Fy / M : py;
     }
-    if ( o->cost ) o->cost[ i ] = S;
-    if ( o->nvert ) o->nvert[ i ] = P->m;
+    if ( o->cost ) o->cost[ oi ] = S;
+    if ( o->nvert ) o->nvert[ oi ] = P->m;
     if ( o->nb ) {
         int c = 0;
         for ( int k = 0; k < P->m; ++k ) {
             int j = P->id[ k ];
             if ( j < 0 ) continue;
-            if ( c >= o->cap ) { o->nb[ i ] = c; return OD_ERR_NEIGHBOURS; }
+            if ( c >= o->cap ) { o->nb[ oi ] = c; return OD_ERR_NEIGHBOURS; }
             int k1 = k + 1 == P->m ? 0 : k + 1;
             double meas = dens_edge2( pb, P->x[ k ] + px, P->y[ k ] + py, P->x[ k1 ] + px, P->y[ k1 ] + py );
             double dx = pb->pos[ 2 * j ] - px, dy = pb->pos[ 2 * j + 1 ] - py;
-            o->nid[ ( long ) i * o->cap + c ] = j;
-            o->nm[ ( long ) i * o->cap + c ] = meas;
-            o->nc[ ( long ) i * o->cap + c ] = meas / ( 2 * sqrt( dx * dx + dy * dy ) );
+            o->nid[ ( long ) oi * o->cap + c ] = j;
+            o->nm[ ( long ) oi * o->cap + c ] = meas;
+            o->nc[ ( long ) oi * o->cap + c ] = meas / ( 2 * sqrt( dx * dx + dy * dy ) );
             ++c;
         }
-        o->nb[ i ] = c;
+        o->nb[ oi ] = c;
     }
     return OD_OK;
 }
@@ -869,7 +869,7 @@ static int cell3( const od_pb *pb, long i, int brute, poly3 *P ) {
     return OD_OK;
 }
 
-static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
+static int write3( const od_pb *pb, long i, long oi, const poly3 *P, const od_out *o ) {
     const double *p = pb->pos + 3 * i;
     double V, F[ 3 ], S, M;
     const int gauss = pb->dkind == DENS_GAUSS;
@@ -883,28 +883,28 @@ static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
         M = r * V;
         S *= r;
     }
-    if ( o->mass ) o->mass[ i ] = M;
-    if ( o->bary ) for ( int a = 0; a < 3; ++a ) o->bary[ 3 * i + a ] = V > 0 ? p[ a ] + F[ a ] / V : p[ a ];
-    if ( o->cost ) o->cost[ i ] = S;
+    if ( o->mass ) o->mass[ oi ] = M;
+    if ( o->bary ) for ( int a = 0; a < 3; ++a ) o->bary[ 3 * oi + a ] = V > 0 ? p[ a ] + F[ a ] / V : p[ a ];
+    if ( o->cost ) o->cost[ oi ] = S;
     if ( o->nvert ) {
         int nv = 0;
         for ( int f = 0; f < P->nf; ++f ) nv += P->nv[ f ];
-        o->nvert[ i ] = nv;
+        o->nvert[ oi ] = nv;
     }
     if ( o->nb ) {
         int c = 0;
         for ( int f = 0; f < P->nf; ++f ) {
             int j = P->id[ f ];
             if ( j < 0 ) continue;
-            if ( c >= o->cap ) { o->nb[ i ] = c; return OD_ERR_NEIGHBOURS; }
+            if ( c >= o->cap ) { o->nb[ oi ] = c; return OD_ERR_NEIGHBOURS; }
             double meas = gauss ? gauss_face3( pb, P, f, p ) : r * face_area3( P, f );
             double q[ 3 ] = { pb->pos[ 3 * j ] - p[ 0 ], pb->pos[ 3 * j + 1 ] - p[ 1 ], pb->pos[ 3 * j + 2 ] - p[ 2 ] };
-            o->nid[ ( long ) i * o->cap + c ] = j;
-            o->nm[ ( long ) i * o->cap + c ] = meas;
-            o->nc[ ( long ) i * o->cap + c ] = meas / ( 2 * sqrt( dot3( q, q ) ) );
+            o->nid[ ( long ) oi * o->cap + c ] = j;
+            o->nm[ ( long ) oi * o->cap + c ] = meas;
+            o->nc[ ( long ) oi * o->cap + c ] = meas / ( 2 * sqrt( dot3( q, q ) ) );
             ++c;
         }
-        o->nb[ i ] = c;
+        o->nb[ oi ] = c;
     }
     return OD_OK;
 }
@@ -912,26 +912,29 @@ static int write3( const od_pb *pb, long i, const poly3 *P, const od_out *o ) {
 /* ------------------------------------------------------------------------------------------------ */
 /* one diagram: every cell, in parallel                                                           */
 /* ------------------------------------------------------------------------------------------------ */
-static int diagram( od_pb *pb, int brute, const od_out *o, long *bad ) {
+/* `rows` (NULL: every cell) the cells to compute, `nrows` of them, output k for cell rows[ k ] */
+static int diagram_rows( od_pb *pb, int brute, const od_out *o, long nrows, const long *rows, long *bad ) {
     int status = OD_OK;
     long first_bad = -1;
     if ( pb->dim == 3 && pb->dkind == DENS_IMAGE ) return OD_ERR_UNSUPPORTED;
     gl_init();
     build_grid( pb );
+    const long count = rows ? nrows : pb->n;
 #pragma omp parallel
     {
         void *buf = malloc( pb->dim == 2 ? 2 * sizeof( poly2 ) : sizeof( poly3 ) );
 #pragma omp for schedule( dynamic, 4 )
-        for ( long i = 0; i < pb->n; ++i ) {
+        for ( long k = 0; k < count; ++k ) {
+            const long i = rows ? rows[ k ] : k;
             int st;
             if ( pb->dim == 2 ) {
                 poly2 *P = ( poly2 * ) buf, *T = P + 1;
                 st = cell2( pb, i, brute, P, T );
-                if ( st == OD_OK ) st = write2( pb, i, P, o );
+                if ( st == OD_OK ) st = write2( pb, i, k, P, o );
             } else {
                 poly3 *P = ( poly3 * ) buf;
                 st = cell3( pb, i, brute, P );
-                if ( st == OD_OK ) st = write3( pb, i, P, o );
+                if ( st == OD_OK ) st = write3( pb, i, k, P, o );
             }
             if ( st != OD_OK ) {
 #pragma omp critical
@@ -944,6 +947,8 @@ static int diagram( od_pb *pb, int brute, const od_out *o, long *bad ) {
     if ( bad ) *bad = first_bad;
     return status;
 }
+
+static int diagram( od_pb *pb, int brute, const od_out *o, long *bad ) { return diagram_rows( pb, brute, o, 0, NULL, bad ); }
 
 static void init_pb( od_pb *pb, int dim, long n, const double *pos, const double *w, const double *box, int dkind, const double *dpar, const double *dval ) {
     memset( pb, 0, sizeof( *pb ) );
@@ -960,6 +965,20 @@ int od_cells( int dim, long n, const double *pos, const double *w, const double 
     init_pb( &pb, dim, n, pos, w, box, dkind, dpar, dval );
     od_out o = { mass, bary, cost, cap, nb, nid, nc, nm, nvert };
     return diagram( &pb, brute, &o, bad );
+}
+
+/* THE CELLS of a subset: the diagram of all the seeds, computed for cells rows[ 0 .. nrows ) only; output k (every output
+   array holds nrows rows) is cell rows[ k ]'s; `bad` the first failing seed */
+int od_cells_rows( int dim, long n, const double *pos, const double *w, const double *box, int dkind, const double *dpar,
+                   const double *dval, long nrows, const long *rows, double *mass, double *bary, double *cost, int cap, int *nb, int *nid,
+                   double *nc, double *nm, int *nvert, long *bad ) {
+    if ( dim != 2 && dim != 3 ) return OD_ERR_ARGS;
+    for ( long k = 0; k < nrows; ++k )
+        if ( rows[ k ] < 0 || rows[ k ] >= n ) return OD_ERR_ARGS;
+    od_pb pb;
+    init_pb( &pb, dim, n, pos, w, box, dkind, dpar, dval );
+    od_out o = { mass, bary, cost, cap, nb, nid, nc, nm, nvert };
+    return diagram_rows( &pb, 0, &o, nrows, rows, bad );
 }
 
 int od_max_threads( void ) {

@@ -541,6 +541,7 @@ struct SolveJob {
     double polish_before = 0;           // ... and the members' residual before the current one
     // lin_precision 1: the FP32 copies of the inner CG (matrix values [n * cap], diagonal and five vectors [n])
     char *mx_mem = nullptr;
+    bool mx_off = false;                // set once a refinement stalled: this solve's later systems take the FP64 CG
     float *val32 = nullptr, *dia32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr;
 };
 
@@ -1347,7 +1348,13 @@ static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
         if ( S[ SC_CONV ] != 0 ) {
             J.stats[ ST_LIN_NB_ITER ] += S[ SC_ITER ];
             if ( S[ SC_BNORM ] > 0 ) J.stats[ ST_LIN_WORST ] = std::max( J.stats[ ST_LIN_WORST ], S[ SC_RNORM ] / S[ SC_BNORM ] );
-            if ( S[ SC_FAIL ] != 0 ) {
+            if ( S[ SC_FAIL ] != 0 && J.mx_mem && ! J.mx_off ) {
+                // the FP32 CG failed on this system (its refinement stalled, or p . A p lost its sign to FP32 rounding):
+                // it is solved again by the FP64 CG (its FP32 multigrid levels inside an FP64 CG), and so are the later
+                // systems of this solve
+                J.mx_off = true;
+                J.pend |= P_NEWTON;
+            } else if ( S[ SC_FAIL ] != 0 ) {
                 J.nstatus = NS_LINEAR_FAILURE;
                 end_stage( c, J );
             } else {
@@ -1397,7 +1404,7 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
     V.nchunk = J.nch_vec;
     V.active = 1;
     V.precond = J.mg_L > 0 ? 1 : 0;
-    if ( J.mx_mem ) {
+    if ( J.mx_mem && ! J.mx_off ) {
         V.mixed = 1;
         V.val32 = J.val32; V.dia32 = J.dia32; V.x32 = J.x32; V.r32 = J.r32; V.z32 = J.z32; V.p32 = J.p32; V.q32 = J.q32;
     }

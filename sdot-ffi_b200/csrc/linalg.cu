@@ -454,7 +454,9 @@ void launch_cg_rz_p( const Launch &L, const VecDev *v, const Chunk *ch, int nch 
 // the bytes of every product and update.  x, the residual r and b stay FP64.  When the inner residual has fallen by
 // MX_INNER (or under half the outer target), x += e in FP64, the residual r = b - A x is recomputed with the FP64 matrix,
 // and the inner CG restarts on it; the outer stop is the FP64 residual's, tol |b|.  A refinement that does not cut the
-// FP64 residual by 10 % is a linear failure (FP32 cannot resolve the system).
+// FP64 residual by 10 % ends the solve with SC_FAIL = 2: the refinement stalls once the condition number times the FP32
+// rounding reaches 1 (the FP32 matrix and products then perturb the system by more than the inner CG gains), as on the
+// Laplacians of a million seeds under a density that varies a hundredfold.
 // Everything runs inside the ordinary sequence of CG launches (so a burst, and its CUDA graph, is unchanged), steered by
 // the problem's scalars: the update's fold sets SC_REFINE; the next p kernel adds e to x instead of updating p; the next
 // product computes the FP64 residual instead of q, resets e and p to 0 and sets alpha = 0, rz = 1 -- so that the
@@ -564,7 +566,7 @@ __global__ void __launch_bounds__( VT ) k_mx_spmv( const VecDev *__restrict__ vs
             V.sc[ SC_NREF ] += 1;
             V.sc[ SC_REFINE ] = 0;
             if ( rn <= V.tol * V.sc[ SC_BNORM ] ) V.sc[ SC_CONV ] = 1;
-            else if ( ! ( rn < 0.9 * V.sc[ SC_RPREV ] ) ) { V.sc[ SC_FAIL ] = 1; V.sc[ SC_CONV ] = 2; }
+            else if ( ! ( rn < 0.9 * V.sc[ SC_RPREV ] ) ) { V.sc[ SC_FAIL ] = 2; V.sc[ SC_CONV ] = 2; }    // (2: the refinement stalls)
             else {
                 V.sc[ SC_RPREV ] = rn;
                 V.sc[ SC_IN0 ] = sqrt( tot[ 1 ] );
