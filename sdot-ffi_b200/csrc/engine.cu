@@ -1428,10 +1428,16 @@ struct VecBatch {
     std::vector<MgLevel> lv[ MG_MAX_LEVELS ];
     std::vector<Chunk> down[ MG_MAX_LEVELS ], up[ MG_MAX_LEVELS ], crs[ MG_MAX_LEVELS ];
     std::vector<MgLevel> bottom;
+    // the cycle's small levels (at most MG_FUSE_ROWS rows, down to the coarsest): one fused launch, a block per problem
+    std::vector<MgLevel> fchain;
+    std::vector<int2> fidx;
+    std::vector<Chunk> build0;                     // the level-0 rows of every problem, for the hierarchy's build
     // device copies
     VecDev *dv = nullptr;
     Chunk *dch = nullptr;
-    MgLevel *dlv[ MG_MAX_LEVELS ], *dbottom = nullptr;
+    MgLevel *dlv[ MG_MAX_LEVELS ], *dbottom = nullptr, *dfchain = nullptr;
+    int2 *dfidx = nullptr;
+    Chunk *dbuild0 = nullptr;
     Chunk *ddown[ MG_MAX_LEVELS ], *dup[ MG_MAX_LEVELS ], *dcrs[ MG_MAX_LEVELS ];
 
     void add( const VecDev &d, const SolveJob *J = nullptr ) {
@@ -1444,18 +1450,28 @@ struct VecBatch {
         for ( int b = 0; b < d.n; b += VCHUNK, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + VCHUNK ), k } );
         if ( ! J || ! J->mg_L || ! d.precond ) return;
         maxL = std::max( maxL, J->mg_L );
+        int f = J->mg_L - 1;                       // the first level of the fused part: at most MG_FUSE_ROWS rows
+        while ( f > 0 && J->mg_n[ f - 1 ] <= MG_FUSE_ROWS ) --f;
+        fidx.push_back( make_int2( int( fchain.size() ), J->mg_L - f ) );
         for ( int l = 0; l < J->mg_L; ++l ) {
             int q = int( lv[ l ].size() );
             lv[ l ].push_back( mg_level( *J, l, p ) );
+            if ( l >= f ) fchain.push_back( lv[ l ].back() );
+            if ( l == 0 ) {
+                int kk = 0;
+                for ( int b = 0; b < J->mg_n[ 0 ]; b += VCHUNK, ++kk ) build0.push_back( Chunk{ q, b, std::min( J->mg_n[ 0 ], b + VCHUNK ), kk } );
+            }
             if ( l + 1 < J->mg_L ) {
                 const int nn = J->mg_n[ l + 1 ];
                 int kk = 0;
-                for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
+                if ( l < f )
+                    for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
                 kk = 0;
                 for ( int b = 0; b < nn; b += MG_CCH, ++kk ) crs[ l ].push_back( Chunk{ q, b, std::min( nn, b + MG_CCH ), kk } );
                 kk = 0;
                 const int n = J->mg_n[ l ];
-                for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
+                if ( l < f )
+                    for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
             } else
                 bottom.push_back( lv[ l ].back() );
         }
@@ -1471,6 +1487,8 @@ struct VecBatch {
             k.push_back( ( long long ) up[ l ].size() );
             k.push_back( ( long long ) crs[ l ].size() );
         }
+        k.push_back( ( long long ) fchain.size() );
+        k.push_back( ( long long ) fidx.size() );
         return k;
     }
     // everything in one copy
@@ -1485,6 +1503,9 @@ struct VecBatch {
             parts.push_back( { crs[ l ].data(), crs[ l ].size() * sizeof( Chunk ) } );
         }
         parts.push_back( { bottom.data(), bottom.size() * sizeof( MgLevel ) } );
+        parts.push_back( { fchain.data(), fchain.size() * sizeof( MgLevel ) } );
+        parts.push_back( { fidx.data(), fidx.size() * sizeof( int2 ) } );
+        parts.push_back( { build0.data(), build0.size() * sizeof( Chunk ) } );
         std::vector<size_t> off;
         size_t total = 0;
         for ( auto &p : parts ) { off.push_back( total ); total += ( p.second + 255 ) & ~size_t( 255 ); }
@@ -1501,20 +1522,23 @@ struct VecBatch {
             dcrs[ l ] = reinterpret_cast<Chunk *>( d + off[ k++ ] );
         }
         dbottom = reinterpret_cast<MgLevel *>( d + off[ k++ ] );
+        dfchain = reinterpret_cast<MgLevel *>( d + off[ k++ ] );
+        dfidx = reinterpret_cast<int2 *>( d + off[ k++ ] );
+        dbuild0 = reinterpret_cast<Chunk *>( d + off[ k++ ] );
     }
     // the hierarchies of every job, from their fresh Laplacians
     void build( const Launch &L, ErrRec *err ) {
         if ( ! mg() ) return;
         std::vector<Chunk> l0;
         // level 0 rows: the vector chunks, re-indexed to the level-0 array
-        launch_mg_level0( L, dlv[ 0 ], dv, dup[ 0 ], int( up[ 0 ].size() ) );
+        launch_mg_level0( L, dlv[ 0 ], dv, dbuild0, int( build0.size() ) );
         for ( int l = 0; l + 1 < maxL; ++l ) launch_mg_coarsen( L, dlv[ l ], int( lv[ l ].size() ), dcrs[ l ], int( crs[ l ].size() ), err );
         launch_mg_bottom_build( L, dbottom, int( bottom.size() ) );
     }
     // z = M^-1 r for every job
     void vcycle( const Launch &L ) {
         for ( int l = 0; l + 1 < maxL; ++l ) launch_mg_down( L, dlv[ l ], dv, ddown[ l ], int( down[ l ].size() ) );
-        launch_mg_bottom( L, dbottom, dv, int( bottom.size() ) );
+        launch_mg_fused( L, dfchain, dfidx, dv, int( fidx.size() ) );
         for ( int l = maxL - 2; l >= 0; --l ) launch_mg_up( L, dlv[ l ], dv, dup[ l ], int( up[ l ].size() ) );
     }
 };

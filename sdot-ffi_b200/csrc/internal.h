@@ -203,7 +203,8 @@ enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, S
                     SC_RPREV,       // mixed CG: the FP64 residual norm of the last refinement
                     SC_NREF,        // mixed CG: refinements so far
                     NB_SC };
-constexpr int VCHUNK = 1024;     // rows per chunk of the vector kernels
+constexpr int VCHUNK = 256;      // rows per chunk of the vector kernels (one block each: many blocks keep loads in flight)
+constexpr int MG_FUSE_ROWS = 4096;   // multigrid levels of at most this many rows run in one launch per problem (k_mg_fused)
 
 // ---- warp helpers ------------------------------------------------------------------------------------
 SDOT_DEV double warp_sum( double v ) {
@@ -395,6 +396,9 @@ void launch_mg_bottom_build( const Launch &L, const MgLevel *lv, int nprob );
 void launch_mg_down( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
 void launch_mg_bottom( const Launch &L, const MgLevel *lv, const VecDev *vs, int nprob );
 void launch_mg_up( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch );
+// the levels of at most MG_FUSE_ROWS rows of each problem, down, bottom and up, one block per problem: chain holds those
+// levels of every problem, idx[ p ] = ( first, count )
+void launch_mg_fused( const Launch &L, const MgLevel *chain, const int2 *idx, const VecDev *vs, int nprob );
 void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 
 // cells2d.cu / cells3d.cu

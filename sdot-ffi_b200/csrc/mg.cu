@@ -255,18 +255,15 @@ __device__ __forceinline__ int lane_rows_end( const Chunk &ch ) {
     return ch.begin + ( ( ch.end - ch.begin + per - 1 ) / per ) * per;
 }
 
-// pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level; MG_LANES lanes per coarse
-// row, each lane every MG_LANES-th of its fine rows
-__global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
-                                                   int nch ) {
-    const Chunk ch = chunks[ blockIdx.x ];
-    const MgLevel &M = lv[ ch.prob ];
+// pre-smoothing from zero (x = w D^-1 b), the residual and its restriction to the next level, for the coarse rows
+// [ I0, I1 ) of level M: MG_LANES lanes per coarse row (thread t of nt; nt a multiple of 32), each lane every MG_LANES-th of
+// its fine rows; every lane of a warp reaches each shuffle
+__device__ __forceinline__ void mg_down_rows( const MgLevel &M, const VecDev *V, int I0, int I1, int t, int nt ) {
     const bool top = M.level == 0;
-    const VecDev *V = vs + M.vec;
-    if ( V->sc[ SC_CONV ] != 0 || V->sc[ SC_REFINE ] != 0 ) return;
-    const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
-    for ( int I = ch.begin + int( threadIdx.x ) / MG_LANES; I < end; I += MGT / MG_LANES ) {
-        const bool in = I < ch.end;
+    const int sub = t % MG_LANES, per = nt / MG_LANES;
+    const int end = I0 + ( ( I1 - I0 + per - 1 ) / per ) * per;
+    for ( int I = I0 + t / MG_LANES; I < end; I += per ) {
+        const bool in = I < I1;
         const int i0 = I * M.pack, i1 = in ? min( M.n, i0 + M.pack ) : i0;
         float acc = 0;
         for ( int i = i0 + sub; i < i1; i += MG_LANES ) {
@@ -287,46 +284,96 @@ __global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ 
     }
 }
 
-// the coarsest level: x = inv b (one warp per problem)
-__global__ void __launch_bounds__( 32 ) k_mg_bottom( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs ) {
-    const MgLevel &M = lv[ blockIdx.x ];
-    if ( vs[ M.vec ].sc[ SC_CONV ] != 0 || vs[ M.vec ].sc[ SC_REFINE ] != 0 ) return;
+// prolongation of the next level's solution and post-smoothing for the fine rows [ i0, i1 ) of level M; level 0 writes z
+// (FP64, or z32 for the mixed CG); MG_LANES lanes per fine row
+__device__ __forceinline__ void mg_up_rows( const MgLevel &M, const VecDev &V, int i0, int i1, int t, int nt ) {
+    const int sub = t % MG_LANES, per = nt / MG_LANES;
+    const int end = i0 + ( ( i1 - i0 + per - 1 ) / per ) * per;
+    for ( int i = i0 + t / MG_LANES; i < end; i += per ) {
+        const bool in = i < i1;
+        const int r = in ? i : i0;
+        float s = 0;
+        for ( int e = M.rp[ r ] + sub; e < M.rp[ r + 1 ]; e += MG_LANES ) {
+            const int j = M.col[ e ];
+            s += M.val[ e ] * ( M.x[ j ] + ALPHA * M.xn[ j / M.pack ] );
+        }
+        s = lanes_sum( s );
+        if ( in && sub == 0 ) {
+            const float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
+            const float ai = M.dia[ i ] * xi - s;
+            const float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - ai );
+            if ( M.level == 0 ) {
+                if ( V.mixed ) V.z32[ i ] = yi;
+                else V.z[ i ] = double( yi );
+            } else
+                M.y[ i ] = yi;
+        }
+    }
+}
+
+// the coarsest level: y = inv b
+__device__ __forceinline__ void mg_bottom_rows( const MgLevel &M, int t, int nt ) {
     const int n = M.n;
-    for ( int i = threadIdx.x; i < n; i += 32 ) {
+    for ( int i = t; i < n; i += nt ) {
         float s = 0;
         for ( int j = 0; j < n; ++j ) s += M.inv[ i * n + j ] * M.b[ j ];
         M.y[ i ] = s;
     }
 }
 
-// prolongation of the next level's solution and post-smoothing; level 0 writes z (FP64); MG_LANES lanes per fine row
+__device__ __forceinline__ bool mg_idle( const VecDev &V ) { return V.sc[ SC_CONV ] != 0 || V.sc[ SC_REFINE ] != 0; }
+
+__global__ void __launch_bounds__( MGT ) k_mg_down( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
+                                                   int nch ) {
+    const Chunk ch = chunks[ blockIdx.x ];
+    const MgLevel &M = lv[ ch.prob ];
+    const VecDev *V = vs + M.vec;
+    if ( mg_idle( *V ) ) return;
+    mg_down_rows( M, V, ch.begin, ch.end, threadIdx.x, MGT );
+}
+
+// the coarsest level: x = inv b (one warp per problem)
+__global__ void __launch_bounds__( 32 ) k_mg_bottom( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs ) {
+    const MgLevel &M = lv[ blockIdx.x ];
+    if ( mg_idle( vs[ M.vec ] ) ) return;
+    mg_bottom_rows( M, threadIdx.x, 32 );
+}
+
 __global__ void __launch_bounds__( MGT ) k_mg_up( const MgLevel *__restrict__ lv, const VecDev *__restrict__ vs, const Chunk *__restrict__ chunks,
                                                  int nch ) {
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
     const VecDev &V = vs[ M.vec ];
-    if ( V.sc[ SC_CONV ] != 0 || V.sc[ SC_REFINE ] != 0 ) return;
-    const int sub = threadIdx.x % MG_LANES, end = lane_rows_end( ch );
-    for ( int i = ch.begin + int( threadIdx.x ) / MG_LANES; i < end; i += MGT / MG_LANES ) {
-        const bool in = i < ch.end;
-        const int r = in ? i : ch.begin;
-        float t = 0;
-        for ( int e = M.rp[ r ] + sub; e < M.rp[ r + 1 ]; e += MG_LANES ) {
-            const int j = M.col[ e ];
-            t += M.val[ e ] * ( M.x[ j ] + ALPHA * M.xn[ j / M.pack ] );
-        }
-        t = lanes_sum( t );
-        if ( in && sub == 0 ) {
-            const float xi = M.x[ i ] + ALPHA * M.xn[ i / M.pack ];
-            const float s = M.dia[ i ] * xi - t;
-            const float yi = xi + OMEGA * M.dinv[ i ] * ( M.b[ i ] - s );
-            if ( M.level == 0 ) {
-                if ( V.mixed ) V.z32[ i ] = yi;
-                else V.z[ i ] = double( yi );
-            }
-            else M.y[ i ] = yi;
-        }
+    if ( mg_idle( V ) ) return;
+    mg_up_rows( M, V, ch.begin, ch.end, threadIdx.x, MGT );
+}
+
+// THE SMALL LEVELS OF A CYCLE IN ONE LAUNCH: one block per problem walks its levels from the first one of at most
+// MG_FUSE_ROWS rows down to the coarsest and back up (chain[ first .. first + count ), `idx` per problem), the block's
+// threads synchronised between levels.  A launch per level and direction there would cost more in launch latency than
+// the levels cost in work (a few thousand rows each, most of them a few hundred).
+constexpr int MGF = 1024;
+__global__ void __launch_bounds__( MGF ) k_mg_fused( const MgLevel *__restrict__ chain, const int2 *__restrict__ idx, const VecDev *__restrict__ vs ) {
+    const int2 c = idx[ blockIdx.x ];
+    const MgLevel *L = chain + c.x;
+    const VecDev &V = vs[ L[ 0 ].vec ];
+    if ( mg_idle( V ) ) return;                 // (block-uniform: one problem per block)
+    for ( int k = 0; k + 1 < c.y; ++k ) {
+        mg_down_rows( L[ k ], &V, 0, L[ k ].nn, threadIdx.x, MGF );
+        __syncthreads();
     }
+    mg_bottom_rows( L[ c.y - 1 ], threadIdx.x, MGF );
+    __syncthreads();
+    for ( int k = c.y - 2; k >= 0; --k ) {
+        mg_up_rows( L[ k ], V, 0, L[ k ].n, threadIdx.x, MGF );
+        __syncthreads();
+    }
+}
+
+void launch_mg_fused( const Launch &L, const MgLevel *chain, const int2 *idx, const VecDev *vs, int nprob ) {
+    if ( nprob <= 0 ) return;
+    k_mg_fused<<<nprob, MGF, 0, L.stream>>>( chain, idx, vs );
+    ++*L.launches;
 }
 
 void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, const Chunk *ch, int nch ) {

@@ -5,7 +5,7 @@ The Laplacian is a weighted 250 x 200 grid graph (50,000 rows, random positive c
 must match the allocating entry point within |x - x_ref| <= 1e-9 max|x_ref| (the rhs mean is summed in a
 different order), use the same CG iteration counts (+-1), leave the device's free memory unchanged, and a size past
 SDOT_NOALLOC_MAX_ROWS is refused with SDOT_ERR_CAPACITY.  Also: a right-hand side with a nonzero mean on a grid whose
-row count is not a multiple of the CG's 1024-row chunks (the last chunk partial), a system with no coupling at all
+row count is not a multiple of the CG's 256-row chunks (the last chunk partial), a system with no coupling at all
 (cols and vals NULL), and host memory refused before any launch."""
 import ctypes
 
@@ -131,8 +131,8 @@ def test_a_size_past_the_static_work_area_is_refused():
 
 
 def test_a_nonzero_mean_rhs_on_a_partial_last_chunk():
-    n, rp, cols, vals, dia = _grid_laplacian(123, 77, 8)          # 9,471 rows: the tenth 1024-row chunk is partial
-    assert n % 1024 != 0
+    n, rp, cols, vals, dia = _grid_laplacian(123, 77, 8)          # 9,471 rows: the last 256-row chunk is partial
+    assert n % 256 != 0
     rng = np.random.default_rng(9)
     rhs = rng.standard_normal((2, n)) + np.array([[3.0], [-0.5]])  # nonzero means: both solves project them out
     ref, got, its_ref = _both(n, rp, cols, vals, dia, rhs)
