@@ -1432,6 +1432,9 @@ struct VecBatch {
     std::vector<MgLevel> fchain;
     std::vector<int2> fidx;
     std::vector<Chunk> build0;                     // the level-0 rows of every problem, for the hierarchy's build
+    struct MgJob { const SolveJob *J; int q[ MG_MAX_LEVELS ]; };    // a problem's index in lv[ l ], per level
+    std::vector<MgJob> mgjobs;
+    bool down_up_planned = false;
     // device copies
     VecDev *dv = nullptr;
     Chunk *dch = nullptr;
@@ -1450,13 +1453,11 @@ struct VecBatch {
         for ( int b = 0; b < d.n; b += VCHUNK, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + VCHUNK ), k } );
         if ( ! J || ! J->mg_L || ! d.precond ) return;
         maxL = std::max( maxL, J->mg_L );
-        int f = J->mg_L - 1;                       // the first level of the fused part: at most MG_FUSE_ROWS rows
-        while ( f > 0 && J->mg_n[ f - 1 ] <= MG_FUSE_ROWS ) --f;
-        fidx.push_back( make_int2( int( fchain.size() ), J->mg_L - f ) );
+        MgJob mj{ J, {} };
         for ( int l = 0; l < J->mg_L; ++l ) {
             int q = int( lv[ l ].size() );
+            mj.q[ l ] = q;
             lv[ l ].push_back( mg_level( *J, l, p ) );
-            if ( l >= f ) fchain.push_back( lv[ l ].back() );
             if ( l == 0 ) {
                 int kk = 0;
                 for ( int b = 0; b < J->mg_n[ 0 ]; b += VCHUNK, ++kk ) build0.push_back( Chunk{ q, b, std::min( J->mg_n[ 0 ], b + VCHUNK ), kk } );
@@ -1464,21 +1465,39 @@ struct VecBatch {
             if ( l + 1 < J->mg_L ) {
                 const int nn = J->mg_n[ l + 1 ];
                 int kk = 0;
-                if ( l < f )
-                    for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
-                kk = 0;
                 for ( int b = 0; b < nn; b += MG_CCH, ++kk ) crs[ l ].push_back( Chunk{ q, b, std::min( nn, b + MG_CCH ), kk } );
-                kk = 0;
-                const int n = J->mg_n[ l ];
-                if ( l < f )
-                    for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
             } else
                 bottom.push_back( lv[ l ].back() );
+        }
+        mgjobs.push_back( mj );
+    }
+    // the cycle's launches: the levels above the fusion threshold one launch per level and direction, the others of each
+    // problem in the fused launch (a block per problem).  A block holds one SM, so the threshold is small when few problems
+    // share the batch (their larger levels are better spread over the GPU) and larger when many do
+    void plan_cycle() {
+        down_up_planned = true;
+        const int T = mgjobs.size() >= 32 ? MG_FUSE_ROWS : MG_FUSE_ROWS / 8;
+        for ( const MgJob &mj : mgjobs ) {
+            const SolveJob *J = mj.J;
+            int f = J->mg_L - 1;
+            while ( f > 0 && J->mg_n[ f - 1 ] <= T ) --f;
+            fidx.push_back( make_int2( int( fchain.size() ), J->mg_L - f ) );
+            for ( int l = 0; l < J->mg_L; ++l ) {
+                const int q = mj.q[ l ];
+                if ( l >= f ) fchain.push_back( lv[ l ][ q ] );
+                if ( l >= f || l + 1 >= J->mg_L ) continue;
+                const int nn = J->mg_n[ l + 1 ], n = J->mg_n[ l ];
+                int kk = 0;
+                for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
+                kk = 0;
+                for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
+            }
         }
     }
     bool mg() const { return maxL > 0; }
     // what the launches of a CG burst depend on: the upload area, the burst, and every table's size
-    std::vector<long long> layout_key( const char *desc, int burst ) const {
+    std::vector<long long> layout_key( const char *desc, int burst ) {
+        if ( ! down_up_planned ) plan_cycle();
         std::vector<long long> k{ ( long long ) ( uintptr_t ) desc, burst, ( long long ) ch.size(), maxL, ( long long ) bottom.size() };
         for ( auto &x : v ) { k.push_back( x.n ); k.push_back( x.precond ); k.push_back( x.mixed ); }
         for ( int l = 0; l < maxL; ++l ) {
@@ -1493,6 +1512,7 @@ struct VecBatch {
     }
     // everything in one copy
     void upload( Ctx &c ) {
+        if ( ! down_up_planned ) plan_cycle();
         std::vector<std::pair<const void *, size_t>> parts;
         parts.push_back( { v.data(), v.size() * sizeof( VecDev ) } );
         parts.push_back( { ch.data(), ch.size() * sizeof( Chunk ) } );

@@ -66,46 +66,64 @@ __global__ void k_mg_level0( const MgLevel *__restrict__ lv, const VecDev *__res
     }
 }
 
-// the (column, value) pairs of coarse row I, gathered by one warp into shared memory; returns their count (-1: too many)
-__device__ int gather_pairs( const MgLevel &M, int I, int *cj, float *cv, int lane ) {
+// the (column, value) pairs of coarse row I, gathered by one warp into shared memory as keys ( column << 11 | pair index )
+// and values by pair index, then sorted by key (a bitonic sort over the warp, padded to a power of 2): the pairs of
+// each coarse column form a run, in pair order.  Returns the pair count (-1: past MG_PAIRS)
+constexpr int MG_KEY_SHIFT = 11;                         // pair indices < 2048 (MG_PAIRS is 1024)
+__device__ int gather_sorted( const MgLevel &M, int I, long long *key, float *cv, int lane ) {
     const int i0 = I * M.pack, i1 = min( M.n, i0 + M.pack );
     int cnt = 0;
     for ( int i = i0; i < i1; ++i ) {
         const int b = M.rp[ i ], e = M.rp[ i + 1 ];
         for ( int base = b; base < e; base += 32 ) {
-            int k = base + lane;
-            if ( k < e && cnt + ( k - base ) < MG_PAIRS ) {
-                cj[ cnt + k - base ] = M.col[ k ] / M.pack;
-                cv[ cnt + k - base ] = M.val[ k ];
+            const int k = base + lane, at = cnt + ( k - base );
+            if ( k < e && at < MG_PAIRS ) {
+                key[ at ] = ( ( long long ) ( M.col[ k ] / M.pack ) << MG_KEY_SHIFT ) | at;
+                cv[ at ] = M.val[ k ];
             }
             cnt += min( 32, e - base );
         }
     }
     __syncwarp();
-    return cnt <= MG_PAIRS ? cnt : -1;
+    if ( cnt > MG_PAIRS ) return -1;
+    int n2 = 1;
+    while ( n2 < cnt ) n2 <<= 1;
+    for ( int k = cnt + lane; k < n2; k += 32 ) key[ k ] = 0x7fffffffffffffffll;
+    __syncwarp();
+    for ( int k = 2; k <= n2; k <<= 1 )
+        for ( int j = k >> 1; j > 0; j >>= 1 ) {
+            for ( int i = lane; i < n2; i += 32 ) {
+                const int l = i ^ j;
+                if ( l > i ) {
+                    const long long x = key[ i ], y = key[ l ];
+                    if ( ( x > y ) == ( ( i & k ) == 0 ) ) { key[ i ] = y; key[ l ] = x; }
+                }
+            }
+            __syncwarp();
+        }
+    return cnt;
 }
 
-// for each pair: is it the first one of its column (and not the diagonal)?  the sum of its column in pair order
-__device__ __forceinline__ bool first_of_column( const int *cj, int cnt, int k, int I ) {
-    const int J = cj[ k ];
-    if ( J == I ) return false;
-    for ( int q = 0; q < k; ++q ) if ( cj[ q ] == J ) return false;
-    return true;
+// in the sorted pairs: does position p start the run of a coarse column other than the diagonal I?
+__device__ __forceinline__ bool run_start( const long long *key, int p, int I ) {
+    const long long J = key[ p ] >> MG_KEY_SHIFT;
+    return J != I && ( p == 0 || ( key[ p - 1 ] >> MG_KEY_SHIFT ) != J );
 }
 
 __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_count( const MgLevel *__restrict__ lv, const Chunk *__restrict__ chunks, int nch,
                                                               ErrRec *err ) {
-    __shared__ int sj[ MG_WARPS ][ MG_PAIRS ];
-    __shared__ float sv[ MG_WARPS ][ MG_PAIRS ];
+    extern __shared__ long long mg_pairs_smem[];
+    long long ( *sk )[ MG_PAIRS ] = reinterpret_cast<long long ( * )[ MG_PAIRS ]>( mg_pairs_smem );
+    float ( *sv )[ MG_PAIRS ] = reinterpret_cast<float ( * )[ MG_PAIRS ]>( mg_pairs_smem + MG_WARPS * MG_PAIRS );
     __shared__ double tot_w[ MG_WARPS ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Chunk ch = chunks[ blockIdx.x ];
     const MgLevel &M = lv[ ch.prob ];
     double tot = 0;
     for ( int I = ch.begin + warp; I < ch.end; I += MG_WARPS ) {
-        int cnt = gather_pairs( M, I, sj[ warp ], sv[ warp ], lane );
+        int cnt = gather_sorted( M, I, sk[ warp ], sv[ warp ], lane );
         int distinct = 0;
-        for ( int k = lane; k < cnt; k += 32 ) distinct += first_of_column( sj[ warp ], cnt, k, I );
+        for ( int k = lane; k < cnt; k += 32 ) distinct += run_start( sk[ warp ], k, I );
         for ( int o = 16; o > 0; o >>= 1 ) distinct += __shfl_xor_sync( 0xffffffffu, distinct, o );
         if ( cnt < 0 ) distinct = M.capn + 1;                           // too many pairs: the level is refused (k_mg_scan)
         if ( lane == 0 ) M.rcn[ I ] = distinct;
@@ -144,8 +162,9 @@ __global__ void __launch_bounds__( 1024 ) k_mg_scan( const MgLevel *__restrict__
 }
 
 __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__restrict__ lv, const Chunk *__restrict__ chunks, int nch ) {
-    __shared__ int sj[ MG_WARPS ][ MG_PAIRS ];
-    __shared__ float sv[ MG_WARPS ][ MG_PAIRS ];
+    extern __shared__ long long mg_pairs_smem[];
+    long long ( *sk )[ MG_PAIRS ] = reinterpret_cast<long long ( * )[ MG_PAIRS ]>( mg_pairs_smem );
+    float ( *sv )[ MG_PAIRS ] = reinterpret_cast<float ( * )[ MG_PAIRS ]>( mg_pairs_smem + MG_WARPS * MG_PAIRS );
     __shared__ int run[ MG_WARPS ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const Chunk ch = chunks[ blockIdx.x ];
@@ -164,22 +183,23 @@ __global__ void __launch_bounds__( 32 * MG_WARPS ) k_mg_fill( const MgLevel *__r
         for ( int w = 0; w < MG_WARPS; ++w ) step += run[ w ];
         __syncthreads();
         if ( I < ch.end ) {
-            int cnt = gather_pairs( M, I, sj[ warp ], sv[ warp ], lane );
+            int cnt = gather_sorted( M, I, sk[ warp ], sv[ warp ], lane );
             if ( cnt < 0 ) cnt = 0;
-            // the distinct columns in pair order, each with its sum in pair order
+            // the distinct columns in increasing order, each with its sum in pair order (its run)
+            const long long *key = sk[ warp ];
             int done = 0;
             float dsum = 0;
             for ( int base = 0; base < cnt; base += 32 ) {
                 int k = base + lane;
-                bool first = k < cnt && first_of_column( sj[ warp ], cnt, k, I );
+                bool first = k < cnt && run_start( key, k, I );
                 float s = 0;
                 if ( first ) {
-                    const int J = sj[ warp ][ k ];
-                    for ( int q = k; q < cnt; ++q ) if ( sj[ warp ][ q ] == J ) s += sv[ warp ][ q ];
+                    const long long J = key[ k ] >> MG_KEY_SHIFT;
+                    for ( int q = k; q < cnt && ( key[ q ] >> MG_KEY_SHIFT ) == J; ++q ) s += sv[ warp ][ key[ q ] & ( ( 1 << MG_KEY_SHIFT ) - 1 ) ];
                 }
                 unsigned m = __ballot_sync( 0xffffffffu, first );
                 int slot = done + __popc( m & ( ( 1u << lane ) - 1 ) );
-                if ( first && ! refused ) { M.coln[ my + slot ] = sj[ warp ][ k ]; M.valn[ my + slot ] = s; }
+                if ( first && ! refused ) { M.coln[ my + slot ] = int( key[ k ] >> MG_KEY_SHIFT ); M.valn[ my + slot ] = s; }
                 float ws = first ? s : 0.f;
                 for ( int o = 16; o > 0; o >>= 1 ) ws += __shfl_xor_sync( 0xffffffffu, ws, o );
                 dsum += ws;
@@ -385,9 +405,17 @@ void launch_mg_level0( const Launch &L, const MgLevel *lv, const VecDev *vs, con
 }
 void launch_mg_coarsen( const Launch &L, const MgLevel *lv, int nprob, const Chunk *ch, int nch, ErrRec *err ) {
     if ( nch <= 0 ) return;
-    k_mg_count<<<nch, 32 * MG_WARPS, 0, L.stream>>>( lv, ch, nch, err );
+    // the pairs of each warp's coarse row: MG_PAIRS keys (8 bytes) and values (4 bytes)
+    constexpr int smem = MG_WARPS * MG_PAIRS * 12;
+    static bool configured = false;
+    if ( ! configured ) {
+        cudaFuncSetAttribute( k_mg_count, cudaFuncAttributeMaxDynamicSharedMemorySize, smem );
+        cudaFuncSetAttribute( k_mg_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem );
+        configured = true;
+    }
+    k_mg_count<<<nch, 32 * MG_WARPS, smem, L.stream>>>( lv, ch, nch, err );
     k_mg_scan<<<nprob, 1024, 0, L.stream>>>( lv );
-    k_mg_fill<<<nch, 32 * MG_WARPS, 0, L.stream>>>( lv, ch, nch );
+    k_mg_fill<<<nch, 32 * MG_WARPS, smem, L.stream>>>( lv, ch, nch );
     *L.launches += 3;
 }
 void launch_mg_bottom_build( const Launch &L, const MgLevel *lv, int nprob ) {

@@ -266,16 +266,13 @@ def _check_aggregated(name, plan, pos, groups, tol):
     assert st["nb_clusters"] == len(groups) and st["nb_aggregated"] == sum(len(g) for g, _ in groups), (name, st["aggregation"])
 
 
-# the clouds of the aggregation tests, with the two this build does not solve yet: in 2D the pair 1e-12 apart makes the
-# first Newton system's CG fail (c_ij ~ 1e10 next to couplings ~ 1); in 3D the triple 1e-10 apart leaves one neighbour
-# cell 5e-14 off (three near-coincident bisector planes) and the damping stagnates above 1e-11 / n
+# the clouds of the aggregation tests (the 2D pair 1e-12 apart puts c_ij ~ 1e10 next to couplings ~ 1 in the first Newton
+# system; in 3D the triple 1e-10 apart makes three near-coincident bisector planes)
 _CLOUDS = [(d, name) for d in (2, 3) for name in ("exact pair", "exact triple", "pair at 1e-9", "pair at 1e-12", "triple at 1e-10",
                                                    "pair and duplicate")]
-_GAPS = {(2, "pair at 1e-12"), (3, "triple at 1e-10")}
 
 
-@pytest.mark.parametrize("d,name", [pytest.param(d, nm, marks=pytest.mark.xfail(reason="a known gap of this build", strict=False))
-                                    if (d, nm) in _GAPS else (d, nm) for d, nm in _CLOUDS])
+@pytest.mark.parametrize("d,name", _CLOUDS)
 def test_the_card_aggregates_as_the_cpu(d, name):
     """tests/test_SdotPlanNd.py:1510-1535, 1785-1805: seeds the doubles cannot separate are merged, and the oracle's
     diagram at the GPU's weights gives each cluster its mass and every other cell its own"""
