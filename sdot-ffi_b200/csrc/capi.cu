@@ -211,7 +211,8 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         if ( facets ) { P.nb = dnb; P.nid = dnid; P.nc = dnc; P.nm = dnm; }
         unsigned flags = F_MASS | F_USER_ORDER | ( facets ? F_FACETS : 0u ) | ( ( out->barycentres || out->costs ) ? F_MOMENTS : 0u );
         std::vector<Chunk> ch;
-        for ( int b = 0, k = 0; b < n; b += CHUNK, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + CHUNK ) ), k } );
+        const int cs = cell_chunk( dim, n );
+        for ( int b = 0, k = 0; b < n; b += cs, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + cs ) ), k } );
         size_t o2 = ( sizeof( ProbDev ) + 255 ) & ~size_t( 255 );
         DevVec dd( c, o2 + ch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
@@ -279,7 +280,8 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         P.gpos = grad_positions ? gp : nullptr;
         P.gw = grad_weights ? gw : nullptr;
         std::vector<Chunk> ch;
-        for ( int b = 0, k = 0; b < n; b += CHUNK, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + CHUNK ) ), k } );
+        const int cs = cell_chunk( dim, n );
+        for ( int b = 0, k = 0; b < n; b += cs, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + cs ) ), k } );
         size_t o2 = ( sizeof( ProbDev ) + 255 ) & ~size_t( 255 );
         DevVec dd( c, o2 + ch.size() * sizeof( Chunk ) );
         CK( cudaMemcpyAsync( dd.p, &P, sizeof( P ), cudaMemcpyHostToDevice, c.stream ) );
@@ -345,7 +347,8 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         P.nb = nb; P.nid = nid; P.nc = nc;
         P.ovf_count = ovf_count; P.ovf_cap = int( n ) + 4096; P.ovf_ids = ovf_ids; P.ovf_c = ovf_c;
         std::vector<Chunk> ch;
-        for ( int b = 0, k = 0; b < n; b += CHUNK, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + CHUNK ) ), k } );
+        const int cs = cell_chunk( dim, n );
+        for ( int b = 0, k = 0; b < n; b += cs, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + cs ) ), k } );
         std::vector<Chunk> vch;
         for ( int b = 0, k = 0; b < n; b += VCHUNK, ++k ) vch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + VCHUNK ) ), k } );
         VecDev V;

@@ -295,16 +295,23 @@ __device__ __forceinline__ bool wclip( WPoly &C, int lane, double nx, double ny,
     double anx = __shfl_sync( FULL, C.lnx, a ), any = __shfl_sync( FULL, C.lny, a ), aoff = __shfl_sync( FULL, C.loff, a );
     double bnx = __shfl_sync( FULL, C.lnx, b ), bny = __shfl_sync( FULL, C.lny, b ), boff = __shfl_sync( FULL, C.loff, b );
     int bid = __shfl_sync( FULL, C.lid, b );
-    double xa = __shfl_sync( FULL, C.vx, a ), ya = __shfl_sync( FULL, C.vy, a ), sa = __shfl_sync( FULL, s, a );
-    double xa1 = __shfl_sync( FULL, C.vx, a1 ), ya1 = __shfl_sync( FULL, C.vy, a1 ), sa1 = __shfl_sync( FULL, s, a1 );
-    double xb = __shfl_sync( FULL, C.vx, b ), yb = __shfl_sync( FULL, C.vy, b ), sb = __shfl_sync( FULL, s, b );
-    double xb1 = __shfl_sync( FULL, C.vx, b1 ), yb1 = __shfl_sync( FULL, C.vy, b1 ), sb1 = __shfl_sync( FULL, s, b1 );
     double Px, Py, Qx, Qy;
     bool okP, okQ;
     isect( anx, any, aoff, nx, ny, off, Px, Py, okP );
     isect( nx, ny, off, bnx, bny, boff, Qx, Qy, okQ );
-    if ( ! okP ) { double t = sa / ( sa - sa1 ); Px = xa + t * ( xa1 - xa ); Py = ya + t * ( ya1 - ya ); }
-    if ( ! okQ ) { double t = sb / ( sb - sb1 ); Qx = xb + t * ( xb1 - xb ); Qy = yb + t * ( yb1 - yb ); }
+    // (okP, okQ are warp uniform: the edges' end points are fetched only for the rare near-parallel fallback)
+    if ( ! okP ) {
+        double xa = __shfl_sync( FULL, C.vx, a ), ya = __shfl_sync( FULL, C.vy, a ), sa = __shfl_sync( FULL, s, a );
+        double xa1 = __shfl_sync( FULL, C.vx, a1 ), ya1 = __shfl_sync( FULL, C.vy, a1 ), sa1 = __shfl_sync( FULL, s, a1 );
+        double t = sa / ( sa - sa1 );
+        Px = xa + t * ( xa1 - xa ); Py = ya + t * ( ya1 - ya );
+    }
+    if ( ! okQ ) {
+        double xb = __shfl_sync( FULL, C.vx, b ), yb = __shfl_sync( FULL, C.vy, b ), sb = __shfl_sync( FULL, s, b );
+        double xb1 = __shfl_sync( FULL, C.vx, b1 ), yb1 = __shfl_sync( FULL, C.vy, b1 ), sb1 = __shfl_sync( FULL, s, b1 );
+        double t = sb / ( sb - sb1 );
+        Qx = xb + t * ( xb1 - xb ); Qy = yb + t * ( yb1 - yb );
+    }
     int src = ( b + 1 + lane ) % m;
     double nvx = __shfl_sync( FULL, C.vx, src ), nvy = __shfl_sync( FULL, C.vy, src );
     double nlx = __shfl_sync( FULL, C.lnx, src ), nly = __shfl_sync( FULL, C.lny, src ), nlo = __shfl_sync( FULL, C.loff, src );

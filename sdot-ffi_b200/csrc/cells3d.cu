@@ -26,15 +26,20 @@ template<int VC_, int PC_, class I_>
 struct Cell3T {
     static constexpr int VC = VC_, PC = PC_;
     typedef I_ I;
-    static constexpr int NONE = int( I_( ~I_( 0 ) ) );   // "no vertex" in `tw`
+    static constexpr int NONE = int( I_( ~I_( 0 ) ) );   // "no vertex" / "no new vertex"
     double vx[ VC ], vy[ VC ], vz[ VC ];
     double area[ 3 * VC ];                       // per (vertex, edge): the face-triangle contribution (integration)
     double nx[ PC ], ny[ PC ], nz[ PC ], no[ PC ];
     int pid[ PC ];
     I va[ VC ], vb[ VC ], vc[ VC ];
+    // the ADJACENCY: ad[ q ][ k ] is the vertex across edge q of vertex k (edge 0 = (va, vb), 1 = (vb, vc), 2 = (vc, va)),
+    // the one holding the reversed directed edge; kept through every cut, so that no cut and no integration searches
+    I ad[ 3 ][ VC ];
     unsigned char out[ VC ];
-    I nt[ VC ][ 3 ];                             // new triples of a cut
-    I tw[ 3 * VC ];                              // gaussians: the vertex across each (vertex, edge) entry, NONE if none
+    I nt[ VC ][ 3 ];                             // new triples of a cut; gaussians: the next entry of each face's list
+    I nk[ VC ];                                  // a cut: the kept vertex across each new vertex's first edge
+    I nidx[ VC ];                                // a cut: the index of each kept vertex after the compaction
+    I e0t[ PC ], e1t[ PC ];                      // a cut: the new vertex whose first (second) plane is this one; NONE between cuts
     double fmp[ PC ];                            // gaussians: the winding-angle part of each face's integral
     double par[ PC ];                            // each face's integral (facets pass)
     unsigned char used[ PC ];                    // plane compaction
@@ -43,8 +48,8 @@ struct Cell3T {
     int nv, np;
 };
 using Cell3 = Cell3T<128, 96, unsigned char>;            // the main kernel, in shared memory
-using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 84 KB
-using Cell3G = Cell3T<32768, 8192, unsigned short>;      // the giant-cell pass (the reference's card_max_vertices, PowerDiagram_Bsp.py:122): one warp a block, about 2.6 MB in global memory
+using Cell3B = Cell3T<1024, 256, unsigned short>;        // the big-cell pass: one warp a block, about 90 KB
+using Cell3G = Cell3T<32768, 8192, unsigned short>;      // the giant-cell pass (the reference's card_max_vertices, PowerDiagram_Bsp.py:122): one warp a block, about 2.8 MB in global memory
 
 // the vertex of planes a, b, c (n . y = o, seed frame), found on the line of the two most transverse of them: from the
 // line's point nearest the seed, by the step the third plane's equation asks for.  The vertex then lies on all three
@@ -53,20 +58,20 @@ using Cell3G = Cell3T<32768, 8192, unsigned short>;      // the giant-cell pass 
 // lost up to 1e-4 of its volume)
 template<class C3>
 __device__ __forceinline__ void solve3( const C3 &C, int a, int b, int c, double &x, double &y, double &z ) {
-    auto cross2 = [&]( int p, int q ) {
+    auto cross2 = [&]( int p, int q ) {          // |n_p x n_q|^2
         const double cx = C.ny[ p ] * C.nz[ q ] - C.nz[ p ] * C.ny[ q ], cy = C.nz[ p ] * C.nx[ q ] - C.nx[ p ] * C.nz[ q ],
                      cz = C.nx[ p ] * C.ny[ q ] - C.ny[ p ] * C.nx[ q ];
-        const double np = C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ];
-        const double nq = C.nx[ q ] * C.nx[ q ] + C.ny[ q ] * C.ny[ q ] + C.nz[ q ] * C.nz[ q ];
-        return ( cx * cx + cy * cy + cz * cz ) / ( np * nq );            // sin^2 of their angle
+        return cx * cx + cy * cy + cz * cz;
     };
-    // the line: the pair with the largest angle; the plane: the third one
-    const double sab = cross2( a, b ), sbc = cross2( b, c ), sca = cross2( c, a );
+    auto norm2 = [&]( int p ) { return C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ]; };
+    // the line: the pair with the largest angle (sin^2 = |n_p x n_q|^2 / |n_p|^2 |n_q|^2, compared times the product of
+    // the three |n|^2); the plane: the third one
+    const double na = norm2( a ), nb = norm2( b ), nc = norm2( c );
+    const double sab = cross2( a, b ) * nc, sbc = cross2( b, c ) * na, sca = cross2( c, a ) * nb;
     int p = a, q = b, r = c;
-    if ( sbc > sab && sbc >= sca ) { p = b; q = c; r = a; }
-    else if ( sca > sab && sca > sbc ) { p = c; q = a; r = b; }
-    const double pn2 = C.nx[ p ] * C.nx[ p ] + C.ny[ p ] * C.ny[ p ] + C.nz[ p ] * C.nz[ p ];
-    const double qn2 = C.nx[ q ] * C.nx[ q ] + C.ny[ q ] * C.ny[ q ] + C.nz[ q ] * C.nz[ q ];
+    double pn2 = na, qn2 = nb;
+    if ( sbc > sab && sbc >= sca ) { p = b; q = c; r = a; pn2 = nb; qn2 = nc; }
+    else if ( sca > sab && sca > sbc ) { p = c; q = a; r = b; pn2 = nc; qn2 = na; }
     const double pq = C.nx[ p ] * C.nx[ q ] + C.ny[ p ] * C.ny[ q ] + C.nz[ p ] * C.nz[ q ];
     const double dx = C.ny[ p ] * C.nz[ q ] - C.nz[ p ] * C.ny[ q ], dy = C.nz[ p ] * C.nx[ q ] - C.nx[ p ] * C.nz[ q ],
                  dz = C.nx[ p ] * C.ny[ q ] - C.ny[ p ] * C.nx[ q ];
@@ -99,6 +104,20 @@ __device__ __forceinline__ int twin_of( const C3 &C, int e0, int e1 ) {
     return -1;
 }
 
+// the adjacency of every vertex by search (the box, a loaded record, a cut whose boundary is not one cycle)
+template<class C3>
+__device__ void rebuild_adj( C3 &C, int lane ) {
+    typedef typename C3::I I;
+    for ( int k = lane; k < C.nv; k += 32 ) {
+        const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
+        for ( int q = 0; q < 3; ++q ) {
+            const int t = twin_of( C, e[ ( q + 1 ) % 3 ], e[ q ] );
+            C.ad[ q ][ k ] = t < 0 ? I( C3::NONE ) : I( t );
+        }
+    }
+    __syncwarp();
+}
+
 template<class C3>
 __device__ void init_box3( C3 &C, int lane, const double *lo, const double *hi, double px, double py, double pz ) {
     // planes: 0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z ; ids -1 .. -6
@@ -127,7 +146,9 @@ __device__ void init_box3( C3 &C, int lane, const double *lo, const double *hi, 
         const double ex = fmax( hi[ 0 ] - px, px - lo[ 0 ] ), ey = fmax( hi[ 1 ] - py, py - lo[ 1 ] ), ez = fmax( hi[ 2 ] - pz, pz - lo[ 2 ] );
         C.L = sqrt( ex * ex + ey * ey + ez * ez );
     }
+    for ( int p = lane; p < C3::PC; p += 32 ) { C.e0t[ p ] = typename C3::I( C3::NONE ); C.e1t[ p ] = typename C3::I( C3::NONE ); }
     __syncwarp();
+    rebuild_adj( C, lane );
 }
 
 // drops the planes no vertex uses (when the plane table is full); false if it cannot make room
@@ -185,22 +206,22 @@ __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double
     __syncwarp();
     if ( lane == 0 ) { C.nx[ P ] = nx; C.ny[ P ] = ny; C.nz[ P ] = nz; C.no[ P ] = off; C.pid[ P ] = id; C.np = P + 1; }
     __syncwarp();
-    // the boundary edges: directed edges of removed vertices whose twin is kept.  Each new vertex (e0, e1, P) is
+    // the boundary edges: directed edges of removed vertices whose twin (`ad`) is kept.  Each new vertex (e0, e1, P) is
     // re-solved from its three planes; where that lands off the edge it replaces (three planes nearly through one
     // line: a cut that grazes the edge), it is taken on the edge instead, from its kept end, where n . y = off.  Its
-    // position waits in `area` (free until the integration) while the kept vertices are compacted.
+    // position waits in `area` (free until the integration) while the kept vertices are compacted; the new vertex whose
+    // first (second) plane is p is recorded in e0t[ p ] (e1t[ p ]), which links the new vertices around the new face.
     int nnew = 0;
     for ( int base = 0; base < nv; base += 32 ) {
         int k = base + lane;
-        I tr[ 3 ][ 3 ];
+        I tr[ 3 ][ 2 ];
         int tt[ 3 ];
         int cnt = 0;
         if ( k < nv && C.out[ k ] ) {
             int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
             for ( int q = 0; q < 3; ++q ) {
-                int e0 = e[ q ], e1 = e[ ( q + 1 ) % 3 ];
-                int t = twin_of( C, e1, e0 );
-                if ( t >= 0 && ! C.out[ t ] ) { tr[ cnt ][ 0 ] = e0; tr[ cnt ][ 1 ] = e1; tr[ cnt ][ 2 ] = P; tt[ cnt ] = t; ++cnt; }
+                const int t = C.ad[ q ][ k ];
+                if ( t != C3::NONE && ! C.out[ t ] ) { tr[ cnt ][ 0 ] = I( e[ q ] ); tr[ cnt ][ 1 ] = I( e[ ( q + 1 ) % 3 ] ); tt[ cnt ] = t; ++cnt; }
             }
         }
         int inc = cnt;
@@ -209,49 +230,93 @@ __device__ bool wclip3( C3 &C, int lane, double nx, double ny, double nz, double
         int total = __shfl_sync( FULL3, inc, 31 );
         int at = nnew + inc - cnt;
         for ( int q = 0; q < cnt; ++q ) {
-            if ( at + q >= VC ) continue;
-            C.nt[ at + q ][ 0 ] = tr[ q ][ 0 ]; C.nt[ at + q ][ 1 ] = tr[ q ][ 1 ]; C.nt[ at + q ][ 2 ] = tr[ q ][ 2 ];
+            const int j = at + q;
+            if ( j >= VC ) continue;
+            C.nt[ j ][ 0 ] = tr[ q ][ 0 ]; C.nt[ j ][ 1 ] = tr[ q ][ 1 ]; C.nt[ j ][ 2 ] = I( P );
             const int t = tt[ q ];
+            C.nk[ j ] = I( t );
+            C.e0t[ tr[ q ][ 0 ] ] = I( j );
+            C.e1t[ tr[ q ][ 1 ] ] = I( j );
             const double Rx = C.vx[ k ], Ry = C.vy[ k ], Rz = C.vz[ k ], Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
             double x, y, z;
             solve3( C, tr[ q ][ 0 ], tr[ q ][ 1 ], P, x, y, z );
             const double ex = Rx - Tx, ey = Ry - Ty, ez = Rz - Tz, e2 = ex * ex + ey * ey + ez * ez;
-            const double u = ( ( x - Tx ) * ex + ( y - Ty ) * ey + ( z - Tz ) * ez ) / e2;   // NaN if the solve failed
-            if ( ! ( u >= -1e-9 && u <= 1 + 1e-9 ) ) {
+            const double un = ( x - Tx ) * ex + ( y - Ty ) * ey + ( z - Tz ) * ez;     // u e2, u the edge parameter (NaN: no solve)
+            if ( ! ( un >= -1e-9 * e2 && un <= ( 1 + 1e-9 ) * e2 ) ) {
                 const double dT = nx * Tx + ny * Ty + nz * Tz - off, dR = nx * Rx + ny * Ry + nz * Rz - off;   // dR > tol >= dT
                 const double s = fmin( 1.0, fmax( 0.0, -dT / ( dR - dT ) ) );
                 x = Tx + s * ex; y = Ty + s * ey; z = Tz + s * ez;
             }
-            C.area[ at + q ] = x; C.area[ VC + at + q ] = y; C.area[ 2 * VC + at + q ] = z;
+            C.area[ j ] = x; C.area[ VC + j ] = y; C.area[ 2 * VC + j ] = z;
         }
         nnew += total;
     }
     __syncwarp();
     const int nkeep = nv - nout;
-    if ( nkeep + nnew > VC || nnew >= VC ) return false;
-    // compaction of the kept vertices, in order (destinations never pass their sources)
+    const bool room = ! ( nkeep + nnew > VC || nnew >= VC );
+    // the new vertices make one cycle around the new face when every plane of the boundary is the first plane of exactly
+    // one new vertex and the second plane of exactly one; otherwise (a removed region that is not a disc, at the limits of
+    // rounding) the adjacency is searched again after the cut
+    bool cyc = true;
+    for ( int j = lane; j < nnew && room; j += 32 )
+        cyc = cyc && C.e0t[ C.nt[ j ][ 0 ] ] == j && C.e1t[ C.nt[ j ][ 1 ] ] == j && C.e0t[ C.nt[ j ][ 1 ] ] != C3::NONE &&
+              C.e1t[ C.nt[ j ][ 0 ] ] != C3::NONE;
+    cyc = __all_sync( FULL3, cyc );
+    if ( ! room ) {
+        for ( int j = lane; j < nnew && j < VC; j += 32 ) { C.e0t[ C.nt[ j ][ 0 ] ] = I( C3::NONE ); C.e1t[ C.nt[ j ][ 1 ] ] = I( C3::NONE ); }
+        __syncwarp();
+        return false;
+    }
+    // compaction of the kept vertices, in order (destinations never pass their sources): first their new indices, then
+    // the moves, their adjacency mapped to those indices (an edge to a removed vertex gets its new vertex below)
     int kept_before = 0;
     for ( int base = 0; base < nv; base += 32 ) {
         int k = base + lane;
         bool keep = k < nv && ! C.out[ k ];
         unsigned m = __ballot_sync( FULL3, keep );
-        int dst = kept_before + __popc( m & ( ( 1u << lane ) - 1 ) );
-        double x = 0, y = 0, z = 0;
-        I a = 0, b = 0, c = 0;
-        if ( keep ) { x = C.vx[ k ]; y = C.vy[ k ]; z = C.vz[ k ]; a = C.va[ k ]; b = C.vb[ k ]; c = C.vc[ k ]; }
-        __syncwarp();
-        if ( keep ) { C.vx[ dst ] = x; C.vy[ dst ] = y; C.vz[ dst ] = z; C.va[ dst ] = a; C.vb[ dst ] = b; C.vc[ dst ] = c; }
-        __syncwarp();
+        if ( keep ) C.nidx[ k ] = I( kept_before + __popc( m & ( ( 1u << lane ) - 1 ) ) );
         kept_before += __popc( m );
     }
-    // the new vertices, placed above
-    for ( int j = lane; j < nnew; j += 32 ) {
-        int d = nkeep + j;
-        C.va[ d ] = C.nt[ j ][ 0 ]; C.vb[ d ] = C.nt[ j ][ 1 ]; C.vc[ d ] = C.nt[ j ][ 2 ];
-        C.vx[ d ] = C.area[ j ]; C.vy[ d ] = C.area[ VC + j ]; C.vz[ d ] = C.area[ 2 * VC + j ];
+    __syncwarp();
+    for ( int base = 0; base < nkeep + nout; base += 32 ) {
+        int k = base + lane;
+        bool keep = k < nv && ! C.out[ k ];
+        int dst = keep ? C.nidx[ k ] : 0;
+        double x = 0, y = 0, z = 0;
+        I a = 0, b = 0, c = 0, j0 = 0, j1 = 0, j2 = 0;
+        if ( keep ) {
+            x = C.vx[ k ]; y = C.vy[ k ]; z = C.vz[ k ]; a = C.va[ k ]; b = C.vb[ k ]; c = C.vc[ k ];
+            const int t0 = C.ad[ 0 ][ k ], t1 = C.ad[ 1 ][ k ], t2 = C.ad[ 2 ][ k ];
+            j0 = t0 == C3::NONE || C.out[ t0 ] ? I( C3::NONE ) : C.nidx[ t0 ];
+            j1 = t1 == C3::NONE || C.out[ t1 ] ? I( C3::NONE ) : C.nidx[ t1 ];
+            j2 = t2 == C3::NONE || C.out[ t2 ] ? I( C3::NONE ) : C.nidx[ t2 ];
+        }
+        __syncwarp();
+        if ( keep ) {
+            C.vx[ dst ] = x; C.vy[ dst ] = y; C.vz[ dst ] = z; C.va[ dst ] = a; C.vb[ dst ] = b; C.vc[ dst ] = c;
+            C.ad[ 0 ][ dst ] = j0; C.ad[ 1 ][ dst ] = j1; C.ad[ 2 ][ dst ] = j2;
+        }
+        __syncwarp();
     }
+    // the new vertices, placed above: edge 0 (e0, e1) faces their kept vertex, edge 1 (e1, P) the new vertex that starts
+    // at e1, edge 2 (P, e0) the one that ends at e0; the kept vertex's edge (e1, e0) faces the new vertex
+    for ( int j = lane; j < nnew; j += 32 ) {
+        const int d = nkeep + j, e0 = C.nt[ j ][ 0 ], e1 = C.nt[ j ][ 1 ];
+        C.va[ d ] = I( e0 ); C.vb[ d ] = I( e1 ); C.vc[ d ] = I( P );
+        C.vx[ d ] = C.area[ j ]; C.vy[ d ] = C.area[ VC + j ]; C.vz[ d ] = C.area[ 2 * VC + j ];
+        const int T = C.nidx[ C.nk[ j ] ];
+        C.ad[ 0 ][ d ] = I( T );
+        C.ad[ 1 ][ d ] = cyc ? I( nkeep + C.e0t[ e1 ] ) : I( C3::NONE );
+        C.ad[ 2 ][ d ] = cyc ? I( nkeep + C.e1t[ e0 ] ) : I( C3::NONE );
+        const int ta = C.va[ T ], tb = C.vb[ T ], tc = C.vc[ T ];
+        const int qT = ( ta == e1 && tb == e0 ) ? 0 : ( ( tb == e1 && tc == e0 ) ? 1 : 2 );
+        C.ad[ qT ][ T ] = I( d );
+    }
+    __syncwarp();
+    for ( int j = lane; j < nnew; j += 32 ) { C.e0t[ C.nt[ j ][ 0 ] ] = I( C3::NONE ); C.e1t[ C.nt[ j ][ 1 ] ] = I( C3::NONE ); }
     if ( lane == 0 ) C.nv = nkeep + nnew;
     __syncwarp();
+    if ( ! cyc ) rebuild_adj( C, lane );
     return true;
 }
 
@@ -512,14 +577,7 @@ template<class C3>
 __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane, double px, double py, double pz, double &M, double &Fx,
                                                 double &Fy, double &Fz, double &S2 ) {
     const int nv = C.nv, np = C.np;
-    for ( int k = lane; k < nv; k += 32 ) {
-        const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
-        for ( int q = 0; q < 3; ++q ) {
-            int t = twin_of( C, e[ ( q + 1 ) % 3 ], e[ q ] );
-            C.tw[ 3 * k + q ] = t < 0 ? ( typename C3::I ) C3::NONE : ( typename C3::I ) t;
-            C.area[ 3 * k + q ] = 0;
-        }
-    }
+    for ( int k = lane; k < 3 * nv; k += 32 ) C.area[ k ] = 0;
     for ( int p = lane; p < np; p += 32 ) C.fmp[ p ] = 0;
     __syncwarp();
     if ( nv == 0 ) return;
@@ -531,7 +589,7 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
         for ( int k = 0; k < nv; ++k ) {
             const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
             for ( int q = 0; q < 3; ++q ) {
-                if ( e[ q ] != p || C.tw[ 3 * k + q ] == C3::NONE ) continue;
+                if ( e[ q ] != p || C.ad[ q ][ k ] == C3::NONE ) continue;
                 if ( prev < 0 ) C.remap[ p ] = ( typename C3::I ) k;
                 else C.nt[ prev ][ pq ] = ( typename C3::I ) k;
                 prev = k;
@@ -586,8 +644,8 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
         // the edge integrals of every (gaussian, entry)
         for ( int base = 0; base < ns * NEp; base += 32 ) {
             const int idx = base + lane, gi = idx / NEp, e = idx - gi * NEp;
-            if ( gi < ns && e < NE && C.tw[ e ] != C3::NONE ) {
-                const int g = nth( gi ), k = e / 3, q = e - 3 * k, t = C.tw[ e ];
+            if ( gi < ns && e < NE && C.ad[ e % 3 ][ e / 3 ] != C3::NONE ) {
+                const int g = nth( gi ), k = e / 3, q = e - 3 * k, t = C.ad[ q ][ k ];
                 const int f = q == 0 ? C.va[ k ] : ( q == 1 ? C.vb[ k ] : C.vc[ k ] );
                 const double *G = P.dval + g * 5;
                 const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
@@ -620,7 +678,7 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
                 double th = 0;
                 for ( int k = C.remap[ p ]; k != C3::NONE; ) {
                     const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
-                    const int t = C.tw[ 3 * k + q ];
+                    const int t = C.ad[ q ][ k ];
                     th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
                     k = C.nt[ k ][ q ];
                 }
@@ -756,8 +814,8 @@ __device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, 
         int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
         double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ];
         for ( int q = 0; q < 3; ++q ) {
-            int f = e[ q ], b = e[ ( q + 1 ) % 3 ];
-            int t = twin_of( C, b, f );
+            const int f = e[ q ];
+            const int t = C.ad[ q ][ k ] == C3::NONE ? -1 : int( C.ad[ q ][ k ] );    // the vertex across edge (f, e[ q + 1 ])
             double a2 = 0;
             if ( t >= 0 ) {
                 double Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
@@ -874,11 +932,11 @@ __device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, 
         for ( int k = lane; k < nv; k += 32 ) {
             const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
             for ( int q = 0; q < 3; ++q ) {
-                const int f = e[ q ], b = e[ ( q + 1 ) % 3 ], j = C.pid[ f ];
+                const int f = e[ q ], j = C.pid[ f ];
                 const double a2 = C.area[ 3 * k + q ];
                 if ( j < 0 || a2 == 0 ) continue;
-                const int t = twin_of( C, b, f );
-                if ( t < 0 ) continue;
+                const int t = C.ad[ q ][ k ];
+                if ( t == C3::NONE ) continue;
                 const double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
                 const double cf = C.no[ f ] / nn;
                 const double gj = P.gm[ user_order ? P.user[ j ] : j ];
@@ -951,9 +1009,9 @@ __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsig
 // once: the warps then mostly wait for instructions.  So the main kernel runs twice: pass 1 clips every gaussian cell and
 // stores it (its used planes and its vertices) in `Split3::mem`; pass 2 loads each one and integrates it.  A cell that
 // finds no room in `mem` is done whole by pass 2.  The record of a cell, 16-byte aligned: int nv, np (16 bytes), then
-// doubles vx, vy, vz [nv] and nx, ny, nz, no [np], ints pid [np], ushorts va, vb, vc [nv].
+// doubles vx, vy, vz [nv] and nx, ny, nz, no [np], ints pid [np], ushorts va, vb, vc [nv] and the adjacency ad [3][nv].
 __device__ __forceinline__ size_t rec3_bytes( int nv, int np ) {
-    return ( 16 + size_t( 8 ) * ( 3 * nv + 4 * np ) + size_t( 4 ) * np + size_t( 6 ) * nv + 15 ) & ~size_t( 15 );
+    return ( 16 + size_t( 8 ) * ( 3 * nv + 4 * np ) + size_t( 4 ) * np + size_t( 12 ) * nv + 15 ) & ~size_t( 15 );
 }
 
 template<class C3>
@@ -974,6 +1032,9 @@ __device__ long long store3( C3 &C, const Split3 &sp, int lane ) {
     for ( int k = lane; k < nv; k += 32 ) {
         v[ k ] = C.vx[ k ]; v[ nv + k ] = C.vy[ k ]; v[ 2 * nv + k ] = C.vz[ k ];
         ids[ k ] = C.va[ k ]; ids[ nv + k ] = C.vb[ k ]; ids[ 2 * nv + k ] = C.vc[ k ];
+        ids[ 3 * nv + k ] = C.ad[ 0 ][ k ] == C3::NONE ? 0xffff : C.ad[ 0 ][ k ];
+        ids[ 4 * nv + k ] = C.ad[ 1 ][ k ] == C3::NONE ? 0xffff : C.ad[ 1 ][ k ];
+        ids[ 5 * nv + k ] = C.ad[ 2 ][ k ] == C3::NONE ? 0xffff : C.ad[ 2 ][ k ];
     }
     for ( int p = lane; p < np; p += 32 ) {
         pl[ p ] = C.nx[ p ]; pl[ np + p ] = C.ny[ p ]; pl[ 2 * np + p ] = C.nz[ p ]; pl[ 3 * np + p ] = C.no[ p ];
@@ -993,6 +1054,10 @@ __device__ void load3( C3 &C, const Split3 &sp, long long at, int lane ) {
     for ( int k = lane; k < nv; k += 32 ) {
         C.vx[ k ] = v[ k ]; C.vy[ k ] = v[ nv + k ]; C.vz[ k ] = v[ 2 * nv + k ];
         C.va[ k ] = I( ids[ k ] ); C.vb[ k ] = I( ids[ nv + k ] ); C.vc[ k ] = I( ids[ 2 * nv + k ] );
+        for ( int q = 0; q < 3; ++q ) {
+            const unsigned short t = ids[ ( 3 + q ) * nv + k ];
+            C.ad[ q ][ k ] = t == 0xffff ? I( C3::NONE ) : I( t );
+        }
     }
     for ( int p = lane; p < np; p += 32 ) {
         C.nx[ p ] = pl[ p ]; C.ny[ p ] = pl[ np + p ]; C.nz[ p ] = pl[ 2 * np + p ]; C.no[ p ] = pl[ 3 * np + p ];

@@ -535,6 +535,8 @@ struct SolveJob {
     std::vector<int> agg_parent, cl_begin, cl_members;
     int *d_cl = nullptr;
     double *ae = nullptr;
+    double *cl_true = nullptr;          // the true couplings inside each cluster ([ members ][ AGG_KMAX + 1 ]), then scratch
+    double c_scale = 1;                 // the scale of a facet's coupling: rho (or the box's mean density) x (3D) the spacing
     int ncl = 0;
     bool full_set = false;              // stats[ residual_full ] computed on the full problem
     int polish_round = 0;               // the re-splitting after an aggregated convergence: rounds done,
@@ -559,7 +561,7 @@ static size_t mg_bytes( int dim, long n, int cap );
 
 size_t job_bytes( int dim, long n, int dkind, long dcount ) {
     const int cap = dim == 2 ? CAP2 : CAP3;
-    const long nch = ( n + CHUNK - 1 ) / CHUNK, nv = ( n + VCHUNK - 1 ) / VCHUNK;
+    const long cs = cell_chunk( dim, n ), nch = ( n + cs - 1 ) / cs, nv = ( n + VCHUNK - 1 ) / VCHUNK;
     size_t b = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                size_t( n ) * 4 + size_t( nch ) * NB_REPORT * 8 + size_t( nv ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) + 40 * 256;
     // geometry: ranked positions, user, rank_of, the grid (about n / 2 cells), the density, and the sort's scratch
@@ -573,7 +575,7 @@ size_t job_bytes( int dim, long n, int dkind, long dcount ) {
 static void alloc_job( Ctx &c, SolveJob &J ) {
     const long n = J.G.n;
     const int dim = J.G.dim, cap = J.cap;
-    J.nch_cells = int( ( n + CHUNK - 1 ) / CHUNK );
+    J.nch_cells = int( ( n + cell_chunk( dim, n ) - 1 ) / cell_chunk( dim, n ) );
     J.nch_vec = int( ( n + VCHUNK - 1 ) / VCHUNK );
     J.ovf_cap = int( n ) + 4096;
     size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
@@ -709,6 +711,14 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         J->cap = D.dim == 2 ? CAP2 : CAP3;
         std::memcpy( J->opt, desc.options, sizeof( J->opt ) );
         J->agg_margin = J->opt[ SDOT_OPT_AGG_MARGIN ];
+        {
+            // the scale of a facet's coupling (gpu/Newton2D.cuh:1273): the density (uniform: rho; else the box's mean, 1 /
+            // volume) times, in 3D, the seeds' spacing
+            double vol = 1;
+            for ( int a = 0; a < D.dim; ++a ) vol *= D.box_hi[ a ] - D.box_lo[ a ];
+            J->c_scale = ( D.density.kind == SDOT_DENSITY_UNIFORM ? D.density.value : 1.0 / std::max( vol, 1e-300 ) ) *
+                         ( D.dim == 3 ? std::cbrt( vol / double( std::max<long>( D.n, 1 ) ) ) : 1.0 );
+        }
         J->lim_on = D.dim == 2 && int( J->opt[ SDOT_OPT_STEP ] ) == 1;     // (3D: the trials, as the reference)
         for ( int k = 0; k < SDOT_NB_STATS; ++k ) J->stats[ k ] = 0;
         const long n = D.n;
@@ -769,6 +779,7 @@ void job_destroy( Ctx &c, SolveJob *J ) {
     if ( J->mg_mem ) dfree( c, J->mg_mem );
     if ( J->mx_mem ) dfree( c, J->mx_mem );
     if ( J->d_cl ) dfree( c, J->d_cl );
+    if ( J->cl_true ) dfree( c, J->cl_true );
     if ( J->ae ) dfree( c, J->ae );
     if ( J->mem ) dfree( c, J->mem );
     if ( J->G.mem ) free_geometry( c, J->G );
@@ -1124,10 +1135,10 @@ static int uf_find( std::vector<int> &p, int i ) {
 
 // the pairs the last Laplacian showed: merged (latched, a cluster only grows), the clusters rebuilt and uploaded
 // (sdotplan/Aggregation.h:109-141, 229-250)
-static void agg_update( Ctx &c, SolveJob &J ) {
+static bool agg_update( Ctx &c, SolveJob &J ) {
     double *cnt = c.hscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_AGG;
     const int k = std::min( int( *cnt ), AGG_CAP );
-    if ( k <= 0 ) return;
+    if ( k <= 0 ) return false;
     std::vector<int2> pairs( k );
     CK( cudaMemcpy( pairs.data(), J.agg_pairs, size_t( k ) * sizeof( int2 ), cudaMemcpyDeviceToHost ) );
     CK( cudaMemsetAsync( c.dscal + size_t( J.slot ) * SLOT_DOUBLES + SLOT_AGG, 0, sizeof( double ), c.stream ) );
@@ -1144,7 +1155,7 @@ static void agg_update( Ctx &c, SolveJob &J ) {
         J.agg_parent[ std::max( a, b ) ] = std::min( a, b );
         changed = true;
     }
-    if ( ! changed ) return;
+    if ( ! changed ) return false;
     std::vector<int> size( n, 0 ), id( n, -1 );
     for ( int i = 0; i < n; ++i ) ++size[ uf_find( J.agg_parent, i ) ];
     J.cl_begin.assign( 1, 0 );
@@ -1163,9 +1174,12 @@ static void agg_update( Ctx &c, SolveJob &J ) {
     J.d_cl = ( int * ) dalloc( c, dev.size() * sizeof( int ) );
     CK( cudaMemcpyAsync( J.d_cl, dev.data(), dev.size() * sizeof( int ), cudaMemcpyHostToDevice, c.stream ) );
     if ( ! J.ae ) J.ae = ( double * ) dalloc( c, size_t( n ) * 8 );
+    if ( J.cl_true ) dfree( c, J.cl_true );
+    J.cl_true = ( double * ) dalloc( c, J.cl_members.size() * ( AGG_KMAX + 2 ) * sizeof( double ) );
     CK( cudaStreamSynchronize( c.stream ) );       // `dev` leaves scope
     J.stats[ ST_NB_CLUSTERS ] = J.ncl;
     J.stats[ ST_NB_AGGREGATED ] = double( J.cl_members.size() );
+    return true;
 }
 
 // the residual of the full problem (every cell its own target), at the accepted masses: max |a - nu| and its relative
@@ -1185,7 +1199,12 @@ static void full_residual( Ctx &c, SolveJob &J, double &worst, double &worst_rel
 }
 
 static void decide( Ctx &c, SolveJob &J, bool had_diag, bool had_cg ) {
-    if ( J.agg_margin > 0 ) agg_update( c, J );
+    if ( J.agg_margin > 0 && agg_update( c, J ) && J.state == J_CG ) {
+        // new clusters on the Laplacian the CG is solving: the system again, with their couplings capped and the direction
+        // tied and corrected after the solve (the reference card merges before its solve, gpu/Newton2D.cuh:1557-1612)
+        J.pend |= P_NEWTON;
+        had_cg = false;
+    }
     if ( had_diag && c.hscal[ size_t( J.slot ) * SLOT_DOUBLES + SLOT_ERR ] != 0 ) {
         // a cell past every capacity: this solve stops with the reference's "card capacity" status (the others go on);
         // its outputs are the moments at the last accepted weights
@@ -1415,6 +1434,7 @@ static VecDev vec_of( Ctx &c, SolveJob &J ) {
         V.agg_margin = J.agg_margin;
         V.agg_tol_abs = J.opt[ SDOT_OPT_TOL_ABS ];
         V.agg_tol_rel = J.opt[ SDOT_OPT_TOL_REL ];
+        V.agg_ccond = 1e9 * J.c_scale;
     }
     return V;
 }
@@ -1707,6 +1727,9 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             bool agg = false;
             for ( auto &v : B->v ) agg |= v.agg_pairs != nullptr;
             if ( agg ) launch_agg_detect( L, B->dv, B->dch, nch );
+            for ( const SolveJob *J : B->jobs )
+                if ( J && J->ncl > 0 && J->cl_true )
+                    launch_agg_cap( L, J->row_ptr, J->col, J->val, J->dia, J->d_cl, J->ncl, 1e6 * J->c_scale, J->cl_true );
             launch_rhs( L, B->dv, B->dch, nch );
             const bool mixed = B == &jacx || B == &mgbx;
             if ( B->mg() ) {
@@ -1723,6 +1746,10 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             c.timer.end( c.stream, 5 );
         }
     }
+    for ( SolveJob *J : jobs )
+        if ( ( J->pend & P_GAUGE ) && J->ncl > 0 && J->cl_true )
+            launch_agg_direction( L, J->row_ptr, J->col, J->val, J->d_cl, J->ncl, J->cl_true, J->nu, J->b, J->x,
+                                  J->cl_true + J->cl_members.size() * ( AGG_KMAX + 1 ) );
     if ( ! gauge.v.empty() ) {
         gauge.upload( c );
         launch_gauge( L, gauge.dv, gauge.dch, int( gauge.ch.size() ) );
@@ -1757,7 +1784,8 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             const int qi = int( Q.size() );
             Q.push_back( P );
             int k = 0;
-            for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) QC.push_back( Chunk{ qi, b, std::min( J->G.n, b + CHUNK ), k } );
+            const int cs = cell_chunk( J->G.dim, J->G.n );
+            for ( int b = 0; b < J->G.n; b += cs, ++k ) QC.push_back( Chunk{ qi, b, std::min( J->G.n, b + cs ), k } );
         }
         const size_t oq = ( Q.size() * sizeof( ProbDev ) + 255 ) & ~size_t( 255 );
         std::vector<char> buf( oq + QC.size() * sizeof( Chunk ) );
@@ -1821,7 +1849,8 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         P.chunk0 = int( CC.size() );
         PP.push_back( P );
         int k = 0;
-        for ( int b = 0; b < J->G.n; b += CHUNK, ++k ) CC.push_back( Chunk{ pi, b, std::min( J->G.n, b + CHUNK ), k } );
+        const int cs = cell_chunk( J->G.dim, J->G.n );
+        for ( int b = 0; b < J->G.n; b += cs, ++k ) CC.push_back( Chunk{ pi, b, std::min( J->G.n, b + cs ), k } );
     }
     // the problems of this tick's diagrams in ONE array (both dimensions), so that the big-cell queue's problem indices mean
     // the same thing to every kernel: [ 2D normal | 2D final (moments) | 3D normal | 3D final ], flags uniform per launch

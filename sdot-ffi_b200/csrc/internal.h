@@ -21,6 +21,16 @@
 namespace sdot {
 
 constexpr int CHUNK = 64;              // seeds per chunk (one block of the cell kernels)
+// seeds per chunk of one problem's diagram: CHUNK for a large problem; for a small one fewer seeds per warp, so that its
+// diagram still spreads over the 148 SMs (the warps the main cell kernels keep resident: 24 an SM in 2D, 16 in 3D).  A
+// function of the problem alone, so that its report folds its chunks in the same order alone and in any batch
+inline int cell_chunk( int dim, long n ) {
+    const long resident = dim == 2 ? 148L * 24 : 148L * 16;
+    const int warps = dim == 2 ? 8 : 4;                   // warps a block of k_cells2d / k_cells3d
+    long per_warp = n / resident;
+    per_warp = per_warp < 1 ? 1 : ( per_warp > CHUNK / warps ? CHUNK / warps : per_warp );
+    return int( per_warp * warps );
+}
 constexpr int CAP2 = 32;               // neighbour table capacity per cell, 2D
 constexpr int CAP3 = 64;               // ... 3D
 constexpr int NB_REPORT = 12;          // doubles of the per-diagram report
@@ -177,6 +187,7 @@ struct VecDev {
     int agg_cap;
     double *agg_count;
     double agg_margin, agg_tol_abs, agg_tol_rel;
+    double agg_ccond;             // a coupling past this is merged whatever the weights (1e9 times the scale of a facet)
 };
 // one level of the multigrid preconditioner of one problem (mg.cu)
 constexpr int MG_BOTTOM = 32;          // the coarsest level has at most this many rows (dense inverse)
@@ -375,6 +386,13 @@ void launch_gauge( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 void launch_polish_weights( const Launch &L, const double *w, double *w2, int n, double shift, const int *idx, const double *val, int k );
 // the pairs the aggregation merges (VecDev.agg_*)
 void launch_agg_detect( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
+// the direction with clusters: their internal couplings capped at `cap` in the CSR the CG solves (the true ones kept in
+// `blk`, [ members ][ AGG_KMAX + 1 ]), then after the solve the members tied and the split corrected by the true local
+// systems (`y`: [ members ] scratch); `cl` = [ begins (ncl + 1) | members ]
+constexpr int AGG_KMAX = 16;
+void launch_agg_cap( const Launch &L, const int *row_ptr, const int *col, double *val, double *dia, const int *cl, int ncl, double cap, double *blk );
+void launch_agg_direction( const Launch &L, const int *row_ptr, const int *col, const double *val, const int *cl, int ncl, const double *blk,
+                           const double *nu, const double *b, double *x, double *y );
 // the cluster shares of the masses: ae[ i ] = nu[ i ] a_C / nu_C for the members i of each cluster C (others untouched)
 void launch_agg_shares( const Launch &L, const double *a, const double *nu, const int *cl_begin, const int *cl_members, int ncl, double *ae );
 // the multigrid-preconditioned CG: init in two halves around the first V-cycle, then per iteration

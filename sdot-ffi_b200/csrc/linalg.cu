@@ -773,7 +773,8 @@ __global__ void __launch_bounds__( VT ) k_agg_detect( const VecDev *__restrict__
             const double ulp = __longlong_as_double( __double_as_longlong( wm ) + 1 ) - wm;     // the spacing of the doubles at wm
             const double nm = fmin( V.nu[ i ], V.nu[ j ] );
             const double tau = fmax( V.agg_tol_abs, fmax( V.agg_tol_rel * nm, 1e-12 * nm ) );
-            if ( V.val[ e ] * ulp * V.agg_margin > tau ) {
+            // (a coupling past 1e9 times the scale of a facet is merged whatever the weights: gpu/Newton2D.cuh:1287-1313)
+            if ( V.val[ e ] * ulp * V.agg_margin > tau || V.val[ e ] > V.agg_ccond ) {
                 const int k = int( atomicAdd( V.agg_count, 1.0 ) );
                 if ( k < V.agg_cap ) V.agg_pairs[ k ] = make_int2( i, j );
             }
@@ -784,6 +785,126 @@ __global__ void __launch_bounds__( VT ) k_agg_detect( const VecDev *__restrict__
 void launch_agg_detect( const Launch &L, const VecDev *v, const Chunk *ch, int nch ) {
     if ( nch <= 0 ) return;
     k_agg_detect<<<nch, VT, 0, L.stream>>>( v, ch, nch );
+    ++*L.launches;
+}
+
+// THE DIRECTION WITH CLUSTERS (the reference card's rule, gpu/Newton2D.cuh:443-478, 1386-1440, 1565-1612): the coupling
+// between two members of a cluster (2.5e10 for a pair 1e-12 apart) is capped at `cap` in the system the CG solves -- the
+// multigrid's FP32 levels do not hold it -- and the true couplings kept aside for the correction after the solve.  One
+// thread per cluster (members sorted by rank): blk[ q * ( AGG_KMAX + 1 ) + p ] the true coupling of member q to member p,
+// blk[ q * ( AGG_KMAX + 1 ) + AGG_KMAX ] the true diagonal of member q (kept for clusters of at most AGG_KMAX members)
+__device__ __forceinline__ int member_of( const int *clm, int b0, int b1, int j ) {
+    int lo = b0, hi = b1;
+    while ( lo < hi ) { const int mid = ( lo + hi ) >> 1; if ( clm[ mid ] < j ) lo = mid + 1; else hi = mid; }
+    return lo < b1 && clm[ lo ] == j ? lo - b0 : -1;
+}
+
+__global__ void k_agg_cap( const int *__restrict__ row_ptr, const int *__restrict__ col, double *val, double *dia, const int *__restrict__ clb,
+                           const int *__restrict__ clm, int ncl, double cap, double *blk ) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if ( c >= ncl ) return;
+    const int b0 = clb[ c ], b1 = clb[ c + 1 ], k = b1 - b0;
+    for ( int q = b0; q < b1; ++q ) {
+        const int i = clm[ q ];
+        double *T = blk + size_t( q ) * ( AGG_KMAX + 1 );
+        if ( k <= AGG_KMAX ) {
+            for ( int p = 0; p < k; ++p ) T[ p ] = 0;
+            T[ AGG_KMAX ] = dia[ i ];
+        }
+        bool capped = false;
+        for ( int e = row_ptr[ i ]; e < row_ptr[ i + 1 ]; ++e ) {
+            const int p = member_of( clm, b0, b1, col[ e ] );
+            if ( p < 0 ) continue;
+            if ( k <= AGG_KMAX ) T[ p ] = val[ e ];
+            if ( val[ e ] > cap ) { val[ e ] = cap; capped = true; }
+        }
+        if ( capped ) {                  // the diagonal summed again, in row order
+            double d = 0;
+            for ( int e = row_ptr[ i ]; e < row_ptr[ i + 1 ]; ++e ) d += val[ e ];
+            dia[ i ] = d > 0 ? d : 1.0;
+        }
+    }
+}
+
+void launch_agg_cap( const Launch &L, const int *row_ptr, const int *col, double *val, double *dia, const int *cl, int ncl, double cap, double *blk ) {
+    if ( ncl <= 0 ) return;
+    k_agg_cap<<<( ncl + 127 ) / 128, 128, 0, L.stream>>>( row_ptr, col, val, dia, cl, cl + ncl + 1, ncl, cap, blk );
+    ++*L.launches;
+}
+
+// ... after the solve of the capped system: each cluster's members tied to their cluster's direction, `x_i = sum nu_j x_j /
+// sum nu_j`, then the split inside the cluster corrected by its exact local system, the rest of x fixed: `L_CC y = b_C -
+// ( L x )_C` with the TRUE couplings, y's mean over the cluster (weighted by the targets) taken out, x_C += y -- one
+// two-level step.  One block: the ties of every cluster, then (reading the tied x) the corrections into `y`, then the sums,
+// so that a cluster never reads another's half-updated members
+__global__ void __launch_bounds__( 128 ) k_agg_direction( const int *__restrict__ row_ptr, const int *__restrict__ col, const double *__restrict__ val,
+                                                         const int *__restrict__ clb, const int *__restrict__ clm, int ncl, const double *__restrict__ blk,
+                                                         const double *__restrict__ nu, const double *__restrict__ b, double *x, double *y ) {
+    for ( int c = threadIdx.x; c < ncl; c += blockDim.x ) {
+        double s = 0, sn = 0;
+        for ( int q = clb[ c ]; q < clb[ c + 1 ]; ++q ) { s += nu[ clm[ q ] ] * x[ clm[ q ] ]; sn += nu[ clm[ q ] ]; }
+        const double xm = sn > 0 ? s / sn : 0.0;
+        for ( int q = clb[ c ]; q < clb[ c + 1 ]; ++q ) x[ clm[ q ] ] = xm;
+    }
+    __syncthreads();
+    for ( int c = threadIdx.x; c < ncl; c += blockDim.x ) {
+        const int b0 = clb[ c ], b1 = clb[ c + 1 ], k = b1 - b0;
+        for ( int q = b0; q < b1; ++q ) y[ q ] = 0;
+        if ( k > AGG_KMAX ) continue;
+        double M[ AGG_KMAX * AGG_KMAX ], r[ AGG_KMAX ];
+        for ( int q = 0; q < k; ++q ) {
+            const int i = clm[ b0 + q ];
+            const double *T = blk + size_t( b0 + q ) * ( AGG_KMAX + 1 );
+            double ld = T[ AGG_KMAX ] * x[ i ];
+            for ( int e = row_ptr[ i ]; e < row_ptr[ i + 1 ]; ++e ) {
+                const int p = member_of( clm, b0, b1, col[ e ] );
+                ld -= ( p >= 0 ? T[ p ] : val[ e ] ) * x[ col[ e ] ];
+            }
+            r[ q ] = b[ i ] - ld;
+            for ( int p = 0; p < k; ++p ) M[ q * k + p ] = p == q ? T[ AGG_KMAX ] : -T[ p ];
+        }
+        // Cholesky of the k x k block (positive definite when the cluster has a neighbour outside it), then the solve
+        bool ok = true;
+        for ( int j = 0; j < k && ok; ++j ) {
+            double d = M[ j * k + j ];
+            for ( int p = 0; p < j; ++p ) d -= M[ j * k + p ] * M[ j * k + p ];
+            if ( ! ( d > 0 ) ) { ok = false; break; }
+            const double l = sqrt( d );
+            M[ j * k + j ] = l;
+            for ( int i = j + 1; i < k; ++i ) {
+                double v = M[ i * k + j ];
+                for ( int p = 0; p < j; ++p ) v -= M[ i * k + p ] * M[ j * k + p ];
+                M[ i * k + j ] = v / l;
+            }
+        }
+        if ( ! ok ) continue;
+        for ( int i = 0; i < k; ++i ) {
+            double v = r[ i ];
+            for ( int p = 0; p < i; ++p ) v -= M[ i * k + p ] * r[ p ];
+            r[ i ] = v / M[ i * k + i ];
+        }
+        for ( int i = k - 1; i >= 0; --i ) {
+            double v = r[ i ];
+            for ( int p = i + 1; p < k; ++p ) v -= M[ p * k + i ] * r[ p ];
+            r[ i ] = v / M[ i * k + i ];
+        }
+        double s = 0, sn = 0;
+        for ( int q = 0; q < k; ++q ) { s += nu[ clm[ b0 + q ] ] * r[ q ]; sn += nu[ clm[ b0 + q ] ]; }
+        const double m = sn > 0 ? s / sn : 0.0;
+        bool fin = true;
+        for ( int q = 0; q < k; ++q ) fin = fin && isfinite( r[ q ] - m );
+        if ( fin )
+            for ( int q = 0; q < k; ++q ) y[ b0 + q ] = r[ q ] - m;
+    }
+    __syncthreads();
+    for ( int c = threadIdx.x; c < ncl; c += blockDim.x )
+        for ( int q = clb[ c ]; q < clb[ c + 1 ]; ++q ) x[ clm[ q ] ] += y[ q ];
+}
+
+void launch_agg_direction( const Launch &L, const int *row_ptr, const int *col, const double *val, const int *cl, int ncl, const double *blk,
+                           const double *nu, const double *b, double *x, double *y ) {
+    if ( ncl <= 0 ) return;
+    k_agg_direction<<<1, 128, 0, L.stream>>>( row_ptr, col, val, cl, cl + ncl + 1, ncl, blk, nu, b, x, y );
     ++*L.launches;
 }
 
