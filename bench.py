@@ -293,20 +293,13 @@ def run_served(reqs, seed, lam):
     return max(done.values()), np.array(lat), h2d, d2h, worst[0], counters, failed[0]
 
 
-# ---- the CPU legs: the oracle in a worker process under a hard wall limit ---------------------------------------------------
+# ---- the CPU legs: the oracle in worker processes under hard wall limits ---------------------------------------------------
 # measured oracle cost per seed of one solve (8 threads): 2D uniform ~40 us, 3D uniform ~110 us, 2D gaussians ~1.5 ms
 # (13 continuation stages); 3D gaussians ~1 s (adaptive tetrahedral quadrature: 956 s for one solve of 1,000 seeds)
-CPU_COST_PER_SEED = {(2, False): 4e-5, (3, False): 1.1e-4, (2, True): 1.5e-3, (3, True): 1.0}
-
-
-def cpu_eligible(r, cap_s):
-    """a request the CPU leg runs: not a 3D gaussian (minutes to hours per solve on the oracle), and a predicted cost
-    under `cap_s` seconds"""
-    return not (r["d"] == 3 and r["gauss"]) and CPU_COST_PER_SEED[(r["d"], r["gauss"])] * r["n"] <= cap_s
 
 
 def cpu_worker(seed, ks):
-    """(child process) the oracle's solve of each request k of `ks` in turn, one JSON line per finished solve"""
+    """(child process) the oracle's solve of each request k of `ks` in turn: a line when a solve starts, one when it ends"""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     print(json.dumps({"threads": O.max_threads()}), flush=True)
@@ -316,50 +309,80 @@ def cpu_worker(seed, ks):
         dens = t._sdot_density()
         od = ("uniform", dens[1]) if dens[0] == "uniform" else ("gauss", dens[1], dens[2], dens[3])
         lo, hi = t.box() if hasattr(t, "box") else (np.zeros(r["d"]), np.ones(r["d"]))
+        print(json.dumps({"start": k}), flush=True)
         t0 = time.perf_counter()
         s = O.solve(positions(seed, r), box=(lo, hi), density=od, tol_abs=0.0, tol_rel=RTOL, lin_tol=1e-8, agg_margin=4.0)
         print(json.dumps({"k": k, "n": r["n"], "secs": time.perf_counter() - t0, "ok": s["stats"]["status"] in CONVERGED}), flush=True)
 
 
-def cpu_sample(reqs, seed, budget_s=20.0, cap_s=8.0):
-    """the oracle (the CPU restatement of the reference's algorithm) on the eligible requests of `reqs`, in stream order,
-    in a worker process killed at `budget_s` of wall time (a hard limit: no solve can overrun it).  value = the solves
-    that met the tolerance / the seconds of the finished solves; a solve cut by the limit is not counted"""
-    ks = [r["k"] for r in reqs if cpu_eligible(r, cap_s)]
-    left_out = sum(1 for r in reqs if r["d"] == 3 and r["gauss"])
-    too_big = len(reqs) - left_out - len(ks)
-    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", ",".join(map(str, ks)), "--seed", str(seed)]
-    proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-    rows, threads = [], [None]
+def cpu_sample(reqs, seed, budget_s=20.0, cap_s=5.0):
+    """the oracle (the CPU restatement of the reference's algorithm) on a seeded random sample of `reqs` -- every kind and
+    size of the stream, none left out -- each request solved in a worker process under a hard limit of `cap_s` seconds,
+    the whole leg under `budget_s` of wall time.  A request past its limit is killed and counted unsolved with the limit
+    as its time (it would take longer): value = solves that met the tolerance / seconds of the sampled requests, an UPPER
+    bound of the CPU's throughput on this mix"""
+    order = [reqs[i] for i in np.random.default_rng([seed, 7]).permutation(len(reqs))]
+    todo = [r["k"] for r in order]
+    by_k = {r["k"]: r for r in order}
+    rows, threads, t_start = [], [None], time.perf_counter()
+    while todo and time.perf_counter() - t_start < budget_s:
+        cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", ",".join(map(str, todo)), "--seed", str(seed)]
+        proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        cur = [None, 0.0]                   # the request being solved, and when it started
+        lock = threading.Lock()
 
-    def read():
-        for line in proc.stdout:
-            try:
-                d = json.loads(line)
-            except ValueError:
-                continue
-            if "threads" in d:
-                threads[0] = d["threads"]
-            else:
-                rows.append(d)
+        def read():
+            for line in proc.stdout:
+                try:
+                    d = json.loads(line)
+                except ValueError:
+                    continue
+                with lock:
+                    if "threads" in d:
+                        threads[0] = d["threads"]
+                    elif "start" in d:
+                        cur[0], cur[1] = d["start"], time.perf_counter()
+                    else:
+                        rows.append(dict(d, capped=False))
+                        todo.remove(d["k"])
+                        cur[0] = None
 
-    th = threading.Thread(target=read, daemon=True)
-    th.start()
-    try:
-        proc.wait(timeout=budget_s)
-    except subprocess.TimeoutExpired:
-        proc.kill()
+        th = threading.Thread(target=read, daemon=True)
+        th.start()
+        killed = None
+        while proc.poll() is None:
+            time.sleep(0.02)
+            with lock:
+                over_cap = cur[0] is not None and time.perf_counter() - cur[1] > cap_s
+                over_budget = time.perf_counter() - t_start > budget_s
+                if over_cap or over_budget:
+                    killed = (cur[0], time.perf_counter() - cur[1]) if cur[0] is not None else None
+                    proc.kill()
         proc.wait()
-    th.join(timeout=5)
+        th.join(timeout=5)
+        if killed is not None:
+            k, el = killed
+            rows.append(dict(k=k, n=by_k[k]["n"], secs=min(el, cap_s), ok=False, capped=True))
+            todo.remove(k)
+        if killed is None and proc.returncode not in (0, None) and not rows:
+            break
     secs = sum(d["secs"] for d in rows)
     solved = sum(1 for d in rows if d["ok"])
-    n_tot = sum(d["n"] for d in rows)
+    kinds = {}
+    for d in rows:
+        r = by_k[d["k"]]
+        key = f"{r['d']}D {'gaussian' if r['gauss'] else 'uniform'}"
+        e = kinds.setdefault(key, [0, 0, 0])
+        e[0] += 1
+        e[1] += bool(d["ok"])
+        e[2] += bool(d["capped"])
+    desc = ", ".join(f"{k}: {v[0]} ({v[1]} solved, {v[2]} past the limit)" for k, v in sorted(kinds.items()))
     return dict(value=solved / secs if secs > 0 else None, unit="solves/s", cores=threads[0] or os.cpu_count(), kind="port",
-                sample=f"{len(rows)} of the {len(ks)} eligible requests finished within a {budget_s:.0f} s wall limit (stream order, "
-                       f"sum N = {n_tot}, {solved} met the tolerance, {sum(d['secs'] for d in rows):.1f} s of solves); left out: "
-                       f"{left_out} 3D-gaussian requests (the oracle's adaptive quadrature takes ~1 s per seed per solve) and {too_big} "
-                       f"whose predicted oracle time exceeds {cap_s:.0f} s; both leave-outs flatter the CPU. oracle/sdot_oracle.c "
-                       f"FP64 + OpenMP, same tolerance: the CPU restatement of sdot's algorithm, not the reference binary")
+                sample=f"{len(rows)} requests drawn at random from the timed ones ({desc}; sum N = {sum(d['n'] for d in rows)}), each "
+                       f"solved under a {cap_s:.0f} s limit within a {budget_s:.0f} s leg; a request past its limit counts as unsolved "
+                       f"with the limit as its time, so the value is an upper bound of the CPU's solves/s on this mix. "
+                       f"oracle/sdot_oracle.c FP64 + OpenMP, same tolerance: the CPU restatement of sdot's algorithm, not the "
+                       f"reference binary")
 
 
 def peaks():
@@ -407,8 +430,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--requests-per-step", type=int, default=8)
     ap.add_argument("--seed", type=int, default=2026)
-    ap.add_argument("--cpu-budget", type=float, default=20.0, help="wall limit (s) of the GPU arm's CPU-baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=30.0, help="wall limit (s) of the GPU arm's CPU-baseline leg")
+    ap.add_argument("--cpu-cap", type=float, default=10.0, help="wall limit (s) of one request's CPU solve (GPU arm's CPU leg)")
     ap.add_argument("--ref-budget", type=float, default=150.0, help="wall limit (s) of the reference arm's CPU solves")
+    ap.add_argument("--ref-cap", type=float, default=15.0, help="wall limit (s) of one request's CPU solve (reference arm)")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cells-only", type=int, default=0, help="diagrams of this many uniform seeds (for a profiler), then exit")
     ap.add_argument("--cells-dim", type=int, default=2)
@@ -483,7 +508,7 @@ def main():
             return
         # the timed slices of the GPU arm's stream, solved by the oracle on every host core under a hard wall limit
         reqs, skipped = stream(a.seed, (a.warmup + a.steps) * R, lambda r: True)
-        cpu = cpu_sample(reqs[a.warmup * R:], a.seed, budget_s=a.ref_budget)
+        cpu = cpu_sample(reqs[a.warmup * R:], a.seed, budget_s=a.ref_budget, cap_s=a.ref_cap)
         v = cpu["value"]
         config["reference_step"] = f"a step's {R} requests at the measured CPU throughput (ms_per_step = R / value)"
         print(json.dumps({"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
@@ -565,7 +590,7 @@ def main():
     cells_b = units * BYTES_PER_CELL[dom]
     achieved = cells_b / (ms / 1000) / 1e9 if ms > 0 else None
     cg_ms, cg_n, cg_rows = kst["cg"]
-    cpu = cpu_sample(timed, a.seed, a.cpu_budget) if rank == 0 else None
+    cpu = cpu_sample(timed, a.seed, a.cpu_budget, a.cpu_cap) if rank == 0 else None
     legs["cpu"] = time.perf_counter() - t_leg
     if rank != 0:
         dist.destroy_process_group()

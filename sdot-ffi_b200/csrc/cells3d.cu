@@ -517,57 +517,74 @@ __device__ __forceinline__ double edge_angle3( double Fx, double Fy, double Fz, 
 
 // A = int erfc( r / s sqrt2 ) / r dtheta and B = int exp( -R^2 / 2 s^2 ) dtheta along the edge K -> T of a face (F the
 // foot of the centre on the face's plane, n its unit normal, h the centre's distance to the plane, r^2 = h^2 + R^2),
-// signed as `edge_angle3`.  erfc( k r ) = exp( -k^2 h^2 ) exp( -k^2 R^2 ) erfcx( k r ): one exponential serves both
-__device__ __noinline__ void edge_gauss3( double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty, double Tz,
-                                          double nx, double ny, double nz, double h, double sg, double &A, double &B ) {
-    A = B = 0;
+// signed as `edge_angle3`.  erfc( k r ) = exp( -k^2 h^2 ) exp( -k^2 R^2 ) erfcx( k r ): one exponential serves both.
+// An EDGE ITEM holds one such integral between its pieces: `edge_setup3` places the pieces, `edge_piece3` integrates one
+// (8 Gauss-Legendre points) -- so that the lanes of a warp can each hold a different edge and take the next one as soon
+// as theirs is done, instead of the whole warp waiting for its longest edge
+struct EdgeItem3 {
+    double d, h2, k2, kr, eh, us, chs, vs, kd, v0, dv, u1, ua, A, B, sgn;
+    int np, j;
+};
+
+__device__ __forceinline__ void edge_setup3( EdgeItem3 &I, double Fx, double Fy, double Fz, double Kx, double Ky, double Kz, double Tx, double Ty,
+                                             double Tz, double nx, double ny, double nz, double h, double sg ) {
+    I.A = I.B = 0;
+    I.np = I.j = 0;
     const double ax = Kx - Fx, ay = Ky - Fy, az = Kz - Fz, ex = Tx - Kx, ey = Ty - Ky, ez = Tz - Kz;
     const double L = sqrt( ex * ex + ey * ey + ez * ez );
     if ( ! ( L > 0 ) ) return;
-    const double ux = ex / L, uy = ey / L, uz = ez / L;
+    const double iL = 1 / L, ux = ex * iL, uy = ey * iL, uz = ez * iL;
     const double s0 = ax * ux + ay * uy + az * uz, s1 = s0 + L;
     const double qx = ax - s0 * ux, qy = ay - s0 * uy, qz = az - s0 * uz;
     const double d = sqrt( qx * qx + qy * qy + qz * qz );
     if ( ! ( d > 0 ) ) return;
     const double bx = Tx - Fx, by = Ty - Fy, bz = Tz - Fz;
     const double o = -( nx * ( ay * bz - az * by ) + ny * ( az * bx - ax * bz ) + nz * ( ax * by - ay * bx ) );
-    const double sgn = o >= 0 ? 1.0 : -1.0;
+    I.sgn = o >= 0 ? 1.0 : -1.0;
     // (past |s / d| = 1e17, u = 40.4, the kernel 1 / cosh u is under 1e-17)
-    const double u0 = asinh( fmax( -1e17, fmin( 1e17, s0 / d ) ) ), u1 = asinh( fmax( -1e17, fmin( 1e17, s1 / d ) ) );
+    const double id = 1 / d;
+    const double x0 = fmax( -1e17, fmin( 1e17, s0 * id ) ), x1 = fmax( -1e17, fmin( 1e17, s1 * id ) );
+    const double u0 = asinh( x0 ), u1 = asinh( x1 );
     const double fs = G3_FR * sg, c = fmin( 1e17, fs / ( G3_WU * d ) );      // sinh of the u where the two bounds meet
-    const double us = asinh( c ), chs = sqrt( 1 + c * c ), vs = us / G3_WU, kd = d / fs;
-    auto V = [&]( double u ) {
+    I.us = asinh( c ); I.chs = sqrt( 1 + c * c ); I.vs = I.us / G3_WU; I.kd = d / fs;
+    auto V = [&]( double u, double x ) {          // (cosh u = sqrt( 1 + x^2 ) at u = asinh x)
         const double a = fabs( u );
-        return copysign( a <= us ? a / G3_WU : vs + kd * ( cosh( a ) - chs ), u );
+        return copysign( a <= I.us ? a / G3_WU : I.vs + I.kd * ( sqrt( 1 + x * x ) - I.chs ), u );
     };
-    auto Vinv = [&]( double v ) {
-        const double a = fabs( v );
-        return copysign( a <= vs ? a * G3_WU : acosh( chs + ( a - vs ) / kd ), v );
-    };
-    const double v0 = V( u0 ), v1 = V( u1 );
-    const int np = max( 1, min( G3_MAX_PIECES, int( ceil( v1 - v0 ) ) ) );
-    const double dv = ( v1 - v0 ) / np, kr = 0.7071067811865476 / sg, k2 = kr * kr, h2 = h * h;
-    const double eh = exp( -k2 * h2 );
-    double ua = u0;
-    for ( int j = 0; j < np; ++j ) {
-        const double ub = j + 1 == np ? u1 : Vinv( v0 + ( j + 1 ) * dv );
-        const double hw = 0.5 * ( ub - ua ), mid = 0.5 * ( ub + ua );
-#pragma unroll 2
-        for ( int q = 0; q < 8; ++q ) {
-            const double uq = mid + hw * c_g3x[ q ], w = hw * c_g3w[ q ];
-            const double eu = exp( uq ), ich = 2 / ( eu + 1 / eu );       // 1 / cosh u
-            const double R = d / ich, R2 = R * R;
-            const double gw = w * ich * exp( -k2 * R2 );
-            B += gw;
-            if ( h != 0 ) {
-                const double r = sqrt( h2 + R2 );
-                A += gw * eh * erfcx( kr * r ) / r;
-            }
-        }
-        ua = ub;
+    I.v0 = V( u0, x0 );
+    const double v1 = V( u1, x1 );
+    I.np = max( 1, min( G3_MAX_PIECES, int( ceil( v1 - I.v0 ) ) ) );
+    I.dv = ( v1 - I.v0 ) / I.np;
+    I.kr = 0.7071067811865476 / sg; I.k2 = I.kr * I.kr; I.h2 = h * h;
+    I.eh = exp( -I.k2 * I.h2 );
+    I.d = d; I.u1 = u1; I.ua = u0;
+}
+
+__device__ __forceinline__ void edge_piece3( EdgeItem3 &I ) {
+    double ub = I.u1;
+    if ( I.j + 1 < I.np ) {
+        const double a = fabs( I.v0 + ( I.j + 1 ) * I.dv );
+        ub = copysign( a <= I.vs ? a * G3_WU : acosh( I.chs + ( a - I.vs ) / I.kd ), I.v0 + ( I.j + 1 ) * I.dv );
     }
-    A *= sgn;
-    B *= sgn;
+    const double hw = 0.5 * ( ub - I.ua ), mid = 0.5 * ( ub + I.ua );
+    double A = 0, B = 0;
+#pragma unroll 2
+    for ( int q = 0; q < 8; ++q ) {
+        const double uq = mid + hw * c_g3x[ q ], w = hw * c_g3w[ q ];
+        // 1 / cosh u = 2 e^u / ( e^2u + 1 ) and R = d cosh u, from one division
+        const double eu = exp( uq ), s1 = eu * eu + 1, iq = 1 / ( eu * s1 );
+        const double ich = 2 * eu * eu * iq, R = 0.5 * I.d * s1 * s1 * iq, R2 = R * R;
+        const double gw = w * ich * exp( -I.k2 * R2 );
+        B += gw;
+        if ( I.h2 != 0 ) {
+            const double r2 = I.h2 + R2, ir = rsqrt( r2 );
+            A += gw * I.eh * erfcx( I.kr * ( r2 * ir ) ) * ir;
+        }
+    }
+    I.A += A;
+    I.B += B;
+    I.ua = ub;
+    ++I.j;
 }
 
 // the gaussian sums over the clipped cell: lane parts of the mass, of the first moment about the seed and of
@@ -626,10 +643,10 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
         Fx += gx + cx * dM; Fy += gy + cy * dM; Fz += gz + cz * dM;
         S2 += s2g * ( 3 * dM - h * b ) + 2 * ( cx * gx + cy * gy + cz * gz ) + ( cx * cx + cy * cy + cz * cz ) * dM;
     };
-    // items are (gaussian of the group's selection, entry or face), lane-consecutive; with at least 32 entries (faces)
-    // per gaussian, the 32 items of one round hold distinct entries (faces), so their sums into `area` (`fmp`) never
-    // meet, and each entry's (face's) sum runs in gaussian order
-    const int NE = 3 * nv, NEp = NE > 32 ? NE : 32, NPp = np > 32 ? np : 32;
+    // the face items are (gaussian of the group's selection, face), lane-consecutive; with at least 32 faces per
+    // gaussian, the 32 items of one round hold distinct faces, so their sums into `fmp` never meet, and each face's sum
+    // runs in gaussian order
+    const int NE = 3 * nv, NPp = np > 32 ? np : 32;
     for ( int g0 = 0; g0 < ng; g0 += 32 ) {
         const int gn = min( 32, ng - g0 );
         unsigned sel = 0;
@@ -641,26 +658,59 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
             for ( int k = 0; k < i; ++k ) m &= m - 1;
             return g0 + __ffs( m ) - 1;
         };
-        // the edge integrals of every (gaussian, entry)
-        for ( int base = 0; base < ns * NEp; base += 32 ) {
-            const int idx = base + lane, gi = idx / NEp, e = idx - gi * NEp;
-            if ( gi < ns && e < NE && C.ad[ e % 3 ][ e / 3 ] != C3::NONE ) {
-                const int g = nth( gi ), k = e / 3, q = e - 3 * k, t = C.ad[ q ][ k ];
-                const int f = q == 0 ? C.va[ k ] : ( q == 1 ? C.vb[ k ] : C.vc[ k ] );
-                const double *G = P.dval + g * 5;
-                const double cx = G[ 0 ] - px, cy = G[ 1 ] - py, cz = G[ 2 ] - pz, sg = G[ 3 ], mg = G[ 4 ];
-                const double s2g = sg * sg, KG = mg / ( 15.749609945722419 * s2g * sg );          // (2 pi)^{3/2}
-                const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] );
-                const double nhx = C.nx[ f ] / nn, nhy = C.ny[ f ] / nn, nhz = C.nz[ f ] / nn;
-                const double h = ( C.no[ f ] - ( C.nx[ f ] * cx + C.ny[ f ] * cy + C.nz[ f ] * cz ) ) / nn;
-                double A, B;
-                edge_gauss3( cx + h * nhx, cy + h * nhy, cz + h * nhz, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx,
-                             nhy, nhz, h, sg, A, B );
-                const double b = -KG * exp( -h * h * 0.5 / s2g ) * s2g * B;
-                C.area[ e ] += b;
-                add( h * INV4PI * mg * A, b, h, nhx, nhy, nhz, cx, cy, cz, s2g );
+        // the edge integrals of every (gaussian, entry), as a queue: a lane whose item is done takes the next one (items
+        // in gaussian-major order), every lane integrates one piece of its item per step.  An item's part goes to its entry
+        // of `area` when it is done; two lanes finishing the same entry in one step add in lane order
+        {
+            const int total = ns * NE;
+            int nxt = 0, item = -1;
+            EdgeItem3 I;
+            I.np = I.j = 0;
+            double h = 0, nhx = 0, nhy = 0, nhz = 0, cx = 0, cy = 0, cz = 0, s2g = 0, mg = 0, KG = 0;
+            for ( int guard = 0; guard < 1 << 20; ++guard ) {
+                const bool need = item < 0;
+                const unsigned nm = __ballot_sync( FULL3, need );
+                const int mine = nxt + __popc( nm & ( ( 1u << lane ) - 1 ) );
+                nxt = min( total, nxt + __popc( nm ) );
+                if ( need && mine < total ) {
+                    item = mine;
+                    const int gi = mine / NE, e = mine - gi * NE, k = e / 3, q = e - 3 * k, t = C.ad[ q ][ k ];
+                    const int g = nth( gi );
+                    const double *G = P.dval + g * 5;
+                    const double sg = G[ 3 ];
+                    cx = G[ 0 ] - px; cy = G[ 1 ] - py; cz = G[ 2 ] - pz; mg = G[ 4 ];
+                    s2g = sg * sg; KG = mg / ( 15.749609945722419 * s2g * sg );          // (2 pi)^{3/2}
+                    if ( t == C3::NONE ) I.np = I.j = 0;
+                    else {
+                        const int f = q == 0 ? C.va[ k ] : ( q == 1 ? C.vb[ k ] : C.vc[ k ] );
+                        const double nn = sqrt( C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ] ), inn = 1 / nn;
+                        nhx = C.nx[ f ] * inn; nhy = C.ny[ f ] * inn; nhz = C.nz[ f ] * inn;
+                        h = ( C.no[ f ] - ( C.nx[ f ] * cx + C.ny[ f ] * cy + C.nz[ f ] * cz ) ) * inn;
+                        edge_setup3( I, cx + h * nhx, cy + h * nhy, cz + h * nhz, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ],
+                                     C.vz[ t ], nhx, nhy, nhz, h, sg );
+                    }
+                }
+                if ( ! __any_sync( FULL3, item >= 0 ) ) break;
+                if ( item >= 0 && I.j < I.np ) edge_piece3( I );
+                const bool done = item >= 0 && I.j >= I.np;
+                const unsigned dm = __ballot_sync( FULL3, done && I.np > 0 );
+                if ( done ) {
+                    const int e = item % NE;
+                    if ( I.np > 0 ) {
+                        const double A = I.sgn * I.A, B = I.sgn * I.B;
+                        const double b = -KG * I.eh * s2g * B;             // (eh = exp( -h^2 / 2 s^2 ))
+                        const unsigned same = __match_any_sync( dm, e );
+                        const int rank = __popc( same & ( ( 1u << lane ) - 1 ) ), nsame = __popc( same );
+                        for ( int r = 0; r < nsame; ++r ) {
+                            if ( r == rank ) C.area[ e ] += b;
+                            __syncwarp( same );
+                        }
+                        add( h * INV4PI * mg * A, b, h, nhx, nhy, nhz, cx, cy, cz, s2g );
+                    }
+                    item = -1;
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
         // per (gaussian, face): the winding angle of the face about the foot of c, its part of the face integral and of
         // the flux of the erfc field's constant part
@@ -675,15 +725,35 @@ __device__ __noinline__ void integrate_gauss3( C3 &C, const ProbDev &P, int lane
                 const double nhx = C.nx[ p ] / nn, nhy = C.ny[ p ] / nn, nhz = C.nz[ p ] / nn;
                 const double h = ( C.no[ p ] - ( C.nx[ p ] * cx + C.ny[ p ] * cy + C.nz[ p ] * cz ) ) / nn;
                 const double Fx0 = cx + h * nhx, Fy0 = cy + h * nhy, Fz0 = cz + h * nhz;
-                double th = 0;
+                // the face is convex: its winding angle about the foot is 2 pi inside (every edge turns the same way, the
+                // signs of `edge_angle3`'s cross products), 0 outside (both signs); a foot within 1e-6 (sine) of an edge's
+                // line takes the walk of the angles
+                int npos = 0, nneg = 0;
+                bool near = false;
                 for ( int k = C.remap[ p ]; k != C3::NONE; ) {
                     const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
                     const int t = C.ad[ q ][ k ];
-                    th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
+                    const double ax = C.vx[ k ] - Fx0, ay = C.vy[ k ] - Fy0, az = C.vz[ k ] - Fz0;
+                    const double bx = C.vx[ t ] - Fx0, by = C.vy[ t ] - Fy0, bz = C.vz[ t ] - Fz0;
+                    const double o = -( nhx * ( ay * bz - az * by ) + nhy * ( az * bx - ax * bz ) + nhz * ( ax * by - ay * bx ) );
+                    const double a2 = ax * ax + ay * ay + az * az, b2 = bx * bx + by * by + bz * bz;
+                    if ( ! ( o * o > 1e-12 * a2 * b2 ) ) near = true;
+                    else if ( o > 0 ) ++npos;
+                    else ++nneg;
                     k = C.nt[ k ][ q ];
                 }
-                const double kk = rint( th / TWO_PI );
-                const double Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
+                double Th = nneg == 0 ? TWO_PI : ( npos == 0 ? -TWO_PI : 0.0 );
+                if ( near ) {
+                    double th = 0;
+                    for ( int k = C.remap[ p ]; k != C3::NONE; ) {
+                        const int q = C.va[ k ] == p ? 0 : ( C.vb[ k ] == p ? 1 : 2 );
+                        const int t = C.ad[ q ][ k ];
+                        th += edge_angle3( Fx0, Fy0, Fz0, C.vx[ k ], C.vy[ k ], C.vz[ k ], C.vx[ t ], C.vy[ t ], C.vz[ t ], nhx, nhy, nhz );
+                        k = C.nt[ k ][ q ];
+                    }
+                    const double kk = rint( th / TWO_PI );
+                    Th = fabs( th - TWO_PI * kk ) < 1e-6 ? TWO_PI * kk : th;
+                }
                 if ( Th != 0 ) {
                     const double I = KG * exp( -h * h * 0.5 / s2g ) * s2g * Th;
                     C.fmp[ p ] += I;
@@ -1069,8 +1139,9 @@ __device__ void load3( C3 &C, const Split3 &sp, long long at, int lane ) {
 
 // the main kernel: one warp per cell, W3 cells of a chunk at a time.  mode 0: every cell whole.  mode 1 (pass 1) and
 // mode 2 (pass 2): the cells of a gaussian problem are clipped and stored by pass 1 and integrated by pass 2 (the report
-// too); the other problems are done whole by pass 1 and skipped by pass 2
-__global__ void __launch_bounds__( 32 * W3, 5 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
+// too); the other problems are done whole by pass 1 and skipped by pass 2.  (The warps' cells, about 55 KB of shared
+// memory a block, hold 4 blocks on an SM: the registers are bounded for 4, not more.)
+__global__ void __launch_bounds__( 32 * W3, 4 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                         unsigned flags, ErrRec *err, OvfList *ovf, int mode, Split3 sp ) {
     extern __shared__ char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
