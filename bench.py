@@ -442,6 +442,7 @@ def main():
                     help="cells-only / solve-only target: uniform, a 4-gaussian mixture like the stream's, or (2D solve-only) the "
                          "1024 x 1024 image of 16 gaussians plus a 1 %% floor")
     ap.add_argument("--solve-only", type=int, default=0, help="one solve of this many uniform seeds (for a profiler), then exit")
+    ap.add_argument("--value-only", action="store_true", help="the warm-up and timed batched steps alone, one short line (for a profiler)")
     ap.add_argument("--solve-linear", default="auto", choices=["auto", "cg", "mg"])
     ap.add_argument("--solve-step", default="auto", choices=["auto", "trials", "limits"])
     ap.add_argument("--solve-lin-precision", default="fp64", choices=["fp64", "mixed"])
@@ -562,6 +563,14 @@ def main():
     kst = _lib.kernel_stats()
     _lib.set_timing(False)
     legs["warmup_and_value"] = time.perf_counter() - t_leg
+    if a.value_only:
+        if rank == 0:
+            print(json.dumps({"value_only": True, "value": (a.steps * R * world - len(failed)) / secs, "unit": "solves/s", "steps": a.steps,
+                              "requests_per_step": R, "gpu_launches": int(launches),
+                              "kernel_ms": {k: round(v[0], 3) for k, v in kst.items()}}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
     t_leg = time.perf_counter()
     # only the solves that reached the mass tolerance count
     nfail = len(failed)

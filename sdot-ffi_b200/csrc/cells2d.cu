@@ -499,7 +499,7 @@ __device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )
     __syncthreads();
     if ( am_last ) {
         __threadfence();
-        fold_reports_block( P );
+        fold_reports_block<8>( P );
     }
     __syncthreads();
 }

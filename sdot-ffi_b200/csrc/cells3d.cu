@@ -1197,7 +1197,7 @@ __global__ void __launch_bounds__( 32 * W3, 4 ) k_cells3d( const ProbDev *__rest
             __syncthreads();
             if ( sh_last ) {
                 __threadfence();
-                fold_reports_block( P );
+                fold_reports_block<W3>( P );
             }
             __syncthreads();
         }
@@ -1250,6 +1250,9 @@ void launch_cells3d_giant( const Launch &L, const ProbDev *probs, const OvfList 
     ++*L.launches;
 }
 
+// four blocks of the main kernel on an SM (its static shared memory is under 4 KB; 1 KB a block is the system's)
+static_assert( 4 * ( W3 * sizeof( Cell3 ) + 4096 + 1024 ) <= 228 * 1024, "the main 3D kernel keeps four blocks on an SM" );
+
 void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
                      const Split3 *sp ) {
     if ( nchunks <= 0 ) return;
@@ -1257,6 +1260,7 @@ void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks,
     static bool configured = false;
     if ( ! configured ) {
         cudaFuncSetAttribute( k_cells3d, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
+        cudaFuncSetAttribute( k_cells3d, cudaFuncAttributePreferredSharedMemoryCarveout, 100 );
         configured = true;
     }
     if ( ! sp ) {

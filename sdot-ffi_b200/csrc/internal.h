@@ -275,8 +275,10 @@ struct Rep {
 // the last block of a problem folds its chunks' reports: thread t the chunks t, t + blockDim, ... in order, then the
 // lanes of each warp by a shuffle tree, then the warps in order -- a fixed tree, whatever the scheduling. Every thread
 // of the block calls it (blockDim a multiple of 32); the result goes to P.report and the problem's counter is reset
+// (NW: the warps of the block at most -- the fold's shared memory counts against the cell kernels' occupancy)
+template<int NW>
 __device__ __forceinline__ void fold_reports_block( const ProbDev &P ) {
-    __shared__ double sh_fold[ 32 ][ NB_REPORT ];
+    __shared__ double sh_fold[ NW ][ NB_REPORT ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = int( blockDim.x >> 5 );
     Rep r;
     r.init();
