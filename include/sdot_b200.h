@@ -105,7 +105,7 @@ typedef struct sdot_context_s *sdot_context;
 int32_t sdot_abi_version(void);
 
 /* a context owns a CUDA stream and a stream-ordered device pool on `device`; `pool_limit` bytes (0: no
-   limit besides the device) bound what the context keeps cached.  Replaces the reference's per-call
+   limit besides the device) bound what the pool hands out at once (see sdot_context_memory).  Replaces the reference's per-call
    `queue` + `allocator` pair (docs/guide/ffi-internals.md:1-126, gpu/Cell2D.cuh:1519-1537). */
 int32_t sdot_context_create(int32_t device, uint64_t pool_limit, sdot_context *out, sdot_status *st);
 void sdot_context_destroy(sdot_context ctx);
@@ -113,9 +113,16 @@ void *sdot_context_stream(sdot_context ctx);                 /* the cudaStream_t
 int32_t sdot_context_synchronize(sdot_context ctx, sdot_status *st);
 /* kernels this library launched on the context since its creation (a counter for benchmarks) */
 uint64_t sdot_context_kernel_launches(sdot_context ctx);
+/* the context's device pool: bytes handed out now, the most handed out at once since the last reset, and the limit
+   given at creation (0: none).  A context created with a `pool_limit` refuses, with SDOT_ERR_NO_MEMORY, any allocation
+   past it, and a solve whose model (`sdot_solve_bytes`) does not fit in what is left before anything is built -- the
+   reference's check of the card's memory (CardMemory.check_card_memory, src/sdot/CardMemory.py:158-190).
+   Synchronises the context's stream. */
+int32_t sdot_context_memory(sdot_context ctx, uint64_t *in_use, uint64_t *peak, uint64_t *limit, int32_t reset_peak);
 /* CUDA-event timing of the kernels by class (the reference's LOOM_KERNEL_TIMING, bench/README.md:112-140);
    also switched on for every context by the environment variable SDOT_KERNEL_TIMING=1 */
 enum sdot_kernel_class { SDOT_K_CELLS2D = 0, SDOT_K_CELLS3D, SDOT_K_LAPLACIAN, SDOT_K_CG, SDOT_K_VECTOR, SDOT_K_INDEX, SDOT_K_REPORT,
+                         SDOT_K_MULTIGRID,   /* the multigrid hierarchy's build and the CG's start on it */
                          SDOT_NB_KERNEL_CLASSES };
 int32_t sdot_context_set_timing(sdot_context ctx, int32_t on);
 /* accumulated device time (ms), launches and units (seeds for the cells, rows x iterations for the CG) of a class

@@ -127,6 +127,26 @@ void *sdot_context_stream( sdot_context ctx ) { return ctx ? ( void * ) ctx->c.s
 
 uint64_t sdot_context_kernel_launches( sdot_context ctx ) { return ctx ? ctx->c.launches : 0; }
 
+int32_t sdot_context_memory( sdot_context ctx, uint64_t *in_use, uint64_t *peak, uint64_t *limit, int32_t reset_peak ) {
+    if ( ! ctx ) return SDOT_ERR_ARGS;
+    std::lock_guard<std::mutex> lock( ctx->mu );
+    sdot_status st;
+    return guard( &st, [&] {
+        Ctx &c = ctx->c;
+        CK( cudaSetDevice( c.device ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+        uint64_t high = 0;
+        CK( cudaMemPoolGetAttribute( c.pool, cudaMemPoolAttrUsedMemHigh, &high ) );
+        if ( in_use ) *in_use = pool_in_use( c );
+        if ( peak ) *peak = uint64_t( high );
+        if ( limit ) *limit = c.pool_limit;
+        if ( reset_peak ) {
+            uint64_t zero = 0;
+            CK( cudaMemPoolSetAttribute( c.pool, cudaMemPoolAttrUsedMemHigh, &zero ) );
+        }
+    } );
+}
+
 int32_t sdot_context_set_timing( sdot_context ctx, int32_t on ) {
     if ( ! ctx ) return SDOT_ERR_ARGS;
     ctx->c.timer.on = on != 0;

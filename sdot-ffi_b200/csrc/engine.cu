@@ -28,9 +28,23 @@ void check_cuda( cudaError_t e, const char *what ) {
     throw Error( SDOT_ERR_CUDA, std::string( what ) + ": " + cudaGetErrorString( e ) );
 }
 
+// the bytes the context's pool hands out now
+uint64_t pool_in_use( Ctx &c ) {
+    uint64_t used = 0;
+    CK( cudaMemPoolGetAttribute( c.pool, cudaMemPoolAttrUsedMemCurrent, &used ) );
+    return uint64_t( used );
+}
+
 void *dalloc( Ctx &c, size_t bytes ) {
     void *p = nullptr;
     if ( bytes == 0 ) bytes = 256;
+    if ( c.pool_limit ) {
+        const uint64_t used = pool_in_use( c );
+        if ( used + bytes > c.pool_limit )
+            throw Error( SDOT_ERR_NO_MEMORY, "device pool refused " + std::to_string( bytes ) + " bytes: the context's limit is " +
+                                                 std::to_string( c.pool_limit ) + " and " + std::to_string( used ) + " are in use",
+                         -1, ( long long ) bytes );
+    }
     cudaError_t e = cudaMallocFromPoolAsync( &p, bytes, c.pool, c.stream );
     if ( e == cudaErrorMemoryAllocation ) {
         cudaGetLastError();
@@ -56,6 +70,7 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
     CK( cudaMemPoolCreate( &c.pool, &props ) );
     uint64_t thr = pool_limit ? pool_limit : UINT64_MAX;
     CK( cudaMemPoolSetAttribute( c.pool, cudaMemPoolAttrReleaseThreshold, &thr ) );
+    c.pool_limit = pool_limit;
     c.max_slots = 4096;
     c.dscal = ( double * ) dalloc( c, size_t( c.max_slots ) * SLOT_DOUBLES * 8 );
     CK( cudaMemsetAsync( c.dscal, 0, size_t( c.max_slots ) * SLOT_DOUBLES * 8, c.stream ) );
@@ -604,7 +619,8 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     J.ocost = A.take<double>( n );
 }
 
-constexpr int MG_CCH = 256;          // coarse rows per chunk of the coarsening kernels
+constexpr int MG_CCH = 16;           // coarse rows per chunk of the coarsening kernels (4 a warp: a small level still spreads)
+constexpr int MG_RCH = 64;           // rows per chunk of the cycle's per-level kernels (one pass of a block)
 
 // the level sizes of the hierarchy of a problem of n seeds; 0 levels when it is too small to need one
 static int mg_levels( int dim, long n, int *sizes ) {
@@ -704,6 +720,18 @@ SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
         throw Error( SDOT_ERR_UNSUPPORTED, "option precision: FP64 clipping only (0)" );
     if ( desc.options[ SDOT_OPT_LIN_PRECISION ] != 0 && desc.options[ SDOT_OPT_LIN_PRECISION ] != 1 )
         throw Error( SDOT_ERR_ARGS, "option lin_precision: 0 (FP64 CG) or 1 (FP32 CG with FP64 iterative refinement)" );
+    if ( c.pool_limit ) {
+        // THE MEMORY MODEL before anything is built (CardMemory.check_card_memory, src/sdot/CardMemory.py:158-190): a solve
+        // that cannot fit in what the pool has left is refused at once, with what it needs
+        const uint64_t need = sdot_solve_bytes( D.dim, D.n, &D.density ), used = pool_in_use( c );
+        if ( used + need > c.pool_limit )
+            throw Error( SDOT_ERR_NO_MEMORY, "the solve of " + std::to_string( D.n ) + " seeds needs about " + std::to_string( need ) +
+                                                 " bytes of the device (" + std::to_string( need / std::max<long>( D.n, 1 ) ) +
+                                                 " per seed, sdot_solve_bytes) and the context's pool has " +
+                                                 std::to_string( c.pool_limit > used ? c.pool_limit - used : 0 ) +
+                                                 " left: solve fewer seeds, or give the context a larger pool_limit",
+                         -1, ( long long ) need );
+    }
     SolveJob *J = new SolveJob;
     try {
         J->t_begin = now_s();
@@ -1508,9 +1536,9 @@ struct VecBatch {
                 if ( l >= f || l + 1 >= J->mg_L ) continue;
                 const int nn = J->mg_n[ l + 1 ], n = J->mg_n[ l ];
                 int kk = 0;
-                for ( int b = 0; b < nn; b += VCHUNK, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + VCHUNK ), kk } );
+                for ( int b = 0; b < nn; b += MG_RCH, ++kk ) down[ l ].push_back( Chunk{ q, b, std::min( nn, b + MG_RCH ), kk } );
                 kk = 0;
-                for ( int b = 0; b < n; b += VCHUNK, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + VCHUNK ), kk } );
+                for ( int b = 0; b < n; b += MG_RCH, ++kk ) up[ l ].push_back( Chunk{ q, b, std::min( n, b + MG_RCH ), kk } );
             }
         }
     }
@@ -1733,6 +1761,8 @@ static void launch_pending( Ctx &c, std::vector<SolveJob *> &jobs ) {
             launch_rhs( L, B->dv, B->dch, nch );
             const bool mixed = B == &jacx || B == &mgbx;
             if ( B->mg() ) {
+                c.timer.end( c.stream, 5 );
+                c.timer.begin( c.stream, K_MULTIGRID, rows );
                 B->build( L, c.derr );
                 if ( mixed ) launch_mx_init( L, B->dv, B->dch, nch );
                 else launch_cg_init0( L, B->dv, B->dch, nch );

@@ -24,6 +24,7 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
+    uint64_t pool_limit = 0;          // bytes the pool may hand out at once (0: no limit but the device's)
     unsigned long long launches = 0;
     // engine-wide per-slot scalars: [slot][ 2 * NB_REPORT + NB_SC ] doubles, and two counters per slot
     int max_slots = 0;
@@ -79,6 +80,7 @@ int run_giant_cells( Ctx &c, const ProbDev *dprob, unsigned flags );
 // problems: NULL when there are none, or when the pool cannot give it (the kernel then takes one pass)
 const Split3 *split3_for( Ctx &c, int nchunks, long gcells );
 void *dalloc( Ctx &c, size_t bytes );
+uint64_t pool_in_use( Ctx &c );
 void dfree( Ctx &c, void *p );
 
 // a bump allocator over one device allocation

@@ -329,7 +329,7 @@ SDOT_DEV bool wmaj_claims( const double *a, double b, const double *lo, const do
 
 // ---- launchers (each in the .cu next to its kernels) --------------------------------------------------
 // CUDA-event timing per kernel class (off by default; `sdot_context_set_timing`)
-enum KClass : int { K_CELLS2D = 0, K_CELLS3D, K_LAPLACIAN, K_CG, K_VECTOR, K_INDEX, K_REPORT, NB_KCLASS };
+enum KClass : int { K_CELLS2D = 0, K_CELLS3D, K_LAPLACIAN, K_CG, K_VECTOR, K_INDEX, K_REPORT, K_MULTIGRID, NB_KCLASS };
 struct Timer {
     bool on = false;
     struct Rec { int kind; cudaEvent_t a, b; double units; };

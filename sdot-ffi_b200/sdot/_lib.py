@@ -82,6 +82,8 @@ SIGNATURES = {
     "sdot_context_synchronize": (ctypes.c_int32, [_P, ctypes.POINTER(Status)]),
     "sdot_context_kernel_launches": (ctypes.c_uint64, [_P]),
     "sdot_context_set_timing": (ctypes.c_int32, [_P, ctypes.c_int32]),
+    "sdot_context_memory": (ctypes.c_int32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                             ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]),
     "sdot_context_kernel_stats": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
                                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     "sdot_cells": (ctypes.c_int32, [_P, ctypes.POINTER(DiagramDesc), ctypes.POINTER(CellsOut), ctypes.POINTER(Status)]),
@@ -161,6 +163,36 @@ def context(device=None):
                 raise_for(L.sdot_context_create(dev, 0, ctypes.byref(h), ctypes.byref(st)), st, "sdot_context_create")
                 ctx = _contexts[dev] = h
     return ctx
+
+
+def new_context(device=None, pool_limit=0):
+    """a context of its own (not the process's), its pool limited to `pool_limit` bytes (0: no limit); free it with
+    `destroy_context`"""
+    L = load()
+    h = ctypes.c_void_p()
+    st = Status()
+    dev = device_index() if device is None else int(device)
+    raise_for(L.sdot_context_create(dev, int(pool_limit), ctypes.byref(h), ctypes.byref(st)), st, "sdot_context_create")
+    return h
+
+
+def destroy_context(h):
+    load().sdot_context_destroy(h)
+
+
+def context_memory(ctx=None, reset_peak=False):
+    """the context's pool: bytes in use, the peak since the last reset, and the limit (0: none)"""
+    u, p, l = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    code = load().sdot_context_memory(ctx or context(), ctypes.byref(u), ctypes.byref(p), ctypes.byref(l), int(bool(reset_peak)))
+    raise_for(code, Status(), "sdot_context_memory")
+    return dict(in_use=int(u.value), peak=int(p.value), limit=int(l.value))
+
+
+def solve_bytes(dim, n, dens):
+    """the memory model of one solve (sdot_solve_bytes, the reference's CardMemory.card_solve_bytes)"""
+    keep = []
+    D = density_struct(dens, keep)
+    return int(load().sdot_solve_bytes(int(dim), int(n), ctypes.byref(D)))
 
 
 def ptr(a):
@@ -329,8 +361,9 @@ def solve_out(n, d, cap_history, keep):
     return so, res
 
 
-def solve_batch(problems, options_list, cap_history=512):
-    """`problems`: list of (pos, nu, w0, lo, hi, dens); returns a list of result dicts (or exceptions)"""
+def solve_batch(problems, options_list, cap_history=512, ctx=None):
+    """`problems`: list of (pos, nu, w0, lo, hi, dens); returns a list of result dicts (or exceptions); `ctx`: a context of
+    `new_context` (default: the process's)"""
     L = load()
     keep = []
     count = len(problems)
@@ -344,7 +377,7 @@ def solve_batch(problems, options_list, cap_history=512):
         outs[k] = so
         results.append(res)
     sts = (Status * count)()
-    L.sdot_solve_batch(context(), count, descs, outs, sts)
+    L.sdot_solve_batch(ctx or context(), count, descs, outs, sts)
     final = []
     for k in range(count):
         if sts[k].code != SDOT_OK:
@@ -365,7 +398,7 @@ def kernel_launches():
     return int(load().sdot_context_kernel_launches(context()))
 
 
-KERNEL_CLASSES = ["cells2d", "cells3d", "laplacian", "cg", "vector", "index", "report"]
+KERNEL_CLASSES = ["cells2d", "cells3d", "laplacian", "cg", "vector", "index", "report", "multigrid"]
 
 
 def set_timing(on=True):

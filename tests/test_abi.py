@@ -87,16 +87,32 @@ def test_calls_fail_loudly_without_a_device():
     assert st.message
 
 
-def test_a_c_program_binds_the_library(tmp_path):
-    """tests/c_caller.c, a plain C caller of the header (no Python in its process), compiles with gcc -std=c11
-    -Wall -Werror and links against the library; without a device it reports the context's CUDA error and stops"""
-    import torch
-    if torch.cuda.is_available():
-        pytest.skip("a device is present: the solve itself is the GPU test's")
+def _build_c_caller(tmp_path):
     libdir = os.path.dirname(_lib.LIB_PATH)
     exe = tmp_path / "c_caller"
     subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
                     os.path.join(ROOT, "tests", "c_caller.c"), "-o", str(exe), "-L", libdir, "-lsdot_b200",
                     f"-Wl,-rpath,{libdir}", "-lm"], check=True)
-    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    return exe
+
+
+def test_a_c_program_binds_the_library(tmp_path):
+    """tests/c_caller.c, a plain C caller of the header (no Python in its process), compiles with gcc -std=c11
+    -Wall -Werror and links against the library; without a device it reports the context's CUDA error and stops"""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present: the solve itself is test_a_c_program_solves_on_the_device's")
+    out = subprocess.run([str(_build_c_caller(tmp_path))], check=True, capture_output=True, text=True).stdout.split()
     assert out[0] == "context" and int(out[1]) == _lib.SDOT_ERR_CUDA, out
+
+
+@pytest.mark.gpu
+def test_a_c_program_solves_on_the_device(tmp_path):
+    """the same plain C program on a GPU: its 2D solve of 2000 seeds through sdot_solve (host buffers) converges to the
+    relative mass tolerance 1e-8, with the library's own kernels launched"""
+    out = subprocess.run([str(_build_c_caller(tmp_path))], check=True, capture_output=True, text=True).stdout.split()
+    assert out[0] == "solve", out
+    code, status, worst, launches = int(out[1]), int(out[2]), float(out[3]), int(out[4])
+    assert code == _lib.SDOT_OK and status == 1, out          # status 1: converged
+    assert worst <= 1e-8, worst
+    assert launches > 0, out
