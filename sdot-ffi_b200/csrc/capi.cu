@@ -335,7 +335,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         build_geometry( c, G, dim, n, desc->positions, desc->box_lo, desc->box_hi, desc->density, desc->memory );
         struct Free { Ctx &c; Geometry &G; ~Free() { free_geometry( c, G ); } } fg{ c, G };
         const int cap = dim == 2 ? CAP2 : CAP3;
-        const long nch = ( n + VCHUNK - 1 ) / VCHUNK;
+        const long nch = ( n + vec_chunk( n ) - 1 ) / vec_chunk( n );
         size_t bytes = size_t( n ) * 8 * 3 + size_t( n ) * cap * 12 * 2 + size_t( n + 1 ) * 4 + size_t( n ) * 8 + size_t( nch ) * 32 + NB_SC * 8 +
                        64 + 16 * 256;
         DevVec mem( c, bytes );
@@ -370,7 +370,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         const int cs = cell_chunk( dim, n );
         for ( int b = 0, k = 0; b < n; b += cs, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + cs ) ), k } );
         std::vector<Chunk> vch;
-        for ( int b = 0, k = 0; b < n; b += VCHUNK, ++k ) vch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + VCHUNK ) ), k } );
+        for ( int b = 0, k = 0; b < n; b += vec_chunk( n ), ++k ) vch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + vec_chunk( n ) ) ), k } );
         VecDev V;
         std::memset( &V, 0, sizeof( V ) );
         V.n = int( n ); V.cap = cap; V.nb = nb; V.nid = nid; V.nc = nc; V.row_ptr = rp; V.col = col; V.val = val; V.dia = ddia; V.rowcnt = rowcnt;
@@ -438,7 +438,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
         const long long nnz = hrp[ n ];
         if ( nnz >= ( 1ll << 31 ) ) throw Error( SDOT_ERR_ARGS, "nnz must fit int32" );
         std::vector<int> rp32( hrp.begin(), hrp.end() );
-        const long nch = ( n + VCHUNK - 1 ) / VCHUNK;
+        const long nch = ( n + vec_chunk( n ) - 1 ) / vec_chunk( n );
         size_t bytes = size_t( n + 1 ) * 4 + size_t( nnz + 1 ) * 12 + size_t( n ) * 8 * 9 + size_t( nch ) * 32 + NB_SC * 8 + 64 + 16 * 256;
         if ( mixed ) bytes += size_t( nnz + 1 ) * 4 + size_t( n ) * 4 * 6 + 8 * 256;
         DevVec mem( c, bytes );
@@ -491,7 +491,7 @@ int32_t sdot_linear_solve( sdot_context ctx, int64_t n, const int64_t *row_ptr, 
             CK( cudaMemcpyAsync( ddia, dia, n * 8, kind, c.stream ) );
         }
         std::vector<Chunk> vch;
-        for ( int bb = 0, k = 0; bb < n; bb += VCHUNK, ++k ) vch.push_back( Chunk{ 0, bb, int( std::min<long>( n, bb + VCHUNK ) ), k } );
+        for ( int bb = 0, k = 0; bb < n; bb += vec_chunk( n ), ++k ) vch.push_back( Chunk{ 0, bb, int( std::min<long>( n, bb + vec_chunk( n ) ) ), k } );
         VecDev V;
         std::memset( &V, 0, sizeof( V ) );
         V.n = int( n ); V.row_ptr = rp; V.col = col; V.val = val; V.dia = ddia;

@@ -576,7 +576,7 @@ static size_t mg_bytes( int dim, long n, int cap );
 
 size_t job_bytes( int dim, long n, int dkind, long dcount ) {
     const int cap = dim == 2 ? CAP2 : CAP3;
-    const long cs = cell_chunk( dim, n ), nch = ( n + cs - 1 ) / cs, nv = ( n + VCHUNK - 1 ) / VCHUNK;
+    const long cs = cell_chunk( dim, n ), nch = ( n + cs - 1 ) / cs, nv = ( n + vec_chunk( n ) - 1 ) / vec_chunk( n );
     size_t b = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                size_t( n ) * 4 + size_t( nch ) * NB_REPORT * 8 + size_t( nv ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) + 40 * 256;
     // geometry: ranked positions, user, rank_of, the grid (about n / 2 cells), the density, and the sort's scratch
@@ -591,7 +591,7 @@ static void alloc_job( Ctx &c, SolveJob &J ) {
     const long n = J.G.n;
     const int dim = J.G.dim, cap = J.cap;
     J.nch_cells = int( ( n + cell_chunk( dim, n ) - 1 ) / cell_chunk( dim, n ) );
-    J.nch_vec = int( ( n + VCHUNK - 1 ) / VCHUNK );
+    J.nch_vec = int( ( n + vec_chunk( n ) - 1 ) / vec_chunk( n ) );
     J.ovf_cap = int( n ) + 4096;
     size_t bytes = size_t( n ) * 8 * 18 + 2 * ( size_t( n ) * 4 + size_t( n ) * cap * 12 ) + size_t( n + 1 ) * 4 + size_t( n ) * cap * 12 +
                    size_t( n ) * 4 + size_t( J.nch_cells ) * NB_REPORT * 8 + size_t( J.nch_vec ) * 4 * 8 + 64 + size_t( n ) * 8 * ( dim + 1 ) +
@@ -1498,7 +1498,8 @@ struct VecBatch {
         v.push_back( x );
         jobs.push_back( J );
         int k = 0;
-        for ( int b = 0; b < d.n; b += VCHUNK, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + VCHUNK ), k } );
+        const int vc = vec_chunk( d.n );
+        for ( int b = 0; b < d.n; b += vc, ++k ) ch.push_back( Chunk{ p, b, std::min( d.n, b + vc ), k } );
         if ( ! J || ! J->mg_L || ! d.precond ) return;
         maxL = std::max( maxL, J->mg_L );
         MgJob mj{ J, {} };
@@ -1508,7 +1509,7 @@ struct VecBatch {
             lv[ l ].push_back( mg_level( *J, l, p ) );
             if ( l == 0 ) {
                 int kk = 0;
-                for ( int b = 0; b < J->mg_n[ 0 ]; b += VCHUNK, ++kk ) build0.push_back( Chunk{ q, b, std::min( J->mg_n[ 0 ], b + VCHUNK ), kk } );
+                for ( int b = 0; b < J->mg_n[ 0 ]; b += vc, ++kk ) build0.push_back( Chunk{ q, b, std::min( J->mg_n[ 0 ], b + vc ), kk } );
             }
             if ( l + 1 < J->mg_L ) {
                 const int nn = J->mg_n[ l + 1 ];

@@ -215,6 +215,9 @@ enum Scalar : int { SC_RZ = 0, SC_ALPHA, SC_BETA, SC_BNORM, SC_RNORM, SC_CONV, S
                     SC_NREF,        // mixed CG: refinements so far
                     NB_SC };
 constexpr int VCHUNK = 256;      // rows per chunk of the vector kernels (one block each: many blocks keep loads in flight)
+// rows per chunk of one problem's vector kernels: VCHUNK for a large problem, fewer for a small one so that its CG still
+// spreads over the 148 SMs.  A function of the problem alone: its reductions fold in the same order alone and in any batch
+inline int vec_chunk( long n ) { return n >= 148L * 2 * VCHUNK ? VCHUNK : ( n >= 148L * VCHUNK ? VCHUNK / 2 : VCHUNK / 4 ); }
 constexpr int MG_FUSE_ROWS = 4096;   // multigrid levels of at most this many rows run in one launch per problem (k_mg_fused)
 
 // ---- warp helpers ------------------------------------------------------------------------------------
