@@ -373,13 +373,6 @@ __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py,
         const int l = e.x >> 16, X = e.x & 0xffff, Y = e.y;
         const int x0 = X << l, y0 = Y << l;
         const int x1 = min( ( X + 1 ) << l, g0 ) - 1, y1 = min( ( Y + 1 ) << l, g1 ) - 1;
-        if ( x0 >= cx - rd && x1 <= cx + rd && y0 >= cy - rd && y1 <= cy + rd ) continue;
-        const size_t rec = P.poff[ l ] + ( size_t ) Y * lev_dim( g0, l ) + X;
-        const double b = wmaj_b( P, rec );
-        if ( b < -1e299 ) continue;
-        const double lo[ 2 ] = { P.go[ 0 ] + x0 * P.gh[ 0 ], P.go[ 1 ] + y0 * P.gh[ 1 ] };
-        const double hi[ 2 ] = { P.go[ 0 ] + ( x1 + 1 ) * P.gh[ 0 ], P.go[ 1 ] + ( y1 + 1 ) * P.gh[ 1 ] };
-        if ( ! claims( lo, hi, P.wpyr + rec * 3, b ) ) continue;
         if ( l <= WALK_LEAF ) {
             const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;           // at most 4 x 4
             int beg = 0, cnt = 0;
@@ -397,24 +390,43 @@ __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py,
             R2 = radius2();
             continue;
         }
-        // the children, farthest pushed first so that the nearest is walked first
-        const int dx1 = lev_dim( g0, l - 1 ), dy1 = lev_dim( g1, l - 1 );
-        double cd[ 4 ];
-        int cc[ 4 ], nc = 0;
-        for ( int k = 0; k < 4; ++k ) {
-            const int X2 = 2 * X + ( k & 1 ), Y2 = 2 * Y + ( k >> 1 );
-            if ( X2 >= dx1 || Y2 >= dy1 ) continue;
-            const int a0 = X2 << ( l - 1 ), b0 = Y2 << ( l - 1 );
-            const int a1 = min( ( X2 + 1 ) << ( l - 1 ), g0 ) - 1, b1 = min( ( Y2 + 1 ) << ( l - 1 ), g1 ) - 1;
-            double d = cells_dist2( P, a0, a1, b0, b1, px, py );
-            int q = nc++;
-            while ( q > 0 && cd[ q - 1 ] < d ) { cd[ q ] = cd[ q - 1 ]; cc[ q ] = cc[ q - 1 ]; --q; }
-            cd[ q ] = d;
-            cc[ q ] = ( X2 << 16 ) | Y2;
+        // the (up to 4) children, lane k the child k, tested when their parent is expanded (their majorant records loaded
+        // together): in the grid, not all inside the walked rings, not empty, claiming a vertex of the cell
+        const int X2 = 2 * X + ( lane & 1 ), Y2 = 2 * Y + ( ( lane >> 1 ) & 1 );
+        const int a0 = X2 << ( l - 1 ), b0 = Y2 << ( l - 1 );
+        const int a1 = min( ( X2 + 1 ) << ( l - 1 ), g0 ) - 1, b1 = min( ( Y2 + 1 ) << ( l - 1 ), g1 ) - 1;
+        bool ok = lane < 4 && X2 < lev_dim( g0, l - 1 ) && Y2 < lev_dim( g1, l - 1 ) &&
+                  ! ( a0 >= cx - rd && a1 <= cx + rd && b0 >= cy - rd && b1 <= cy + rd );
+        double cb = -1e300, ca0 = 0, ca1 = 0, dd = 0;
+        if ( ok ) {
+            const size_t rec = P.poff[ l - 1 ] + ( size_t ) Y2 * lev_dim( g0, l - 1 ) + X2;
+            cb = wmaj_b( P, rec );
+            ca0 = P.wpyr[ rec * 3 ];
+            ca1 = P.wpyr[ rec * 3 + 1 ];
+            dd = cells_dist2( P, a0, a1, b0, b1, px, py );
+            ok = cb >= -1e299;
         }
+        unsigned todo = __ballot_sync( FULL, ok ), claim = 0;
+        while ( todo ) {
+            const int c = __ffs( todo ) - 1;
+            todo &= todo - 1;
+            const double A[ 2 ] = { __shfl_sync( FULL, ca0, c ), __shfl_sync( FULL, ca1, c ) }, B = __shfl_sync( FULL, cb, c );
+            const int ca = __shfl_sync( FULL, a0, c ), ca1i = __shfl_sync( FULL, a1, c ), cb0 = __shfl_sync( FULL, b0, c ),
+                      cb1 = __shfl_sync( FULL, b1, c );
+            const double lo[ 2 ] = { P.go[ 0 ] + ca * P.gh[ 0 ], P.go[ 1 ] + cb0 * P.gh[ 1 ] };
+            const double hi[ 2 ] = { P.go[ 0 ] + ( ca1i + 1 ) * P.gh[ 0 ], P.go[ 1 ] + ( cb1 + 1 ) * P.gh[ 1 ] };
+            if ( claims( lo, hi, A, B ) ) claim |= 1u << c;
+        }
+        // the claiming children pushed farthest first (equal distances in child order), so that the nearest is walked first
+        int rank = 0;
+#pragma unroll
+        for ( int c = 0; c < 4; ++c ) {
+            const double dc = __shfl_sync( FULL, dd, c );
+            if ( ( ( claim >> c ) & 1 ) && ( dc > dd || ( dc == dd && c < lane ) ) ) ++rank;
+        }
+        const int nc = __popc( claim );
         if ( sp + nc > WALK_STACK ) return;                // cannot happen below 2^21 cells per side
-        if ( lane == 0 )
-            for ( int k = 0; k < nc; ++k ) stk[ sp + k ] = make_int2( ( ( l - 1 ) << 16 ) | ( cc[ k ] >> 16 ), cc[ k ] & 0xffff );
+        if ( ( claim >> lane ) & 1 ) stk[ sp + rank ] = make_int2( ( ( l - 1 ) << 16 ) | X2, Y2 );
         sp += nc;
         __syncwarp();
     }

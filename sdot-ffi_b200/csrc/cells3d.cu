@@ -395,7 +395,9 @@ constexpr int WALK_LEAF3 = 1;        // the walk's leaves: blocks of 2 x 2 x 2 g
 
 // the pyramid of weight majorants, depth first, nearest child first, skipping the cells within Chebyshev distance rd of
 // c0 (the shells already walked) and the blocks that claim no vertex of the cell (wmaj_claims); a leaf block has
-// one cell per lane, each tested by `may_cut3`, clipped together
+// one cell per lane, each tested by `may_cut3`, clipped together.  A node's children are tested when it is expanded, one
+// child per lane for their majorant records (eight loads in flight instead of one per pop), then each against the cell's
+// vertices; only the claiming children are pushed
 template<class C3>
 __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, const int *c0, int rd,
                                int2 *stk, bool &overflow ) {
@@ -410,27 +412,9 @@ __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double 
         __syncwarp();
         const int l = e.x >> 22, X[ 3 ] = { ( e.x >> 11 ) & 0x7ff, e.x & 0x7ff, e.y };
         int a0[ 3 ], a1[ 3 ];
-        bool inside = true;
         for ( int a = 0; a < 3; ++a ) {
             a0[ a ] = X[ a ] << l;
             a1[ a ] = min( ( X[ a ] + 1 ) << l, g[ a ] ) - 1;
-            inside = inside && a0[ a ] >= c0[ a ] - rd && a1[ a ] <= c0[ a ] + rd;
-        }
-        if ( inside ) continue;
-        const size_t rec = P.poff[ l ] + ( ( size_t ) X[ 2 ] * lev_dim( g[ 1 ], l ) + X[ 1 ] ) * lev_dim( g[ 0 ], l ) + X[ 0 ];
-        const double b = wmaj_b( P, rec );
-        if ( b < -1e299 ) continue;
-        {
-            // does the block claim a vertex of the cell?
-            double lo[ 3 ], hi[ 3 ];
-            for ( int q = 0; q < 3; ++q ) { lo[ q ] = P.go[ q ] + a0[ q ] * P.gh[ q ]; hi[ q ] = P.go[ q ] + ( a1[ q ] + 1 ) * P.gh[ q ]; }
-            const double *am = P.wpyr + rec * 4;
-            bool may = false;
-            for ( int k = lane; k < C.nv && ! may; k += 32 ) {
-                const double v[ 3 ] = { C.vx[ k ], C.vy[ k ], C.vz[ k ] }, Xp[ 3 ] = { px + v[ 0 ], py + v[ 1 ], pz + v[ 2 ] };
-                may = wmaj_claims( am, b, lo, hi, Xp, v, 3, wi );
-            }
-            if ( ! __any_sync( FULL3, may ) ) continue;
         }
         if ( l <= WALK_LEAF3 ) {
             const int bw[ 3 ] = { a1[ 0 ] - a0[ 0 ] + 1, a1[ 1 ] - a0[ 1 ] + 1, a1[ 2 ] - a0[ 2 ] + 1 };   // at most 2 x 2 x 2
@@ -451,31 +435,53 @@ __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double 
             R2 = radius2_3( C, lane );
             continue;
         }
-        // the (up to 8) children, sorted farthest first so that the nearest is popped first
-        int d1[ 3 ];
-        for ( int a = 0; a < 3; ++a ) d1[ a ] = lev_dim( g[ a ], l - 1 );
-        double cd[ 8 ];
-        int2 ce[ 8 ];
-        int nc = 0;
-        for ( int k = 0; k < 8; ++k ) {
-            int Y[ 3 ], b0[ 3 ], b1[ 3 ];
-            bool ok = true;
-            for ( int a = 0; a < 3; ++a ) {
-                Y[ a ] = 2 * X[ a ] + ( ( k >> a ) & 1 );
-                ok = ok && Y[ a ] < d1[ a ];
-                b0[ a ] = Y[ a ] << ( l - 1 );
-                b1[ a ] = min( ( Y[ a ] + 1 ) << ( l - 1 ), g[ a ] ) - 1;
-            }
-            if ( ! ok ) continue;
-            double d = cells_dist2_3( P, b0, b1, px, py, pz );
-            int q = nc++;
-            while ( q > 0 && cd[ q - 1 ] < d ) { cd[ q ] = cd[ q - 1 ]; ce[ q ] = ce[ q - 1 ]; --q; }
-            cd[ q ] = d;
-            ce[ q ] = make_int2( ( ( l - 1 ) << 22 ) | ( Y[ 0 ] << 11 ) | Y[ 1 ], Y[ 2 ] );
+        // the (up to 8) children, lane k the child k: in the grid, not all inside the walked shells, not empty
+        int Y[ 3 ], b0[ 3 ], b1[ 3 ];
+        bool ok = lane < 8, inside = true;
+        for ( int a = 0; a < 3; ++a ) {
+            Y[ a ] = 2 * X[ a ] + ( ( lane >> a ) & 1 );
+            ok = ok && Y[ a ] < lev_dim( g[ a ], l - 1 );
+            b0[ a ] = Y[ a ] << ( l - 1 );
+            b1[ a ] = min( ( Y[ a ] + 1 ) << ( l - 1 ), g[ a ] ) - 1;
+            inside = inside && b0[ a ] >= c0[ a ] - rd && b1[ a ] <= c0[ a ] + rd;
         }
+        ok = ok && ! inside;
+        double cb = -1e300, ca[ 3 ] = { 0, 0, 0 }, lo[ 3 ] = { 0, 0, 0 }, hi[ 3 ] = { 0, 0, 0 }, dd = 0;
+        if ( ok ) {
+            const size_t rec = P.poff[ l - 1 ] + ( ( size_t ) Y[ 2 ] * lev_dim( g[ 1 ], l - 1 ) + Y[ 1 ] ) * lev_dim( g[ 0 ], l - 1 ) + Y[ 0 ];
+            cb = wmaj_b( P, rec );
+            const double *am = P.wpyr + rec * 4;
+            ca[ 0 ] = am[ 0 ]; ca[ 1 ] = am[ 1 ]; ca[ 2 ] = am[ 2 ];
+            for ( int q = 0; q < 3; ++q ) { lo[ q ] = P.go[ q ] + b0[ q ] * P.gh[ q ]; hi[ q ] = P.go[ q ] + ( b1[ q ] + 1 ) * P.gh[ q ]; }
+            dd = cells_dist2_3( P, b0, b1, px, py, pz );
+            ok = cb >= -1e299;
+        }
+        // does each child claim a vertex of the cell?  (lanes over the vertices, the child's record broadcast)
+        unsigned todo = __ballot_sync( FULL3, ok ), claim = 0;
+        while ( todo ) {
+            const int c = __ffs( todo ) - 1;
+            todo &= todo - 1;
+            const double A[ 3 ] = { __shfl_sync( FULL3, ca[ 0 ], c ), __shfl_sync( FULL3, ca[ 1 ], c ), __shfl_sync( FULL3, ca[ 2 ], c ) };
+            const double B = __shfl_sync( FULL3, cb, c );
+            const double LO[ 3 ] = { __shfl_sync( FULL3, lo[ 0 ], c ), __shfl_sync( FULL3, lo[ 1 ], c ), __shfl_sync( FULL3, lo[ 2 ], c ) };
+            const double HI[ 3 ] = { __shfl_sync( FULL3, hi[ 0 ], c ), __shfl_sync( FULL3, hi[ 1 ], c ), __shfl_sync( FULL3, hi[ 2 ], c ) };
+            bool may = false;
+            for ( int k = lane; k < C.nv && ! may; k += 32 ) {
+                const double v[ 3 ] = { C.vx[ k ], C.vy[ k ], C.vz[ k ] }, Xp[ 3 ] = { px + v[ 0 ], py + v[ 1 ], pz + v[ 2 ] };
+                may = wmaj_claims( A, B, LO, HI, Xp, v, 3, wi );
+            }
+            if ( __any_sync( FULL3, may ) ) claim |= 1u << c;
+        }
+        // the claiming children pushed farthest first (equal distances in child order), so that the nearest is popped first
+        int rank = 0;
+#pragma unroll
+        for ( int c = 0; c < 8; ++c ) {
+            const double dc = __shfl_sync( FULL3, dd, c );
+            if ( ( ( claim >> c ) & 1 ) && ( dc > dd || ( dc == dd && c < lane ) ) ) ++rank;
+        }
+        const int nc = __popc( claim );
         if ( sp + nc > WALK_STACK3 ) return;               // cannot happen below 2^13 cells per side
-        if ( lane == 0 )
-            for ( int k = 0; k < nc; ++k ) stk[ sp + k ] = ce[ k ];
+        if ( ( claim >> lane ) & 1 ) stk[ sp + rank ] = make_int2( ( ( l - 1 ) << 22 ) | ( Y[ 0 ] << 11 ) | Y[ 1 ], Y[ 2 ] );
         sp += nc;
         __syncwarp();
     }
