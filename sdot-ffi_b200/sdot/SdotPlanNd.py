@@ -28,8 +28,9 @@ _INT_STATS = ("nb_iter", "nb_diag", "nb_backtracks", "nb_overflowed", "nb_cell_l
 #: the tolerance; and the weight gap of an exact duplicate, relative to the cloud's squared extent (SdotPlanNd.py:121)
 _AGGREGATE_MARGIN = 4.0
 
-#: `Tuning.step`: the trials of KMT's damping, or the limits of the cells below the floor (2D; 3D takes the trials)
-_STEP = {"auto": 0, "trials": 0, "limits": 1}
+#: `Tuning.step`: the trials of KMT's damping, or the limits of the cells below the floor; "auto" is the limits in 2D and
+#: the trials in 3D, as the reference (SdotPlanNd.py:461-462: the engine takes the trials in 3D whatever the option says)
+_STEP = {"auto": 1, "trials": 0, "limits": 1}
 _DUPLICATE_GAP = 1e-6
 
 
@@ -70,7 +71,7 @@ def solver_options(settings, n, d=None):
                 lin_method=0 if tun.linear_solver == "cg" else 1, precision=0,
                 lin_precision=1 if getattr(tun, "linear_precision", "fp64") == "mixed" else 0,
                 agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0),
-                step=_STEP[tun.step])
+                step=0 if tun.step == "auto" and d is not None and d != 2 else _STEP[tun.step])
 
 
 def _box_of(problem):

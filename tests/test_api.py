@@ -49,6 +49,7 @@ def test_settings_map_onto_the_option_vector():
     assert solver_options(Iterative(tuning=Tuning(step="limits")), 10)["step"] == 1
     assert solver_options(Iterative(tuning=Tuning(step="trials")), 10)["step"] == 0
     assert solver_options(Iterative(tuning=Tuning(step="limits")), 10, 2)["step"] == 1
+    assert solver_options(Iterative(), 10, 2)["step"] == 1          # "auto": the limits in 2D (SdotPlanNd.py:462)
     with pytest.raises(ValueError):                    # SdotPlanNd.py:461-465: the limits step is 2D only
         solver_options(Iterative(tuning=Tuning(step="limits")), 10, 3)
     assert solver_options(Iterative(), 10, 3)["step"] == 0
