@@ -96,7 +96,9 @@ typedef struct sdot_cells_out {
     int32_t *nb_ids;              /* [n, cap]   neighbour user index                                         */
     double *nb_coef;              /* [n, cap]   c_ij = int_facet rho / (2 |p_i - p_j|)  (sdotplan/Laplacian.h:7) */
     double *nb_measure;           /* [n, cap]   int_facet rho (the face length / area for rho = 1)            */
-    int32_t precision;            /* 0: FP64 clipping (1, FP32 clipping + FP64 re-check: SDOT_ERR_UNSUPPORTED) */
+    int32_t precision;            /* 0: FP64 clipping; 1 (2D): FP32 clipping with FP64 re-checks of the vertices */
+                                  /* within the FP32 band, every vertex re-solved in FP64 before the integration */
+                                  /* (the reference's float kernel, gpu/Cell2D.cuh:56-60, 991-1042); 3D: refused */
 } sdot_cells_out;
 
 typedef struct sdot_context_s *sdot_context;
@@ -202,7 +204,7 @@ enum sdot_option {
     SDOT_OPT_CONV_RATIO,
     SDOT_OPT_CONV_MIN,
     SDOT_OPT_LIN_METHOD,          /* 0 Jacobi-PCG, 1 multigrid-PCG                                            */
-    SDOT_OPT_PRECISION,           /* 0 FP64 clipping (1, FP32 clipping + FP64 re-check: SDOT_ERR_UNSUPPORTED) */
+    SDOT_OPT_PRECISION,           /* 0 FP64 clipping; 1 FP32 clipping + FP64 re-checks (2D; 3D: UNSUPPORTED) */
     SDOT_OPT_LIN_PRECISION,       /* 0 FP64 CG; 1 FP32 inner CG with FP64 iterative refinement                */
     SDOT_OPT_AGG_MARGIN,          /* aggregation of near-coincident seeds: merge a pair when c_ij ulp(w) margin  */
                                   /* > the tolerance (sdotplan/Aggregation.h); 0: off; the reference uses 4      */

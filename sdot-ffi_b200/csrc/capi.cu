@@ -183,8 +183,9 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         CK( cudaSetDevice( c.device ) );
         const int dim = desc->dim;
         const long n = desc->n;
-        if ( out->precision != 0 )
-            throw Error( SDOT_ERR_UNSUPPORTED, "precision 1 (FP32 clipping with an FP64 re-check) is not built: FP64 clipping only (precision 0)" );
+        if ( out->precision != 0 && out->precision != 1 ) throw Error( SDOT_ERR_ARGS, "precision: 0 (FP64 clipping) or 1 (FP32 clipping)" );
+        if ( out->precision == 1 && dim != 2 )
+            throw Error( SDOT_ERR_UNSUPPORTED, "precision 1 (FP32 clipping with FP64 re-checks) is built in 2D; 3D clips in FP64 (precision 0)" );
         const bool facets = out->nb_count || out->nb_ids || out->nb_coef || out->nb_measure;
         if ( facets && ( ! out->nb_count || ! out->nb_ids || ! out->nb_coef || out->cap <= 0 ) )
             throw Error( SDOT_ERR_ARGS, "facets need nb_count, nb_ids, nb_coef and cap > 0" );
@@ -222,6 +223,7 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         }
         ProbDev P;
         G.fill( P );
+        P.fp32 = out->precision == 1;
         P.cap = cap;
         P.w = wr;
         P.wmax_slot = slot;
@@ -241,7 +243,8 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         const Split3 *sp = dim == 3 && P.dkind == D_GAUSS ? split3_for( c, int( ch.size() ), n ) : nullptr;
         c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, double( n ) );
         launch_wpyr( L, dd.as<ProbDev>(), 1 );
-        if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf );
+        if ( dim == 2 ) launch_cells2d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf,
+                                        P.fp32 ? 2 : 1 );
         else launch_cells3d( L, dd.as<ProbDev>(), ( Chunk * ) ( ( char * ) dd.p + o2 ), int( ch.size() ), flags, c.derr, c.dovf, sp );
         c.timer.end( c.stream, sp ? 2 : 1 );
         run_big_cells( c, dd.as<ProbDev>(), flags );
@@ -294,6 +297,7 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         launch_wmax( L, wr, int( n ), slot );
         ProbDev P;
         G.fill( P );
+        P.fp32 = 0;
         P.w = wr;
         P.wmax_slot = slot;
         P.gm = gm.d;
@@ -361,6 +365,7 @@ int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t
         launch_wmax( L, wr, int( n ), slot );
         ProbDev P;
         G.fill( P );
+        P.fp32 = 0;
         P.cap = cap;
         P.w = wr;
         P.wmax_slot = slot;

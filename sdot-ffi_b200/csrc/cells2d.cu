@@ -258,6 +258,7 @@ struct WPoly {
     double vx, vy;             // vertex `lane`
     double lnx, lny, loff;     // line of edge lane -> lane + 1
     int lid;
+    static constexpr double R2_MARGIN = 1, CLAIM_REL = 1e-12;    // (the security tests on the vertices: exact)
 };
 
 // keep n . y <= off; false past 32 vertices
@@ -477,6 +478,226 @@ __device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int l
     }
 }
 
+// ---- THE FP32 CLIP (precision "mixed": the reference's float kernel and its FP64 re-solve, gpu/Cell2D.cuh:56-60, 991-1042) ------
+// The polygon is held in FP32 (vertices and lines in registers: half the shuffles of a cut) and every decision is the FP64
+// kernel's: a vertex is tested in FP32 against a band that bounds the FP32 error of the test, and only a vertex inside the
+// band is re-checked in FP64, re-solved from its two lines as the FP64 kernel holds it; a new vertex is computed in FP32
+// where its two lines cross at more than 1/20 rad, else in FP64 (then rounded).  At the end every vertex is re-solved in
+// FP64 from its two lines (the seeds' positions and weights read again) and the cell is integrated as the FP64 one.
+struct WPolyF {
+    int m;
+    float vx, vy;              // vertex `lane`
+    float lnx, lny, loff;      // line of edge lane -> lane + 1
+    int lid;
+    bool ip;                   // interpolated on its edge (two lines nearly parallel, as the FP64 kernel does): kept as is
+    // the security tests on FP32 vertices: the radius inflated, the majorants' claims with a margin of 1e-5
+    static constexpr double R2_MARGIN = 1 + 1e-5, CLAIM_REL = 1e-5;
+};
+
+// the FP32 band of a test n . v - off at vertices of |v|_1 <= Rs: 64 float eps of the terms (the test's own rounding and
+// that of a vertex crossed in FP32 at more than 1/20 rad)
+constexpr float F32_BAND = 3.814697265625e-6f;        // 2^-18
+
+// the FP64 line of edge `id` of the cell of seed (px, py, wi): a seed's bisector (as cut_by_ranges makes it) or a box side
+// (as the kernel's start makes it)
+__device__ __forceinline__ void line64( const ProbDev &P, int id, double px, double py, double wi, double &a, double &b, double &c ) {
+    if ( id >= 0 ) {
+        a = P.pos[ 2 * ( size_t ) id ] - px;
+        b = P.pos[ 2 * ( size_t ) id + 1 ] - py;
+        const double qw = P.w ? P.w[ id ] : 0.0;
+        c = 0.5 * ( ( wi - qw ) + ( a * a + b * b ) );
+    } else {
+        const int side = -1 - id;
+        a = side == 1 ? 1.0 : ( side == 3 ? -1.0 : 0.0 );
+        b = side == 0 ? -1.0 : ( side == 2 ? 1.0 : 0.0 );
+        c = side == 0 ? -( P.lo[ 1 ] - py ) : ( side == 1 ? P.hi[ 0 ] - px : ( side == 2 ? P.hi[ 1 ] - py : -( P.lo[ 0 ] - px ) ) );
+    }
+}
+
+// the FP32 crossing of two lines, along line 1 (as `isect`); good: they cross at more than 1/20 rad
+__device__ __forceinline__ void isectf( float a1, float b1, float c1, float a2, float b2, float c2, float &x, float &y, bool &good ) {
+    const float det = a1 * b2 - a2 * b1;
+    good = det * det > 0.0025f * ( a1 * a1 + b1 * b1 ) * ( a2 * a2 + b2 * b2 );
+    const float k = c1 / ( a1 * a1 + b1 * b1 ), fx = k * a1, fy = k * b1;
+    const float t = ( c2 - ( a2 * fx + b2 * fy ) ) / det;
+    x = fx - t * b1;
+    y = fy + t * a1;
+}
+
+// the crossing of the lines id1 then id2 in FP64 (as the FP64 kernel computes it), rounded; ok false: nearly parallel
+__device__ __forceinline__ void isect64_ids( const ProbDev &P, int id1, int id2, double px, double py, double wi, float &x, float &y, bool &ok ) {
+    double a1, b1, c1, a2, b2, c2, X, Y;
+    line64( P, id1, px, py, wi, a1, b1, c1 );
+    line64( P, id2, px, py, wi, a2, b2, c2 );
+    isect( a1, b1, c1, a2, b2, c2, X, Y, ok );
+    x = float( X );
+    y = float( Y );
+}
+
+// keep n . y <= off (n, off: the candidate's FP64 bisector); Rs bounds |v|_1 over the polygon; false past 32 vertices
+__device__ __forceinline__ bool wclip( WPolyF &C, int lane, double nx64, double ny64, double off64, int id, float Rs, const ProbDev &P, double px,
+                                       double py, double wi ) {
+    const int m = C.m;
+    const float nx = float( nx64 ), ny = float( ny64 ), off = float( off64 );
+    const float band = F32_BAND * ( ( fabsf( nx ) + fabsf( ny ) ) * Rs + fabsf( off ) );
+    const float sf = nx * C.vx + ny * C.vy - off;
+    double s = sf;
+    const int plid = __shfl_sync( FULL, C.lid, lane == 0 ? ( m > 0 ? m - 1 : 0 ) : lane - 1 );
+    const bool unc = lane < m && fabsf( sf ) <= band;
+    if ( __any_sync( FULL, unc ) && unc ) {
+        // the FP64 re-check: the vertex as the FP64 kernel holds it, the crossing of its two lines
+        float x = C.vx, y = C.vy;
+        bool ok = false;
+        double X = C.vx, Y = C.vy;
+        if ( ! C.ip ) {
+            double a1, b1, c1, a2, b2, c2;
+            line64( P, plid, px, py, wi, a1, b1, c1 );
+            line64( P, C.lid, px, py, wi, a2, b2, c2 );
+            isect( a1, b1, c1, a2, b2, c2, X, Y, ok );
+            if ( ! ok ) { X = x; Y = y; }
+        }
+        s = nx64 * X + ny64 * Y - off64;
+    }
+    unsigned out = __ballot_sync( FULL, lane < m && s > 0 );
+    if ( ! out ) return true;
+    unsigned valid = m >= 32 ? FULL : ( ( 1u << m ) - 1 );
+    if ( out == valid ) { C.m = 0; return true; }
+    unsigned in = valid & ~out;
+    unsigned rot_out = ( ( out >> 1 ) | ( out << ( m - 1 ) ) ) & valid;
+    unsigned rot_in = ( ( in >> 1 ) | ( in << ( m - 1 ) ) ) & valid;
+    unsigned A = in & rot_out, B = out & rot_in;
+    int a, b;
+    if ( __popc( A ) == 1 ) {
+        a = __ffs( A ) - 1;
+        b = __ffs( B ) - 1;
+    } else {
+        double sv = lane < m ? s : -1e300;
+        double smax = warp_max( sv );
+        int kstar = __ffs( __ballot_sync( FULL, lane < m && sv == smax ) ) - 1;
+        int da = ( A >> lane ) & 1 ? ( ( kstar - lane ) % m + m ) % m : 1 << 20;
+        int db = ( B >> lane ) & 1 ? ( ( lane - kstar ) % m + m ) % m : 1 << 20;
+        for ( int o = 16; o > 0; o >>= 1 ) { da = min( da, __shfl_xor_sync( FULL, da, o ) ); db = min( db, __shfl_xor_sync( FULL, db, o ) ); }
+        a = ( ( kstar - da ) % m + m ) % m;
+        b = ( kstar + db ) % m;
+    }
+    int K = ( ( a - b - 1 ) % m + m ) % m + 1;
+    if ( K + 2 > 32 ) return false;
+    int a1 = a + 1 == m ? 0 : a + 1, b1 = b + 1 == m ? 0 : b + 1;
+    const float anx = __shfl_sync( FULL, C.lnx, a ), any = __shfl_sync( FULL, C.lny, a ), aoff = __shfl_sync( FULL, C.loff, a );
+    const float bnx = __shfl_sync( FULL, C.lnx, b ), bny = __shfl_sync( FULL, C.lny, b ), boff = __shfl_sync( FULL, C.loff, b );
+    const int aid = __shfl_sync( FULL, C.lid, a ), bid = __shfl_sync( FULL, C.lid, b );
+    float Px, Py, Qx, Qy;
+    bool gP, gQ, ipP = false, ipQ = false;
+    isectf( anx, any, aoff, nx, ny, off, Px, Py, gP );
+    isectf( nx, ny, off, bnx, bny, boff, Qx, Qy, gQ );
+    // (gP, gQ warp uniform) a crossing at less than 1/20 rad: in FP64, from the two FP64 lines; nearly parallel there too:
+    // on the edge, as the FP64 kernel
+    if ( ! gP ) {
+        double a1x, a1y, a1c, X, Y;
+        bool ok;
+        line64( P, aid, px, py, wi, a1x, a1y, a1c );
+        isect( a1x, a1y, a1c, nx64, ny64, off64, X, Y, ok );
+        Px = float( X ); Py = float( Y );
+        if ( ! ok ) {
+            const float xa = __shfl_sync( FULL, C.vx, a ), ya = __shfl_sync( FULL, C.vy, a );
+            const double sa = __shfl_sync( FULL, s, a );
+            const float xa1 = __shfl_sync( FULL, C.vx, a1 ), ya1 = __shfl_sync( FULL, C.vy, a1 );
+            const double sa1 = __shfl_sync( FULL, s, a1 );
+            const double t = sa / ( sa - sa1 );
+            Px = float( xa + t * ( xa1 - xa ) ); Py = float( ya + t * ( ya1 - ya ) );
+            ipP = true;
+        }
+    }
+    if ( ! gQ ) {
+        double b1x, b1y, b1c, X, Y;
+        bool ok;
+        line64( P, bid, px, py, wi, b1x, b1y, b1c );
+        isect( nx64, ny64, off64, b1x, b1y, b1c, X, Y, ok );
+        Qx = float( X ); Qy = float( Y );
+        if ( ! ok ) {
+            const float xb = __shfl_sync( FULL, C.vx, b ), yb = __shfl_sync( FULL, C.vy, b );
+            const double sb = __shfl_sync( FULL, s, b );
+            const float xb1 = __shfl_sync( FULL, C.vx, b1 ), yb1 = __shfl_sync( FULL, C.vy, b1 );
+            const double sb1 = __shfl_sync( FULL, s, b1 );
+            const double t = sb / ( sb - sb1 );
+            Qx = float( xb + t * ( xb1 - xb ) ); Qy = float( yb + t * ( yb1 - yb ) );
+            ipQ = true;
+        }
+    }
+    int src = ( b + 1 + lane ) % m;
+    float nvx = __shfl_sync( FULL, C.vx, src ), nvy = __shfl_sync( FULL, C.vy, src );
+    float nlx = __shfl_sync( FULL, C.lnx, src ), nly = __shfl_sync( FULL, C.lny, src ), nlo = __shfl_sync( FULL, C.loff, src );
+    int nli = __shfl_sync( FULL, C.lid, src );
+    bool nip = __shfl_sync( FULL, int( C.ip ), src ) != 0;
+    if ( lane == K ) { nvx = Px; nvy = Py; nlx = nx; nly = ny; nlo = off; nli = id; nip = ipP; }
+    if ( lane == K + 1 ) { nvx = Qx; nvy = Qy; nlx = bnx; nly = bny; nlo = boff; nli = bid; nip = ipQ; }
+    C.vx = nvx; C.vy = nvy; C.lnx = nlx; C.lny = nly; C.loff = nlo; C.lid = nli; C.ip = nip;
+    C.m = K + 2;
+    return true;
+}
+
+__device__ __forceinline__ void cut_by_ranges( WPolyF &C, const ProbDev &P, int lane, int s, double px, double py, double wi, int beg, int cnt,
+                                               bool &overflow ) {
+    int inc = cnt;
+#pragma unroll
+    for ( int o = 1; o < 32; o <<= 1 ) { int t = __shfl_up_sync( FULL, inc, o ); if ( lane >= o ) inc += t; }
+    const int total = __shfl_sync( FULL, inc, 31 );
+    const int exc = inc - cnt;
+    for ( int t0 = 0; t0 < total && C.m > 0 && ! overflow; t0 += 32 ) {
+        const int t = t0 + lane;
+        int owner = 0;
+#pragma unroll
+        for ( int st = 16; st > 0; st >>= 1 ) { int v = __shfl_sync( FULL, inc, owner + st - 1 ); if ( v <= t ) owner += st; }
+        owner = owner > 31 ? 31 : owner;
+        int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
+        int j = obeg + ( t - oexc );
+        bool valid = t < total && j != s;
+        double qx = 0, qy = 0, off = 0;
+        if ( valid ) {
+            qx = P.pos[ 2 * ( size_t ) j ] - px;
+            qy = P.pos[ 2 * ( size_t ) j + 1 ] - py;
+            double qw = P.w ? P.w[ j ] : 0.0;
+            off = 0.5 * ( ( wi - qw ) + ( qx * qx + qy * qy ) );
+        }
+        // the parallel pre-test in FP32: a candidate within the band of a vertex goes on to the clip, which decides in FP64
+        float Rs = lane < C.m ? fabsf( C.vx ) + fabsf( C.vy ) : 0.f;
+#pragma unroll
+        for ( int o = 16; o > 0; o >>= 1 ) Rs = fmaxf( Rs, __shfl_xor_sync( FULL, Rs, o ) );
+        const float fx = float( qx ), fy = float( qy ), fo = float( off );
+        const float band = F32_BAND * ( ( fabsf( fx ) + fabsf( fy ) ) * Rs + fabsf( fo ) );
+        bool cuts = false;
+        for ( int k = 0; k < C.m; ++k ) {
+            const float X = __shfl_sync( FULL, C.vx, k ), Y = __shfl_sync( FULL, C.vy, k );
+            cuts |= fx * X + fy * Y - fo > -band;
+        }
+        unsigned todo = __ballot_sync( FULL, valid && cuts );
+        while ( todo ) {
+            int k = __ffs( todo ) - 1;
+            todo &= todo - 1;
+            double nx = __shfl_sync( FULL, qx, k ), ny = __shfl_sync( FULL, qy, k ), no = __shfl_sync( FULL, off, k );
+            int nid = __shfl_sync( FULL, j, k );
+            if ( ! wclip( C, lane, nx, ny, no, nid, Rs, P, px, py, wi ) ) { overflow = true; break; }
+            if ( C.m == 0 ) break;
+        }
+    }
+}
+
+// the FP32 polygon in FP64: every vertex re-solved from its two lines (the FP64 kernel's crossing), the lines in FP64
+__device__ __forceinline__ void to_fp64( const WPolyF &F, WPoly &C, const ProbDev &P, int lane, double px, double py, double wi ) {
+    C.m = F.m;
+    C.lid = F.lid;
+    double a = 0, b = 0, c = 0;
+    if ( lane < F.m ) line64( P, F.lid, px, py, wi, a, b, c );
+    C.lnx = a; C.lny = b; C.loff = c;
+    const int prv = lane == 0 ? ( F.m > 0 ? F.m - 1 : 0 ) : lane - 1;
+    const double pa = __shfl_sync( FULL, a, prv ), pb = __shfl_sync( FULL, b, prv ), pc = __shfl_sync( FULL, c, prv );
+    double X = F.vx, Y = F.vy;
+    bool ok = false;
+    if ( lane < F.m && ! F.ip ) isect( pa, pb, pc, a, b, c, X, Y, ok );
+    C.vx = ok ? X : double( F.vx );
+    C.vy = ok ? Y : double( F.vy );
+}
+
 __device__ __forceinline__ void record_error( const ProbDev &P, ErrRec *err, int code, int prob, int seed, int needed ) {
     if ( P.perr ) *P.perr = 1.0;
     if ( atomicCAS( &err->code, 0, code ) == 0 ) { err->kind = 2; err->prob = prob; err->seed = seed; err->needed = needed; }
@@ -516,6 +737,81 @@ __device__ void finish_report( const ProbDev &P, const Chunk &ch, double ( *sh )
     __syncthreads();
 }
 
+__device__ __forceinline__ void start_flags( WPoly & ) {}
+__device__ __forceinline__ void start_flags( WPolyF &C ) { C.ip = false; }
+
+// THE CLIP of the cell of seed s (rank): the box, then the grid's rings, then the pyramid of weight majorants; `Poly`
+// the FP64 polygon (WPoly) or the FP32 one (WPolyF, precision "mixed")
+template<class Poly>
+__device__ __forceinline__ void clip2( Poly &C, const ProbDev &P, int lane, int s, double px, double py, double wi, double wmax, int2 *stk,
+                                       bool &overflow ) {
+    C.m = 4;
+    start_flags( C );
+    {
+        double lx = P.lo[ 0 ] - px, ly = P.lo[ 1 ] - py, hx = P.hi[ 0 ] - px, hy = P.hi[ 1 ] - py;
+        C.vx = ( lane == 1 || lane == 2 ) ? hx : lx;
+        C.vy = ( lane >= 2 ) ? hy : ly;
+        C.lnx = lane == 1 ? 1.0 : ( lane == 3 ? -1.0 : 0.0 );
+        C.lny = lane == 0 ? -1.0 : ( lane == 2 ? 1.0 : 0.0 );
+        C.loff = lane == 0 ? -ly : ( lane == 1 ? hx : ( lane == 2 ? hy : -lx ) );
+        C.lid = -1 - lane;
+    }
+    // ---- the walk over the grid rings
+    const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
+    int cx = int( floor( ( px - P.go[ 0 ] ) / P.gh[ 0 ] ) ), cy = int( floor( ( py - P.go[ 1 ] ) / P.gh[ 1 ] ) );
+    cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
+    cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
+    int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
+    int rd = -1;                 // the rings walked, when the pyramid takes over
+    for ( int r = 0; r <= rmax && C.m > 0 && ! overflow; ++r ) {
+        const int ncell = r == 0 ? 1 : 8 * r;
+        // a grid cell farther than the security radius of its own largest weight holds no cutting seed
+        double R2 = Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 );
+        for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
+            int ci = cb + lane, beg = 0, cnt = 0;
+            if ( ci < ncell ) {
+                int dx, dy;
+                ring_offset( r, ci, dx, dy );
+                int x = cx + dx, y = cy + dy;
+                if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
+                    const size_t gc = ( size_t ) y * g0 + x;
+                    if ( may_cut( cells_dist2( P, x, x, y, y, px, py ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2, wi ) ) {
+                        int2 rg = P.cell_range[ gc ];
+                        beg = rg.x;
+                        cnt = rg.y - rg.x;
+                    }
+                }
+            }
+            cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
+        }
+        if ( C.m == 0 || overflow ) break;
+        R2 = Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 );
+        double ex = R2 + wmax - wi;
+        if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
+        // the pyramid once the global bound reaches well past the next rings (non-uniform weights)
+        if ( P.wpyr && r >= RINGS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
+    }
+    if ( rd >= 0 && C.m > 0 && ! overflow )
+        walk_pyramid2(
+            P, lane, px, py, wi, cx, cy, rd, stk,
+            [&]( int beg, int cnt ) {
+                cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
+                return C.m > 0 && ! overflow;
+            },
+            [&]() { return Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 ); },
+            [&]( const double *lo, const double *hi, const double *a, double b ) {
+                bool may = false;
+                if ( lane < C.m ) {
+                    const double X[ 2 ] = { px + C.vx, py + C.vy }, v[ 2 ] = { C.vx, C.vy };
+                    may = wmaj_claims( a, b, lo, hi, X, v, 2, wi, Poly::CLAIM_REL );
+                }
+                return __any_sync( FULL, may ) != 0;
+            } );
+}
+
+// the main kernel, one warp per cell; F32: the launch for the problems that clip in FP32 (the others skip its chunks, and
+// the FP64 launch skips theirs -- one kernel each keeps each clip's registers to itself)
+template<bool F32>
 __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                     unsigned flags, ErrRec *err, OvfList *ovf ) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -525,6 +821,7 @@ __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict
     for ( int c = blockIdx.x; c < nchunks; c += gridDim.x ) {
         const Chunk ch = chunks[ c ];
         const ProbDev &P = probs[ ch.prob ];
+        if ( ( P.fp32 != 0 ) != F32 ) continue;          // (block uniform: the other launch's)
         double *rep = sh_rep[ warp ];          // this warp's report accumulators (lane 0 updates them)
         if ( lane == 0 ) {
             Rep r0;
@@ -536,68 +833,13 @@ __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict
             const double px = P.pos[ 2 * ( size_t ) s ], py = P.pos[ 2 * ( size_t ) s + 1 ];
             const double wi = P.w ? P.w[ s ] : 0.0;
             WPoly C;
-            C.m = 4;
-            {
-                double lx = P.lo[ 0 ] - px, ly = P.lo[ 1 ] - py, hx = P.hi[ 0 ] - px, hy = P.hi[ 1 ] - py;
-                C.vx = ( lane == 1 || lane == 2 ) ? hx : lx;
-                C.vy = ( lane >= 2 ) ? hy : ly;
-                C.lnx = lane == 1 ? 1.0 : ( lane == 3 ? -1.0 : 0.0 );
-                C.lny = lane == 0 ? -1.0 : ( lane == 2 ? 1.0 : 0.0 );
-                C.loff = lane == 0 ? -ly : ( lane == 1 ? hx : ( lane == 2 ? hy : -lx ) );
-                C.lid = -1 - lane;
-            }
             bool overflow = false;
-            // ---- the walk over the grid rings
-            const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
-            int cx = int( floor( ( px - P.go[ 0 ] ) / P.gh[ 0 ] ) ), cy = int( floor( ( py - P.go[ 1 ] ) / P.gh[ 1 ] ) );
-            cx = cx < 0 ? 0 : ( cx >= g0 ? g0 - 1 : cx );
-            cy = cy < 0 ? 0 : ( cy >= g1 ? g1 - 1 : cy );
-            int rmax = max( max( cx, g0 - 1 - cx ), max( cy, g1 - 1 - cy ) );
-            int rd = -1;                 // the rings walked, when the pyramid takes over
-            for ( int r = 0; r <= rmax && C.m > 0 && ! overflow; ++r ) {
-                const int ncell = r == 0 ? 1 : 8 * r;
-                // a grid cell farther than the security radius of its own largest weight holds no cutting seed
-                double R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
-                for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
-                    int ci = cb + lane, beg = 0, cnt = 0;
-                    if ( ci < ncell ) {
-                        int dx, dy;
-                        ring_offset( r, ci, dx, dy );
-                        int x = cx + dx, y = cy + dy;
-                        if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
-                            const size_t gc = ( size_t ) y * g0 + x;
-                            if ( may_cut( cells_dist2( P, x, x, y, y, px, py ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2, wi ) ) {
-                                int2 rg = P.cell_range[ gc ];
-                                beg = rg.x;
-                                cnt = rg.y - rg.x;
-                            }
-                        }
-                    }
-                    cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
-                }
-                if ( C.m == 0 || overflow ) break;
-                R2 = warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 );
-                double ex = R2 + wmax - wi;
-                if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
-                // the pyramid once the global bound reaches well past the next rings (non-uniform weights)
-                if ( P.wpyr && r >= RINGS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
-            }
-            if ( rd >= 0 && C.m > 0 && ! overflow )
-                walk_pyramid2(
-                    P, lane, px, py, wi, cx, cy, rd, sh_stk[ warp ],
-                    [&]( int beg, int cnt ) {
-                        cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
-                        return C.m > 0 && ! overflow;
-                    },
-                    [&]() { return warp_max( lane < C.m ? C.vx * C.vx + C.vy * C.vy : 0.0 ); },
-                    [&]( const double *lo, const double *hi, const double *a, double b ) {
-                        bool may = false;
-                        if ( lane < C.m ) {
-                            const double X[ 2 ] = { px + C.vx, py + C.vy }, v[ 2 ] = { C.vx, C.vy };
-                            may = wmaj_claims( a, b, lo, hi, X, v, 2, wi );
-                        }
-                        return __any_sync( FULL, may ) != 0;
-                    } );
+            if constexpr ( F32 ) {
+                WPolyF F;
+                clip2( F, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
+                if ( ! overflow ) to_fp64( F, C, P, lane, px, py, wi );
+            } else
+                clip2( C, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
             const int user = P.user[ s ];
             if ( overflow ) {
                 // past the 32 vertices a warp holds: the global-memory pass rebuilds it (report included)
@@ -755,10 +997,11 @@ void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, 
     ++*L.launches;
 }
 
-void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf ) {
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
+                     int clips ) {
     if ( nchunks <= 0 ) return;
-    k_cells2d<<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
-    ++*L.launches;
+    if ( clips & 1 ) { k_cells2d<false><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf ); ++*L.launches; }
+    if ( clips & 2 ) { k_cells2d<true><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf ); ++*L.launches; }
 }
 
 // ---- the big cells: one warp per cell, the polygon in global memory (two buffers of VBIG vertices) ---------------------------

@@ -716,8 +716,10 @@ static bool convolvable( const SolveJob &J ) { return J.G.dkind == D_GAUSS || ( 
 
 SolveJob *job_create( Ctx &c, const sdot_solve_desc &desc ) {
     const sdot_diagram_desc &D = desc.diagram;
-    if ( desc.options[ SDOT_OPT_PRECISION ] != 0 )
-        throw Error( SDOT_ERR_UNSUPPORTED, "option precision: FP64 clipping only (0)" );
+    if ( desc.options[ SDOT_OPT_PRECISION ] != 0 && desc.options[ SDOT_OPT_PRECISION ] != 1 )
+        throw Error( SDOT_ERR_ARGS, "option precision: 0 (FP64 clipping) or 1 (FP32 clipping with FP64 re-checks)" );
+    if ( desc.options[ SDOT_OPT_PRECISION ] == 1 && desc.diagram.dim != 2 )
+        throw Error( SDOT_ERR_UNSUPPORTED, "option precision 1 (FP32 clipping with FP64 re-checks) is built in 2D; 3D clips in FP64 (0)" );
     if ( desc.options[ SDOT_OPT_LIN_PRECISION ] != 0 && desc.options[ SDOT_OPT_LIN_PRECISION ] != 1 )
         throw Error( SDOT_ERR_ARGS, "option lin_precision: 0 (FP64 CG) or 1 (FP32 CG with FP64 iterative refinement)" );
     if ( c.pool_limit ) {
@@ -1847,6 +1849,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
         with_diag.push_back( J );
         ProbDev P;
         J->G.fill( P );
+        P.fp32 = int( J->opt[ SDOT_OPT_PRECISION ] ) == 1;
         P.cap = J->cap;
         P.w = R.w;
         P.wmax_slot = R.wslot;
@@ -1931,7 +1934,10 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
                     for ( auto &ch : CX[ q ] ) gseeds += PX[ ch.prob ].dkind == D_GAUSS ? ch.end - ch.begin : 0;
                 const Split3 *sp = dim == 3 ? split3_for( c, int( CX[ q ].size() ), gseeds ) : nullptr;
                 c.timer.begin( c.stream, dim == 2 ? K_CELLS2D : K_CELLS3D, seeds );
-                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf );
+                int clips = 0;
+                if ( dim == 2 )
+                    for ( auto &ch : CX[ q ] ) clips |= PX[ ch.prob ].fp32 ? 2 : 1;
+                if ( dim == 2 ) launch_cells2d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf, clips );
                 else launch_cells3d( L, dp, dc, int( CX[ q ].size() ), flags, c.derr, c.dovf, sp );
                 c.timer.end( c.stream, sp ? 2 : 1 );
             }
@@ -1963,6 +1969,7 @@ void jobs_tick( Ctx &c, std::vector<SolveJob *> &jobs ) {
             LimDev D;
             std::memset( &D, 0, sizeof( D ) );
             J->G.fill( D.P );
+            D.P.fp32 = 0;
             D.P.cap = J->cap;
             D.P.w = J->w;
             D.d = J->d;

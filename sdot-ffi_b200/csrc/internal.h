@@ -56,6 +56,7 @@ __host__ __device__ inline int wmom_size( int dim ) { return dim == 2 ? 9 : 14; 
 
 struct ProbDev {
     int dim, dkind, cap, n;
+    int fp32;                     // 2D: the clip in FP32 with FP64 re-checks (precision "mixed"), the outputs in FP64
     double lo[3], hi[3];
     int g[3];
     double go[3], gh[3], ghmin;
@@ -316,7 +317,9 @@ SDOT_DEV double wmaj_b( const ProbDev &P, size_t node ) {
 // may a seed of a node with majorant w <= a . q + b, q in the box [ lo, hi ], claim the point X = p_i + v of seed i's
 // cell?  Its power distance there is at least min_q |X - q|^2 - a . q - b = dist^2( X + a/2, box ) - a . X - |a|^2/4 - b,
 // against |v|^2 - w_i for seed i (with a margin of rounding)
-SDOT_DEV bool wmaj_claims( const double *a, double b, const double *lo, const double *hi, const double *X, const double *v, int dim, double wi ) {
+// (rel: the margin, relative to the terms; larger for a vertex held in FP32)
+SDOT_DEV bool wmaj_claims( const double *a, double b, const double *lo, const double *hi, const double *X, const double *v, int dim, double wi,
+                           double rel = 1e-12 ) {
     double d2 = 0, aX = 0, a2 = 0, v2 = 0;
     for ( int q = 0; q < dim; ++q ) {
         double u = X[ q ] + 0.5 * a[ q ];
@@ -327,7 +330,7 @@ SDOT_DEV bool wmaj_claims( const double *a, double b, const double *lo, const do
         v2 += v[ q ] * v[ q ];
     }
     double lhs = d2 - aX - 0.25 * a2 - b, rhs = v2 - wi;
-    return lhs < rhs + 1e-12 * ( fabs( aX ) + fabs( b ) + fabs( wi ) + v2 + d2 );
+    return lhs < rhs + rel * ( fabs( aX ) + fabs( b ) + fabs( wi ) + v2 + d2 );
 }
 
 // ---- launchers (each in the .cu next to its kernels) --------------------------------------------------
@@ -427,7 +430,9 @@ void launch_trial( const Launch &L, const VecDev *v, const Chunk *ch, int nch );
 // cells2d.cu / cells3d.cu
 // the limits of the cells below the floor (one thread a cell; chunks of CHUNK cells over the LimDev array)
 void launch_limits2d( const Launch &L, const LimDev *lims, const Chunk *chunks, int nchunks );
-void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf );
+// clips: bit 0 the problems that clip in FP64, bit 1 those that clip in FP32 (ProbDev.fp32): one launch each
+void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
+                     int clips = 1 );
 // the queued big cells (count known on the host), polygons in `scratch` (VBIG vertices x 2 buffers per warp)
 void launch_cells2d_big( const Launch &L, const ProbDev *probs, const OvfList *ovf, int count, unsigned flags, ErrRec *err, char *scratch,
                          int warps );

@@ -100,9 +100,12 @@ class PowerDiagram:
         self._positions = pos
         self._weights = None if weights is None else np.asarray(weights, dtype=np.float64).reshape(n).copy()
         self.distribution = distribution
-        if kernel_dtype not in (None, "FP64", "fp64", "double"):
-            raise NotImplementedError("PowerDiagram: kernel_dtype FP64 only in this build (B200 clips in FP64 at half the FP32 rate)")
-        self._kernel_dtype = "FP64"
+        if kernel_dtype not in (None, "FP64", "fp64", "double", "FP32", "fp32", "float"):
+            raise ValueError(f"PowerDiagram: unknown kernel_dtype {kernel_dtype!r} ( 'FP64' or 'FP32' )")
+        # FP32: the clip in FP32 with FP64 re-checks, the outputs in FP64 (the reference's float kernel); 2D only here
+        self._kernel_dtype = "FP32" if kernel_dtype in ("FP32", "fp32", "float") else "FP64"
+        if self._kernel_dtype == "FP32" and d != 2:
+            raise NotImplementedError("PowerDiagram: kernel_dtype FP32 is built in 2D; 3D clips in FP64")
 
     # ---- the seeds ----------------------------------------------------------------------------------------
     @property
@@ -125,6 +128,9 @@ class PowerDiagram:
     def dim_count(self):
         return self._positions.shape[1]
 
+    def _precision(self):
+        return 1 if self._kernel_dtype == "FP32" else 0
+
     @property
     def kernel_dtype(self):
         return self._kernel_dtype
@@ -138,12 +144,12 @@ class PowerDiagram:
     @property
     def measures(self):
         """the measure of each cell, [n], in the order of `positions` (the integral of the distribution if any)"""
-        return _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density())["masses"]
+        return _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), precision=self._precision())["masses"]
 
     @property
     def moments(self):
         """`( masses, first, second )`: int rho, int x rho [n, d], int |x|^2 rho (PowerDiagram.py:448-477)"""
-        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_moments=True)
+        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_moments=True, precision=self._precision())
         m, b, c = r["masses"], r["barycentres"], r["costs"]
         first = m[:, None] * b
         p = self._positions
@@ -152,18 +158,18 @@ class PowerDiagram:
 
     def barycenters_and_costs(self):
         """`( masses, barycentres [n, d], costs [n] = int_cell |x - p_i|^2 rho )`, one sweep"""
-        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_moments=True)
+        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_moments=True, precision=self._precision())
         return r["masses"], r["barycentres"], r["costs"]
 
     def hessian_rows(self):
         """`( nb_nbrs, ids, vals )`: per cell its seed neighbours and `int_facet rho / ( 2 |p_i - p_j| )`
         (PowerDiagram.py:478-497).  Host arrays."""
-        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_facets=True)
+        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_facets=True, precision=self._precision())
         return r["nb_count"].astype(int), r["nb_ids"], r["nb_coef"]
 
     def facets(self):
         """`( nb_nbrs, ids, coef, measure )`: as `hessian_rows`, plus `int_facet rho` (the face length / area for rho = 1)"""
-        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_facets=True)
+        r = _lib.cells(self._positions, self._weights, self.box_min, self.box_max, self._density(), want_facets=True, precision=self._precision())
         return r["nb_count"].astype(int), r["nb_ids"], r["nb_coef"], r["nb_measure"]
 
     def laplacian(self):

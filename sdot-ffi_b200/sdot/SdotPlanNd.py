@@ -61,14 +61,14 @@ def solver_options(settings, n, d=None):
         raise ValueError(f"unknown residual: {tun.residual!r} ( {', '.join(_RESIDUAL)} )")
     if tun.linear_solver not in ("auto", "cg", "mg", "amg"):
         raise NotImplementedError(f"linear_solver = {tun.linear_solver!r}: 'auto' / 'mg' (multigrid-PCG) or 'cg' (Jacobi-PCG) in this build")
-    if settings.kernel_dtype != "FP64":
-        raise NotImplementedError(f"precision = {settings.precision!r}: FP64 cells only in this build")
+    if settings.kernel_dtype == "FP32" and d is not None and d != 2:
+        raise NotImplementedError(f"precision = {settings.precision!r}: the FP32 clip is built in 2D; 3D clips in FP64 ( 'fp64' / 'auto' )")
     return dict(tol_abs=settings.tol, tol_rel=float(tun.mass_rtol), maxit=settings.max_iter, max_backtracks=tun.max_backtracks,
                 t_min=tun.t_min, mult_ok=tun.restart_factor, residual=_RESIDUAL[tun.residual], power=tun.residual_power,
                 switch=tun.residual_switch, lin_tol=float(tun.linear_tol or 1e-6), lin_maxit=int(tun.linear_maxit or 20000),
                 keep_start=int(bool(tun.keep_start)), continuation=_CONTINUATION[settings.continuation], conv_threshold=tun.conv_threshold,
                 conv_s0=float(tun.conv_start or 0.0), conv_ratio=float(tun.conv_ratio), conv_min=float(tun.conv_min or 0.0),
-                lin_method=0 if tun.linear_solver == "cg" else 1, precision=0,
+                lin_method=0 if tun.linear_solver == "cg" else 1, precision=1 if settings.kernel_dtype == "FP32" else 0,
                 lin_precision=1 if getattr(tun, "linear_precision", "fp64") == "mixed" else 0,
                 agg_margin=(float(_AGGREGATE_MARGIN if tun.aggregation_margin is None else tun.aggregation_margin) if settings.aggregate else 0.0),
                 step=0 if tun.step == "auto" and d is not None and d != 2 else _STEP[tun.step])

@@ -246,12 +246,13 @@ def diagram_desc(pos, weights, lo, hi, dens, keep, memory=SDOT_HOST):
     return desc
 
 
-def cells(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None):
+def cells(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None, precision=0):
     """one diagram on the GPU; host arrays in and out.  A cell with more facets than the table's row is reported
-    with the capacity it needs, and the call runs again with that capacity (PowerDiagram.py:198-215)."""
+    with the capacity it needs, and the call runs again with that capacity (PowerDiagram.py:198-215).  `precision` 1:
+    the clip in FP32 with FP64 re-checks (2D)"""
     while True:
         try:
-            return _cells_once(pos, weights, lo, hi, dens, want_facets, want_moments, cap)
+            return _cells_once(pos, weights, lo, hi, dens, want_facets, want_moments, cap, precision)
         except KernelFailure as e:
             grown = max(int(e.needed), 2 * (cap or 32))
             if not want_facets or e.needed <= (cap or 0) or grown > 8192:
@@ -259,7 +260,7 @@ def cells(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap
             cap = grown
 
 
-def _cells_once(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None):
+def _cells_once(pos, weights, lo, hi, dens, want_facets=False, want_moments=False, cap=None, precision=0):
     L = load()
     keep = []
     pos = f64(pos)
@@ -267,6 +268,7 @@ def _cells_once(pos, weights, lo, hi, dens, want_facets=False, want_moments=Fals
     w = None if weights is None else f64(weights).reshape(-1)
     desc = diagram_desc(pos, w, lo, hi, dens, keep)
     out = CellsOut()
+    out.precision = int(precision)
     res = {"masses": np.zeros(n)}
     out.masses = res["masses"].ctypes.data
     if want_moments:

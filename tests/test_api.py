@@ -55,8 +55,9 @@ def test_settings_map_onto_the_option_vector():
     assert solver_options(Iterative(), 10, 3)["step"] == 0
     with pytest.raises(ValueError):
         solver_options(Iterative(tuning=Tuning(step="bisection")), 10)
+    assert solver_options(Iterative(precision="mixed"), 10, 2)["precision"] == 1     # the FP32 clip (2D)
     with pytest.raises(NotImplementedError):
-        solver_options(Iterative(precision="mixed"), 10)
+        solver_options(Iterative(precision="mixed"), 10, 3)
     with pytest.raises(ValueError):
         Iterative(precision="fp16")
     with pytest.raises(ValueError):

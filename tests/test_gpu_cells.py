@@ -15,11 +15,11 @@ from sdot import PowerDiagram, box_half_spaces
 pytestmark = pytest.mark.gpu
 
 
-def _pd(pos, w=None, lo=None, hi=None, dist=None):
+def _pd(pos, w=None, lo=None, hi=None, dist=None, kernel_dtype=None):
     d = pos.shape[1]
     lo = np.zeros(d) if lo is None else lo
     hi = np.ones(d) if hi is None else hi
-    return PowerDiagram(pos, w, boundaries=box_half_spaces(lo, hi), distribution=dist)
+    return PowerDiagram(pos, w, boundaries=box_half_spaces(lo, hi), distribution=dist, kernel_dtype=kernel_dtype)
 
 
 def test_known_answers(known_answers):
@@ -36,7 +36,7 @@ def test_known_answers(known_answers):
             assert abs(m.sum() - case["total"]) < tol * max(1, case["total"]), case["name"]
 
 
-def _compare(pos, w, dens=None, n_check=None):
+def _compare(pos, w, dens=None, n_check=None, kernel_dtype=None):
     d = pos.shape[1]
     lo, hi = np.zeros(d), np.ones(d)
     od = None
@@ -44,7 +44,7 @@ def _compare(pos, w, dens=None, n_check=None):
     if dens is not None:
         od, dist = dens
     ref = O.cells(pos, w, box=(lo, hi), density=od)
-    pd = _pd(pos, w, lo, hi, dist)
+    pd = _pd(pos, w, lo, hi, dist, kernel_dtype)
     nb, ids, coef, meas = pd.facets()
     m, bary, cost = pd.barycenters_and_costs()
     assert ref["status"] == 0
@@ -88,6 +88,60 @@ def test_uniform_cells_match_the_oracle(n, wscale):
     w = rng.uniform(0, wscale, size=n) if wscale else None
     m = _compare(pos, w)
     assert abs(m.sum() - 1) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["uniform", "weights", "image", "gaussians"])
+def test_the_fp32_clip_matches_the_oracle(case):
+    """precision "mixed" (kernel_dtype FP32: the clip in FP32, a vertex within the FP32 band of a plane re-checked in FP64,
+    every vertex re-solved in FP64 before the integration -- the reference's float kernel, gpu/Cell2D.cuh:56-60, 991-1042)
+    against the FP64 oracle, with the FP64 clip's tolerances: masses within 1e-10 relative, neighbour sets of the
+    non-degenerate facets bit-exact, c_ij within 1e-10 of the row's largest"""
+    rng = np.random.default_rng(77)
+    n = 20000
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, 2e-5, size=n) if case == "weights" else None
+    dens = None
+    if case == "image":
+        img = sdot.Image(rng.uniform(0.1, 1.0, size=(64, 48)), frame=[1 / 64, 1 / 48])
+        dens = (("image", [0, 0], [1 / 64, 1 / 48], img.normalized_version().values), img)
+    if case == "gaussians":
+        c, s = rng.uniform(0.3, 0.7, size=(4, 2)), rng.uniform(0.05, 0.15, size=4)
+        g = sdot.SumOfGaussians(c, s, support_box=(np.zeros(2), np.ones(2)))
+        dens = (("gauss", c, s, g.normalized_version().weights), g)
+    m = _compare(pos, w, dens, kernel_dtype="FP32")
+    if case in ("uniform", "weights"):
+        assert abs(m.sum() - 1) < 1e-12
+
+
+@pytest.mark.parametrize("n,wscale", [(20000, 0.0), (100000, 1.0)])
+def test_the_fp32_clip_gives_the_fp64_cells(n, wscale):
+    """the FP32 clip decides every vertex as the FP64 one (its band sends the doubtful ones to an FP64 re-check) and
+    re-solves every vertex from the same two lines: the same neighbour tables as the FP64 clip, masses, centroids and
+    coefficients within 1e-13 relative; the two kernels' times are printed side by side"""
+    import time
+    from sdot import _lib
+    rng = np.random.default_rng(5 + n)
+    pos = rng.uniform(size=(n, 2))
+    w = rng.uniform(0, wscale * n ** -1.0, size=n) if wscale else None
+    out = {}
+    for dt in ("FP64", "FP32"):
+        pd = _pd(pos, w, kernel_dtype=dt)
+        pd.facets()
+        _lib.set_timing(True)
+        _lib.kernel_stats(reset=True)
+        nb, ids, coef, meas = _pd(pos, w, kernel_dtype=dt).facets()
+        ms = _lib.kernel_stats()["cells2d"][0]
+        _lib.set_timing(False)
+        m, bary, _ = _pd(pos, w, kernel_dtype=dt).barycenters_and_costs()
+        out[dt] = (nb, ids, coef, m, bary, ms)
+    (nb, ids, coef, m, bary, t64), (nb2, ids2, coef2, m2, bary2, t32) = out["FP64"], out["FP32"]
+    assert (nb == nb2).all()
+    for i in range(n):
+        assert set(ids[i, : nb[i]]) == set(ids2[i, : nb2[i]]), i
+    assert np.abs(m - m2).max() <= 1e-13 * m.max()
+    assert np.abs(bary - bary2).max() <= 1e-12
+    assert np.abs(np.sort(coef, axis=1) - np.sort(coef2, axis=1)).max() <= 1e-13 * coef.max()
+    print(f"\n2D cells, {n} seeds: FP64 clip {1e6 * t64 / n:.2f} ns per cell, FP32 clip {1e6 * t32 / n:.2f} ns per cell")
 
 
 @pytest.mark.parametrize("n,wscale", [(500, 0.0), (20000, 0.0), (20000, 2e-4)])

@@ -43,6 +43,30 @@ def test_plain_2d_fp64_n10000_matches_the_oracle():
     assert len(plan.history) >= plan.stats["nb_iter"] + 1
 
 
+@pytest.mark.parametrize("target", ["uniform", "gaussians"])
+def test_the_fp32_clip_solve_reaches_the_fp64_plan(target):
+    """precision "mixed" (the clip in FP32 with FP64 re-checks, every vertex re-solved in FP64): the 2D Newton converges to
+    max |m - nu| / nu <= 1e-8 as the FP64 one; the oracle's diagram at its weights confirms it; its weights agree with
+    the FP64 solve's within 1e-9 of max|w|"""
+    n = 10000
+    rng = np.random.default_rng(20260303)
+    pos = rng.uniform(size=(n, 2))
+    dst = None
+    od = None
+    if target == "gaussians":
+        c, s = rng.uniform(0.3, 0.7, size=(4, 2)), rng.uniform(0.05, 0.15, size=4)
+        dst = sdot.SumOfGaussians(c, s, support_box=(np.zeros(2), np.ones(2)))
+        od = ("gauss", c, s, dst.normalized_version().weights)
+    a = _solve(pos, dst)
+    b = _solve(pos, dst, precision="mixed")
+    assert a.converged and b.converged, (a.stats["status"], b.stats["status"])
+    nu = np.asarray(b.target_masses).reshape(-1)
+    assert np.abs(b.cell_masses / nu - 1).max() <= 1e-8
+    chk = O.cells(pos, b.weights, density=od)["mass"]
+    assert np.abs(chk / nu - 1).max() <= 1e-8 * (1 + 1e-6)
+    assert np.abs(a.weights - b.weights).max() <= 1e-9 * np.abs(a.weights).max()
+
+
 @pytest.mark.parametrize("lin", ["cg", "mg"])
 @pytest.mark.parametrize("lp", ["fp64", "mixed"])
 def test_both_linear_solvers_reach_the_same_plan(lin, lp):

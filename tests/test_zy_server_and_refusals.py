@@ -51,13 +51,14 @@ def test_the_server_returns_the_plans_of_the_batched_solve():
 
 
 def test_the_unbuilt_precisions_are_refused():
-    """no silent FP64 in place of the FP32-clip variant: `precision` 1 of a cells call, and the `precision` option of a
-    solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch; `lin_precision` 2 is an argument error"""
+    """no silent FP64 in place of an FP32 clip that is not built: in 3D, `precision` 1 of a cells call, and the
+    `precision` option of a solve, are SDOT_ERR_UNSUPPORTED (NotImplementedError), before any launch; `lin_precision` 2
+    is an argument error"""
     import ctypes
     from sdot import _lib
     from sdot.SdotPlanNd import solver_options
-    pos = np.random.default_rng(3).uniform(size=(200, 2))
-    lo, hi = np.zeros(2), np.ones(2)
+    pos = np.random.default_rng(3).uniform(size=(200, 3))
+    lo, hi = np.zeros(3), np.ones(3)
     keep = []
     desc = _lib.diagram_desc(pos, None, lo, hi, ("uniform", 1.0), keep)
     m = np.zeros(200)
@@ -70,7 +71,7 @@ def test_the_unbuilt_precisions_are_refused():
     opts = dict(solver_options(Iterative(), 200), lin_precision=2)
     r = _lib.solve_batch([(pos, None, None, lo, hi, ("uniform", 1.0))], [opts])[0]
     assert isinstance(r, ValueError), r
-    assert np.abs(_pd(pos).measures.sum() - 1) < 1e-12          # the context is still usable
+    assert np.abs(_pd(pos[:, :2]).measures.sum() - 1) < 1e-12   # the context is still usable
 
 
 def test_the_weights_are_differentiable():
