@@ -3,7 +3,6 @@
 // gpu/Bsp2D.cuh:366-456): consecutive ranks are neighbours in space, and every seed is found by the
 // cell it falls in.  Its weight majorants are a pyramid of maxima over the grid (below).
 #include "internal.h"
-#include <cub/device/device_radix_sort.cuh>
 
 namespace sdot {
 
@@ -84,17 +83,126 @@ void launch_keys( const Launch &L, const double *pos, int n, int dim, const int 
     ++*L.launches;
 }
 
+// ---- THE SORT of the Morton keys (the reference sorts its own keys too, gpu/Bsp2D.cuh:72-186) --------------------------------
+// A stable least-significant-digit radix sort of ( key, value ) pairs on the keys' low `bits` bits, 8 bits a pass, three
+// launches a pass: the digit histogram of every tile of RS_TILE keys (digit-major: [ digit ][ tile ]), its exclusive scan
+// (the place of each tile's keys of each digit), and the scatter, which ranks a tile's keys of one digit in index order --
+// 8 rounds of 256 consecutive keys, a warp's equal digits found by __match_any_sync, the warps' counts summed in warp
+// order -- so that equal digits keep their order and every pass is stable.
+constexpr int RS_T = 256, RS_K = 8, RS_TILE = RS_T * RS_K, RS_BINS = 256;
+
+__global__ void __launch_bounds__( RS_T ) k_rs_hist( const unsigned long long *__restrict__ keys, int n, int shift, int *hist, int tiles ) {
+    __shared__ int h[ RS_BINS ];
+    h[ threadIdx.x ] = 0;
+    __syncthreads();
+    const int t0 = blockIdx.x * RS_TILE;
+    for ( int k = threadIdx.x; k < RS_TILE; k += RS_T ) {
+        const int i = t0 + k;
+        if ( i < n ) atomicAdd( &h[ int( ( keys[ i ] >> shift ) & 0xff ) ], 1 );
+    }
+    __syncthreads();
+    hist[ ( size_t ) threadIdx.x * tiles + blockIdx.x ] = h[ threadIdx.x ];
+}
+
+// exclusive scan of `count` ints in place, one block of 1024 threads (warp scans, then the warps' totals)
+__global__ void __launch_bounds__( 1024 ) k_rs_scan( int *v, long count ) {
+    __shared__ int wt[ 32 ];
+    __shared__ long long carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ( threadIdx.x == 0 ) carry = 0;
+    __syncthreads();
+    for ( long base = 0; base < count; base += 1024 ) {
+        const long i = base + threadIdx.x;
+        const int x = i < count ? v[ i ] : 0;
+        int inc = x;
+#pragma unroll
+        for ( int o = 1; o < 32; o <<= 1 ) { const int t = __shfl_up_sync( 0xffffffffu, inc, o ); if ( lane >= o ) inc += t; }
+        if ( lane == 31 ) wt[ warp ] = inc;
+        __syncthreads();
+        if ( warp == 0 ) {
+            int w = wt[ lane ], wi = w;
+#pragma unroll
+            for ( int o = 1; o < 32; o <<= 1 ) { const int t = __shfl_up_sync( 0xffffffffu, wi, o ); if ( lane >= o ) wi += t; }
+            wt[ lane ] = wi - w;                               // exclusive prefix of the warps' totals
+        }
+        __syncthreads();
+        const long long c = carry;
+        if ( i < count ) v[ i ] = int( c + wt[ warp ] + inc - x );
+        __syncthreads();
+        if ( threadIdx.x == 1023 ) carry = c + wt[ warp ] + inc;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__( RS_T ) k_rs_scatter( const unsigned long long *__restrict__ kin, const int *__restrict__ vin,
+                                                       unsigned long long *kout, int *vout, int n, int shift, const int *__restrict__ off,
+                                                       int tiles ) {
+    __shared__ int cnt[ RS_T / 32 ][ RS_BINS ];
+    __shared__ int base[ RS_BINS ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    base[ threadIdx.x ] = off[ ( size_t ) threadIdx.x * tiles + blockIdx.x ];
+    const int t0 = blockIdx.x * RS_TILE;
+    for ( int r = 0; r < RS_K; ++r ) {
+        for ( int w = 0; w < RS_T / 32; ++w ) cnt[ w ][ threadIdx.x ] = 0;
+        __syncthreads();
+        const int i = t0 + r * RS_T + threadIdx.x;
+        const bool in = i < n;
+        unsigned long long key = 0;
+        int val = 0, d = RS_BINS;                          // (RS_BINS: no key)
+        if ( in ) { key = kin[ i ]; val = vin[ i ]; d = int( ( key >> shift ) & 0xff ); }
+        const unsigned peers = __match_any_sync( 0xffffffffu, d );
+        const int lower = __popc( peers & ( ( 1u << lane ) - 1 ) );
+        if ( in && lower == 0 ) cnt[ warp ][ d ] = __popc( peers );
+        __syncthreads();
+        if ( in ) {
+            int rank = base[ d ] + lower;
+            for ( int w = 0; w < warp; ++w ) rank += cnt[ w ][ d ];
+            kout[ rank ] = key;
+            vout[ rank ] = val;
+        }
+        __syncthreads();
+        int add = 0;
+        for ( int w = 0; w < RS_T / 32; ++w ) add += cnt[ w ][ threadIdx.x ];
+        base[ threadIdx.x ] += add;
+        __syncthreads();
+    }
+}
+
 size_t radix_temp_bytes( int n, int bits ) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs( nullptr, bytes, ( const unsigned long long * ) nullptr, ( unsigned long long * ) nullptr,
-                                     ( const int * ) nullptr, ( int * ) nullptr, n, 0, bits );
-    return bytes;
+    (void) bits;
+    const size_t tiles = ( size_t( n ) + RS_TILE - 1 ) / RS_TILE;
+    return ( ( size_t( n ) * 8 + 255 ) & ~size_t( 255 ) ) + ( ( size_t( n ) * 4 + 255 ) & ~size_t( 255 ) ) + tiles * RS_BINS * 4 + 256;
 }
 
 void radix_sort( const Launch &L, void *temp, size_t temp_bytes, const unsigned long long *kin, unsigned long long *kout, const int *vin,
                  int *vout, int n, int bits ) {
-    cub::DeviceRadixSort::SortPairs( temp, temp_bytes, kin, kout, vin, vout, n, 0, bits, L.stream );
-    *L.launches += ( bits + 7 ) / 8 + 1;
+    (void) temp_bytes;
+    if ( n <= 0 ) return;
+    const int passes = ( bits + 7 ) / 8;
+    if ( passes == 0 ) {
+        cudaMemcpyAsync( kout, kin, size_t( n ) * 8, cudaMemcpyDeviceToDevice, L.stream );
+        cudaMemcpyAsync( vout, vin, size_t( n ) * 4, cudaMemcpyDeviceToDevice, L.stream );
+        return;
+    }
+    const int tiles = ( n + RS_TILE - 1 ) / RS_TILE;
+    char *t = static_cast<char *>( temp );
+    unsigned long long *kt = reinterpret_cast<unsigned long long *>( t );
+    int *vt = reinterpret_cast<int *>( t + ( ( size_t( n ) * 8 + 255 ) & ~size_t( 255 ) ) );
+    int *hist = reinterpret_cast<int *>( reinterpret_cast<char *>( vt ) + ( ( size_t( n ) * 4 + 255 ) & ~size_t( 255 ) ) );
+    const unsigned long long *ks = kin;
+    const int *vs = vin;
+    for ( int p = 0; p < passes; ++p ) {
+        // the last pass writes the output; the passes before alternate so that it does
+        const bool to_out = ( passes - 1 - p ) % 2 == 0;
+        unsigned long long *kd = to_out ? kout : kt;
+        int *vd = to_out ? vout : vt;
+        k_rs_hist<<<tiles, RS_T, 0, L.stream>>>( ks, n, 8 * p, hist, tiles );
+        k_rs_scan<<<1, 1024, 0, L.stream>>>( hist, long( tiles ) * RS_BINS );
+        k_rs_scatter<<<tiles, RS_T, 0, L.stream>>>( ks, vs, kd, vd, n, 8 * p, hist, tiles );
+        *L.launches += 3;
+        ks = kd;
+        vs = vd;
+    }
 }
 
 __global__ void k_gather( const double *__restrict__ pos, const int *__restrict__ vals, int n, int dim, double *pos_ranked, int *user,
