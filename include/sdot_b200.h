@@ -146,6 +146,17 @@ int32_t sdot_cells(sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_o
 int32_t sdot_cells_vjp(sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, double *grad_positions,
                        double *grad_weights, sdot_status *st);
 
+/* the adjoint of the masses and of the first moments F_i = int_{cell_i} x rho (world frame: the mass times the
+   barycentre that sdot_cells writes): given `grad_masses` [n] and / or `grad_first` [n, dim] (either may be NULL, not both),
+   writes `grad_positions` [n, dim] and `grad_weights` [n] (either may be NULL).  Replaces the backward of
+   `PowerDiagram.moment(k)` for k < dim (src/sdot/PowerDiagram.py:341-353, "differentiable like measures"), which
+   `SdotPlanNd._attach_derivatives` turns into the barycentres' derivative (SdotPlanNd.py:1018-1070).  A facet ij moves
+   by dw / 2|p_ij| with a weight and by (x - p_i).dp_i / |p_ij| with a seed, so with G = gF_i - gF_j:
+   grad_w_i += G . int_facet x rho / 2|p_ij|, grad_p_i += ((G . p_i) int_facet (x - p_i) rho
+   + int_facet (x - p_i)(x - p_i)^T rho G) / |p_ij|.  A constant density only (SDOT_ERR_UNSUPPORTED otherwise). */
+int32_t sdot_cells_vjp_moments(sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, const double *grad_first,
+                               double *grad_positions, double *grad_weights, sdot_status *st);
+
 /* the Laplacian of the Laguerre graph, CSR in user order, bit-symmetric, `dia` = row sum (1 for an empty row).
    `row_ptr` [n+1], `cols` [cap_nnz], `vals` [cap_nnz] (c_ij > 0: the matrix holds -c_ij), `dia` [n].
    `*nnz` receives the entry count; past `cap_nnz` the call fails with SDOT_ERR_CAPACITY and `needed`.

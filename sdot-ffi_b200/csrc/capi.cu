@@ -266,9 +266,10 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
     } );
 }
 
-int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, double *grad_positions, double *grad_weights,
-                        sdot_status *st ) {
-    if ( ! ctx || ! desc || ! grad_masses ) { set_status( st, SDOT_ERR_ARGS, "null argument" ); return SDOT_ERR_ARGS; }
+// the adjoint of the masses and / or of the first moments: one cell pass in user order
+static int32_t cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, const double *grad_first,
+                          double *grad_positions, double *grad_weights, sdot_status *st ) {
+    if ( ! ctx || ! desc || ( ! grad_masses && ! grad_first ) ) { set_status( st, SDOT_ERR_ARGS, "null argument" ); return SDOT_ERR_ARGS; }
     std::lock_guard<std::mutex> lock( ctx->mu );
     return guard( st, [&] {
         Ctx &c = ctx->c;
@@ -278,6 +279,8 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         if ( dim != 2 && dim != 3 ) throw Error( SDOT_ERR_ARGS, "dim must be 2 or 3" );
         if ( dim == 3 && desc->density.kind != SDOT_DENSITY_UNIFORM )
             throw Error( SDOT_ERR_UNSUPPORTED, "the adjoint of 3D cells is written for a constant density (as the reference's card)" );
+        if ( grad_first && desc->density.kind != SDOT_DENSITY_UNIFORM )
+            throw Error( SDOT_ERR_UNSUPPORTED, "the adjoint of the first moments is written for a constant density" );
         Geometry G;
         build_geometry( c, G, dim, n, desc->positions, desc->box_lo, desc->box_hi, desc->density, desc->memory );
         struct Free { Ctx &c; Geometry &G; ~Free() { free_geometry( c, G ); } } fg{ c, G };
@@ -292,6 +295,7 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         Launch L = c.L();
         InArr w( c, desc->weights, n, desc->memory );
         InArr gm( c, grad_masses, n, desc->memory );
+        InArr gf( c, grad_first, size_t( n ) * dim, desc->memory );
         launch_gather_vec( L, w.d, G.user, int( n ), wr, w.d ? 1.0 : 0.0 );
         CK( cudaMemsetAsync( slot, 0, 8, c.stream ) );
         launch_wmax( L, wr, int( n ), slot );
@@ -301,6 +305,7 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         P.w = wr;
         P.wmax_slot = slot;
         P.gm = gm.d;
+        P.gf = gf.d;
         P.gpos = grad_positions ? gp : nullptr;
         P.gw = grad_weights ? gw : nullptr;
         std::vector<Chunk> ch;
@@ -324,6 +329,17 @@ int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const d
         CK( cudaStreamSynchronize( c.stream ) );
         check_errors( c, "sdot_cells_vjp" );
     } );
+}
+
+int32_t sdot_cells_vjp( sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, double *grad_positions, double *grad_weights,
+                        sdot_status *st ) {
+    if ( ! grad_masses ) { set_status( st, SDOT_ERR_ARGS, "null argument" ); return SDOT_ERR_ARGS; }
+    return cells_vjp( ctx, desc, grad_masses, nullptr, grad_positions, grad_weights, st );
+}
+
+int32_t sdot_cells_vjp_moments( sdot_context ctx, const sdot_diagram_desc *desc, const double *grad_masses, const double *grad_first,
+                                double *grad_positions, double *grad_weights, sdot_status *st ) {
+    return cells_vjp( ctx, desc, grad_masses, grad_first, grad_positions, grad_weights, st );
 }
 
 int32_t sdot_laplacian( sdot_context ctx, const sdot_diagram_desc *desc, int64_t cap_nnz, int64_t *row_ptr, int32_t *cols, double *vals, double *dia,

@@ -811,6 +811,39 @@ __device__ __forceinline__ void clip2( Poly &C, const ProbDev &P, int lane, int 
 
 // the main kernel, one warp per cell; F32: the launch for the problems that clip in FP32 (the others skip its chunks, and
 // the FP64 launch skips theirs -- one kernel each keeps each clip's registers to itself)
+// THE ADJOINT of the masses and of the first moments of one cell (its lane's edge), the row `ui` of the outputs: off the
+// clip's register allocation (a call, not inlined)
+__device__ __noinline__ void vjp2( const ProbDev &P, int lane, bool fac, int ui, int uj, double cij, double dist, const EdgeInt &e, double ax,
+                                   double ay, double x1, double y1, double px, double py ) {
+    // the masses: grad_w_i = sum_j c_ij ( g_i - g_j ); grad_p_i = sum_j 2 c_ij ( g_i - g_j ) ( x_ij - p_i )
+    double gw = 0, gpx = 0, gpy = 0;
+    if ( fac && P.gm ) {
+        const double dg = P.gm[ ui ] - P.gm[ uj ];
+        gw = cij * dg;
+        const double cxm = e.mx / e.meas, cym = e.my / e.meas;      // facet centroid, seed frame
+        gpx = 2 * cij * dg * cxm;
+        gpy = 2 * cij * dg * cym;
+    }
+    // the first moments F_i = int_cell x rho (a constant density): the facet ij moves by dw_j / 2|p_ij| when a weight
+    // changes and by ( x - p_i ) . dp_i / |p_ij| when a seed moves, so with G = gF_i - gF_j and y = x - p_i:
+    // grad_w_i += G . int_facet x rho / 2|p_ij|, grad_p_i += ( ( G . p_i ) int_facet y rho + int_facet y y^T rho G ) / |p_ij|
+    if ( fac && P.gf ) {
+        const double gx = P.gf[ 2 * size_t( ui ) ] - P.gf[ 2 * size_t( uj ) ], gy = P.gf[ 2 * size_t( ui ) + 1 ] - P.gf[ 2 * size_t( uj ) + 1 ];
+        gw += ( gx * ( e.meas * px + e.mx ) + gy * ( e.meas * py + e.my ) ) / ( 2 * dist );
+        // the segment A -> B (seed frame): int y y^T = rho len ( 2 A A^T + A B^T + B A^T + 2 B B^T ) / 6
+        const double sxx = e.meas * ( ax * ax + ax * x1 + x1 * x1 ) / 3, syy = e.meas * ( ay * ay + ay * y1 + y1 * y1 ) / 3;
+        const double sxy = e.meas * ( 2 * ax * ay + ax * y1 + x1 * ay + 2 * x1 * y1 ) / 6;
+        const double pg = px * gx + py * gy;
+        gpx += ( pg * e.mx + sxx * gx + sxy * gy ) / dist;
+        gpy += ( pg * e.my + sxy * gx + syy * gy ) / dist;
+    }
+    gw = warp_sum( gw ); gpx = warp_sum( gpx ); gpy = warp_sum( gpy );
+    if ( lane == 0 ) {
+        if ( P.gw ) P.gw[ ui ] = gw;
+        if ( P.gpos ) { P.gpos[ 2 * ( size_t ) ui ] = gpx; P.gpos[ 2 * ( size_t ) ui + 1 ] = gpy; }
+    }
+}
+
 template<bool F32>
 __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                     unsigned flags, ErrRec *err, OvfList *ovf ) {
@@ -898,25 +931,8 @@ __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict
                 }
                 if ( lane == 0 ) P.nb[ row ] = nf;
             }
-            if ( flags & F_VJP ) {
-                // grad_w_i = sum_j c_ij ( g_i - g_j ); grad_p_i = sum_j 2 c_ij ( g_i - g_j ) ( x_ij - p_i )
-                double gi = P.gm[ user_order ? user : s ];
-                double gw = 0, gpx = 0, gpy = 0;
-                if ( fac ) {
-                    double gj = P.gm[ user_order ? P.user[ C.lid ] : C.lid ];
-                    double dg = gi - gj;
-                    gw = cij * dg;
-                    double cxm = e.mx / e.meas, cym = e.my / e.meas;      // facet centroid, seed frame
-                    gpx = 2 * cij * dg * cxm;
-                    gpy = 2 * cij * dg * cym;
-                }
-                gw = warp_sum( gw ); gpx = warp_sum( gpx ); gpy = warp_sum( gpy );
-                if ( lane == 0 ) {
-                    int row = user_order ? user : s;
-                    if ( P.gw ) P.gw[ row ] = gw;
-                    if ( P.gpos ) { P.gpos[ 2 * ( size_t ) row ] = gpx; P.gpos[ 2 * ( size_t ) row + 1 ] = gpy; }
-                }
-            }
+            if ( flags & F_VJP ) vjp2( P, lane, fac, user_order ? user : s, user_order ? P.user[ C.lid < 0 ? 0 : C.lid ] : C.lid, cij, dist, e, C.vx,
+                                       C.vy, x1, y1, px, py );
             if ( moments ) {
                 double fx = warp_sum( e.fx ), fy = warp_sum( e.fy ), s2 = warp_sum( e.s2 );
                 if ( lane == 0 ) {

@@ -1003,7 +1003,13 @@ __device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, 
         // THE ADJOINT of the masses (gpu/Cell3D.cuh:1954-1978), a constant density: grad_w_i = sum_j c_ij ( g_i - g_j ),
         // grad_p_i = sum_j 2 c_ij ( g_i - g_j ) ( x_ij - p_i ), x_ij the facet's centroid -- summed triangle by triangle of
         // the facets, c_f K T, each with its own centroid (no per-facet storage)
-        const double gi = P.gm[ user_order ? user : s ];
+        // The first moments F_i = int_cell x rho: with G = gF_i - gF_j, y = x - p_i and the face triangle ( c_f, K, T ) of
+        // area a, int y = a ( c_f + K + T ) / 3 and int y y^T = a ( c_f c_f^T + K K^T + T T^T + S S^T ) / 12, S = c_f + K + T:
+        // grad_w_i += G . int x rho / 2|p_ij|, grad_p_i += ( ( G . p_i ) int y rho + int y y^T rho G ) / |p_ij|
+        const int ui = user_order ? user : s;
+        const double gi = P.gm ? P.gm[ ui ] : 0.0;
+        const double gfx = P.gf ? P.gf[ 3 * size_t( ui ) ] : 0.0, gfy = P.gf ? P.gf[ 3 * size_t( ui ) + 1 ] : 0.0,
+                     gfz = P.gf ? P.gf[ 3 * size_t( ui ) + 2 ] : 0.0;
         double gw = 0, gx = 0, gy = 0, gz = 0;
         for ( int k = lane; k < nv; k += 32 ) {
             const int e[ 3 ] = { C.va[ k ], C.vb[ k ], C.vc[ k ] };
@@ -1015,12 +1021,28 @@ __device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, 
                 if ( t == C3::NONE ) continue;
                 const double nn = C.nx[ f ] * C.nx[ f ] + C.ny[ f ] * C.ny[ f ] + C.nz[ f ] * C.nz[ f ];
                 const double cf = C.no[ f ] / nn;
-                const double gj = P.gm[ user_order ? P.user[ j ] : j ];
-                const double coef = rho * a2 / ( 2 * sqrt( nn ) ) * ( gi - gj );
-                gw += coef;
-                gx += 2 * coef * ( C.nx[ f ] * cf + C.vx[ k ] + C.vx[ t ] ) / 3;
-                gy += 2 * coef * ( C.ny[ f ] * cf + C.vy[ k ] + C.vy[ t ] ) / 3;
-                gz += 2 * coef * ( C.nz[ f ] * cf + C.vz[ k ] + C.vz[ t ] ) / 3;
+                const size_t uj = user_order ? P.user[ j ] : j;
+                const double dist = sqrt( nn );
+                const double Cx = C.nx[ f ] * cf, Cy = C.ny[ f ] * cf, Cz = C.nz[ f ] * cf;
+                const double Sx = Cx + C.vx[ k ] + C.vx[ t ], Sy = Cy + C.vy[ k ] + C.vy[ t ], Sz = Cz + C.vz[ k ] + C.vz[ t ];
+                if ( P.gm ) {
+                    const double coef = rho * a2 / ( 2 * dist ) * ( gi - P.gm[ uj ] );
+                    gw += coef;
+                    gx += 2 * coef * Sx / 3;
+                    gy += 2 * coef * Sy / 3;
+                    gz += 2 * coef * Sz / 3;
+                }
+                if ( P.gf ) {
+                    const double Gx = gfx - P.gf[ 3 * uj ], Gy = gfy - P.gf[ 3 * uj + 1 ], Gz = gfz - P.gf[ 3 * uj + 2 ];
+                    const double ra = rho * a2;
+                    gw += ( Gx * ( ra * px + ra * Sx / 3 ) + Gy * ( ra * py + ra * Sy / 3 ) + Gz * ( ra * pz + ra * Sz / 3 ) ) / ( 2 * dist );
+                    const double Kx = C.vx[ k ], Ky = C.vy[ k ], Kz = C.vz[ k ], Tx = C.vx[ t ], Ty = C.vy[ t ], Tz = C.vz[ t ];
+                    const double cg = Cx * Gx + Cy * Gy + Cz * Gz, kg = Kx * Gx + Ky * Gy + Kz * Gz, tg = Tx * Gx + Ty * Gy + Tz * Gz,
+                                 sg = Sx * Gx + Sy * Gy + Sz * Gz, pg = px * Gx + py * Gy + pz * Gz;
+                    gx += ( pg * ra * Sx / 3 + ra / 12 * ( Cx * cg + Kx * kg + Tx * tg + Sx * sg ) ) / dist;
+                    gy += ( pg * ra * Sy / 3 + ra / 12 * ( Cy * cg + Ky * kg + Ty * tg + Sy * sg ) ) / dist;
+                    gz += ( pg * ra * Sz / 3 + ra / 12 * ( Cz * cg + Kz * kg + Tz * tg + Sz * sg ) ) / dist;
+                }
             }
         }
         gw = warp_sum( gw ); gx = warp_sum( gx ); gy = warp_sum( gy ); gz = warp_sum( gz );

@@ -81,7 +81,8 @@ struct ProbDev {
     double *nc;                   // [n, cap]
     double *nm;                   // [n, cap]
     const double *nu;             // [n] ranked targets (report)
-    const double *gm;             // [n] cotangent of masses (vjp), ranked
+    const double *gm;             // [n] cotangent of masses (vjp), ranked (NULL: none)
+    const double *gf;             // [n, dim] cotangent of the first moments int_cell x rho, world frame (vjp; NULL: none)
     double *gpos;                 // [n, dim] (vjp)
     double *gw;                   // [n] (vjp)
     double *report;               // [NB_REPORT] per problem (report)

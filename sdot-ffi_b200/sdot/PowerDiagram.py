@@ -190,6 +190,13 @@ class PowerDiagram:
         """the adjoint of `measures`: `( grad_positions [n, d], grad_weights [n] )` for the cotangent `grad_masses`"""
         return _lib.cells_vjp(self._positions, self._weights, self.box_min, self.box_max, self._density(), grad_masses)
 
+    def moments_vjp(self, grad_masses=None, grad_first=None):
+        """the adjoint of the masses and of the first moments `int_cell x rho` [n, d] (the backward of `moment(k)`, k < d,
+        PowerDiagram.py:341-353): `( grad_positions [n, d], grad_weights [n] )`.  A constant density."""
+        if grad_first is None:
+            return self.measures_vjp(np.zeros(self.nb_points) if grad_masses is None else grad_masses)
+        return _lib.cells_vjp(self._positions, self._weights, self.box_min, self.box_max, self._density(), grad_masses, grad_first)
+
 
 class Voronoi(PowerDiagram):
     """the power diagram without weights"""

@@ -88,6 +88,7 @@ SIGNATURES = {
                                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     "sdot_cells": (ctypes.c_int32, [_P, ctypes.POINTER(DiagramDesc), ctypes.POINTER(CellsOut), ctypes.POINTER(Status)]),
     "sdot_cells_vjp": (ctypes.c_int32, [_P, ctypes.POINTER(DiagramDesc), _P, _P, _P, ctypes.POINTER(Status)]),
+    "sdot_cells_vjp_moments": (ctypes.c_int32, [_P, ctypes.POINTER(DiagramDesc), _P, _P, _P, _P, ctypes.POINTER(Status)]),
     "sdot_laplacian": (ctypes.c_int32, [_P, ctypes.POINTER(DiagramDesc), ctypes.c_int64, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64),
                                         ctypes.POINTER(Status)]),
     "sdot_linear_solve": (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P, _P, _P, ctypes.c_int32, _P, _P, ctypes.c_int32, ctypes.c_double,
@@ -288,17 +289,24 @@ def _cells_once(pos, weights, lo, hi, dens, want_facets=False, want_moments=Fals
     return res
 
 
-def cells_vjp(pos, weights, lo, hi, dens, grad_masses):
+def cells_vjp(pos, weights, lo, hi, dens, grad_masses, grad_first=None):
+    """(grad_positions [n, d], grad_weights [n]) for the cotangents of the masses [n] and / or (sdot_cells_vjp_moments)
+    of the first moments int_cell x rho [n, d]"""
     L = load()
     keep = []
     pos = f64(pos)
     n, d = pos.shape
     w = None if weights is None else f64(weights).reshape(-1)
     desc = diagram_desc(pos, w, lo, hi, dens, keep)
-    g = f64(grad_masses).reshape(-1)
+    g = None if grad_masses is None else f64(grad_masses).reshape(-1)
     gp, gw = np.zeros((n, d)), np.zeros(n)
     st = Status()
-    raise_for(L.sdot_cells_vjp(context(), ctypes.byref(desc), ptr(g), ptr(gp), ptr(gw), ctypes.byref(st)), st, "sdot_cells_vjp")
+    if grad_first is None:
+        raise_for(L.sdot_cells_vjp(context(), ctypes.byref(desc), ptr(g), ptr(gp), ptr(gw), ctypes.byref(st)), st, "sdot_cells_vjp")
+    else:
+        gf = f64(grad_first).reshape(n, d)
+        raise_for(L.sdot_cells_vjp_moments(context(), ctypes.byref(desc), None if g is None else ptr(g), ptr(gf), ptr(gp), ptr(gw),
+                                           ctypes.byref(st)), st, "sdot_cells_vjp_moments")
     return gp, gw
 
 

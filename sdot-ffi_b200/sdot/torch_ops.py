@@ -3,12 +3,15 @@
     cost = w2_batch(positions, nu=None, target=None)        # positions [B, N, d] on a CUDA device, FP32 or FP64
     cost.sum().backward()                                   # positions.grad, nu.grad
     w = weights_batch(positions, nu)                        # the fitted weights [B, N], differentiable too
+    b = barycentres_batch(positions, nu)                    # the cells' barycentres [B, N, d], differentiable too
 
 Forward: ONE call of the C ABI (`sdot_solve_batch`) on the device pointers -- the B problems advance together.
 Backward: the hand-written kernel `sdot_w2_backward` -- the envelope theorem at the fitted weights,
 d W2 / d p_i = 2 m_i (p_i - b_i) and d W2 / d nu_i = w_i projected on sum(d nu) = 0 (SdotPlanNd.py:1037-1040,
 1107-1122).  The weights' backward is the implicit-function derivative (SdotPlanNd.py:1018-1050): one Laplacian solve
-and one adjoint of the masses a problem, `weights_vjp`.  PyTorch only owns the device memory and the autograd graph.
+and one adjoint of the masses a problem, `weights_vjp`.  The barycentres' backward (SdotPlanNd.py:1051-1070: first / mass at
+the live weights) adds the adjoint of the masses and first moments at fixed weights (`sdot_cells_vjp_moments`) to the
+weights' own.  PyTorch only owns the device memory and the autograd graph.
 """
 import ctypes
 
@@ -131,14 +134,25 @@ def _solve_one(row, cols, vals, dia, rhs):
     return x[0]
 
 
+def _pullback(pos, w, nub, grad_w, lo, hi, dens, domain_mass):
+    """`weights_vjp` through the C ABI: the Laplacian, its CG solve and the masses adjoint of one problem"""
+    return weights_vjp(pos, w, nub, grad_w, lambda p, ww: _lib.laplacian(p, ww, lo, hi, dens), _solve_one,
+                       lambda p, ww, lam: _lib.cells_vjp(p, ww, lo, hi, dens, lam)[0], domain_mass)
+
+
+def _forward_saved(positions, nu, target, settings):
+    """the batched solve on detached inputs: (weights, masses, barycentres), all [B, N(, d)] on the device"""
+    with torch.enable_grad():
+        p = positions.detach().requires_grad_(True)
+        cost = _W2Batch.apply(p, None if nu is None else nu.detach(), target, settings)
+    node = cost.grad_fn
+    return node.saved_tensors[3], node.saved_tensors[1], node.saved_tensors[2]
+
+
 class _WeightsBatch(torch.autograd.Function):
     @staticmethod
     def forward(ctx, positions, nu, target, settings):
-        with torch.enable_grad():
-            p = positions.detach().requires_grad_(True)
-            cost = _W2Batch.apply(p, None if nu is None else nu.detach(), target, settings)
-        node = cost.grad_fn
-        weights, masses = node.saved_tensors[3], node.saved_tensors[1]
+        weights, masses, _ = _forward_saved(positions, nu, target, settings)
         ctx.save_for_backward(positions, weights, masses, nu if nu is not None else torch.empty(0, device=positions.device))
         ctx.has_nu, ctx.target = nu is not None, target
         return weights.clone()
@@ -155,17 +169,61 @@ class _WeightsBatch(torch.autograd.Function):
             pos = positions[b].detach().to(torch.float64).cpu().numpy()
             w = weights[b].cpu().numpy()
             nub = nu[b].detach().to(torch.float64).cpu().numpy() if ctx.has_nu else None
-            x, xn = weights_vjp(pos, w, nub, grad_w[b].detach().to(torch.float64).cpu().numpy(),
-                                lambda p, ww: _lib.laplacian(p, ww, lo, hi, dens),
-                                _solve_one,
-                                lambda p, ww, lam: _lib.cells_vjp(p, ww, lo, hi, dens, lam)[0],
-                                float(masses[b].sum()))
+            x, xn = _pullback(pos, w, nub, grad_w[b].detach().to(torch.float64).cpu().numpy(), lo, hi, dens, float(masses[b].sum()))
             gp[b] = torch.from_numpy(x)
             if ctx.has_nu:
                 gn[b] = torch.from_numpy(xn)
         gp = gp.to(device=positions.device, dtype=positions.dtype)
         gn = None if gn is None else gn.to(device=positions.device, dtype=nu.dtype)
         return gp, gn, None, None
+
+
+class _BarycentresBatch(torch.autograd.Function):
+    """b_i = F_i / m_i (F_i = int_cell x rho) at the fitted weights; an empty cell keeps its seed (SdotPlanNd.py:1066-1068).
+    For a cotangent g_b: g_F = g_b / m, g_m = - (g_b . b) / m; the adjoint at fixed weights gives the explicit part and a
+    cotangent of the weights, which the implicit function theorem carries to the positions and target masses."""
+
+    @staticmethod
+    def forward(ctx, positions, nu, target, settings):
+        weights, masses, bary = _forward_saved(positions, nu, target, settings)
+        ctx.save_for_backward(positions, weights, masses, bary, nu if nu is not None else torch.empty(0, device=positions.device))
+        ctx.has_nu, ctx.target = nu is not None, target
+        return bary.clone()
+
+    @staticmethod
+    def backward(ctx, grad_b):
+        positions, weights, masses, bary, nu = ctx.saved_tensors
+        B, N, d = positions.shape
+        dens, lo, hi = _target_density(ctx.target, d)
+        gp = torch.empty(B, N, d, dtype=torch.float64)
+        gn = torch.empty(B, N, dtype=torch.float64) if ctx.has_nu else None
+        for b in range(B):
+            pos = positions[b].detach().to(torch.float64).cpu().numpy()
+            w, m, bb = weights[b].cpu().numpy(), masses[b].cpu().numpy(), bary[b].cpu().numpy()
+            g = grad_b[b].detach().to(torch.float64).cpu().numpy()
+            full = m > 0
+            inv = np.where(full, 1.0 / np.where(full, m, 1.0), 0.0)
+            gF = g * inv[:, None]
+            gm = -(g * bb).sum(axis=1) * inv
+            gpe, gwe = _lib.cells_vjp(pos, w, lo, hi, dens, gm, gF)
+            nub = nu[b].detach().to(torch.float64).cpu().numpy() if ctx.has_nu else None
+            x, xn = _pullback(pos, w, nub, gwe, lo, hi, dens, float(m.sum()))
+            x = x + gpe
+            x[~full] += g[~full]
+            gp[b] = torch.from_numpy(x)
+            if ctx.has_nu:
+                gn[b] = torch.from_numpy(xn)
+        gp = gp.to(device=positions.device, dtype=positions.dtype)
+        gn = None if gn is None else gn.to(device=positions.device, dtype=nu.dtype)
+        return gp, gn, None, None
+
+
+def barycentres_batch(positions, nu=None, target=None, settings=None):
+    """the barycentres of the cells of the B transports [B, N, d] (FP64) at the fitted weights, differentiable wrt
+    `positions` [B, N, d] and `nu` [B, N] (a constant density): the adjoint of the masses and first moments, then the
+    weights' implicit derivative, one Laplacian solve a problem"""
+    settings = settings or Iterative(tol=0.0, tuning=Tuning(mass_rtol=1e-12))
+    return _BarycentresBatch.apply(positions, nu, target, settings)
 
 
 def weights_batch(positions, nu=None, target=None, settings=None):

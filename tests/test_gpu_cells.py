@@ -337,6 +337,42 @@ def test_the_adjoint_is_the_derivative_of_the_measures():
             assert abs(fd - gp[i, a]) < 1e-5 * max(1, abs(fd))
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_adjoint_of_the_first_moments_is_their_derivative(d):
+    """PowerDiagram.py:341-353 (`moment(k)`, k < d, differentiable like the measures): `sdot_cells_vjp_moments` for the
+    cotangents of the masses and of the first moments int_cell x rho, against central differences of the GPU cells at
+    fixed weights, in the weights and the positions (1e-5 of the largest derivative)"""
+    rng = np.random.default_rng(10 + d)
+    n = 300
+    pos = rng.uniform(size=(n, d))
+    w = rng.uniform(0, 1e-3, size=n)
+    g = rng.standard_normal(n)
+    G = rng.standard_normal((n, d))
+
+    def f(p, ww):
+        m, first, _ = _pd(p, ww).moments
+        return g @ m + (G * first).sum()
+    gp, gw = _pd(pos, w).moments_vjp(g, G)
+    gp0, gw0 = _pd(pos, w).moments_vjp(None, G)
+    gp1, gw1 = _pd(pos, w).measures_vjp(g)
+    assert np.abs(gp0 + gp1 - gp).max() < 1e-12 * np.abs(gp).max() and np.abs(gw0 + gw1 - gw).max() < 1e-12 * np.abs(gw).max()
+    assert abs(gw.sum()) < 1e-10 * np.abs(gw).max()          # a constant added to every weight moves no facet
+    h = 1e-6
+    scale = max(np.abs(gp).max(), np.abs(gw).max())
+    for i in range(0, n, 29):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        fd = (f(pos, wp) - f(pos, wm)) / (2 * h)
+        assert abs(fd - gw[i]) < 1e-5 * scale, (i, fd, gw[i])
+        for a in range(d):
+            pp, pm = pos.copy(), pos.copy()
+            pp[i, a] += h
+            pm[i, a] -= h
+            fd = (f(pp, w) - f(pm, w)) / (2 * h)
+            assert abs(fd - gp[i, a]) < 1e-5 * scale, (i, a, fd, gp[i, a])
+
+
 def test_the_3d_adjoint_is_the_derivative_of_the_measures():
     """gpu/Cell3D.cuh:1954-1978: the adjoint of the 3D masses (constant density) against central differences"""
     rng = np.random.default_rng(7)

@@ -103,6 +103,39 @@ def test_the_weights_are_differentiable():
         assert abs(float(nu.grad[0, k]) - fd) < 1e-5 * max(1.0, abs(fd)), (k, float(nu.grad[0, k]), fd)
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_barycentres_are_differentiable(d):
+    """SdotPlanNd.py:1051-1070 (the barycentres first / mass at the live weights, with their implicit derivative):
+    `torch_ops.barycentres_batch`'s backward (the adjoint of the masses and first moments, then the weights' implicit
+    derivative) against central differences of the GPU solve's barycentres, in the positions and the target masses"""
+    import torch
+    from sdot.torch_ops import barycentres_batch
+    rng = np.random.default_rng(8 + d)
+    n = 200 if d == 2 else 80
+    pos = torch.tensor(rng.uniform(0.2, 0.8, size=(1, n, d)), dtype=torch.float64, device="cuda", requires_grad=True)
+    nu = torch.tensor(rng.uniform(0.5, 1.5, size=(1, n)), dtype=torch.float64, device="cuda", requires_grad=True)
+    settings = Iterative(tol=0.0, max_iter=100, tuning=Tuning(mass_rtol=1e-12))
+    g = torch.tensor(rng.standard_normal((1, n, d)), dtype=torch.float64, device="cuda")
+    (barycentres_batch(pos, nu, settings=settings) * g).sum().backward()
+
+    def loss(p, q):
+        with torch.no_grad():
+            return float((barycentres_batch(p, q, settings=settings) * g).sum())
+    h = 1e-5
+    scale = max(1.0, float(pos.grad.abs().max()))
+    for k, a in ((3, 0), (50, 1), (71, d - 1), (n - 1, 0)):
+        e = torch.zeros_like(pos)
+        e[0, k, a] = h
+        fd = (loss(pos.detach() + e, nu.detach()) - loss(pos.detach() - e, nu.detach())) / (2 * h)
+        assert abs(float(pos.grad[0, k, a]) - fd) < 1e-5 * scale, (k, a, float(pos.grad[0, k, a]), fd)
+    scale = max(1.0, float(nu.grad.abs().max()))
+    for k in (0, 41, n - 2):
+        e = torch.zeros_like(nu)
+        e[0, k] = h
+        fd = (loss(pos.detach(), nu.detach() + e) - loss(pos.detach(), nu.detach() - e)) / (2 * h)
+        assert abs(float(nu.grad[0, k]) - fd) < 1e-5 * scale, (k, float(nu.grad[0, k]), fd)
+
+
 @pytest.mark.parametrize("shape", [(40, 30), (12, 10, 8), (20, 20, 20)])
 def test_grids_give_the_exact_boxes(shape):
     """tests/test_CardCells.py:166-187, 900-941: seeds on a grid (cuts through vertices already on the cell, the ties a
