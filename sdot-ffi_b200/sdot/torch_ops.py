@@ -127,6 +127,26 @@ def weights_vjp(pos, w, nu, grad_w, laplacian, solve, masses_vjp, domain_mass=1.
     return gp, gnu
 
 
+def barycentres_vjp(pos, w, nu, masses, bary, grad_b, moments_vjp, laplacian, solve, masses_vjp, domain_mass=1.0):
+    """the derivative of the barycentres of one transport at its fitted weights (SdotPlanNd.py:1051-1070).
+
+    b_i = F_i / m_i with F_i = int_cell x rho; an empty cell keeps its seed. For a cotangent g of the barycentres:
+    g_F = g / m and g_m = - (g . b) / m; `moments_vjp(pos, w, g_m, g_F)` gives (grad_p, grad_w) of m and F at fixed
+    weights; the weights' cotangent grad_w is carried to the positions and target masses by `weights_vjp` (its other
+    arguments). Returns (grad_p [n, d], grad_nu [n] or None)."""
+    g = np.asarray(grad_b, dtype=np.float64)
+    m = np.asarray(masses, dtype=np.float64).reshape(-1)
+    full = m > 0
+    inv = np.where(full, 1.0 / np.where(full, m, 1.0), 0.0)
+    gF = g * inv[:, None]
+    gm = -(g * np.asarray(bary, dtype=np.float64)).sum(axis=1) * inv
+    gpe, gwe = moments_vjp(pos, w, gm, gF)
+    gp, gnu = weights_vjp(pos, w, nu, gwe, laplacian, solve, masses_vjp, domain_mass)
+    gp = gp + np.asarray(gpe, dtype=np.float64)
+    gp[~full] += g[~full]
+    return gp, gnu
+
+
 def _solve_one(row, cols, vals, dia, rhs):
     x, its = _lib.linear_solve(row, cols, vals, dia, rhs, tol=1e-12, method=1)
     if its[0] < 0:
@@ -201,15 +221,10 @@ class _BarycentresBatch(torch.autograd.Function):
             pos = positions[b].detach().to(torch.float64).cpu().numpy()
             w, m, bb = weights[b].cpu().numpy(), masses[b].cpu().numpy(), bary[b].cpu().numpy()
             g = grad_b[b].detach().to(torch.float64).cpu().numpy()
-            full = m > 0
-            inv = np.where(full, 1.0 / np.where(full, m, 1.0), 0.0)
-            gF = g * inv[:, None]
-            gm = -(g * bb).sum(axis=1) * inv
-            gpe, gwe = _lib.cells_vjp(pos, w, lo, hi, dens, gm, gF)
             nub = nu[b].detach().to(torch.float64).cpu().numpy() if ctx.has_nu else None
-            x, xn = _pullback(pos, w, nub, gwe, lo, hi, dens, float(m.sum()))
-            x = x + gpe
-            x[~full] += g[~full]
+            x, xn = barycentres_vjp(pos, w, nub, m, bb, g, lambda p, ww, gm, gF: _lib.cells_vjp(p, ww, lo, hi, dens, gm, gF),
+                                    lambda p, ww: _lib.laplacian(p, ww, lo, hi, dens), _solve_one,
+                                    lambda p, ww, lam: _lib.cells_vjp(p, ww, lo, hi, dens, lam)[0], float(m.sum()))
             gp[b] = torch.from_numpy(x)
             if ctx.has_nu:
                 gn[b] = torch.from_numpy(xn)

@@ -179,6 +179,78 @@ def test_the_weights_derivative_is_the_derivative_of_the_solve(d):
     assert np.abs(gn - fn).max() < 1e-7 * np.abs(fn).max()
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_barycentres_derivative_is_the_derivative_of_the_solve(d):
+    """SdotPlanNd.py:1051-1070: the barycentres' derivative (`torch_ops.barycentres_vjp`, the backward of
+    `barycentres_batch`: the adjoint of the masses and first moments at fixed weights, then the weights' implicit
+    derivative), driven by the oracle's diagram and finite-difference adjoints, against central differences of the whole
+    oracle solve's barycentres in the positions and the target masses (1e-6 of the largest component)"""
+    import oracle as O
+    from sdot.torch_ops import barycentres_vjp
+    rng = np.random.default_rng(20 + d)
+    n = 12 if d == 2 else 8
+    pos = rng.uniform(0.2, 0.8, size=(n, d))
+    nu = rng.uniform(0.5, 1.5, n)
+
+    def solve(p, q):
+        s = O.solve(p, nu=q / q.sum(), tol_abs=1e-15, maxit=100)
+        assert s["stats"]["status"] == 1
+        return s
+
+    def laplacian(p, w):
+        r = O.cells(p, w)
+        row, cols, vals = [0], [], []
+        for i in range(n):
+            k = r["nb"][i]
+            cols += list(r["nid"][i, :k])
+            vals += list(r["nc"][i, :k])
+            row.append(row[-1] + k)
+        return np.array(row), np.array(cols), np.array(vals), np.array([r["nc"][i, : r["nb"][i]].sum() for i in range(n)])
+
+    def dense_solve(row, cols, vals, dia, rhs):
+        L = np.diag(dia)
+        for i in range(n):
+            L[i, cols[row[i]:row[i + 1]]] -= vals[row[i]:row[i + 1]]
+        return np.linalg.lstsq(0.5 * (L + L.T), rhs, rcond=None)[0]
+
+    def fd_adjoint(p, w, f, h=1e-7):
+        """(grad_p, grad_w) of the scalar f(cells at p, w) by central differences"""
+        gp, gw = np.zeros_like(p), np.zeros(n)
+        for k in range(n):
+            wp, wm = w.copy(), w.copy()
+            wp[k] += h
+            wm[k] -= h
+            gw[k] = (f(O.cells(p, wp)) - f(O.cells(p, wm))) / (2 * h)
+            for a in range(d):
+                pp, pm = p.copy(), p.copy()
+                pp[k, a] += h
+                pm[k, a] -= h
+                gp[k, a] = (f(O.cells(pp, w)) - f(O.cells(pm, w))) / (2 * h)
+        return gp, gw
+
+    def moments_vjp(p, w, gm, gF):
+        return fd_adjoint(p, w, lambda r: gm @ r["mass"] + (gF * r["mass"][:, None] * r["bary"]).sum())
+
+    def masses_vjp(p, w, lam):
+        return fd_adjoint(p, w, lambda r: lam @ r["mass"])[0]
+
+    s = solve(pos, nu)
+    g = rng.standard_normal((n, d))
+    gp, gn = barycentres_vjp(pos, s["weights"], nu, s["masses"], s["bary"], g, moments_vjp, laplacian, dense_solve, masses_vjp,
+                             float(s["masses"].sum()))
+    h = 1e-6
+    fp = np.zeros_like(pos)
+    for k in range(n):
+        for a in range(d):
+            pp, pm = pos.copy(), pos.copy()
+            pp[k, a] += h
+            pm[k, a] -= h
+            fp[k, a] = ((solve(pp, nu)["bary"] - solve(pm, nu)["bary"]) * g).sum() / (2 * h)
+    fn = np.array([((solve(pos, nu + h * e)["bary"] - solve(pos, nu - h * e)["bary"]) * g).sum() / (2 * h) for e in np.eye(n)])
+    assert np.abs(gp - fp).max() < 1e-6 * np.abs(fp).max(), np.abs(gp - fp).max()
+    assert np.abs(gn - fn).max() < 1e-6 * np.abs(fn).max(), np.abs(gn - fn).max()
+
+
 def test_the_domain_comes_from_the_density_alone():
     """tests/test_SdotPlanNd.py:409-438 (its host part): the domain of a gaussian target is the support it declares,
     `centres +- 6 sigma`, not the envelope of the diracs; a target that declares no support is refused"""
