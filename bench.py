@@ -236,12 +236,13 @@ def run_value_step(reqs, seed, torch, check):
     return secs, _lib.kernel_launches() - l0, worst, failed
 
 
-def run_plain(reqs, seed):
-    """one-at-a-time GPU solves through the public API (host arrays): seconds, worst mass error"""
+def run_plain(reqs, seed, keep_per_dim=4):
+    """one-at-a-time GPU solves through the public API (host arrays): seconds, worst mass error, failures, and the fitted
+    weights of the first `keep_per_dim` converged requests of each dimension ([(request, weights)])"""
     from sdot import OtProblem, SumOfDiracs
     from sdot.SdotPlanNd import SdotPlanNd
     t0 = time.perf_counter()
-    worst, failed = 0.0, 0
+    worst, failed, fits = 0.0, 0, []
     for r in reqs:
         plan = OtProblem(SumOfDiracs(positions(seed, r)), target_of(r)).solve(settings())
         if not plan.converged:
@@ -249,7 +250,35 @@ def run_plain(reqs, seed):
             continue
         if plan.stats["status"] == "converged":
             worst = max(worst, float(np.abs(plan.cell_masses / plan.target_masses - 1).max()))
-    return time.perf_counter() - t0, worst, failed
+        if sum(1 for q, _ in fits if q["d"] == r["d"]) < keep_per_dim:
+            fits.append((r, np.asarray(plan.weights, dtype=np.float64)))
+    return time.perf_counter() - t0, worst, failed, fits
+
+
+def gather_model(fits, dim, seed):
+    """the neighbour search's record reads per cell, from the device counters (sdot_context_set_counters), on one diagram at
+    the fitted weights of the kept requests of dimension `dim` (untimed, after the timed legs).  These reads mostly hit L2:
+    the bytes they add to the compulsory ones are a second denominator of the cell kernel's roofline, not DRAM traffic."""
+    from sdot import PowerDiagram, _lib
+    sel = [(r, w) for r, w in fits if r["d"] == dim]
+    if not sel:
+        return None
+    _lib.gather_counters(dim, reset=True)
+    _lib.set_counters(True)
+    try:
+        for r, w in sel:
+            t = target_of(r).normalized_version(nb_dims=dim)
+            PowerDiagram(positions(seed, r), w, boundaries=t.bounding_half_spaces(), distribution=t).measures
+    finally:
+        _lib.set_counters(False)
+    c = _lib.gather_counters(dim, reset=True)
+    cells = max(c["cells"], 1)
+    per = {k: c[k] / cells for k in ("candidates", "grid_cells", "grid_ranges", "nodes")}
+    rec = 8.0 * (dim + 1)              # a seed (position + weight) or a pyramid node (affine majorant)
+    extra = per["candidates"] * rec + per["grid_cells"] * 8 + per["grid_ranges"] * 8 + per["nodes"] * rec
+    return {"per_cell": {k: round(v, 2) for k, v in per.items()}, "bytes_per_cell": BYTES_PER_CELL[dim] + extra,
+            "sample": f"one diagram at the fitted weights of {len(sel)} timed {dim}D requests (k = {[r['k'] for r, _ in sel]}, "
+                      f"{c['cells']} cells), counted by the kernel's counting instantiation"}
 
 
 def run_served(reqs, seed, lam):
@@ -580,7 +609,7 @@ def main():
 
     # plain one-at-a-time on the same requests
     pr = timed
-    p_secs, p_worst, p_failed = run_plain(pr, a.seed)
+    p_secs, p_worst, p_failed, fits = run_plain(pr, a.seed)
     plain = (len(pr) - p_failed) / p_secs
     legs["plain"] = time.perf_counter() - t_leg
     t_leg = time.perf_counter()
@@ -599,6 +628,18 @@ def main():
     cells_b = units * BYTES_PER_CELL[dom]
     achieved = cells_b / (ms / 1000) / 1e9 if ms > 0 else None
     cg_ms, cg_n, cg_rows = kst["cg"]
+    gather = None
+    if rank == 0 and achieved:
+        try:
+            gm = gather_model(fits, dom, a.seed)
+            if gm is not None:
+                ga = gm["bytes_per_cell"] * units / (ms / 1000) / 1e9
+                gather = dict(gm, achieved=ga, frac=ga / hbm, unit="GB/s",
+                              note="search reads counted on the device; they count L2-resident re-reads, not DRAM traffic")
+        except Exception as e:          # a measurement aid: the line stands without it
+            print(f"warning: gather model leg: {e}", file=sys.stderr)
+    legs["gather"] = time.perf_counter() - t_leg
+    t_leg = time.perf_counter()
     cpu = cpu_sample(timed, a.seed, a.cpu_budget, a.cpu_cap) if rank == 0 else None
     legs["cpu"] = time.perf_counter() - t_leg
     if rank != 0:
@@ -619,7 +660,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": f"cells{dom}d (k_cells{dom}d)", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm if achieved else None, "traffic": traffic_of(f"k_cells{dom}d", units / max(nl, 1)),
                      "peak_kind": peak_kind, "algorithmic_bytes_per_cell": BYTES_PER_CELL[dom], "cells_per_launch": units / max(nl, 1),
-                     "avg_launch_ms": ms / max(nl, 1), "cg_ms_share": cg_ms / max(1e-9, 1000 * secs),
+                     "avg_launch_ms": ms / max(nl, 1), "gather_model": gather, "cg_ms_share": cg_ms / max(1e-9, 1000 * secs),
                      "cells_ms_share": ms / max(1e-9, 1000 * secs),
                      "kernel_ms": {k: round(v[0], 3) for k, v in kst.items()},
                      "busy_share": sum(v[0] for v in kst.values()) / max(1e-9, 1000 * secs)},

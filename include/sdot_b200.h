@@ -127,6 +127,17 @@ enum sdot_kernel_class { SDOT_K_CELLS2D = 0, SDOT_K_CELLS3D, SDOT_K_LAPLACIAN, S
                          SDOT_K_MULTIGRID,   /* the multigrid hierarchy's build and the CG's start on it */
                          SDOT_NB_KERNEL_CLASSES };
 int32_t sdot_context_set_timing(sdot_context ctx, int32_t on);
+/* THE GATHER MODEL of the cell kernels' traffic (what the search reads beyond the compulsory bytes, mostly from L2):
+   while on, every `sdot_cells` of the context counts, per dimension, the records its neighbour search reads --
+   candidate seeds (position + weight, 8 (dim + 1) bytes each), grid cells whose weight majorant it tested (8 bytes),
+   grid cells whose seed range it read (8 bytes), pyramid nodes (affine majorant, 8 (dim + 1) bytes) -- in kernel
+   instantiations of their own (the uncounted ones are unchanged).  A measurement aid with no counterpart in the
+   reference, whose device counters (gpu/Cell2D.cuh:363) hold facets and overflow lists only.  The big-cell passes are
+   not counted. */
+int32_t sdot_context_set_counters(sdot_context ctx, int32_t on);
+/* the counts of `dim` (2 or 3) since the last reset: counts[5] = { cells built, candidate seeds, grid cells tested,
+   grid ranges read, pyramid nodes }; synchronises the context's stream */
+int32_t sdot_context_gather_counters(sdot_context ctx, int32_t dim, uint64_t *counts, int32_t reset);
 /* accumulated device time (ms), launches and units (seeds for the cells, rows x iterations for the CG) of a class
    since the last reset; synchronises the context's stream */
 int32_t sdot_context_kernel_stats(sdot_context ctx, int32_t kernel_class, double *ms, uint64_t *launches, double *units, int32_t reset);

@@ -170,6 +170,38 @@ int32_t sdot_context_kernel_stats( sdot_context ctx, int32_t kernel_class, doubl
     } );
 }
 
+int32_t sdot_context_set_counters( sdot_context ctx, int32_t on ) {
+    if ( ! ctx ) return SDOT_ERR_ARGS;
+    std::lock_guard<std::mutex> lock( ctx->mu );
+    ctx->c.gather_on = on != 0;
+    return SDOT_OK;
+}
+
+int32_t sdot_context_gather_counters( sdot_context ctx, int32_t dim, uint64_t *counts, int32_t reset ) {
+    if ( ! ctx || ! counts || ( dim != 2 && dim != 3 ) ) return SDOT_ERR_ARGS;
+    std::lock_guard<std::mutex> lock( ctx->mu );
+    sdot_status st;
+    return guard( &st, [&] {
+        Ctx &c = ctx->c;
+        CK( cudaSetDevice( c.device ) );
+        unsigned long long h[ NB_GATHER * GATHER_SLOTS ];
+        unsigned long long *d = c.dgather + size_t( dim - 2 ) * NB_GATHER * GATHER_SLOTS;
+        CK( cudaMemcpyAsync( h, d, sizeof( h ), cudaMemcpyDeviceToHost, c.stream ) );
+        CK( cudaStreamSynchronize( c.stream ) );
+        counts[ 0 ] = c.gather_cells[ dim - 2 ];
+        for ( int k = 0; k < NB_GATHER; ++k ) {
+            uint64_t sum = 0;
+            for ( int q = 0; q < GATHER_SLOTS; ++q ) sum += h[ k * GATHER_SLOTS + q ];
+            counts[ 1 + k ] = sum;
+        }
+        if ( reset ) {
+            CK( cudaMemsetAsync( d, 0, sizeof( h ), c.stream ) );
+            CK( cudaStreamSynchronize( c.stream ) );
+            c.gather_cells[ dim - 2 ] = 0;
+        }
+    } );
+}
+
 int32_t sdot_context_synchronize( sdot_context ctx, sdot_status *st ) {
     if ( ! ctx ) { set_status( st, SDOT_ERR_ARGS, "null context" ); return SDOT_ERR_ARGS; }
     return guard( st, [&] { CK( cudaSetDevice( ctx->c.device ) ); CK( cudaStreamSynchronize( ctx->c.stream ) ); } );
@@ -232,6 +264,11 @@ int32_t sdot_cells( sdot_context ctx, const sdot_diagram_desc *desc, sdot_cells_
         P.cost = out->costs ? dc : nullptr;
         if ( facets ) { P.nb = dnb; P.nid = dnid; P.nc = dnc; P.nm = dnm; }
         unsigned flags = F_MASS | F_USER_ORDER | ( facets ? F_FACETS : 0u ) | ( ( out->barycentres || out->costs ) ? F_MOMENTS : 0u );
+        if ( c.gather_on ) {
+            P.gather = c.dgather + size_t( dim - 2 ) * NB_GATHER * GATHER_SLOTS;
+            flags |= F_GATHER;
+            c.gather_cells[ dim - 2 ] += uint64_t( n );
+        }
         std::vector<Chunk> ch;
         const int cs = cell_chunk( dim, n );
         for ( int b = 0, k = 0; b < n; b += cs, ++k ) ch.push_back( Chunk{ 0, b, int( std::min<long>( n, b + cs ) ), k } );

@@ -359,7 +359,7 @@ constexpr int WALK_LEAF = 1;         // the walk's leaves: blocks of 2 x 2 grid 
 // (`claims( lo, hi, a, b )`, warp-uniform).  At a leaf block, lane k holds the seed range of its k-th cell (empty if
 // `may_cut` rules it out) and `cut( beg, cnt )` clips by them; it returns false to stop.  `radius2()` is the cell's
 // squared radius.  Lane 0 writes the stack.
-template<class Cut, class Radius2, class Claims>
+template<bool CNT, class Cut, class Radius2, class Claims>
 __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py, double wi, int cx, int cy, int rd, int2 *stk, Cut cut,
                                Radius2 radius2, Claims claims ) {
     const int g0 = P.g[ 0 ], g1 = P.g[ 1 ];
@@ -377,15 +377,22 @@ __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py,
         if ( l <= WALK_LEAF ) {
             const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;           // at most 2 x 2
             int beg = 0, cnt = 0;
+            bool tested = false, ranged = false;
             if ( lane < bw * bh ) {
                 const int x = x0 + lane % bw, y = y0 + lane / bw;
                 const bool walked = x >= cx - rd && x <= cx + rd && y >= cy - rd && y <= cy + rd;
                 const size_t gc = ( size_t ) y * g0 + x;
+                tested = ! walked;
                 if ( ! walked && may_cut( cells_dist2( P, x, x, y, y, px, py ), wmaj_b( P, gc ), R2, wi ) ) {
                     int2 rg = P.cell_range[ gc ];
                     beg = rg.x;
                     cnt = rg.y - rg.x;
+                    ranged = true;
                 }
+            }
+            if constexpr ( CNT ) if ( P.gather ) {
+                count_reads( P, lane, G_GRID, __popc( __ballot_sync( FULL, tested ) ) );
+                count_reads( P, lane, G_RANGE, __popc( __ballot_sync( FULL, ranged ) ) );
             }
             if ( ! cut( beg, cnt ) ) return;
             R2 = radius2();
@@ -399,6 +406,7 @@ __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py,
         bool ok = lane < 4 && X2 < lev_dim( g0, l - 1 ) && Y2 < lev_dim( g1, l - 1 ) &&
                   ! ( a0 >= cx - rd && a1 <= cx + rd && b0 >= cy - rd && b1 <= cy + rd );
         double cb = -1e300, ca0 = 0, ca1 = 0, dd = 0;
+        if constexpr ( CNT ) if ( P.gather ) count_reads( P, lane, G_NODE, __popc( __ballot_sync( FULL, ok ) ) );
         if ( ok ) {
             const size_t rec = P.poff[ l - 1 ] + ( size_t ) Y2 * lev_dim( g0, l - 1 ) + X2;
             cb = wmaj_b( P, rec );
@@ -435,6 +443,7 @@ __device__ void walk_pyramid2( const ProbDev &P, int lane, double px, double py,
 
 // the seeds of up to 32 grid cells (lane k: the range [ beg, beg + cnt ) of one cell) as candidates, 32 at a time:
 // a parallel pre-test against the polygon, then the clips of those that cut, in lane order
+template<bool CNT>
 __device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int lane, int s, double px, double py, double wi, int beg, int cnt,
                                                bool &overflow ) {
     int inc = cnt;
@@ -451,6 +460,7 @@ __device__ __forceinline__ void cut_by_ranges( WPoly &C, const ProbDev &P, int l
         int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
         int j = obeg + ( t - oexc );
         bool valid = t < total && j != s;
+        if constexpr ( CNT ) if ( P.gather ) count_reads( P, lane, G_CAND, __popc( __ballot_sync( FULL, valid ) ) );
         double qx = 0, qy = 0, off = 0;
         if ( valid ) {
             qx = P.pos[ 2 * ( size_t ) j ] - px;
@@ -636,6 +646,7 @@ __device__ __forceinline__ bool wclip( WPolyF &C, int lane, double nx64, double 
     return true;
 }
 
+template<bool CNT>
 __device__ __forceinline__ void cut_by_ranges( WPolyF &C, const ProbDev &P, int lane, int s, double px, double py, double wi, int beg, int cnt,
                                                bool &overflow ) {
     int inc = cnt;
@@ -652,6 +663,7 @@ __device__ __forceinline__ void cut_by_ranges( WPolyF &C, const ProbDev &P, int 
         int obeg = __shfl_sync( FULL, beg, owner ), oexc = __shfl_sync( FULL, exc, owner );
         int j = obeg + ( t - oexc );
         bool valid = t < total && j != s;
+        if constexpr ( CNT ) if ( P.gather ) count_reads( P, lane, G_CAND, __popc( __ballot_sync( FULL, valid ) ) );
         double qx = 0, qy = 0, off = 0;
         if ( valid ) {
             qx = P.pos[ 2 * ( size_t ) j ] - px;
@@ -742,7 +754,7 @@ __device__ __forceinline__ void start_flags( WPolyF &C ) { C.ip = false; }
 
 // THE CLIP of the cell of seed s (rank): the box, then the grid's rings, then the pyramid of weight majorants; `Poly`
 // the FP64 polygon (WPoly) or the FP32 one (WPolyF, precision "mixed")
-template<class Poly>
+template<bool CNT, class Poly>
 __device__ __forceinline__ void clip2( Poly &C, const ProbDev &P, int lane, int s, double px, double py, double wi, double wmax, int2 *stk,
                                        bool &overflow ) {
     C.m = 4;
@@ -769,20 +781,27 @@ __device__ __forceinline__ void clip2( Poly &C, const ProbDev &P, int lane, int 
         double R2 = Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 );
         for ( int cb = 0; cb < ncell && C.m > 0 && ! overflow; cb += 32 ) {
             int ci = cb + lane, beg = 0, cnt = 0;
+            bool tested = false, ranged = false;
             if ( ci < ncell ) {
                 int dx, dy;
                 ring_offset( r, ci, dx, dy );
                 int x = cx + dx, y = cy + dy;
                 if ( x >= 0 && x < g0 && y >= 0 && y < g1 ) {
                     const size_t gc = ( size_t ) y * g0 + x;
+                    tested = P.wpyr != nullptr;
                     if ( may_cut( cells_dist2( P, x, x, y, y, px, py ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2, wi ) ) {
                         int2 rg = P.cell_range[ gc ];
                         beg = rg.x;
                         cnt = rg.y - rg.x;
+                        ranged = true;
                     }
                 }
             }
-            cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
+            if constexpr ( CNT ) if ( P.gather ) {
+                count_reads( P, lane, G_GRID, __popc( __ballot_sync( FULL, tested ) ) );
+                count_reads( P, lane, G_RANGE, __popc( __ballot_sync( FULL, ranged ) ) );
+            }
+            cut_by_ranges<CNT>( C, P, lane, s, px, py, wi, beg, cnt, overflow );
         }
         if ( C.m == 0 || overflow ) break;
         R2 = Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 );
@@ -792,10 +811,10 @@ __device__ __forceinline__ void clip2( Poly &C, const ProbDev &P, int lane, int 
         if ( P.wpyr && r >= RINGS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
     }
     if ( rd >= 0 && C.m > 0 && ! overflow )
-        walk_pyramid2(
+        walk_pyramid2<CNT>(
             P, lane, px, py, wi, cx, cy, rd, stk,
             [&]( int beg, int cnt ) {
-                cut_by_ranges( C, P, lane, s, px, py, wi, beg, cnt, overflow );
+                cut_by_ranges<CNT>( C, P, lane, s, px, py, wi, beg, cnt, overflow );
                 return C.m > 0 && ! overflow;
             },
             [&]() { return Poly::R2_MARGIN * warp_max( lane < C.m ? double( C.vx * C.vx + C.vy * C.vy ) : 0.0 ); },
@@ -844,7 +863,7 @@ __device__ __noinline__ void vjp2( const ProbDev &P, int lane, bool fac, int ui,
     }
 }
 
-template<bool F32>
+template<bool F32, bool CNT>
 __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                     unsigned flags, ErrRec *err, OvfList *ovf ) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -869,10 +888,10 @@ __global__ void __launch_bounds__( 256, 3 ) k_cells2d( const ProbDev *__restrict
             bool overflow = false;
             if constexpr ( F32 ) {
                 WPolyF F;
-                clip2( F, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
+                clip2<CNT>( F, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
                 if ( ! overflow ) to_fp64( F, C, P, lane, px, py, wi );
             } else
-                clip2( C, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
+                clip2<CNT>( C, P, lane, s, px, py, wi, wmax, sh_stk[ warp ], overflow );
             const int user = P.user[ s ];
             if ( overflow ) {
                 // past the 32 vertices a warp holds: the global-memory pass rebuilds it (report included)
@@ -1016,8 +1035,18 @@ void launch_report( const Launch &L, const ProbDev *probs, const Chunk *chunks, 
 void launch_cells2d( const Launch &L, const ProbDev *probs, const Chunk *chunks, int nchunks, unsigned flags, ErrRec *err, OvfList *ovf,
                      int clips ) {
     if ( nchunks <= 0 ) return;
-    if ( clips & 1 ) { k_cells2d<false><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf ); ++*L.launches; }
-    if ( clips & 2 ) { k_cells2d<true><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf ); ++*L.launches; }
+    // the counting instantiations only when the search's reads are counted (F_GATHER): the others compile without them
+    const bool cnt = flags & F_GATHER;
+    if ( clips & 1 ) {
+        if ( cnt ) k_cells2d<false, true><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+        else k_cells2d<false, false><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+        ++*L.launches;
+    }
+    if ( clips & 2 ) {
+        if ( cnt ) k_cells2d<true, true><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+        else k_cells2d<true, false><<<nchunks, 256, 0, L.stream>>>( probs, chunks, nchunks, flags, err, ovf );
+        ++*L.launches;
+    }
 }
 
 // ---- the big cells: one warp per cell, the polygon in global memory (two buffers of VBIG vertices) ---------------------------
@@ -1191,7 +1220,7 @@ __global__ void __launch_bounds__( 32 ) k_cells2d_big( const ProbDev *__restrict
             }
             return __any_sync( FULL, may ) != 0;
         };
-        if ( rd >= 0 && m > 0 && ! overflow ) walk_pyramid2( P, lane, px, py, wi, cx, cy, rd, stk, cut_lanes, radius2, claims );
+        if ( rd >= 0 && m > 0 && ! overflow ) walk_pyramid2<false>( P, lane, px, py, wi, cx, cy, rd, stk, cut_lanes, radius2, claims );
         const int user = P.user[ s ];
         if ( overflow ) {
             // past the global-memory polygon: an error of its problem -- or, in a trial diagram, a refused step

@@ -348,7 +348,7 @@ __device__ __forceinline__ double radius2_3( const C3 &C, int lane ) {
 
 // the seeds of up to 32 grid cells (lane k: the range [ beg, beg + cnt ) of one cell) as candidates, 32 at a time:
 // each lane pre-tests one candidate against every vertex, then the cuts run in lane order
-template<class C3>
+template<bool CNT, class C3>
 __device__ void cut_by_ranges3( C3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, int beg, int cnt,
                                 bool &overflow ) {
     int inc = cnt;
@@ -365,6 +365,7 @@ __device__ void cut_by_ranges3( C3 &C, const ProbDev &P, int lane, int s, double
         int obeg = __shfl_sync( FULL3, beg, owner ), oexc = __shfl_sync( FULL3, exc, owner );
         int j = obeg + ( t - oexc );
         bool valid = t < total && j != s;
+        if constexpr ( CNT ) if ( P.gather ) count_reads( P, lane, G_CAND, __popc( __ballot_sync( FULL3, valid ) ) );
         double qx = 0, qy = 0, qz = 0, off = 0;
         if ( valid ) {
             qx = P.pos[ 3 * ( size_t ) j ] - px;
@@ -398,7 +399,7 @@ constexpr int WALK_LEAF3 = 1;        // the walk's leaves: blocks of 2 x 2 x 2 g
 // one cell per lane, each tested by `may_cut3`, clipped together.  A node's children are tested when it is expanded, one
 // child per lane for their majorant records (eight loads in flight instead of one per pop), then each against the cell's
 // vertices; only the claiming children are pushed
-template<class C3>
+template<bool CNT, class C3>
 __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double px, double py, double pz, double wi, const int *c0, int rd,
                                int2 *stk, bool &overflow ) {
     const int *g = P.g;
@@ -419,18 +420,25 @@ __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double 
         if ( l <= WALK_LEAF3 ) {
             const int bw[ 3 ] = { a1[ 0 ] - a0[ 0 ] + 1, a1[ 1 ] - a0[ 1 ] + 1, a1[ 2 ] - a0[ 2 ] + 1 };   // at most 2 x 2 x 2
             int beg = 0, cnt = 0;
+            bool tested = false, ranged = false;
             if ( lane < bw[ 0 ] * bw[ 1 ] * bw[ 2 ] ) {
                 int x[ 3 ] = { a0[ 0 ] + lane % bw[ 0 ], a0[ 1 ] + ( lane / bw[ 0 ] ) % bw[ 1 ], a0[ 2 ] + lane / ( bw[ 0 ] * bw[ 1 ] ) };
                 bool walked = true;
                 for ( int a = 0; a < 3; ++a ) walked = walked && x[ a ] >= c0[ a ] - rd && x[ a ] <= c0[ a ] + rd;
                 const size_t gc = ( ( size_t ) x[ 2 ] * g[ 1 ] + x[ 1 ] ) * g[ 0 ] + x[ 0 ];
+                tested = ! walked;
                 if ( ! walked && may_cut3( cells_dist2_3( P, x, x, px, py, pz ), wmaj_b( P, gc ), R2, wi ) ) {
                     int2 rg = P.cell_range[ gc ];
                     beg = rg.x;
                     cnt = rg.y - rg.x;
+                    ranged = true;
                 }
             }
-            cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
+            if constexpr ( CNT ) if ( P.gather ) {
+                count_reads( P, lane, G_GRID, __popc( __ballot_sync( FULL3, tested ) ) );
+                count_reads( P, lane, G_RANGE, __popc( __ballot_sync( FULL3, ranged ) ) );
+            }
+            cut_by_ranges3<CNT>( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
             if ( overflow || C.nv == 0 ) return;
             R2 = radius2_3( C, lane );
             continue;
@@ -447,6 +455,7 @@ __device__ void walk_pyramid3( C3 &C, const ProbDev &P, int lane, int s, double 
         }
         ok = ok && ! inside;
         double cb = -1e300, ca[ 3 ] = { 0, 0, 0 }, lo[ 3 ] = { 0, 0, 0 }, hi[ 3 ] = { 0, 0, 0 }, dd = 0;
+        if constexpr ( CNT ) if ( P.gather ) count_reads( P, lane, G_NODE, __popc( __ballot_sync( FULL3, ok ) ) );
         if ( ok ) {
             const size_t rec = P.poff[ l - 1 ] + ( ( size_t ) Y[ 2 ] * lev_dim( g[ 1 ], l - 1 ) + Y[ 1 ] ) * lev_dim( g[ 0 ], l - 1 ) + Y[ 0 ];
             cb = wmaj_b( P, rec );
@@ -812,7 +821,7 @@ __device__ __forceinline__ void queue3( const ProbDev &P, ErrRec *err, OvfList *
 // THE CELL of seed s (rank) of problem `prob`, first half: the clip.  A cell past the vertex / plane capacities of this
 // pass is queued on `ovf` for the next pass (main -> big -> giant; NULL: an error of its problem) and the call returns
 // false (nothing written); true: the clipped cell is in C (possibly empty)
-template<class C3>
+template<bool CNT, class C3>
 __device__ __noinline__ bool clip3( C3 &C, const ProbDev &P, int prob, int s, int lane, ErrRec *err, OvfList *ovf, int2 *stk, double wmax, bool big ) {
     const double px = P.pos[ 3 * ( size_t ) s ], py = P.pos[ 3 * ( size_t ) s + 1 ], pz = P.pos[ 3 * ( size_t ) s + 2 ];
     const double wi = P.w ? P.w[ s ] : 0.0;
@@ -832,20 +841,27 @@ __device__ __noinline__ bool clip3( C3 &C, const ProbDev &P, int prob, int s, in
         const double R2s = radius2_3( C, lane );
         for ( int cb = 0; cb < ncube && C.nv > 0 && ! overflow; cb += 32 ) {
             int ci = cb + lane, beg = 0, cnt = 0;
+            bool tested = false, ranged = false;
             if ( ci < ncube ) {
                 int dx = ci % side - r, dy = ( ci / side ) % side - r, dz = ci / ( side * side ) - r;
                 bool shell = max( abs( dx ), max( abs( dy ), abs( dz ) ) ) == r;
                 int x[ 3 ] = { c0[ 0 ] + dx, c0[ 1 ] + dy, c0[ 2 ] + dz };
                 if ( shell && x[ 0 ] >= 0 && x[ 0 ] < P.g[ 0 ] && x[ 1 ] >= 0 && x[ 1 ] < P.g[ 1 ] && x[ 2 ] >= 0 && x[ 2 ] < P.g[ 2 ] ) {
                     const size_t gc = ( ( size_t ) x[ 2 ] * P.g[ 1 ] + x[ 1 ] ) * P.g[ 0 ] + x[ 0 ];
+                    tested = P.wpyr != nullptr;
                     if ( may_cut3( cells_dist2_3( P, x, x, px, py, pz ), P.wpyr ? wmaj_b( P, gc ) : wmax, R2s, wi ) ) {
                         int2 rg = P.cell_range[ gc ];
                         beg = rg.x;
                         cnt = rg.y - rg.x;
+                        ranged = true;
                     }
                 }
             }
-            cut_by_ranges3( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
+            if constexpr ( CNT ) if ( P.gather ) {
+                count_reads( P, lane, G_GRID, __popc( __ballot_sync( FULL3, tested ) ) );
+                count_reads( P, lane, G_RANGE, __popc( __ballot_sync( FULL3, ranged ) ) );
+            }
+            cut_by_ranges3<CNT>( C, P, lane, s, px, py, pz, wi, beg, cnt, overflow );
         }
         if ( C.nv == 0 || overflow ) break;
         double R2 = radius2_3( C, lane );
@@ -853,7 +869,7 @@ __device__ __noinline__ bool clip3( C3 &C, const ProbDev &P, int prob, int s, in
         if ( r * P.ghmin >= sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) ) break;
         if ( P.wpyr && r >= SHELLS_FIRST && r < rmax && sqrt( R2 ) + sqrt( ex > 0 ? ex : 0.0 ) > ( r + 2 ) * P.ghmin ) { rd = r; break; }
     }
-    if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3( C, P, lane, s, px, py, pz, wi, c0, rd, stk, overflow );
+    if ( rd >= 0 && C.nv > 0 && ! overflow ) walk_pyramid3<CNT>( C, P, lane, s, px, py, pz, wi, c0, rd, stk, overflow );
     const int user = P.user[ s ];
     if ( overflow ) {
         // past the capacity of this warp's cell: the next pass rebuilds it -- but a trial diagram does not go past the big
@@ -1094,10 +1110,10 @@ __device__ __noinline__ bool finish3( C3 &C, const ProbDev &P, int prob, int s, 
 }
 
 // THE CELL, both halves
-template<class C3>
+template<bool CNT, class C3>
 __device__ bool cell3( C3 &C, const ProbDev &P, int prob, int s, int lane, unsigned flags, ErrRec *err, OvfList *ovf, int2 *stk, double wmax,
                        double *rep, bool big ) {
-    if ( ! clip3( C, P, prob, s, lane, err, ovf, stk, wmax, big ) ) return false;
+    if ( ! clip3<CNT>( C, P, prob, s, lane, err, ovf, stk, wmax, big ) ) return false;
     return finish3( C, P, prob, s, lane, flags, err, ovf, rep, big );
 }
 
@@ -1169,6 +1185,7 @@ __device__ void load3( C3 &C, const Split3 &sp, long long at, int lane ) {
 // mode 2 (pass 2): the cells of a gaussian problem are clipped and stored by pass 1 and integrated by pass 2 (the report
 // too); the other problems are done whole by pass 1 and skipped by pass 2.  (The warps' cells, about 55 KB of shared
 // memory a block, hold 4 blocks on an SM: the registers are bounded for 4, not more.)
+template<bool CNT>
 __global__ void __launch_bounds__( 32 * W3, 4 ) k_cells3d( const ProbDev *__restrict__ probs, const Chunk *__restrict__ chunks, int nchunks,
                                                         unsigned flags, ErrRec *err, OvfList *ovf, int mode, Split3 sp ) {
     extern __shared__ char smem[];
@@ -1190,13 +1207,13 @@ __global__ void __launch_bounds__( 32 * W3, 4 ) k_cells3d( const ProbDev *__rest
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
         for ( int s = ch.begin + warp; s < ch.end; s += W3 ) {
             if ( ! two ) {
-                cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
+                cell3<CNT>( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
                 continue;
             }
             long long *slot = sp.slot + ( size_t ) cidx * CHUNK + ( s - ch.begin );
             if ( mode == 1 ) {
                 long long at = -2;                  // queued for the big-cell pass
-                if ( clip3( C, P, ch.prob, s, lane, err, ovf, sh_stk[ warp ], wmax, false ) ) at = store3( C, sp, lane );
+                if ( clip3<CNT>( C, P, ch.prob, s, lane, err, ovf, sh_stk[ warp ], wmax, false ) ) at = store3( C, sp, lane );
                 if ( lane == 0 ) *slot = at;
                 __syncwarp();
             } else {
@@ -1205,7 +1222,7 @@ __global__ void __launch_bounds__( 32 * W3, 4 ) k_cells3d( const ProbDev *__rest
                     load3( C, sp, at, lane );
                     finish3( C, P, ch.prob, s, lane, flags, err, ovf, rp, false );
                 } else if ( at == -1 )              // no room in pass 1: the whole cell here
-                    cell3( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
+                    cell3<CNT>( C, P, ch.prob, s, lane, flags, err, ovf, sh_stk[ warp ], wmax, rp, false );
             }
         }
         if ( report ) {
@@ -1247,7 +1264,7 @@ __global__ void __launch_bounds__( 32 ) k_cells3d_big( const ProbDev *__restrict
         if ( P.dim != 3 ) continue;
         const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
-        cell3( C, P, item.prob, item.seed, lane, fl, err, next, stk, wmax, nullptr, true );
+        cell3<false>( C, P, item.prob, item.seed, lane, fl, err, next, stk, wmax, nullptr, true );
     }
 }
 
@@ -1264,7 +1281,7 @@ __global__ void __launch_bounds__( 32 ) k_cells3d_giant( const ProbDev *__restri
         if ( P.dim != 3 ) continue;
         const unsigned fl = flags ? flags : ( P.first ? ( F_MOMENTS | F_USER_ORDER ) : ( F_MASS | F_FACETS ) );
         const double wmax = P.wmax_slot ? order_dbl( *P.wmax_slot ) : 0.0;
-        cell3( C, P, item.prob, item.seed, lane, fl, err, nullptr, stk, wmax, nullptr, true );
+        cell3<false>( C, P, item.prob, item.seed, lane, fl, err, nullptr, stk, wmax, nullptr, true );
     }
 }
 
@@ -1287,18 +1304,22 @@ void launch_cells3d( const Launch &L, const ProbDev *probs, const Chunk *chunks,
     const size_t smem = sizeof( Cell3 ) * W3;
     static bool configured = false;
     if ( ! configured ) {
-        cudaFuncSetAttribute( k_cells3d, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
-        cudaFuncSetAttribute( k_cells3d, cudaFuncAttributePreferredSharedMemoryCarveout, 100 );
+        for ( auto k : { k_cells3d<false>, k_cells3d<true> } ) {
+            cudaFuncSetAttribute( k, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) );
+            cudaFuncSetAttribute( k, cudaFuncAttributePreferredSharedMemoryCarveout, 100 );
+        }
         configured = true;
     }
+    // the counting instantiation only when the search's reads are counted (F_GATHER): the other compiles without them
+    auto *kern = ( flags & F_GATHER ) ? k_cells3d<true> : k_cells3d<false>;
     if ( ! sp ) {
-        k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 0, Split3{} );
+        kern<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 0, Split3{} );
         ++*L.launches;
         return;
     }
     cudaMemsetAsync( sp->used, 0, sizeof( unsigned long long ), L.stream );
-    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 1, *sp );
-    k_cells3d<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 2, *sp );
+    kern<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 1, *sp );
+    kern<<<nchunks, 32 * W3, smem, L.stream>>>( probs, chunks, nchunks, flags, err, ovf, 2, *sp );
     *L.launches += 2;
 }
 

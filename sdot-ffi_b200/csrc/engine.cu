@@ -78,6 +78,8 @@ void ctx_init( Ctx &c, int device, uint64_t pool_limit ) {
     CK( cudaMemsetAsync( c.dcount, 0, size_t( c.max_slots ) * 4 * sizeof( unsigned ), c.stream ) );
     c.derr = ( ErrRec * ) dalloc( c, sizeof( ErrRec ) );
     CK( cudaMemsetAsync( c.derr, 0, sizeof( ErrRec ), c.stream ) );
+    c.dgather = ( unsigned long long * ) dalloc( c, GATHER_BYTES );
+    CK( cudaMemsetAsync( c.dgather, 0, GATHER_BYTES, c.stream ) );
     CK( cudaMallocHost( &c.hscal, size_t( c.max_slots ) * SLOT_DOUBLES * 8 ) );
     CK( cudaMallocHost( &c.herr, sizeof( ErrRec ) ) );
     std::memset( c.herr, 0, sizeof( ErrRec ) );
@@ -113,6 +115,7 @@ void ctx_release( Ctx &c ) {
         if ( c.dscal ) cudaFreeAsync( c.dscal, c.stream );
         if ( c.dcount ) cudaFreeAsync( c.dcount, c.stream );
         if ( c.derr ) cudaFreeAsync( c.derr, c.stream );
+        if ( c.dgather ) cudaFreeAsync( c.dgather, c.stream );
         if ( c.dovf ) cudaFreeAsync( c.dovf, c.stream );
         if ( c.big_scratch ) cudaFreeAsync( c.big_scratch, c.stream );
         if ( c.dgiant ) cudaFreeAsync( c.dgiant, c.stream );

@@ -64,8 +64,14 @@ struct Ctx {
     Split3 split{};
     size_t split_slots = 0;
     Timer timer;
+    // the search's read counters of the standalone diagrams (sdot_cells) of dims 2 and 3, on request: [2][NB_GATHER][32]
+    // on the device, and the cells those diagrams built
+    unsigned long long *dgather = nullptr;
+    bool gather_on = false;
+    uint64_t gather_cells[ 2 ] = { 0, 0 };
     Launch L() { return Launch{ stream, &launches, &timer }; }
 };
+constexpr size_t GATHER_BYTES = size_t( 2 ) * NB_GATHER * GATHER_SLOTS * sizeof( unsigned long long );
 constexpr int SLOT_ERR = 2 * NB_REPORT + NB_SC;                 // a problem's capacity-failure flag
 constexpr int SLOT_AGG = SLOT_ERR + 1;                           // the near-coincident pairs its last Laplacian showed
 constexpr int SLOT_LIM = SLOT_AGG + 1;                           // the limits step: cells below the floor, smallest limit

@@ -46,7 +46,8 @@ enum DiagFlags : unsigned {
     F_REPORT = 16u,         // the Newton report (needs nu)
     F_USER_ORDER = 32u,     // write outputs at user index instead of rank
     F_VJP = 64u,            // adjoint gather (grad of masses)
-    F_FP32 = 128u           // FP32 clipping with FP64 re-check
+    F_FP32 = 128u,          // FP32 clipping with FP64 re-check
+    F_GATHER = 256u         // count the search's reads into ProbDev.gather (set with it)
 };
 
 constexpr int MAX_LEV = 24;      // levels of the weight majorants (grids up to 2^23 cells per side)
@@ -83,6 +84,7 @@ struct ProbDev {
     const double *nu;             // [n] ranked targets (report)
     const double *gm;             // [n] cotangent of masses (vjp), ranked (NULL: none)
     const double *gf;             // [n, dim] cotangent of the first moments int_cell x rho, world frame (vjp; NULL: none)
+    unsigned long long *gather;   // [NB_GATHER][32] the search's record reads (NULL: not counted), see count_reads
     double *gpos;                 // [n, dim] (vjp)
     double *gw;                   // [n] (vjp)
     double *report;               // [NB_REPORT] per problem (report)
@@ -221,6 +223,16 @@ constexpr int VCHUNK = 256;      // rows per chunk of the vector kernels (one bl
 // spreads over the 148 SMs.  A function of the problem alone: its reductions fold in the same order alone and in any batch
 inline int vec_chunk( long n ) { return n >= 148L * 2 * VCHUNK ? VCHUNK : ( n >= 148L * VCHUNK ? VCHUNK / 2 : VCHUNK / 4 ); }
 constexpr int MG_FUSE_ROWS = 4096;   // multigrid levels of at most this many rows run in one launch per problem (k_mg_fused)
+
+// ---- the search's reads, counted on request: the gather model of the cell kernels' traffic ------------------------
+// candidate seed records (position + weight), grid cells whose weight majorant was read, grid cells whose seed range
+// was read, pyramid node records (affine majorant); spread over 32 slots by block so the atomics do not queue on one word
+enum { G_CAND = 0, G_GRID, G_RANGE, G_NODE, NB_GATHER };
+constexpr int GATHER_SLOTS = 32;
+// `n` reads of kind `what` for the current cell: called by every lane of the warp, counted once
+SDOT_DEV void count_reads( const ProbDev &P, int lane, int what, unsigned n ) {
+    if ( lane == 0 && n ) atomicAdd( P.gather + what * GATHER_SLOTS + ( blockIdx.x & ( GATHER_SLOTS - 1 ) ), ( unsigned long long ) n );
+}
 
 // ---- warp helpers ------------------------------------------------------------------------------------
 SDOT_DEV double warp_sum( double v ) {

@@ -82,6 +82,8 @@ SIGNATURES = {
     "sdot_context_synchronize": (ctypes.c_int32, [_P, ctypes.POINTER(Status)]),
     "sdot_context_kernel_launches": (ctypes.c_uint64, [_P]),
     "sdot_context_set_timing": (ctypes.c_int32, [_P, ctypes.c_int32]),
+    "sdot_context_set_counters": (ctypes.c_int32, [_P, ctypes.c_int32]),
+    "sdot_context_gather_counters": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]),
     "sdot_context_memory": (ctypes.c_int32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                              ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]),
     "sdot_context_kernel_stats": (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64),
@@ -426,6 +428,23 @@ def kernel_stats(reset=False):
     if reset:
         L.sdot_context_kernel_stats(context(), 0, None, None, None, 1)
     return res
+
+
+GATHER_KINDS = ("cells", "candidates", "grid_cells", "grid_ranges", "nodes")
+
+
+def set_counters(on=True):
+    """count the neighbour search's record reads of every `cells` call (sdot_context_set_counters)"""
+    load().sdot_context_set_counters(context(), int(bool(on)))
+
+
+def gather_counters(dim, reset=False):
+    """{kind: count} of the `dim`-D diagrams since the last reset (sdot_context_gather_counters)"""
+    c = (ctypes.c_uint64 * 5)()
+    code = load().sdot_context_gather_counters(context(), int(dim), c, int(bool(reset)))
+    if code:
+        raise RuntimeError(f"sdot_context_gather_counters: code {code}")
+    return dict(zip(GATHER_KINDS, (int(x) for x in c)))
 
 
 def stream():

@@ -373,6 +373,38 @@ def test_the_adjoint_of_the_first_moments_is_their_derivative(d):
             assert abs(fd - gp[i, a]) < 1e-5 * scale, (i, a, fd, gp[i, a])
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_search_counters_leave_the_cells_unchanged(d):
+    """the gather model's device counters (sdot_context_set_counters): the counting instantiation of the cell kernel gives
+    the same cells bit for bit, its counts repeat exactly, every neighbour's seed is among the candidates read, the
+    spread weights send the search through the pyramid, and nothing is counted once the counters are off"""
+    from sdot import _lib
+    rng = np.random.default_rng(30 + d)
+    n = 20000
+    pos = rng.uniform(size=(n, d))
+    w = rng.uniform(0, 1e-3 if d == 2 else 3e-2, n)
+    pd = _pd(pos, w)
+    m0 = pd.measures
+    nb = pd.hessian_rows()[0]
+    _lib.gather_counters(d, reset=True)
+    _lib.set_counters(True)
+    try:
+        m1 = pd.measures
+        c1 = _lib.gather_counters(d, reset=True)
+        m2 = pd.measures
+        c2 = _lib.gather_counters(d, reset=True)
+    finally:
+        _lib.set_counters(False)
+    assert np.array_equal(m0, m1) and np.array_equal(m1, m2)
+    assert c1 == c2, (c1, c2)
+    assert c1["cells"] == n
+    assert c1["candidates"] >= nb.sum(), (c1, nb.sum())
+    assert c1["grid_ranges"] > 0 and c1["grid_cells"] > 0 and c1["nodes"] > 0, c1
+    print(f"\n{d}D n={n}: per cell " + ", ".join(f"{k} {v / n:.1f}" for k, v in c1.items() if k != "cells"))
+    pd.measures
+    assert _lib.gather_counters(d)["candidates"] == 0
+
+
 def test_the_3d_adjoint_is_the_derivative_of_the_measures():
     """gpu/Cell3D.cuh:1954-1978: the adjoint of the 3D masses (constant density) against central differences"""
     rng = np.random.default_rng(7)
