@@ -87,6 +87,19 @@ def test_calls_fail_loudly_without_a_device():
     assert st.message
 
 
+def test_the_counters_and_the_moments_adjoint_refuse_null_arguments():
+    """argument checks that come before any device work: a null context, a missing output, a dimension other than 2 or 3,
+    an adjoint with neither cotangent"""
+    L = _lib.load()
+    counts = (ctypes.c_uint64 * 5)()
+    assert L.sdot_context_set_counters(None, 1) == _lib.SDOT_ERR_ARGS
+    assert L.sdot_context_gather_counters(None, 2, counts, 0) == _lib.SDOT_ERR_ARGS
+    st = _lib.Status()
+    desc = _lib.DiagramDesc()
+    assert L.sdot_cells_vjp_moments(None, ctypes.byref(desc), None, None, None, None, ctypes.byref(st)) == _lib.SDOT_ERR_ARGS
+    assert st.code == _lib.SDOT_ERR_ARGS and st.message
+
+
 def _build_c_caller(tmp_path):
     libdir = os.path.dirname(_lib.LIB_PATH)
     exe = tmp_path / "c_caller"
